@@ -1,0 +1,159 @@
+"""ctypes / numpy mirrors of the structs declared in include/hw_b200.h.
+
+The numpy dtypes reproduce the byte layout of the C structs (checked against
+``sizeof`` by the tests), so lane buffers move between numpy, torch and the
+C ABI without conversion.
+"""
+import ctypes as C
+
+import numpy as np
+
+LANE = 64
+NUM_ANALOGS = 4
+NUM_BINS = 300
+NUM_STATES = 13
+LATENT_FRAMES = 24          # ViterbiStitchLookback + ROI lookForward + stitchFrames
+
+HW_OK = 0
+STATUS_NAMES = {
+    0: "HW_OK", 1: "HW_ERR_INVALID_ARG", 2: "HW_ERR_CUDA", 3: "HW_ERR_BAD_POOL",
+    4: "HW_ERR_FRAME_ORDER", 5: "HW_ERR_NOT_INITIALIZED", 6: "HW_ERR_UNSUPPORTED",
+    7: "HW_ERR_TIMEOUT", 8: "HW_ERR_OUT_OF_MEMORY", 9: "HW_ERR_NUMERIC",
+    10: "HW_ERR_INTERNAL",
+}
+
+FILTER_TYPES = {
+    "MultiScaleLarge": 0, "MultiScaleMedium": 1, "MultiScaleSmall": 2,
+    "TwoScaleLarge": 3, "TwoScaleMedium": 4, "TwoScaleSmall": 5,
+}
+FIXED_ESTIMATIONS, INITIAL_ESTIMATIONS, DYNAMIC_ESTIMATIONS = 0, 1, 2
+
+
+class Analog(C.Structure):
+    _fields_ = [
+        ("base_label", C.c_char),
+        ("rel_amplitude", C.c_float),
+        ("excess_noise_cv", C.c_float),
+        ("pulse_width_s", C.c_float),
+        ("ipd_s", C.c_float),
+        ("pw2_slow_step_ratio", C.c_float),
+        ("ipd2_slow_step_ratio", C.c_float),
+    ]
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("frame_rate", C.c_double),
+        ("photoelectron_sensitivity", C.c_float),
+        ("ref_snr", C.c_float),
+        ("shot_var_coeff", C.c_float),
+        ("pedestal", C.c_int16),
+        ("analogs", Analog * NUM_ANALOGS),
+        ("filter_type", C.c_int32),
+        ("mean_bias_adjust", C.c_float),
+        ("sigma_bias_adjust", C.c_float),
+        ("mean_ema_scale_strides", C.c_float),
+        ("sigma_ema_scale_strides", C.c_float),
+        ("jump_suppression", C.c_float),
+        ("bin_size_coeff", C.c_float),
+        ("bin_size_low_bound_coeff", C.c_float),
+        ("baseline_stat_min_frame_count", C.c_uint32),
+        ("fallback_baseline_sigma", C.c_float),
+        ("num_frames_pre_accum_stats", C.c_uint32),
+        ("min_frames_for_estimate", C.c_uint32),
+        ("analog_mix_fraction_threshold", C.c_float * 2),
+        ("scale_snr_conf_tol", C.c_float),
+        ("em_iteration_limit", C.c_uint32),
+        ("gtest_stat_factor", C.c_float),
+        ("iterate_to_limit", C.c_int32),
+        ("min_analog_snr_thresh0", C.c_float),
+        ("min_analog_snr_thresh1", C.c_float),
+        ("pulse_amp_regularization", C.c_float),
+        ("model_update_method", C.c_uint32),
+        ("snr_drop_thresh", C.c_float),
+        ("success_confidence_thresh", C.c_float),
+        ("confidence_half_life", C.c_float * 2),
+        ("viterbi_alpha", C.c_float),
+        ("viterbi_beta", C.c_float),
+        ("viterbi_gamma", C.c_float),
+        ("roi_filter_type", C.c_int32),
+        ("roi_upper_threshold", C.c_float),
+        ("roi_lower_threshold", C.c_float),
+        ("max_calls_per_zmw", C.c_uint32),
+        ("xsp_amp_thresh", C.c_double),
+        ("xsp_width_thresh", C.c_float),
+        ("model_estimation_mode", C.c_int32),
+        ("static_baseline_mean", C.c_float),
+        ("static_baseline_variance", C.c_float),
+    ]
+
+    def copy(self):
+        c = Config()
+        C.memmove(C.byref(c), C.byref(self), C.sizeof(Config))
+        return c
+
+
+class FrameInterval(C.Structure):
+    _fields_ = [("lower", C.c_int32), ("upper", C.c_int32)]
+
+    def __repr__(self):
+        return f"[{self.lower}, {self.upper})"
+
+    def tuple(self):
+        return (self.lower, self.upper)
+
+
+def _f32(n): return (np.float32, (n,))
+
+
+STAT_ACCUM_DT = np.dtype([("offset", np.float32, (LANE,)), ("moment0", np.float32, (LANE,)),
+                          ("moment1", np.float32, (LANE,)), ("moment2", np.float32, (LANE,))])
+AUTOCORR_DT = np.dtype([("basic_stats", STAT_ACCUM_DT), ("moment2", np.float32, (LANE,)),
+                        ("fbuf", np.float32, (4, LANE)), ("bbuf", np.float32, (4, LANE)),
+                        ("bidx", np.uint8, (2, LANE))])
+BLSTATS_DT = np.dtype([("full_autocorr", AUTOCORR_DT), ("trace_min", np.int16, (LANE,)),
+                       ("trace_max", np.int16, (LANE,)), ("baseline_stats", STAT_ACCUM_DT),
+                       ("raw_baseline_sum", np.float32, (LANE,)),
+                       ("background_stats", STAT_ACCUM_DT)])
+ANALOG_MODE_DT = np.dtype([("means", np.uint16, (LANE,)), ("vars", np.uint16, (LANE,)),
+                           ("weights", np.uint16, (LANE,))])
+LANE_MODEL_DT = np.dtype([("analogs", ANALOG_MODE_DT, (NUM_ANALOGS,)), ("baseline", ANALOG_MODE_DT),
+                          ("confidence", np.uint16, (LANE,))])
+LANE_HIST_DT = np.dtype([("low_bound", np.float32, (LANE,)), ("bin_size", np.float32, (LANE,)),
+                         ("outlier_count_low", np.uint16, (LANE,)),
+                         ("outlier_count_high", np.uint16, (LANE,)),
+                         ("bin_count", np.uint16, (NUM_BINS, LANE))])
+HIST_BOUNDS_DT = np.dtype([("upper_bounds", np.float32, (LANE,)), ("lower_bounds", np.float32, (LANE,))])
+PULSE_DT = np.dtype([("start", np.uint32), ("width", np.uint16), ("mean_signal", np.uint16),
+                     ("mid_signal", np.uint16), ("max_signal", np.uint16), ("signal_m2", np.float32),
+                     ("label", np.uint8), ("is_reject", np.uint8), ("pad_", np.uint8, (2,))])
+DME_DIAG_DT = np.dtype([("iter_count", np.int32, (LANE,)), ("converged", np.int32, (LANE,)),
+                        ("log_like", np.float32, (LANE,)), ("status", np.int32, (LANE,)),
+                        ("confidence", np.float32, (LANE,)), ("lane_iterations", np.int32),
+                        ("pad_", np.int32, (15,))])
+
+SIZES = {
+    "hw_stat_accum_state": (STAT_ACCUM_DT, 1024),
+    "hw_autocorr_accum_state": (AUTOCORR_DT, 3456),
+    "hw_baseliner_stats": (BLSTATS_DT, 6016),
+    "hw_lane_model": (LANE_MODEL_DT, 2048),
+    "hw_lane_histogram": (LANE_HIST_DT, 39168),
+    "hw_lane_hist_bounds": (HIST_BOUNDS_DT, 512),
+    "hw_pulse": (PULSE_DT, 20),
+    "hw_dme_diag": (DME_DIAG_DT, 1344),
+}
+
+
+def ptr(a):
+    """ctypes void pointer to a numpy array's data (or None)."""
+    if a is None:
+        return None
+    return C.c_void_p(a.ctypes.data)
+
+
+def f16_to_f32(bits):
+    return np.asarray(bits, dtype=np.uint16).view(np.float16).astype(np.float32)
+
+
+def f32_to_f16(x):
+    return np.asarray(x, dtype=np.float32).astype(np.float16).view(np.uint16)

@@ -1,0 +1,555 @@
+// C ABI of hw_b200: per-pool handles that own the device state of each filter
+// and launch the sm_100a kernels.  See include/hw_b200.h for the contract.
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "hw_device.cuh"
+
+
+using namespace hwk;
+
+namespace {
+
+thread_local std::string g_lastError = "";
+
+int Fail(int code, const std::string& msg)
+{
+    g_lastError = msg;
+    return code;
+}
+
+int CudaFail(cudaError_t e, const char* where)
+{
+    g_lastError = std::string(where) + ": " + cudaGetErrorString(e);
+    return HW_ERR_CUDA;
+}
+
+#define HW_CUDA(call, where) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) return CudaFail(e_, where); } while (0)
+
+template <typename T>
+int DevAlloc(T** p, size_t count, const char* where)
+{
+    *p = nullptr;
+    if (count == 0) return HW_OK;
+    cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+    if (e != cudaSuccess)
+    {
+        *p = nullptr;
+        if (e == cudaErrorMemoryAllocation) { cudaGetLastError(); return Fail(HW_ERR_OUT_OF_MEMORY, std::string(where) + ": out of device memory"); }
+        return CudaFail(e, where);
+    }
+    return HW_OK;
+}
+
+int PrepareConfig(const hw_config* cfg, hwp::Derived* d, KParams* k)
+{
+    if (!cfg) return Fail(HW_ERR_INVALID_ARG, "config is NULL");
+    std::string err;
+    if (!hwp::Validate(*cfg, &err)) return Fail(HW_ERR_INVALID_ARG, "invalid configuration: " + err);
+    if (!hwp::Derive(*cfg, d, &err)) return Fail(HW_ERR_INVALID_ARG, "invalid configuration: " + err);
+    if (cfg->gtest_stat_factor >= 0.0f)
+        return Fail(HW_ERR_UNSUPPORTED, "GTestStatFactor >= 0 (G-test confidence factor) is not built; the reference default is -1");
+    if (cfg->roi_filter_type != HW_ROI_DEFAULT)
+        return Fail(HW_ERR_UNSUPPORTED, "RoiFilterNoOp is not built; the reference default is RoiFilterDefault");
+    FillParams(*cfg, *d, k);
+    return HW_OK;
+}
+
+inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Reads back and clears a device error word (synchronous).
+int TakeDeviceError(int* dErr, cudaStream_t s, const char* where)
+{
+    int h = 0;
+    HW_CUDA(cudaMemcpyAsync(&h, dErr, sizeof(int), cudaMemcpyDeviceToHost, s), where);
+    HW_CUDA(cudaStreamSynchronize(s), where);
+    if (h != 0)
+    {
+        HW_CUDA(cudaMemsetAsync(dErr, 0, sizeof(int), s), where);
+        return h;
+    }
+    return HW_OK;
+}
+
+}   // namespace
+
+// ---------------------------------------------------------------------------
+
+struct hw_baseliner
+{
+    hw_config cfg;
+    hwp::Derived d;
+    KParams k;
+    uint32_t poolId = 0, lanes = 0, F = 0;
+    int slots16 = 0;
+    int16_t* st16 = nullptr;
+    float* st32 = nullptr;
+};
+
+struct hw_blstats_aggregator
+{
+    uint32_t poolId = 0, lanes = 0;
+    hw_baseliner_stats* acc = nullptr;
+    hw_frame_interval fi{0, 0};
+};
+
+struct hw_histogram
+{
+    hw_config cfg;
+    hwp::Derived d;
+    KParams k;
+    uint32_t poolId = 0, lanes = 0;
+    hw_lane_histogram* hist = nullptr;
+    int16_t* edgePrev = nullptr;
+    uint8_t* edgeBits = nullptr;
+    int* err = nullptr;
+    bool initialized = false;
+    hw_frame_interval fi{0, 0};
+};
+
+struct hw_dme
+{
+    hw_config cfg;
+    hwp::Derived d;
+    KParams k;
+    uint32_t poolId = 0, lanes = 0;
+    float* scratch = nullptr;
+    int* err = nullptr;
+};
+
+struct hw_labeler
+{
+    hw_config cfg;
+    hwp::Derived d;
+    KParams k;
+    uint32_t poolId = 0, lanes = 0, F = 0;
+    hw_lane_model* latModel = nullptr;
+    int16_t* latLabel = nullptr;
+    int16_t* latRoi = nullptr;
+    int16_t* latTrc = nullptr;
+    int16_t* prevLat = nullptr;
+    uint32_t* tb = nullptr;
+};
+
+struct hw_pulse_accumulator
+{
+    hw_config cfg;
+    hwp::Derived d;
+    KParams k;
+    uint32_t poolId = 0, lanes = 0, F = 0;
+    uint32_t* segStart = nullptr;
+    int16_t* segFirst = nullptr;
+    int16_t* segLast = nullptr;
+    int16_t* segMax = nullptr;
+    float* segTotal = nullptr;
+    float* segM2 = nullptr;
+    int16_t* segLabel = nullptr;
+};
+
+extern "C" {
+
+const char* hw_last_error_string(void) { return g_lastError.c_str(); }
+
+const char* hw_version(void) { return "hw_b200 0.1.0 (sm_100a)"; }
+
+int hw_config_default(hw_config* cfg)
+{
+    if (!cfg) return Fail(HW_ERR_INVALID_ARG, "config is NULL");
+    hwp::DefaultConfig(cfg);
+    return HW_OK;
+}
+
+int hw_config_validate(const hw_config* cfg)
+{
+    hwp::Derived d;
+    KParams k;
+    return PrepareConfig(cfg, &d, &k);
+}
+
+int hw_transition_matrix(const hw_config* cfg, float out[HW_NUM_STATES][HW_NUM_STATES])
+{
+    if (!cfg || !out) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    hwp::TransitionMatrix(*cfg, out);
+    return HW_OK;
+}
+
+uint32_t hw_labeler_latent_frames(void) { return (uint32_t)kLatent; }
+
+// ---- Baseliner -------------------------------------------------------------
+
+int hw_baseliner_create(const hw_config* cfg, uint32_t pool_id, uint32_t lanes, uint32_t frames_per_chunk,
+                        hw_baseliner** out)
+{
+    if (!out) return Fail(HW_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    auto b = std::make_unique<hw_baseliner>();
+    int rc = PrepareConfig(cfg, &b->d, &b->k);
+    if (rc) return rc;
+    if (lanes == 0) return Fail(HW_ERR_INVALID_ARG, "lanes must be positive");
+    if (frames_per_chunk == 0 || frames_per_chunk % (uint32_t)b->d.aggStride != 0)
+        return Fail(HW_ERR_INVALID_ARG, "frames_per_chunk must be a positive multiple of the filter's aggregate stride");
+    b->cfg = *cfg;
+    b->poolId = pool_id;
+    b->lanes = lanes;
+    b->F = frames_per_chunk;
+    b->slots16 = BaselinerNumSlots16(cfg->filter_type);
+    const size_t nZmw = (size_t)lanes * kLane;
+    if ((rc = DevAlloc(&b->st16, (size_t)b->slots16 * nZmw, "hw_baseliner_create"))) return rc;
+    if ((rc = DevAlloc(&b->st32, 3 * nZmw, "hw_baseliner_create"))) { cudaFree(b->st16); return rc; }
+    HW_CUDA(cudaMemset(b->st16, 0, (size_t)b->slots16 * nZmw * sizeof(int16_t)), "hw_baseliner_create");
+    std::vector<float> init(3 * nZmw, 0.0f);
+    for (size_t i = 0; i < nZmw; ++i) init[2 * nZmw + i] = 2.0f;   // blSigmaEma_ initial value
+    HW_CUDA(cudaMemcpy(b->st32, init.data(), init.size() * sizeof(float), cudaMemcpyHostToDevice), "hw_baseliner_create");
+    *out = b.release();
+    return HW_OK;
+}
+
+int hw_baseliner_destroy(hw_baseliner* b)
+{
+    if (!b) return HW_OK;
+    cudaFree(b->st16);
+    cudaFree(b->st32);
+    delete b;
+    return HW_OK;
+}
+
+int hw_baseliner_startup_latency(const hw_baseliner* b, uint32_t* frames)
+{
+    if (!b || !frames) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    *frames = b->d.baselinerStartupLatency;
+    return HW_OK;
+}
+
+int hw_baseliner_process(hw_baseliner* b, const int16_t* d_trace, int32_t first_frame, int16_t* d_out,
+                         hw_baseliner_stats* d_stats, void* stream)
+{
+    (void)first_frame;
+    if (!b || !d_trace || !d_out || !d_stats) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    BaselinerArgs a{d_trace, d_out, d_stats, b->st16, b->st32, (int)b->lanes, (int)b->F};
+    HW_CUDA(LaunchBaseliner(b->cfg.filter_type, a, b->k, S(stream)), "hw_baseliner_process");
+    return HW_OK;
+}
+
+// ---- Aggregator --------------------------------------------------------------
+
+int hw_blstats_aggregator_create(uint32_t pool_id, uint32_t lanes, hw_blstats_aggregator** out)
+{
+    if (!out || lanes == 0) return Fail(HW_ERR_INVALID_ARG, "bad argument");
+    *out = nullptr;
+    auto a = std::make_unique<hw_blstats_aggregator>();
+    a->poolId = pool_id;
+    a->lanes = lanes;
+    int rc = DevAlloc(&a->acc, lanes, "hw_blstats_aggregator_create");
+    if (rc) return rc;
+    HW_CUDA(LaunchAggReset(a->acc, (int)lanes, 0), "hw_blstats_aggregator_create");
+    HW_CUDA(cudaDeviceSynchronize(), "hw_blstats_aggregator_create");
+    *out = a.release();
+    return HW_OK;
+}
+
+int hw_blstats_aggregator_destroy(hw_blstats_aggregator* a)
+{
+    if (!a) return HW_OK;
+    cudaFree(a->acc);
+    delete a;
+    return HW_OK;
+}
+
+int hw_blstats_aggregator_add(hw_blstats_aggregator* a, const hw_baseliner_stats* d_stats, hw_frame_interval fi,
+                              void* stream)
+{
+    if (!a || !d_stats) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    const bool aEmpty = a->fi.lower == a->fi.upper, bEmpty = fi.lower == fi.upper;
+    if (!aEmpty && !bEmpty && a->fi.upper != fi.lower)
+        return Fail(HW_ERR_FRAME_ORDER, "baseliner metrics are not adjacent to the aggregated frame interval");
+    HW_CUDA(LaunchAggMerge(a->acc, d_stats, (int)a->lanes, S(stream)), "hw_blstats_aggregator_add");
+    if (aEmpty) a->fi = fi;
+    else if (!bEmpty) a->fi = hw_frame_interval{std::min(a->fi.lower, fi.lower), std::max(a->fi.upper, fi.upper)};
+    return HW_OK;
+}
+
+int hw_blstats_aggregator_get(const hw_blstats_aggregator* a, hw_baseliner_stats* d_out, hw_frame_interval* fi,
+                              void* stream)
+{
+    if (!a || !d_out) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    HW_CUDA(cudaMemcpyAsync(d_out, a->acc, sizeof(hw_baseliner_stats) * a->lanes, cudaMemcpyDeviceToDevice, S(stream)),
+            "hw_blstats_aggregator_get");
+    if (fi) *fi = a->fi;
+    return HW_OK;
+}
+
+int hw_blstats_aggregator_reset(hw_blstats_aggregator* a, void* stream)
+{
+    if (!a) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    HW_CUDA(LaunchAggReset(a->acc, (int)a->lanes, S(stream)), "hw_blstats_aggregator_reset");
+    a->fi = hw_frame_interval{0, 0};
+    return HW_OK;
+}
+
+// ---- Histogram ---------------------------------------------------------------
+
+int hw_histogram_create(const hw_config* cfg, uint32_t pool_id, uint32_t lanes, hw_histogram** out)
+{
+    if (!out) return Fail(HW_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    auto h = std::make_unique<hw_histogram>();
+    int rc = PrepareConfig(cfg, &h->d, &h->k);
+    if (rc) return rc;
+    if (lanes == 0) return Fail(HW_ERR_INVALID_ARG, "lanes must be positive");
+    h->cfg = *cfg;
+    h->poolId = pool_id;
+    h->lanes = lanes;
+    const size_t nZmw = (size_t)lanes * kLane;
+    if ((rc = DevAlloc(&h->hist, lanes, "hw_histogram_create"))) return rc;
+    if ((rc = DevAlloc(&h->edgePrev, nZmw, "hw_histogram_create"))) return rc;
+    if ((rc = DevAlloc(&h->edgeBits, nZmw, "hw_histogram_create"))) return rc;
+    if ((rc = DevAlloc(&h->err, 1, "hw_histogram_create"))) return rc;
+    HW_CUDA(cudaMemset(h->hist, 0, sizeof(hw_lane_histogram) * lanes), "hw_histogram_create");
+    HW_CUDA(cudaMemset(h->edgePrev, 0, nZmw * sizeof(int16_t)), "hw_histogram_create");
+    HW_CUDA(cudaMemset(h->edgeBits, 0, nZmw), "hw_histogram_create");
+    HW_CUDA(cudaMemset(h->err, 0, sizeof(int)), "hw_histogram_create");
+    *out = h.release();
+    return HW_OK;
+}
+
+int hw_histogram_destroy(hw_histogram* h)
+{
+    if (!h) return HW_OK;
+    cudaFree(h->hist);
+    cudaFree(h->edgePrev);
+    cudaFree(h->edgeBits);
+    cudaFree(h->err);
+    delete h;
+    return HW_OK;
+}
+
+int hw_histogram_add_batch(hw_histogram* h, const int16_t* d_traces, uint32_t frames, hw_frame_interval fi,
+                           const hw_lane_model* d_models, void* stream)
+{
+    if (!h || !d_traces || !d_models) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    if (!h->initialized)
+        return Fail(HW_ERR_NOT_INITIALIZED, "Cannot aggregate trace data into histograms before calling Reset with the desired histogram bounds");
+    const bool aEmpty = h->fi.lower == h->fi.upper, bEmpty = fi.lower == fi.upper;
+    if (!aEmpty && !bEmpty && h->fi.upper != fi.lower)
+        return Fail(HW_ERR_FRAME_ORDER, "trace batch is not adjacent to the histogram's frame interval");
+    HW_CUDA(LaunchHistAdd(h->hist, h->edgePrev, h->edgeBits, d_traces, (int)frames, d_models, (int)h->lanes, S(stream)),
+            "hw_histogram_add_batch");
+    if (aEmpty) h->fi = fi;
+    else if (!bEmpty) h->fi = hw_frame_interval{std::min(h->fi.lower, fi.lower), std::max(h->fi.upper, fi.upper)};
+    return HW_OK;
+}
+
+int hw_histogram_reset_from_stats(hw_histogram* h, const hw_baseliner_stats* d_stats, void* stream)
+{
+    if (!h || !d_stats) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    HW_CUDA(LaunchHistResetStats(h->hist, d_stats, (int)h->lanes, h->k, h->err, S(stream)), "hw_histogram_reset_from_stats");
+    h->initialized = true;
+    h->fi = hw_frame_interval{0, 0};
+    int e = TakeDeviceError(h->err, S(stream), "hw_histogram_reset_from_stats");
+    if (e) return Fail(e, "UHistogramSimd: lowerBound must be less than upperBound and bins must not underflow");
+    return HW_OK;
+}
+
+int hw_histogram_reset_from_bounds(hw_histogram* h, const hw_lane_hist_bounds* d_bounds, void* stream)
+{
+    if (!h || !d_bounds) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    HW_CUDA(LaunchHistResetBounds(h->hist, d_bounds, (int)h->lanes, h->err, S(stream)), "hw_histogram_reset_from_bounds");
+    h->initialized = true;
+    h->fi = hw_frame_interval{0, 0};
+    int e = TakeDeviceError(h->err, S(stream), "hw_histogram_reset_from_bounds");
+    if (e) return Fail(e, "UHistogramSimd: lowerBound must be less than upperBound and bins must not underflow");
+    return HW_OK;
+}
+
+int hw_histogram_get(const hw_histogram* h, hw_lane_histogram* d_out, hw_frame_interval* fi, void* stream)
+{
+    if (!h || !d_out) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    HW_CUDA(cudaMemcpyAsync(d_out, h->hist, sizeof(hw_lane_histogram) * h->lanes, cudaMemcpyDeviceToDevice, S(stream)),
+            "hw_histogram_get");
+    if (fi) *fi = h->fi;
+    return HW_OK;
+}
+
+// ---- DME -----------------------------------------------------------------------
+
+int hw_dme_create(const hw_config* cfg, uint32_t pool_id, uint32_t lanes, hw_dme** out)
+{
+    if (!out) return Fail(HW_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    auto d = std::make_unique<hw_dme>();
+    int rc = PrepareConfig(cfg, &d->d, &d->k);
+    if (rc) return rc;
+    if (lanes == 0) return Fail(HW_ERR_INVALID_ARG, "lanes must be positive");
+    d->cfg = *cfg;
+    d->poolId = pool_id;
+    d->lanes = lanes;
+    if ((rc = DevAlloc(&d->scratch, (size_t)lanes * 3 * (kBins + 1) * kLane, "hw_dme_create"))) return rc;
+    if ((rc = DevAlloc(&d->err, 1, "hw_dme_create"))) return rc;
+    HW_CUDA(cudaMemset(d->err, 0, sizeof(int)), "hw_dme_create");
+    *out = d.release();
+    return HW_OK;
+}
+
+int hw_dme_destroy(hw_dme* d)
+{
+    if (!d) return HW_OK;
+    cudaFree(d->scratch);
+    cudaFree(d->err);
+    delete d;
+    return HW_OK;
+}
+
+int hw_dme_init_models(hw_dme* d, const hw_baseliner_stats* d_stats, hw_lane_model* d_models, void* stream)
+{
+    if (!d || !d_stats || !d_models) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    HW_CUDA(LaunchInitModels(d_models, d_stats, (int)d->lanes, d->k, S(stream)), "hw_dme_init_models");
+    return HW_OK;
+}
+
+int hw_dme_estimate(hw_dme* d, const hw_lane_histogram* d_hist, const hw_baseliner_stats* d_stats,
+                    hw_frame_interval hist_fi, hw_frame_interval model_fi, hw_lane_model* d_models,
+                    hw_dme_diag* d_diag, void* stream)
+{
+    if (!d || !d_hist || !d_stats || !d_models) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    if (hist_fi.lower == hist_fi.upper || model_fi.lower == model_fi.upper)
+        return Fail(HW_ERR_INVALID_ARG, "frame intervals must not be empty");
+    DmeArgs a{d_hist, d_stats, d_models, d_diag, d->scratch, d->err, (int)d->lanes,
+              model_fi.lower + (model_fi.upper - model_fi.lower) / 2,
+              hist_fi.lower + (hist_fi.upper - hist_fi.lower) / 2};
+    HW_CUDA(LaunchDmeEstimate(a, d->k, S(stream)), "hw_dme_estimate");
+    int e = TakeDeviceError(d->err, S(stream), "hw_dme_estimate");
+    if (e) return Fail(e, "DME: a reference sanity assertion failed (non-finite estimate or bad SNR-drop threshold)");
+    return HW_OK;
+}
+
+// ---- Frame labeler ---------------------------------------------------------------
+
+int hw_labeler_create(const hw_config* cfg, uint32_t pool_id, uint32_t lanes, uint32_t frames_per_chunk,
+                      hw_labeler** out)
+{
+    if (!out) return Fail(HW_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    auto l = std::make_unique<hw_labeler>();
+    int rc = PrepareConfig(cfg, &l->d, &l->k);
+    if (rc) return rc;
+    if (lanes == 0) return Fail(HW_ERR_INVALID_ARG, "lanes must be positive");
+    if (frames_per_chunk < (uint32_t)(kLatent + kLookback) || frames_per_chunk > 1024)
+        return Fail(HW_ERR_INVALID_ARG, "frames_per_chunk must be in [40, 1024]");
+    l->cfg = *cfg;
+    l->poolId = pool_id;
+    l->lanes = lanes;
+    l->F = frames_per_chunk;
+    const size_t nZmw = (size_t)lanes * kLane;
+    if ((rc = DevAlloc(&l->latModel, lanes, "hw_labeler_create"))) return rc;
+    if ((rc = DevAlloc(&l->latLabel, nZmw, "hw_labeler_create"))) return rc;
+    if ((rc = DevAlloc(&l->latRoi, nZmw, "hw_labeler_create"))) return rc;
+    if ((rc = DevAlloc(&l->latTrc, nZmw, "hw_labeler_create"))) return rc;
+    if ((rc = DevAlloc(&l->prevLat, (size_t)kLatent * nZmw, "hw_labeler_create"))) return rc;
+    if ((rc = DevAlloc(&l->tb, (size_t)(frames_per_chunk + kLookback) * nZmw, "hw_labeler_create"))) return rc;
+    HW_CUDA(cudaMemset(l->latLabel, 0, nZmw * 2), "hw_labeler_create");
+    HW_CUDA(cudaMemset(l->latRoi, 0, nZmw * 2), "hw_labeler_create");
+    HW_CUDA(cudaMemset(l->latTrc, 0, nZmw * 2), "hw_labeler_create");
+    HW_CUDA(cudaMemset(l->prevLat, 0, (size_t)kLatent * nZmw * 2), "hw_labeler_create");
+    // LatentViterbi ctor (FrameLabelerHost.cpp:58-70): baseline N(0, 50), analogs N(1000, 10).
+    std::vector<hw_lane_model> m(lanes);
+    std::memset(m.data(), 0, sizeof(hw_lane_model) * lanes);
+    for (auto& lm : m)
+        for (int z = 0; z < kLane; ++z)
+        {
+            lm.baseline.means[z] = f32_to_f16_bits(0.0f);
+            lm.baseline.vars[z] = f32_to_f16_bits(50.0f);
+            for (int a = 0; a < kAnalogs; ++a)
+            {
+                lm.analogs[a].means[z] = f32_to_f16_bits(1000.0f);
+                lm.analogs[a].vars[z] = f32_to_f16_bits(10.0f);
+            }
+        }
+    HW_CUDA(cudaMemcpy(l->latModel, m.data(), sizeof(hw_lane_model) * lanes, cudaMemcpyHostToDevice), "hw_labeler_create");
+    *out = l.release();
+    return HW_OK;
+}
+
+int hw_labeler_destroy(hw_labeler* l)
+{
+    if (!l) return HW_OK;
+    cudaFree(l->latModel);
+    cudaFree(l->latLabel);
+    cudaFree(l->latRoi);
+    cudaFree(l->latTrc);
+    cudaFree(l->prevLat);
+    cudaFree(l->tb);
+    delete l;
+    return HW_OK;
+}
+
+int hw_labeler_process(hw_labeler* l, const int16_t* d_traces, const hw_lane_model* d_models, int16_t* d_labels,
+                       int16_t* d_latent_out, float* d_viterbi_score, void* stream)
+{
+    if (!l || !d_traces || !d_models || !d_labels) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    LabelerArgs a{d_traces, d_models, d_labels, d_latent_out, d_viterbi_score, l->latModel, l->latLabel, l->latRoi,
+                  l->latTrc, l->prevLat, l->tb, (int)l->lanes, (int)l->F};
+    HW_CUDA(LaunchLabeler(a, l->k, S(stream)), "hw_labeler_process");
+    return HW_OK;
+}
+
+// ---- Pulse accumulator -----------------------------------------------------------
+
+int hw_pulse_accumulator_create(const hw_config* cfg, uint32_t pool_id, uint32_t lanes, uint32_t frames_per_chunk,
+                                hw_pulse_accumulator** out)
+{
+    if (!out) return Fail(HW_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    auto p = std::make_unique<hw_pulse_accumulator>();
+    int rc = PrepareConfig(cfg, &p->d, &p->k);
+    if (rc) return rc;
+    if (lanes == 0 || frames_per_chunk < (uint32_t)kLatent) return Fail(HW_ERR_INVALID_ARG, "bad lanes or frames_per_chunk");
+    p->cfg = *cfg;
+    p->poolId = pool_id;
+    p->lanes = lanes;
+    p->F = frames_per_chunk;
+    const size_t nZmw = (size_t)lanes * kLane;
+    if ((rc = DevAlloc(&p->segStart, nZmw, "hw_pulse_accumulator_create"))) return rc;
+    if ((rc = DevAlloc(&p->segFirst, nZmw, "hw_pulse_accumulator_create"))) return rc;
+    if ((rc = DevAlloc(&p->segLast, nZmw, "hw_pulse_accumulator_create"))) return rc;
+    if ((rc = DevAlloc(&p->segMax, nZmw, "hw_pulse_accumulator_create"))) return rc;
+    if ((rc = DevAlloc(&p->segTotal, nZmw, "hw_pulse_accumulator_create"))) return rc;
+    if ((rc = DevAlloc(&p->segM2, nZmw, "hw_pulse_accumulator_create"))) return rc;
+    if ((rc = DevAlloc(&p->segLabel, nZmw, "hw_pulse_accumulator_create"))) return rc;
+    HW_CUDA(cudaMemset(p->segStart, 0, nZmw * 4), "hw_pulse_accumulator_create");
+    HW_CUDA(cudaMemset(p->segFirst, 0, nZmw * 2), "hw_pulse_accumulator_create");
+    HW_CUDA(cudaMemset(p->segLast, 0, nZmw * 2), "hw_pulse_accumulator_create");
+    HW_CUDA(cudaMemset(p->segMax, 0, nZmw * 2), "hw_pulse_accumulator_create");
+    HW_CUDA(cudaMemset(p->segTotal, 0, nZmw * 4), "hw_pulse_accumulator_create");
+    HW_CUDA(cudaMemset(p->segM2, 0, nZmw * 4), "hw_pulse_accumulator_create");
+    HW_CUDA(cudaMemset(p->segLabel, 0, nZmw * 2), "hw_pulse_accumulator_create");
+    *out = p.release();
+    return HW_OK;
+}
+
+int hw_pulse_accumulator_destroy(hw_pulse_accumulator* p)
+{
+    if (!p) return HW_OK;
+    cudaFree(p->segStart); cudaFree(p->segFirst); cudaFree(p->segLast); cudaFree(p->segMax);
+    cudaFree(p->segTotal); cudaFree(p->segM2); cudaFree(p->segLabel);
+    delete p;
+    return HW_OK;
+}
+
+int hw_pulse_accumulator_process(hw_pulse_accumulator* p, const int16_t* d_labels, const int16_t* d_latent_trace,
+                                 const int16_t* d_trace, int32_t first_frame, const hw_lane_model* d_models,
+                                 hw_pulse* d_pulses, uint32_t* d_lens, uint32_t* d_overflows,
+                                 hw_stat_accum_state* d_blstats, void* stream)
+{
+    if (!p || !d_labels || !d_latent_trace || !d_trace || !d_models || !d_pulses || !d_lens || !d_overflows || !d_blstats)
+        return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    PulseArgs a{d_labels, d_latent_trace, d_trace, d_models, d_pulses, d_lens, d_overflows, d_blstats,
+                p->segStart, p->segFirst, p->segLast, p->segMax, p->segTotal, p->segM2, p->segLabel,
+                (int)p->lanes, (int)p->F, (uint32_t)first_frame};
+    HW_CUDA(LaunchPulses(a, p->k, S(stream)), "hw_pulse_accumulator_process");
+    return HW_OK;
+}
+
+}   // extern "C"

@@ -1,0 +1,184 @@
+// Device-side helpers shared by the hw_b200 kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+
+#include "../../include/hw_b200.h"
+#include "hw_math.h"
+#include "hw_params.h"
+
+namespace hwk {
+
+using namespace hwm;
+
+constexpr int kLane = HW_LANE_SIZE;
+constexpr int kAnalogs = HW_NUM_ANALOGS;
+constexpr int kBins = HW_NUM_BINS;
+constexpr int kStates = HW_NUM_STATES;
+constexpr int kLatent = hwp::kLatentFrames;
+constexpr int kLookback = hwp::kViterbiStitchLookback;
+constexpr int kStitch = hwp::kRoiStitchFrames;
+
+__device__ __forceinline__ float h2f(uint16_t b) { return __half2float(__ushort_as_half(b)); }
+__device__ __forceinline__ uint16_t f2h(float f) { return __half_as_ushort(__float2half_rn(f)); }
+
+// Device error word shared by the kernels of one launch: the first failing
+// check stores its code; the host reads it after the launch.
+struct ErrWord
+{
+    int* p;
+    __device__ void Set(int code) const { if (p) atomicCAS(p, 0, code); }
+};
+
+// Per-run constants copied from hwp::Derived into kernel parameter space.
+struct KParams
+{
+    // baseliner
+    float cMeanBias, cSigmaBias, meanEmaAlpha, sigmaEmaAlpha, jumpTolCoeff, scaler;
+    int pedestal;
+    // histogram
+    float binSizeMin, binSizeCoeff, fallbackSigma;
+    float minFrameCount;
+    // dme
+    float blVarMin, blVarMax, blVarNominal, logTwoPi, minPulseMean, rpaSum2, rpaMin;
+    float shotVarCoeff, refSnr;
+    float relAmp[kAnalogs], cv2[kAnalogs];
+    float scaleSnrConfTol, pulseAmpReg, snrDropThresh, successConfThresh;
+    float snrThresh0, snrThresh1, amft0, amft1;
+    float halfLife0, halfLife1;
+    int emIterLimit, iterToLimit, updateMethod;
+    // labeler
+    float trans[kStates][kStates];
+    float sqrtHalfPi, sqrt2, sqrt3, roiUpper, roiLower;
+    // pulses
+    float ampThresh, widthThresh;
+    int maxCalls;
+    uint8_t analogMap[kAnalogs];
+};
+
+inline void FillParams(const hw_config& cfg, const hwp::Derived& d, KParams* k)
+{
+    k->cMeanBias = d.cMeanBias; k->cSigmaBias = d.cSigmaBias;
+    k->meanEmaAlpha = d.meanEmaAlpha; k->sigmaEmaAlpha = d.sigmaEmaAlpha;
+    k->jumpTolCoeff = d.jumpTolCoeff; k->scaler = d.scaler; k->pedestal = d.pedestal;
+    k->binSizeMin = d.binSizeMin; k->binSizeCoeff = cfg.bin_size_coeff;
+    k->fallbackSigma = cfg.fallback_baseline_sigma;
+    k->minFrameCount = (float)cfg.baseline_stat_min_frame_count;
+    k->blVarMin = d.blVarMin; k->blVarMax = d.blVarMax; k->blVarNominal = d.blVarNominal;
+    k->logTwoPi = d.logTwoPi; k->minPulseMean = d.minPulseMean; k->rpaSum2 = d.rpaSum2; k->rpaMin = d.rpaMin;
+    k->shotVarCoeff = cfg.shot_var_coeff; k->refSnr = cfg.ref_snr;
+    for (int a = 0; a < kAnalogs; ++a)
+    {
+        k->relAmp[a] = cfg.analogs[a].rel_amplitude;
+        const float cv = cfg.analogs[a].excess_noise_cv;
+        k->cv2[a] = cv * cv;
+        k->analogMap[a] = d.analogMap[a];
+    }
+    k->scaleSnrConfTol = cfg.scale_snr_conf_tol; k->pulseAmpReg = cfg.pulse_amp_regularization;
+    k->snrDropThresh = cfg.snr_drop_thresh; k->successConfThresh = cfg.success_confidence_thresh;
+    k->snrThresh0 = cfg.min_analog_snr_thresh0; k->snrThresh1 = cfg.min_analog_snr_thresh1;
+    k->amft0 = cfg.analog_mix_fraction_threshold[0]; k->amft1 = cfg.analog_mix_fraction_threshold[1];
+    k->halfLife0 = cfg.confidence_half_life[0]; k->halfLife1 = cfg.confidence_half_life[1];
+    k->emIterLimit = (int)cfg.em_iteration_limit; k->iterToLimit = cfg.iterate_to_limit;
+    k->updateMethod = (int)cfg.model_update_method;
+    for (int r = 0; r < kStates; ++r)
+        for (int c = 0; c < kStates; ++c) k->trans[r][c] = d.trans[r][c];
+    k->sqrtHalfPi = d.sqrtHalfPi; k->sqrt2 = d.sqrt2; k->sqrt3 = d.sqrt3;
+    k->roiUpper = cfg.roi_upper_threshold; k->roiLower = cfg.roi_lower_threshold;
+    k->ampThresh = d.ampThresh; k->widthThresh = d.widthThresh; k->maxCalls = (int)cfg.max_calls_per_zmw;
+}
+
+// ModelSignalCovar, DetectionModelHost.cpp:237-245
+__device__ __forceinline__ float SignalCovar(const KParams& k, float cv2, float mean, float blVar)
+{
+    float r = blVar;
+    r += k.shotVarCoeff * mean;
+    r += cv2 * (mean * mean);
+    return r;
+}
+
+// ---- kernel argument blocks and launchers ----------------------------------
+
+struct BaselinerArgs
+{
+    const int16_t* trace;        // [lanes][F][64]
+    int16_t* out;                // [lanes][F][64]
+    hw_baseliner_stats* stats;   // [lanes]
+    int16_t* st16;               // [NumI16Slots][nZmw]
+    float* st32;                 // [3][nZmw]
+    int lanes;
+    int F;
+};
+
+struct DmeArgs
+{
+    const hw_lane_histogram* hist;
+    const hw_baseliner_stats* stats;
+    hw_lane_model* models;
+    hw_dme_diag* diag;          // may be null
+    float* scratch;             // [lanes][3][kBins + 1][64]
+    int* err;
+    int lanes;
+    int32_t tModel, tEst;       // frame-interval centers (model, histogram)
+};
+
+struct LabelerArgs
+{
+    const int16_t* trace;         // [lanes][F][64]
+    const hw_lane_model* models;  // [lanes] new models
+    int16_t* labels;              // [lanes][F][64]
+    int16_t* latOut;              // [lanes][24][64] or null
+    float* score;                 // [lanes][64] or null
+    // state
+    hw_lane_model* latModel;      // [lanes]
+    int16_t* latLabel;            // [nZmw]
+    int16_t* latRoi;              // [nZmw]
+    int16_t* latTrc;              // [nZmw]
+    int16_t* prevLat;             // [lanes][24][64]
+    uint32_t* tb;                 // [lanes][F + 16][64] scratch
+    int lanes;
+    int F;
+};
+
+struct PulseArgs
+{
+    const int16_t* labels;        // [lanes][F][64]
+    const int16_t* latTrace;      // [lanes][24][64]
+    const int16_t* trace;         // [lanes][F][64]
+    const hw_lane_model* models;  // [lanes]
+    hw_pulse* pulses;             // [lanes][64][cap]
+    uint32_t* lens;               // [lanes][64]
+    uint32_t* ovf;                // [lanes][64]
+    hw_stat_accum_state* bls;     // [lanes]
+    // segment state, [nZmw] each
+    uint32_t* segStart;
+    int16_t* segFirst;
+    int16_t* segLast;
+    int16_t* segMax;
+    float* segTotal;
+    float* segM2;
+    int16_t* segLabel;
+    int lanes;
+    int F;
+    uint32_t firstFrame;
+};
+
+int BaselinerNumSlots16(int ft);
+cudaError_t LaunchBaseliner(int ft, const BaselinerArgs& a, const KParams& k, cudaStream_t s);
+cudaError_t LaunchAggReset(hw_baseliner_stats* s, int lanes, cudaStream_t st);
+cudaError_t LaunchAggMerge(hw_baseliner_stats* acc, const hw_baseliner_stats* in, int lanes, cudaStream_t st);
+cudaError_t LaunchHistResetStats(hw_lane_histogram* h, const hw_baseliner_stats* s, int lanes, const KParams& k,
+                                 int* err, cudaStream_t st);
+cudaError_t LaunchHistResetBounds(hw_lane_histogram* h, const hw_lane_hist_bounds* b, int lanes, int* err,
+                                  cudaStream_t st);
+cudaError_t LaunchHistAdd(hw_lane_histogram* h, int16_t* prev, uint8_t* bits, const int16_t* traces, int frames,
+                          const hw_lane_model* models, int lanes, cudaStream_t st);
+cudaError_t LaunchInitModels(hw_lane_model* m, const hw_baseliner_stats* s, int lanes, const KParams& k,
+                             cudaStream_t st);
+cudaError_t LaunchDmeEstimate(const DmeArgs& a, const KParams& k, cudaStream_t s);
+cudaError_t LaunchLabeler(const LabelerArgs& a, const KParams& k, cudaStream_t s);
+cudaError_t LaunchPulses(const PulseArgs& a, const KParams& k, cudaStream_t s);
+
+}   // namespace hwk

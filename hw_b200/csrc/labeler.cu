@@ -1,0 +1,355 @@
+// Frame labeler: ROI gating + 13-state subframe Viterbi for sm_100a.
+//
+// Restates TA/FrameLabelerHost.cpp:54-612, TA/SubframeScorer.h:152-318 and
+// TA/RoiHost.h:75-249 (TA = src/basecaller/basecaller/traceAnalysis).
+//
+// One thread per ZMW.  Per chunk a thread
+//   1. runs the ROI forward recursion over the 24 latent frames and the chunk,
+//      keeping the 2-bit ROI codes packed 16 per word in local memory, then
+//      the backward recursion (1 bit per frame);
+//   2. runs the max-plus Viterbi over 24 latent + F-8 chunk frames + 16
+//      look-ahead frames in fp32 with the reference's operation order and
+//      tie rule (a later source state wins ties);
+//   3. stores one 28-bit traceback word per frame: the arg-max source of each
+//      destination row, coded in 4 bits for the 9-way rows (baseline and the
+//      four pulse-up rows) and 1 bit for the 2-way rows (full and down);
+//   4. back-propagates the normalised end-state probabilities 16 frames,
+//      picks the anchor state and traces back F frames.
+// Traceback words live in a global scratch laid out [lane][frame][zmw] so
+// each warp writes and reads one 128-byte line per frame.
+#include "hw_device.cuh"
+
+namespace hwk {
+
+// BlockStateSubframeScorer for one ZMW (SubframeScorer.h:152-318).
+struct ZScorer
+{
+    float bgMean, bInvVar, bgFixed, x0;
+    float ffMean[4], pInvVar[4], ffFixed[4], logPMean[4], x1[4];
+    float fbMean, fbNormTerm, fbScale;
+
+    __device__ __forceinline__ void Setup(const KParams& k, const hw_lane_model& m, int z)
+    {
+        constexpr float log2pi_f = 1.8378770664f;
+        const float nhalf = -0.5f, halfVal = 0.5f, oneSixth = 1.0f / 6.0f;
+        const float bMean = h2f(m.baseline.means[z]);
+        const float bVar = h2f(m.baseline.vars[z]);
+        const float bSigma = sqrtf(bVar);
+        x0 = add_rn(bMean, mul_rn(bSigma, k.sqrtHalfPi));
+        bInvVar = 1.0f / bVar;
+#pragma unroll
+        for (int a = 0; a < kAnalogs; ++a)
+        {
+            const float aMean = h2f(m.analogs[a].means[z]);
+            logPMean[a] = hw_logf(aMean - bMean);
+            const float aVar = h2f(m.analogs[a].vars[z]);
+            const float aSigma = sqrtf(aVar);
+            x1[a] = aMean - mul_rn(aSigma, k.sqrtHalfPi);
+            pInvVar[a] = 1.0f / aVar;
+            ffFixed[a] = mul_rn(nhalf, hw_logf(aVar)) - log2pi_f / 2.0f;
+            ffMean[a] = aMean;
+        }
+        {
+            const float aMean = ffMean[3];
+            const float aVar = h2f(m.analogs[3].vars[z]);
+            const float eMean = mul_rn(halfVal, bMean + aMean);
+            float eVar = mul_rn(oneSixth, aMean - bMean);
+            eVar = add_rn(eVar, bVar + aVar);
+            eVar = mul_rn(eVar, halfVal);
+            fbMean = eMean;
+            fbNormTerm = mul_rn(-0.5f, add_rn(log2pi_f, hw_logf(eVar)));
+            fbScale = 0.5f / eVar;
+        }
+        bgFixed = mul_rn(nhalf, hw_logf(bVar)) - log2pi_f / 2.0f;
+        bgMean = bMean;
+    }
+
+    __device__ __forceinline__ float Subframe(int a, float val) const
+    {
+        const bool lowExtrema = val < x0;
+        const float cap = lowExtrema ? x0 : x1[a];
+        float fixedTerm = lowExtrema ? bInvVar : pInvVar[a];
+        fixedTerm = mul_rn(-0.5f, fixedTerm);
+        const bool extrema = lowExtrema | (val > x1[a]);
+        const float dv = val - cap;
+        float s = (extrema ? mul_rn(fixedTerm, mul_rn(dv, dv)) : 0.0f) - logPMean[a];
+        if (a == kAnalogs - 1)
+        {
+            const float dm = val - fbMean;
+            const float fb = fbNormTerm - mul_rn(mul_rn(dm, dm), fbScale);
+            s = (x0 <= x1[a]) ? s : fb;
+        }
+        return s;
+    }
+
+    // StateScores for states 0..8 (states 9..12 repeat 5..8).
+    __device__ __forceinline__ void Scores(float data, float* out) const
+    {
+        {
+            const float y = data - bgMean;
+            out[0] = add_rn(mul_rn(mul_rn(mul_rn(-0.5f, y), bInvVar), y), bgFixed);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+        {
+            const float y = data - ffMean[i];
+            out[1 + i] = add_rn(mul_rn(mul_rn(mul_rn(-0.5f, y), pInvVar[i]), y), ffFixed[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+        {
+            float score = Subframe(i, data);
+            score = (data > ffMean[i]) ? fmin_sse(fmin_sse(score, out[1 + i] - 1.0f), 0.0f) : score;
+            out[5 + i] = score;
+        }
+    }
+};
+
+// Max over a row: first entry, then the contiguous segment; ties go to the
+// later entry (Recursion, FrameLabelerHost.cpp:214-264).
+template <int R>
+__device__ __forceinline__ void ViterbiRow(const KParams& k, float score, const float* ll, float& outVal, int& outIdx)
+{
+    constexpr int first = (R == 0 || (R >= 5 && R <= 8)) ? 0 : (R <= 4 ? R : R - 8);
+    constexpr int sb = (R == 0 || (R >= 5 && R <= 8)) ? 5 : (R <= 4 ? R + 4 : R - 4);
+    constexpr int se = (R == 0 || (R >= 5 && R <= 8)) ? 13 : sb + 1;
+    float mv = add_rn(add_rn(score, k.trans[R][first]), ll[first]);
+    int idx = first;
+#pragma unroll
+    for (int p = sb; p < se; ++p)
+    {
+        const float v = add_rn(add_rn(score, k.trans[R][p]), ll[p]);
+        const bool c = v >= mv;
+        mv = c ? v : mv;
+        idx = c ? p : idx;
+    }
+    outVal = mv;
+    outIdx = idx;
+}
+
+// One Viterbi recursion step; returns the packed traceback word.
+__device__ __forceinline__ uint32_t ViterbiStep(const KParams& k, const ZScorer& sc, float data, bool isRoi, float* ll)
+{
+    float sco[9];
+    sc.Scores(data, sco);
+    float nl[kStates];
+    int idx[kStates];
+    ViterbiRow<0>(k, sco[0], ll, nl[0], idx[0]);
+    ViterbiRow<1>(k, sco[1], ll, nl[1], idx[1]);
+    ViterbiRow<2>(k, sco[2], ll, nl[2], idx[2]);
+    ViterbiRow<3>(k, sco[3], ll, nl[3], idx[3]);
+    ViterbiRow<4>(k, sco[4], ll, nl[4], idx[4]);
+    ViterbiRow<5>(k, sco[5], ll, nl[5], idx[5]);
+    ViterbiRow<6>(k, sco[6], ll, nl[6], idx[6]);
+    ViterbiRow<7>(k, sco[7], ll, nl[7], idx[7]);
+    ViterbiRow<8>(k, sco[8], ll, nl[8], idx[8]);
+    ViterbiRow<9>(k, sco[5], ll, nl[9], idx[9]);
+    ViterbiRow<10>(k, sco[6], ll, nl[10], idx[10]);
+    ViterbiRow<11>(k, sco[7], ll, nl[11], idx[11]);
+    ViterbiRow<12>(k, sco[8], ll, nl[12], idx[12]);
+    const float pen = isRoi ? 0.0f : __int_as_float(0x7f800000);
+    ll[0] = nl[0];
+#pragma unroll
+    for (int r = 1; r < kStates; ++r) ll[r] = nl[r] - pen;
+    uint32_t w = (idx[0] == 0) ? 0u : (uint32_t)(idx[0] - 4);
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+    {
+        const int i = idx[5 + u];
+        w |= ((i == 0) ? 0u : (uint32_t)(i - 4)) << (4 + 4 * u);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+    {
+        w |= (idx[1 + u] == 1 + u ? 0u : 1u) << (20 + u);
+        w |= (idx[9 + u] == 1 + u ? 0u : 1u) << (24 + u);
+    }
+    return w;
+}
+
+// Source state of `state` recorded in traceback word `w`.
+__device__ __forceinline__ int TraceSource(uint32_t w, int state)
+{
+    if (state == 0 || state >= 5 && state <= 8)
+    {
+        const int shift = (state == 0) ? 0 : 4 + 4 * (state - 5);
+        const int c = (w >> shift) & 15u;
+        return c == 0 ? 0 : c + 4;
+    }
+    if (state <= 4)
+    {
+        const int b = (w >> (20 + state - 1)) & 1u;
+        return b ? state + 4 : state;
+    }
+    const int b = (w >> (24 + state - 9)) & 1u;
+    return b ? state - 4 : state - 8;
+}
+
+
+constexpr int kMaxRoiWords = (1024 + 22 + 15) / 16;   // F up to 1024
+
+__global__ void __launch_bounds__(128) LabelerKernel(LabelerArgs A, KParams k)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= A.lanes * kLane) return;
+    const int l = g / kLane, z = g % kLane;
+    const int F = A.F;
+    const int nRoi = F + kLookback + kStitch;
+    const int16_t* chunk = A.trace + (size_t)l * F * kLane + z;
+    int16_t* pl = A.prevLat + (size_t)l * kLatent * kLane + z;
+    const hw_lane_model& oldM = A.latModel[l];
+    const hw_lane_model& newM = A.models[l];
+
+    // ---- ROI (ComputeRoi, FrameLabelerHost.cpp:267-309; RoiHost.h:110-249)
+    uint32_t roiw[kMaxRoiWords];
+    {
+        const float inv1 = 1.0f / sqrtf(h2f(oldM.baseline.vars[z]));
+        const float inv2 = 1.0f / sqrtf(h2f(newM.baseline.vars[z]));
+        float p0 = mul_rn((float)A.latTrc[g], inv1);
+        float p1 = mul_rn((float)pl[0], inv1);
+        float p2 = mul_rn((float)pl[kLane], inv1);
+        uint32_t prevRoi = (uint16_t)A.latRoi[g];
+        uint32_t word = 0;
+        int ri = 0;
+        auto process = [&](float sn) {
+            float mval = p1;
+            mval = fmax_sse(mval, (p0 + p1) / k.sqrt2);
+            mval = fmax_sse(mval, add_rn(p0 + p1, p2) / k.sqrt3);
+            mval = fmax_sse(mval, add_rn(add_rn(p0 + p1, p2), sn) / 2.0f);
+            const float thresh = (prevRoi & 1u) ? k.roiLower : k.roiUpper;
+            const uint32_t v = ((mval >= thresh) ? 1u : 0u) | ((mval >= k.roiLower) ? 2u : 0u);
+            word |= v << (2 * (ri & 15));
+            if ((ri & 15) == 15) { roiw[ri >> 4] = word; word = 0; }
+            ++ri;
+            prevRoi = v;
+            p0 = p1; p1 = p2; p2 = sn;
+        };
+        for (int i = hwp::kRoiLookForward; i < kLatent; ++i) process(mul_rn((float)pl[(size_t)i * kLane], inv1));
+        for (int i = 0; i < F; ++i) process(mul_rn((float)__ldg(chunk + (size_t)i * kLane), inv2));
+        if (ri & 15) roiw[ri >> 4] = word;
+        // Backward recursion: 2-bit codes become 0/1 (in place, bit 0 of each code).
+        uint32_t pr = 0;
+        for (int wi = (nRoi - 1) >> 4; wi >= 0; --wi)
+        {
+            uint32_t wv = roiw[wi];
+            uint32_t outw = 0;
+            const int hi = (wi == ((nRoi - 1) >> 4)) ? ((nRoi - 1) & 15) : 15;
+            for (int j = hi; j >= 0; --j)
+            {
+                const uint32_t code = (wv >> (2 * j)) & 3u;
+                const uint32_t b = (code & 1u) | (((code & 2u) != 0u) & (pr != 0u));
+                pr = b;
+                outw |= b << (2 * j);
+            }
+            roiw[wi] = outw;
+        }
+    }
+    auto roiBit = [&](int f) -> bool { return (roiw[f >> 4] >> (2 * (f & 15))) & 1u; };
+
+    // ---- Viterbi (LabelBlock, FrameLabelerHost.cpp:314-448)
+    float ll[kStates];
+    {
+        const int bc = A.latLabel[g];
+#pragma unroll
+        for (int i = 0; i < kStates; ++i) ll[i] = (bc == i) ? 0.0f : -__int_as_float(0x7f800000);
+    }
+    uint32_t* tb = A.tb + (size_t)l * (F + kLookback) * kLane + z;
+    ZScorer sc;
+    sc.Setup(k, oldM, z);
+    for (int f = 0; f < kLatent; ++f)
+        tb[(size_t)f * kLane] = ViterbiStep(k, sc, (float)pl[(size_t)f * kLane], roiBit(f), ll);
+    sc.Setup(k, newM, z);
+    const int anchor = F - kLatent;
+    for (int f = 0; f < anchor; ++f)
+        tb[(size_t)(f + kLatent) * kLane] = ViterbiStep(k, sc, (float)__ldg(chunk + (size_t)f * kLane), roiBit(f + kLatent), ll);
+    float anchorLL[kStates];
+#pragma unroll
+    for (int i = 0; i < kStates; ++i) anchorLL[i] = ll[i];
+    for (int f = anchor; f < anchor + kLookback; ++f)
+        tb[(size_t)(f + kLatent) * kLane] = ViterbiStep(k, sc, (float)__ldg(chunk + (size_t)f * kLane), roiBit(f + kLatent), ll);
+
+    // Normalize (FrameLabelerHost.cpp:186-205) and back-propagation.
+    float prob[kStates];
+    {
+        float mx = ll[0];
+#pragma unroll
+        for (int i = 1; i < kStates; ++i) mx = fmax_sse(ll[i], mx);
+        float sum = 0.0f;
+#pragma unroll
+        for (int i = 0; i < kStates; ++i) { prob[i] = hw_expf(ll[i] - mx); sum = add_rn(sum, prob[i]); }
+        const float inv = 1.0f / sum;
+#pragma unroll
+        for (int i = 0; i < kStates; ++i) prob[i] = mul_rn(prob[i], inv);
+    }
+    for (int i = F + kLookback - 1; i > F - 1; --i)
+    {
+        const uint32_t w = tb[(size_t)i * kLane];
+        float np[kStates];
+#pragma unroll
+        for (int s = 0; s < kStates; ++s) np[s] = 0.0f;
+#pragma unroll
+        for (int from = 0; from < kStates; ++from)
+        {
+            const int to = TraceSource(w, from);
+#pragma unroll
+            for (int s = 0; s < kStates; ++s) np[s] = (s == to) ? add_rn(np[s], prob[from]) : np[s];
+        }
+#pragma unroll
+        for (int s = 0; s < kStates; ++s) prob[s] = np[s];
+    }
+    float maxP = prob[0];
+    int anchorState = 0;
+#pragma unroll
+    for (int i = 1; i < kStates; ++i)
+    {
+        const bool c = maxP > prob[i];
+        maxP = c ? maxP : prob[i];
+        anchorState = c ? anchorState : i;
+    }
+    float ret = anchorLL[0];
+#pragma unroll
+    for (int i = 1; i < kStates; ++i) ret = (anchorState == i) ? anchorLL[i] : ret;
+
+    int ts = anchorState;
+    int16_t* out = A.labels + (size_t)l * F * kLane + z;
+    for (int f = F - 1; f >= 0; --f)
+    {
+        out[(size_t)f * kLane] = (int16_t)ts;
+        ts = TraceSource(tb[(size_t)f * kLane], ts);
+    }
+
+    // Latent state update.
+    A.latRoi[g] = (int16_t)roiBit(F - 1);
+    A.latLabel[g] = (int16_t)anchorState;
+    A.latTrc[g] = chunk[(size_t)(anchor - 1) * kLane];
+    if (A.score) A.score[g] = ret;
+    for (int f = 0; f < kLatent; ++f)
+    {
+        const int16_t v = pl[(size_t)f * kLane];
+        if (A.latOut) A.latOut[((size_t)l * kLatent + f) * kLane + z] = v;
+        pl[(size_t)f * kLane] = chunk[(size_t)(anchor + f) * kLane];
+    }
+}
+
+// The lane's old model is replaced by the new one after all its ZMWs used it.
+__global__ void LabelerModelCopyKernel(hw_lane_model* dst, const hw_lane_model* src, int lanes)
+{
+    const int n = lanes * (int)(sizeof(hw_lane_model) / 4);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) reinterpret_cast<uint32_t*>(dst)[i] = reinterpret_cast<const uint32_t*>(src)[i];
+}
+
+cudaError_t LaunchLabeler(const LabelerArgs& a, const KParams& k, cudaStream_t s)
+{
+    if (a.F > 1024) return cudaErrorInvalidValue;
+    const int threads = 128;
+    const int blocks = (a.lanes * kLane + threads - 1) / threads;
+    LabelerKernel<<<blocks, threads, 0, s>>>(a, k);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const int n = a.lanes * (int)(sizeof(hw_lane_model) / 4);
+    LabelerModelCopyKernel<<<(n + 255) / 256, 256, 0, s>>>(a.latModel, a.models, a.lanes);
+    return cudaGetLastError();
+}
+
+}   // namespace hwk

@@ -1,0 +1,294 @@
+// Baseline-statistics aggregation, trace histogram and model initialisation.
+//
+// Restates (TA = src/basecaller/basecaller/traceAnalysis, DT = .../dataTypes,
+// CM = .../common):
+//   TA/BaselineStatsAggregatorHost.cpp:37-45 + CM/AutocorrAccumulator.cpp:71-103
+//   TA/TraceHistogramAccumHost.cpp:82-169, TA/EdgeFrameClassifier.h:72-94,
+//   DT/UHistogramSimd.{h:199-229, cpp:51-97}
+//   TA/DmeEmHost.cpp:872-925 (InitLaneDetModel)
+// One thread per ZMW; lane structs are structure-of-arrays so every access is
+// a coalesced row of 64 values.
+#include "hw_device.cuh"
+
+namespace hwk {
+
+// ---- BaselinerStatAccumulator::Merge -------------------------------------
+
+__global__ void AggResetKernel(hw_baseliner_stats* s, int lanes)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= lanes * kLane) return;
+    const int l = g / kLane, z = g % kLane;
+    hw_baseliner_stats& S = s[l];
+    hw_stat_accum_state* st[3] = {&S.full_autocorr.basic_stats, &S.baseline_stats, &S.background_stats};
+    for (auto* p : st) { p->offset[z] = 0; p->moment0[z] = 0; p->moment1[z] = 0; p->moment2[z] = 0; }
+    S.full_autocorr.moment2[z] = 0;
+    for (int k = 0; k < 4; ++k) { S.full_autocorr.fbuf[k][z] = 0; S.full_autocorr.bbuf[k][z] = 0; }
+    S.full_autocorr.bidx[0][z] = 0;
+    S.full_autocorr.bidx[1][z] = 0;
+    S.trace_min[z] = 32767;
+    S.trace_max[z] = -32768;
+    S.raw_baseline_sum[z] = 0;
+}
+
+__global__ void AggMergeKernel(hw_baseliner_stats* acc, const hw_baseliner_stats* in, int lanes)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= lanes * kLane) return;
+    const int l = g / kLane, z = g % kLane;
+    hw_baseliner_stats& A = acc[l];
+    const hw_baseliner_stats& B = in[l];
+    auto mergeStat = [z](hw_stat_accum_state& a, const hw_stat_accum_state& b) {
+        a.moment0[z] += b.moment0[z];
+        a.moment1[z] += b.moment1[z];
+        a.moment2[z] += b.moment2[z];
+    };
+    // AutocorrAccumulator::Merge
+    mergeStat(A.full_autocorr.basic_stats, B.full_autocorr.basic_stats);
+    float m2 = A.full_autocorr.moment2[z] + B.full_autocorr.moment2[z];
+    const int tfbi = B.full_autocorr.bidx[0][z], tbbi = B.full_autocorr.bidx[1][z];
+    const int fbi = A.full_autocorr.bidx[0][z], bbi = A.full_autocorr.bidx[1][z];
+    const int n1 = 4 - tfbi;
+    for (int k = 0; k < 4 - n1; ++k)
+    {
+        const int i = (bbi + k) % 4, j = (tbbi + n1 + k) % 4;
+        m2 = add_rn(m2, mul_rn(A.full_autocorr.bbuf[i][z], B.full_autocorr.fbuf[k][z]));
+        A.full_autocorr.bbuf[i][z] = B.full_autocorr.bbuf[j][z];
+    }
+    const int n2 = 4 - fbi;
+    for (int k = 0; k < n2; ++k) A.full_autocorr.fbuf[fbi + k][z] = B.full_autocorr.fbuf[k][z];
+    A.full_autocorr.moment2[z] = m2;
+    A.full_autocorr.bidx[0][z] = (uint8_t)(fbi + n2);
+    A.full_autocorr.bidx[1][z] = (uint8_t)((bbi + (4 - n1)) % 4);
+    A.trace_min[z] = min(A.trace_min[z], B.trace_min[z]);
+    A.trace_max[z] = max(A.trace_max[z], B.trace_max[z]);
+    mergeStat(A.baseline_stats, B.baseline_stats);
+    A.raw_baseline_sum[z] += B.raw_baseline_sum[z];
+    mergeStat(A.background_stats, B.background_stats);
+}
+
+// StatAccumulator::Mean / Variance (CM/StatAccumulator.h:85-97)
+__device__ __forceinline__ float StatMean(const hw_stat_accum_state& s, int z)
+{
+    return s.moment1[z] / s.moment0[z] + s.offset[z];
+}
+
+__device__ __forceinline__ float StatVariance(const hw_stat_accum_state& s, int z)
+{
+    const float m0 = s.moment0[z], m1 = s.moment1[z], m2 = s.moment2[z];
+    float var = mul_rn(m1, m1) / m0;
+    var = (m2 - var) / (m0 - 1.0f);
+    var = fmax_sse(var, 0.0f);
+    return (m0 > 1.0f) ? var : __int_as_float(0x7fffffff);
+}
+
+// ---- Histogram ------------------------------------------------------------
+
+// UHistogramSimd ctor checks (UHistogramSimd.cpp:66-96).
+__device__ __forceinline__ bool HistBoundsOk(float lo, float up, float bs)
+{
+    bool ok = !(lo >= up) && !(bs <= 0.0f);
+    float prev = lo;
+    for (int i = 1; i <= kBins; ++i)
+    {
+        const float si = add_rn(mul_rn(bs, (float)i), lo);
+        ok &= !(prev == si);
+        prev = si;
+    }
+    return ok;
+}
+
+__device__ __forceinline__ void HistClear(hw_lane_histogram& H, int z)
+{
+    H.outlier_count_low[z] = 0;
+    H.outlier_count_high[z] = 0;
+    for (int b = 0; b < kBins; ++b) H.bin_count[b][z] = 0;
+}
+
+// TraceHistogramAccumHost::ResetImpl(const BaselinerMetrics&), :96-126
+__global__ void HistResetStatsKernel(hw_lane_histogram* hist, const hw_baseliner_stats* stats, int lanes,
+                                     KParams k, int* err)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= lanes * kLane) return;
+    const int l = g / kLane, z = g % kLane;
+    const hw_stat_accum_state& s = stats[l].baseline_stats;
+    const bool suff = s.moment0[z] >= k.minFrameCount;
+    const float mean = suff ? StatMean(s, z) : 0.0f;
+    const float sigma = suff ? sqrtf(StatVariance(s, z)) : k.fallbackSigma;
+    const float binSize = fmax_sse(mul_rn(k.binSizeCoeff, sigma), k.binSizeMin);
+    const float lo = mean - mul_rn(4.0f, sigma);
+    const float up = add_rn(lo, mul_rn(float(kBins), binSize));
+    const float bs = (up - lo) / static_cast<float>(kBins);
+    hw_lane_histogram& H = hist[l];
+    H.low_bound[z] = lo;
+    H.bin_size[z] = bs;
+    HistClear(H, z);
+    if (!HistBoundsOk(lo, up, bs)) atomicCAS(err, 0, HW_ERR_NUMERIC);
+}
+
+// TraceHistogramAccumHost::ResetImpl(const UnifiedCudaArray<LaneHistBounds>&), :82-94
+__global__ void HistResetBoundsKernel(hw_lane_histogram* hist, const hw_lane_hist_bounds* b, int lanes, int* err)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= lanes * kLane) return;
+    const int l = g / kLane, z = g % kLane;
+    const float lo = b[l].lower_bounds[z], up = b[l].upper_bounds[z];
+    const float bs = (up - lo) / static_cast<float>(kBins);
+    hist[l].low_bound[z] = lo;
+    hist[l].bin_size[z] = bs;
+    HistClear(hist[l], z);
+    if (!HistBoundsOk(lo, up, bs)) atomicCAS(err, 0, HW_ERR_NUMERIC);
+}
+
+// Edge classifier state per ZMW: prev frame and a two-deep baseline history.
+struct EdgeState
+{
+    int16_t* prev;      // [nZmw]
+    uint8_t* bits;      // [nZmw]: bit0 isBl(t-1), bit1 isBl(t-2), bits 2-3 count (0..2)
+};
+
+constexpr int kHistLanesPerBlock = 2;
+
+// AddBlock (TraceHistogramAccumHost.cpp:140-169): edge scrubbing with the fp16
+// baseline mode, then UHistogramSimd::AddDatum.  Counts of the lane are held
+// in shared memory for the chunk (one u16 per bin and ZMW; each thread only
+// touches its own ZMW's column, so no atomics are needed).
+__global__ void __launch_bounds__(kLane * kHistLanesPerBlock)
+HistAddKernel(hw_lane_histogram* hist, EdgeState es, const int16_t* traces, int frames,
+              const hw_lane_model* models, int lanes)
+{
+    extern __shared__ uint16_t histSmem[];
+    auto cnt = reinterpret_cast<uint16_t (*)[kBins + 1][kLane]>(histSmem);
+    const int ll = threadIdx.x / kLane, z = threadIdx.x % kLane;
+    const int l = blockIdx.x * kHistLanesPerBlock + ll;
+    if (l >= lanes) return;    // whole lanes only: no block-wide sync below
+    const int g = l * kLane + z;
+    hw_lane_histogram& H = hist[l];
+    for (int b = 0; b < kBins; ++b) cnt[ll][b][z] = H.bin_count[b][z];
+    uint16_t nLow = H.outlier_count_low[z], nHigh = H.outlier_count_high[z];
+    const float lower = H.low_bound[z], binSize = H.bin_size[z];
+    const float bm = h2f(models[l].baseline.means[z]);
+    const float bv = h2f(models[l].baseline.vars[z]);
+    const int16_t thr = i16_wrap(cvt_rn_i32(add_rn(mul_rn(2.0f, sqrtf(bv)), bm)));
+    int16_t prev = es.prev[g];
+    uint8_t bits = es.bits[g];
+    bool b1 = bits & 1, b2 = (bits >> 1) & 1;
+    int n = (bits >> 2) & 3;
+    const int16_t* tr = traces + (size_t)l * frames * kLane + z;
+    for (int f = 0; f < frames; ++f)
+    {
+        const int16_t x = __ldg(tr + (size_t)f * kLane);
+        const bool isBl = x < thr;
+        const bool edge = (n == 2) ? (isBl ^ b2) : true;
+        const float xv = (float)prev;
+        prev = x;
+        b2 = b1; b1 = isBl; n = (n < 2) ? n + 1 : 2;
+        const bool sel = !edge;
+        int bin = floor_cast_i32((xv - lower) / binSize);
+        const bool mLow = sel & (bin < 0);
+        const bool mHigh = sel & (bin >= kBins);
+        nLow = (uint16_t)(nLow + (mLow ? 1 : 0));
+        nHigh = (uint16_t)(nHigh + (mHigh ? 1 : 0));
+        if ((!sel) | mLow | mHigh) bin = kBins;
+        cnt[ll][bin][z] = (uint16_t)(cnt[ll][bin][z] + 1);
+    }
+    for (int b = 0; b < kBins; ++b) H.bin_count[b][z] = cnt[ll][b][z];
+    H.outlier_count_low[z] = nLow;
+    H.outlier_count_high[z] = nHigh;
+    es.prev[g] = prev;
+    es.bits[g] = (uint8_t)((b1 ? 1 : 0) | (b2 ? 2 : 0) | (n << 2));
+}
+
+// ---- DmeEmHost::InitLaneDetModel (DmeEmHost.cpp:872-925) ------------------
+
+__global__ void InitModelsKernel(hw_lane_model* models, const hw_baseliner_stats* stats, int lanes, KParams k,
+                                 int fixedModel, float fixedMean, float fixedVar)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= lanes * kLane) return;
+    const int l = g / kLane, z = g % kLane;
+    hw_lane_model& m = models[l];
+    if (fixedModel)
+    {
+        // FixedModelBatchAnalyzer (BatchAnalyzer.cpp:77-101) sets means and
+        // variances only; weights and confidence keep their values.
+        return;
+    }
+    const hw_stat_accum_state& bl = stats[l].baseline_stats;
+    const float blWeight = bl.moment0[z] / stats[l].full_autocorr.basic_stats.moment0[z];
+    float blMean = StatMean(bl, z);
+    float blVar = StatVariance(bl, z);
+    blMean = isnan(blMean) ? 0.0f : blMean;
+    blVar = isnan(blVar) ? 100.0f : blVar;
+    blVar = fmin_sse(fmax_sse(blVar, k.blVarMin), k.blVarMax);
+    m.confidence[z] = f2h(0.1f);
+    m.baseline.weights[z] = f2h(blWeight);
+    m.baseline.means[z] = f2h(blMean);
+    m.baseline.vars[z] = f2h(blVar);
+    const float amw = (1.0f - blWeight) / (float)kAnalogs;
+    const float refSignal = mul_rn(k.refSnr, sqrtf(blVar));
+    for (int a = 0; a < kAnalogs; ++a)
+    {
+        m.analogs[a].weights[z] = f2h(amw);
+        const float aMean = fmax_sse(0.0f, add_rn(blMean, mul_rn(k.relAmp[a], refSignal)));
+        m.analogs[a].means[z] = f2h(aMean);
+        m.analogs[a].vars[z] = f2h(SignalCovar(k, k.cv2[a], aMean, blVar));
+    }
+}
+
+// ---- launchers -------------------------------------------------------------
+
+static inline int Blocks(int lanes, int threads) { return (lanes * kLane + threads - 1) / threads; }
+
+cudaError_t LaunchAggReset(hw_baseliner_stats* s, int lanes, cudaStream_t st)
+{
+    AggResetKernel<<<Blocks(lanes, 256), 256, 0, st>>>(s, lanes);
+    return cudaGetLastError();
+}
+
+cudaError_t LaunchAggMerge(hw_baseliner_stats* acc, const hw_baseliner_stats* in, int lanes, cudaStream_t st)
+{
+    AggMergeKernel<<<Blocks(lanes, 256), 256, 0, st>>>(acc, in, lanes);
+    return cudaGetLastError();
+}
+
+cudaError_t LaunchHistResetStats(hw_lane_histogram* h, const hw_baseliner_stats* s, int lanes, const KParams& k,
+                                 int* err, cudaStream_t st)
+{
+    HistResetStatsKernel<<<Blocks(lanes, 128), 128, 0, st>>>(h, s, lanes, k, err);
+    return cudaGetLastError();
+}
+
+cudaError_t LaunchHistResetBounds(hw_lane_histogram* h, const hw_lane_hist_bounds* b, int lanes, int* err,
+                                  cudaStream_t st)
+{
+    HistResetBoundsKernel<<<Blocks(lanes, 128), 128, 0, st>>>(h, b, lanes, err);
+    return cudaGetLastError();
+}
+
+cudaError_t LaunchHistAdd(hw_lane_histogram* h, int16_t* prev, uint8_t* bits, const int16_t* traces, int frames,
+                          const hw_lane_model* models, int lanes, cudaStream_t st)
+{
+    EdgeState es{prev, bits};
+    const int blocks = (lanes + kHistLanesPerBlock - 1) / kHistLanesPerBlock;
+    const size_t smem = sizeof(uint16_t) * kHistLanesPerBlock * (kBins + 1) * kLane;
+    static bool attrSet = false;
+    if (!attrSet)
+    {
+        cudaError_t e = cudaFuncSetAttribute(HistAddKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attrSet = true;
+    }
+    HistAddKernel<<<blocks, kLane * kHistLanesPerBlock, smem, st>>>(h, es, traces, frames, models, lanes);
+    return cudaGetLastError();
+}
+
+cudaError_t LaunchInitModels(hw_lane_model* m, const hw_baseliner_stats* s, int lanes, const KParams& k,
+                             cudaStream_t st)
+{
+    InitModelsKernel<<<Blocks(lanes, 128), 128, 0, st>>>(m, s, lanes, k, 0, 0.0f, 0.0f);
+    return cudaGetLastError();
+}
+
+}   // namespace hwk

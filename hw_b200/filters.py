@@ -1,0 +1,195 @@
+"""Host-side mirrors of the reference's per-pool filter interfaces.
+
+Each class wraps one C-ABI handle and keeps the reference's method names and
+argument meaning (src/basecaller/basecaller/traceAnalysis):
+
+  Baseliner                  Baseliner.h:53-79 (operator(), StartupLatency)
+  BaselineStatsAggregator    BaselineStatsAggregator.h:45-104
+  TraceHistogramAccumulator  TraceHistogramAccumulator.h:96-154
+  DmeEmEstimator             CoreDMEstimator.h:151-162 (InitDetectionModels, Estimate)
+  FrameLabeler               FrameLabeler.h:67-74
+  PulseAccumulator           PulseAccumulator.h:68-74
+
+Device buffers are torch CUDA tensors (torch only provides device memory and
+the stream); all computation happens in libhw_b200.so.
+"""
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import abi
+from .native import check, lib
+
+
+def _stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _p(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+def struct_buffer(dtype, n, device="cuda"):
+    """Uninitialised device buffer for n structs of a numpy structured dtype."""
+    return torch.empty(n * dtype.itemsize, dtype=torch.uint8, device=device)
+
+
+def struct_to_numpy(t, dtype):
+    return t.detach().cpu().numpy().view(dtype)
+
+
+def numpy_to_struct(a, device="cuda"):
+    return torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).reshape(-1).copy()).to(device)
+
+
+class _Handle:
+    _destroy = None
+
+    def __init__(self):
+        self._h = C.c_void_p()
+
+    def close(self):
+        if self._h and self._h.value:
+            getattr(lib(), self._destroy)(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Baseliner(_Handle):
+    _destroy = "hw_baseliner_destroy"
+
+    def __init__(self, cfg, pool_id, lanes, frames_per_chunk):
+        super().__init__()
+        self.lanes, self.F = lanes, frames_per_chunk
+        check(lib().hw_baseliner_create(C.byref(cfg), pool_id, lanes, frames_per_chunk, C.byref(self._h)))
+
+    def startup_latency(self):
+        v = C.c_uint32()
+        check(lib().hw_baseliner_startup_latency(self._h, C.byref(v)))
+        return v.value
+
+    def __call__(self, trace, first_frame, out=None, stats=None):
+        """Returns (baseline-subtracted traces, per-lane BaselinerStatAccumState)."""
+        assert trace.dtype == torch.int16 and trace.is_cuda and trace.is_contiguous()
+        out = torch.empty_like(trace) if out is None else out
+        stats = struct_buffer(abi.BLSTATS_DT, self.lanes) if stats is None else stats
+        check(lib().hw_baseliner_process(self._h, _p(trace), int(first_frame), _p(out), _p(stats), _stream()))
+        return out, stats
+
+
+class BaselineStatsAggregator(_Handle):
+    _destroy = "hw_blstats_aggregator_destroy"
+
+    def __init__(self, pool_id, lanes):
+        super().__init__()
+        self.lanes = lanes
+        check(lib().hw_blstats_aggregator_create(pool_id, lanes, C.byref(self._h)))
+
+    def add_metrics(self, stats, frame_interval):
+        check(lib().hw_blstats_aggregator_add(self._h, _p(stats), abi.FrameInterval(*frame_interval), _stream()))
+
+    def trace_stats(self):
+        out = struct_buffer(abi.BLSTATS_DT, self.lanes)
+        fi = abi.FrameInterval()
+        check(lib().hw_blstats_aggregator_get(self._h, _p(out), C.byref(fi), _stream()))
+        return out, fi.tuple()
+
+    def reset(self):
+        check(lib().hw_blstats_aggregator_reset(self._h, _stream()))
+
+
+class TraceHistogramAccumulator(_Handle):
+    _destroy = "hw_histogram_destroy"
+
+    def __init__(self, cfg, pool_id, lanes):
+        super().__init__()
+        self.lanes = lanes
+        check(lib().hw_histogram_create(C.byref(cfg), pool_id, lanes, C.byref(self._h)))
+
+    def add_batch(self, traces, frame_interval, models):
+        frames = traces.shape[1]
+        check(lib().hw_histogram_add_batch(self._h, _p(traces), frames, abi.FrameInterval(*frame_interval),
+                                           _p(models), _stream()))
+
+    def reset_from_stats(self, stats):
+        check(lib().hw_histogram_reset_from_stats(self._h, _p(stats), _stream()))
+
+    def reset_from_bounds(self, bounds):
+        check(lib().hw_histogram_reset_from_bounds(self._h, _p(bounds), _stream()))
+
+    def histogram(self):
+        out = struct_buffer(abi.LANE_HIST_DT, self.lanes)
+        fi = abi.FrameInterval()
+        check(lib().hw_histogram_get(self._h, _p(out), C.byref(fi), _stream()))
+        return out, fi.tuple()
+
+
+class DmeEmEstimator(_Handle):
+    _destroy = "hw_dme_destroy"
+
+    def __init__(self, cfg, pool_id, lanes):
+        super().__init__()
+        self.lanes = lanes
+        check(lib().hw_dme_create(C.byref(cfg), pool_id, lanes, C.byref(self._h)))
+
+    def init_detection_models(self, stats, models=None):
+        models = struct_buffer(abi.LANE_MODEL_DT, self.lanes) if models is None else models
+        check(lib().hw_dme_init_models(self._h, _p(stats), _p(models), _stream()))
+        return models
+
+    def estimate(self, hist, hist_fi, stats, models, model_fi, diag=True):
+        """Updates `models` in place; returns per-lane hw_dme_diag (device) or None."""
+        d = struct_buffer(abi.DME_DIAG_DT, self.lanes) if diag else None
+        check(lib().hw_dme_estimate(self._h, _p(hist), _p(stats), abi.FrameInterval(*hist_fi),
+                                    abi.FrameInterval(*model_fi), _p(models), _p(d), _stream()))
+        return d
+
+
+class FrameLabeler(_Handle):
+    _destroy = "hw_labeler_destroy"
+
+    def __init__(self, cfg, pool_id, lanes, frames_per_chunk):
+        super().__init__()
+        self.lanes, self.F = lanes, frames_per_chunk
+        self.latent_frames = lib().hw_labeler_latent_frames()
+        check(lib().hw_labeler_create(C.byref(cfg), pool_id, lanes, frames_per_chunk, C.byref(self._h)))
+
+    def __call__(self, traces, models):
+        """Returns (labels [lanes,F,64] lagging 24 frames, latent traces [lanes,24,64], viterbi score)."""
+        labels = torch.empty_like(traces)
+        lat = torch.empty((self.lanes, self.latent_frames, abi.LANE), dtype=torch.int16, device=traces.device)
+        score = torch.empty((self.lanes, abi.LANE), dtype=torch.float32, device=traces.device)
+        check(lib().hw_labeler_process(self._h, _p(traces), _p(models), _p(labels), _p(lat), _p(score), _stream()))
+        return labels, lat, score
+
+
+class PulseAccumulator(_Handle):
+    _destroy = "hw_pulse_accumulator_destroy"
+
+    def __init__(self, cfg, pool_id, lanes, frames_per_chunk):
+        super().__init__()
+        self.lanes, self.F = lanes, frames_per_chunk
+        self.cap = cfg.max_calls_per_zmw
+        check(lib().hw_pulse_accumulator_create(C.byref(cfg), pool_id, lanes, frames_per_chunk, C.byref(self._h)))
+
+    def __call__(self, labels, latent, traces, first_frame, models):
+        dev = labels.device
+        pulses = torch.empty(self.lanes * abi.LANE * self.cap * abi.PULSE_DT.itemsize, dtype=torch.uint8, device=dev)
+        lens = torch.empty((self.lanes, abi.LANE), dtype=torch.int32, device=dev)
+        ovf = torch.empty((self.lanes, abi.LANE), dtype=torch.int32, device=dev)
+        bls = struct_buffer(abi.STAT_ACCUM_DT, self.lanes)
+        check(lib().hw_pulse_accumulator_process(self._h, _p(labels), _p(latent), _p(traces), int(first_frame),
+                                                 _p(models), _p(pulses), _p(lens), _p(ovf), _p(bls), _stream()))
+        return pulses, lens, ovf, bls
+
+
+def default_config():
+    cfg = abi.Config()
+    check(lib().hw_config_default(C.byref(cfg)))
+    return cfg

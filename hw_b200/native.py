@@ -1,0 +1,86 @@
+"""Loads libhw_b200.so and declares the C ABI of include/hw_b200.h.
+
+The product path has no CPU fallback: if the shared library is missing or
+cannot be loaded, every call raises.
+"""
+import ctypes as C
+import os
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libhw_b200.so")
+
+_lib = None
+
+
+class HwError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{abi.STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"hw_b200 CUDA library not built: {LIB_PATH} (run python -m hw_b200.build)")
+    L = C.CDLL(LIB_PATH)
+    vp, i32, u32 = C.c_void_p, C.c_int32, C.c_uint32
+    FI = abi.FrameInterval
+    PCFG = C.POINTER(abi.Config)
+    PPV = C.POINTER(C.c_void_p)
+    sigs = {
+        "hw_last_error_string": ([], C.c_char_p),
+        "hw_version": ([], C.c_char_p),
+        "hw_config_default": ([PCFG], C.c_int),
+        "hw_config_validate": ([PCFG], C.c_int),
+        "hw_transition_matrix": ([PCFG, vp], C.c_int),
+        "hw_labeler_latent_frames": ([], u32),
+        "hw_baseliner_create": ([PCFG, u32, u32, u32, PPV], C.c_int),
+        "hw_baseliner_destroy": ([vp], C.c_int),
+        "hw_baseliner_startup_latency": ([vp, C.POINTER(u32)], C.c_int),
+        "hw_baseliner_process": ([vp, vp, i32, vp, vp, vp], C.c_int),
+        "hw_blstats_aggregator_create": ([u32, u32, PPV], C.c_int),
+        "hw_blstats_aggregator_destroy": ([vp], C.c_int),
+        "hw_blstats_aggregator_add": ([vp, vp, FI, vp], C.c_int),
+        "hw_blstats_aggregator_get": ([vp, vp, C.POINTER(FI), vp], C.c_int),
+        "hw_blstats_aggregator_reset": ([vp, vp], C.c_int),
+        "hw_histogram_create": ([PCFG, u32, u32, PPV], C.c_int),
+        "hw_histogram_destroy": ([vp], C.c_int),
+        "hw_histogram_add_batch": ([vp, vp, u32, FI, vp, vp], C.c_int),
+        "hw_histogram_reset_from_stats": ([vp, vp, vp], C.c_int),
+        "hw_histogram_reset_from_bounds": ([vp, vp, vp], C.c_int),
+        "hw_histogram_get": ([vp, vp, C.POINTER(FI), vp], C.c_int),
+        "hw_dme_create": ([PCFG, u32, u32, PPV], C.c_int),
+        "hw_dme_destroy": ([vp], C.c_int),
+        "hw_dme_init_models": ([vp, vp, vp, vp], C.c_int),
+        "hw_dme_estimate": ([vp, vp, vp, FI, FI, vp, vp, vp], C.c_int),
+        "hw_labeler_create": ([PCFG, u32, u32, u32, PPV], C.c_int),
+        "hw_labeler_destroy": ([vp], C.c_int),
+        "hw_labeler_process": ([vp, vp, vp, vp, vp, vp, vp], C.c_int),
+        "hw_pulse_accumulator_create": ([PCFG, u32, u32, u32, PPV], C.c_int),
+        "hw_pulse_accumulator_destroy": ([vp], C.c_int),
+        "hw_pulse_accumulator_process": ([vp, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp], C.c_int),
+    }
+    for name, (args, res) in sigs.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def check(rc):
+    if rc != 0:
+        raise HwError(rc, lib().hw_last_error_string().decode())
+    return rc
+
+
+def exported_symbols():
+    """Names of the C ABI functions declared in include/hw_b200.h."""
+    import re
+    hdr = os.path.join(_HERE, os.pardir, "include", "hw_b200.h")
+    text = open(hdr).read()
+    return sorted(set(re.findall(r"^(?:int|const char\*|uint32_t)\s+(hw_[a-z0-9_]+)\(", text, re.M)))

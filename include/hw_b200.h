@@ -1,0 +1,356 @@
+/*
+ * hw_b200 — C ABI of the B200-native smrt-basecaller trace-analysis chain.
+ *
+ * The chain is: multi-scale morphological baseliner -> baseline statistics
+ * aggregation -> edge-scrubbed trace histogram -> detection-model EM ->
+ * ROI-gated 13-state subframe Viterbi frame labeler -> pulse accumulator.
+ * Each stage sits behind one opaque handle that mirrors one of the
+ * reference's per-pool filter objects (src/basecaller/basecaller/traceAnalysis):
+ *
+ *   hw_baseliner             <- Baseliner / HostMultiScaleBaseliner
+ *                               (traceAnalysis/Baseliner.h:53-79)
+ *   hw_blstats_aggregator    <- BaselineStatsAggregator
+ *                               (traceAnalysis/BaselineStatsAggregator.h:45-104)
+ *   hw_histogram             <- TraceHistogramAccumulator
+ *                               (traceAnalysis/TraceHistogramAccumulator.h:52-155)
+ *   hw_dme                   <- CoreDMEstimator / DmeEmHost
+ *                               (traceAnalysis/CoreDMEstimator.h:151-162)
+ *   hw_labeler               <- FrameLabeler / FrameLabelerHost
+ *                               (traceAnalysis/FrameLabeler.h:67-74)
+ *   hw_pulse_accumulator     <- PulseAccumulator / HostPulseAccumulator
+ *                               (traceAnalysis/PulseAccumulator.h:68-74)
+ *   hw_analyzer              <- BatchAnalyzer + DetectionModelEstimator
+ *                               (analyzer/BatchAnalyzer.cpp:149-375,
+ *                                traceAnalysis/DetectionModelEstimator.cpp:93-160)
+ *
+ * Conventions
+ *   - Every function returns an hw_status (0 = HW_OK). No exceptions cross
+ *     the ABI; hw_last_error_string() describes the last failure on the
+ *     calling thread.
+ *   - Pointers named d_* are device pointers; the caller owns them.  State
+ *     that persists between chunks is owned by the handle, in device memory.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = default stream).
+ *     Calls are asynchronous on that stream unless documented otherwise.
+ *     A handle is not re-entrant: issue its calls from one thread, in
+ *     chunk order (the reference analyzer is non-reentrant per pool too,
+ *     analyzer/BatchAnalyzer.h:75-78).
+ *   - Batch layout is the reference BatchData block-major layout
+ *     (dataTypes/BatchData.h:78-355): data[lane][frame][zmw] with 64 ZMWs per
+ *     lane.
+ *   - The lane structs below reproduce the member order and sizes of the
+ *     reference's lane SoA types so buffers can be exchanged unchanged.
+ */
+#ifndef HW_B200_H_
+#define HW_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HW_LANE_SIZE   64   /* common/MongoConstants.h laneSize */
+#define HW_NUM_ANALOGS 4    /* common/MongoConstants.h numAnalogs */
+#define HW_NUM_BINS    300  /* dataTypes/PoolHistogram.h:47 LaneHistogram::numBins */
+#define HW_NUM_STATES  13   /* traceAnalysis/SubframeLabelManager.h numStates */
+#define HW_AUTOCORR_LAG 4   /* common/AutocorrAccumState.h lag */
+
+typedef enum hw_status {
+    HW_OK = 0,
+    HW_ERR_INVALID_ARG = 1,      /* bad pointer, size or configuration value */
+    HW_ERR_CUDA = 2,             /* a CUDA runtime call failed */
+    HW_ERR_BAD_POOL = 3,         /* batch belongs to another pool */
+    HW_ERR_FRAME_ORDER = 4,      /* batch is not the next chunk in time */
+    HW_ERR_NOT_INITIALIZED = 5,  /* e.g. histogram used before its first Reset */
+    HW_ERR_UNSUPPORTED = 6,      /* option of the reference not built here */
+    HW_ERR_TIMEOUT = 7,          /* a bounded device wait gave up */
+    HW_ERR_OUT_OF_MEMORY = 8,
+    HW_ERR_NUMERIC = 9,          /* a reference assertion on the data failed
+                                    (e.g. histogram bounds, DME sanity checks) */
+    HW_ERR_INTERNAL = 10
+} hw_status;
+
+/* BasecallerBaselinerConfig::FilterTypes (dataTypes/configs/BasecallerBaselinerConfig.h) */
+typedef enum hw_filter_type {
+    HW_FILTER_MULTISCALE_LARGE = 0,
+    HW_FILTER_MULTISCALE_MEDIUM = 1,
+    HW_FILTER_MULTISCALE_SMALL = 2,
+    HW_FILTER_TWOSCALE_LARGE = 3,
+    HW_FILTER_TWOSCALE_MEDIUM = 4,
+    HW_FILTER_TWOSCALE_SMALL = 5
+} hw_filter_type;
+
+/* BasecallerRoiConfig::RoiFilterType */
+typedef enum hw_roi_filter { HW_ROI_DEFAULT = 0, HW_ROI_NOOP = 1 } hw_roi_filter;
+
+/* BasecallerAlgorithmConfig::ModelEstimationMode */
+typedef enum hw_estimation_mode {
+    HW_FIXED_ESTIMATIONS = 0,
+    HW_INITIAL_ESTIMATIONS = 1,   /* SingleEstimateBatchAnalyzer */
+    HW_DYNAMIC_ESTIMATIONS = 2    /* DynamicEstimateBatchAnalyzer */
+} hw_estimation_mode;
+
+/* One analog's kinetics and amplitude (pa-common AuxData::AnalogMode fields used on the path). */
+typedef struct hw_analog {
+    char  base_label;             /* 'A','C','G','T' */
+    float rel_amplitude;          /* relAmplitude */
+    float excess_noise_cv;        /* excessNoiseCV */
+    float pulse_width_s;          /* pulseWidth, seconds */
+    float ipd_s;                  /* interPulseDistance, seconds */
+    float pw2_slow_step_ratio;    /* pw2SlowStepRatio */
+    float ipd2_slow_step_ratio;   /* ipd2SlowStepRatio */
+} hw_analog;
+
+/* All parameters of the path.  hw_config_default() fills reference defaults. */
+typedef struct hw_config {
+    /* AnalysisConfig / MovieInfo */
+    double   frame_rate;                 /* frames per second */
+    float    photoelectron_sensitivity;  /* e-/DN; baseliner and histogram scaler */
+    float    ref_snr;                    /* SNR of an analog with relAmplitude 1 */
+    float    shot_var_coeff;             /* CoreDMEstimator::Configuration::shotVarCoeff */
+    int16_t  pedestal;
+    hw_analog analogs[HW_NUM_ANALOGS];   /* brightest first, dimmest last */
+
+    /* BasecallerBaselinerConfig */
+    int32_t  filter_type;                /* hw_filter_type */
+    float    mean_bias_adjust;
+    float    sigma_bias_adjust;
+    float    mean_ema_scale_strides;
+    float    sigma_ema_scale_strides;
+    float    jump_suppression;
+
+    /* BasecallerTraceHistogramConfig */
+    float    bin_size_coeff;
+    float    bin_size_low_bound_coeff;
+    uint32_t baseline_stat_min_frame_count;
+    float    fallback_baseline_sigma;
+
+    /* BasecallerDmeConfig */
+    uint32_t num_frames_pre_accum_stats;
+    uint32_t min_frames_for_estimate;
+    float    analog_mix_fraction_threshold[2];
+    float    scale_snr_conf_tol;
+    uint32_t em_iteration_limit;
+    float    gtest_stat_factor;          /* < 0 disables the G-test (default -1) */
+    int32_t  iterate_to_limit;
+    float    min_analog_snr_thresh0;
+    float    min_analog_snr_thresh1;
+    float    pulse_amp_regularization;
+    uint32_t model_update_method;        /* 0, 1 (default) or 2 */
+    float    snr_drop_thresh;
+    float    success_confidence_thresh;
+    float    confidence_half_life[2];
+
+    /* BasecallerFrameLabelerConfig */
+    float    viterbi_alpha;
+    float    viterbi_beta;
+    float    viterbi_gamma;
+    int32_t  roi_filter_type;            /* hw_roi_filter */
+    float    roi_upper_threshold;
+    float    roi_lower_threshold;
+
+    /* BasecallerPulseAccumConfig */
+    uint32_t max_calls_per_zmw;
+    double   xsp_amp_thresh;
+    float    xsp_width_thresh;
+
+    /* BasecallerAlgorithmConfig */
+    int32_t  model_estimation_mode;      /* hw_estimation_mode */
+    /* StaticDetModelConfig (used only with HW_FIXED_ESTIMATIONS) */
+    float    static_baseline_mean;
+    float    static_baseline_variance;
+} hw_config;
+
+/* ---- Lane structs (64 ZMWs each, structure-of-arrays) ------------------ */
+
+/* common/StatAccumState.h StatAccumStateT<float,64> */
+typedef struct hw_stat_accum_state {
+    float offset[HW_LANE_SIZE];
+    float moment0[HW_LANE_SIZE];
+    float moment1[HW_LANE_SIZE];
+    float moment2[HW_LANE_SIZE];
+} hw_stat_accum_state;
+
+/* common/AutocorrAccumState.h AutocorrAccumState */
+typedef struct hw_autocorr_accum_state {
+    hw_stat_accum_state basic_stats;
+    float   moment2[HW_LANE_SIZE];
+    float   fbuf[HW_AUTOCORR_LAG][HW_LANE_SIZE];
+    float   bbuf[HW_AUTOCORR_LAG][HW_LANE_SIZE];
+    uint8_t bidx[2][HW_LANE_SIZE];
+} hw_autocorr_accum_state;
+
+/* dataTypes/BaselinerStatAccumState.h BaselinerStatAccumState */
+typedef struct hw_baseliner_stats {
+    hw_autocorr_accum_state full_autocorr;
+    int16_t trace_min[HW_LANE_SIZE];
+    int16_t trace_max[HW_LANE_SIZE];
+    hw_stat_accum_state baseline_stats;
+    float   raw_baseline_sum[HW_LANE_SIZE];
+    hw_stat_accum_state background_stats;
+} hw_baseliner_stats;
+
+/* dataTypes/LaneDetectionModel.h LaneAnalogMode<PBHalf,64>; IEEE binary16 bits */
+typedef struct hw_lane_analog_mode {
+    uint16_t means[HW_LANE_SIZE];
+    uint16_t vars[HW_LANE_SIZE];
+    uint16_t weights[HW_LANE_SIZE];
+} hw_lane_analog_mode;
+
+/* dataTypes/LaneDetectionModel.h LaneModelParameters<PBHalf,64> (2048 bytes) */
+typedef struct hw_lane_model {
+    hw_lane_analog_mode analogs[HW_NUM_ANALOGS];
+    hw_lane_analog_mode baseline;
+    uint16_t confidence[HW_LANE_SIZE];
+} hw_lane_model;
+
+/* dataTypes/PoolHistogram.h LaneHistogram<float, unsigned short> */
+typedef struct hw_lane_histogram {
+    float    low_bound[HW_LANE_SIZE];
+    float    bin_size[HW_LANE_SIZE];
+    uint16_t outlier_count_low[HW_LANE_SIZE];
+    uint16_t outlier_count_high[HW_LANE_SIZE];
+    uint16_t bin_count[HW_NUM_BINS][HW_LANE_SIZE];
+} hw_lane_histogram;
+
+/* traceAnalysis/TraceHistogramAccumulator.h:41 LaneHistBounds */
+typedef struct hw_lane_hist_bounds {
+    float upper_bounds[HW_LANE_SIZE];
+    float lower_bounds[HW_LANE_SIZE];
+} hw_lane_hist_bounds;
+
+/* dataTypes/Pulse.h Pulse (20 bytes; signals in 0.1 DN fixed point) */
+typedef struct hw_pulse {
+    uint32_t start;
+    uint16_t width;
+    uint16_t mean_signal;
+    uint16_t mid_signal;
+    uint16_t max_signal;
+    float    signal_m2;
+    uint8_t  label;        /* Pulse::NucleotideLabel: A=0, C, G, T, N, NONE */
+    uint8_t  is_reject;
+    uint8_t  pad_[2];
+} hw_pulse;
+
+/* Per-ZMW DME diagnostics (traceAnalysis/MaxLikelihoodDiagnostics.h; the
+ * reference computes these but does not export them). */
+typedef struct hw_dme_diag {
+    int32_t iter_count[HW_LANE_SIZE];   /* iteration of first convergence */
+    int32_t converged[HW_LANE_SIZE];
+    float   log_like[HW_LANE_SIZE];
+    int32_t status[HW_LANE_SIZE];       /* CoreDMEstimator::ZmwStatus bits */
+    float   confidence[HW_LANE_SIZE];   /* confidence of the fresh estimate */
+    int32_t lane_iterations;            /* EM iterations the lane executed */
+    int32_t pad_[15];
+} hw_dme_diag;
+
+/* IntInterval<int32_t>: [lower, upper); empty when lower == upper. */
+typedef struct hw_frame_interval {
+    int32_t lower;
+    int32_t upper;
+} hw_frame_interval;
+
+/* ---- Library ------------------------------------------------------------ */
+
+const char* hw_last_error_string(void);
+const char* hw_version(void);
+
+/* Reference defaults for every parameter (PB_CONFIG_PARAM defaults in
+ * in dataTypes/configs) plus the analog set of the synthetic workloads. */
+int hw_config_default(hw_config* cfg);
+
+/* Configuration checks of the reference (ValidateConfig<> specialisations and
+ * the Configure() asserts). */
+int hw_config_validate(const hw_config* cfg);
+
+/* Transition matrix of the subframe Viterbi in log space, dense [to][from]
+ * with -inf where the sparse pattern has no entry
+ * (traceAnalysis/SubframeScorer.cpp:36-223). Host-only, synchronous. */
+int hw_transition_matrix(const hw_config* cfg, float out[HW_NUM_STATES][HW_NUM_STATES]);
+
+/* ---- Baseliner (traceAnalysis/Baseliner.h:53-79) ------------------------- */
+typedef struct hw_baseliner hw_baseliner;
+int hw_baseliner_create(const hw_config* cfg, uint32_t pool_id, uint32_t lanes,
+                        uint32_t frames_per_chunk, hw_baseliner** out);
+int hw_baseliner_destroy(hw_baseliner* b);
+/* MultiScaleBaseliner::StartupLatency (traceAnalysis/MultiScaleBaseliner.h:92-99) */
+int hw_baseliner_startup_latency(const hw_baseliner* b, uint32_t* frames);
+/* FilterBaseline: d_trace[lanes][F][64] int16 -> d_out (same shape) and one
+ * hw_baseliner_stats per lane.  first_frame must continue the previous call. */
+int hw_baseliner_process(hw_baseliner* b, const int16_t* d_trace, int32_t first_frame,
+                         int16_t* d_out, hw_baseliner_stats* d_stats, void* stream);
+
+/* ---- Baseline statistics aggregator (BaselineStatsAggregator.h:45-104) -- */
+typedef struct hw_blstats_aggregator hw_blstats_aggregator;
+int hw_blstats_aggregator_create(uint32_t pool_id, uint32_t lanes, hw_blstats_aggregator** out);
+int hw_blstats_aggregator_destroy(hw_blstats_aggregator* a);
+int hw_blstats_aggregator_add(hw_blstats_aggregator* a, const hw_baseliner_stats* d_stats,
+                              hw_frame_interval fi, void* stream);
+int hw_blstats_aggregator_get(const hw_blstats_aggregator* a, hw_baseliner_stats* d_out,
+                              hw_frame_interval* fi, void* stream);
+int hw_blstats_aggregator_reset(hw_blstats_aggregator* a, void* stream);
+
+/* ---- Trace histogram (TraceHistogramAccumulator.h:96-154) -------------- */
+typedef struct hw_histogram hw_histogram;
+int hw_histogram_create(const hw_config* cfg, uint32_t pool_id, uint32_t lanes, hw_histogram** out);
+int hw_histogram_destroy(hw_histogram* h);
+/* AddBatch: edge-frame scrubbing with the fp16 models, then binning. */
+int hw_histogram_add_batch(hw_histogram* h, const int16_t* d_traces, uint32_t frames,
+                           hw_frame_interval fi, const hw_lane_model* d_models, void* stream);
+/* Reset(const BaselinerMetrics&): bounds from aggregated baseline stats. */
+int hw_histogram_reset_from_stats(hw_histogram* h, const hw_baseliner_stats* d_stats, void* stream);
+/* Reset(UnifiedCudaArray<LaneHistBounds>): explicit bounds. */
+int hw_histogram_reset_from_bounds(hw_histogram* h, const hw_lane_hist_bounds* d_bounds, void* stream);
+/* Histogram(): copy out one hw_lane_histogram per lane. */
+int hw_histogram_get(const hw_histogram* h, hw_lane_histogram* d_out, hw_frame_interval* fi,
+                     void* stream);
+
+/* ---- Detection-model estimator (CoreDMEstimator.h:151-162, DmeEmHost) --- */
+typedef struct hw_dme hw_dme;
+int hw_dme_create(const hw_config* cfg, uint32_t pool_id, uint32_t lanes, hw_dme** out);
+int hw_dme_destroy(hw_dme* d);
+/* InitDetectionModels (DmeEmHost.cpp:857-925). */
+int hw_dme_init_models(hw_dme* d, const hw_baseliner_stats* d_stats, hw_lane_model* d_models,
+                       void* stream);
+/* Estimate (DmeEmHost.cpp:131-615): EM on the histograms, confidence-weighted
+ * update of d_models in place.  model_fi is the models' frame interval,
+ * hist_fi the histograms'.  d_diag (may be NULL) receives per-ZMW EM
+ * diagnostics.  Synchronous: a failed reference assertion returns
+ * HW_ERR_NUMERIC. */
+int hw_dme_estimate(hw_dme* d, const hw_lane_histogram* d_hist, const hw_baseliner_stats* d_stats,
+                    hw_frame_interval hist_fi, hw_frame_interval model_fi,
+                    hw_lane_model* d_models, hw_dme_diag* d_diag, void* stream);
+
+/* ---- Frame labeler (FrameLabeler.h:67-74, FrameLabelerHost.cpp:314-612) - */
+typedef struct hw_labeler hw_labeler;
+int hw_labeler_create(const hw_config* cfg, uint32_t pool_id, uint32_t lanes,
+                      uint32_t frames_per_chunk, hw_labeler** out);
+int hw_labeler_destroy(hw_labeler* l);
+/* Labels lag the traces by hw_labeler_latent_frames() (24) frames.
+ * d_labels[lanes][F][64] int16; d_latent_out[lanes][24][64] receives the
+ * traces the first 24 labels belong to (LabelsBatch::LatentTrace);
+ * d_viterbi_score[lanes][64] the anchor log-likelihood. */
+int hw_labeler_process(hw_labeler* l, const int16_t* d_traces, const hw_lane_model* d_models,
+                       int16_t* d_labels, int16_t* d_latent_out, float* d_viterbi_score,
+                       void* stream);
+uint32_t hw_labeler_latent_frames(void);
+
+/* ---- Pulse accumulator (PulseAccumulator.h:68-74, HostPulseAccumulator) - */
+typedef struct hw_pulse_accumulator hw_pulse_accumulator;
+int hw_pulse_accumulator_create(const hw_config* cfg, uint32_t pool_id, uint32_t lanes,
+                                uint32_t frames_per_chunk, hw_pulse_accumulator** out);
+int hw_pulse_accumulator_destroy(hw_pulse_accumulator* p);
+/* d_pulses[lanes][64][max_calls_per_zmw]; d_lens/d_overflows[lanes][64];
+ * d_blstats one hw_stat_accum_state per lane (PulseDetectorMetrics). */
+int hw_pulse_accumulator_process(hw_pulse_accumulator* p, const int16_t* d_labels,
+                                 const int16_t* d_latent_trace, const int16_t* d_trace,
+                                 int32_t first_frame, const hw_lane_model* d_models,
+                                 hw_pulse* d_pulses, uint32_t* d_lens, uint32_t* d_overflows,
+                                 hw_stat_accum_state* d_blstats, void* stream);
+
+#ifdef __cplusplus
+}   /* extern "C" */
+#endif
+
+#endif  /* HW_B200_H_ */

@@ -1,0 +1,1686 @@
+// CPU oracle for the smrt-basecaller trace-analysis chain.
+//
+// TEST INFRASTRUCTURE ONLY.  This file restates, on the CPU, the reference's
+// Host* implementations of the path (cdunn2001/hw, src/basecaller/...), so
+// that tests can check the CUDA library against it and bench.py can time it
+// as the CPU baseline.  Nothing in the hw_b200 product loads or calls it.
+//
+// The restatement is literal: every stage keeps the reference's order of
+// floating-point operations, its lane-wide (64-ZMW) control flow, its integer
+// wrap-around and its float->int conversions (cvtps2dq semantics).  exp/log
+// are the project's Cephes-method routines (hw_b200/csrc/hw_math.h), the same
+// ones the kernels call; the reference uses an SSE port of Cephes.  pow, exp2
+// and log2 (used a few times per estimate) are evaluated in double precision
+// and rounded to float on both sides.
+//
+// Each function cites the reference file:line it follows.  Abbreviations:
+//   TA = src/basecaller/basecaller/traceAnalysis, DT = src/basecaller/dataTypes,
+//   CM = src/basecaller/common, AN = src/basecaller/basecaller/analyzer.
+//
+// Build: oracle/Makefile (g++ -O3 -march=native -ffp-contract=off -fopenmp).
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include <omp.h>
+
+#include "../include/hw_b200.h"
+#include "../hw_b200/csrc/hw_math.h"
+#include "../hw_b200/csrc/hw_params.h"
+
+using namespace hwm;
+using hwp::kLane;
+using hwp::kAnalogs;
+using hwp::kBins;
+using hwp::kStates;
+
+#define FZ for (int z = 0; z < kLane; ++z)
+
+namespace {
+
+thread_local std::string g_err;
+
+const float kInf = std::numeric_limits<float>::infinity();
+const float kNaN = std::numeric_limits<float>::quiet_NaN();
+
+inline float pow_f(float x, float y) { return (float)std::pow((double)x, (double)y); }
+inline float exp2_f(float x) { return (float)std::exp2((double)x); }
+inline float log2_f(float x) { return (float)std::log2((double)x); }
+
+// ---------------------------------------------------------------------------
+// CM/StatAccumulator.h:48-252 (offset is always 0 on this path).
+struct StatAcc
+{
+    float off[kLane], m0[kLane], m1[kLane], m2[kLane];
+    void Reset() { FZ { off[z] = 0; m0[z] = 0; m1[z] = 0; m2[z] = 0; } }
+    void Load(const hw_stat_accum_state& s)
+    { FZ { off[z] = s.offset[z]; m0[z] = s.moment0[z]; m1[z] = s.moment1[z]; m2[z] = s.moment2[z]; } }
+    void Store(hw_stat_accum_state& s) const
+    { FZ { s.offset[z] = off[z]; s.moment0[z] = m0[z]; s.moment1[z] = m1[z]; s.moment2[z] = m2[z]; } }
+    // AddSample(value), :160-166
+    void Add(int z, float v) { const float x = v - off[z]; m0[z] += 1.0f; m1[z] += x; m2[z] += x * x; }
+    // AddSample(value, mask), :168-174
+    void AddMasked(int z, float v, bool m)
+    {
+        const float x = v - off[z];
+        const float a0 = m0[z] + 1.0f, a1 = m1[z] + x, a2 = m2[z] + x * x;
+        m0[z] = m ? a0 : m0[z]; m1[z] = m ? a1 : m1[z]; m2[z] = m ? a2 : m2[z];
+    }
+    // Merge, :176-184
+    void Merge(const StatAcc& o) { FZ { m0[z] += o.m0[z]; m1[z] += o.m1[z]; m2[z] += o.m2[z]; } }
+    // Mean, :85-88
+    float Mean(int z) const { return m1[z] / m0[z] + off[z]; }
+    // Variance, :90-97
+    float Variance(int z) const
+    {
+        float var = m1[z] * m1[z] / m0[z];
+        var = (m2[z] - var) / (m0[z] - 1.0f);
+        var = fmax_sse(var, 0.0f);
+        return (m0[z] > 1.0f) ? var : kNaN;
+    }
+};
+
+// CM/AutocorrAccumulator.{h,cpp} with lag 4.
+struct AutocorrAcc
+{
+    StatAcc stats;
+    float m2[kLane];
+    float fBuf[4][kLane], bBuf[4][kLane];
+    uint16_t fbi, bbi;
+    void Reset()
+    {
+        stats.Reset();
+        FZ { m2[z] = 0; for (int k = 0; k < 4; ++k) { fBuf[k][z] = 0; bBuf[k][z] = 0; } }
+        fbi = 0; bbi = 0;
+    }
+    void Load(const hw_autocorr_accum_state& s)
+    {
+        stats.Load(s.basic_stats);
+        FZ { m2[z] = s.moment2[z]; for (int k = 0; k < 4; ++k) { fBuf[k][z] = s.fbuf[k][z]; bBuf[k][z] = s.bbuf[k][z]; } }
+        fbi = s.bidx[0][0]; bbi = s.bidx[1][0];
+    }
+    void Store(hw_autocorr_accum_state& s) const
+    {
+        stats.Store(s.basic_stats);
+        FZ { s.moment2[z] = m2[z]; for (int k = 0; k < 4; ++k) { s.fbuf[k][z] = fBuf[k][z]; s.bbuf[k][z] = bBuf[k][z]; } }
+        FZ { s.bidx[0][z] = (uint8_t)fbi; s.bidx[1][z] = (uint8_t)bbi; }
+    }
+    // AddSample, AutocorrAccumulator.cpp:29-39 (lane-wide indices)
+    void AddRow(const float* v)
+    {
+        const bool fill = fbi < 4;
+        const int slot = bbi % 4;
+        FZ
+        {
+            const float x = v[z] - stats.off[z];
+            if (fill) fBuf[fbi][z] = x;
+            m2[z] += bBuf[slot][z] * x;
+            bBuf[slot][z] = x;
+            stats.Add(z, v[z]);
+        }
+        if (fill) ++fbi;
+        bbi = (uint16_t)((bbi + 1) % 4);
+    }
+    // Merge, AutocorrAccumulator.cpp:71-103
+    void Merge(const AutocorrAcc& t)
+    {
+        stats.Merge(t.stats);
+        FZ m2[z] += t.m2[z];
+        const int n1 = 4 - t.fbi;
+        for (int k = 0; k < 4 - n1; ++k)
+        {
+            const int i = (bbi + k) % 4, j = (t.bbi + n1 + k) % 4;
+            FZ { m2[z] += bBuf[i][z] * t.fBuf[k][z]; bBuf[i][z] = t.bBuf[j][z]; }
+        }
+        const int n2 = 4 - fbi;
+        for (int k = 0; k < n2; ++k) FZ fBuf[fbi + k][z] = t.fBuf[k][z];
+        fbi = (uint16_t)(fbi + n2);
+        bbi = (uint16_t)((bbi + (4 - n1)) % 4);
+    }
+};
+
+// DT/BaselinerStatAccumulator.{h,cpp}
+struct BlStatAcc
+{
+    AutocorrAcc corr;
+    int16_t tmin[kLane], tmax[kLane];
+    StatAcc blStats;
+    float rawSum[kLane];
+    StatAcc bgStats;
+    void Reset()
+    {
+        corr.Reset(); blStats.Reset(); bgStats.Reset();
+        FZ { tmin[z] = 32767; tmax[z] = -32768; rawSum[z] = 0.0f; }
+    }
+    void Load(const hw_baseliner_stats& s)
+    {
+        corr.Load(s.full_autocorr);
+        FZ { tmin[z] = s.trace_min[z]; tmax[z] = s.trace_max[z]; rawSum[z] = s.raw_baseline_sum[z]; }
+        blStats.Load(s.baseline_stats); bgStats.Load(s.background_stats);
+    }
+    void Store(hw_baseliner_stats& s) const
+    {
+        corr.Store(s.full_autocorr);
+        FZ { s.trace_min[z] = tmin[z]; s.trace_max[z] = tmax[z]; s.raw_baseline_sum[z] = rawSum[z]; }
+        blStats.Store(s.baseline_stats); bgStats.Store(s.background_stats);
+    }
+    // AddSample, BaselinerStatAccumulator.cpp:39-53
+    void AddSample(const int16_t* raw, const int16_t* bls, const bool* isBl)
+    {
+        float bs[kLane];
+        FZ bs[z] = (float)bls[z];
+        corr.AddRow(bs);
+        FZ
+        {
+            tmin[z] = std::min(bls[z], tmin[z]);
+            tmax[z] = std::max(bls[z], tmax[z]);
+            blStats.AddMasked(z, bs[z], isBl[z]);
+            rawSum[z] += (float)(isBl[z] ? raw[z] : (int16_t)0);
+        }
+    }
+    // Merge, BaselinerStatAccumulator.cpp:62-73
+    void Merge(const BlStatAcc& o)
+    {
+        corr.Merge(o.corr);
+        FZ { tmin[z] = std::min(tmin[z], o.tmin[z]); tmax[z] = std::max(tmax[z], o.tmax[z]); }
+        blStats.Merge(o.blStats);
+        FZ rawSum[z] += o.rawSum[z];
+        bgStats.Merge(o.bgStats);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Baseliner: TA/HostMultiScaleBaseliner.{h,cpp}, TA/BlockFilterStage.cpp,
+// TA/TraceFilters.cpp, TA/WindowBuffer.h.
+
+// WindowBuffer<LaneArray<short>> with capacity w, always full after
+// construction (w zeros pushed, BlockFilterStage.h:24-31).
+struct WinBuf
+{
+    int w = 0, start = 0, counter = 0;
+    std::vector<int16_t> d;      // w slots x 64
+    int16_t hold[kLane];
+    void Init(int width)
+    {
+        w = width; start = 0; counter = 0;
+        d.assign((size_t)w * kLane, 0);
+        FZ hold[z] = 0;
+    }
+    int16_t* at(int j) { return &d[(size_t)((start + j) % w) * kLane]; }
+    void push(const int16_t* x)
+    {
+        std::memcpy(&d[(size_t)start * kLane], x, sizeof(int16_t) * kLane);
+        start = (start + 1) % w;
+        counter = (counter + 1) % w;
+    }
+};
+
+struct Stage
+{
+    hwp::StageSpec spec;
+    WinBuf wb;
+    // BlockFilterStage::operator() + extremumFilterHgw (TraceFilters.cpp:11-57),
+    // in place on block[F][64].
+    void Run(int16_t* block, int F)
+    {
+        const int w = spec.width;
+        const int dist = F / spec.nf;
+        int16_t s[kLane], front[kLane], y[kLane];
+        std::memcpy(s, wb.hold, sizeof(s));
+        int outIdx = 0;
+        auto op = [this](int16_t a, int16_t b) -> int16_t {
+            return spec.isMax ? std::max(a, b) : std::min(a, b);
+        };
+        for (int i = 0; i < dist; i += spec.stride)
+        {
+            if (wb.counter == 0)
+            {
+                for (int j = w - 1; j > 0; --j)
+                {
+                    int16_t* rj = wb.at(j); int16_t* rj1 = wb.at(j - 1);
+                    FZ rj1[z] = op(rj[z], rj1[z]);
+                }
+                std::memcpy(s, wb.at(w - 1), sizeof(s));
+            }
+            else
+            {
+                const int16_t* b = wb.at(w - 1);
+                FZ s[z] = op(s[z], b[z]);
+            }
+            std::memcpy(front, wb.at(0), sizeof(front));
+            wb.push(block + (size_t)i * kLane);
+            FZ y[z] = op(s[z], front[z]);
+            std::memcpy(block + (size_t)outIdx * kLane, y, sizeof(y));
+            ++outIdx;
+        }
+        std::memcpy(wb.hold, s, sizeof(s));
+    }
+};
+
+struct LaneBaseliner
+{
+    std::vector<Stage> lower, upper;
+    float uemaSum[kLane], uemaWeight[kLane], sigmaEma[kLane];
+    int16_t latData[kLane], latRaw[kLane];
+    bool latL[kLane], latH1[kLane], latH2[kLane];
+
+    void Init(const hwp::Derived& d)
+    {
+        hwp::StageSpec sp[2 * hwp::kMaxScales];
+        int n = hwp::StageSpecs(d.fp, false, sp);
+        lower.resize(n);
+        for (int i = 0; i < n; ++i) { lower[i].spec = sp[i]; lower[i].wb.Init(sp[i].width); }
+        n = hwp::StageSpecs(d.fp, true, sp);
+        upper.resize(n);
+        for (int i = 0; i < n; ++i) { upper[i].spec = sp[i]; upper[i].wb.Init(sp[i].width); }
+        FZ
+        {
+            uemaSum[z] = 0.0f; uemaWeight[z] = 0.0f; sigmaEma[z] = 2.0f;
+            latData[z] = 0; latRaw[z] = 0; latL[z] = latH1[z] = latH2[z] = false;
+        }
+    }
+
+    // GetSmoothedBlEstimate, HostMultiScaleBaseliner.cpp:179-212
+    void Smoothed(const hwp::Derived& d, const int16_t* lo, const int16_t* up, float* out)
+    {
+        constexpr float minSigma = .288675135f;
+        const float ma = d.meanEmaAlpha, sa = d.sigmaEmaAlpha;
+        FZ
+        {
+            const float sigma = fmax_sse((float)i16_wrap(up[z] - lo[z]) / d.cSigmaBias, minSigma);
+            const float newSigmaEma = sa * sigmaEma[z] + (1.0f - sa) * sigma;
+            const float blEst = 0.5f * (float)i16_wrap(up[z] + lo[z]) + d.cMeanBias * newSigmaEma;
+            const bool mask = (uemaWeight[z] == 0.0f)
+                            | (blEst - uemaSum[z] / uemaWeight[z] < d.jumpTolCoeff * sigmaEma[z]);
+            const float newWeight = ma * uemaWeight[z] + (1.0f - ma);
+            const float newSum = ma * uemaSum[z] + (1.0f - ma) * blEst;
+            uemaWeight[z] = mask ? newWeight : uemaWeight[z];
+            uemaSum[z] = mask ? newSum : uemaSum[z];
+            sigmaEma[z] = mask ? newSigmaEma : sigmaEma[z];
+            out[z] = uemaSum[z] / uemaWeight[z];
+        }
+    }
+
+    // AddToBaselineStats, HostMultiScaleBaseliner.cpp:148-176
+    void AddToStats(const hwp::Derived& d, const int16_t* trace, const int16_t* bls, BlStatAcc& st)
+    {
+        bool mask[kLane], hp1[kLane];
+        FZ
+        {
+            const float thrLow = 4.5f * sigmaEma[z];
+            const float thrHigh = 4.5f * sigmaEma[z];
+            hp1[z] = (float)bls[z] < thrHigh * d.scaler;
+            mask[z] = latH1[z] & latL[z] & hp1[z];
+            latL[z] = (float)bls[z] < thrLow * d.scaler;
+            latH2[z] = latH1[z];
+            latH1[z] = hp1[z];
+        }
+        st.AddSample(latRaw, latData, mask);
+        FZ { latRaw[z] = trace[z]; latData[z] = bls[z]; }
+    }
+
+    // EstimateBaseline, HostMultiScaleBaseliner.cpp:95-146
+    void Estimate(const hwp::Derived& d, const int16_t* trace, int F, int16_t* out, BlStatAcc& st,
+                  std::vector<int16_t>& lo, std::vector<int16_t>& up)
+    {
+        lo.assign(trace, trace + (size_t)F * kLane);
+        up.assign(trace, trace + (size_t)F * kLane);
+        for (auto& s : lower) s.Run(lo.data(), F);
+        for (auto& s : upper) s.Run(up.data(), F);
+        const int stride = d.aggStride;
+        const int fdSize = F / stride;
+        st.Reset();
+        int t = 0;
+        int16_t lv[kLane], uv[kLane], raw[kLane], bls[kLane], bg[kLane];
+        float blEst[kLane], sub[kLane];
+        for (int i = 0; i < fdSize; ++i)
+        {
+            FZ
+            {
+                lv[z] = i16_wrap(lo[(size_t)i * kLane + z] - d.pedestal);
+                uv[z] = i16_wrap(up[(size_t)i * kLane + z] - d.pedestal);
+            }
+            Smoothed(d, lv, uv, blEst);
+            FZ sub[z] = blEst[z] * d.scaler;
+            for (int j = 0; j < stride; ++j, ++t)
+            {
+                const int16_t* tr = trace + (size_t)t * kLane;
+                FZ
+                {
+                    const float rs = (float)i16_wrap(tr[z] - d.pedestal) * d.scaler;
+                    bls[z] = to_i16_wrap(rs - sub[z]);
+                    raw[z] = to_i16_wrap(rs);
+                    out[(size_t)t * kLane + z] = bls[z];
+                }
+                AddToStats(d, raw, bls, st);
+            }
+            FZ bg[z] = to_i16_wrap(sub[z]);
+            FZ st.bgStats.Add(z, (float)bg[z]);
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Histogram: TA/TraceHistogramAccumHost.cpp, TA/EdgeFrameClassifier.h,
+// DT/UHistogramSimd.{h,cpp}
+
+struct LaneHist
+{
+    float lower[kLane], binSize[kLane];
+    uint16_t nLow[kLane], nHigh[kLane];
+    uint16_t count[kBins + 1][kLane];
+    bool valid = false;
+};
+
+struct EdgeClassifier
+{
+    int16_t prev[kLane];
+    bool hist[2][kLane];
+    int hsize;   // 0, 1, 2 (full)
+    int hfront;
+    void Init() { FZ { prev[z] = 0; hist[0][z] = hist[1][z] = false; } hsize = 0; hfront = 0; }
+};
+
+// UHistogramSimd ctor, UHistogramSimd.cpp:51-97: returns false on the
+// reference's throw conditions.
+bool HistInit(LaneHist& h, const float* lo, const float* up)
+{
+    bool ok = true;
+    FZ
+    {
+        if (lo[z] >= up[z]) ok = false;
+        const float bs = (up[z] - lo[z]) / static_cast<float>(kBins);
+        if (bs <= 0.0f) ok = false;
+        // binStart_[i] = binSize_*i + lowerBound must strictly change
+        // (the last boundary is then overwritten by upperBound).
+        float prevStart = lo[z];
+        for (int i = 1; i <= kBins; ++i)
+        {
+            const float si = bs * (float)i + lo[z];
+            if (prevStart == si) ok = false;
+            prevStart = si;
+        }
+        h.lower[z] = lo[z];
+        h.binSize[z] = bs;
+        h.nLow[z] = 0; h.nHigh[z] = 0;
+        for (int b = 0; b <= kBins; ++b) h.count[b][z] = 0;
+    }
+    h.valid = true;
+    return ok;
+}
+
+// ---------------------------------------------------------------------------
+// Detection model (float view): TA/DetectionModelHost.{h,cpp}
+
+struct Model
+{
+    float bw[kLane], bm[kLane], bv[kLane];
+    float aw[kAnalogs][kLane], am[kAnalogs][kLane], av[kAnalogs][kLane];
+    float conf[kLane];
+    hw_frame_interval fi;
+};
+
+inline int32_t CenterInt(const hw_frame_interval& fi) { return fi.lower + (fi.upper - fi.lower) / 2; }
+
+void ModelFromLane(const hw_lane_model& l, hw_frame_interval fi, Model& m)
+{
+    FZ
+    {
+        m.bw[z] = f16_bits_to_f32(l.baseline.weights[z]);
+        m.bm[z] = f16_bits_to_f32(l.baseline.means[z]);
+        m.bv[z] = f16_bits_to_f32(l.baseline.vars[z]);
+        for (int a = 0; a < kAnalogs; ++a)
+        {
+            m.aw[a][z] = f16_bits_to_f32(l.analogs[a].weights[z]);
+            m.am[a][z] = f16_bits_to_f32(l.analogs[a].means[z]);
+            m.av[a][z] = f16_bits_to_f32(l.analogs[a].vars[z]);
+        }
+        m.conf[z] = f16_bits_to_f32(l.confidence[z]);
+    }
+    m.fi = fi;
+}
+
+// ExportTo, DetectionModelHost.cpp:226-234, 277-285
+void ModelToLane(const Model& m, hw_lane_model& l)
+{
+    const float varMax = round_f16(65000.0f);
+    FZ
+    {
+        l.baseline.weights[z] = f32_to_f16_bits(m.bw[z]);
+        l.baseline.means[z] = f32_to_f16_bits(m.bm[z]);
+        l.baseline.vars[z] = f32_to_f16_bits(fmin_sse(m.bv[z], varMax));
+        for (int a = 0; a < kAnalogs; ++a)
+        {
+            l.analogs[a].weights[z] = f32_to_f16_bits(m.aw[a][z]);
+            l.analogs[a].means[z] = f32_to_f16_bits(m.am[a][z]);
+            l.analogs[a].vars[z] = f32_to_f16_bits(fmin_sse(m.av[a][z], varMax));
+        }
+        l.confidence[z] = f32_to_f16_bits(m.conf[z]);
+    }
+}
+
+struct DmeCtx
+{
+    const hw_config* cfg;
+    const hwp::Derived* d;
+};
+
+// ModelSignalCovar, DetectionModelHost.cpp:237-245
+inline float SignalCovar(const DmeCtx& c, float cv2, float mean, float blVar)
+{
+    float r = blVar;
+    r += c.cfg->shot_var_coeff * mean;
+    r += cv2 * (mean * mean);
+    return r;
+}
+
+// XsnCoeffCVSq, DetectionModelHost.cpp:248-256
+inline float XsnCoeffCVSq(const DmeCtx& c, float mean, float covar, float blVar)
+{
+    float r = covar - blVar;
+    r -= mean * c.cfg->shot_var_coeff;
+    r /= (mean * mean);
+    return r;
+}
+
+// Update0/1/2, DetectionModelHost.cpp:52-187
+void ModelUpdate(const DmeCtx& c, Model& t, const Model& o, const float* fraction)
+{
+    const uint32_t method = c.cfg->model_update_method;
+    FZ
+    {
+        const float a = 1.0f - fraction[z];
+        const float b = fraction[z];
+        if (method == 0)
+        {
+            t.bm[z] = a * t.bm[z] + b * o.bm[z];
+            t.bv[z] = a * t.bv[z] + b * o.bv[z];
+            for (int i = 0; i < kAnalogs; ++i)
+            {
+                t.am[i][z] = a * t.am[i][z] + b * o.am[i][z];
+                t.av[i][z] = a * t.av[i][z] + b * o.av[i][z];
+            }
+        }
+        else
+        {
+            const float prevBlCovar = t.bv[z];
+            const float bw = a * t.bw[z] + b * o.bw[z];
+            t.bw[z] = bw;
+            t.bm[z] = a * t.bm[z] + b * o.bm[z];
+            const float bv = pow_f(t.bv[z], a) * pow_f(o.bv[z], b);
+            t.bv[z] = bv;
+            const float aw = 0.25f * (1.0f - bw);
+            for (int i = 0; i < kAnalogs; ++i)
+            {
+                t.aw[i][z] = aw;
+                float cv2;
+                if (method == 1)
+                {
+                    const float cv = c.cfg->analogs[i].excess_noise_cv;
+                    cv2 = cv * cv;
+                }
+                else
+                {
+                    const float tX = XsnCoeffCVSq(c, t.am[i][z], t.av[i][z], prevBlCovar);
+                    const float oX = XsnCoeffCVSq(c, o.am[i][z], o.av[i][z], o.bv[z]);
+                    cv2 = a * tX + b * oX;
+                }
+                const float am = pow_f(t.am[i][z], a) * pow_f(o.am[i][z], b);
+                t.am[i][z] = am;
+                t.av[i][z] = SignalCovar(c, cv2, am, bv);
+            }
+        }
+    }
+    t.fi = o.fi;
+}
+
+// Update(other), DetectionModelHost.cpp:207-223
+void ModelUpdate(const DmeCtx& c, Model& t, const Model& o)
+{
+    float confSum[kLane], frac[kLane];
+    FZ
+    {
+        confSum[z] = t.conf[z] + o.conf[z];
+        frac[z] = (confSum[z] > 0.0f) ? o.conf[z] / confSum[z] : 0.0f;
+    }
+    ModelUpdate(c, t, o, frac);
+    FZ t.conf[z] = confSum[z];
+}
+
+}   // namespace
+
+// ---------------------------------------------------------------------------
+// The pool object: one instance of every filter for one pool.
+
+struct OraclePool
+{
+    hw_config cfg;
+    hwp::Derived d;
+    uint32_t poolId, lanes, F;
+
+    // Baseliner
+    std::vector<LaneBaseliner> bl;
+    int32_t blNextFrame = 0;
+    // Aggregator
+    std::vector<BlStatAcc> agg;
+    hw_frame_interval aggFi{0, 0};
+    // Histogram
+    std::vector<LaneHist> hist;
+    std::vector<EdgeClassifier> edge;
+    bool histInit = false;
+    hw_frame_interval histFi{0, 0};
+    // Labeler latent state (FrameLabelerHost.cpp:54-114)
+    std::vector<hw_lane_model> latModel;
+    std::vector<int16_t> latLabel, latRoi, latTrc, prevLat;   // [lane][64], [lane][24][64]
+    // Pulse accumulator segments (HostPulseAccumulator.h:64-173)
+    struct Segment
+    {
+        uint32_t start[kLane], end[kLane];
+        int16_t first[kLane], last[kLane], mx[kLane];
+        float total[kLane], m2[kLane];
+        int16_t label[kLane];
+    };
+    std::vector<Segment> seg;
+
+    bool Init(const hw_config& c, uint32_t pid, uint32_t nl, uint32_t f)
+    {
+        cfg = c; poolId = pid; lanes = nl; F = f;
+        std::string err;
+        if (!hwp::Validate(cfg, &err) || !hwp::Derive(cfg, &d, &err)) { g_err = err; return false; }
+        if (F % d.aggStride != 0 || F < (uint32_t)hwp::kLatentFrames + hwp::kViterbiStitchLookback)
+        { g_err = "frames_per_chunk incompatible with the filter strides or latency"; return false; }
+        bl.resize(lanes);
+        for (auto& b : bl) b.Init(d);
+        agg.resize(lanes);
+        for (auto& a : agg) a.Reset();
+        hist.resize(lanes);
+        edge.resize(lanes);
+        for (auto& e : edge) e.Init();
+        latModel.resize(lanes);
+        latLabel.assign((size_t)lanes * kLane, 0);
+        latRoi.assign((size_t)lanes * kLane, 0);
+        latTrc.assign((size_t)lanes * kLane, 0);
+        prevLat.assign((size_t)lanes * hwp::kLatentFrames * kLane, 0);
+        for (auto& m : latModel)
+        {
+            std::memset(&m, 0, sizeof(m));
+            FZ
+            {
+                m.baseline.means[z] = f32_to_f16_bits(0.0f);
+                m.baseline.vars[z] = f32_to_f16_bits(50.0f);
+                for (int a = 0; a < kAnalogs; ++a)
+                {
+                    m.analogs[a].means[z] = f32_to_f16_bits(1000.0f);
+                    m.analogs[a].vars[z] = f32_to_f16_bits(10.0f);
+                }
+            }
+        }
+        seg.resize(lanes);
+        for (auto& s : seg) std::memset(&s, 0, sizeof(s));
+        return true;
+    }
+
+    // ---- Baseliner --------------------------------------------------------
+    int Baseline(const int16_t* trace, int32_t firstFrame, int16_t* out, hw_baseliner_stats* stats)
+    {
+        const size_t blk = (size_t)F * kLane;
+        int status = HW_OK;
+#pragma omp parallel
+        {
+            std::vector<int16_t> lo, up;
+            BlStatAcc st;
+#pragma omp for schedule(dynamic, 4)
+            for (int64_t l = 0; l < (int64_t)lanes; ++l)
+            {
+                bl[l].Estimate(d, trace + l * blk, (int)F, out + l * blk, st, lo, up);
+                st.Store(stats[l]);
+            }
+        }
+        blNextFrame = firstFrame + (int32_t)F;
+        return status;
+    }
+
+    // ---- BaselineStatsAggregatorHost.cpp --------------------------------
+    void AggAdd(const hw_baseliner_stats* stats, hw_frame_interval fi)
+    {
+#pragma omp parallel for schedule(static)
+        for (int64_t l = 0; l < (int64_t)lanes; ++l)
+        {
+            BlStatAcc o;
+            o.Load(stats[l]);
+            agg[l].Merge(o);
+        }
+        if (aggFi.lower == aggFi.upper) aggFi = fi;
+        else if (fi.lower != fi.upper)
+            aggFi = hw_frame_interval{std::min(aggFi.lower, fi.lower), std::max(aggFi.upper, fi.upper)};
+    }
+    void AggGet(hw_baseliner_stats* out, hw_frame_interval* fi) const
+    {
+        for (uint32_t l = 0; l < lanes; ++l) agg[l].Store(out[l]);
+        if (fi) *fi = aggFi;
+    }
+    void AggReset()
+    {
+        for (auto& a : agg) a.Reset();
+        aggFi = hw_frame_interval{0, 0};
+    }
+
+    // ---- TraceHistogramAccumHost::ResetImpl(metrics), :96-126 -----------
+    int HistResetStats(const hw_baseliner_stats* stats)
+    {
+        bool ok = true;
+        for (uint32_t l = 0; l < lanes; ++l)
+        {
+            StatAcc s;
+            s.Load(stats[l].baseline_stats);
+            float lo[kLane], up[kLane];
+            FZ
+            {
+                const bool suff = s.m0[z] >= (float)cfg.baseline_stat_min_frame_count;
+                const float mean = suff ? s.Mean(z) : 0.0f;
+                const float sigma = suff ? std::sqrt(s.Variance(z)) : cfg.fallback_baseline_sigma;
+                const float binSize = fmax_sse(cfg.bin_size_coeff * sigma, d.binSizeMin);
+                lo[z] = mean - 4.0f * sigma;
+                up[z] = lo[z] + float(kBins) * binSize;
+            }
+            ok &= HistInit(hist[l], lo, up);
+        }
+        histInit = true;
+        histFi = hw_frame_interval{0, 0};
+        if (!ok) { g_err = "UHistogramSimd: bad histogram bounds"; return HW_ERR_NUMERIC; }
+        return HW_OK;
+    }
+
+    int HistResetBounds(const hw_lane_hist_bounds* b)
+    {
+        bool ok = true;
+        for (uint32_t l = 0; l < lanes; ++l) ok &= HistInit(hist[l], b[l].lower_bounds, b[l].upper_bounds);
+        histInit = true;
+        histFi = hw_frame_interval{0, 0};
+        if (!ok) { g_err = "UHistogramSimd: bad histogram bounds"; return HW_ERR_NUMERIC; }
+        return HW_OK;
+    }
+
+    // ---- AddBlock, TraceHistogramAccumHost.cpp:140-169 ------------------
+    int HistAdd(const int16_t* traces, uint32_t frames, hw_frame_interval fi, const hw_lane_model* models)
+    {
+        if (!histInit)
+        {
+            g_err = "Cannot aggregate trace data into histograms before calling Reset with the desired histogram bounds";
+            return HW_ERR_NOT_INITIALIZED;
+        }
+#pragma omp parallel for schedule(dynamic, 4)
+        for (int64_t l = 0; l < (int64_t)lanes; ++l)
+        {
+            LaneHist& h = hist[l];
+            EdgeClassifier& e = edge[l];
+            int16_t thr[kLane];
+            FZ
+            {
+                const float bm = f16_bits_to_f32(models[l].baseline.means[z]);
+                const float bv = f16_bits_to_f32(models[l].baseline.vars[z]);
+                thr[z] = i16_wrap(cvt_rn_i32(2.0f * std::sqrt(bv) + bm));
+            }
+            const int16_t* tr = traces + (size_t)l * frames * kLane;
+            for (uint32_t f = 0; f < frames; ++f)
+            {
+                const int16_t* fr = tr + (size_t)f * kLane;
+                const bool full = (e.hsize == 2);
+                const int slotFront = e.hfront;
+                FZ
+                {
+                    // EdgeFrameClassifier::IsEdgeFrame (EdgeFrameClassifier.h:72-94)
+                    const bool isBl = fr[z] < thr[z];
+                    const bool edgeF = full ? (isBl ^ e.hist[slotFront][z]) : true;
+                    const int16_t cand = e.prev[z];
+                    e.prev[z] = fr[z];
+                    // UHistogramSimd::AddDatum (UHistogramSimd.h:207-229)
+                    const bool sel = !edgeF;
+                    const float x = (float)cand;
+                    int32_t bin = floor_cast_i32((x - h.lower[z]) / h.binSize[z]);
+                    const bool mLow = sel & (bin < 0);
+                    const bool mHigh = sel & (bin >= kBins);
+                    if (mLow) h.nLow[z] = (uint16_t)(h.nLow[z] + 1);
+                    if (mHigh) h.nHigh[z] = (uint16_t)(h.nHigh[z] + 1);
+                    if ((!sel) | mLow | mHigh) bin = kBins;
+                    h.count[bin][z] = (uint16_t)(h.count[bin][z] + 1);
+                }
+                // CircularArray<LaneMask,2>::push_back (CM/CircularArray.h)
+                if (e.hsize < 2)
+                {
+                    const int slot = (e.hfront + e.hsize) % 2;
+                    FZ e.hist[slot][z] = fr[z] < thr[z];
+                    ++e.hsize;
+                }
+                else
+                {
+                    const int slot = e.hfront;
+                    FZ e.hist[slot][z] = fr[z] < thr[z];
+                    e.hfront = (e.hfront + 1) % 2;
+                }
+            }
+        }
+        if (histFi.lower == histFi.upper) histFi = fi;
+        else histFi = hw_frame_interval{std::min(histFi.lower, fi.lower), std::max(histFi.upper, fi.upper)};
+        return HW_OK;
+    }
+
+    // HistogramImpl, TraceHistogramAccumHost.cpp:172-199
+    void HistGet(hw_lane_histogram* out, hw_frame_interval* fi) const
+    {
+        for (uint32_t l = 0; l < lanes; ++l)
+        {
+            const LaneHist& h = hist[l];
+            FZ
+            {
+                out[l].low_bound[z] = h.lower[z];
+                out[l].bin_size[z] = h.binSize[z];
+                out[l].outlier_count_low[z] = h.nLow[z];
+                out[l].outlier_count_high[z] = h.nHigh[z];
+                for (int b = 0; b < kBins; ++b) out[l].bin_count[b][z] = h.count[b][z];
+            }
+        }
+        if (fi) *fi = histFi;
+    }
+
+    // ---- DmeEmHost::InitLaneDetModel, DmeEmHost.cpp:872-925 -------------
+    void InitModels(const hw_baseliner_stats* stats, hw_lane_model* out)
+    {
+        const DmeCtx c{&cfg, &d};
+        const bool fixedBl = false;
+        for (uint32_t l = 0; l < lanes; ++l)
+        {
+            StatAcc blS, tot;
+            blS.Load(stats[l].baseline_stats);
+            tot.Load(stats[l].full_autocorr.basic_stats);
+            hw_lane_model& m = out[l];
+            FZ
+            {
+                const float blWeight = blS.m0[z] / tot.m0[z];
+                float blMean = fixedBl ? 0.0f : blS.Mean(z);
+                float blVar = blS.Variance(z);
+                blMean = std::isnan(blMean) ? 0.0f : blMean;     // FallbackBaselineMean
+                blVar = std::isnan(blVar) ? 100.0f : blVar;      // FallbackBaselineVariance
+                blVar = fmin_sse(fmax_sse(blVar, d.blVarMin), d.blVarMax);
+                m.confidence[z] = f32_to_f16_bits(0.1f);
+                m.baseline.weights[z] = f32_to_f16_bits(blWeight);
+                m.baseline.means[z] = f32_to_f16_bits(blMean);
+                m.baseline.vars[z] = f32_to_f16_bits(blVar);
+                const float amw = (1.0f - blWeight) / (float)kAnalogs;
+                const float refSignal = cfg.ref_snr * std::sqrt(blVar);
+                for (int a = 0; a < kAnalogs; ++a)
+                {
+                    m.analogs[a].weights[z] = f32_to_f16_bits(amw);
+                    const float aMean = fmax_sse(0.0f, blMean + cfg.analogs[a].rel_amplitude * refSignal);
+                    m.analogs[a].means[z] = f32_to_f16_bits(aMean);
+                    const float cv = cfg.analogs[a].excess_noise_cv;
+                    m.analogs[a].vars[z] = f32_to_f16_bits(SignalCovar(c, cv * cv, aMean, blVar));
+                }
+            }
+        }
+    }
+
+    int Estimate(const hw_lane_histogram* h, const hw_baseliner_stats* stats, hw_frame_interval histFi_,
+                 hw_frame_interval modelFi, hw_lane_model* models, hw_dme_diag* diag);
+
+    int Label(const int16_t* traces, const hw_lane_model* models, int16_t* labels, int16_t* latOut, float* score);
+
+    int Pulses(const int16_t* labels, const int16_t* latTrace, const int16_t* trace, int32_t firstFrame,
+               const hw_lane_model* models, hw_pulse* pulses, uint32_t* lens, uint32_t* ovf,
+               hw_stat_accum_state* blstats);
+};
+
+// ---------------------------------------------------------------------------
+// DME: TA/DmeEmHost.cpp:131-852
+
+namespace {
+
+struct UHist   // UHistogramSimd built from a LaneHistogram (UHistogramSimd.cpp:100-121)
+{
+    const hw_lane_histogram* h;
+    float BinStart(int b, int z) const { return h->low_bound[z] + (float)b * h->bin_size[z]; }
+    uint16_t Count(int b, int z) const { return b < kBins ? h->bin_count[b][z] : (uint16_t)0; }
+    uint16_t InRange(int z) const
+    {
+        uint16_t s = 0;
+        for (int b = 0; b < kBins; ++b) s = (uint16_t)(s + h->bin_count[b][z]);
+        return s;
+    }
+    uint16_t Total(int z) const
+    { return (uint16_t)(InRange(z) + (uint16_t)(h->outlier_count_low[z] + h->outlier_count_high[z])); }
+
+    // CumulativeCount, UHistogramSimd.cpp:204-242
+    float Cumulative(float x, int z) const
+    {
+        const float lb = BinStart(0, z), ub = BinStart(kBins, z);
+        const bool mNan = std::isnan(x), mLow = x < lb, mHigh = x >= ub;
+        const bool inB = !(mNan | mLow | mHigh);
+        int32_t xbin = floor_cast_i32((x - lb) / h->bin_size[z]);
+        xbin = inB ? xbin : 0;
+        const float xrem = x - BinStart(xbin, z);
+        const float xbinCount = (float)Count(xbin, z);
+        float cc = (float)h->outlier_count_low[z];
+        uint16_t cn = 0;
+        for (int i = 0; i < std::min(kBins, xbin); ++i) cn = (uint16_t)(cn + h->bin_count[i][z]);
+        cc += (float)cn;
+        cc += xbinCount * xrem / h->bin_size[z];
+        cc = mLow ? (float)h->outlier_count_low[z] : cc;
+        cc = mHigh ? (float)(uint16_t)(h->outlier_count_low[z] + InRange(z)) : cc;
+        cc = mNan ? kNaN : cc;
+        return cc;
+    }
+
+    // Fractile, UHistogramSimd.cpp:142-201 (per ZMW)
+    float Fractile(float frac, int z) const
+    {
+        const float nfz = frac * (float)Total(z);
+        uint16_t n = h->outlier_count_low[z];
+        if (n > 0 && n >= nfz) return -kInf;
+        int i = 0;
+        while ((n == 0 || n < nfz) && i < kBins) n = (uint16_t)(n + h->bin_count[i++][z]);
+        if (n < nfz) return kInf;
+        i -= 1;
+        const float x0 = BinStart(i, z);
+        const uint16_t niz = h->bin_count[i][z];
+        const int m = (int)n - (int)niz;
+        return x0 + h->bin_size[z] * (nfz - (float)m) / (float)(niz + 1);
+    }
+};
+
+}   // namespace
+
+int OraclePool::Estimate(const hw_lane_histogram* hh, const hw_baseliner_stats* stats, hw_frame_interval hfi,
+                         hw_frame_interval pfi, hw_lane_model* models, hw_dme_diag* diag)
+{
+    const DmeCtx c{&cfg, &d};
+    int status = HW_OK;
+    std::string errMsg;
+    const int nModes = kAnalogs + 1;
+    const int nB = kBins;
+
+#pragma omp parallel
+    {
+        std::vector<float> tau((size_t)nModes * (nB + 1) * kLane);
+        std::vector<float> bprob((size_t)(nB + 1) * kLane), binProb((size_t)nB * kLane), nj((size_t)nB * kLane);
+#pragma omp for schedule(dynamic, 1)
+        for (int64_t l = 0; l < (int64_t)lanes; ++l)
+        {
+            Model det;
+            ModelFromLane(models[l], pfi, det);
+            BlStatAcc bsa;
+            bsa.Load(stats[l]);
+            UHist hist{&hh[l]};
+
+            // EvolveModel, DmeEmHost.cpp:806-834
+            {
+                const int32_t tModel = CenterInt(det.fi), tEst = CenterInt(hfi);
+                const float thl = 0.5f * (float)(tModel + tEst);
+                const float t0 = 56160.0f, t1 = 168480.0f;
+                const float hl0 = cfg.confidence_half_life[0], hl1 = cfg.confidence_half_life[1];
+                const float hl = hl0 + (hl1 - hl0) * satlin_std(t0, t1, thl);
+                // EvolveConfidence, DetectionModelHost.h:166-177
+                const float tDiff = static_cast<float>(CenterInt(hfi) - CenterInt(det.fi));
+                FZ { const float m = exp2_f(-std::abs(tDiff) / hl); det.conf[z] *= m; }
+                det.fi = hfi;
+            }
+
+            // PrelimEstimate, DmeEmHost.cpp:161-214
+            Model work = det;
+            {
+                const float blVarMax = d.blVarMax;
+                FZ
+                {
+                    const float nBl = bsa.blStats.m0[z];
+                    const float tot = bsa.corr.stats.m0[z];
+                    const float blWeight = fmax_sse(nBl / tot, 0.01f);
+                    const bool mask = nBl >= 3.0f;
+                    float blVar = mask ? bsa.blStats.Variance(z) : work.bv[z];
+                    blVar = fmin_sse(fmax_sse(blVar, d.blVarMin), blVarMax);
+                    const float blMean = mask ? bsa.blStats.Mean(z) : work.bm[z];
+                    const float scale = std::sqrt(blVar / work.bv[z]);
+                    for (int i = 0; i < kAnalogs; ++i)
+                    {
+                        const float mean = work.am[i][z] * scale;
+                        const float cv = cfg.analogs[i].excess_noise_cv;
+                        const float cv2 = cv * cv;
+                        work.am[i][z] = mean;
+                        work.av[i][z] = SignalCovar(c, cv2, mean, blVar);
+                        work.aw[i][z] = 0.25f * (1.0f - blWeight);
+                    }
+                    work.bw[z] = blWeight;
+                    work.bm[z] = blMean;
+                    work.bv[z] = blVar;
+                    float conf = 0.1f * satlin_sse(0.0f, 500.0f, nBl - 3.0f);
+                    conf *= satlin_sse(blVarMax, 0.5f * (d.blVarNominal + blVarMax), blVar);
+                    work.conf[z] = conf;
+                }
+            }
+            ModelUpdate(c, det, work);
+            work = det;
+
+            // PrelimScaleFactor, DmeEmHost.cpp:620-654
+            float scaleFactor[kLane];
+            FZ
+            {
+                const float bgSigma = std::sqrt(work.bv[z]);
+                const float thresh = 2.5f * bgSigma + work.bm[z];
+                const float bgCount = hist.Cumulative(thresh, z);
+                const float totalCount = (float)(uint16_t)(hh[l].outlier_count_low[z] + hist.InRange(z));
+                const float fractile = 0.5f * (bgCount + totalCount) / totalCount;
+                float avg = 0.0f;
+                for (int a = 0; a < kAnalogs; ++a) avg += work.am[a][z];
+                avg /= static_cast<float>(kAnalogs);
+                const float w = satlin_sse(0.0f, cfg.scale_snr_conf_tol, work.conf[z]);
+                float sf = hist.Fractile(fractile, z) / avg;
+                sf = (1.0f - w) * sf + w;
+                scaleFactor[z] = fmin_sse(fmax_sse(sf, 0.1f), 10.0f);
+            }
+            // ScaleModelSnr, DmeEmHost.cpp:837-852
+            FZ
+            {
+                const float blCovar = work.bv[z];
+                for (int a = 0; a < kAnalogs; ++a)
+                {
+                    work.am[a][z] = scaleFactor[z] * work.am[a][z];
+                    const float cv = cfg.analogs[a].excess_noise_cv;
+                    work.av[a][z] = SignalCovar(c, cv * cv, work.am[a][z], blCovar);
+                }
+            }
+
+            // EM setup, DmeEmHost.cpp:253-361
+            const float rhoMin = 0.001f;
+            float rho[5][kLane], mu[5][kLane], var[5][kLane];
+            float rhoEst[5][kLane], muEst[5][kLane], varEst[5][kLane];
+            float varQuant[kLane], s[kLane], sExpect[kLane], sExpectW[kLane];
+            float logLike[kLane], binProbMin[kLane], nSum[kLane];
+            int32_t zStatus[kLane];
+            bool conv[kLane], mConverged[kLane];
+            int32_t mIter[kLane];
+            float mLogLike[kLane];
+            float rpa[kAnalogs];
+            for (int a = 0; a < kAnalogs; ++a) rpa[a] = cfg.analogs[a].rel_amplitude;
+            FZ
+            {
+                rho[0][z] = fmax_sse(work.bw[z], rhoMin);
+                mu[0][z] = work.bm[z];
+                var[0][z] = work.bv[z];
+                for (int a = 0; a < kAnalogs; ++a)
+                {
+                    rho[a + 1][z] = fmax_sse(work.aw[a][z], rhoMin);
+                    mu[a + 1][z] = work.am[a][z];
+                    var[a + 1][z] = work.av[a][z];
+                }
+                const float bs = hh[l].bin_size[z];
+                varQuant[z] = (bs * bs) / 12.0f;
+                for (int k = 0; k < 5; ++k) var[k][z] += varQuant[z];
+                var[0][z] = fmin_sse(var[0][z], d.blVarMax);
+                // Eigen fixed-size-5 sum: (r0 + r1) + (r2 + (r3 + r4))
+                const float rs = (rho[0][z] + rho[1][z]) + (rho[2][z] + (rho[3][z] + rho[4][z]));
+                for (int k = 0; k < 5; ++k) rho[k][z] = rho[k][z] / rs;
+                for (int k = 0; k < 5; ++k) { rhoEst[k][z] = rho[k][z]; muEst[k][z] = mu[k][z]; varEst[k][z] = var[k][z]; }
+                // Eigen fixed-size-4 sum: (p0 + p1) + (p2 + p3)
+                const float p0 = mu[1][z] * rpa[0], p1 = mu[2][z] * rpa[1], p2 = mu[3][z] * rpa[2], p3 = mu[4][z] * rpa[3];
+                s[z] = ((p0 + p1) + (p2 + p3)) / d.rpaSum2;
+                sExpect[z] = s[z] / scaleFactor[z];
+                sExpectW[z] = det.conf[z] * cfg.pulse_amp_regularization;
+                logLike[z] = std::numeric_limits<float>::lowest();
+                const uint16_t nf = hist.Total(z);
+                binProbMin[z] = fmax_sse((float)nf * bs, 1.0f) * std::numeric_limits<float>::min();
+                zStatus[z] = (nf < 160u) ? 2 /*INSUF_DATA*/ : 0;
+                mConverged[z] = false; mIter[z] = 0; mLogLike[z] = -kInf;
+                nSum[z] = 0.0f;
+            }
+            for (int j = 0; j < nB; ++j)
+                FZ { nj[(size_t)j * kLane + z] = (float)hh[l].bin_count[j][z]; nSum[z] += nj[(size_t)j * kLane + z]; }
+
+            auto TAU = [&](int m, int b) -> float* { return &tau[((size_t)m * (nB + 1) + b) * kLane]; };
+            auto BP = [&](int b) -> float* { return &bprob[(size_t)b * kLane]; };
+            auto BPR = [&](int b) -> float* { return &binProb[(size_t)b * kLane]; };
+
+            const unsigned iterLimit = cfg.em_iteration_limit;
+            unsigned it = 0;
+            for (; it < iterLimit; ++it)
+            {
+                float varinv[5][kLane], pref[5][kLane];
+                const float halfLog2pi = 0.5f * d.logTwoPi;
+                FZ for (int k = 0; k < 5; ++k)
+                {
+                    varinv[k][z] = 1.0f / var[k][z];
+                    pref[k][z] = (hw_logf(rho[k][z]) - 0.5f * hw_logf(var[k][z])) - halfLog2pi;
+                }
+                float probSum[kLane], wps[kLane], ci[5][kLane], mom1[5][kLane];
+                FZ { probSum[z] = 0; wps[z] = 0; for (int k = 0; k < 5; ++k) { ci[k][z] = 0; mom1[k][z] = 0; } }
+
+                auto corner = [&](int b) {
+                    FZ
+                    {
+                        const float x = hist.BinStart(b, z);
+                        float t[5];
+                        for (int i = 0; i < 5; ++i)
+                        {
+                            const float y = x - mu[i][z];
+                            t[i] = pref[i][z] - 0.5f * y * y * varinv[i][z];
+                        }
+                        float tmax = t[0];
+                        for (int i = 1; i < 5; ++i) tmax = fmax_sse(tmax, t[i]);
+                        float se = hw_expf(t[0] - tmax);
+                        for (int i = 1; i < 5; ++i) se = se + hw_expf(t[i] - tmax);
+                        const float llb = tmax + hw_logf(se);
+                        for (int i = 0; i < 5; ++i) TAU(i, b)[z] = hw_expf(t[i] - llb);
+                        BP(b)[z] = hw_expf(llb);
+                    }
+                };
+                auto center = [&](int b) {
+                    FZ
+                    {
+                        const float bs = hh[l].bin_size[z];
+                        const float bp0 = BP(b)[z], bp1 = BP(b + 1)[z];
+                        const float bpr = fmax_sse(0.5f * bs * (bp0 + bp1), binProbMin[z]);
+                        BPR(b)[z] = bpr;
+                        probSum[z] += bpr;
+                        const float njb = nj[(size_t)b * kLane + z];
+                        wps[z] += njb * hw_logf(bpr);
+                        const float factor = njb / bpr;
+                        const float x0 = hist.BinStart(b, z), x1 = hist.BinStart(b + 1, z);
+                        for (int m = 0; m < 5; ++m)
+                        {
+                            const float tmp1 = bp0 * TAU(m, b)[z];
+                            const float tmp2 = bp1 * TAU(m, b + 1)[z];
+                            ci[m][z] += (tmp1 + tmp2) * factor;
+                            mom1[m][z] += (tmp1 * x0 + tmp2 * x1) * factor;
+                        }
+                    }
+                };
+                corner(0);
+                for (int b = 0; b < nB; ++b) { corner(b + 1); center(b); }
+
+                bool anyConv = false, allDone = true;
+                FZ
+                {
+                    const float hb = 0.5f * hh[l].bin_size[z];
+                    for (int k = 0; k < 5; ++k) { ci[k][z] *= hb; mom1[k][z] *= hb; }
+                    const float prev = logLike[z];
+                    float ll = wps[z] - nSum[z] * hw_logf(probSum[z]);
+                    const float ds = s[z] - sExpect[z];
+                    ll -= 0.5f * (ds * ds) * sExpectW[z];
+                    logLike[z] = ll;
+                    const float delta = ll - prev;
+                    const float convTol = 1e-4f * fmax_sse(ll, -ll);
+                    bool cv = (delta >= 0) & (delta < convTol);
+                    cv &= (ll >= mLogLike[z]);
+                    conv[z] = cv;
+                    // MaxLikelihoodDiagnostics::Converged (MaxLikelihoodDiagnostics.h:85-96)
+                    mIter[z] = (cv & !mConverged[z]) ? (int32_t)it : mIter[z];
+                    mLogLike[z] = cv ? ll : mLogLike[z];
+                    mConverged[z] |= cv;
+                    anyConv |= cv;
+                    allDone &= (mConverged[z] | (zStatus[z] != 0));
+                }
+                if (anyConv)
+                    FZ for (int k = 0; k < 5; ++k)
+                    {
+                        rhoEst[k][z] = conv[z] ? rho[k][z] : rhoEst[k][z];
+                        muEst[k][z] = conv[z] ? mu[k][z] : muEst[k][z];
+                        varEst[k][z] = conv[z] ? var[k][z] : varEst[k][z];
+                    }
+                if (!cfg.iterate_to_limit && allDone) break;
+
+                // M-step, DmeEmHost.cpp:494-565
+                FZ
+                {
+                    for (int k = 0; k < 5; ++k) ci[k][z] = fmax_sse(ci[k][z], 0.1f);
+                    for (int k = 0; k < 5; ++k) rho[k][z] = ci[k][z] / nSum[z];
+                    const float rs = (rho[0][z] + rho[1][z]) + (rho[2][z] + (rho[3][z] + rho[4][z]));
+                    for (int k = 0; k < 5; ++k) rho[k][z] = rho[k][z] / rs;
+                    mu[0][z] = mom1[0][z] / ci[0][z];
+                    float numer = 0.0f, denom = 0.0f;
+                    for (int a = 0; a < kAnalogs; ++a)
+                    {
+                        const int i = a + 1;
+                        numer += rpa[a] * varinv[i][z] * mom1[i][z];
+                        denom += (rpa[a] * rpa[a]) * varinv[i][z] * ci[i][z];
+                    }
+                    numer += sExpect[z] * sExpectW[z];
+                    denom += sExpectW[z];
+                    float sv = numer / denom;
+                    const float sMin = fmax_sse(0.5f * std::sqrt(var[0][z]), d.minPulseMean) / d.rpaMin;
+                    const bool vls = sv < sMin;
+                    sv = vls ? sMin : sv;
+                    if (vls) zStatus[z] |= 4;   // VLOW_SIGNAL
+                    s[z] = sv;
+                    for (int a = 0; a < kAnalogs; ++a) mu[a + 1][z] = sv * rpa[a];
+                }
+                float mom2[kLane];
+                FZ mom2[z] = 0.0f;
+                for (int j = 0; j < nB; ++j)
+                {
+                    const int k = j + 1;
+                    FZ
+                    {
+                        const float x0 = hist.BinStart(j, z) - mu[0][z];
+                        const float x1 = hist.BinStart(k, z) - mu[0][z];
+                        float tmp = BP(j)[z] * x0 * x0 * TAU(0, j)[z];
+                        tmp += BP(k)[z] * x1 * x1 * TAU(0, k)[z];
+                        tmp *= nj[(size_t)j * kLane + z] / BPR(j)[z];
+                        mom2[z] += tmp;
+                    }
+                }
+                FZ
+                {
+                    mom2[z] *= 0.5f * hh[l].bin_size[z];
+                    float v0 = mom2[z] / ci[0][z] + varQuant[z];
+                    v0 = fmin_sse(fmax_sse(v0, d.blVarMin), d.blVarMax);
+                    var[0][z] = v0;
+                    for (int a = 0; a < kAnalogs; ++a)
+                    {
+                        const float cv = cfg.analogs[a].excess_noise_cv;
+                        var[a + 1][z] = SignalCovar(c, cv * cv, mu[a + 1][z], v0);
+                    }
+                }
+            }
+            const int laneIters = (int)std::min(it + 1, iterLimit);
+
+            bool finite = true;
+            FZ
+            {
+                if (!mConverged[z]) zStatus[z] |= 1;    // NO_CONVERGE
+                for (int k = 0; k < 5; ++k)
+                    finite &= std::isfinite(rhoEst[k][z]) & std::isfinite(muEst[k][z]) & std::isfinite(varEst[k][z]);
+                work.bw[z] = rhoEst[0][z]; work.bm[z] = muEst[0][z]; work.bv[z] = varEst[0][z];
+                for (int a = 0; a < kAnalogs; ++a)
+                { work.aw[a][z] = rhoEst[a + 1][z]; work.am[a][z] = muEst[a + 1][z]; work.av[a][z] = varEst[a + 1][z]; }
+            }
+            if (!finite)
+            {
+#pragma omp critical
+                { status = HW_ERR_NUMERIC; errMsg = "DME: non-finite EM estimate (all(isfinite(...)) assertion)"; }
+            }
+
+            // ComputeConfidence, DmeEmHost.cpp:717-803 (G-test disabled: pValue = 1)
+            float conf[kLane];
+            bool assertOk = true;
+            FZ
+            {
+                float cf[8];
+                cf[0] = mConverged[z] ? 1.0f : 0.0f;
+                cf[1] = satlin_sse(0.05f, 0.15f, work.bw[z]);
+                float x = (work.bm[z] * work.bm[z]) / work.bv[z];
+                x = hw_expf(-x / 2.0f);
+                cf[2] = x;
+                x = log2_f(work.bv[z] / det.bv[z]);
+                const float bgVarTol = 1.5f / (0.5f + det.conf[z]);
+                x = hw_expf(-x * x / (2.0f * (bgVarTol * bgVarTol)));
+                cf[3] = x;
+                x = 1.0f;
+                if (cfg.analog_mix_fraction_threshold[1] > 0.0f)
+                {
+                    const float t0 = cfg.analog_mix_fraction_threshold[0], t1 = cfg.analog_mix_fraction_threshold[1];
+                    x *= satlin_sse(t0, t1, work.aw[0][z]);
+                    x *= satlin_sse(t0, t1, work.aw[kAnalogs - 1][z]);
+                }
+                cf[4] = x;
+                x = work.am[kAnalogs - 1][z];
+                const float bgSigma = std::sqrt(work.bv[z]);
+                x /= bgSigma;
+                cf[5] = satlin_sse(cfg.min_analog_snr_thresh0, cfg.min_analog_snr_thresh1, x);
+                if (cfg.snr_drop_thresh < 0.0f) cf[6] = 1.0f;
+                else
+                {
+                    const float snrEst = work.am[0][z] / bgSigma;
+                    const float r0 = det.am[0][z], r1 = det.am[1][z];
+                    const float refBgSigma = std::sqrt(det.bv[z]);
+                    assertOk &= (r0 >= 0.0f) & (r1 >= 0.0f) & (refBgSigma >= 0.0f);
+                    const float refSnr0 = r0 / refBgSigma;
+                    float refSnr1 = r1 / refBgSigma;
+                    refSnr1 *= cfg.snr_drop_thresh;
+                    refSnr1 *= fmin_sse(det.conf[z], 1.0f);
+                    assertOk &= (refSnr1 < refSnr0);
+                    cf[6] = satlin_sse(refSnr1, std::sqrt(refSnr0 * refSnr1), snrEst);
+                }
+                cf[7] = 1.0f;
+                float cc = 1.0f;
+                for (int k = 0; k < 8; ++k) cc *= cf[k];
+                cc = fmin_sse(fmax_sse(0.0f, cc), 1.0f);
+                cc = (cc >= cfg.success_confidence_thresh) ? cc : 0.0f;
+                conf[z] = cc;
+                work.conf[z] = cc;
+            }
+            if (!assertOk)
+            {
+#pragma omp critical
+                { status = HW_ERR_NUMERIC; errMsg = "DME: Bad threshold in SNR Drop confidence factor"; }
+            }
+            ModelUpdate(c, det, work);
+            ModelToLane(det, models[l]);
+            if (diag)
+            {
+                FZ
+                {
+                    diag[l].iter_count[z] = mIter[z];
+                    diag[l].converged[z] = mConverged[z] ? 1 : 0;
+                    diag[l].log_like[z] = mLogLike[z];
+                    diag[l].status[z] = zStatus[z];
+                    diag[l].confidence[z] = conf[z];
+                }
+                diag[l].lane_iterations = laneIters;
+            }
+        }
+    }
+    if (status != HW_OK) g_err = errMsg;
+    return status;
+}
+
+// ---------------------------------------------------------------------------
+// Frame labeler: TA/FrameLabelerHost.cpp:54-612, TA/SubframeScorer.h,
+// TA/RoiHost.h
+
+namespace {
+
+// BlockStateSubframeScorer (SubframeScorer.h:152-318), one ZMW.
+struct Scorer
+{
+    float bgMean, bInvVar, bgFixed, x0;
+    float ffMean[4], pInvVar[4], ffFixed[4], logPMean[4], x1[4];
+    float fbMean, fbVar, fbNormTerm, fbScale;
+
+    void Setup(const hwp::Derived& d, const hw_lane_model& m, int z)
+    {
+        constexpr float log2pi_f = 1.8378770664f;
+        const float nhalf = -0.5f;
+        const float halfVal = 0.5f, oneSixth = 1.0f / 6.0f;
+        const float bMean = f16_bits_to_f32(m.baseline.means[z]);
+        const float bVar = f16_bits_to_f32(m.baseline.vars[z]);
+        const float bSigma = std::sqrt(bVar);
+        x0 = bMean + bSigma * d.sqrtHalfPi;
+        bInvVar = 1.0f / bVar;
+        for (int a = 0; a < kAnalogs; ++a)
+        {
+            const float aMean = f16_bits_to_f32(m.analogs[a].means[z]);
+            logPMean[a] = hw_logf(aMean - bMean);
+            const float aVar = f16_bits_to_f32(m.analogs[a].vars[z]);
+            const float aSigma = std::sqrt(aVar);
+            x1[a] = aMean - aSigma * d.sqrtHalfPi;
+            pInvVar[a] = 1.0f / aVar;
+        }
+        {
+            const float aMean = f16_bits_to_f32(m.analogs[3].means[z]);
+            const float aVar = f16_bits_to_f32(m.analogs[3].vars[z]);
+            float eMean = halfVal * (bMean + aMean);
+            float eVar = oneSixth * (aMean - bMean);
+            eVar += bVar + aVar;
+            eVar *= halfVal;
+            fbMean = eMean;
+            fbVar = eVar;
+            // NormalLog::operator() (SubframeScorer.h:117-123); its two
+            // data-independent terms are the same on every call.
+            fbNormTerm = -0.5f * (log2pi_f + hw_logf(fbVar));
+            fbScale = 0.5f / fbVar;
+        }
+        const float normConst = log2pi_f / 2.0f;
+        bgFixed = nhalf * hw_logf(bVar) - normConst;
+        bgMean = bMean;
+        for (int i = 0; i < kAnalogs; ++i)
+        {
+            const float aVar = f16_bits_to_f32(m.analogs[i].vars[z]);
+            ffFixed[i] = nhalf * hw_logf(aVar) - normConst;
+            ffMean[i] = f16_bits_to_f32(m.analogs[i].means[z]);
+        }
+    }
+
+    // SubframeScore, SubframeScorer.h:264-295
+    float Subframe(int a, float val) const
+    {
+        const float nhalf = -0.5f;
+        const bool lowExtrema = val < x0;
+        const float cap = lowExtrema ? x0 : x1[a];
+        float fixedTerm = lowExtrema ? bInvVar : pInvVar[a];
+        fixedTerm = nhalf * fixedTerm;
+        const bool extrema = lowExtrema | (val > x1[a]);
+        const float dv = val - cap;
+        float s = (extrema ? fixedTerm * (dv * dv) : 0.0f) - logPMean[a];
+        if (a == kAnalogs - 1)
+        {
+            const float dm = val - fbMean;
+            const float fb = fbNormTerm - (dm * dm) * fbScale;
+            s = (x0 <= x1[a]) ? s : fb;
+        }
+        return s;
+    }
+
+    // StateScores, SubframeScorer.h:185-228
+    void Scores(float data, float* out) const
+    {
+        const float nhalf = -0.5f;
+        {
+            const float y = data - bgMean;
+            out[0] = nhalf * y * bInvVar * y + bgFixed;
+        }
+        float full[4];
+        for (int i = 0; i < 4; ++i)
+        {
+            const float y = data - ffMean[i];
+            full[i] = nhalf * y * pInvVar[i] * y + ffFixed[i];
+            out[1 + i] = full[i];
+        }
+        for (int i = 0; i < 4; ++i)
+        {
+            float score = Subframe(i, data);
+            score = (data > ffMean[i]) ? fmin_sse(fmin_sse(score, full[i] - 1.0f), 0.0f) : score;
+            out[5 + i] = score;
+            out[9 + i] = score;
+        }
+    }
+};
+
+}   // namespace
+
+int OraclePool::Label(const int16_t* traces, const hw_lane_model* models, int16_t* labels,
+                      int16_t* latOut, float* score)
+{
+    const int L = hwp::kLatentFrames;
+    const int LB = hwp::kViterbiStitchLookback;
+    const int nRoi = (int)F + LB + hwp::kRoiStitchFrames;   // roi workspace frames
+    const hwp::SparseRows sp = hwp::TransitionPattern();
+    const bool roiNoop = (cfg.roi_filter_type == HW_ROI_NOOP);
+    if (roiNoop) { g_err = "RoiFilterNoOp is not built"; return HW_ERR_UNSUPPORTED; }
+
+#pragma omp parallel
+    {
+        std::vector<uint16_t> tb((size_t)(F + LB) * kStates);   // traceback per frame per state
+        std::vector<uint8_t> roi(nRoi);
+        std::vector<float> tr((size_t)(F + L));
+#pragma omp for schedule(dynamic, 1)
+        for (int64_t l = 0; l < (int64_t)lanes; ++l)
+        {
+            const int16_t* chunk = traces + (size_t)l * F * kLane;
+            int16_t* pl = &prevLat[(size_t)l * L * kLane];
+            const hw_lane_model& oldM = latModel[l];
+            const hw_lane_model& newM = models[l];
+            for (int z = 0; z < kLane; ++z)
+            {
+                // ComputeRoi (FrameLabelerHost.cpp:267-309, RoiHost.h:110-249)
+                const float inv1 = 1 / std::sqrt(f16_bits_to_f32(oldM.baseline.vars[z]));
+                const float inv2 = 1 / std::sqrt(f16_bits_to_f32(newM.baseline.vars[z]));
+                float prev[3];
+                prev[0] = (float)latTrc[(size_t)l * kLane + z] * inv1;
+                prev[1] = (float)pl[0 * kLane + z] * inv1;
+                prev[2] = (float)pl[1 * kLane + z] * inv1;
+                uint16_t prevRoi = (uint16_t)latRoi[(size_t)l * kLane + z];
+                int ri = 0;
+                auto process = [&](float sn) {
+                    float mval = prev[1];
+                    mval = fmax_sse(mval, (prev[0] + prev[1]) / d.sqrt2);
+                    mval = fmax_sse(mval, (prev[0] + prev[1] + prev[2]) / d.sqrt3);
+                    mval = fmax_sse(mval, (prev[0] + prev[1] + prev[2] + sn) / 2.0f);
+                    const float thresh = (prevRoi & 1u) ? cfg.roi_lower_threshold : cfg.roi_upper_threshold;
+                    const uint16_t v1 = (mval >= thresh) ? 1u : 0u;
+                    const uint16_t v2 = (mval >= cfg.roi_lower_threshold) ? 2u : 0u;
+                    const uint16_t v = v1 | v2;
+                    roi[ri++] = (uint8_t)v;
+                    prevRoi = v;
+                    prev[0] = prev[1]; prev[1] = prev[2]; prev[2] = sn;
+                };
+                for (int i = hwp::kRoiLookForward; i < L; ++i) process((float)pl[(size_t)i * kLane + z] * inv1);
+                for (int i = 0; i < (int)F; ++i) process((float)chunk[(size_t)i * kLane + z] * inv2);
+                {
+                    uint16_t pr = 0;
+                    for (int i = nRoi - 1; i >= 0; --i)
+                    {
+                        const bool b = (roi[i] & 1u) | ((roi[i] & 2u) && pr != 0);
+                        pr = b ? 1u : 0u;
+                        roi[i] = b ? 1u : 0u;
+                    }
+                }
+
+                // LabelBlock (FrameLabelerHost.cpp:314-448)
+                float ll[kStates], la[kStates];
+                const int bc = latLabel[(size_t)l * kLane + z];
+                for (int i = 0; i < kStates; ++i) ll[i] = (bc == i) ? 0.0f : -kInf;
+                for (int f = 0; f < L; ++f) tr[f] = (float)pl[(size_t)f * kLane + z];
+                for (int f = 0; f < (int)F; ++f) tr[L + f] = (float)chunk[(size_t)f * kLane + z];
+
+                Scorer sc;
+                float anchorLL[kStates];
+                auto recursion = [&](int lf, float data) {
+                    float sco[kStates];
+                    sc.Scores(data, sco);
+                    const bool isRoi = roi[lf] != 0;
+                    for (int r = 0; r < kStates; ++r)
+                    {
+                        const float score = sco[r];
+                        int idx = sp.first[r];
+                        float mv = score + d.trans[r][idx] + ll[idx];
+                        for (int p = sp.segBegin[r]; p < sp.segEnd[r]; ++p)
+                        {
+                            const float v = score + d.trans[r][p] + ll[p];
+                            const bool cnd = v >= mv;
+                            mv = cnd ? v : mv;
+                            idx = cnd ? p : idx;
+                        }
+                        const float penalty = (r == 0 || isRoi) ? 0.0f : kInf;
+                        la[r] = mv - penalty;
+                        tb[(size_t)lf * kStates + r] = (uint16_t)idx;
+                    }
+                    for (int r = 0; r < kStates; ++r) ll[r] = la[r];
+                };
+                sc.Setup(d, oldM, z);
+                for (int f = 0; f < L; ++f) recursion(f, tr[f]);
+                sc.Setup(d, newM, z);
+                const int anchor = (int)F - L;
+                for (int f = 0; f < anchor; ++f) recursion(f + L, tr[L + f]);
+                for (int i = 0; i < kStates; ++i) anchorLL[i] = ll[i];
+                for (int f = anchor; f < anchor + LB; ++f) recursion(f + L, tr[L + f]);
+
+                // Normalize (FrameLabelerHost.cpp:186-205)
+                float prob[kStates];
+                {
+                    float mx = ll[0];
+                    for (int i = 1; i < kStates; ++i) mx = fmax_sse(ll[i], mx);
+                    float sum = 0.0f;
+                    for (int i = 0; i < kStates; ++i) { prob[i] = hw_expf(ll[i] - mx); sum += prob[i]; }
+                    const float inv = 1 / sum;
+                    for (int i = 0; i < kStates; ++i) prob[i] *= inv;
+                }
+                for (int i = (int)F + LB - 1; i > (int)F - 1; --i)
+                {
+                    float np[kStates];
+                    for (int s = 0; s < kStates; ++s) np[s] = 0.0f;
+                    for (int from = 0; from < kStates; ++from)
+                        np[tb[(size_t)i * kStates + from]] += prob[from];
+                    for (int s = 0; s < kStates; ++s) prob[s] = np[s];
+                }
+                float maxP = prob[0];
+                int anchorState = 0;
+                for (int i = 1; i < kStates; ++i)
+                {
+                    const bool cnd = maxP > prob[i];
+                    maxP = cnd ? maxP : prob[i];
+                    anchorState = cnd ? anchorState : i;
+                }
+                int ts = anchorState;
+                int16_t* out = labels + (size_t)l * F * kLane;
+                for (int f = (int)F - 1; f >= 0; --f)
+                {
+                    out[(size_t)f * kLane + z] = (int16_t)ts;
+                    ts = tb[(size_t)f * kStates + ts];
+                }
+                latRoi[(size_t)l * kLane + z] = roi[F - 1];
+                latLabel[(size_t)l * kLane + z] = (int16_t)anchorState;
+                latTrc[(size_t)l * kLane + z] = chunk[(size_t)(anchor - 1) * kLane + z];
+                if (score) score[(size_t)l * kLane + z] = anchorLL[anchorState];
+            }
+            // LatentTrace of the returned batch = traces the first 24 labels
+            // belong to; then the latent buffer advances to this chunk's tail.
+            if (latOut) std::memcpy(latOut + (size_t)l * L * kLane, pl, sizeof(int16_t) * L * kLane);
+            std::memcpy(pl, chunk + (size_t)(F - L) * kLane, sizeof(int16_t) * L * kLane);
+            latModel[l] = newM;
+        }
+    }
+    return HW_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Pulse accumulator: TA/HostPulseAccumulator.{h,cpp}, DT/Pulse.h,
+// DT/BatchVectors.h:105-119
+
+namespace {
+inline uint16_t ToFixed(float v) { return static_cast<uint16_t>(v / .1f + 0.5f); }
+}
+
+int OraclePool::Pulses(const int16_t* labels, const int16_t* latTrace, const int16_t* trace, int32_t firstFrame,
+                       const hw_lane_model* models, hw_pulse* pulses, uint32_t* lens, uint32_t* ovf,
+                       hw_stat_accum_state* blstats)
+{
+    const int L = hwp::kLatentFrames;
+    const uint32_t cap = cfg.max_calls_per_zmw;
+    const float maxSignal = 65535 * .1f;
+    const float minSignal = 0.0f;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t l = 0; l < (int64_t)lanes; ++l)
+    {
+        Segment& s = seg[l];
+        StatAcc bs;
+        bs.Reset();
+        uint32_t* ln = lens + (size_t)l * kLane;
+        uint32_t* ov = ovf + (size_t)l * kLane;
+        hw_pulse* pz = pulses + (size_t)l * kLane * cap;
+        FZ { ln[z] = 0; ov[z] = 0; }
+        float minMean[kLane];
+        FZ minMean[z] = f16_bits_to_f32(models[l].analogs[kAnalogs - 1].means[z]);
+        for (uint32_t rel = 0; rel < F; ++rel)
+        {
+            const uint32_t absF = rel + (uint32_t)firstFrame;
+            const int16_t* lab = labels + ((size_t)l * F + rel) * kLane;
+            const int16_t* sig = (rel < (uint32_t)L) ? latTrace + ((size_t)l * L + rel) * kLane
+                                                     : trace + ((size_t)l * F + (rel - L)) * kLane;
+            FZ
+            {
+                const int16_t label = lab[z];
+                const int16_t signal = sig[z];
+                const bool isUp = (label > kAnalogs) & (label <= 2 * kAnalogs);
+                const bool boundary = isUp | ((label == 0) & (s.label[z] != 0));
+                const bool pulseM = s.label[z] != 0;
+                if (boundary & pulseM)
+                {
+                    // LabelsSegment::ToPulse (HostPulseAccumulator.h:106-138)
+                    const int width = (int)(absF - s.start[z]);
+                    const float rawMean = float(s.total[z] + s.last[z] + s.first[z]) / width;
+                    const float rawMid = float(s.total[z]) / (width - 2);
+                    const bool keep = (width >= d.widthThresh) || (rawMean * width >= d.ampThresh * minMean[z]);
+                    hw_pulse p;
+                    std::memset(&p, 0, sizeof(p));
+                    p.start = s.start[z];
+                    p.width = (uint16_t)width;
+                    p.mean_signal = ToFixed(std::min(maxSignal, std::max(minSignal, rawMean)));
+                    p.mid_signal = ToFixed(width < 3 ? 0.0f : std::min(maxSignal, std::max(minSignal, rawMid)));
+                    p.max_signal = ToFixed(std::min(maxSignal, std::max(minSignal, static_cast<float>(s.mx[z]))));
+                    p.signal_m2 = s.m2[z];
+                    int lb = s.label[z];
+                    if (lb > 2 * kAnalogs) lb -= 2 * kAnalogs;
+                    if ((lb > kAnalogs) & (lb <= 2 * kAnalogs)) lb -= kAnalogs;
+                    p.label = d.analogMap[lb - 1];
+                    p.is_reject = keep ? 0 : 1;
+                    if (ln[z] < cap) pz[(size_t)z * cap + ln[z]++] = p;
+                    else ov[z]++;
+                }
+                // ResetSegment / AddSignal (HostPulseAccumulator.h:140-161)
+                if (boundary)
+                {
+                    s.start[z] = absF; s.end[z] = 0; s.first[z] = signal; s.last[z] = 0;
+                    s.mx[z] = signal; s.total[z] = 0.0f; s.m2[z] = 0.0f; s.label[z] = label;
+                }
+                else
+                {
+                    s.total[z] = s.total[z] + s.last[z];
+                    s.m2[z] = s.m2[z] + float(s.last[z]) * s.last[z];
+                    s.last[z] = signal;
+                    s.mx[z] = std::max(s.mx[z], signal);
+                }
+                const bool isBl = (!pulseM) & (!boundary);
+                bs.AddMasked(z, (float)signal, isBl);
+            }
+        }
+        bs.Store(blstats[l]);
+    }
+    return HW_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C API for ctypes (tests and bench.py only)
+
+extern "C" {
+
+const char* or_last_error(void) { return g_err.c_str(); }
+
+int or_config_default(hw_config* c) { hwp::DefaultConfig(c); return HW_OK; }
+
+int or_transition_matrix(const hw_config* c, float* out)
+{
+    float t[kStates][kStates];
+    hwp::TransitionMatrix(*c, t);
+    std::memcpy(out, t, sizeof(t));
+    return HW_OK;
+}
+
+void* or_pool_create(const hw_config* cfg, uint32_t poolId, uint32_t lanes, uint32_t F)
+{
+    auto p = std::make_unique<OraclePool>();
+    if (!p->Init(*cfg, poolId, lanes, F)) return nullptr;
+    return p.release();
+}
+
+void or_pool_destroy(void* p) { delete static_cast<OraclePool*>(p); }
+
+int or_set_threads(int n) { if (n > 0) omp_set_num_threads(n); return omp_get_max_threads(); }
+
+uint32_t or_baseliner_startup_latency(void* p) { return static_cast<OraclePool*>(p)->d.baselinerStartupLatency; }
+
+int or_baseline(void* p, const int16_t* trace, int32_t firstFrame, int16_t* out, hw_baseliner_stats* stats)
+{ return static_cast<OraclePool*>(p)->Baseline(trace, firstFrame, out, stats); }
+
+int or_agg_add(void* p, const hw_baseliner_stats* s, hw_frame_interval fi)
+{ static_cast<OraclePool*>(p)->AggAdd(s, fi); return HW_OK; }
+
+int or_agg_get(void* p, hw_baseliner_stats* out, hw_frame_interval* fi)
+{ static_cast<OraclePool*>(p)->AggGet(out, fi); return HW_OK; }
+
+int or_agg_reset(void* p) { static_cast<OraclePool*>(p)->AggReset(); return HW_OK; }
+
+int or_hist_reset_from_stats(void* p, const hw_baseliner_stats* s)
+{ return static_cast<OraclePool*>(p)->HistResetStats(s); }
+
+int or_hist_reset_from_bounds(void* p, const hw_lane_hist_bounds* b)
+{ return static_cast<OraclePool*>(p)->HistResetBounds(b); }
+
+int or_hist_add(void* p, const int16_t* tr, uint32_t frames, hw_frame_interval fi, const hw_lane_model* m)
+{ return static_cast<OraclePool*>(p)->HistAdd(tr, frames, fi, m); }
+
+int or_hist_get(void* p, hw_lane_histogram* out, hw_frame_interval* fi)
+{ static_cast<OraclePool*>(p)->HistGet(out, fi); return HW_OK; }
+
+int or_dme_init_models(void* p, const hw_baseliner_stats* s, hw_lane_model* out)
+{ static_cast<OraclePool*>(p)->InitModels(s, out); return HW_OK; }
+
+int or_dme_estimate(void* p, const hw_lane_histogram* h, const hw_baseliner_stats* s, hw_frame_interval hfi,
+                    hw_frame_interval mfi, hw_lane_model* m, hw_dme_diag* diag)
+{ return static_cast<OraclePool*>(p)->Estimate(h, s, hfi, mfi, m, diag); }
+
+int or_label(void* p, const int16_t* tr, const hw_lane_model* m, int16_t* labels, int16_t* latOut, float* score)
+{ return static_cast<OraclePool*>(p)->Label(tr, m, labels, latOut, score); }
+
+int or_pulses(void* p, const int16_t* labels, const int16_t* lat, const int16_t* tr, int32_t firstFrame,
+              const hw_lane_model* m, hw_pulse* pulses, uint32_t* lens, uint32_t* ovf, hw_stat_accum_state* bs)
+{ return static_cast<OraclePool*>(p)->Pulses(labels, lat, tr, firstFrame, m, pulses, lens, ovf, bs); }
+
+float or_expf(float x) { return hw_expf(x); }
+float or_logf(float x) { return hw_logf(x); }
+uint16_t or_f32_to_f16(float x) { return f32_to_f16_bits(x); }
+int16_t or_to_i16(float x) { return to_i16_wrap(x); }
+
+}   // extern "C"

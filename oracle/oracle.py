@@ -1,0 +1,181 @@
+"""ctypes binding of the CPU oracle (oracle/hw_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, never by the hw_b200 package.  The oracle is a
+literal CPU restatement of the reference's Host* trace-analysis path.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from hw_b200 import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_build", "libhw_oracle.so")
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        vp, i32, u32 = C.c_void_p, C.c_int32, C.c_uint32
+        FI = abi.FrameInterval
+        L.or_last_error.restype = C.c_char_p
+        L.or_config_default.argtypes = [C.POINTER(abi.Config)]
+        L.or_transition_matrix.argtypes = [C.POINTER(abi.Config), vp]
+        L.or_pool_create.argtypes = [C.POINTER(abi.Config), u32, u32, u32]
+        L.or_pool_create.restype = vp
+        L.or_pool_destroy.argtypes = [vp]
+        L.or_set_threads.argtypes = [C.c_int]
+        L.or_baseliner_startup_latency.argtypes = [vp]
+        L.or_baseliner_startup_latency.restype = u32
+        L.or_baseline.argtypes = [vp, vp, i32, vp, vp]
+        L.or_agg_add.argtypes = [vp, vp, FI]
+        L.or_agg_get.argtypes = [vp, vp, C.POINTER(FI)]
+        L.or_agg_reset.argtypes = [vp]
+        L.or_hist_reset_from_stats.argtypes = [vp, vp]
+        L.or_hist_reset_from_bounds.argtypes = [vp, vp]
+        L.or_hist_add.argtypes = [vp, vp, u32, FI, vp]
+        L.or_hist_get.argtypes = [vp, vp, C.POINTER(FI)]
+        L.or_dme_init_models.argtypes = [vp, vp, vp]
+        L.or_dme_estimate.argtypes = [vp, vp, vp, FI, FI, vp, vp]
+        L.or_label.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.or_pulses.argtypes = [vp, vp, vp, vp, i32, vp, vp, vp, vp, vp]
+        L.or_expf.argtypes = [C.c_float]
+        L.or_expf.restype = C.c_float
+        L.or_logf.argtypes = [C.c_float]
+        L.or_logf.restype = C.c_float
+        L.or_f32_to_f16.argtypes = [C.c_float]
+        L.or_f32_to_f16.restype = C.c_uint16
+        L.or_to_i16.argtypes = [C.c_float]
+        L.or_to_i16.restype = C.c_int16
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise RuntimeError(f"oracle: {abi.STATUS_NAMES.get(rc, rc)}: {lib().or_last_error().decode()}")
+
+
+def default_config():
+    c = abi.Config()
+    lib().or_config_default(C.byref(c))
+    return c
+
+
+def transition_matrix(cfg):
+    out = np.zeros((abi.NUM_STATES, abi.NUM_STATES), np.float32)
+    lib().or_transition_matrix(C.byref(cfg), abi.ptr(out))
+    return out
+
+
+def set_threads(n):
+    return lib().or_set_threads(int(n))
+
+
+class Pool:
+    """All Host* filters of one pool (baseliner, aggregator, histogram, DME,
+    labeler, pulse accumulator) with the reference's per-stage calls."""
+
+    def __init__(self, cfg, lanes, frames_per_chunk, pool_id=0):
+        self.cfg = cfg.copy()
+        self.lanes = lanes
+        self.F = frames_per_chunk
+        self.h = lib().or_pool_create(C.byref(self.cfg), pool_id, lanes, frames_per_chunk)
+        if not self.h:
+            raise RuntimeError("oracle pool create failed: " + lib().or_last_error().decode())
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_pool_destroy(self.h)
+            self.h = None
+
+    def startup_latency(self):
+        return lib().or_baseliner_startup_latency(self.h)
+
+    def baseline(self, trace, first_frame):
+        trace = np.ascontiguousarray(trace, dtype=np.int16)
+        out = np.empty_like(trace)
+        stats = np.zeros(self.lanes, abi.BLSTATS_DT)
+        _check(lib().or_baseline(self.h, abi.ptr(trace), first_frame, abi.ptr(out), abi.ptr(stats)))
+        return out, stats
+
+    def agg_add(self, stats, fi):
+        _check(lib().or_agg_add(self.h, abi.ptr(stats), abi.FrameInterval(*fi)))
+
+    def agg_get(self):
+        out = np.zeros(self.lanes, abi.BLSTATS_DT)
+        fi = abi.FrameInterval()
+        _check(lib().or_agg_get(self.h, abi.ptr(out), C.byref(fi)))
+        return out, fi.tuple()
+
+    def agg_reset(self):
+        _check(lib().or_agg_reset(self.h))
+
+    def hist_reset_from_stats(self, stats):
+        _check(lib().or_hist_reset_from_stats(self.h, abi.ptr(stats)))
+
+    def hist_reset_from_bounds(self, bounds):
+        _check(lib().or_hist_reset_from_bounds(self.h, abi.ptr(bounds)))
+
+    def hist_add(self, traces, fi, models):
+        traces = np.ascontiguousarray(traces, dtype=np.int16)
+        frames = traces.shape[1]
+        _check(lib().or_hist_add(self.h, abi.ptr(traces), frames, abi.FrameInterval(*fi), abi.ptr(models)))
+
+    def hist_get(self):
+        out = np.zeros(self.lanes, abi.LANE_HIST_DT)
+        fi = abi.FrameInterval()
+        _check(lib().or_hist_get(self.h, abi.ptr(out), C.byref(fi)))
+        return out, fi.tuple()
+
+    def init_models(self, stats):
+        out = np.zeros(self.lanes, abi.LANE_MODEL_DT)
+        _check(lib().or_dme_init_models(self.h, abi.ptr(stats), abi.ptr(out)))
+        return out
+
+    def estimate(self, hist, stats, hist_fi, model_fi, models):
+        models = models.copy()
+        diag = np.zeros(self.lanes, abi.DME_DIAG_DT)
+        _check(lib().or_dme_estimate(self.h, abi.ptr(hist), abi.ptr(stats), abi.FrameInterval(*hist_fi),
+                                     abi.FrameInterval(*model_fi), abi.ptr(models), abi.ptr(diag)))
+        return models, diag
+
+    def label(self, traces, models):
+        traces = np.ascontiguousarray(traces, dtype=np.int16)
+        labels = np.empty_like(traces)
+        lat = np.empty((self.lanes, abi.LATENT_FRAMES, abi.LANE), np.int16)
+        score = np.empty((self.lanes, abi.LANE), np.float32)
+        _check(lib().or_label(self.h, abi.ptr(traces), abi.ptr(models), abi.ptr(labels), abi.ptr(lat),
+                              abi.ptr(score)))
+        return labels, lat, score
+
+    def pulses(self, labels, latent, traces, first_frame, models):
+        cap = self.cfg.max_calls_per_zmw
+        pulses = np.zeros((self.lanes, abi.LANE, cap), abi.PULSE_DT)
+        lens = np.zeros((self.lanes, abi.LANE), np.uint32)
+        ovf = np.zeros((self.lanes, abi.LANE), np.uint32)
+        bls = np.zeros(self.lanes, abi.STAT_ACCUM_DT)
+        _check(lib().or_pulses(self.h, abi.ptr(np.ascontiguousarray(labels)), abi.ptr(np.ascontiguousarray(latent)),
+                               abi.ptr(np.ascontiguousarray(traces)), first_frame, abi.ptr(models),
+                               abi.ptr(pulses), abi.ptr(lens), abi.ptr(ovf), abi.ptr(bls)))
+        return pulses, lens, ovf, bls
+
+
+def expf(x):
+    return lib().or_expf(float(x))
+
+
+def logf(x):
+    return lib().or_logf(float(x))
