@@ -1,0 +1,376 @@
+#!/usr/bin/env python
+"""Throughput of the smrt-basecaller trace-analysis chain on B200.
+
+Workload (chip scale): 1,048,576 ZMWs = 16,384 lanes of 64, as 4 pools of 4096
+lanes, 512-frame int16 chunks from the device trace generator (lognormal gain
+sigma 0.2, 15% empty ZMWs, 0.05 DN/frame baseline random walk), reference
+default analysis parameters (MultiScaleLarge baseliner, dynamic estimation:
+every pool re-estimates its detection models every 4000 frames, staggered by
+pool).  The run first streams the start-up chunks (untimed) until every pool
+is in its periodic estimation cycle; a step is then one chunk of the whole
+chip through baseliner -> statistics -> histogram -> (EM when due) ->
+labeler -> pulses.  K is rounded to whole 8-chunk estimation cycles is not
+needed for correctness but the default K=8 covers exactly one.
+
+  value : ZMW-frames/s with the chunks already in HBM
+  e2e   : same through hw_analyzer_process with the chunk copied from pinned
+          host memory and the pulse output copied back inside the timed region
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl hw|reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FRAMES = 512
+LANES_PER_POOL = 4096
+POOLS = 4
+KERNELS_PER_STAGE = {"baseline": 1, "aggregate": 1, "histogram": 1, "model_init": 1, "dme": 1,
+                     "hist_reset": 2, "labeler": 2, "pulses": 1}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["hw", "reference"], default="hw")
+    ap.add_argument("--lanes-per-pool", type=int, default=LANES_PER_POOL)
+    ap.add_argument("--pools", type=int, default=POOLS)
+    ap.add_argument("--cpu-lanes", type=int, default=512, help="lanes in the CPU-baseline sample")
+    ap.add_argument("--cpu-steps", type=int, default=8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def startup_chunks(cfg, pools):
+    """Chunks until every pool has entered its periodic estimation cycle."""
+    from hw_b200 import abi, native
+    import ctypes as C
+    b = C.c_void_p()
+    native.check(native.lib().hw_baseliner_create(C.byref(cfg), 0, 1, FRAMES, C.byref(b)))
+    lat = C.c_uint32()
+    native.lib().hw_baseliner_startup_latency(b, C.byref(lat))
+    native.lib().hw_baseliner_destroy(b)
+    chunks_per_est = (max(cfg.min_frames_for_estimate, 1) + FRAMES - 1) // FRAMES
+    last_delay = ((pools - 1) % chunks_per_est) * FRAMES
+    start = (lat.value + last_delay + FRAMES - 1) // FRAMES          # first chunk the last pool analyses
+    pre = (cfg.num_frames_pre_accum_stats + FRAMES - 1) // FRAMES    # histogram start-up
+    return start + pre + chunks_per_est
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5], f[6], f[7], f[8]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for n, v in zip(names, r[2:]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "samples": len(rows), "reasons": sorted(reasons)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return None
+
+
+def labeler_dram_profile():
+    """DRAM bytes per ZMW-frame of the labeler kernel from the committed ncu summary."""
+    try:
+        d = json.load(open(os.path.join(ROOT, "profiles", "labeler_dram.json")))
+        return d
+    except Exception:
+        return None
+
+
+def labeler_alg_bytes_per_zmw(F):
+    # trace read 2F, labels written 2F, latent traces r+w 2x48, previous model
+    # r+w 2x32, boundary label/ROI/latent frame r+w 2x6, new model read 32,
+    # LatentTrace output 48, viterbi score 4.
+    return 4 * F + 96 + 64 + 12 + 32 + 48 + 4
+
+
+def cpu_baseline(cfg, lanes, steps, warmup, threads):
+    """The oracle (CPU restatement of the reference Host* path) on a sample of lanes."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from hw_b200 import filters as Fl
+    oracle.set_threads(threads)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from harness import OracleBackend, Pipeline
+    pipe = Pipeline(OracleBackend(cfg, lanes, FRAMES, 0), cfg, 0)
+    gen = Fl.TraceGenerator(lanes, workload=1, zmw_offset=0)
+    n0 = startup_chunks(cfg, 1) + warmup
+    total = n0 + steps
+    t_timed = 0.0
+    for c in range(total):
+        chunk = gen.next(c * FRAMES, FRAMES).cpu().numpy()
+        t0 = time.perf_counter()
+        pipe.process(chunk, c * FRAMES)
+        dt = time.perf_counter() - t0
+        if c >= n0:
+            t_timed += dt
+    zf = lanes * 64 * FRAMES * steps
+    return zf / t_timed, t_timed
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup()
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    from hw_b200 import filters as Fl, workloads
+    cfg = workloads.chip_config()
+    total_lanes = args.lanes_per_pool * args.pools
+    zmws = total_lanes * 64
+    threads = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        out = None
+        if rank == 0:
+            rate, secs = cpu_baseline(cfg, args.cpu_lanes, max(args.steps, 1), args.warmup, threads)
+            sample = (f"{args.cpu_lanes} lanes ({args.cpu_lanes * 64} ZMWs) x {args.steps} steady-state "
+                      f"512-frame chunks after start-up, {secs:.1f} s of CPU time")
+            out = {"metric": "ZMW-frames/s", "value": rate, "unit": "ZMW-frames/s", "impl": "reference",
+                   "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                   "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                   "dtype": "int16+f32", "data": "synthetic",
+                   "config": {"workload": "chip: 1,048,576 ZMWs x 512-frame chunks (sampled on CPU)",
+                              "lanes": total_lanes, "frames_per_chunk": FRAMES, "pools": args.pools},
+                   "cpu_baseline": {"value": rate, "unit": "ZMW-frames/s", "cores": threads, "kind": "port",
+                                    "sample": sample},
+                   "e2e": {"value": rate, "unit": "ZMW-frames/s", "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}}
+            print(json.dumps(out), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    analyzers = [Fl.BatchAnalyzer(cfg, p, args.lanes_per_pool, FRAMES) for p in range(args.pools)]
+    gen = Fl.TraceGenerator(total_lanes, workload=1, zmw_offset=rank * zmws)
+    lpp = args.lanes_per_pool
+    stream = torch.cuda.current_stream()
+
+    def run_chunk(chunk, c):
+        for p, a in enumerate(analyzers):
+            a(chunk[p * lpp:(p + 1) * lpp], c * FRAMES)
+
+    # Start-up and warm-up (untimed).
+    n_start = startup_chunks(cfg, args.pools)
+    buf = torch.empty((total_lanes, FRAMES, 64), dtype=torch.int16, device="cuda")
+    c = 0
+    for _ in range(n_start + args.warmup):
+        gen.next(c * FRAMES, FRAMES, out=buf)
+        run_chunk(buf, c)
+        c += 1
+    torch.cuda.synchronize()
+
+    # Device-resident timed region.
+    K = args.steps
+    dev_chunks = []
+    for k in range(K):
+        t = torch.empty((total_lanes, FRAMES, 64), dtype=torch.int16, device="cuda")
+        gen.next((c + k) * FRAMES, FRAMES, out=t)
+        dev_chunks.append(t)
+    for a in analyzers:
+        a.profile(True)
+        a.stage_times()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(K):
+        run_chunk(dev_chunks[k], c + k)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    c += K
+    del dev_chunks
+    stage = {}
+    for a in analyzers:
+        for kname, (t_ms, n) in a.stage_times().items():
+            s = stage.setdefault(kname, [0.0, 0])
+            s[0] += t_ms
+            s[1] += n
+        a.profile(False)
+    launches = sum(n * KERNELS_PER_STAGE[k] for k, (_, n) in stage.items())
+
+    zf_step = zmws * FRAMES
+    value = zf_step * K * world / (ms / 1e3)
+
+    # End-to-end through the C ABI: pinned host chunk -> device, analyse, pulses -> host.
+    e2e = None
+    if not args.no_e2e:
+        host_chunks = []
+        tmp = torch.empty((total_lanes, FRAMES, 64), dtype=torch.int16, device="cuda")
+        for k in range(K):
+            gen.next((c + k) * FRAMES, FRAMES, out=tmp)
+            h = torch.empty((total_lanes, FRAMES, 64), dtype=torch.int16, pin_memory=True)
+            h.copy_(tmp)
+            host_chunks.append(h)
+        cap = cfg.max_calls_per_zmw
+        host_out = [(torch.empty(a.pulses.numel(), dtype=torch.uint8, pin_memory=True),
+                     torch.empty(a.lens.shape, dtype=torch.int32, pin_memory=True),
+                     torch.empty(a.ovf.shape, dtype=torch.int32, pin_memory=True)) for a in analyzers]
+        torch.cuda.synchronize()
+        barrier()
+        e0.record(stream)
+        for k in range(K):
+            tmp.copy_(host_chunks[k], non_blocking=True)
+            run_chunk(tmp, c + k)
+            for a, (hp, hl, ho) in zip(analyzers, host_out):
+                hl.copy_(a.lens, non_blocking=True)
+                ho.copy_(a.ovf, non_blocking=True)
+                hp.copy_(a.pulses, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+        c += K
+        h2d = total_lanes * FRAMES * 64 * 2
+        d2h = sum(a.pulses.numel() + a.lens.numel() * 4 + a.ovf.numel() * 4 for a in analyzers)
+        e2e = {"value": zf_step * K * world / (ms_e2e / 1e3), "unit": "ZMW-frames/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / K}
+        del host_chunks
+
+    # Roofline of the dominant kernel (the frame labeler) from the live stage timers.
+    peaks = measured_peaks()
+    lab_ms, lab_n = stage.get("labeler", (0.0, 0))
+    lab_bytes_launch = labeler_alg_bytes_per_zmw(FRAMES) * lpp * 64
+    roof = None
+    if lab_n:
+        avg_s = lab_ms / lab_n / 1e3
+        achieved = lab_bytes_launch / avg_s / 1e9
+        peak = peaks["hbm_gbs"] if peaks else 6650.0
+        prof = labeler_dram_profile()
+        traffic = None
+        if prof:
+            traffic = prof["dram_bytes_per_zmw_frame"] * lpp * 64 * FRAMES
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic,
+                "kernel": "LabelerKernel", "launch_ms": lab_ms / lab_n,
+                "alg_bytes_per_launch": lab_bytes_launch,
+                "peak_source": "measured" if peaks else "fallback"}
+        if prof and "issue_frac" in prof:
+            roof["issue_roofline"] = {"frac": prof["issue_frac"], "source": "ncu sm__inst_executed"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, secs = cpu_baseline(cfg, args.cpu_lanes, args.cpu_steps, args.warmup, threads)
+        cpu = {"value": rate, "unit": "ZMW-frames/s", "cores": threads, "kind": "port",
+               "sample": f"{args.cpu_lanes} lanes ({args.cpu_lanes * 64} ZMWs) x {args.cpu_steps} "
+                         f"steady-state 512-frame chunks after start-up ({secs:.1f} s)"}
+
+    if rank == 0:
+        out = {
+            "metric": "ZMW-frames/s", "value": value, "unit": "ZMW-frames/s", "n_gpus": world,
+            "steps": K, "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int16+f32", "data": "synthetic",
+            "config": {"workload": "chip: 1,048,576 ZMWs (16,384 lanes, 4 pools) x 512-frame chunks, "
+                                   "reference default parameters, dynamic DME",
+                       "zmws_per_gpu": zmws, "frames_per_chunk": FRAMES, "pools": args.pools,
+                       "startup_chunks": n_start, "inputs": "1 GiB chunk per step, larger than L2"},
+            "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
+            "clocks": clk,
+            "stage_ms": {k: v[0] / K for k, v in stage.items()},
+        }
+        print(json.dumps(out), flush=True)
+    for a in analyzers:
+        a.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -93,6 +93,30 @@ class Config(C.Structure):
         return c
 
 
+class GenParams(C.Structure):
+    _fields_ = [
+        ("seed", C.c_uint64),
+        ("baseline_mean", C.c_float),
+        ("baseline_sigma", C.c_float),
+        ("amplitudes", C.c_float * NUM_ANALOGS),
+        ("amp_cv", C.c_float),
+        ("pulse_width_mean", C.c_float),
+        ("ipd_mean", C.c_float),
+        ("shot_coeff", C.c_float),
+        ("gain_sigma", C.c_float),
+        ("empty_fraction", C.c_float),
+        ("walk_sigma", C.c_float),
+        ("amp_scale_sigma", C.c_float),
+        ("rate_min", C.c_float),
+        ("rate_max", C.c_float),
+        ("decay_fraction", C.c_float),
+        ("decay_frames", C.c_int32),
+        ("step_frame", C.c_int32),
+        ("step_dn", C.c_float),
+        ("step_fraction", C.c_float),
+    ]
+
+
 class FrameInterval(C.Structure):
     _fields_ = [("lower", C.c_int32), ("upper", C.c_int32)]
 

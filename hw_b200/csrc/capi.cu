@@ -553,3 +553,283 @@ int hw_pulse_accumulator_process(hw_pulse_accumulator* p, const int16_t* d_label
 }
 
 }   // extern "C"
+
+// ---- Batch analyzer ------------------------------------------------------------
+// BatchAnalyzer (analyzer/BatchAnalyzer.cpp:149-375) with the
+// DetectionModelEstimator state machine (DetectionModelEstimator.cpp:93-160).
+// All stages of a chunk are enqueued on one stream; the aggregated statistics
+// and the histogram are read in place by the model kernels.
+
+struct hw_analyzer
+{
+    enum Status { HIST_INIT = 0, DME_INIT = 1, SEQUENCING = 2 };
+    hw_config cfg;
+    hwp::Derived d;
+    KParams k;
+    uint32_t poolId = 0, lanes = 0, F = 0;
+    hw_baseliner* bl = nullptr;
+    hw_blstats_aggregator* agg = nullptr;
+    hw_histogram* hist = nullptr;
+    hw_dme* dme = nullptr;
+    hw_labeler* lab = nullptr;
+    hw_pulse_accumulator* pa = nullptr;
+    int16_t* bls = nullptr;
+    hw_baseliner_stats* stats = nullptr;
+    hw_lane_model* models = nullptr;
+    int16_t* labels = nullptr;
+    int16_t* latent = nullptr;
+    float* score = nullptr;
+    hw_stat_accum_state* paStats = nullptr;
+    hw_dme_diag* diag = nullptr;
+    bool diagValid = false;
+    hw_frame_interval modelFi{0, 0};
+    int status = HIST_INIT;
+    int32_t framesRemaining = 0;
+    bool initialized = false;
+    bool fullEstimation = false;
+    uint32_t blLatency = 0;
+    int32_t poolDelay = 0;
+    int32_t nextFrame = 0;
+    // Stage timers (AnalysisProfiler counterpart, TA/AnalysisProfiler.h):
+    // event pairs recorded around each stage while profiling is enabled.
+    bool profiling = false;
+    std::vector<cudaEvent_t> evPool;
+    size_t evUsed = 0;
+    std::vector<std::pair<int, size_t>> evMarks;   // (stage, index of start event)
+
+    cudaEvent_t NextEvent()
+    {
+        if (evUsed == evPool.size())
+        {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+            evPool.push_back(e);
+        }
+        return evPool[evUsed++];
+    }
+    size_t Begin(int stage, cudaStream_t s)
+    {
+        if (!profiling) return 0;
+        const size_t i = evUsed;
+        cudaEvent_t e0 = NextEvent(), e1 = NextEvent();
+        if (!e0 || !e1) return 0;
+        cudaEventRecord(e0, s);
+        evMarks.emplace_back(stage, i);
+        return i + 1;
+    }
+    void End(size_t tok, cudaStream_t s)
+    {
+        if (tok) cudaEventRecord(evPool[tok], s);
+    }
+
+    ~hw_analyzer()
+    {
+        for (auto e : evPool) cudaEventDestroy(e);
+        hw_baseliner_destroy(bl);
+        hw_blstats_aggregator_destroy(agg);
+        hw_histogram_destroy(hist);
+        hw_dme_destroy(dme);
+        hw_labeler_destroy(lab);
+        hw_pulse_accumulator_destroy(pa);
+        cudaFree(bls); cudaFree(stats); cudaFree(models); cudaFree(labels); cudaFree(latent);
+        cudaFree(score); cudaFree(paStats); cudaFree(diag);
+    }
+
+    // DetectionModelEstimator::AddBatch
+    int DmeAdd(hw_frame_interval fi, cudaStream_t s, bool* ran)
+    {
+        int rc;
+        *ran = false;
+        size_t t = Begin(HW_STAGE_AGGREGATE, s);
+        if ((rc = hw_blstats_aggregator_add(agg, stats, fi, s))) return rc;
+        End(t, s);
+        if (status != HIST_INIT)
+        {
+            t = Begin(HW_STAGE_HISTOGRAM, s);
+            if ((rc = hw_histogram_add_batch(hist, bls, F, fi, models, s))) return rc;
+            End(t, s);
+        }
+        if (status != SEQUENCING)
+        {
+            t = Begin(HW_STAGE_MODEL_INIT, s);
+            if ((rc = hw_dme_init_models(dme, agg->acc, models, s))) return rc;
+            End(t, s);
+            modelFi = agg->fi;
+        }
+        framesRemaining -= (int32_t)F;
+        if (framesRemaining <= 0)
+        {
+            if (status == DME_INIT) status = SEQUENCING;
+            if (status == SEQUENCING)
+            {
+                *ran = true;
+                t = Begin(HW_STAGE_DME, s);
+                if ((rc = hw_dme_estimate(dme, hist->hist, agg->acc, hist->fi, modelFi, models, diag, s))) return rc;
+                End(t, s);
+                diagValid = true;
+                modelFi = hist->fi;
+            }
+            t = Begin(HW_STAGE_HIST_RESET, s);
+            if ((rc = hw_histogram_reset_from_stats(hist, agg->acc, s))) return rc;
+            if ((rc = hw_blstats_aggregator_reset(agg, s))) return rc;
+            End(t, s);
+            if (status == HIST_INIT) status = DME_INIT;
+            framesRemaining = (int32_t)cfg.min_frames_for_estimate;
+        }
+        return HW_OK;
+    }
+
+    int LabelAndPulse(int32_t ff, hw_pulse* pulses, uint32_t* lens, uint32_t* ovf, cudaStream_t s)
+    {
+        int rc;
+        size_t t = Begin(HW_STAGE_LABELER, s);
+        if ((rc = hw_labeler_process(lab, bls, models, labels, latent, score, s))) return rc;
+        End(t, s);
+        t = Begin(HW_STAGE_PULSES, s);
+        rc = hw_pulse_accumulator_process(pa, labels, latent, bls, ff, models, pulses, lens, ovf, paStats, s);
+        End(t, s);
+        return rc;
+    }
+};
+
+extern "C" {
+
+int hw_analyzer_create(const hw_config* cfg, uint32_t pool_id, uint32_t lanes, uint32_t frames_per_chunk,
+                       hw_analyzer** out)
+{
+    if (!out) return Fail(HW_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    auto a = std::make_unique<hw_analyzer>();
+    int rc = PrepareConfig(cfg, &a->d, &a->k);
+    if (rc) return rc;
+    if (cfg->model_estimation_mode == HW_FIXED_ESTIMATIONS)
+        return Fail(HW_ERR_UNSUPPORTED, "FixedModelBatchAnalyzer is not built");
+    a->cfg = *cfg;
+    a->poolId = pool_id;
+    a->lanes = lanes;
+    a->F = frames_per_chunk;
+    if ((rc = hw_baseliner_create(cfg, pool_id, lanes, frames_per_chunk, &a->bl))) return rc;
+    if ((rc = hw_blstats_aggregator_create(pool_id, lanes, &a->agg))) return rc;
+    if ((rc = hw_histogram_create(cfg, pool_id, lanes, &a->hist))) return rc;
+    if ((rc = hw_dme_create(cfg, pool_id, lanes, &a->dme))) return rc;
+    if ((rc = hw_labeler_create(cfg, pool_id, lanes, frames_per_chunk, &a->lab))) return rc;
+    if ((rc = hw_pulse_accumulator_create(cfg, pool_id, lanes, frames_per_chunk, &a->pa))) return rc;
+    const size_t nZmw = (size_t)lanes * kLane;
+    if ((rc = DevAlloc(&a->bls, nZmw * frames_per_chunk, "hw_analyzer_create"))) return rc;
+    if ((rc = DevAlloc(&a->stats, lanes, "hw_analyzer_create"))) return rc;
+    if ((rc = DevAlloc(&a->models, lanes, "hw_analyzer_create"))) return rc;
+    if ((rc = DevAlloc(&a->labels, nZmw * frames_per_chunk, "hw_analyzer_create"))) return rc;
+    if ((rc = DevAlloc(&a->latent, nZmw * kLatent, "hw_analyzer_create"))) return rc;
+    if ((rc = DevAlloc(&a->score, nZmw, "hw_analyzer_create"))) return rc;
+    if ((rc = DevAlloc(&a->paStats, lanes, "hw_analyzer_create"))) return rc;
+    if ((rc = DevAlloc(&a->diag, lanes, "hw_analyzer_create"))) return rc;
+    HW_CUDA(cudaMemset(a->models, 0, sizeof(hw_lane_model) * lanes), "hw_analyzer_create");
+    a->framesRemaining = (int32_t)cfg->num_frames_pre_accum_stats;
+    a->blLatency = a->d.baselinerStartupLatency;
+    const uint32_t chunksPerEstimate = (std::max(cfg->min_frames_for_estimate, 1u) + frames_per_chunk - 1) / frames_per_chunk;
+    a->poolDelay = (int32_t)((pool_id % chunksPerEstimate) * frames_per_chunk);
+    *out = a.release();
+    return HW_OK;
+}
+
+int hw_analyzer_destroy(hw_analyzer* a)
+{
+    delete a;
+    return HW_OK;
+}
+
+int hw_analyzer_process(hw_analyzer* a, const int16_t* d_trace, int32_t first_frame, hw_pulse* d_pulses,
+                        uint32_t* d_lens, uint32_t* d_overflows, int32_t* emitted, int32_t* estimated, void* stream)
+{
+    if (!a || !d_trace || !d_pulses || !d_lens || !d_overflows) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    if (first_frame != a->nextFrame) return Fail(HW_ERR_FRAME_ORDER, "Bad frame ID.");
+    cudaStream_t s = S(stream);
+    int rc;
+    bool ran = false, emit = false;
+    const size_t nZmw = (size_t)a->lanes * kLane;
+    {
+        const size_t t = a->Begin(HW_STAGE_BASELINE, s);
+        if ((rc = hw_baseliner_process(a->bl, d_trace, first_frame, a->bls, a->stats, s))) return rc;
+        a->End(t, s);
+    }
+    const hw_frame_interval fi{first_frame, first_frame + (int32_t)a->F};
+    if (a->cfg.model_estimation_mode == HW_INITIAL_ESTIMATIONS)
+    {
+        // SingleEstimateBatchAnalyzer::AnalyzeImpl (BatchAnalyzer.cpp:177-256)
+        if (!a->initialized && first_frame > (int32_t)a->blLatency)
+        {
+            if ((rc = a->DmeAdd(fi, s, &ran))) return rc;
+            a->initialized = ran;
+        }
+        if (a->initialized)
+        {
+            if ((rc = a->LabelAndPulse(first_frame, d_pulses, d_lens, d_overflows, s))) return rc;
+            emit = true;
+        }
+    }
+    else
+    {
+        // DynamicEstimateBatchAnalyzer::AnalyzeImpl (BatchAnalyzer.cpp:289-375)
+        if (first_frame >= (int32_t)a->blLatency + a->poolDelay)
+        {
+            if ((rc = a->DmeAdd(fi, s, &ran))) return rc;
+            if (ran) a->fullEstimation = true;
+            if ((rc = a->LabelAndPulse(first_frame, d_pulses, d_lens, d_overflows, s))) return rc;
+            emit = a->fullEstimation;
+        }
+    }
+    if (!emit)
+    {
+        HW_CUDA(cudaMemsetAsync(d_lens, 0, nZmw * sizeof(uint32_t), s), "hw_analyzer_process");
+        HW_CUDA(cudaMemsetAsync(d_overflows, 0, nZmw * sizeof(uint32_t), s), "hw_analyzer_process");
+    }
+    a->nextFrame = first_frame + (int32_t)a->F;
+    if (emitted) *emitted = emit ? 1 : 0;
+    if (estimated) *estimated = ran ? 1 : 0;
+    return HW_OK;
+}
+
+int hw_analyzer_models(const hw_analyzer* a, hw_lane_model* d_out, hw_frame_interval* fi, void* stream)
+{
+    if (!a || !d_out) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    HW_CUDA(cudaMemcpyAsync(d_out, a->models, sizeof(hw_lane_model) * a->lanes, cudaMemcpyDeviceToDevice, S(stream)),
+            "hw_analyzer_models");
+    if (fi) *fi = a->modelFi;
+    return HW_OK;
+}
+
+int hw_analyzer_last_diag(const hw_analyzer* a, hw_dme_diag* d_out, int32_t* valid, void* stream)
+{
+    if (!a || !d_out) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    if (valid) *valid = a->diagValid ? 1 : 0;
+    if (!a->diagValid) return HW_OK;
+    HW_CUDA(cudaMemcpyAsync(d_out, a->diag, sizeof(hw_dme_diag) * a->lanes, cudaMemcpyDeviceToDevice, S(stream)),
+            "hw_analyzer_last_diag");
+    return HW_OK;
+}
+
+int hw_analyzer_profile(hw_analyzer* a, int32_t enable)
+{
+    if (!a) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    a->profiling = enable != 0;
+    return HW_OK;
+}
+
+int hw_analyzer_stage_times(hw_analyzer* a, double ms[HW_NUM_STAGES], uint32_t launches[HW_NUM_STAGES])
+{
+    if (!a || !ms || !launches) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    for (int i = 0; i < HW_NUM_STAGES; ++i) { ms[i] = 0.0; launches[i] = 0; }
+    for (const auto& m : a->evMarks)
+    {
+        HW_CUDA(cudaEventSynchronize(a->evPool[m.second + 1]), "hw_analyzer_stage_times");
+        float t = 0.0f;
+        HW_CUDA(cudaEventElapsedTime(&t, a->evPool[m.second], a->evPool[m.second + 1]), "hw_analyzer_stage_times");
+        ms[m.first] += t;
+        launches[m.first] += 1;
+    }
+    a->evMarks.clear();
+    a->evUsed = 0;
+    return HW_OK;
+}
+
+}   // extern "C"

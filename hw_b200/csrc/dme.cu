@@ -496,6 +496,7 @@ __global__ void __launch_bounds__(kLane) DmeEstimateKernel(DmeArgs A, KParams k)
         D.status[z] = zStatus;
         D.confidence[z] = conf;
         if (z == 0) D.lane_iterations = laneIters;
+        if (z < 15) D.pad_[z] = 0;
     }
 }
 

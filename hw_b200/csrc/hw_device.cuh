@@ -180,5 +180,7 @@ cudaError_t LaunchInitModels(hw_lane_model* m, const hw_baseliner_stats* s, int 
 cudaError_t LaunchDmeEstimate(const DmeArgs& a, const KParams& k, cudaStream_t s);
 cudaError_t LaunchLabeler(const LabelerArgs& a, const KParams& k, cudaStream_t s);
 cudaError_t LaunchPulses(const PulseArgs& a, const KParams& k, cudaStream_t s);
+struct GenArgs;
+cudaError_t LaunchGen(const GenArgs& a, cudaStream_t s);
 
 }   // namespace hwk

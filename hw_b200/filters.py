@@ -189,6 +189,79 @@ class PulseAccumulator(_Handle):
         return pulses, lens, ovf, bls
 
 
+class BatchAnalyzer(_Handle):
+    """One pool's full chain (BatchAnalyzer + DetectionModelEstimator)."""
+    _destroy = "hw_analyzer_destroy"
+
+    def __init__(self, cfg, pool_id, lanes, frames_per_chunk):
+        super().__init__()
+        self.lanes, self.F = lanes, frames_per_chunk
+        self.cap = cfg.max_calls_per_zmw
+        check(lib().hw_analyzer_create(C.byref(cfg), pool_id, lanes, frames_per_chunk, C.byref(self._h)))
+        dev = "cuda"
+        self.pulses = torch.empty(lanes * abi.LANE * self.cap * abi.PULSE_DT.itemsize, dtype=torch.uint8, device=dev)
+        self.lens = torch.empty((lanes, abi.LANE), dtype=torch.int32, device=dev)
+        self.ovf = torch.empty((lanes, abi.LANE), dtype=torch.int32, device=dev)
+
+    def __call__(self, trace, first_frame, pulses=None, lens=None, ovf=None):
+        """Returns (pulses, lens, overflows, emitted, estimated); buffers are reused between calls."""
+        pulses = self.pulses if pulses is None else pulses
+        lens = self.lens if lens is None else lens
+        ovf = self.ovf if ovf is None else ovf
+        em, est = C.c_int32(), C.c_int32()
+        check(lib().hw_analyzer_process(self._h, _p(trace), int(first_frame), _p(pulses), _p(lens), _p(ovf),
+                                        C.byref(em), C.byref(est), _stream()))
+        return pulses, lens, ovf, bool(em.value), bool(est.value)
+
+    STAGES = ("baseline", "aggregate", "histogram", "model_init", "dme", "hist_reset", "labeler", "pulses")
+
+    def profile(self, enable=True):
+        check(lib().hw_analyzer_profile(self._h, 1 if enable else 0))
+
+    def stage_times(self):
+        """{stage: (device ms, launches)} since the previous call (synchronises)."""
+        import numpy as _np
+        ms = _np.zeros(len(self.STAGES), _np.float64)
+        n = _np.zeros(len(self.STAGES), _np.uint32)
+        check(lib().hw_analyzer_stage_times(self._h, abi.ptr(ms), abi.ptr(n)))
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(self.STAGES)}
+
+    def models(self):
+        out = struct_buffer(abi.LANE_MODEL_DT, self.lanes)
+        fi = abi.FrameInterval()
+        check(lib().hw_analyzer_models(self._h, _p(out), C.byref(fi), _stream()))
+        return out, fi.tuple()
+
+    def last_diag(self):
+        out = struct_buffer(abi.DME_DIAG_DT, self.lanes)
+        valid = C.c_int32()
+        check(lib().hw_analyzer_last_diag(self._h, _p(out), C.byref(valid), _stream()))
+        return out if valid.value else None
+
+
+class TraceGenerator(_Handle):
+    """Device synthetic-trace source (workload 0, 1, 2 or 4 defaults)."""
+    _destroy = "hw_trace_generator_destroy"
+
+    def __init__(self, lanes, workload=1, zmw_offset=0, params=None, seed=None):
+        super().__init__()
+        self.lanes = lanes
+        p = abi.GenParams()
+        if params is None:
+            check(lib().hw_gen_params_default(int(workload), C.byref(p)))
+        else:
+            p = params
+        if seed is not None:
+            p.seed = seed
+        self.params = p
+        check(lib().hw_trace_generator_create(C.byref(p), lanes, zmw_offset, C.byref(self._h)))
+
+    def next(self, first_frame, frames, out=None):
+        out = torch.empty((self.lanes, frames, abi.LANE), dtype=torch.int16, device="cuda") if out is None else out
+        check(lib().hw_trace_generator_next(self._h, _p(out), int(first_frame), frames, _stream()))
+        return out
+
+
 def default_config():
     cfg = abi.Config()
     check(lib().hw_config_default(C.byref(cfg)))

@@ -63,6 +63,17 @@ def lib():
         "hw_pulse_accumulator_create": ([PCFG, u32, u32, u32, PPV], C.c_int),
         "hw_pulse_accumulator_destroy": ([vp], C.c_int),
         "hw_pulse_accumulator_process": ([vp, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp], C.c_int),
+        "hw_analyzer_create": ([PCFG, u32, u32, u32, PPV], C.c_int),
+        "hw_analyzer_destroy": ([vp], C.c_int),
+        "hw_analyzer_process": ([vp, vp, i32, vp, vp, vp, C.POINTER(i32), C.POINTER(i32), vp], C.c_int),
+        "hw_analyzer_models": ([vp, vp, C.POINTER(FI), vp], C.c_int),
+        "hw_analyzer_last_diag": ([vp, vp, C.POINTER(i32), vp], C.c_int),
+        "hw_analyzer_profile": ([vp, i32], C.c_int),
+        "hw_analyzer_stage_times": ([vp, vp, vp], C.c_int),
+        "hw_gen_params_default": ([C.c_int, C.POINTER(abi.GenParams)], C.c_int),
+        "hw_trace_generator_create": ([C.POINTER(abi.GenParams), u32, C.c_uint64, PPV], C.c_int),
+        "hw_trace_generator_destroy": ([vp], C.c_int),
+        "hw_trace_generator_next": ([vp, vp, i32, u32, vp], C.c_int),
     }
     for name, (args, res) in sigs.items():
         f = getattr(L, name)

@@ -349,6 +349,85 @@ int hw_pulse_accumulator_process(hw_pulse_accumulator* p, const int16_t* d_label
                                  hw_pulse* d_pulses, uint32_t* d_lens, uint32_t* d_overflows,
                                  hw_stat_accum_state* d_blstats, void* stream);
 
+/* ---- Batch analyzer (analyzer/BatchAnalyzer.cpp:149-375) ----------------
+ * One pool's complete chain: baseliner, the DetectionModelEstimator state
+ * machine (DetectionModelEstimator.cpp:93-160: stats aggregation, histogram,
+ * model initialisation and EM estimation), frame labeler and pulse
+ * accumulator, with the SingleEstimate (HW_INITIAL_ESTIMATIONS) or
+ * DynamicEstimate (HW_DYNAMIC_ESTIMATIONS) schedule of the reference.
+ * max_pool_id is unused by the reference schedule and kept for symmetry. */
+typedef struct hw_analyzer hw_analyzer;
+int hw_analyzer_create(const hw_config* cfg, uint32_t pool_id, uint32_t lanes, uint32_t frames_per_chunk,
+                       hw_analyzer** out);
+int hw_analyzer_destroy(hw_analyzer* a);
+/* BatchAnalyzer::operator(): d_trace[lanes][F][64] must be the next chunk
+ * (first_frame == previous first_frame + F, starting at 0); otherwise
+ * HW_ERR_FRAME_ORDER.  Pulses go to d_pulses[lanes][64][max_calls_per_zmw]
+ * with counts in d_lens / d_overflows; *emitted is set to 0 while the
+ * reference would return an empty pulse batch (start-up), 1 otherwise.
+ * *estimated is set to 1 when this chunk ran a full DME estimate. */
+int hw_analyzer_process(hw_analyzer* a, const int16_t* d_trace, int32_t first_frame, hw_pulse* d_pulses,
+                        uint32_t* d_lens, uint32_t* d_overflows, int32_t* emitted, int32_t* estimated,
+                        void* stream);
+/* Current detection models of the pool and their frame interval. */
+int hw_analyzer_models(const hw_analyzer* a, hw_lane_model* d_out, hw_frame_interval* fi, void* stream);
+/* Diagnostics of the most recent DME estimate (*valid = 0 if none yet). */
+int hw_analyzer_last_diag(const hw_analyzer* a, hw_dme_diag* d_out, int32_t* valid, void* stream);
+
+/* Stage timers (the AnalysisProfiler stages of TA/AnalysisProfiler.h:31-60):
+ * while enabled, CUDA events bracket every stage the analyzer enqueues;
+ * hw_analyzer_stage_times synchronises, returns the summed device time and
+ * launch count per stage since the previous call, and clears them. */
+enum {
+    HW_STAGE_BASELINE = 0,
+    HW_STAGE_AGGREGATE = 1,
+    HW_STAGE_HISTOGRAM = 2,
+    HW_STAGE_MODEL_INIT = 3,
+    HW_STAGE_DME = 4,
+    HW_STAGE_HIST_RESET = 5,
+    HW_STAGE_LABELER = 6,
+    HW_STAGE_PULSES = 7,
+    HW_NUM_STAGES = 8
+};
+int hw_analyzer_profile(hw_analyzer* a, int32_t enable);
+int hw_analyzer_stage_times(hw_analyzer* a, double ms[HW_NUM_STAGES], uint32_t launches[HW_NUM_STAGES]);
+
+/* ---- Synthetic traces ------------------------------------------------------
+ * Device generator used by the benchmarks and tests in place of camera data
+ * (a counter-based RNG: every chunk is reproducible from seed, ZMW index and
+ * frame index). */
+typedef struct hw_gen_params {
+    uint64_t seed;
+    float    baseline_mean;      /* DN */
+    float    baseline_sigma;     /* DN */
+    float    amplitudes[HW_NUM_ANALOGS];   /* DN, brightest first */
+    float    amp_cv;             /* per-pulse amplitude CV */
+    float    pulse_width_mean;   /* frames (geometric) */
+    float    ipd_mean;           /* frames (geometric gap) */
+    float    shot_coeff;         /* added variance per DN of pulse signal */
+    float    gain_sigma;         /* per-ZMW lognormal gain on amplitudes */
+    float    empty_fraction;     /* fraction of ZMWs without pulses */
+    float    walk_sigma;         /* baseline random-walk step, DN per frame */
+    float    amp_scale_sigma;    /* extra per-ZMW lognormal amplitude factor */
+    float    rate_min, rate_max; /* per-ZMW pulse rate (pulses/frame) if rate_max > 0 */
+    float    decay_fraction;     /* amplitude decay reached at decay_frames */
+    int32_t  decay_frames;
+    int32_t  step_frame;         /* baseline step start frame (< 0: none) */
+    float    step_dn;
+    float    step_fraction;      /* fraction of ZMWs with the step */
+} hw_gen_params;
+
+/* Defaults of workload 0 (small), 1 (chip), 2 (uneven pools) and 4 (streaming). */
+int hw_gen_params_default(int workload, hw_gen_params* p);
+typedef struct hw_trace_generator hw_trace_generator;
+int hw_trace_generator_create(const hw_gen_params* p, uint32_t lanes, uint64_t zmw_offset,
+                              hw_trace_generator** out);
+int hw_trace_generator_destroy(hw_trace_generator* g);
+/* Writes frames [first_frame, first_frame + frames) for all lanes; chunks
+ * must be requested in order. */
+int hw_trace_generator_next(hw_trace_generator* g, int16_t* d_out, int32_t first_frame, uint32_t frames,
+                            void* stream);
+
 #ifdef __cplusplus
 }   /* extern "C" */
 #endif
