@@ -30,20 +30,36 @@ template <int FT> struct FLayout
 {
     using S = FSpec<FT>;
     static constexpr int nStages = 2 * S::n;           // per filter
+    static constexpr int kSmemMaxWidth = 17;           // wider windows stay in global memory
     static constexpr int Width(int k) { return S::w[k / 2]; }
     // lower: erode, dilate, then erode/dilate; upper: dilate, erode, then erode/dilate
     static constexpr bool IsMax(bool upper, int k) { return (k < 2 && upper) ? (k == 0) : (k % 2 == 1); }
-    static constexpr int RingTotal()
+    static constexpr bool InSmem(int k) { return Width(k) <= kSmemMaxWidth; }
+    static constexpr int Idx(bool upper, int k) { return (upper ? nStages : 0) + k; }   // 0 .. 2*nStages-1
+    // Every stage keeps S[W] (suffix extrema of the previous block) and B[W]
+    // (inputs of the current block) in shared or global memory.
+    static constexpr int SmemSlots()
     {
         int t = 0;
-        for (int k = 0; k < nStages; ++k) t += Width(k);
+        for (int k = 0; k < nStages; ++k) if (InSmem(k)) t += 2 * Width(k);
         return 2 * t;
     }
-    static constexpr int RingOffset(bool upper, int k)
+    static constexpr int Offset(bool upper, int k)   // within its storage (smem or global)
     {
-        int t = upper ? RingTotal() / 2 : 0;
-        for (int j = 0; j < k; ++j) t += Width(j);
+        int t = 0;
+        for (int u = 0; u < 2; ++u)
+            for (int j = 0; j < nStages; ++j)
+            {
+                if (u == (upper ? 1 : 0) && j == k) return t;
+                if (InSmem(j) == InSmem(k)) t += 2 * Width(j);
+            }
         return t;
+    }
+    static constexpr int GlobalRingSlots()
+    {
+        int t = 0;
+        for (int k = 0; k < nStages; ++k) if (!InSmem(k)) t += 2 * Width(k);
+        return 2 * t;
     }
     static constexpr int CumStride(int i)
     {
@@ -52,100 +68,147 @@ template <int FT> struct FLayout
         return c;
     }
     static constexpr int AggStride() { return CumStride(S::n - 1); }
-    // int16 state slots: rings, then (hold, counter) per stage, then latData, latRaw, masks
-    static constexpr int SlotHold(bool upper, int k) { return RingTotal() + 2 * ((upper ? nStages : 0) + k); }
-    static constexpr int SlotLatData() { return RingTotal() + 4 * nStages; }
+    // int16 state: smem-resident arrays, global-resident arrays, then (P, c)
+    // per stage, then latData, latRaw, masks.
+    static constexpr int SlotSmem() { return 0; }
+    static constexpr int SlotGlobal() { return SmemSlots(); }
+    static constexpr int SlotPC(bool upper, int k) { return SmemSlots() + GlobalRingSlots() + 2 * Idx(upper, k); }
+    static constexpr int SlotLatData() { return SmemSlots() + GlobalRingSlots() + 4 * nStages; }
     static constexpr int NumI16Slots() { return SlotLatData() + 3; }
 };
 
-// One van Herk/Gil-Werman window stage (TraceFilters.cpp:11-57 with the
-// WindowBuffer of WindowBuffer.h: ring head == counter at all times).
+// One van Herk/Gil-Werman window stage.  The output for each input is the
+// extremum of the W previous inputs (TraceFilters.cpp:11-57 with the window
+// state of WindowBuffer.h; the initial window holds W zeros).  The state is
+// the suffix extrema S of the previous block of W inputs, the running
+// extremum P of the current block and the current block's inputs B; the
+// output at block position c is op(S[c], P).  `base` points at S[0] of this
+// thread and `stride` separates consecutive array elements.
 template <int W, bool IsMax>
-__device__ __forceinline__ int16_t StageStep(int16_t* ring, int16_t& hold, int16_t& counter, int16_t x)
+__device__ __forceinline__ int16_t StageStep(int16_t* base, int stride, int16_t& P, int16_t& counter, int16_t x)
 {
     auto op = [](int16_t a, int16_t b) -> int16_t {
         return IsMax ? (a > b ? a : b) : (a < b ? a : b);
     };
+    int16_t* S = base;
+    int16_t* B = base + W * stride;
     const int c = counter;
-    int16_t s;
-    if (c == 0)
+    const int16_t y = op(S[c * stride], P);
+    B[c * stride] = x;
+    P = op(P, x);
+    if (c + 1 == W)
     {
+        int16_t acc = x;
+        S[(W - 1) * stride] = acc;
 #pragma unroll 4
-        for (int j = W - 1; j > 0; --j) ring[j - 1] = op(ring[j], ring[j - 1]);
-        s = ring[W - 1];
+        for (int j = W - 2; j >= 0; --j)
+        {
+            acc = op(B[j * stride], acc);
+            S[j * stride] = acc;
+        }
+        P = IsMax ? (int16_t)-32768 : (int16_t)32767;
+        counter = 0;
     }
     else
     {
-        s = op(hold, ring[c - 1]);
+        counter = (int16_t)(c + 1);
     }
-    const int16_t front = ring[c];
-    ring[c] = x;
-    hold = s;
-    counter = (int16_t)((c + 1 == W) ? 0 : c + 1);
-    return op(s, front);
+    return y;
+}
+
+struct StageMem
+{
+    int16_t* smem;     // this thread's column in shared memory
+    int sstride;       // blockDim.x
+    int16_t* gmem;     // this ZMW's column of the global-resident arrays
+    int gstride;       // nZmw
+};
+
+template <int FT, bool Upper, int K>
+__device__ __forceinline__ int16_t Stage(const StageMem& m, int16_t* pc, int16_t x)
+{
+    using Lay = FLayout<FT>;
+    constexpr int W = Lay::Width(K);
+    constexpr int off = Lay::Offset(Upper, K);
+    constexpr int i = Lay::Idx(Upper, K);
+    if constexpr (Lay::InSmem(K))
+        return StageStep<W, Lay::IsMax(Upper, K)>(m.smem + off * m.sstride, m.sstride, pc[2 * i], pc[2 * i + 1], x);
+    else
+        return StageStep<W, Lay::IsMax(Upper, K)>(m.gmem + (size_t)off * m.gstride, m.gstride, pc[2 * i], pc[2 * i + 1], x);
 }
 
 template <int FT, bool Upper, int Scale>
-__device__ __forceinline__ int16_t RunScale(int16_t* ring, int16_t* hc, int16_t x)
+__device__ __forceinline__ int16_t RunScale(const StageMem& m, int16_t* pc, int16_t x)
 {
-    using Lay = FLayout<FT>;
-    constexpr int k0 = 2 * Scale, k1 = 2 * Scale + 1;
-    constexpr int o0 = Lay::RingOffset(Upper, k0) - (Upper ? Lay::RingTotal() / 2 : 0);
-    constexpr int o1 = Lay::RingOffset(Upper, k1) - (Upper ? Lay::RingTotal() / 2 : 0);
-    const int16_t y = StageStep<Lay::Width(k0), Lay::IsMax(Upper, k0)>(ring + o0, hc[2 * k0], hc[2 * k0 + 1], x);
-    return StageStep<Lay::Width(k1), Lay::IsMax(Upper, k1)>(ring + o1, hc[2 * k1], hc[2 * k1 + 1], y);
+    const int16_t y = Stage<FT, Upper, 2 * Scale>(m, pc, x);
+    return Stage<FT, Upper, 2 * Scale + 1>(m, pc, y);
 }
 
 // Feeds frame t (relative to the chunk) through one multi-scale filter; returns
 // true and the envelope value when the last stage produced an output.
 template <int FT, bool Upper>
-__device__ __forceinline__ bool FeedFilter(int t, int16_t x, int16_t* ring, int16_t* hc, int16_t& out)
+__device__ __forceinline__ bool FeedFilter(int t, int16_t x, const StageMem& m, int16_t* pc, int16_t& out)
 {
     using S = FSpec<FT>;
     using Lay = FLayout<FT>;
     if (t % Lay::CumStride(0) != 0) return false;
-    int16_t y = RunScale<FT, Upper, 0>(ring, hc, x);
+    int16_t y = RunScale<FT, Upper, 0>(m, pc, x);
     if constexpr (S::n > 1)
     {
         if (t % Lay::CumStride(1) != 0) return false;
-        y = RunScale<FT, Upper, 1>(ring, hc, y);
+        y = RunScale<FT, Upper, 1>(m, pc, y);
     }
     if constexpr (S::n > 2)
     {
         if (t % Lay::CumStride(2) != 0) return false;
-        y = RunScale<FT, Upper, 2>(ring, hc, y);
+        y = RunScale<FT, Upper, 2>(m, pc, y);
     }
     out = y;
     return true;
 }
 
-
+// Initial filter state: every window holds W zeros (S = 0), the current block
+// is empty (P = identity of the stage's operation, counter 0).
 template <int FT>
-__global__ void __launch_bounds__(128) BaselinerKernel(BaselinerArgs a, KParams k)
+__global__ void BaselinerInitKernel(int16_t* st16, float* st32, int lanes)
 {
     using Lay = FLayout<FT>;
-    constexpr int RT = Lay::RingTotal();
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nZmw = lanes * kLane;
+    if (g >= nZmw) return;
+    for (int i = 0; i < Lay::NumI16Slots(); ++i) st16[(size_t)i * nZmw + g] = 0;
+    for (int u = 0; u < 2; ++u)
+        for (int k = 0; k < Lay::nStages; ++k)
+            st16[(size_t)Lay::SlotPC(u == 1, k) * nZmw + g] = Lay::IsMax(u == 1, k) ? (int16_t)-32768 : (int16_t)32767;
+    st32[(size_t)0 * nZmw + g] = 0.0f;
+    st32[(size_t)1 * nZmw + g] = 0.0f;
+    st32[(size_t)2 * nZmw + g] = 2.0f;     // blSigmaEma_ initial value
+}
+
+template <int FT>
+__global__ void __launch_bounds__(64, 6) BaselinerKernel(BaselinerArgs a, KParams k)
+{
+    using Lay = FLayout<FT>;
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     const int nZmw = a.lanes * kLane;
-    if (g >= nZmw) return;
+    if (g >= nZmw) return;     // whole lanes only: nZmw is a multiple of the block size
     const int lane = g / kLane, z = g % kLane;
 
-    // Load window state (rings are indexed dynamically: local memory).
-    int16_t ringL[RT / 2], ringU[RT / 2];
-    int16_t hcL[2 * Lay::nStages], hcU[2 * Lay::nStages];
+    // Window state: narrow windows in shared memory (one column per thread),
+    // wide ones used in place in global memory.
+    extern __shared__ int16_t blSmem[];
+    constexpr int SS = Lay::SmemSlots();
+    const StageMem mem{blSmem + threadIdx.x, (int)blockDim.x, a.st16 + (size_t)Lay::SlotGlobal() * nZmw + g, nZmw};
 #pragma unroll 8
-    for (int i = 0; i < RT / 2; ++i)
-    {
-        ringL[i] = a.st16[(size_t)i * nZmw + g];
-        ringU[i] = a.st16[(size_t)(i + RT / 2) * nZmw + g];
-    }
+    for (int i = 0; i < SS; ++i) blSmem[i * blockDim.x + threadIdx.x] = a.st16[(size_t)(Lay::SlotSmem() + i) * nZmw + g];
+    int16_t pc[4 * Lay::nStages];
 #pragma unroll
-    for (int s = 0; s < Lay::nStages; ++s)
+    for (int i = 0; i < 2 * Lay::nStages; ++i)
     {
-        hcL[2 * s] = a.st16[(size_t)Lay::SlotHold(false, s) * nZmw + g];
-        hcL[2 * s + 1] = a.st16[(size_t)(Lay::SlotHold(false, s) + 1) * nZmw + g];
-        hcU[2 * s] = a.st16[(size_t)Lay::SlotHold(true, s) * nZmw + g];
-        hcU[2 * s + 1] = a.st16[(size_t)(Lay::SlotHold(true, s) + 1) * nZmw + g];
+        const bool up = i >= Lay::nStages;
+        const int k = up ? i - Lay::nStages : i;
+        pc[2 * i] = a.st16[(size_t)Lay::SlotPC(up, k) * nZmw + g];
+        pc[2 * i + 1] = a.st16[(size_t)(Lay::SlotPC(up, k) + 1) * nZmw + g];
     }
     int16_t latData = a.st16[(size_t)Lay::SlotLatData() * nZmw + g];
     int16_t latRaw = a.st16[(size_t)(Lay::SlotLatData() + 1) * nZmw + g];
@@ -169,12 +232,24 @@ __global__ void __launch_bounds__(128) BaselinerKernel(BaselinerArgs a, KParams 
     const int16_t ped = (int16_t)k.pedestal;
     float sub = 0.0f;
 
-    for (int t = 0; t < a.F; ++t)
+    // Frames go in blocks of 16: every cumulative stride divides 16 and F is a
+    // multiple of the aggregate stride (16), so with the block fully unrolled
+    // the set of filter scales that run at each frame is known at compile time.
+    constexpr int kB = 16;
+    static_assert(Lay::AggStride() == 16, "block size must be the aggregate stride");
+    for (int t0 = 0; t0 < a.F; t0 += kB)
     {
-        const int16_t x = __ldg(tr + (size_t)t * kLane);
+    int16_t xb[kB];
+#pragma unroll
+    for (int j = 0; j < kB; ++j) xb[j] = __ldg(tr + (size_t)(t0 + j) * kLane);
+#pragma unroll
+    for (int j = 0; j < kB; ++j)
+    {
+        const int t = t0 + j;
+        const int16_t x = xb[j];
         int16_t lo = 0, up = 0;
-        const bool haveL = FeedFilter<FT, false>(t, x, ringL, hcL, lo);
-        FeedFilter<FT, true>(t, x, ringU, hcU, up);
+        const bool haveL = FeedFilter<FT, false>(j, x, mem, pc, lo);
+        FeedFilter<FT, true>(j, x, mem, pc, up);
         if (haveL)
         {
             // GetSmoothedBlEstimate (HostMultiScaleBaseliner.cpp:179-212)
@@ -229,21 +304,18 @@ __global__ void __launch_bounds__(128) BaselinerKernel(BaselinerArgs a, KParams 
         latRaw = raw;
         latData = bls;
     }
+    }
 
     // Store state.
 #pragma unroll 8
-    for (int i = 0; i < RT / 2; ++i)
-    {
-        a.st16[(size_t)i * nZmw + g] = ringL[i];
-        a.st16[(size_t)(i + RT / 2) * nZmw + g] = ringU[i];
-    }
+    for (int i = 0; i < SS; ++i) a.st16[(size_t)(Lay::SlotSmem() + i) * nZmw + g] = blSmem[i * blockDim.x + threadIdx.x];
 #pragma unroll
-    for (int s = 0; s < Lay::nStages; ++s)
+    for (int i = 0; i < 2 * Lay::nStages; ++i)
     {
-        a.st16[(size_t)Lay::SlotHold(false, s) * nZmw + g] = hcL[2 * s];
-        a.st16[(size_t)(Lay::SlotHold(false, s) + 1) * nZmw + g] = hcL[2 * s + 1];
-        a.st16[(size_t)Lay::SlotHold(true, s) * nZmw + g] = hcU[2 * s];
-        a.st16[(size_t)(Lay::SlotHold(true, s) + 1) * nZmw + g] = hcU[2 * s + 1];
+        const bool up = i >= Lay::nStages;
+        const int k = up ? i - Lay::nStages : i;
+        a.st16[(size_t)Lay::SlotPC(up, k) * nZmw + g] = pc[2 * i];
+        a.st16[(size_t)(Lay::SlotPC(up, k) + 1) * nZmw + g] = pc[2 * i + 1];
     }
     a.st16[(size_t)Lay::SlotLatData() * nZmw + g] = latData;
     a.st16[(size_t)(Lay::SlotLatData() + 1) * nZmw + g] = latRaw;
@@ -299,18 +371,48 @@ int BaselinerNumSlots16(int ft)
     return -1;
 }
 
+template <int FT>
+cudaError_t LaunchBaselinerT(const BaselinerArgs& a, const KParams& k, cudaStream_t s)
+{
+    const int threads = kLane;
+    const size_t smem = sizeof(int16_t) * FLayout<FT>::SmemSlots() * threads;
+    static bool attr = false;
+    if (!attr)
+    {
+        cudaError_t e = cudaFuncSetAttribute(BaselinerKernel<FT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    BaselinerKernel<FT><<<a.lanes, threads, smem, s>>>(a, k);
+    return cudaGetLastError();
+}
+
 cudaError_t LaunchBaseliner(int ft, const BaselinerArgs& a, const KParams& k, cudaStream_t s)
 {
-    const int threads = 128;
-    const int blocks = (a.lanes * kLane + threads - 1) / threads;
     switch (ft)
     {
-    case 0: BaselinerKernel<0><<<blocks, threads, 0, s>>>(a, k); break;
-    case 1: BaselinerKernel<1><<<blocks, threads, 0, s>>>(a, k); break;
-    case 2: BaselinerKernel<2><<<blocks, threads, 0, s>>>(a, k); break;
-    case 3: BaselinerKernel<3><<<blocks, threads, 0, s>>>(a, k); break;
-    case 4: BaselinerKernel<4><<<blocks, threads, 0, s>>>(a, k); break;
-    case 5: BaselinerKernel<5><<<blocks, threads, 0, s>>>(a, k); break;
+    case 0: return LaunchBaselinerT<0>(a, k, s);
+    case 1: return LaunchBaselinerT<1>(a, k, s);
+    case 2: return LaunchBaselinerT<2>(a, k, s);
+    case 3: return LaunchBaselinerT<3>(a, k, s);
+    case 4: return LaunchBaselinerT<4>(a, k, s);
+    case 5: return LaunchBaselinerT<5>(a, k, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t LaunchBaselinerInit(int ft, int16_t* st16, float* st32, int lanes, cudaStream_t s)
+{
+    const int threads = 128;
+    const int blocks = (lanes * kLane + threads - 1) / threads;
+    switch (ft)
+    {
+    case 0: BaselinerInitKernel<0><<<blocks, threads, 0, s>>>(st16, st32, lanes); break;
+    case 1: BaselinerInitKernel<1><<<blocks, threads, 0, s>>>(st16, st32, lanes); break;
+    case 2: BaselinerInitKernel<2><<<blocks, threads, 0, s>>>(st16, st32, lanes); break;
+    case 3: BaselinerInitKernel<3><<<blocks, threads, 0, s>>>(st16, st32, lanes); break;
+    case 4: BaselinerInitKernel<4><<<blocks, threads, 0, s>>>(st16, st32, lanes); break;
+    case 5: BaselinerInitKernel<5><<<blocks, threads, 0, s>>>(st16, st32, lanes); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -199,10 +199,8 @@ int hw_baseliner_create(const hw_config* cfg, uint32_t pool_id, uint32_t lanes, 
     const size_t nZmw = (size_t)lanes * kLane;
     if ((rc = DevAlloc(&b->st16, (size_t)b->slots16 * nZmw, "hw_baseliner_create"))) return rc;
     if ((rc = DevAlloc(&b->st32, 3 * nZmw, "hw_baseliner_create"))) { cudaFree(b->st16); return rc; }
-    HW_CUDA(cudaMemset(b->st16, 0, (size_t)b->slots16 * nZmw * sizeof(int16_t)), "hw_baseliner_create");
-    std::vector<float> init(3 * nZmw, 0.0f);
-    for (size_t i = 0; i < nZmw; ++i) init[2 * nZmw + i] = 2.0f;   // blSigmaEma_ initial value
-    HW_CUDA(cudaMemcpy(b->st32, init.data(), init.size() * sizeof(float), cudaMemcpyHostToDevice), "hw_baseliner_create");
+    HW_CUDA(LaunchBaselinerInit(cfg->filter_type, b->st16, b->st32, (int)lanes, 0), "hw_baseliner_create");
+    HW_CUDA(cudaDeviceSynchronize(), "hw_baseliner_create");
     *out = b.release();
     return HW_OK;
 }

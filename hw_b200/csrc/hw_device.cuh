@@ -167,6 +167,7 @@ struct PulseArgs
 
 int BaselinerNumSlots16(int ft);
 cudaError_t LaunchBaseliner(int ft, const BaselinerArgs& a, const KParams& k, cudaStream_t s);
+cudaError_t LaunchBaselinerInit(int ft, int16_t* st16, float* st32, int lanes, cudaStream_t s);
 cudaError_t LaunchAggReset(hw_baseliner_stats* s, int lanes, cudaStream_t st);
 cudaError_t LaunchAggMerge(hw_baseliner_stats* acc, const hw_baseliner_stats* in, int lanes, cudaStream_t st);
 cudaError_t LaunchHistResetStats(hw_lane_histogram* h, const hw_baseliner_stats* s, int lanes, const KParams& k,

@@ -106,25 +106,31 @@ struct ZScorer
 };
 
 // Max over a row: first entry, then the contiguous segment; ties go to the
-// later entry (Recursion, FrameLabelerHost.cpp:214-264).
+// later entry (Recursion, FrameLabelerHost.cpp:214-264).  Instead of the
+// source state the row returns its traceback code already shifted into place:
+// 9-way rows (baseline, pulse-up) code source s as 0 for state 0 and s - 4
+// for states 5..12 in 4 bits; 2-way rows (full, down) code the second source
+// as a single bit, which is just the outcome of the one comparison.
 template <int R>
-__device__ __forceinline__ void ViterbiRow(const KParams& k, float score, const float* ll, float& outVal, int& outIdx)
+__device__ __forceinline__ float ViterbiRow(const KParams& k, float score, const float* ll, uint32_t& code)
 {
-    constexpr int first = (R == 0 || (R >= 5 && R <= 8)) ? 0 : (R <= 4 ? R : R - 8);
-    constexpr int sb = (R == 0 || (R >= 5 && R <= 8)) ? 5 : (R <= 4 ? R + 4 : R - 4);
-    constexpr int se = (R == 0 || (R >= 5 && R <= 8)) ? 13 : sb + 1;
+    constexpr bool nineWay = (R == 0 || (R >= 5 && R <= 8));
+    constexpr int first = nineWay ? 0 : (R <= 4 ? R : R - 8);
+    constexpr int sb = nineWay ? 5 : (R <= 4 ? R + 4 : R - 4);
+    constexpr int se = nineWay ? 13 : sb + 1;
+    constexpr int shift = (R == 0) ? 0 : (R <= 4 ? 20 + R - 1 : (R <= 8 ? 4 + 4 * (R - 5) : 24 + R - 9));
     float mv = add_rn(add_rn(score, k.trans[R][first]), ll[first]);
-    int idx = first;
+    uint32_t c = 0u;
 #pragma unroll
     for (int p = sb; p < se; ++p)
     {
         const float v = add_rn(add_rn(score, k.trans[R][p]), ll[p]);
-        const bool c = v >= mv;
-        mv = c ? v : mv;
-        idx = c ? p : idx;
+        const bool ge = v >= mv;
+        mv = ge ? v : mv;
+        c = ge ? ((uint32_t)(nineWay ? p - 4 : 1) << shift) : c;
     }
-    outVal = mv;
-    outIdx = idx;
+    code = c;
+    return mv;
 }
 
 // One Viterbi recursion step; returns the packed traceback word.
@@ -133,38 +139,25 @@ __device__ __forceinline__ uint32_t ViterbiStep(const KParams& k, const ZScorer&
     float sco[9];
     sc.Scores(data, sco);
     float nl[kStates];
-    int idx[kStates];
-    ViterbiRow<0>(k, sco[0], ll, nl[0], idx[0]);
-    ViterbiRow<1>(k, sco[1], ll, nl[1], idx[1]);
-    ViterbiRow<2>(k, sco[2], ll, nl[2], idx[2]);
-    ViterbiRow<3>(k, sco[3], ll, nl[3], idx[3]);
-    ViterbiRow<4>(k, sco[4], ll, nl[4], idx[4]);
-    ViterbiRow<5>(k, sco[5], ll, nl[5], idx[5]);
-    ViterbiRow<6>(k, sco[6], ll, nl[6], idx[6]);
-    ViterbiRow<7>(k, sco[7], ll, nl[7], idx[7]);
-    ViterbiRow<8>(k, sco[8], ll, nl[8], idx[8]);
-    ViterbiRow<9>(k, sco[5], ll, nl[9], idx[9]);
-    ViterbiRow<10>(k, sco[6], ll, nl[10], idx[10]);
-    ViterbiRow<11>(k, sco[7], ll, nl[11], idx[11]);
-    ViterbiRow<12>(k, sco[8], ll, nl[12], idx[12]);
+    uint32_t cd[kStates];
+    nl[0] = ViterbiRow<0>(k, sco[0], ll, cd[0]);
+    nl[1] = ViterbiRow<1>(k, sco[1], ll, cd[1]);
+    nl[2] = ViterbiRow<2>(k, sco[2], ll, cd[2]);
+    nl[3] = ViterbiRow<3>(k, sco[3], ll, cd[3]);
+    nl[4] = ViterbiRow<4>(k, sco[4], ll, cd[4]);
+    nl[5] = ViterbiRow<5>(k, sco[5], ll, cd[5]);
+    nl[6] = ViterbiRow<6>(k, sco[6], ll, cd[6]);
+    nl[7] = ViterbiRow<7>(k, sco[7], ll, cd[7]);
+    nl[8] = ViterbiRow<8>(k, sco[8], ll, cd[8]);
+    nl[9] = ViterbiRow<9>(k, sco[5], ll, cd[9]);
+    nl[10] = ViterbiRow<10>(k, sco[6], ll, cd[10]);
+    nl[11] = ViterbiRow<11>(k, sco[7], ll, cd[11]);
+    nl[12] = ViterbiRow<12>(k, sco[8], ll, cd[12]);
     const float pen = isRoi ? 0.0f : __int_as_float(0x7f800000);
     ll[0] = nl[0];
 #pragma unroll
     for (int r = 1; r < kStates; ++r) ll[r] = nl[r] - pen;
-    uint32_t w = (idx[0] == 0) ? 0u : (uint32_t)(idx[0] - 4);
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-    {
-        const int i = idx[5 + u];
-        w |= ((i == 0) ? 0u : (uint32_t)(i - 4)) << (4 + 4 * u);
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-    {
-        w |= (idx[1 + u] == 1 + u ? 0u : 1u) << (20 + u);
-        w |= (idx[9 + u] == 1 + u ? 0u : 1u) << (24 + u);
-    }
-    return w;
+    return ((cd[0] | cd[1] | cd[2]) | (cd[3] | cd[4] | cd[5])) | ((cd[6] | cd[7] | cd[8]) | (cd[9] | cd[10] | cd[11])) | cd[12];
 }
 
 // Source state of `state` recorded in traceback word `w`.
@@ -187,6 +180,7 @@ __device__ __forceinline__ int TraceSource(uint32_t w, int state)
 
 
 constexpr int kMaxRoiWords = (1024 + 22 + 15) / 16;   // F up to 1024
+constexpr int kBatch = 8;                              // frames loaded ahead
 
 __global__ void __launch_bounds__(128) LabelerKernel(LabelerArgs A, KParams k)
 {
@@ -225,7 +219,14 @@ __global__ void __launch_bounds__(128) LabelerKernel(LabelerArgs A, KParams k)
             p0 = p1; p1 = p2; p2 = sn;
         };
         for (int i = hwp::kRoiLookForward; i < kLatent; ++i) process(mul_rn((float)pl[(size_t)i * kLane], inv1));
-        for (int i = 0; i < F; ++i) process(mul_rn((float)__ldg(chunk + (size_t)i * kLane), inv2));
+        for (int i0 = 0; i0 < F; i0 += kBatch)
+        {
+            int16_t x[kBatch];
+#pragma unroll
+            for (int j = 0; j < kBatch; ++j) x[j] = __ldg(chunk + (size_t)(i0 + j) * kLane);
+#pragma unroll
+            for (int j = 0; j < kBatch; ++j) process(mul_rn((float)x[j], inv2));
+        }
         if (ri & 15) roiw[ri >> 4] = word;
         // Backward recursion: 2-bit codes become 0/1 (in place, bit 0 of each code).
         uint32_t pr = 0;
@@ -256,17 +257,37 @@ __global__ void __launch_bounds__(128) LabelerKernel(LabelerArgs A, KParams k)
     uint32_t* tb = A.tb + (size_t)l * (F + kLookback) * kLane + z;
     ZScorer sc;
     sc.Setup(k, oldM, z);
+    uint32_t roiWord = roiw[0];
     for (int f = 0; f < kLatent; ++f)
-        tb[(size_t)f * kLane] = ViterbiStep(k, sc, (float)pl[(size_t)f * kLane], roiBit(f), ll);
+    {
+        if ((f & 15) == 0) roiWord = roiw[f >> 4];
+        const bool isRoi = (roiWord >> (2 * (f & 15))) & 1u;
+        tb[(size_t)f * kLane] = ViterbiStep(k, sc, (float)pl[(size_t)f * kLane], isRoi, ll);
+    }
     sc.Setup(k, newM, z);
     const int anchor = F - kLatent;
-    for (int f = 0; f < anchor; ++f)
-        tb[(size_t)(f + kLatent) * kLane] = ViterbiStep(k, sc, (float)__ldg(chunk + (size_t)f * kLane), roiBit(f + kLatent), ll);
     float anchorLL[kStates];
+    // Chunk frames 0 .. anchor + 15 (labels kLatent .. F + 15).  F is a multiple
+    // of 8 and kLatent = 24, so the batches never straddle the anchor.
+    for (int f0 = 0; f0 < anchor + kLookback; f0 += kBatch)
+    {
+        int16_t x[kBatch];
 #pragma unroll
-    for (int i = 0; i < kStates; ++i) anchorLL[i] = ll[i];
-    for (int f = anchor; f < anchor + kLookback; ++f)
-        tb[(size_t)(f + kLatent) * kLane] = ViterbiStep(k, sc, (float)__ldg(chunk + (size_t)f * kLane), roiBit(f + kLatent), ll);
+        for (int j = 0; j < kBatch; ++j) x[j] = __ldg(chunk + (size_t)(f0 + j) * kLane);
+        if (f0 == anchor)
+        {
+#pragma unroll
+            for (int i = 0; i < kStates; ++i) anchorLL[i] = ll[i];
+        }
+#pragma unroll
+        for (int j = 0; j < kBatch; ++j)
+        {
+            const int lf = f0 + j + kLatent;
+            if ((lf & 15) == 0) roiWord = roiw[lf >> 4];
+            const bool isRoi = (roiWord >> (2 * (lf & 15))) & 1u;
+            tb[(size_t)lf * kLane] = ViterbiStep(k, sc, (float)x[j], isRoi, ll);
+        }
+    }
 
     // Normalize (FrameLabelerHost.cpp:186-205) and back-propagation.
     float prob[kStates];
@@ -312,10 +333,17 @@ __global__ void __launch_bounds__(128) LabelerKernel(LabelerArgs A, KParams k)
 
     int ts = anchorState;
     int16_t* out = A.labels + (size_t)l * F * kLane + z;
-    for (int f = F - 1; f >= 0; --f)
+    for (int f0 = F - kBatch; f0 >= 0; f0 -= kBatch)
     {
-        out[(size_t)f * kLane] = (int16_t)ts;
-        ts = TraceSource(tb[(size_t)f * kLane], ts);
+        uint32_t w[kBatch];
+#pragma unroll
+        for (int j = 0; j < kBatch; ++j) w[j] = tb[(size_t)(f0 + j) * kLane];
+#pragma unroll
+        for (int j = kBatch - 1; j >= 0; --j)
+        {
+            out[(size_t)(f0 + j) * kLane] = (int16_t)ts;
+            ts = TraceSource(w[j], ts);
+        }
     }
 
     // Latent state update.
@@ -341,7 +369,7 @@ __global__ void LabelerModelCopyKernel(hw_lane_model* dst, const hw_lane_model* 
 
 cudaError_t LaunchLabeler(const LabelerArgs& a, const KParams& k, cudaStream_t s)
 {
-    if (a.F > 1024) return cudaErrorInvalidValue;
+    if (a.F > 1024 || a.F % kBatch != 0) return cudaErrorInvalidValue;
     const int threads = 128;
     const int blocks = (a.lanes * kLane + threads - 1) / threads;
     LabelerKernel<<<blocks, threads, 0, s>>>(a, k);

@@ -31,11 +31,25 @@ __global__ void __launch_bounds__(128) PulseKernel(PulseArgs A, KParams k)
     const int16_t* lab = A.labels + (size_t)l * A.F * kLane + z;
     const int16_t* lat = A.latTrace + (size_t)l * kLatent * kLane + z;
     const int16_t* tr = A.trace + (size_t)l * A.F * kLane + z;
-    for (int rel = 0; rel < A.F; ++rel)
+    constexpr int kB = 8;
+    for (int rel0 = 0; rel0 < A.F; rel0 += kB)
     {
+        // Load the next kB labels and signals ahead of use (F % 8 == 0).
+        int16_t lbB[kB], sgB[kB];
+#pragma unroll
+        for (int j = 0; j < kB; ++j)
+        {
+            const int r = rel0 + j;
+            lbB[j] = __ldg(lab + (size_t)r * kLane);
+            sgB[j] = (r < kLatent) ? __ldg(lat + (size_t)r * kLane) : __ldg(tr + (size_t)(r - kLatent) * kLane);
+        }
+#pragma unroll
+        for (int j = 0; j < kB; ++j)
+        {
+        const int rel = rel0 + j;
         const uint32_t absF = (uint32_t)rel + A.firstFrame;
-        const int16_t lb = __ldg(lab + (size_t)rel * kLane);
-        const int16_t signal = (rel < kLatent) ? __ldg(lat + (size_t)rel * kLane) : __ldg(tr + (size_t)(rel - kLatent) * kLane);
+        const int16_t lb = lbB[j];
+        const int16_t signal = sgB[j];
         const bool isUp = (lb > kAnalogs) & (lb <= 2 * kAnalogs);
         const bool boundary = isUp | ((lb == 0) & (label != 0));
         const bool pulseM = label != 0;
@@ -78,6 +92,7 @@ __global__ void __launch_bounds__(128) PulseKernel(PulseArgs A, KParams k)
             const float x = (float)signal;
             b0 += 1.0f; b1 = add_rn(b1, x); b2 = add_rn(b2, mul_rn(x, x));
         }
+            }
     }
     A.segStart[g] = start; A.segFirst[g] = first; A.segLast[g] = last; A.segMax[g] = mx;
     A.segTotal[g] = total; A.segM2[g] = m2; A.segLabel[g] = label;
@@ -91,6 +106,7 @@ __global__ void __launch_bounds__(128) PulseKernel(PulseArgs A, KParams k)
 
 cudaError_t LaunchPulses(const PulseArgs& a, const KParams& k, cudaStream_t s)
 {
+    if (a.F % 8 != 0) return cudaErrorInvalidValue;
     const int threads = 128;
     const int blocks = (a.lanes * kLane + threads - 1) / threads;
     PulseKernel<<<blocks, threads, 0, s>>>(a, k);

@@ -148,7 +148,8 @@ struct EdgeState
     uint8_t* bits;      // [nZmw]: bit0 isBl(t-1), bit1 isBl(t-2), bits 2-3 count (0..2)
 };
 
-constexpr int kHistLanesPerBlock = 2;
+constexpr int kHistLanesPerBlock = 1;
+constexpr int kHistBatch = 8;
 
 // AddBlock (TraceHistogramAccumHost.cpp:140-169): edge scrubbing with the fp16
 // baseline mode, then UHistogramSimd::AddDatum.  Counts of the lane are held
@@ -176,9 +177,7 @@ HistAddKernel(hw_lane_histogram* hist, EdgeState es, const int16_t* traces, int 
     bool b1 = bits & 1, b2 = (bits >> 1) & 1;
     int n = (bits >> 2) & 3;
     const int16_t* tr = traces + (size_t)l * frames * kLane + z;
-    for (int f = 0; f < frames; ++f)
-    {
-        const int16_t x = __ldg(tr + (size_t)f * kLane);
+    auto step = [&](int16_t x) {
         const bool isBl = x < thr;
         const bool edge = (n == 2) ? (isBl ^ b2) : true;
         const float xv = (float)prev;
@@ -192,7 +191,17 @@ HistAddKernel(hw_lane_histogram* hist, EdgeState es, const int16_t* traces, int 
         nHigh = (uint16_t)(nHigh + (mHigh ? 1 : 0));
         if ((!sel) | mLow | mHigh) bin = kBins;
         cnt[ll][bin][z] = (uint16_t)(cnt[ll][bin][z] + 1);
+    };
+    int f = 0;
+    for (; f + kHistBatch <= frames; f += kHistBatch)
+    {
+        int16_t x[kHistBatch];
+#pragma unroll
+        for (int j = 0; j < kHistBatch; ++j) x[j] = __ldg(tr + (size_t)(f + j) * kLane);
+#pragma unroll
+        for (int j = 0; j < kHistBatch; ++j) step(x[j]);
     }
+    for (; f < frames; ++f) step(__ldg(tr + (size_t)f * kLane));
     for (int b = 0; b < kBins; ++b) H.bin_count[b][z] = cnt[ll][b][z];
     H.outlier_count_low[z] = nLow;
     H.outlier_count_high[z] = nHigh;
