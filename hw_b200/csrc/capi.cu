@@ -76,6 +76,17 @@ int TakeDeviceError(int* dErr, cudaStream_t s, const char* where)
 
 }   // namespace
 
+int hwk::SetLastError(int code, const char* msg)
+{
+    g_lastError = msg;
+    return code;
+}
+
+int hwk::PrepareConfigNoAlloc(const hw_config* cfg, hwp::Derived* d, KParams* k)
+{
+    return PrepareConfig(cfg, d, k);
+}
+
 // ---------------------------------------------------------------------------
 
 struct hw_baseliner

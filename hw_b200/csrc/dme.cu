@@ -506,4 +506,74 @@ cudaError_t LaunchDmeEstimate(const DmeArgs& a, const KParams& k, cudaStream_t s
     return cudaGetLastError();
 }
 
+// ---- Estimate without device allocation -------------------------------------
+// Callers such as a pre-allocated real-time pipeline or code running inside a
+// custom allocator's callbacks may not be allowed to call cudaMalloc.  For
+// them hw_dme_estimate_noalloc keeps the EM's per-bin scratch in this fixed
+// file-scope array instead of a handle-owned allocation.  Every GPU that
+// loads the library holds it (about 28 MiB) until the process exits.
+constexpr uint32_t kNoAllocMaxLanes = 128;
+constexpr size_t kDmeScratchFloatsPerLane = (size_t)3 * (kBins + 1) * kLane;
+static __device__ __align__(256) float g_dmeNoAllocScratch[kNoAllocMaxLanes * kDmeScratchFloatsPerLane];
+static __device__ __align__(256) int g_dmeNoAllocErr[64];
+
 }   // namespace hwk
+
+#include <mutex>
+
+extern "C" int hw_dme_estimate_noalloc(const hw_config* cfg, uint32_t lanes, const hw_lane_histogram* d_hist,
+                                       const hw_baseliner_stats* d_stats, hw_frame_interval hist_fi,
+                                       hw_frame_interval model_fi, hw_lane_model* d_models, hw_dme_diag* d_diag,
+                                       void* stream)
+{
+    using namespace hwk;
+    if (!cfg || !d_hist || !d_stats || !d_models) return SetLastError(HW_ERR_INVALID_ARG, "NULL argument");
+    if (lanes == 0 || lanes > kNoAllocMaxLanes)
+        return SetLastError(HW_ERR_INVALID_ARG,
+                            "hw_dme_estimate_noalloc: lanes must be in [1, 128]; split larger pools into calls of at most 128 lanes");
+    if (hist_fi.lower == hist_fi.upper || model_fi.lower == model_fi.upper)
+        return SetLastError(HW_ERR_INVALID_ARG, "frame intervals must not be empty");
+    hwp::Derived d;
+    KParams k;
+    int rc = PrepareConfigNoAlloc(cfg, &d, &k);
+    if (rc) return rc;
+
+    // Device addresses of the file-scope arrays, looked up once per device
+    // with that device current (host code cannot use the symbols directly).
+    static std::mutex mu;
+    static float* scratch[64] = {};
+    static int* err[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+        return SetLastError(HW_ERR_CUDA, "hw_dme_estimate_noalloc: no current CUDA device");
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (!scratch[dev])
+        {
+            float* p = nullptr;
+            int* e = nullptr;
+            cudaError_t ce = cudaGetSymbolAddress((void**)&p, g_dmeNoAllocScratch);
+            if (ce == cudaSuccess) ce = cudaGetSymbolAddress((void**)&e, g_dmeNoAllocErr);
+            if (ce != cudaSuccess)
+                return SetLastError(HW_ERR_CUDA, cudaGetErrorString(ce));
+            scratch[dev] = p;
+            err[dev] = e;
+        }
+    }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    // The error word keeps the previous call's value: clear it first.  The
+    // scratch needs no clearing: every bin is written before it is read.
+    cudaError_t ce = cudaMemsetAsync(err[dev], 0, sizeof(int), s);
+    if (ce != cudaSuccess) return SetLastError(HW_ERR_CUDA, cudaGetErrorString(ce));
+    DmeArgs a{d_hist, d_stats, d_models, d_diag, scratch[dev], err[dev], (int)lanes,
+              model_fi.lower + (model_fi.upper - model_fi.lower) / 2,
+              hist_fi.lower + (hist_fi.upper - hist_fi.lower) / 2};
+    ce = LaunchDmeEstimate(a, k, s);
+    if (ce != cudaSuccess) return SetLastError(HW_ERR_CUDA, cudaGetErrorString(ce));
+    int h = 0;
+    ce = cudaMemcpyAsync(&h, err[dev], sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    if (ce != cudaSuccess) return SetLastError(HW_ERR_CUDA, cudaGetErrorString(ce));
+    if (h) return SetLastError(h, "DME: a reference sanity assertion failed (non-finite estimate or bad SNR-drop threshold)");
+    return HW_OK;
+}

@@ -182,6 +182,10 @@ cudaError_t LaunchDmeEstimate(const DmeArgs& a, const KParams& k, cudaStream_t s
 cudaError_t LaunchLabeler(const LabelerArgs& a, const KParams& k, cudaStream_t s);
 cudaError_t LaunchPulses(const PulseArgs& a, const KParams& k, cudaStream_t s);
 struct GenArgs;
+// Records the thread's last error message (capi.cu) and returns code.
+int SetLastError(int code, const char* msg);
+// Configuration checks and derived constants without heap allocation on success.
+int PrepareConfigNoAlloc(const hw_config* cfg, hwp::Derived* d, KParams* k);
 cudaError_t LaunchGen(const GenArgs& a, cudaStream_t s);
 
 }   // namespace hwk

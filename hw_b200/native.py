@@ -57,6 +57,7 @@ def lib():
         "hw_dme_destroy": ([vp], C.c_int),
         "hw_dme_init_models": ([vp, vp, vp, vp], C.c_int),
         "hw_dme_estimate": ([vp, vp, vp, FI, FI, vp, vp, vp], C.c_int),
+        "hw_dme_estimate_noalloc": ([PCFG, u32, vp, vp, FI, FI, vp, vp, vp], C.c_int),
         "hw_labeler_create": ([PCFG, u32, u32, u32, PPV], C.c_int),
         "hw_labeler_destroy": ([vp], C.c_int),
         "hw_labeler_process": ([vp, vp, vp, vp, vp, vp, vp], C.c_int),

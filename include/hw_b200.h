@@ -322,6 +322,22 @@ int hw_dme_estimate(hw_dme* d, const hw_lane_histogram* d_hist, const hw_baselin
                     hw_frame_interval hist_fi, hw_frame_interval model_fi,
                     hw_lane_model* d_models, hw_dme_diag* d_diag, void* stream);
 
+/* Same estimate as hw_dme_estimate for callers that cannot allocate device
+ * memory (for example code that runs inside a custom allocator or a
+ * pre-sized real-time pipeline).  It needs no handle: the EM scratch is a
+ * fixed file-scope device array of about 28 MiB that every GPU loading the
+ * library holds until the process exits, so at most 128 lanes are accepted
+ * per call (HW_ERR_INVALID_ARG above that; split a pool into sub-ranges).
+ * The first call on each device looks up the array's device address, so
+ * make that first call before any stream capture.  All calls share the one
+ * array: calls that overlap on the GPU (different streams, threads or
+ * processes sharing a context) race.  Synchronous like hw_dme_estimate.
+ * This entry point has no counterpart in the reference. */
+int hw_dme_estimate_noalloc(const hw_config* cfg, uint32_t lanes, const hw_lane_histogram* d_hist,
+                            const hw_baseliner_stats* d_stats, hw_frame_interval hist_fi,
+                            hw_frame_interval model_fi, hw_lane_model* d_models, hw_dme_diag* d_diag,
+                            void* stream);
+
 /* ---- Frame labeler (FrameLabeler.h:67-74, FrameLabelerHost.cpp:314-612) - */
 typedef struct hw_labeler hw_labeler;
 int hw_labeler_create(const hw_config* cfg, uint32_t pool_id, uint32_t lanes,
