@@ -695,7 +695,10 @@ struct hw_analyzer
         if ((rc = hw_labeler_process(lab, bls, models, labels, latent, score, s))) return rc;
         End(t, s);
         t = Begin(HW_STAGE_PULSES, s);
-        rc = hw_pulse_accumulator_process(pa, labels, latent, bls, ff, models, pulses, lens, ovf, paStats, s);
+        // The labels batch starts hw_labeler_latent_frames() before the trace
+        // chunk (LabelsBatchFactory::NewBatch, LabelsBatch.h:112-121).
+        rc = hw_pulse_accumulator_process(pa, labels, latent, bls, ff - (int32_t)hwp::kLatentFrames, models, pulses,
+                                          lens, ovf, paStats, s);
         End(t, s);
         return rc;
     }

@@ -358,7 +358,11 @@ int hw_pulse_accumulator_create(const hw_config* cfg, uint32_t pool_id, uint32_t
                                 uint32_t frames_per_chunk, hw_pulse_accumulator** out);
 int hw_pulse_accumulator_destroy(hw_pulse_accumulator* p);
 /* d_pulses[lanes][64][max_calls_per_zmw]; d_lens/d_overflows[lanes][64];
- * d_blstats one hw_stat_accum_state per lane (PulseDetectorMetrics). */
+ * d_blstats one hw_stat_accum_state per lane (PulseDetectorMetrics).
+ * first_frame is the frame of d_labels[0]: the trace chunk's first frame
+ * minus hw_labeler_latent_frames(), as in the reference's labels batch
+ * metadata (LabelsBatch.h:112-121).  Pulse starts are first_frame + the
+ * relative frame, in uint32 arithmetic. */
 int hw_pulse_accumulator_process(hw_pulse_accumulator* p, const int16_t* d_labels,
                                  const int16_t* d_latent_trace, const int16_t* d_trace,
                                  int32_t first_frame, const hw_lane_model* d_models,

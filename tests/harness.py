@@ -180,7 +180,8 @@ class Pipeline:
     def _label_and_pulse(self, bls, ff, rec):
         labels, lat, score = self.b.label(bls, self.models)
         rec["labels"], rec["latent"], rec["score"] = labels, lat, score
-        rec["pulses"] = self.b.pulses(labels, lat, bls, ff, self.models)
+        # the labels batch starts LATENT_FRAMES before the trace chunk (LabelsBatch.h:112-121)
+        rec["pulses"] = self.b.pulses(labels, lat, bls, ff - abi.LATENT_FRAMES, self.models)
 
     def process(self, chunk, ff):
         """One chunk; returns the dict of stage outputs."""
