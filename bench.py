@@ -9,8 +9,10 @@ every pool re-estimates its detection models every 4000 frames, staggered by
 pool).  The run first streams the start-up chunks (untimed) until every pool
 is in its periodic estimation cycle; a step is then one chunk of the whole
 chip through baseliner -> statistics -> histogram -> (EM when due) ->
-labeler -> pulses.  K is rounded to whole 8-chunk estimation cycles is not
-needed for correctness but the default K=8 covers exactly one.
+labeler -> pulses.  The default K = 8 steps covers exactly one 8-chunk
+estimation cycle, so every pool runs its EM once inside the timed region.
+With --gpus N each rank analyses its own chip-sized ZMW range (weak
+scaling, no data exchange).
 
   value : ZMW-frames/s with the chunks already in HBM
   e2e   : same through hw_analyzer_process with the chunk copied from pinned
@@ -217,7 +219,8 @@ def main():
         return
 
     analyzers = [Fl.BatchAnalyzer(cfg, p, args.lanes_per_pool, FRAMES) for p in range(args.pools)]
-    gen = Fl.TraceGenerator(total_lanes, workload=1, zmw_offset=rank * zmws)
+    from hw_b200.shard import zmw_offset
+    gen = Fl.TraceGenerator(total_lanes, workload=1, zmw_offset=zmw_offset(rank, zmws))
     lpp = args.lanes_per_pool
     stream = torch.cuda.current_stream()
 
@@ -252,13 +255,7 @@ def main():
             import torch.distributed as dist
             dist.barrier()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        import torch.distributed as dist
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    from hw_b200.shard import max_over_ranks
 
     clocks = ClockSampler(local)
     barrier()

@@ -374,7 +374,7 @@ inline void DefaultConfig(hw_config* c)
     c->xsp_width_thresh = 3.5f;
     c->model_estimation_mode = HW_DYNAMIC_ESTIMATIONS;
     c->static_baseline_mean = 0.0f;
-    c->static_baseline_variance = 100.0f;
+    c->static_baseline_variance = 33.0f;     // StaticDetModelConfig.h:44
 }
 
 // ValidateConfig<> checks of the reference configs and Configure() asserts.

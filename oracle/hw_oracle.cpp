@@ -1678,6 +1678,26 @@ int or_pulses(void* p, const int16_t* labels, const int16_t* lat, const int16_t*
               const hw_lane_model* m, hw_pulse* pulses, uint32_t* lens, uint32_t* ovf, hw_stat_accum_state* bs)
 { return static_cast<OraclePool*>(p)->Pulses(labels, lat, tr, firstFrame, m, pulses, lens, ovf, bs); }
 
+// One BlockFilterStage (TraceFilters.cpp:11-57 on a WindowBuffer that starts
+// with `width` zeros) with stride 1 over `chunks` consecutive blocks of F
+// frames of one lane: in/out[chunks][F][64].  Pins the window semantics
+// against the reference's extrema-filter sawtooth test.
+int or_extremum_stage(int width, int isMax, const int16_t* in, int F, int chunks, int16_t* out)
+{
+    if (width < 1 || F < 1 || chunks < 0) { g_err = "or_extremum_stage: bad size"; return HW_ERR_INVALID_ARG; }
+    Stage st;
+    st.spec = hwp::StageSpec{width, 1, 1, isMax != 0};
+    st.wb.Init(width);
+    std::vector<int16_t> block((size_t)F * kLane);
+    for (int c = 0; c < chunks; ++c)
+    {
+        std::memcpy(block.data(), in + (size_t)c * F * kLane, sizeof(int16_t) * block.size());
+        st.Run(block.data(), F);
+        std::memcpy(out + (size_t)c * F * kLane, block.data(), sizeof(int16_t) * block.size());
+    }
+    return HW_OK;
+}
+
 float or_expf(float x) { return hw_expf(x); }
 float or_logf(float x) { return hw_logf(x); }
 uint16_t or_f32_to_f16(float x) { return f32_to_f16_bits(x); }

@@ -51,6 +51,7 @@ def lib():
         L.or_dme_estimate.argtypes = [vp, vp, vp, FI, FI, vp, vp]
         L.or_label.argtypes = [vp, vp, vp, vp, vp, vp]
         L.or_pulses.argtypes = [vp, vp, vp, vp, i32, vp, vp, vp, vp, vp]
+        L.or_extremum_stage.argtypes = [C.c_int, C.c_int, vp, C.c_int, C.c_int, vp]
         L.or_expf.argtypes = [C.c_float]
         L.or_expf.restype = C.c_float
         L.or_logf.argtypes = [C.c_float]
@@ -179,3 +180,12 @@ def expf(x):
 
 def logf(x):
     return lib().or_logf(float(x))
+
+
+def extremum_stage(width, is_max, blocks):
+    """One window stage (stride 1) over blocks[chunks][F][64] of one lane."""
+    blocks = np.ascontiguousarray(blocks, dtype=np.int16)
+    out = np.empty_like(blocks)
+    _check(lib().or_extremum_stage(int(width), int(bool(is_max)), abi.ptr(blocks), blocks.shape[1],
+                                   blocks.shape[0], abi.ptr(out)))
+    return out
