@@ -14,6 +14,8 @@
 // baselined trace written once, with coalesced 64-byte warp accesses.
 // Each stage window keeps the reference's van Herk/Gil-Werman state (ring of w
 // values, holdover, counter) so the filter outputs are bit-identical.
+#include <type_traits>
+
 #include "hw_device.cuh"
 
 namespace hwk {
@@ -144,23 +146,34 @@ __device__ __forceinline__ int16_t RunScale(const StageMem& m, int16_t* pc, int1
     return Stage<FT, Upper, 2 * Scale + 1>(m, pc, y);
 }
 
-// Feeds frame t (relative to the chunk) through one multi-scale filter; returns
-// true and the envelope value when the last stage produced an output.
-template <int FT, bool Upper>
-__device__ __forceinline__ bool FeedFilter(int t, int16_t x, const StageMem& m, int16_t* pc, int16_t& out)
+// Feeds one frame through one multi-scale filter; returns true and the
+// envelope value when the last stage produced an output.  Cumulative strides
+// are 1, 2 or 16 and chunks are multiples of 16 frames, so the scales that
+// run depend only on the frame's phase within its 16-frame block:
+// Phase 0 = first frame of the block, 1 = other even frames, 2 = odd frames.
+template <int Phase>
+__host__ __device__ constexpr bool ScaleRuns(int cumStride)
+{
+    return cumStride == 1 || (cumStride == 2 && Phase <= 1) || (cumStride == 16 && Phase == 0);
+}
+
+template <int FT, bool Upper, int Phase>
+__device__ __forceinline__ bool FeedFilter(int16_t x, const StageMem& m, int16_t* pc, int16_t& out)
 {
     using S = FSpec<FT>;
     using Lay = FLayout<FT>;
-    if (t % Lay::CumStride(0) != 0) return false;
+    static_assert(Lay::CumStride(0) <= 2 && (S::n < 2 || Lay::CumStride(1) <= 16) && Lay::AggStride() == 16,
+                  "phase scheme needs cumulative strides 1|2, 2, 16");
+    if constexpr (!ScaleRuns<Phase>(Lay::CumStride(0))) return false;
     int16_t y = RunScale<FT, Upper, 0>(m, pc, x);
     if constexpr (S::n > 1)
     {
-        if (t % Lay::CumStride(1) != 0) return false;
+        if constexpr (!ScaleRuns<Phase>(Lay::CumStride(1))) return false;
         y = RunScale<FT, Upper, 1>(m, pc, y);
     }
     if constexpr (S::n > 2)
     {
-        if (t % Lay::CumStride(2) != 0) return false;
+        if constexpr (!ScaleRuns<Phase>(Lay::CumStride(2))) return false;
         y = RunScale<FT, Upper, 2>(m, pc, y);
     }
     out = y;
@@ -232,24 +245,19 @@ __global__ void __launch_bounds__(64, 6) BaselinerKernel(BaselinerArgs a, KParam
     const int16_t ped = (int16_t)k.pedestal;
     float sub = 0.0f;
 
-    // Frames go in blocks of 16: every cumulative stride divides 16 and F is a
-    // multiple of the aggregate stride (16), so with the block fully unrolled
-    // the set of filter scales that run at each frame is known at compile time.
-    constexpr int kB = 16;
+    // Frames go in blocks of 16 (the aggregate stride): the first frame of a
+    // block, the other even frames and the odd frames each get their own
+    // specialisation of the frame body, with the trace loaded two frames ahead.
     static_assert(Lay::AggStride() == 16, "block size must be the aggregate stride");
-    for (int t0 = 0; t0 < a.F; t0 += kB)
-    {
-    int16_t xb[kB];
-#pragma unroll
-    for (int j = 0; j < kB; ++j) xb[j] = __ldg(tr + (size_t)(t0 + j) * kLane);
-#pragma unroll
-    for (int j = 0; j < kB; ++j)
-    {
-        const int t = t0 + j;
-        const int16_t x = xb[j];
+    int16_t xn0 = __ldg(tr), xn1 = __ldg(tr + kLane);
+    auto frame = [&](auto phaseTag, int t) {
+        constexpr int Ph = decltype(phaseTag)::value;
+        const int16_t x = xn0;
+        xn0 = xn1;
+        if (t + 2 < a.F) xn1 = __ldg(tr + (size_t)(t + 2) * kLane);
         int16_t lo = 0, up = 0;
-        const bool haveL = FeedFilter<FT, false>(j, x, mem, pc, lo);
-        FeedFilter<FT, true>(j, x, mem, pc, up);
+        const bool haveL = FeedFilter<FT, false, Ph>(x, mem, pc, lo);
+        FeedFilter<FT, true, Ph>(x, mem, pc, up);
         if (haveL)
         {
             // GetSmoothedBlEstimate (HostMultiScaleBaseliner.cpp:179-212)
@@ -303,7 +311,17 @@ __global__ void __launch_bounds__(64, 6) BaselinerKernel(BaselinerArgs a, KParam
         }
         latRaw = raw;
         latData = bls;
-    }
+    };
+#pragma unroll 1
+    for (int t0 = 0; t0 < a.F; t0 += 16)
+    {
+        frame(std::integral_constant<int, 0>{}, t0);
+#pragma unroll 1
+        for (int j = 1; j < 16; j += 2)
+        {
+            frame(std::integral_constant<int, 2>{}, t0 + j);
+            if (j + 1 < 16) frame(std::integral_constant<int, 1>{}, t0 + j + 1);
+        }
     }
 
     // Store state.

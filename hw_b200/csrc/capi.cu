@@ -714,8 +714,6 @@ int hw_analyzer_create(const hw_config* cfg, uint32_t pool_id, uint32_t lanes, u
     auto a = std::make_unique<hw_analyzer>();
     int rc = PrepareConfig(cfg, &a->d, &a->k);
     if (rc) return rc;
-    if (cfg->model_estimation_mode == HW_FIXED_ESTIMATIONS)
-        return Fail(HW_ERR_UNSUPPORTED, "FixedModelBatchAnalyzer is not built");
     a->cfg = *cfg;
     a->poolId = pool_id;
     a->lanes = lanes;
@@ -736,6 +734,15 @@ int hw_analyzer_create(const hw_config* cfg, uint32_t pool_id, uint32_t lanes, u
     if ((rc = DevAlloc(&a->paStats, lanes, "hw_analyzer_create"))) return rc;
     if ((rc = DevAlloc(&a->diag, lanes, "hw_analyzer_create"))) return rc;
     HW_CUDA(cudaMemset(a->models, 0, sizeof(hw_lane_model) * lanes), "hw_analyzer_create");
+    if (cfg->model_estimation_mode == HW_FIXED_ESTIMATIONS)
+    {
+        // FixedModelBatchAnalyzer: the static model in every lane, from the start
+        hw_lane_model m;
+        hwp::StaticModel(*cfg, &m);
+        std::vector<hw_lane_model> host(lanes, m);
+        HW_CUDA(cudaMemcpy(a->models, host.data(), sizeof(hw_lane_model) * lanes, cudaMemcpyHostToDevice),
+                "hw_analyzer_create");
+    }
     a->framesRemaining = (int32_t)cfg->num_frames_pre_accum_stats;
     a->blLatency = a->d.baselinerStartupLatency;
     const uint32_t chunksPerEstimate = (std::max(cfg->min_frames_for_estimate, 1u) + frames_per_chunk - 1) / frames_per_chunk;
@@ -765,7 +772,13 @@ int hw_analyzer_process(hw_analyzer* a, const int16_t* d_trace, int32_t first_fr
         a->End(t, s);
     }
     const hw_frame_interval fi{first_frame, first_frame + (int32_t)a->F};
-    if (a->cfg.model_estimation_mode == HW_INITIAL_ESTIMATIONS)
+    if (a->cfg.model_estimation_mode == HW_FIXED_ESTIMATIONS)
+    {
+        // FixedModelBatchAnalyzer::AnalyzeImpl (BatchAnalyzer.cpp:172-207)
+        if ((rc = a->LabelAndPulse(first_frame, d_pulses, d_lens, d_overflows, s))) return rc;
+        emit = true;
+    }
+    else if (a->cfg.model_estimation_mode == HW_INITIAL_ESTIMATIONS)
     {
         // SingleEstimateBatchAnalyzer::AnalyzeImpl (BatchAnalyzer.cpp:177-256)
         if (!a->initialized && first_frame > (int32_t)a->blLatency)

@@ -131,7 +131,7 @@ __device__ __forceinline__ float StatVarianceD(const hw_stat_accum_state& s, int
 }
 
 
-__global__ void __launch_bounds__(kLane) DmeEstimateKernel(DmeArgs A, KParams k)
+__global__ void __launch_bounds__(kLane, 8) DmeEstimateKernel(DmeArgs A, KParams k)
 {
     const int l = blockIdx.x;
     const int z = threadIdx.x;
@@ -303,7 +303,30 @@ __global__ void __launch_bounds__(kLane) DmeEstimateKernel(DmeArgs A, KParams k)
         }
         float probSum = 0.0f, wps = 0.0f;
         float ci[5] = {0, 0, 0, 0, 0}, mom1[5] = {0, 0, 0, 0, 0};
-        float tauPrev[5], bpPrev = 0.0f, xPrev = 0.0f;
+        // Only bins with a count contribute to c_i, mom1, wps and (in the
+        // M-step) mom2: an empty bin adds (finite) x 0 = +-0 to sums that start
+        // at +0 and therefore never hold -0, which leaves them unchanged.  So
+        // the responsibilities (5 exps), log(binProb) and n_j / binProb are
+        // only evaluated next to occupied bins; the boundary density, which
+        // every bin probability needs, is always evaluated.
+        // The shortcut needs every boundary density finite: llb <= max(pref) +
+        // log(5), so finite prefactors, means and inverse variances with
+        // max(pref) < 80 guarantee it.  Otherwise the reference path runs.
+        bool safe = true;
+        {
+            float pmax = pref[0];
+#pragma unroll
+            for (int i = 0; i < 5; ++i)
+            {
+                safe &= isfinite(pref[i]) & isfinite(mu[i]) & isfinite(varinv[i]);
+                pmax = fmaxf(pmax, pref[i]);
+            }
+            safe &= pmax < 80.0f;
+        }
+        float tauPrev[5] = {0, 0, 0, 0, 0}, bpPrev = 0.0f, xPrev = 0.0f;
+        uint32_t nPrev = 0;
+        // bin counts are loaded one boundary ahead of their use
+        uint32_t nNext = (uint32_t)H.bin_count[0][z];
         for (int b = 0; b <= kBins; ++b)
         {
             // cornerComp(b)
@@ -318,39 +341,65 @@ __global__ void __launch_bounds__(kLane) DmeEstimateKernel(DmeArgs A, KParams k)
             float tmax = t[0];
 #pragma unroll
             for (int i = 1; i < 5; ++i) tmax = fmax_sse(tmax, t[i]);
-            float se = hw_expf(t[0] - tmax);
+            const uint32_t nCur = nNext;
+            nNext = (b + 1 < kBins) ? (uint32_t)H.bin_count[b + 1][z] : 0u;
+            const bool needTau = (nPrev != 0u) | (nCur != 0u) | !safe;
+            // Far tails: with every t finite and below -106, llb = tmax +
+            // log(se) with 1 <= se <= 5 stays below -104.3, where hw_expf
+            // returns exactly 0, so bp is 0 without evaluating it.
+            bool allFinite = true;
 #pragma unroll
-            for (int i = 1; i < 5; ++i) se = add_rn(se, hw_expf(t[i] - tmax));
-            const float llb = add_rn(tmax, hw_logf(se));
+            for (int i = 0; i < 5; ++i) allFinite &= isfinite(t[i]);
+            const bool tail = !needTau & allFinite & (tmax < -106.0f);
+            float bp = 0.0f, llb = 0.0f;
+            if (!tail)
+            {
+                float se = hw_expf(t[0] - tmax);
+#pragma unroll
+                for (int i = 1; i < 5; ++i) se = add_rn(se, hw_expf(t[i] - tmax));
+                llb = add_rn(tmax, hw_logf(se));
+                bp = hw_expf(llb);
+            }
             float tau[5];
+            if (needTau)
+            {
 #pragma unroll
-            for (int i = 0; i < 5; ++i) tau[i] = hw_expf(t[i] - llb);
-            const float bp = hw_expf(llb);
-            bpS[(size_t)b * kLane + z] = bp;
-            tau0S[(size_t)b * kLane + z] = tau[0];
+                for (int i = 0; i < 5; ++i) tau[i] = hw_expf(t[i] - llb);
+                bpS[(size_t)b * kLane + z] = bp;
+                tau0S[(size_t)b * kLane + z] = tau[0];
+            }
+            else
+            {
+#pragma unroll
+                for (int i = 0; i < 5; ++i) tau[i] = 0.0f;
+            }
             if (b > 0)
             {
                 // centerComp(b - 1)
                 const int c = b - 1;
                 const float bpr = fmax_sse(mul_rn(mul_rn(0.5f, binSize), add_rn(bpPrev, bp)), binProbMin);
                 probSum = add_rn(probSum, bpr);
-                const float njb = (float)H.bin_count[c][z];
-                wps = add_rn(wps, mul_rn(njb, hw_logf(bpr)));
-                const float factor = njb / bpr;
-                facS[(size_t)c * kLane + z] = factor;
-#pragma unroll
-                for (int m = 0; m < 5; ++m)
+                if ((nPrev != 0u) | !safe)
                 {
-                    const float tmp1 = mul_rn(bpPrev, tauPrev[m]);
-                    const float tmp2 = mul_rn(bp, tau[m]);
-                    ci[m] = add_rn(ci[m], mul_rn(add_rn(tmp1, tmp2), factor));
-                    mom1[m] = add_rn(mom1[m], mul_rn(add_rn(mul_rn(tmp1, xPrev), mul_rn(tmp2, x)), factor));
+                    const float njb = (float)nPrev;
+                    wps = add_rn(wps, mul_rn(njb, hw_logf(bpr)));
+                    const float factor = njb / bpr;
+                    facS[(size_t)c * kLane + z] = factor;
+#pragma unroll
+                    for (int m = 0; m < 5; ++m)
+                    {
+                        const float tmp1 = mul_rn(bpPrev, tauPrev[m]);
+                        const float tmp2 = mul_rn(bp, tau[m]);
+                        ci[m] = add_rn(ci[m], mul_rn(add_rn(tmp1, tmp2), factor));
+                        mom1[m] = add_rn(mom1[m], mul_rn(add_rn(mul_rn(tmp1, xPrev), mul_rn(tmp2, x)), factor));
+                    }
                 }
             }
 #pragma unroll
             for (int i = 0; i < 5; ++i) tauPrev[i] = tau[i];
             bpPrev = bp;
             xPrev = x;
+            nPrev = nCur;
         }
         const float hb = mul_rn(0.5f, binSize);
 #pragma unroll
@@ -405,19 +454,33 @@ __global__ void __launch_bounds__(kLane) DmeEstimateKernel(DmeArgs A, KParams k)
 #pragma unroll
         for (int a = 0; a < kAnalogs; ++a) mu[a + 1] = mul_rn(sv, k.relAmp[a]);
         // Background variance: second pass over the bins.
+        // The scratch values of boundary j + 1 are those of boundary j in the
+        // next bin, so each is loaded once, one bin ahead of its use.  Scratch
+        // slots of boundaries next to empty bins hold stale values; they are
+        // loaded but only used for occupied bins (or when !safe, where every
+        // boundary was written).
         float mom2 = 0.0f;
-        float bpj = bpS[z], t0j = tau0S[z];
-        float xj = binStart(0) - mu[0];
-        for (int j = 0; j < kBins; ++j)
         {
-            const float bpk = bpS[(size_t)(j + 1) * kLane + z];
-            const float t0k = tau0S[(size_t)(j + 1) * kLane + z];
-            const float xk = binStart(j + 1) - mu[0];
-            float tmp = mul_rn(mul_rn(mul_rn(bpj, xj), xj), t0j);
-            tmp = add_rn(tmp, mul_rn(mul_rn(mul_rn(bpk, xk), xk), t0k));
-            tmp = mul_rn(tmp, facS[(size_t)j * kLane + z]);
-            mom2 = add_rn(mom2, tmp);
-            bpj = bpk; t0j = t0k; xj = xk;
+            float bpj = bpS[z], t0j = tau0S[z];
+            uint32_t nj = (uint32_t)H.bin_count[0][z];
+            for (int j = 0; j < kBins; ++j)
+            {
+                const float bpk = bpS[(size_t)(j + 1) * kLane + z], t0k = tau0S[(size_t)(j + 1) * kLane + z];
+                const float fj = facS[(size_t)j * kLane + z];
+                const uint32_t nk = (j + 1 < kBins) ? (uint32_t)H.bin_count[j + 1][z] : 0u;
+                if (!safe || nj != 0u)      // an empty bin adds +0 (see the E-step)
+                {
+                    const float xj = binStart(j) - mu[0];
+                    const float xk = binStart(j + 1) - mu[0];
+                    float tmp = mul_rn(mul_rn(mul_rn(bpj, xj), xj), t0j);
+                    tmp = add_rn(tmp, mul_rn(mul_rn(mul_rn(bpk, xk), xk), t0k));
+                    tmp = mul_rn(tmp, fj);
+                    mom2 = add_rn(mom2, tmp);
+                }
+                bpj = bpk;
+                t0j = t0k;
+                nj = nk;
+            }
         }
         mom2 = mul_rn(mom2, mul_rn(0.5f, binSize));
         float v0 = add_rn(mom2 / ci[0], varQuant);

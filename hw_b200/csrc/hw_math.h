@@ -93,13 +93,18 @@ HW_HD float scale2(float y, int n)
 }
 
 // Natural exponential, Cephes expf method with fused polynomial steps.
+// Written without branches: the special cases (NaN, overflow above
+// 88.72283935546875, underflow to 0 below -103.97208404541016) are selected
+// after an in-range evaluation, so that several independent calls can be
+// interleaved by the compiler.
 HW_HD float hw_expf(float x)
 {
-    if (x != x) return x;
-    if (x > 88.72283935546875f) return bits_f32(0x7f800000u);
-    if (x < -103.97208404541016f) return 0.0f;
-    const float z = floorf(fma_rn(x, 1.44269504088896341f, 0.5f));
-    float r = fma_rn(z, -0.693359375f, x);
+    const bool isNan = x != x;
+    const bool hi = x > 88.72283935546875f;
+    const bool lo = x < -103.97208404541016f;
+    const float xc = (isNan | hi | lo) ? 0.0f : x;
+    const float z = floorf(fma_rn(xc, 1.44269504088896341f, 0.5f));
+    float r = fma_rn(z, -0.693359375f, xc);
     r = fma_rn(z, 2.12194440e-4f, r);
     float p = 1.9875691500e-4f;
     p = fma_rn(p, r, 1.3981999507e-3f);
@@ -109,35 +114,30 @@ HW_HD float hw_expf(float x)
     p = fma_rn(p, r, 5.0000001201e-1f);
     const float r2 = mul_rn(r, r);
     const float y = add_rn(fma_rn(p, r2, r), 1.0f);
-    return scale2(y, (int)z);
+    float out = scale2(y, (int)z);
+    out = lo ? 0.0f : out;
+    out = hi ? bits_f32(0x7f800000u) : out;
+    return isNan ? x : out;
 }
 
-// Natural logarithm, Cephes logf method with fused polynomial steps.
+// Natural logarithm, Cephes logf method with fused polynomial steps.  Also
+// branch-free: NaN -> NaN, x < 0 -> NaN, +-0 -> -inf, +inf -> +inf are
+// selected after the evaluation; denormals are scaled by 2^32 first.
 HW_HD float hw_logf(float x)
 {
-    if (x != x) return x;
-    if (x < 0.0f) return bits_f32(0x7fc00000u);
-    if (x == 0.0f) return bits_f32(0xff800000u);
+    const bool isNan = x != x;
+    const bool neg = x < 0.0f;
+    const bool zero = x == 0.0f;
     uint32_t u = f32_bits(x);
-    if (u == 0x7f800000u) return x;
-    int e = 0;
-    if (u < 0x00800000u)            // denormal: normalise by 2^32
-    {
-        u = f32_bits(mul_rn(x, 4294967296.0f));
-        e = -32;
-    }
+    const bool isInf = u == 0x7f800000u;
+    const bool den = u < 0x00800000u;            // denormal (or +0): normalise by 2^32
+    u = den ? f32_bits(mul_rn(x, 4294967296.0f)) : u;
     // frexp: x = m * 2^e with m in [0.5, 1)
-    e += (int)((u >> 23) & 0xffu) - 126;
+    int e = (den ? -32 : 0) + (int)((u >> 23) & 0xffu) - 126;
     float m = bits_f32((u & 0x807fffffu) | 0x3f000000u);
-    if (m < 0.707106781186547524f)
-    {
-        e -= 1;
-        m = add_rn(add_rn(m, m), -1.0f);
-    }
-    else
-    {
-        m = add_rn(m, -1.0f);
-    }
+    const bool small = m < 0.707106781186547524f;
+    e -= small ? 1 : 0;
+    m = small ? add_rn(add_rn(m, m), -1.0f) : add_rn(m, -1.0f);
     const float z = mul_rn(m, m);
     float y = 7.0376836292e-2f;
     y = fma_rn(y, m, -1.1514610310e-1f);
@@ -154,7 +154,10 @@ HW_HD float hw_logf(float x)
     y = fma_rn(z, -0.5f, y);
     float r = add_rn(m, y);
     r = fma_rn(fe, 0.693359375f, r);
-    return r;
+    r = isInf ? x : r;
+    r = zero ? bits_f32(0xff800000u) : r;
+    r = neg ? bits_f32(0x7fc00000u) : r;
+    return isNan ? x : r;
 }
 
 // x86 cvtps2dq under round-to-nearest-even.

@@ -14,6 +14,7 @@
 #include <string>
 
 #include "../../include/hw_b200.h"
+#include "hw_math.h"
 
 namespace hwp {
 
@@ -412,7 +413,40 @@ inline bool Validate(const hw_config& c, std::string* err)
     { *err = "roi filter type out of range"; return false; }
     if (c.model_estimation_mode < 0 || c.model_estimation_mode > 2)
     { *err = "model estimation mode out of range"; return false; }
+    if (c.model_estimation_mode == HW_FIXED_ESTIMATIONS && !(c.static_baseline_variance >= 0.0f))
+    { *err = "StaticDetModelConfig baselineVariance must be non-negative"; return false; }
     return true;
+}
+
+// The fixed detection model of FixedModelBatchAnalyzer (analyzer/
+// BatchAnalyzer.cpp:119-144) with StaticDetModelConfig::SetupAnalogs
+// (dataTypes/configs/StaticDetModelConfig.h:53-68): baseline mean/variance
+// from the config, analog a at mean = blMean + relAmp[a] * refSnr * sqrt(blVar)
+// and variance blVar + mean + (cv[a] * mean)^2, stored as fp16 in every ZMW.
+// Weights and confidence are 0: the labeler and the pulse accumulator read
+// only means and variances.
+inline void StaticModel(const hw_config& c, hw_lane_model* m)
+{
+    std::memset(m, 0, sizeof(*m));
+    const float blMean = c.static_baseline_mean;
+    const float blVar = c.static_baseline_variance;
+    const float refSignal = c.ref_snr * std::sqrt(blVar);
+    for (int z = 0; z < kLane; ++z)
+    {
+        m->baseline.means[z] = hwm::f32_to_f16_bits(blMean);
+        m->baseline.vars[z] = hwm::f32_to_f16_bits(blVar);
+    }
+    for (int a = 0; a < kAnalogs; ++a)
+    {
+        const float mean = blMean + c.analogs[a].rel_amplitude * refSignal;
+        const float cm = c.analogs[a].excess_noise_cv * mean;
+        const float var = (blVar + mean) + cm * cm;
+        for (int z = 0; z < kLane; ++z)
+        {
+            m->analogs[a].means[z] = hwm::f32_to_f16_bits(mean);
+            m->analogs[a].vars[z] = hwm::f32_to_f16_bits(var);
+        }
+    }
 }
 
 }   // namespace hwp

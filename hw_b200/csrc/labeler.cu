@@ -219,13 +219,16 @@ __global__ void __launch_bounds__(128) LabelerKernel(LabelerArgs A, KParams k)
             p0 = p1; p1 = p2; p2 = sn;
         };
         for (int i = hwp::kRoiLookForward; i < kLatent; ++i) process(mul_rn((float)pl[(size_t)i * kLane], inv1));
-        for (int i0 = 0; i0 < F; i0 += kBatch)
         {
-            int16_t x[kBatch];
-#pragma unroll
-            for (int j = 0; j < kBatch; ++j) x[j] = __ldg(chunk + (size_t)(i0 + j) * kLane);
-#pragma unroll
-            for (int j = 0; j < kBatch; ++j) process(mul_rn((float)x[j], inv2));
+            int16_t y0 = __ldg(chunk), y1 = __ldg(chunk + kLane);
+#pragma unroll 2
+            for (int i = 0; i < F; ++i)
+            {
+                const int16_t y = y0;
+                y0 = y1;
+                if (i + 2 < F) y1 = __ldg(chunk + (size_t)(i + 2) * kLane);
+                process(mul_rn((float)y, inv2));
+            }
         }
         if (ri & 15) roiw[ri >> 4] = word;
         // Backward recursion: 2-bit codes become 0/1 (in place, bit 0 of each code).
@@ -267,26 +270,27 @@ __global__ void __launch_bounds__(128) LabelerKernel(LabelerArgs A, KParams k)
     sc.Setup(k, newM, z);
     const int anchor = F - kLatent;
     float anchorLL[kStates];
-    // Chunk frames 0 .. anchor + 15 (labels kLatent .. F + 15).  F is a multiple
-    // of 8 and kLatent = 24, so the batches never straddle the anchor.
-    for (int f0 = 0; f0 < anchor + kLookback; f0 += kBatch)
+    // Chunk frames 0 .. anchor + 15 (labels kLatent .. F + 15).  The loop
+    // stays rolled (one Viterbi step is several hundred instructions; copies
+    // of it overflow the instruction cache) and the trace is loaded two
+    // frames ahead of use.
+    const int nFrames = anchor + kLookback;
+    int16_t x0 = __ldg(chunk), x1 = __ldg(chunk + kLane);
+#pragma unroll 1
+    for (int f = 0; f < nFrames; ++f)
     {
-        int16_t x[kBatch];
-#pragma unroll
-        for (int j = 0; j < kBatch; ++j) x[j] = __ldg(chunk + (size_t)(f0 + j) * kLane);
-        if (f0 == anchor)
+        const int16_t x = x0;
+        x0 = x1;
+        if (f + 2 < nFrames) x1 = __ldg(chunk + (size_t)(f + 2) * kLane);
+        if (f == anchor)
         {
 #pragma unroll
             for (int i = 0; i < kStates; ++i) anchorLL[i] = ll[i];
         }
-#pragma unroll
-        for (int j = 0; j < kBatch; ++j)
-        {
-            const int lf = f0 + j + kLatent;
-            if ((lf & 15) == 0) roiWord = roiw[lf >> 4];
-            const bool isRoi = (roiWord >> (2 * (lf & 15))) & 1u;
-            tb[(size_t)lf * kLane] = ViterbiStep(k, sc, (float)x[j], isRoi, ll);
-        }
+        const int lf = f + kLatent;
+        if ((lf & 15) == 0) roiWord = roiw[lf >> 4];
+        const bool isRoi = (roiWord >> (2 * (lf & 15))) & 1u;
+        tb[(size_t)lf * kLane] = ViterbiStep(k, sc, (float)x, isRoi, ll);
     }
 
     // Normalize (FrameLabelerHost.cpp:186-205) and back-propagation.

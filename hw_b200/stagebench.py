@@ -12,7 +12,7 @@ import json
 
 import torch
 
-from . import filters as Fl, workloads
+from . import abi, filters as Fl, workloads
 
 
 def main():
@@ -34,10 +34,18 @@ def main():
         emitted += int(em)
     torch.cuda.synchronize()
     times = an.stage_times()
-    print(json.dumps({"lanes": a.lanes, "chunks": a.chunks, "emitted_chunks": emitted,
-                      "pulses_last_chunk": int(lens.sum().item()),
-                      "stage_ms_total": {k: v[0] for k, v in times.items()},
-                      "stage_launches": {k: v[1] for k, v in times.items()}}))
+    out = {"lanes": a.lanes, "chunks": a.chunks, "emitted_chunks": emitted,
+           "pulses_last_chunk": int(lens.sum().item()),
+           "stage_ms_total": {k: v[0] for k, v in times.items()},
+           "stage_launches": {k: v[1] for k, v in times.items()}}
+    diag = an.last_diag()
+    if diag is not None:
+        d = Fl.struct_to_numpy(diag, abi.DME_DIAG_DT)
+        it = d["lane_iterations"].astype(float)
+        out["dme_lane_iterations"] = {"mean": float(it.mean()), "max": int(it.max()),
+                                      "hist": [int((d["lane_iterations"] == i).sum()) for i in range(21)]}
+        out["dme_converged_fraction"] = float(d["converged"].mean())
+    print(json.dumps(out))
 
 
 if __name__ == "__main__":

@@ -1678,6 +1678,13 @@ int or_pulses(void* p, const int16_t* labels, const int16_t* lat, const int16_t*
               const hw_lane_model* m, hw_pulse* pulses, uint32_t* lens, uint32_t* ovf, hw_stat_accum_state* bs)
 { return static_cast<OraclePool*>(p)->Pulses(labels, lat, tr, firstFrame, m, pulses, lens, ovf, bs); }
 
+// The fixed detection model of FixedModelBatchAnalyzer, one lane.
+int or_static_model(const hw_config* c, hw_lane_model* out)
+{
+    hwp::StaticModel(*c, out);
+    return HW_OK;
+}
+
 // One BlockFilterStage (TraceFilters.cpp:11-57 on a WindowBuffer that starts
 // with `width` zeros) with stride 1 over `chunks` consecutive blocks of F
 // frames of one lane: in/out[chunks][F][64].  Pins the window semantics

@@ -51,6 +51,7 @@ def lib():
         L.or_dme_estimate.argtypes = [vp, vp, vp, FI, FI, vp, vp]
         L.or_label.argtypes = [vp, vp, vp, vp, vp, vp]
         L.or_pulses.argtypes = [vp, vp, vp, vp, i32, vp, vp, vp, vp, vp]
+        L.or_static_model.argtypes = [C.POINTER(abi.Config), vp]
         L.or_extremum_stage.argtypes = [C.c_int, C.c_int, vp, C.c_int, C.c_int, vp]
         L.or_expf.argtypes = [C.c_float]
         L.or_expf.restype = C.c_float
@@ -189,3 +190,10 @@ def extremum_stage(width, is_max, blocks):
     _check(lib().or_extremum_stage(int(width), int(bool(is_max)), abi.ptr(blocks), blocks.shape[1],
                                    blocks.shape[0], abi.ptr(out)))
     return out
+
+
+def static_model(cfg, lanes):
+    """The FixedModelBatchAnalyzer detection model for `lanes` lanes."""
+    one = np.zeros(1, abi.LANE_MODEL_DT)
+    _check(lib().or_static_model(C.byref(cfg), abi.ptr(one)))
+    return np.repeat(one, lanes)

@@ -123,7 +123,8 @@ class GpuBackend:
 
 
 class Pipeline:
-    """One pool's analyzer over a backend (SingleEstimate or DynamicEstimate)."""
+    """One pool's analyzer over a backend (FixedModel, SingleEstimate or
+    DynamicEstimate)."""
 
     HIST_INIT, DME_INIT, SEQUENCING = 0, 1, 2
 
@@ -190,7 +191,13 @@ class Pipeline:
         rec["bls"], rec["stats"] = bls, stats
         fi = (ff, ff + self.F)
         mode = self.cfg.model_estimation_mode
-        if mode == abi.INITIAL_ESTIMATIONS:
+        if mode == abi.FIXED_ESTIMATIONS:
+            # FixedModelBatchAnalyzer::AnalyzeImpl (BatchAnalyzer.cpp:172-207)
+            if self.models is None:
+                import oracle
+                self.models = oracle.static_model(self.cfg, self.b.lanes)
+            self._label_and_pulse(bls, ff, rec)
+        elif mode == abi.INITIAL_ESTIMATIONS:
             if not self.initialized and ff > self.bl_latency:
                 self.initialized = self._dme_add(bls, stats, fi, rec)
             if self.initialized:

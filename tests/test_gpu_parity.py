@@ -168,6 +168,48 @@ def test_native_analyzer_matches_stagewise_pipeline():
         assert estimated == ("models" in r)
 
 
+def _fixed_config():
+    cfg = workloads.small_config()
+    cfg.model_estimation_mode = abi.FIXED_ESTIMATIONS
+    cfg.static_baseline_mean = 0.0
+    cfg.static_baseline_variance = 64.0      # the synthetic baseline sigma is 8 DN
+    return cfg
+
+
+def test_fixed_model_bit_exact():
+    """FixedModelBatchAnalyzer schedule: label and pulse every chunk with the
+    static model (BatchAnalyzer.cpp:119-207)."""
+    cfg = _fixed_config()
+    tr = synth.traces(2, 512 * 4, seed=17)
+    stages = _lockstep(cfg, tr, 512)
+    assert "pulses" in stages and "models" not in stages
+
+
+def test_native_fixed_analyzer_matches_stagewise_pipeline():
+    import torch
+    from hw_b200 import filters as Fl
+    cfg = _fixed_config()
+    lanes, F, C = 2, 512, 4
+    tr = synth.traces(lanes, F * C, seed=23)
+    ref = harness.Pipeline(harness.GpuBackend(cfg, lanes, F), cfg)
+    an = Fl.BatchAnalyzer(cfg, 0, lanes, F)
+    for c in range(C):
+        chunk = np.ascontiguousarray(tr[:, c * F:(c + 1) * F])
+        r = ref.process(chunk, c * F)
+        pulses, lens, ovf, emitted, estimated = an(torch.from_numpy(chunk).cuda(), c * F)
+        assert emitted and not estimated
+        pr, lr, _, _ = r["pulses"]
+        lens = lens.cpu().numpy()
+        assert np.array_equal(lr, lens.astype(np.uint32))
+        pg = Fl.struct_to_numpy(pulses, abi.PULSE_DT).reshape(lanes, 64, cfg.max_calls_per_zmw)
+        for l in range(lanes):
+            for z in range(64):
+                assert np.array_equal(pr[l, z, :lr[l, z]].view(np.uint8), pg[l, z, :lens[l, z]].view(np.uint8))
+    m, _ = an.models()
+    assert np.array_equal(Fl.struct_to_numpy(m, abi.LANE_MODEL_DT).view(np.uint8),
+                          ref.models.view(np.uint8))
+
+
 def test_analyzer_rejects_out_of_order_chunks():
     import torch
     from hw_b200 import filters as Fl

@@ -456,3 +456,25 @@ def test_dme_em_snr_sweep(sim_snr):
         assert (np.abs(r_mean - cd_mean) <= tol_m).all(), (m, r_mean[0], cd_mean, tol_m)
         tol_v = 5 * np.sqrt(2.0 / (total * w - 1)) * cd_var
         assert (np.abs(r_var - cd_var) <= tol_v).all(), (m, r_var[0], cd_var, tol_v)
+
+
+def test_static_model_restates_setup_analogs():
+    """FixedModelBatchAnalyzer's model (BatchAnalyzer.cpp:119-144) from
+    StaticDetModelConfig::SetupAnalogs (StaticDetModelConfig.h:53-68), in float
+    arithmetic and stored as fp16."""
+    cfg = workloads.small_config()
+    cfg.static_baseline_mean = 3.0
+    cfg.static_baseline_variance = 33.0
+    m = oracle.static_model(cfg, 2)
+    f32 = np.float32
+    bl_mean, bl_var = f32(3.0), f32(33.0)
+    ref_signal = f32(f32(cfg.ref_snr) * np.sqrt(bl_var, dtype=np.float32))
+    assert (m["baseline"]["means"] == abi.f32_to_f16(bl_mean)).all()
+    assert (m["baseline"]["vars"] == abi.f32_to_f16(bl_var)).all()
+    for a in range(4):
+        mean = f32(bl_mean + f32(f32(cfg.analogs[a].rel_amplitude) * ref_signal))
+        cm = f32(f32(cfg.analogs[a].excess_noise_cv) * mean)
+        var = f32(f32(bl_var + mean) + f32(cm * cm))
+        assert (m["analogs"][:, a]["means"] == abi.f32_to_f16(mean)).all()
+        assert (m["analogs"][:, a]["vars"] == abi.f32_to_f16(var)).all()
+    assert not m["confidence"].any() and not m["analogs"]["weights"].any()
