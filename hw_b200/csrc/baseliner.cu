@@ -86,7 +86,7 @@ template <int FT> struct FLayout
 // extremum P of the current block and the current block's inputs B; the
 // output at block position c is op(S[c], P).  `base` points at S[0] of this
 // thread and `stride` separates consecutive array elements.
-template <int W, bool IsMax>
+template <int W, bool IsMax, bool Batched>
 __device__ __forceinline__ int16_t StageStep(int16_t* base, int stride, int16_t& P, int16_t& counter, int16_t x)
 {
     auto op = [](int16_t a, int16_t b) -> int16_t {
@@ -100,13 +100,27 @@ __device__ __forceinline__ int16_t StageStep(int16_t* base, int stride, int16_t&
     P = op(P, x);
     if (c + 1 == W)
     {
+        // New suffix extrema of the completed block.  For windows in global
+        // memory the inputs are read in batches of 4 before the batch's results
+        // are stored, so the loads overlap instead of each waiting behind the
+        // previous store.
         int16_t acc = x;
         S[(W - 1) * stride] = acc;
-#pragma unroll 4
-        for (int j = W - 2; j >= 0; --j)
+        constexpr int kBatch = Batched ? 4 : 1;
+#pragma unroll 1
+        for (int j0 = W - 2; j0 >= 0; j0 -= kBatch)
         {
-            acc = op(B[j * stride], acc);
-            S[j * stride] = acc;
+            int16_t b[kBatch];
+#pragma unroll
+            for (int q = 0; q < kBatch; ++q)
+                if (j0 - q >= 0) b[q] = B[(j0 - q) * stride];
+#pragma unroll
+            for (int q = 0; q < kBatch; ++q)
+                if (j0 - q >= 0)
+                {
+                    acc = op(b[q], acc);
+                    S[(j0 - q) * stride] = acc;
+                }
         }
         P = IsMax ? (int16_t)-32768 : (int16_t)32767;
         counter = 0;
@@ -134,9 +148,9 @@ __device__ __forceinline__ int16_t Stage(const StageMem& m, int16_t* pc, int16_t
     constexpr int off = Lay::Offset(Upper, K);
     constexpr int i = Lay::Idx(Upper, K);
     if constexpr (Lay::InSmem(K))
-        return StageStep<W, Lay::IsMax(Upper, K)>(m.smem + off * m.sstride, m.sstride, pc[2 * i], pc[2 * i + 1], x);
+        return StageStep<W, Lay::IsMax(Upper, K), false>(m.smem + off * m.sstride, m.sstride, pc[2 * i], pc[2 * i + 1], x);
     else
-        return StageStep<W, Lay::IsMax(Upper, K)>(m.gmem + (size_t)off * m.gstride, m.gstride, pc[2 * i], pc[2 * i + 1], x);
+        return StageStep<W, Lay::IsMax(Upper, K), true>(m.gmem + (size_t)off * m.gstride, m.gstride, pc[2 * i], pc[2 * i + 1], x);
 }
 
 template <int FT, bool Upper, int Scale>

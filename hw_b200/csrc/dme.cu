@@ -131,7 +131,7 @@ __device__ __forceinline__ float StatVarianceD(const hw_stat_accum_state& s, int
 }
 
 
-__global__ void __launch_bounds__(kLane, 8) DmeEstimateKernel(DmeArgs A, KParams k)
+__global__ void __launch_bounds__(kLane, 12) DmeEstimateKernel(DmeArgs A, KParams k)
 {
     const int l = blockIdx.x;
     const int z = threadIdx.x;
@@ -254,9 +254,18 @@ __global__ void __launch_bounds__(kLane, 8) DmeEstimateKernel(DmeArgs A, KParams
         work.av[a] = SignalCovar(k, k.cv2[a], work.am[a], work.bv);
     }
 
+    // Values needed only before and after the EM iterations (the prior model
+    // and the estimates at the latest converged iteration) wait in per-thread
+    // shared-memory columns, which keeps them out of registers in the loop.
+    __shared__ float shDet[16][kLane];
+    __shared__ float shEst[15][kLane];
+    auto rhoEst = [&](int i) -> float& { return shEst[i][z]; };
+    auto muEst = [&](int i) -> float& { return shEst[5 + i][z]; };
+    auto varEst = [&](int i) -> float& { return shEst[10 + i][z]; };
+
     // EM setup (DmeEmHost.cpp:253-361)
     const float rhoMin = 0.001f;
-    float rho[5], mu[5], var[5], rhoEst[5], muEst[5], varEst[5];
+    float rho[5], mu[5], var[5];
     rho[0] = fmax_sse(work.bw, rhoMin); mu[0] = work.bm; var[0] = work.bv;
     for (int a = 0; a < kAnalogs; ++a)
     {
@@ -271,7 +280,7 @@ __global__ void __launch_bounds__(kLane, 8) DmeEstimateKernel(DmeArgs A, KParams
         const float rs = (rho[0] + rho[1]) + (rho[2] + (rho[3] + rho[4]));
         for (int i = 0; i < 5; ++i) rho[i] = rho[i] / rs;
     }
-    for (int i = 0; i < 5; ++i) { rhoEst[i] = rho[i]; muEst[i] = mu[i]; varEst[i] = var[i]; }
+    for (int i = 0; i < 5; ++i) { rhoEst(i) = rho[i]; muEst(i) = mu[i]; varEst(i) = var[i]; }
     float s;
     {
         const float p0 = mul_rn(mu[1], k.relAmp[0]), p1 = mul_rn(mu[2], k.relAmp[1]);
@@ -280,6 +289,14 @@ __global__ void __launch_bounds__(kLane, 8) DmeEstimateKernel(DmeArgs A, KParams
     }
     const float sExpect = s / scaleFactor;
     const float sExpectW = mul_rn(det.conf, k.pulseAmpReg);
+    {
+        shDet[0][z] = det.bw; shDet[1][z] = det.bm; shDet[2][z] = det.bv; shDet[3][z] = det.conf;
+#pragma unroll
+        for (int a = 0; a < kAnalogs; ++a)
+        {
+            shDet[4 + a][z] = det.aw[a]; shDet[8 + a][z] = det.am[a]; shDet[12 + a][z] = det.av[a];
+        }
+    }
     float logLike = -3.40282347e+38f;
     const float binProbMin = mul_rn(fmax_sse(mul_rn((float)total, binSize), 1.0f), 1.17549435e-38f);
     int zStatus = (total < 160u) ? 2 : 0;
@@ -419,7 +436,7 @@ __global__ void __launch_bounds__(kLane, 8) DmeEstimateKernel(DmeArgs A, KParams
         if (cv)
         {
 #pragma unroll
-            for (int i = 0; i < 5; ++i) { rhoEst[i] = rho[i]; muEst[i] = mu[i]; varEst[i] = var[i]; }
+            for (int i = 0; i < 5; ++i) { rhoEst(i) = rho[i]; muEst(i) = mu[i]; varEst(i) = var[i]; }
         }
         const int allDone = __syncthreads_and(mConverged | (zStatus != 0));
         if (!k.iterToLimit && allDone) break;
@@ -494,10 +511,18 @@ __global__ void __launch_bounds__(kLane, 8) DmeEstimateKernel(DmeArgs A, KParams
     if (!mConverged) zStatus |= 1;
     bool finite = true;
 #pragma unroll
-    for (int i = 0; i < 5; ++i) finite &= isfinite(rhoEst[i]) & isfinite(muEst[i]) & isfinite(varEst[i]);
-    work.bw = rhoEst[0]; work.bm = muEst[0]; work.bv = varEst[0];
+    for (int i = 0; i < 5; ++i) finite &= isfinite(rhoEst(i)) & isfinite(muEst(i)) & isfinite(varEst(i));
+    work.bw = rhoEst(0); work.bm = muEst(0); work.bv = varEst(0);
 #pragma unroll
-    for (int a = 0; a < kAnalogs; ++a) { work.aw[a] = rhoEst[a + 1]; work.am[a] = muEst[a + 1]; work.av[a] = varEst[a + 1]; }
+    for (int a = 0; a < kAnalogs; ++a) { work.aw[a] = rhoEst(a + 1); work.am[a] = muEst(a + 1); work.av[a] = varEst(a + 1); }
+    {
+        det.bw = shDet[0][z]; det.bm = shDet[1][z]; det.bv = shDet[2][z]; det.conf = shDet[3][z];
+#pragma unroll
+        for (int a = 0; a < kAnalogs; ++a)
+        {
+            det.aw[a] = shDet[4 + a][z]; det.am[a] = shDet[8 + a][z]; det.av[a] = shDet[12 + a][z];
+        }
+    }
     if (!finite) atomicCAS(A.err, 0, HW_ERR_NUMERIC);
 
     // ComputeConfidence (DmeEmHost.cpp:717-803), G-test disabled (pValue 1)
