@@ -339,7 +339,8 @@ def main():
                 "alg_bytes_per_launch": lab_bytes_launch,
                 "peak_source": "measured" if peaks else "fallback"}
         if prof and "issue_frac" in prof:
-            roof["issue_roofline"] = {"frac": prof["issue_frac"], "source": "ncu sm__inst_executed"}
+            roof["issue_roofline"] = {"frac": prof["issue_frac"],
+                                      "source": "ncu smsp__issue_active of the labeler, small case"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
