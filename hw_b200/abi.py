@@ -27,6 +27,7 @@ FILTER_TYPES = {
     "TwoScaleLarge": 3, "TwoScaleMedium": 4, "TwoScaleSmall": 5,
 }
 FIXED_ESTIMATIONS, INITIAL_ESTIMATIONS, DYNAMIC_ESTIMATIONS = 0, 1, 2
+EM_START_PLAIN, EM_START_PROPOSAL, EM_START_BETTER = 0, 1, 2
 
 
 class Analog(C.Structure):

@@ -131,25 +131,80 @@ __device__ __forceinline__ float StatVarianceD(const hw_stat_accum_state& s, int
 }
 
 
-__global__ void __launch_bounds__(kLane, 12) DmeEstimateKernel(DmeArgs A, KParams k)
+// Histogram geometry and totals of one ZMW (UHistogramSimd arithmetic in
+// uint16 where the reference keeps counts in uint16).
+struct EmHist
 {
-    const int l = blockIdx.x;
-    const int z = threadIdx.x;
-    const hw_lane_histogram& H = A.hist[l];
-    const hw_baseliner_stats& BS = A.stats[l];
-    float* bpS = A.scratch + (size_t)l * 3 * (kBins + 1) * kLane;
-    float* tau0S = bpS + (size_t)(kBins + 1) * kLane;
-    float* facS = tau0S + (size_t)(kBins + 1) * kLane;
+    const hw_lane_histogram* H;
+    int z;
+    float lb, binSize, varQuant, binProbMin, nSum;
+    uint16_t inRange, nLowOut, total;
+    __device__ __forceinline__ float BinStart(int b) const { return add_rn(lb, mul_rn((float)b, binSize)); }
+    __device__ __forceinline__ uint32_t Count(int b) const { return H->bin_count[b][z]; }
+};
 
-    ModelF det;
-    LoadModel(A.models[l], z, det);
+__device__ __forceinline__ void LoadEmHist(const hw_lane_histogram& H, int z, EmHist& h)
+{
+    h.H = &H;
+    h.z = z;
+    uint16_t inRange = 0;
+    float nSum = 0.0f;
+    for (int b = 0; b < kBins; ++b)
+    {
+        const uint16_t c = H.bin_count[b][z];
+        inRange = (uint16_t)(inRange + c);
+        nSum += (float)c;
+    }
+    h.inRange = inRange;
+    h.nSum = nSum;
+    h.nLowOut = H.outlier_count_low[z];
+    h.total = (uint16_t)(inRange + (uint16_t)(h.nLowOut + H.outlier_count_high[z]));
+    h.lb = H.low_bound[z];
+    h.binSize = H.bin_size[z];
+    h.varQuant = mul_rn(h.binSize, h.binSize) / 12.0f;
+    h.binProbMin = mul_rn(fmax_sse(mul_rn((float)h.total, h.binSize), 1.0f), 1.17549435e-38f);
+}
+
+// The EM's free parameters (DmeEmHost.cpp:253-361): mixture fractions, means
+// and variances of the baseline and the four analog modes, and the analog
+// amplitude scale s (analog means are s * relAmp).
+struct EmVars
+{
+    float rho[5], mu[5], var[5];
+    float s;
+};
+
+// Regularisation of s toward the preliminary estimate.
+struct EmReg
+{
+    float sExpect, sExpectW;
+};
+
+// s of the EM set-up: the relative-amplitude projection of the analog means.
+__device__ __forceinline__ float EmScale(const KParams& k, const float mu[5])
+{
+    const float p0 = mul_rn(mu[1], k.relAmp[0]), p1 = mul_rn(mu[2], k.relAmp[1]);
+    const float p2 = mul_rn(mu[3], k.relAmp[2]), p3 = mul_rn(mu[4], k.relAmp[3]);
+    return ((p0 + p1) + (p2 + p3)) / k.rpaSum2;
+}
+
+// Everything the reference does before its EM iterations: EvolveModel,
+// PrelimEstimate and its confidence-weighted update, PrelimScaleFactor,
+// ScaleModelSnr and the EM set-up (DmeEmHost.cpp:161-361, 620-654, 806-852).
+// Leaves the updated prior model in `det` and the EM start in `v`.
+__device__ __forceinline__ void DmePrelude(const KParams& k, const hw_lane_model& M, const hw_baseliner_stats& BS,
+                                           const EmHist& h, int tModel, int tEst, ModelF& det, EmVars& v, EmReg& r)
+{
+    const int z = h.z;
+    const hw_lane_histogram& H = *h.H;
+    LoadModel(M, z, det);
 
     // EvolveModel (DmeEmHost.cpp:806-834) + EvolveConfidence (DetectionModelHost.h:166-177)
     {
-        const float thl = mul_rn(0.5f, (float)(A.tModel + A.tEst));
+        const float thl = mul_rn(0.5f, (float)(tModel + tEst));
         const float t0 = 56160.0f, t1 = 168480.0f;
         const float hl = add_rn(k.halfLife0, mul_rn(k.halfLife1 - k.halfLife0, satlin_std(t0, t1, thl)));
-        const float tDiff = static_cast<float>(A.tEst - A.tModel);
+        const float tDiff = static_cast<float>(tEst - tModel);
         det.conf = mul_rn(det.conf, exp2_d(-fabsf(tDiff) / hl));
     }
 
@@ -181,13 +236,8 @@ __global__ void __launch_bounds__(kLane, 12) DmeEstimateKernel(DmeArgs A, KParam
     ModelUpdate(k, det, work);
     work = det;
 
-    // Histogram totals (uint16 arithmetic as in UHistogramSimd)
-    uint16_t inRange = 0;
-    for (int b = 0; b < kBins; ++b) inRange = (uint16_t)(inRange + H.bin_count[b][z]);
-    const uint16_t nLowOut = H.outlier_count_low[z];
-    const uint16_t total = (uint16_t)(inRange + (uint16_t)(nLowOut + H.outlier_count_high[z]));
-    const float lb = H.low_bound[z], binSize = H.bin_size[z];
-    auto binStart = [&](int b) { return add_rn(lb, mul_rn((float)b, binSize)); };
+    const float lb = h.lb, binSize = h.binSize;
+    const uint16_t nLowOut = h.nLowOut, inRange = h.inRange, total = h.total;
 
     // PrelimScaleFactor (DmeEmHost.cpp:620-654)
     float scaleFactor;
@@ -198,12 +248,12 @@ __global__ void __launch_bounds__(kLane, 12) DmeEstimateKernel(DmeArgs A, KParam
         float bgCount;
         {
             const float x = thresh;
-            const float ub = binStart(kBins);
+            const float ub = h.BinStart(kBins);
             const bool mNan = isnan(x), mLow = x < lb, mHigh = x >= ub;
             const bool inB = !(mNan | mLow | mHigh);
             int xbin = floor_cast_i32((x - lb) / binSize);
             xbin = inB ? xbin : 0;
-            const float xrem = x - binStart(xbin);
+            const float xrem = x - h.BinStart(xbin);
             const float xbinCount = (float)(xbin < kBins ? H.bin_count[xbin][z] : (uint16_t)0);
             float cc = (float)nLowOut;
             uint16_t cn = 0;
@@ -236,7 +286,7 @@ __global__ void __launch_bounds__(kLane, 12) DmeEstimateKernel(DmeArgs A, KParam
                 else
                 {
                     i -= 1;
-                    const float x0 = binStart(i);
+                    const float x0 = h.BinStart(i);
                     const uint16_t niz = H.bin_count[i][z];
                     const int m = (int)n - (int)niz;
                     frv = add_rn(x0, mul_rn(binSize, nfz - (float)m) / (float)(niz + 1));
@@ -254,6 +304,241 @@ __global__ void __launch_bounds__(kLane, 12) DmeEstimateKernel(DmeArgs A, KParam
         work.av[a] = SignalCovar(k, k.cv2[a], work.am[a], work.bv);
     }
 
+    // EM setup (DmeEmHost.cpp:253-361)
+    const float rhoMin = 0.001f;
+    v.rho[0] = fmax_sse(work.bw, rhoMin); v.mu[0] = work.bm; v.var[0] = work.bv;
+    for (int a = 0; a < kAnalogs; ++a)
+    {
+        v.rho[a + 1] = fmax_sse(work.aw[a], rhoMin);
+        v.mu[a + 1] = work.am[a];
+        v.var[a + 1] = work.av[a];
+    }
+    for (int i = 0; i < 5; ++i) v.var[i] += h.varQuant;
+    v.var[0] = fmin_sse(v.var[0], k.blVarMax);
+    {
+        const float rs = (v.rho[0] + v.rho[1]) + (v.rho[2] + (v.rho[3] + v.rho[4]));
+        for (int i = 0; i < 5; ++i) v.rho[i] = v.rho[i] / rs;
+    }
+    v.s = EmScale(k, v.mu);
+    r.sExpect = v.s / scaleFactor;
+    r.sExpectW = mul_rn(det.conf, k.pulseAmpReg);
+}
+
+// One E-step over the 301 bin boundaries and 300 bins (DmeEmHost.cpp:363-492):
+// returns the log-likelihood, fills the mode totals ci, first moments mom1 and
+// inverse variances, and writes what the background-variance M-step needs to
+// the lane's scratch.
+//
+// Only bins with a count contribute to c_i, mom1, wps and (in the M-step)
+// mom2: an empty bin adds (finite) x 0 = +-0 to sums that start at +0 and
+// therefore never hold -0, which leaves them unchanged.  So the
+// responsibilities (5 exps), log(binProb) and n_j / binProb are only
+// evaluated next to occupied bins; the boundary density, which every bin
+// probability needs, is always evaluated.  The shortcut needs every boundary
+// density finite: llb <= max(pref) + log(5), so finite prefactors, means and
+// inverse variances with max(pref) < 80 guarantee it (`safe`).  Otherwise the
+// reference path runs.
+__device__ __forceinline__ float EmEStep(const KParams& k, const EmHist& h, const EmVars& v, const EmReg& r,
+                                         float* bpS, float* tau0S, float* facS, float ci[5], float mom1[5],
+                                         float varinv[5], bool& safeOut)
+{
+    const int z = h.z;
+    const float halfLog2pi = mul_rn(0.5f, k.logTwoPi);
+    float pref[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+    {
+        varinv[i] = 1.0f / v.var[i];
+        pref[i] = (hw_logf(v.rho[i]) - mul_rn(0.5f, hw_logf(v.var[i]))) - halfLog2pi;
+    }
+    float probSum = 0.0f, wps = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 5; ++i) { ci[i] = 0.0f; mom1[i] = 0.0f; }
+    bool safe = true;
+    {
+        float pmax = pref[0];
+#pragma unroll
+        for (int i = 0; i < 5; ++i)
+        {
+            safe &= isfinite(pref[i]) & isfinite(v.mu[i]) & isfinite(varinv[i]);
+            pmax = fmaxf(pmax, pref[i]);
+        }
+        safe &= pmax < 80.0f;
+    }
+    float tauPrev[5] = {0, 0, 0, 0, 0}, bpPrev = 0.0f, xPrev = 0.0f;
+    uint32_t nPrev = 0;
+    // bin counts are loaded one boundary ahead of their use
+    uint32_t nNext = h.Count(0);
+    for (int b = 0; b <= kBins; ++b)
+    {
+        // cornerComp(b)
+        const float x = h.BinStart(b);
+        float t[5];
+#pragma unroll
+        for (int i = 0; i < 5; ++i)
+        {
+            const float y = x - v.mu[i];
+            t[i] = pref[i] - mul_rn(mul_rn(mul_rn(0.5f, y), y), varinv[i]);
+        }
+        float tmax = t[0];
+#pragma unroll
+        for (int i = 1; i < 5; ++i) tmax = fmax_sse(tmax, t[i]);
+        const uint32_t nCur = nNext;
+        nNext = (b + 1 < kBins) ? h.Count(b + 1) : 0u;
+        const bool needTau = (nPrev != 0u) | (nCur != 0u) | !safe;
+        // Far tails: with every t finite and below -106, llb = tmax +
+        // log(se) with 1 <= se <= 5 stays below -104.3, where hw_expf
+        // returns exactly 0, so bp is 0 without evaluating it.
+        bool allFinite = true;
+#pragma unroll
+        for (int i = 0; i < 5; ++i) allFinite &= isfinite(t[i]);
+        const bool tail = !needTau & allFinite & (tmax < -106.0f);
+        float bp = 0.0f, llb = 0.0f;
+        if (!tail)
+        {
+            float se = hw_expf(t[0] - tmax);
+#pragma unroll
+            for (int i = 1; i < 5; ++i) se = add_rn(se, hw_expf(t[i] - tmax));
+            llb = add_rn(tmax, hw_logf(se));
+            bp = hw_expf(llb);
+        }
+        float tau[5];
+        if (needTau)
+        {
+#pragma unroll
+            for (int i = 0; i < 5; ++i) tau[i] = hw_expf(t[i] - llb);
+            bpS[(size_t)b * kLane + z] = bp;
+            tau0S[(size_t)b * kLane + z] = tau[0];
+        }
+        else
+        {
+#pragma unroll
+            for (int i = 0; i < 5; ++i) tau[i] = 0.0f;
+        }
+        if (b > 0)
+        {
+            // centerComp(b - 1)
+            const int c = b - 1;
+            const float bpr = fmax_sse(mul_rn(mul_rn(0.5f, h.binSize), add_rn(bpPrev, bp)), h.binProbMin);
+            probSum = add_rn(probSum, bpr);
+            if ((nPrev != 0u) | !safe)
+            {
+                const float njb = (float)nPrev;
+                wps = add_rn(wps, mul_rn(njb, hw_logf(bpr)));
+                const float factor = njb / bpr;
+                facS[(size_t)c * kLane + z] = factor;
+#pragma unroll
+                for (int m = 0; m < 5; ++m)
+                {
+                    const float tmp1 = mul_rn(bpPrev, tauPrev[m]);
+                    const float tmp2 = mul_rn(bp, tau[m]);
+                    ci[m] = add_rn(ci[m], mul_rn(add_rn(tmp1, tmp2), factor));
+                    mom1[m] = add_rn(mom1[m], mul_rn(add_rn(mul_rn(tmp1, xPrev), mul_rn(tmp2, x)), factor));
+                }
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 5; ++i) tauPrev[i] = tau[i];
+        bpPrev = bp;
+        xPrev = x;
+        nPrev = nCur;
+    }
+    const float hb = mul_rn(0.5f, h.binSize);
+#pragma unroll
+    for (int m = 0; m < 5; ++m) { ci[m] = mul_rn(ci[m], hb); mom1[m] = mul_rn(mom1[m], hb); }
+    float ll = wps - mul_rn(h.nSum, hw_logf(probSum));
+    const float ds = v.s - r.sExpect;
+    ll = ll - mul_rn(mul_rn(0.5f, mul_rn(ds, ds)), r.sExpectW);
+    safeOut = safe;
+    return ll;
+}
+
+// One M-step (DmeEmHost.cpp:494-565) from the E-step's sums; ci is floored in
+// place.  Sets bit 4 (VLOW_SIGNAL) of zStatus when s is clamped to its floor.
+__device__ __forceinline__ void EmMStep(const KParams& k, const EmHist& h, const EmReg& r, bool safe,
+                                        const float* bpS, const float* tau0S, const float* facS, float ci[5],
+                                        const float mom1[5], const float varinv[5], EmVars& v, int& zStatus)
+{
+    const int z = h.z;
+#pragma unroll
+    for (int i = 0; i < 5; ++i) ci[i] = fmax_sse(ci[i], 0.1f);
+#pragma unroll
+    for (int i = 0; i < 5; ++i) v.rho[i] = ci[i] / h.nSum;
+    {
+        const float rs = (v.rho[0] + v.rho[1]) + (v.rho[2] + (v.rho[3] + v.rho[4]));
+#pragma unroll
+        for (int i = 0; i < 5; ++i) v.rho[i] = v.rho[i] / rs;
+    }
+    v.mu[0] = mom1[0] / ci[0];
+    float numer = 0.0f, denom = 0.0f;
+#pragma unroll
+    for (int a = 0; a < kAnalogs; ++a)
+    {
+        const int i = a + 1;
+        numer = add_rn(numer, mul_rn(mul_rn(k.relAmp[a], varinv[i]), mom1[i]));
+        denom = add_rn(denom, mul_rn(mul_rn(mul_rn(k.relAmp[a], k.relAmp[a]), varinv[i]), ci[i]));
+    }
+    numer = add_rn(numer, mul_rn(r.sExpect, r.sExpectW));
+    denom = add_rn(denom, r.sExpectW);
+    float sv = numer / denom;
+    const float sMin = fmax_sse(mul_rn(0.5f, sqrtf(v.var[0])), k.minPulseMean) / k.rpaMin;
+    const bool vls = sv < sMin;
+    sv = vls ? sMin : sv;
+    if (vls) zStatus |= 4;
+    v.s = sv;
+#pragma unroll
+    for (int a = 0; a < kAnalogs; ++a) v.mu[a + 1] = mul_rn(sv, k.relAmp[a]);
+    // Background variance: second pass over the bins.  The scratch values of
+    // boundary j + 1 are those of boundary j in the next bin, so each is
+    // loaded once, one bin ahead of its use.  Scratch slots of boundaries next
+    // to empty bins hold stale values; they are loaded but only used for
+    // occupied bins (or when !safe, where every boundary was written).
+    float mom2 = 0.0f;
+    {
+        float bpj = bpS[z], t0j = tau0S[z];
+        uint32_t nj = h.Count(0);
+        for (int j = 0; j < kBins; ++j)
+        {
+            const float bpk = bpS[(size_t)(j + 1) * kLane + z], t0k = tau0S[(size_t)(j + 1) * kLane + z];
+            const float fj = facS[(size_t)j * kLane + z];
+            const uint32_t nk = (j + 1 < kBins) ? h.Count(j + 1) : 0u;
+            if (!safe || nj != 0u)      // an empty bin adds +0 (see the E-step)
+            {
+                const float xj = h.BinStart(j) - v.mu[0];
+                const float xk = h.BinStart(j + 1) - v.mu[0];
+                float tmp = mul_rn(mul_rn(mul_rn(bpj, xj), xj), t0j);
+                tmp = add_rn(tmp, mul_rn(mul_rn(mul_rn(bpk, xk), xk), t0k));
+                tmp = mul_rn(tmp, fj);
+                mom2 = add_rn(mom2, tmp);
+            }
+            bpj = bpk;
+            t0j = t0k;
+            nj = nk;
+        }
+    }
+    mom2 = mul_rn(mom2, mul_rn(0.5f, h.binSize));
+    float v0 = add_rn(mom2 / ci[0], h.varQuant);
+    v0 = fmin_sse(fmax_sse(v0, k.blVarMin), k.blVarMax);
+    v.var[0] = v0;
+#pragma unroll
+    for (int a = 0; a < kAnalogs; ++a) v.var[a + 1] = SignalCovar(k, k.cv2[a], v.mu[a + 1], v0);
+}
+
+__global__ void __launch_bounds__(kLane, 12) DmeEstimateKernel(DmeArgs A, KParams k)
+{
+    const int l = blockIdx.x;
+    const int z = threadIdx.x;
+    float* bpS = A.scratch + (size_t)l * 3 * (kBins + 1) * kLane;
+    float* tau0S = bpS + (size_t)(kBins + 1) * kLane;
+    float* facS = tau0S + (size_t)(kBins + 1) * kLane;
+
+    EmHist h;
+    LoadEmHist(A.hist[l], z, h);
+    ModelF det;
+    EmVars v;
+    EmReg r;
+    DmePrelude(k, A.models[l], A.stats[l], h, A.tModel, A.tEst, det, v, r);
+
     // Values needed only before and after the EM iterations (the prior model
     // and the estimates at the latest converged iteration) wait in per-thread
     // shared-memory columns, which keeps them out of registers in the loop.
@@ -262,33 +547,7 @@ __global__ void __launch_bounds__(kLane, 12) DmeEstimateKernel(DmeArgs A, KParam
     auto rhoEst = [&](int i) -> float& { return shEst[i][z]; };
     auto muEst = [&](int i) -> float& { return shEst[5 + i][z]; };
     auto varEst = [&](int i) -> float& { return shEst[10 + i][z]; };
-
-    // EM setup (DmeEmHost.cpp:253-361)
-    const float rhoMin = 0.001f;
-    float rho[5], mu[5], var[5];
-    rho[0] = fmax_sse(work.bw, rhoMin); mu[0] = work.bm; var[0] = work.bv;
-    for (int a = 0; a < kAnalogs; ++a)
-    {
-        rho[a + 1] = fmax_sse(work.aw[a], rhoMin);
-        mu[a + 1] = work.am[a];
-        var[a + 1] = work.av[a];
-    }
-    const float varQuant = mul_rn(binSize, binSize) / 12.0f;
-    for (int i = 0; i < 5; ++i) var[i] += varQuant;
-    var[0] = fmin_sse(var[0], k.blVarMax);
-    {
-        const float rs = (rho[0] + rho[1]) + (rho[2] + (rho[3] + rho[4]));
-        for (int i = 0; i < 5; ++i) rho[i] = rho[i] / rs;
-    }
-    for (int i = 0; i < 5; ++i) { rhoEst(i) = rho[i]; muEst(i) = mu[i]; varEst(i) = var[i]; }
-    float s;
-    {
-        const float p0 = mul_rn(mu[1], k.relAmp[0]), p1 = mul_rn(mu[2], k.relAmp[1]);
-        const float p2 = mul_rn(mu[3], k.relAmp[2]), p3 = mul_rn(mu[4], k.relAmp[3]);
-        s = ((p0 + p1) + (p2 + p3)) / k.rpaSum2;
-    }
-    const float sExpect = s / scaleFactor;
-    const float sExpectW = mul_rn(det.conf, k.pulseAmpReg);
+    for (int i = 0; i < 5; ++i) { rhoEst(i) = v.rho[i]; muEst(i) = v.mu[i]; varEst(i) = v.var[i]; }
     {
         shDet[0][z] = det.bw; shDet[1][z] = det.bm; shDet[2][z] = det.bv; shDet[3][z] = det.conf;
 #pragma unroll
@@ -298,133 +557,19 @@ __global__ void __launch_bounds__(kLane, 12) DmeEstimateKernel(DmeArgs A, KParam
         }
     }
     float logLike = -3.40282347e+38f;
-    const float binProbMin = mul_rn(fmax_sse(mul_rn((float)total, binSize), 1.0f), 1.17549435e-38f);
-    int zStatus = (total < 160u) ? 2 : 0;
+    int zStatus = (h.total < 160u) ? 2 : 0;
     bool mConverged = false;
     int mIter = 0;
     float mLogLike = -__int_as_float(0x7f800000);
-    float nSum = 0.0f;
-    for (int j = 0; j < kBins; ++j) nSum += (float)H.bin_count[j][z];
 
     const int iterLimit = k.emIterLimit;
-    const float halfLog2pi = mul_rn(0.5f, k.logTwoPi);
     int it = 0;
     for (; it < iterLimit; ++it)
     {
-        float varinv[5], pref[5];
-#pragma unroll
-        for (int i = 0; i < 5; ++i)
-        {
-            varinv[i] = 1.0f / var[i];
-            pref[i] = (hw_logf(rho[i]) - mul_rn(0.5f, hw_logf(var[i]))) - halfLog2pi;
-        }
-        float probSum = 0.0f, wps = 0.0f;
-        float ci[5] = {0, 0, 0, 0, 0}, mom1[5] = {0, 0, 0, 0, 0};
-        // Only bins with a count contribute to c_i, mom1, wps and (in the
-        // M-step) mom2: an empty bin adds (finite) x 0 = +-0 to sums that start
-        // at +0 and therefore never hold -0, which leaves them unchanged.  So
-        // the responsibilities (5 exps), log(binProb) and n_j / binProb are
-        // only evaluated next to occupied bins; the boundary density, which
-        // every bin probability needs, is always evaluated.
-        // The shortcut needs every boundary density finite: llb <= max(pref) +
-        // log(5), so finite prefactors, means and inverse variances with
-        // max(pref) < 80 guarantee it.  Otherwise the reference path runs.
-        bool safe = true;
-        {
-            float pmax = pref[0];
-#pragma unroll
-            for (int i = 0; i < 5; ++i)
-            {
-                safe &= isfinite(pref[i]) & isfinite(mu[i]) & isfinite(varinv[i]);
-                pmax = fmaxf(pmax, pref[i]);
-            }
-            safe &= pmax < 80.0f;
-        }
-        float tauPrev[5] = {0, 0, 0, 0, 0}, bpPrev = 0.0f, xPrev = 0.0f;
-        uint32_t nPrev = 0;
-        // bin counts are loaded one boundary ahead of their use
-        uint32_t nNext = (uint32_t)H.bin_count[0][z];
-        for (int b = 0; b <= kBins; ++b)
-        {
-            // cornerComp(b)
-            const float x = binStart(b);
-            float t[5];
-#pragma unroll
-            for (int i = 0; i < 5; ++i)
-            {
-                const float y = x - mu[i];
-                t[i] = pref[i] - mul_rn(mul_rn(mul_rn(0.5f, y), y), varinv[i]);
-            }
-            float tmax = t[0];
-#pragma unroll
-            for (int i = 1; i < 5; ++i) tmax = fmax_sse(tmax, t[i]);
-            const uint32_t nCur = nNext;
-            nNext = (b + 1 < kBins) ? (uint32_t)H.bin_count[b + 1][z] : 0u;
-            const bool needTau = (nPrev != 0u) | (nCur != 0u) | !safe;
-            // Far tails: with every t finite and below -106, llb = tmax +
-            // log(se) with 1 <= se <= 5 stays below -104.3, where hw_expf
-            // returns exactly 0, so bp is 0 without evaluating it.
-            bool allFinite = true;
-#pragma unroll
-            for (int i = 0; i < 5; ++i) allFinite &= isfinite(t[i]);
-            const bool tail = !needTau & allFinite & (tmax < -106.0f);
-            float bp = 0.0f, llb = 0.0f;
-            if (!tail)
-            {
-                float se = hw_expf(t[0] - tmax);
-#pragma unroll
-                for (int i = 1; i < 5; ++i) se = add_rn(se, hw_expf(t[i] - tmax));
-                llb = add_rn(tmax, hw_logf(se));
-                bp = hw_expf(llb);
-            }
-            float tau[5];
-            if (needTau)
-            {
-#pragma unroll
-                for (int i = 0; i < 5; ++i) tau[i] = hw_expf(t[i] - llb);
-                bpS[(size_t)b * kLane + z] = bp;
-                tau0S[(size_t)b * kLane + z] = tau[0];
-            }
-            else
-            {
-#pragma unroll
-                for (int i = 0; i < 5; ++i) tau[i] = 0.0f;
-            }
-            if (b > 0)
-            {
-                // centerComp(b - 1)
-                const int c = b - 1;
-                const float bpr = fmax_sse(mul_rn(mul_rn(0.5f, binSize), add_rn(bpPrev, bp)), binProbMin);
-                probSum = add_rn(probSum, bpr);
-                if ((nPrev != 0u) | !safe)
-                {
-                    const float njb = (float)nPrev;
-                    wps = add_rn(wps, mul_rn(njb, hw_logf(bpr)));
-                    const float factor = njb / bpr;
-                    facS[(size_t)c * kLane + z] = factor;
-#pragma unroll
-                    for (int m = 0; m < 5; ++m)
-                    {
-                        const float tmp1 = mul_rn(bpPrev, tauPrev[m]);
-                        const float tmp2 = mul_rn(bp, tau[m]);
-                        ci[m] = add_rn(ci[m], mul_rn(add_rn(tmp1, tmp2), factor));
-                        mom1[m] = add_rn(mom1[m], mul_rn(add_rn(mul_rn(tmp1, xPrev), mul_rn(tmp2, x)), factor));
-                    }
-                }
-            }
-#pragma unroll
-            for (int i = 0; i < 5; ++i) tauPrev[i] = tau[i];
-            bpPrev = bp;
-            xPrev = x;
-            nPrev = nCur;
-        }
-        const float hb = mul_rn(0.5f, binSize);
-#pragma unroll
-        for (int m = 0; m < 5; ++m) { ci[m] = mul_rn(ci[m], hb); mom1[m] = mul_rn(mom1[m], hb); }
+        float ci[5], mom1[5], varinv[5];
+        bool safe;
+        const float ll = EmEStep(k, h, v, r, bpS, tau0S, facS, ci, mom1, varinv, safe);
         const float prev = logLike;
-        float ll = wps - mul_rn(nSum, hw_logf(probSum));
-        const float ds = s - sExpect;
-        ll = ll - mul_rn(mul_rn(0.5f, mul_rn(ds, ds)), sExpectW);
         logLike = ll;
         const float delta = ll - prev;
         const float convTol = mul_rn(1e-4f, fmax_sse(ll, -ll));
@@ -436,75 +581,11 @@ __global__ void __launch_bounds__(kLane, 12) DmeEstimateKernel(DmeArgs A, KParam
         if (cv)
         {
 #pragma unroll
-            for (int i = 0; i < 5; ++i) { rhoEst(i) = rho[i]; muEst(i) = mu[i]; varEst(i) = var[i]; }
+            for (int i = 0; i < 5; ++i) { rhoEst(i) = v.rho[i]; muEst(i) = v.mu[i]; varEst(i) = v.var[i]; }
         }
         const int allDone = __syncthreads_and(mConverged | (zStatus != 0));
         if (!k.iterToLimit && allDone) break;
-
-        // M-step (DmeEmHost.cpp:494-565)
-#pragma unroll
-        for (int i = 0; i < 5; ++i) ci[i] = fmax_sse(ci[i], 0.1f);
-#pragma unroll
-        for (int i = 0; i < 5; ++i) rho[i] = ci[i] / nSum;
-        {
-            const float rs = (rho[0] + rho[1]) + (rho[2] + (rho[3] + rho[4]));
-#pragma unroll
-            for (int i = 0; i < 5; ++i) rho[i] = rho[i] / rs;
-        }
-        mu[0] = mom1[0] / ci[0];
-        float numer = 0.0f, denom = 0.0f;
-#pragma unroll
-        for (int a = 0; a < kAnalogs; ++a)
-        {
-            const int i = a + 1;
-            numer = add_rn(numer, mul_rn(mul_rn(k.relAmp[a], varinv[i]), mom1[i]));
-            denom = add_rn(denom, mul_rn(mul_rn(mul_rn(k.relAmp[a], k.relAmp[a]), varinv[i]), ci[i]));
-        }
-        numer = add_rn(numer, mul_rn(sExpect, sExpectW));
-        denom = add_rn(denom, sExpectW);
-        float sv = numer / denom;
-        const float sMin = fmax_sse(mul_rn(0.5f, sqrtf(var[0])), k.minPulseMean) / k.rpaMin;
-        const bool vls = sv < sMin;
-        sv = vls ? sMin : sv;
-        if (vls) zStatus |= 4;
-        s = sv;
-#pragma unroll
-        for (int a = 0; a < kAnalogs; ++a) mu[a + 1] = mul_rn(sv, k.relAmp[a]);
-        // Background variance: second pass over the bins.
-        // The scratch values of boundary j + 1 are those of boundary j in the
-        // next bin, so each is loaded once, one bin ahead of its use.  Scratch
-        // slots of boundaries next to empty bins hold stale values; they are
-        // loaded but only used for occupied bins (or when !safe, where every
-        // boundary was written).
-        float mom2 = 0.0f;
-        {
-            float bpj = bpS[z], t0j = tau0S[z];
-            uint32_t nj = (uint32_t)H.bin_count[0][z];
-            for (int j = 0; j < kBins; ++j)
-            {
-                const float bpk = bpS[(size_t)(j + 1) * kLane + z], t0k = tau0S[(size_t)(j + 1) * kLane + z];
-                const float fj = facS[(size_t)j * kLane + z];
-                const uint32_t nk = (j + 1 < kBins) ? (uint32_t)H.bin_count[j + 1][z] : 0u;
-                if (!safe || nj != 0u)      // an empty bin adds +0 (see the E-step)
-                {
-                    const float xj = binStart(j) - mu[0];
-                    const float xk = binStart(j + 1) - mu[0];
-                    float tmp = mul_rn(mul_rn(mul_rn(bpj, xj), xj), t0j);
-                    tmp = add_rn(tmp, mul_rn(mul_rn(mul_rn(bpk, xk), xk), t0k));
-                    tmp = mul_rn(tmp, fj);
-                    mom2 = add_rn(mom2, tmp);
-                }
-                bpj = bpk;
-                t0j = t0k;
-                nj = nk;
-            }
-        }
-        mom2 = mul_rn(mom2, mul_rn(0.5f, binSize));
-        float v0 = add_rn(mom2 / ci[0], varQuant);
-        v0 = fmin_sse(fmax_sse(v0, k.blVarMin), k.blVarMax);
-        var[0] = v0;
-#pragma unroll
-        for (int a = 0; a < kAnalogs; ++a) var[a + 1] = SignalCovar(k, k.cv2[a], mu[a + 1], v0);
+        EmMStep(k, h, r, safe, bpS, tau0S, facS, ci, mom1, varinv, v, zStatus);
     }
     const int laneIters = it + 1 < iterLimit ? it + 1 : iterLimit;
 
@@ -512,6 +593,7 @@ __global__ void __launch_bounds__(kLane, 12) DmeEstimateKernel(DmeArgs A, KParam
     bool finite = true;
 #pragma unroll
     for (int i = 0; i < 5; ++i) finite &= isfinite(rhoEst(i)) & isfinite(muEst(i)) & isfinite(varEst(i));
+    ModelF work;
     work.bw = rhoEst(0); work.bm = muEst(0); work.bv = varEst(0);
 #pragma unroll
     for (int a = 0; a < kAnalogs; ++a) { work.aw[a] = rhoEst(a + 1); work.am[a] = muEst(a + 1); work.av[a] = varEst(a + 1); }
@@ -594,6 +676,144 @@ cudaError_t LaunchDmeEstimate(const DmeArgs& a, const KParams& k, cudaStream_t s
     return cudaGetLastError();
 }
 
+// ---- Single-ZMW EM fit (learned initializer) ------------------------------------
+// The reference's EM steps for each ZMW on its own: from the plain start of
+// DmePrelude, from a caller's proposal, or from whichever of the two has the
+// higher log-likelihood; maxIter iterations for every ZMW (no lane-wide stop)
+// and no final confidence blend.  Records the first iteration that meets the
+// reference's convergence test and the first iteration whose parameters lie
+// within `tol` of a target.  No counterpart in the reference.
+struct DmeFitArgs
+{
+    const hw_lane_histogram* hist;
+    const hw_baseliner_stats* stats;
+    const hw_lane_model* models;
+    const float* proposal;     // [lanes][15][64] or null
+    const float* target;       // [lanes][15][64] or null
+    float* scratch;            // [lanes][3][301][64]
+    float* params;             // [lanes][15][64]
+    int32_t* iters;            // [lanes][5][64]
+    float* loglike;            // [lanes][3][64]
+    int lanes, tModel, tEst, mode, maxIter;
+    float tol;
+};
+
+// Largest relative distance of the parameters from a target column, with
+// floors 0.01 (fractions), 1 DN (means) and 1 DN^2 (variances).
+__device__ __forceinline__ float EmDistance(const EmVars& v, const float* t, int z)
+{
+    float d = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+    {
+        const float tr = t[i * kLane + z], tm = t[(5 + i) * kLane + z], tv = t[(10 + i) * kLane + z];
+        d = fmaxf(d, fabsf(v.rho[i] - tr) / fmaxf(fabsf(tr), 0.01f));
+        d = fmaxf(d, fabsf(v.mu[i] - tm) / fmaxf(fabsf(tm), 1.0f));
+        d = fmaxf(d, fabsf(v.var[i] - tv) / fmaxf(fabsf(tv), 1.0f));
+    }
+    return d;
+}
+
+// Largest relative change between two parameter sets (same floors).
+__device__ __forceinline__ float EmStep(const EmVars& a, const EmVars& b)
+{
+    float d = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+    {
+        d = fmaxf(d, fabsf(a.rho[i] - b.rho[i]) / fmaxf(fabsf(a.rho[i]), 0.01f));
+        d = fmaxf(d, fabsf(a.mu[i] - b.mu[i]) / fmaxf(fabsf(a.mu[i]), 1.0f));
+        d = fmaxf(d, fabsf(a.var[i] - b.var[i]) / fmaxf(fabsf(a.var[i]), 1.0f));
+    }
+    return d;
+}
+
+__global__ void __launch_bounds__(kLane, 12) DmeEmFitKernel(DmeFitArgs A, KParams k)
+{
+    const int l = blockIdx.x;
+    const int z = threadIdx.x;
+    float* bpS = A.scratch + (size_t)l * 3 * (kBins + 1) * kLane;
+    float* tau0S = bpS + (size_t)(kBins + 1) * kLane;
+    float* facS = tau0S + (size_t)(kBins + 1) * kLane;
+
+    EmHist h;
+    LoadEmHist(A.hist[l], z, h);
+    ModelF det;
+    EmVars v;
+    EmReg r;
+    DmePrelude(k, A.models[l], A.stats[l], h, A.tModel, A.tEst, det, v, r);
+
+    float ci[5], mom1[5], varinv[5];
+    bool safe;
+    const float llPlain = EmEStep(k, h, v, r, bpS, tau0S, facS, ci, mom1, varinv, safe);
+    float llStart = llPlain;
+    int fellBack = 0;
+    if (A.mode != HW_EM_START_PLAIN)
+    {
+        const float* Q = A.proposal + (size_t)l * 15 * kLane;
+        EmVars p;
+#pragma unroll
+        for (int i = 0; i < 5; ++i)
+        {
+            p.rho[i] = Q[i * kLane + z];
+            p.mu[i] = Q[(5 + i) * kLane + z];
+            p.var[i] = Q[(10 + i) * kLane + z];
+        }
+        p.s = EmScale(k, p.mu);
+        const float llProp = EmEStep(k, h, p, r, bpS, tau0S, facS, ci, mom1, varinv, safe);
+        const bool usePlain = (A.mode == HW_EM_START_BETTER) && !(llProp >= llPlain);
+        if (usePlain) fellBack = 1;
+        else
+        {
+            v = p;
+            llStart = llProp;
+        }
+    }
+    const float* T = A.target ? A.target + (size_t)l * 15 * kLane : nullptr;
+    int zStatus = (h.total < 160u) ? 2 : 0;
+    int tolIter = -1, stepIter = -1, mIter = 0;
+    bool mConverged = false;
+    float logLike = -3.40282347e+38f, mLogLike = -__int_as_float(0x7f800000), last = llStart;
+    for (int it = 0; it < A.maxIter; ++it)
+    {
+        if (T && tolIter < 0 && EmDistance(v, T, z) <= A.tol) tolIter = it;
+        const float ll = EmEStep(k, h, v, r, bpS, tau0S, facS, ci, mom1, varinv, safe);
+        const float prev = logLike;
+        logLike = ll;
+        const float delta = ll - prev;
+        const float convTol = mul_rn(1e-4f, fmax_sse(ll, -ll));
+        bool cv = (delta >= 0) & (delta < convTol);
+        cv &= (ll >= mLogLike);
+        mIter = (cv & !mConverged) ? it : mIter;
+        mLogLike = cv ? ll : mLogLike;
+        mConverged |= cv;
+        last = ll;
+        const EmVars before = v;
+        EmMStep(k, h, r, safe, bpS, tau0S, facS, ci, mom1, varinv, v, zStatus);
+        if (stepIter < 0 && EmStep(v, before) <= A.tol) stepIter = it + 1;
+    }
+    if (T && tolIter < 0 && EmDistance(v, T, z) <= A.tol) tolIter = A.maxIter;
+
+    float* P = A.params + (size_t)l * 15 * kLane;
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+    {
+        P[i * kLane + z] = v.rho[i];
+        P[(5 + i) * kLane + z] = v.mu[i];
+        P[(10 + i) * kLane + z] = v.var[i];
+    }
+    int32_t* I = A.iters + (size_t)l * 5 * kLane;
+    I[0 * kLane + z] = mConverged ? mIter : -1;
+    I[1 * kLane + z] = tolIter;
+    I[2 * kLane + z] = fellBack;
+    I[3 * kLane + z] = zStatus;
+    I[4 * kLane + z] = stepIter;
+    float* L = A.loglike + (size_t)l * 3 * kLane;
+    L[0 * kLane + z] = llPlain;
+    L[1 * kLane + z] = llStart;
+    L[2 * kLane + z] = last;
+}
+
 // ---- Estimate without device allocation -------------------------------------
 // Callers such as a pre-allocated real-time pipeline or code running inside a
 // custom allocator's callbacks may not be allowed to call cudaMalloc.  For
@@ -663,5 +883,42 @@ extern "C" int hw_dme_estimate_noalloc(const hw_config* cfg, uint32_t lanes, con
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
     if (ce != cudaSuccess) return SetLastError(HW_ERR_CUDA, cudaGetErrorString(ce));
     if (h) return SetLastError(h, "DME: a reference sanity assertion failed (non-finite estimate or bad SNR-drop threshold)");
+    return HW_OK;
+}
+
+extern "C" int hw_dme_em_fit_scratch_bytes(uint32_t lanes, uint64_t* bytes)
+{
+    if (!bytes) return hwk::SetLastError(HW_ERR_INVALID_ARG, "bytes is NULL");
+    *bytes = (uint64_t)lanes * hwk::kDmeScratchFloatsPerLane * sizeof(float);
+    return HW_OK;
+}
+
+extern "C" int hw_dme_em_fit(const hw_config* cfg, uint32_t lanes, const hw_lane_histogram* d_hist,
+                             const hw_baseliner_stats* d_stats, hw_frame_interval hist_fi,
+                             hw_frame_interval model_fi, const hw_lane_model* d_models, int start,
+                             const float* d_proposal, const float* d_target, float tol, uint32_t max_iter,
+                             float* d_scratch, float* d_params, int32_t* d_iters, float* d_loglike, void* stream)
+{
+    using namespace hwk;
+    if (!cfg || !d_hist || !d_stats || !d_models || !d_scratch || !d_params || !d_iters || !d_loglike)
+        return SetLastError(HW_ERR_INVALID_ARG, "NULL argument");
+    if (start < HW_EM_START_PLAIN || start > HW_EM_START_BETTER)
+        return SetLastError(HW_ERR_INVALID_ARG, "hw_dme_em_fit: start must be HW_EM_START_PLAIN, _PROPOSAL or _BETTER");
+    if (start != HW_EM_START_PLAIN && !d_proposal)
+        return SetLastError(HW_ERR_INVALID_ARG, "hw_dme_em_fit: a proposal start needs d_proposal");
+    if (lanes == 0 || max_iter > 100000)
+        return SetLastError(HW_ERR_INVALID_ARG, "hw_dme_em_fit: lanes must be positive and max_iter at most 100000");
+    if (hist_fi.lower == hist_fi.upper || model_fi.lower == model_fi.upper)
+        return SetLastError(HW_ERR_INVALID_ARG, "frame intervals must not be empty");
+    hwp::Derived d;
+    KParams k;
+    int rc = PrepareConfigNoAlloc(cfg, &d, &k);
+    if (rc) return rc;
+    DmeFitArgs a{d_hist, d_stats, d_models, d_proposal, d_target, d_scratch, d_params, d_iters, d_loglike,
+                 (int)lanes, model_fi.lower + (model_fi.upper - model_fi.lower) / 2,
+                 hist_fi.lower + (hist_fi.upper - hist_fi.lower) / 2, start, (int)max_iter, tol};
+    DmeEmFitKernel<<<lanes, kLane, 0, reinterpret_cast<cudaStream_t>(stream)>>>(a, k);
+    const cudaError_t ce = cudaGetLastError();
+    if (ce != cudaSuccess) return SetLastError(HW_ERR_CUDA, cudaGetErrorString(ce));
     return HW_OK;
 }

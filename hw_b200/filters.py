@@ -151,6 +151,25 @@ class DmeEmEstimator(_Handle):
         return d
 
 
+def em_fit(cfg, lanes, hist, stats, hist_fi, model_fi, models, start=0, proposal=None, target=None, tol=1e-4,
+           max_iter=20, scratch=None):
+    """Single-ZMW EM fit (hw_dme_em_fit) on device buffers; returns
+    (params [lanes][15][64] float32, iters [lanes][5][64] int32,
+    loglike [lanes][3][64] float32) as CUDA tensors."""
+    dev = "cuda"
+    params = torch.empty((lanes, 15, abi.LANE), dtype=torch.float32, device=dev)
+    iters = torch.empty((lanes, 5, abi.LANE), dtype=torch.int32, device=dev)
+    ll = torch.empty((lanes, 3, abi.LANE), dtype=torch.float32, device=dev)
+    if scratch is None:
+        nbytes = C.c_uint64()
+        check(lib().hw_dme_em_fit_scratch_bytes(lanes, C.byref(nbytes)))
+        scratch = torch.empty(nbytes.value // 4, dtype=torch.float32, device=dev)
+    check(lib().hw_dme_em_fit(C.byref(cfg), lanes, _p(hist), _p(stats), abi.FrameInterval(*hist_fi),
+                              abi.FrameInterval(*model_fi), _p(models), int(start), _p(proposal), _p(target),
+                              float(tol), int(max_iter), _p(scratch), _p(params), _p(iters), _p(ll), _stream()))
+    return params, iters, ll
+
+
 class FrameLabeler(_Handle):
     _destroy = "hw_labeler_destroy"
 

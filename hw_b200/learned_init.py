@@ -1,0 +1,328 @@
+"""Learned DME initializer: data, training and evaluation on the GPU.
+
+The network (hw_learned_init_* in libhw_b200.so) maps a ZMW's 300-bin trace
+histogram and baseline statistics to an EM start; hw_dme_em_fit runs the
+reference's EM from it and falls back to the reference's own start whenever
+the proposal's log-likelihood is lower.  Nothing here has a counterpart in
+the reference.
+
+Data.  Traces come from the uneven-pool generator (workload 2: per-ZMW
+lognormal amplitude factors with sigma 0.3, pulse rates uniform in
+0.02-0.12 per frame).  Each pool runs the single-estimate schedule of
+DetectionModelEstimator (statistics pre-accumulation, then a 4096-frame
+histogram) up to its first estimate; the inputs of that estimate (histogram,
+baseliner statistics, prior model) are kept.  The label of a ZMW is the
+fixed point of the reference's EM from the reference start, run for
+`fit_iters` iterations.
+
+Metrics, each from the plain start and from the learned start:
+  * iterations to the fixed point: the first iteration whose 15 parameters
+    (fractions, means, variances) are all within 1e-4 relative (floors
+    0.01 / 1 DN / 1 DN^2) of the plain EM's fixed point;
+  * iterations to the parameter-step rule: the first iteration whose update
+    changes no parameter by more than 1e-4 relative;
+  * iterations to the reference's own stopping rule (log-likelihood gain
+    below 1e-4 of |logL|, DmeEmHost.cpp:458-475).
+ZMWs whose plain EM does not reach its own fixed point within the budget are
+left out of the averages and counted in `resolved_fraction`.
+"""
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import abi, filters as Fl, workloads
+from .native import check, lib
+
+FEAT, OUT, OUT_USED = 304, 32, 19
+NORM_SIZE = 2 * FEAT + 2 * OUT
+
+
+def data_config():
+    """Single-estimate schedule with a 4096-frame histogram."""
+    cfg = workloads.small_config()
+    cfg.model_estimation_mode = abi.INITIAL_ESTIMATIONS
+    cfg.min_frames_for_estimate = 4096
+    return cfg
+
+
+class Pool:
+    """The inputs of one pool's first DME estimate, on the device."""
+
+    def __init__(self, cfg, lanes, hist, stats, hist_fi, models, model_fi):
+        self.cfg, self.lanes = cfg, lanes
+        self.hist, self.stats, self.models = hist, stats, models
+        self.hist_fi, self.model_fi = hist_fi, model_fi
+
+
+def estimate_inputs(cfg, lanes, pool_id=0, seed=None, frames_per_chunk=512, workload=2):
+    """Runs the baseliner and the DetectionModelEstimator schedule
+    (DetectionModelEstimator.cpp:93-160, single-estimate analyzer) on
+    generated traces until the first estimate is due; returns its Pool."""
+    F = frames_per_chunk
+    gen = Fl.TraceGenerator(lanes, workload=workload, zmw_offset=pool_id * lanes * abi.LANE, seed=seed)
+    bl = Fl.Baseliner(cfg, pool_id, lanes, F)
+    agg = Fl.BaselineStatsAggregator(pool_id, lanes)
+    hist = Fl.TraceHistogramAccumulator(cfg, pool_id, lanes)
+    dme = Fl.DmeEmEstimator(cfg, pool_id, lanes)
+    HIST_INIT, DME_INIT, SEQUENCING = 0, 1, 2
+    status, remaining = HIST_INIT, int(cfg.num_frames_pre_accum_stats)
+    latency = bl.startup_latency()
+    models = model_fi = None
+    trace = torch.empty((lanes, F, abi.LANE), dtype=torch.int16, device="cuda")
+    for c in range(100000):
+        ff = c * F
+        gen.next(ff, F, out=trace)
+        bls, st = bl(trace, ff)
+        if ff <= latency:
+            continue
+        fi = (ff, ff + F)
+        agg.add_metrics(st, fi)
+        if status != HIST_INIT:
+            hist.add_batch(bls, fi, models)
+        if status != SEQUENCING:
+            s, afi = agg.trace_stats()
+            models = dme.init_detection_models(s).clone()
+            model_fi = afi
+        remaining -= F
+        if remaining <= 0:
+            if status == DME_INIT:
+                status = SEQUENCING
+            if status == SEQUENCING:
+                h, hfi = hist.histogram()
+                s, _ = agg.trace_stats()
+                out = Pool(cfg, lanes, h.clone(), s.clone(), hfi, models, model_fi)
+                for o in (gen, bl, agg, hist, dme):
+                    o.close()
+                return out
+            s, _ = agg.trace_stats()
+            hist.reset_from_stats(s)
+            agg.reset()
+            if status == HIST_INIT:
+                status = DME_INIT
+            remaining = int(cfg.min_frames_for_estimate)
+    raise RuntimeError("estimate never became due")
+
+
+def fit(pool, start=0, proposal=None, target=None, tol=1e-4, max_iter=1000):
+    """hw_dme_em_fit on a Pool: (params [lanes][15][64], iters [lanes][5][64],
+    loglike [lanes][3][64]) CUDA tensors."""
+    return Fl.em_fit(pool.cfg, pool.lanes, pool.hist, pool.stats, pool.hist_fi, pool.model_fi, pool.models,
+                     start=start, proposal=proposal, target=target, tol=tol, max_iter=max_iter)
+
+
+def features(pool):
+    out = torch.empty((pool.lanes * abi.LANE, FEAT), dtype=torch.float32, device="cuda")
+    check(lib().hw_learned_init_features(pool.lanes, Fl._p(pool.hist), Fl._p(pool.stats), Fl._p(out), Fl._stream()))
+    return out
+
+
+def targets(pool, params):
+    out = torch.empty((pool.lanes * abi.LANE, OUT), dtype=torch.float32, device="cuda")
+    check(lib().hw_learned_init_targets(C.byref(pool.cfg), pool.lanes, Fl._p(params), Fl._p(pool.hist), Fl._p(out),
+                                        Fl._stream()))
+    return out
+
+
+class Network:
+    """One hw_learned_init handle: BF16 MLP with FP32 master weights and AdamW."""
+
+    def __init__(self, max_batch=4096, seed=1):
+        self._h = C.c_void_p()
+        check(lib().hw_learned_init_create(max_batch, seed, C.byref(self._h)))
+        n = C.c_uint32()
+        check(lib().hw_learned_init_param_count(C.byref(n)))
+        self.n_params = n.value
+        self.max_batch = max_batch
+
+    def close(self):
+        if self._h:
+            lib().hw_learned_init_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def get(self):
+        p = np.empty(self.n_params, np.float32)
+        nm = np.empty(NORM_SIZE, np.float32)
+        check(lib().hw_learned_init_get_params(self._h, abi.ptr(p), abi.ptr(nm)))
+        return p, nm
+
+    def set(self, params=None, norm=None):
+        p = None if params is None else np.ascontiguousarray(params, np.float32)
+        nm = None if norm is None else np.ascontiguousarray(norm, np.float32)
+        check(lib().hw_learned_init_set_params(self._h, abi.ptr(p), abi.ptr(nm)))
+
+    def save(self, path):
+        p, nm = self.get()
+        np.savez(path, params=p, norm=nm)
+
+    def load(self, path):
+        d = np.load(path)
+        self.set(d["params"], d["norm"])
+
+    def fit_normalization(self, feats, tgts):
+        """Input and output standardisation from (up to 262,144 of) the
+        training rows, computed on the host."""
+        nm = np.zeros(NORM_SIZE, np.float32)
+        rows = np.random.default_rng(0).permutation(feats.shape[0])[:262144]
+        sel = torch.from_numpy(np.sort(rows)).cuda()
+        f = feats.index_select(0, sel).cpu().numpy().astype(np.float64)
+        t = tgts.index_select(0, sel).cpu().numpy().astype(np.float64)
+        nm[:FEAT] = f.mean(0)
+        nm[FEAT:2 * FEAT] = np.maximum(f.std(0), 1e-3)
+        nm[2 * FEAT:2 * FEAT + OUT] = t.mean(0)
+        nm[2 * FEAT + OUT:] = np.maximum(t.std(0), 1e-4)
+        nm[2 * FEAT + OUT_USED:2 * FEAT + OUT] = 0.0
+        nm[2 * FEAT + OUT + OUT_USED:] = 1.0
+        self.set(norm=nm)
+
+    def forward(self, feats):
+        out = torch.empty((feats.shape[0], OUT), dtype=torch.float32, device="cuda")
+        check(lib().hw_learned_init_forward(self._h, Fl._p(feats), feats.shape[0], Fl._p(out), Fl._stream()))
+        return out
+
+    def proposal(self, pool, out):
+        P = torch.empty((pool.lanes, 15, abi.LANE), dtype=torch.float32, device="cuda")
+        check(lib().hw_learned_init_proposal(self._h, pool.lanes, Fl._p(out), Fl._p(pool.hist), Fl._p(P),
+                                             Fl._stream()))
+        return P
+
+    def gradients(self, feats, tgts, index=None):
+        g = torch.empty(self.n_params, dtype=torch.float32, device="cuda")
+        loss = C.c_float()
+        n = feats.shape[0] if index is None else index.shape[0]
+        check(lib().hw_learned_init_gradients(self._h, Fl._p(feats), Fl._p(tgts), Fl._p(index), n, Fl._p(g),
+                                              C.byref(loss), Fl._stream()))
+        return loss.value, g
+
+    def train(self, feats, tgts, epochs=20, batch=4096, lr=1e-3, weight_decay=0.01, seed=0, log=None,
+              lr_final=1e-5):
+        """AdamW over shuffled mini-batches (the shuffle is an index permutation
+        drawn on the host; the kernels gather the rows), with the learning
+        rate decaying from lr to lr_final on a cosine over all steps."""
+        n = feats.shape[0]
+        rng = np.random.default_rng(seed)
+        loss = C.c_float()
+        history = []
+        per_epoch = max(n // batch, 1)
+        total = epochs * per_epoch
+        step = 0
+        for ep in range(epochs):
+            perm = torch.from_numpy(rng.permutation(n).astype(np.int32)).cuda()
+            tot, steps = 0.0, 0
+            for i0 in range(0, n - batch + 1, batch):
+                idx = perm[i0:i0 + batch]
+                lr_t = lr_final + 0.5 * (lr - lr_final) * (1.0 + np.cos(np.pi * step / max(total, 1)))
+                step += 1
+                check(lib().hw_learned_init_train_step(self._h, Fl._p(feats), Fl._p(tgts), Fl._p(idx), batch, lr_t,
+                                                       weight_decay, C.byref(loss), Fl._stream()))
+                tot += loss.value
+                steps += 1
+            history.append(tot / max(steps, 1))
+            if log:
+                log(f"epoch {ep}: loss {history[-1]:.5f}")
+        return history
+
+
+def _pools(cfg, n_pools, lanes, first_id, seed):
+    return [estimate_inputs(cfg, lanes, pool_id=first_id + i, seed=seed) for i in range(n_pools)]
+
+
+def dataset(pools, fit_iters):
+    """Features, targets and plain fixed points of a list of pools."""
+    feats, tgts, fixed = [], [], []
+    for p in pools:
+        params, _, _ = fit(p, start=0, max_iter=fit_iters)
+        feats.append(features(p))
+        tgts.append(targets(p, params))
+        fixed.append(params)
+    return torch.cat(feats), torch.cat(tgts), fixed
+
+
+def param_distance(a, b):
+    """Largest relative distance over the 15 EM parameters of each ZMW
+    ([lanes][15][64] arrays), floors 0.01 / 1 DN / 1 DN^2 as in hw_dme_em_fit."""
+    floor = np.array([0.01] * 5 + [1.0] * 10, np.float32)[None, :, None]
+    return (np.abs(a - b) / np.maximum(np.abs(b), floor)).max(1)
+
+
+def evaluate(net, pools, fixed, fit_iters, tol=1e-4, settle=100):
+    """EM iterations to the plain fixed point at `tol`, from the plain and the
+    learned start (with fallback), on pools not used for training.  A ZMW is
+    resolved when its plain EM comes within tol of its own fixed point at
+    least `settle` iterations before the end of the budget."""
+    plain_it, learned_it, fell, final_ok, conv_plain, conv_learned, resolved_all = [], [], [], [], [], [], []
+    step_plain, step_learned = [], []
+    for p, tgt in zip(pools, fixed):
+        _, ip, _ = fit(p, start=0, target=tgt, tol=tol, max_iter=fit_iters)
+        out = net.forward(features(p))
+        prop = net.proposal(p, out)
+        pl, il, _ = fit(p, start=abi.EM_START_BETTER, proposal=prop, target=tgt, tol=tol, max_iter=fit_iters)
+        ip, il = ip.cpu().numpy(), il.cpu().numpy()
+        res = (ip[:, 1] >= 0) & (ip[:, 1] <= fit_iters - settle)
+        resolved_all.append(res.ravel())
+        plain_it.append(ip[:, 1][res])
+        learned_it.append(np.where(il[:, 1] < 0, fit_iters, il[:, 1])[res])
+        fell.append(il[:, 2].ravel())
+        final_ok.append((param_distance(pl.cpu().numpy(), tgt.cpu().numpy()) <= tol)[res])
+        conv_plain.append(ip[:, 0][ip[:, 0] >= 0])
+        conv_learned.append(il[:, 0][il[:, 0] >= 0])
+        step_plain.append(np.where(ip[:, 4] < 0, fit_iters, ip[:, 4])[res])
+        step_learned.append(np.where(il[:, 4] < 0, fit_iters, il[:, 4])[res])
+    cat = np.concatenate
+    pi, li = cat(plain_it).astype(np.float64), cat(learned_it).astype(np.float64)
+    return {
+        "zmws": int(cat(resolved_all).size),
+        "resolved_fraction": float(cat(resolved_all).mean()),
+        "em_iters_plain_mean": float(pi.mean()),
+        "em_iters_learned_mean": float(li.mean()),
+        "em_iters_ratio": float(pi.mean() / max(li.mean(), 1e-9)),
+        "fallback_rate": float(cat(fell).mean()),
+        "final_within_tol_fraction": float(cat(final_ok).mean()),
+        "tol": tol,
+        "fit_iters": fit_iters,
+        "reference_criterion_iters_plain_mean": float(cat(conv_plain).mean()),
+        "reference_criterion_iters_learned_mean": float(cat(conv_learned).mean()),
+        "step_criterion_iters_plain_mean": float(cat(step_plain).mean()),
+        "step_criterion_iters_learned_mean": float(cat(step_learned).mean()),
+    }
+
+
+def run(train_pools=8, eval_pools=1, lanes=4096, fit_iters=1000, epochs=40, batch=4096, lr=1e-3, seed=7, log=None):
+    """Generate, label, train and evaluate; returns (network, metrics)."""
+    cfg = data_config()
+    train = _pools(cfg, train_pools, lanes, 0, seed)
+    feats, tgts, _ = dataset(train, fit_iters)
+    del train
+    net = Network(max_batch=batch, seed=seed)
+    net.fit_normalization(feats, tgts)
+    history = net.train(feats, tgts, epochs=epochs, batch=batch, lr=lr, seed=seed, log=log)
+    del feats, tgts
+    held = _pools(cfg, eval_pools, lanes, 1000, seed)
+    fixed = [fit(p, start=0, max_iter=fit_iters)[0] for p in held]
+    metrics = evaluate(net, held, fixed, fit_iters)
+    metrics["train_zmws"] = train_pools * lanes * abi.LANE
+    metrics["final_train_loss"] = history[-1] if history else None
+    return net, metrics
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="train and evaluate the learned DME initializer")
+    ap.add_argument("--train-pools", type=int, default=8)
+    ap.add_argument("--eval-pools", type=int, default=1)
+    ap.add_argument("--lanes", type=int, default=4096)
+    ap.add_argument("--fit-iters", type=int, default=1000)
+    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--save", default=None)
+    a = ap.parse_args()
+    net, m = run(a.train_pools, a.eval_pools, a.lanes, a.fit_iters, a.epochs, log=print)
+    if a.save:
+        net.save(a.save)
+    print(json.dumps(m))

@@ -58,6 +58,21 @@ def lib():
         "hw_dme_init_models": ([vp, vp, vp, vp], C.c_int),
         "hw_dme_estimate": ([vp, vp, vp, FI, FI, vp, vp, vp], C.c_int),
         "hw_dme_estimate_noalloc": ([PCFG, u32, vp, vp, FI, FI, vp, vp, vp], C.c_int),
+        "hw_dme_em_fit_scratch_bytes": ([u32, C.POINTER(C.c_uint64)], C.c_int),
+        "hw_dme_em_fit": ([PCFG, u32, vp, vp, FI, FI, vp, C.c_int, vp, vp, C.c_float, u32, vp, vp, vp, vp, vp],
+                          C.c_int),
+        "hw_learned_init_create": ([u32, C.c_uint64, PPV], C.c_int),
+        "hw_learned_init_destroy": ([vp], C.c_int),
+        "hw_learned_init_param_count": ([C.POINTER(u32)], C.c_int),
+        "hw_learned_init_get_params": ([vp, vp, vp], C.c_int),
+        "hw_learned_init_set_params": ([vp, vp, vp], C.c_int),
+        "hw_learned_init_features": ([u32, vp, vp, vp, vp], C.c_int),
+        "hw_learned_init_targets": ([PCFG, u32, vp, vp, vp, vp], C.c_int),
+        "hw_learned_init_forward": ([vp, vp, u32, vp, vp], C.c_int),
+        "hw_learned_init_proposal": ([vp, u32, vp, vp, vp, vp], C.c_int),
+        "hw_learned_init_gradients": ([vp, vp, vp, vp, u32, vp, C.POINTER(C.c_float), vp], C.c_int),
+        "hw_learned_init_train_step": ([vp, vp, vp, vp, u32, C.c_float, C.c_float, C.POINTER(C.c_float), vp],
+                                       C.c_int),
         "hw_labeler_create": ([PCFG, u32, u32, u32, PPV], C.c_int),
         "hw_labeler_destroy": ([vp], C.c_int),
         "hw_labeler_process": ([vp, vp, vp, vp, vp, vp, vp], C.c_int),

@@ -338,6 +338,80 @@ int hw_dme_estimate_noalloc(const hw_config* cfg, uint32_t lanes, const hw_lane_
                             hw_frame_interval model_fi, hw_lane_model* d_models, hw_dme_diag* d_diag,
                             void* stream);
 
+/* ---- EM fit of single ZMWs, for the learned initializer ------------------
+ * No counterpart in the reference.  Runs the EM steps of hw_dme_estimate
+ * (same arithmetic) for every ZMW on its own for exactly max_iter iterations,
+ * with no lane-wide stopping rule and no final confidence blend, from
+ *   HW_EM_START_PLAIN     the reference's own start (PrelimEstimate and
+ *                         ScaleModelSnr of d_models, DmeEmHost.cpp:161-361),
+ *   HW_EM_START_PROPOSAL  d_proposal,
+ *   HW_EM_START_BETTER    d_proposal unless its log-likelihood is lower than
+ *                         (or not comparable with) the plain start's, in which
+ *                         case the plain start is used ("fell back").
+ * Per-lane layouts (floats unless stated): d_proposal, d_target, d_params
+ * [15][64] = mixture fractions, means and variances of the baseline and the
+ * four analog modes; d_iters int32 [5][64] = first iteration that passes the
+ * reference's convergence test (or -1), first iteration whose parameters are
+ * within `tol` of d_target (relative, with floors 0.01 / 1 DN / 1 DN^2 under
+ * fractions / means / variances; -1 if never, max_iter if only the final
+ * parameters are), fell back (0/1), status bits, and the number of
+ * iterations after which one update first changed the parameters by at most
+ * `tol` (same relative measure; -1 if never); d_loglike [3][64] = log-
+ * likelihood of the plain start, of the start used, and of the last
+ * iteration.  d_target may be NULL.  d_scratch holds
+ * hw_dme_em_fit_scratch_bytes(lanes) bytes.  Asynchronous. */
+typedef enum hw_em_start {
+    HW_EM_START_PLAIN = 0,
+    HW_EM_START_PROPOSAL = 1,
+    HW_EM_START_BETTER = 2
+} hw_em_start;
+int hw_dme_em_fit_scratch_bytes(uint32_t lanes, uint64_t* bytes);
+int hw_dme_em_fit(const hw_config* cfg, uint32_t lanes, const hw_lane_histogram* d_hist,
+                  const hw_baseliner_stats* d_stats, hw_frame_interval hist_fi, hw_frame_interval model_fi,
+                  const hw_lane_model* d_models, int start, const float* d_proposal, const float* d_target,
+                  float tol, uint32_t max_iter, float* d_scratch, float* d_params, int32_t* d_iters,
+                  float* d_loglike, void* stream);
+
+/* ---- Learned DME initializer (no counterpart in the reference) ----------
+ * A 302 -> 256 -> 256 -> 19 MLP with BF16 weights and activations, FP32
+ * accumulation and GELU (tanh form) that proposes each ZMW's EM start from
+ * its trace histogram and baseline statistics; hw_dme_em_fit with
+ * HW_EM_START_BETTER runs the EM from the proposal and falls back to the
+ * reference start when the proposal's log-likelihood is lower.
+ * Rows: features [n][304] (300 sqrt bin shares, baseline mean and variance
+ * in bin units, 2 zero pads), raw targets and outputs [n][32] (19 used:
+ * baseline mean, log variance, 4 analog means, 4 log analog variances, 5
+ * mixture fractions, 4 excess-noise terms; means in bins above the
+ * histogram's low bound, variances in squared bins).  Network outputs are
+ * standardised by the output mean/scale of the normalisation block
+ * [in mean 304][in scale 304][out mean 32][out scale 32]. */
+typedef struct hw_learned_init hw_learned_init;
+int hw_learned_init_create(uint32_t max_batch, uint64_t seed, hw_learned_init** out);
+int hw_learned_init_destroy(hw_learned_init* h);
+int hw_learned_init_param_count(uint32_t* count);
+/* FP32 parameters (W1 [256][304], b1, W2 [256][256], b2, W3 [32][256], b3)
+ * and the normalisation block, to or from host memory (either may be NULL). */
+int hw_learned_init_get_params(const hw_learned_init* h, float* host_params, float* host_norm);
+int hw_learned_init_set_params(hw_learned_init* h, const float* host_params, const float* host_norm);
+int hw_learned_init_features(uint32_t lanes, const hw_lane_histogram* d_hist, const hw_baseliner_stats* d_stats,
+                             float* d_features, void* stream);
+/* Targets from fitted parameters d_params [lanes][15][64] (hw_dme_em_fit layout). */
+int hw_learned_init_targets(const hw_config* cfg, uint32_t lanes, const float* d_params,
+                            const hw_lane_histogram* d_hist, float* d_targets, void* stream);
+/* Standardised outputs of n rows (processed max_batch rows at a time). */
+int hw_learned_init_forward(hw_learned_init* h, const float* d_features, uint32_t n, float* d_out, void* stream);
+/* EM start [lanes][15][64] from the outputs of lanes * 64 rows. */
+int hw_learned_init_proposal(const hw_learned_init* h, uint32_t lanes, const float* d_out,
+                             const hw_lane_histogram* d_hist, float* d_proposal, void* stream);
+/* Mean-squared-error gradients of n <= max_batch rows (rows d_index[i] when
+ * d_index is not NULL); synchronous, *loss receives the loss. */
+int hw_learned_init_gradients(hw_learned_init* h, const float* d_features, const float* d_targets,
+                              const int32_t* d_index, uint32_t n, float* d_grad, float* loss, void* stream);
+/* One AdamW step (betas 0.9/0.999, eps 1e-8, decay on weight matrices). */
+int hw_learned_init_train_step(hw_learned_init* h, const float* d_features, const float* d_targets,
+                               const int32_t* d_index, uint32_t n, float lr, float weight_decay, float* loss,
+                               void* stream);
+
 /* ---- Frame labeler (FrameLabeler.h:67-74, FrameLabelerHost.cpp:314-612) - */
 typedef struct hw_labeler hw_labeler;
 int hw_labeler_create(const hw_config* cfg, uint32_t pool_id, uint32_t lanes,
