@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-learned-init", action="store_true",
+                    help="skip the learned DME initializer measurement (config 3)")
     return ap.parse_args()
 
 
@@ -64,19 +66,8 @@ def dist_setup():
 
 
 def startup_chunks(cfg, pools):
-    """Chunks until every pool has entered its periodic estimation cycle."""
-    from hw_b200 import abi, native
-    import ctypes as C
-    b = C.c_void_p()
-    native.check(native.lib().hw_baseliner_create(C.byref(cfg), 0, 1, FRAMES, C.byref(b)))
-    lat = C.c_uint32()
-    native.lib().hw_baseliner_startup_latency(b, C.byref(lat))
-    native.lib().hw_baseliner_destroy(b)
-    chunks_per_est = (max(cfg.min_frames_for_estimate, 1) + FRAMES - 1) // FRAMES
-    last_delay = ((pools - 1) % chunks_per_est) * FRAMES
-    start = (lat.value + last_delay + FRAMES - 1) // FRAMES          # first chunk the last pool analyses
-    pre = (cfg.num_frames_pre_accum_stats + FRAMES - 1) // FRAMES    # histogram start-up
-    return start + pre + chunks_per_est
+    from hw_b200.workloads import startup_chunks as sc
+    return sc(cfg, pools, FRAMES)
 
 
 class ClockSampler:
@@ -349,6 +340,18 @@ def main():
                "sample": f"{args.cpu_lanes} lanes ({args.cpu_lanes * 64} ZMWs) x {args.cpu_steps} "
                          f"steady-state 512-frame chunks after start-up ({secs:.1f} s)"}
 
+    for a in analyzers:
+        a.close()
+    learned = None
+    if rank == 0 and world == 1 and not args.no_learned_init:
+        # BASELINE metric part 2: EM iterations from the learned start vs the
+        # plain start (2.1M training ZMWs of the uneven-pool generator,
+        # 262K held-out ZMWs), measured after the timed regions.
+        from hw_b200 import learned_init
+        t0 = time.time()
+        _, learned = learned_init.run()
+        learned["seconds"] = time.time() - t0
+
     if rank == 0:
         out = {
             "metric": "ZMW-frames/s", "value": value, "unit": "ZMW-frames/s", "n_gpus": world,
@@ -361,10 +364,9 @@ def main():
             "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
             "clocks": clk,
             "stage_ms": {k: v[0] / K for k, v in stage.items()},
+            "learned_init": learned,
         }
         print(json.dumps(out), flush=True)
-    for a in analyzers:
-        a.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

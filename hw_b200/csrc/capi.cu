@@ -434,6 +434,22 @@ int hw_dme_estimate(hw_dme* d, const hw_lane_histogram* d_hist, const hw_baselin
     return HW_OK;
 }
 
+int hw_dme_estimate_proposal(hw_dme* d, const hw_lane_histogram* d_hist, const hw_baseliner_stats* d_stats,
+                             hw_frame_interval hist_fi, hw_frame_interval model_fi, hw_lane_model* d_models,
+                             hw_dme_diag* d_diag, const float* d_proposal, void* stream)
+{
+    if (!d || !d_hist || !d_stats || !d_models || !d_proposal) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    if (hist_fi.lower == hist_fi.upper || model_fi.lower == model_fi.upper)
+        return Fail(HW_ERR_INVALID_ARG, "frame intervals must not be empty");
+    DmeArgs a{d_hist, d_stats, d_models, d_diag, d->scratch, d->err, (int)d->lanes,
+              model_fi.lower + (model_fi.upper - model_fi.lower) / 2,
+              hist_fi.lower + (hist_fi.upper - hist_fi.lower) / 2, d_proposal};
+    HW_CUDA(LaunchDmeEstimate(a, d->k, S(stream)), "hw_dme_estimate_proposal");
+    int e = TakeDeviceError(d->err, S(stream), "hw_dme_estimate_proposal");
+    if (e) return Fail(e, "DME: a reference sanity assertion failed (non-finite estimate or bad SNR-drop threshold)");
+    return HW_OK;
+}
+
 // ---- Frame labeler ---------------------------------------------------------------
 
 int hw_labeler_create(const hw_config* cfg, uint32_t pool_id, uint32_t lanes, uint32_t frames_per_chunk,
@@ -591,6 +607,11 @@ struct hw_analyzer
     hw_stat_accum_state* paStats = nullptr;
     hw_dme_diag* diag = nullptr;
     bool diagValid = false;
+    // learned EM start (hw_analyzer_set_learned_init), not owned
+    hw_learned_init* net = nullptr;
+    float* lFeat = nullptr;     // [lanes * 64][304]
+    float* lOut = nullptr;      // [lanes * 64][32]
+    float* lProp = nullptr;     // [lanes][15][64]
     hw_frame_interval modelFi{0, 0};
     int status = HIST_INIT;
     int32_t framesRemaining = 0;
@@ -642,6 +663,7 @@ struct hw_analyzer
         hw_pulse_accumulator_destroy(pa);
         cudaFree(bls); cudaFree(stats); cudaFree(models); cudaFree(labels); cudaFree(latent);
         cudaFree(score); cudaFree(paStats); cudaFree(diag);
+        cudaFree(lFeat); cudaFree(lOut); cudaFree(lProp);
     }
 
     // DetectionModelEstimator::AddBatch
@@ -673,7 +695,15 @@ struct hw_analyzer
             {
                 *ran = true;
                 t = Begin(HW_STAGE_DME, s);
-                if ((rc = hw_dme_estimate(dme, hist->hist, agg->acc, hist->fi, modelFi, models, diag, s))) return rc;
+                if (net)
+                {
+                    if ((rc = hw_learned_init_features(lanes, hist->hist, agg->acc, lFeat, s))) return rc;
+                    if ((rc = hw_learned_init_forward(net, lFeat, lanes * kLane, lOut, s))) return rc;
+                    if ((rc = hw_learned_init_proposal(net, lanes, lOut, hist->hist, lProp, s))) return rc;
+                    if ((rc = hw_dme_estimate_proposal(dme, hist->hist, agg->acc, hist->fi, modelFi, models, diag,
+                                                       lProp, s))) return rc;
+                }
+                else if ((rc = hw_dme_estimate(dme, hist->hist, agg->acc, hist->fi, modelFi, models, diag, s))) return rc;
                 End(t, s);
                 diagValid = true;
                 modelFi = hist->fi;
@@ -748,6 +778,21 @@ int hw_analyzer_create(const hw_config* cfg, uint32_t pool_id, uint32_t lanes, u
     const uint32_t chunksPerEstimate = (std::max(cfg->min_frames_for_estimate, 1u) + frames_per_chunk - 1) / frames_per_chunk;
     a->poolDelay = (int32_t)((pool_id % chunksPerEstimate) * frames_per_chunk);
     *out = a.release();
+    return HW_OK;
+}
+
+int hw_analyzer_set_learned_init(hw_analyzer* a, hw_learned_init* net)
+{
+    if (!a) return Fail(HW_ERR_INVALID_ARG, "NULL analyzer");
+    if (net && !a->lFeat)
+    {
+        const size_t n = (size_t)a->lanes * kLane;
+        int rc;
+        if ((rc = DevAlloc(&a->lFeat, n * 304, "hw_analyzer_set_learned_init"))) return rc;
+        if ((rc = DevAlloc(&a->lOut, n * 32, "hw_analyzer_set_learned_init"))) return rc;
+        if ((rc = DevAlloc(&a->lProp, (size_t)a->lanes * 15 * kLane, "hw_analyzer_set_learned_init"))) return rc;
+    }
+    a->net = net;
     return HW_OK;
 }
 

@@ -524,6 +524,34 @@ __device__ __forceinline__ void EmMStep(const KParams& k, const EmHist& h, const
     for (int a = 0; a < kAnalogs; ++a) v.var[a + 1] = SignalCovar(k, k.cv2[a], v.mu[a + 1], v0);
 }
 
+// The learned start: replaces the reference start v by the proposal column Q
+// unless the proposal's log-likelihood is lower (or not comparable); returns
+// 1 when it kept the reference start.  Reports both log-likelihoods.
+__device__ __forceinline__ int ChooseStart(const KParams& k, const EmHist& h, const EmReg& r, const float* Q, bool fallback,
+                                           float* bpS, float* tau0S, float* facS, EmVars& v, float& llPlain,
+                                           float& llStart)
+{
+    const int z = h.z;
+    float ci[5], mom1[5], varinv[5];
+    bool safe;
+    llPlain = EmEStep(k, h, v, r, bpS, tau0S, facS, ci, mom1, varinv, safe);
+    llStart = llPlain;
+    EmVars p;
+#pragma unroll
+    for (int i = 0; i < 5; ++i)
+    {
+        p.rho[i] = Q[i * kLane + z];
+        p.mu[i] = Q[(5 + i) * kLane + z];
+        p.var[i] = Q[(10 + i) * kLane + z];
+    }
+    p.s = EmScale(k, p.mu);
+    const float llProp = EmEStep(k, h, p, r, bpS, tau0S, facS, ci, mom1, varinv, safe);
+    if (fallback && !(llProp >= llPlain)) return 1;
+    v = p;
+    llStart = llProp;
+    return 0;
+}
+
 __global__ void __launch_bounds__(kLane, 12) DmeEstimateKernel(DmeArgs A, KParams k)
 {
     const int l = blockIdx.x;
@@ -538,6 +566,11 @@ __global__ void __launch_bounds__(kLane, 12) DmeEstimateKernel(DmeArgs A, KParam
     EmVars v;
     EmReg r;
     DmePrelude(k, A.models[l], A.stats[l], h, A.tModel, A.tEst, det, v, r);
+    if (A.proposal)
+    {
+        float llPlain, llStart;
+        ChooseStart(k, h, r, A.proposal + (size_t)l * 15 * kLane, true, bpS, tau0S, facS, v, llPlain, llStart);
+    }
 
     // Values needed only before and after the EM iterations (the prior model
     // and the estimates at the latest converged iteration) wait in per-thread
@@ -745,29 +778,15 @@ __global__ void __launch_bounds__(kLane, 12) DmeEmFitKernel(DmeFitArgs A, KParam
 
     float ci[5], mom1[5], varinv[5];
     bool safe;
-    const float llPlain = EmEStep(k, h, v, r, bpS, tau0S, facS, ci, mom1, varinv, safe);
-    float llStart = llPlain;
+    float llPlain, llStart;
     int fellBack = 0;
     if (A.mode != HW_EM_START_PLAIN)
+        fellBack = ChooseStart(k, h, r, A.proposal + (size_t)l * 15 * kLane, A.mode == HW_EM_START_BETTER, bpS, tau0S,
+                               facS, v, llPlain, llStart);
+    else
     {
-        const float* Q = A.proposal + (size_t)l * 15 * kLane;
-        EmVars p;
-#pragma unroll
-        for (int i = 0; i < 5; ++i)
-        {
-            p.rho[i] = Q[i * kLane + z];
-            p.mu[i] = Q[(5 + i) * kLane + z];
-            p.var[i] = Q[(10 + i) * kLane + z];
-        }
-        p.s = EmScale(k, p.mu);
-        const float llProp = EmEStep(k, h, p, r, bpS, tau0S, facS, ci, mom1, varinv, safe);
-        const bool usePlain = (A.mode == HW_EM_START_BETTER) && !(llProp >= llPlain);
-        if (usePlain) fellBack = 1;
-        else
-        {
-            v = p;
-            llStart = llProp;
-        }
+        llPlain = EmEStep(k, h, v, r, bpS, tau0S, facS, ci, mom1, varinv, safe);
+        llStart = llPlain;
     }
     const float* T = A.target ? A.target + (size_t)l * 15 * kLane : nullptr;
     int zStatus = (h.total < 160u) ? 2 : 0;

@@ -122,6 +122,9 @@ struct DmeArgs
     int* err;
     int lanes;
     int32_t tModel, tEst;       // frame-interval centers (model, histogram)
+    // Optional EM start [lanes][15][64] (fractions, means, variances), used
+    // per ZMW unless its log-likelihood is below the reference start's.
+    const float* proposal = nullptr;
 };
 
 struct LabelerArgs

@@ -30,26 +30,45 @@ constexpr int kOutUsed = 19;
 // bins) of the baseliner statistics.  Everything is in units of the
 // histogram's own bin size, which the histogram reset ties to the baseline
 // sigma, so the features do not depend on the trace's offset or gain.
-__global__ void FeaturesKernel(const hw_lane_histogram* __restrict__ hist, const hw_baseliner_stats* __restrict__ st,
-                               float* __restrict__ out)
+// One CTA of 256 threads per lane: the first 64 threads reduce the per-ZMW
+// totals, then the lane's 64 x 304 features are written row after row, so
+// consecutive threads write consecutive addresses.
+constexpr int kFeatThreads = 256;
+
+__global__ void __launch_bounds__(kFeatThreads) FeaturesKernel(const hw_lane_histogram* __restrict__ hist,
+                                                               const hw_baseliner_stats* __restrict__ st,
+                                                               float* __restrict__ out)
 {
-    const int l = blockIdx.x, z = threadIdx.x;
+    const int l = blockIdx.x, tid = threadIdx.x;
     const hw_lane_histogram& H = hist[l];
-    float* f = out + ((size_t)l * kLane + z) * kFeat;
-    float total = 0.0f;
-    for (int b = 0; b < kBins; ++b) total += (float)H.bin_count[b][z];
-    const float inv = total > 0.0f ? 1.0f / total : 0.0f;
-    for (int b = 0; b < kBins; ++b) f[b] = sqrtf((float)H.bin_count[b][z] * inv);
-    const float lb = H.low_bound[z], bs = H.bin_size[z];
-    const hw_stat_accum_state& S = st[l].baseline_stats;
-    const float m0 = S.moment0[z], m1 = S.moment1[z], m2 = S.moment2[z];
-    float mean = m0 > 0.0f ? m1 / m0 + S.offset[z] : lb;
-    float var = m0 > 1.0f ? fmaxf((m2 - m1 * m1 / m0) / (m0 - 1.0f), 0.0f) : bs * bs;
-    float fm = (mean - lb) / bs, fv = var / (bs * bs);
-    f[300] = isfinite(fm) ? fm : 0.0f;
-    f[301] = isfinite(fv) ? fv : 0.0f;
-    f[302] = 0.0f;
-    f[303] = 0.0f;
+    __shared__ float inv[kLane], fMean[kLane], fVar[kLane];
+    if (tid < kLane)
+    {
+        const int z = tid;
+        float total = 0.0f;
+        for (int b = 0; b < kBins; ++b) total += (float)H.bin_count[b][z];
+        inv[z] = total > 0.0f ? 1.0f / total : 0.0f;
+        const float lb = H.low_bound[z], bs = H.bin_size[z];
+        const hw_stat_accum_state& S = st[l].baseline_stats;
+        const float m0 = S.moment0[z], m1 = S.moment1[z], m2 = S.moment2[z];
+        const float mean = m0 > 0.0f ? m1 / m0 + S.offset[z] : lb;
+        const float var = m0 > 1.0f ? fmaxf((m2 - m1 * m1 / m0) / (m0 - 1.0f), 0.0f) : bs * bs;
+        const float fm = (mean - lb) / bs, fv = var / (bs * bs);
+        fMean[z] = isfinite(fm) ? fm : 0.0f;
+        fVar[z] = isfinite(fv) ? fv : 0.0f;
+    }
+    __syncthreads();
+    float* f = out + (size_t)l * kLane * kFeat;
+    for (int e = tid; e < kLane * kFeat; e += kFeatThreads)
+    {
+        const int z = e / kFeat, b = e % kFeat;
+        float v;
+        if (b < kBins) v = sqrtf((float)H.bin_count[b][z] * inv[z]);
+        else if (b == kBins) v = fMean[z];
+        else if (b == kBins + 1) v = fVar[z];
+        else v = 0.0f;
+        f[e] = v;
+    }
 }
 
 // Training targets from fitted EM parameters params [lanes][15][64]:
@@ -523,7 +542,7 @@ int hw_learned_init_features(uint32_t lanes, const hw_lane_histogram* d_hist, co
                              float* d_features, void* stream)
 {
     if (!d_hist || !d_stats || !d_features || lanes == 0) return SetLastError(HW_ERR_INVALID_ARG, "bad argument");
-    FeaturesKernel<<<lanes, kLane, 0, (cudaStream_t)stream>>>(d_hist, d_stats, d_features);
+    FeaturesKernel<<<lanes, kFeatThreads, 0, (cudaStream_t)stream>>>(d_hist, d_stats, d_features);
     return Cuda(cudaGetLastError(), "hw_learned_init_features");
 }
 

@@ -150,6 +150,14 @@ class DmeEmEstimator(_Handle):
                                     abi.FrameInterval(*model_fi), _p(models), _p(d), _stream()))
         return d
 
+    def estimate_proposal(self, hist, hist_fi, stats, models, model_fi, proposal, diag=True):
+        """estimate() from a learned start [lanes][15][64] (hw_dme_estimate_proposal)."""
+        d = struct_buffer(abi.DME_DIAG_DT, self.lanes) if diag else None
+        check(lib().hw_dme_estimate_proposal(self._h, _p(hist), _p(stats), abi.FrameInterval(*hist_fi),
+                                             abi.FrameInterval(*model_fi), _p(models), _p(d), _p(proposal),
+                                             _stream()))
+        return d
+
 
 def em_fit(cfg, lanes, hist, stats, hist_fi, model_fi, models, start=0, proposal=None, target=None, tol=1e-4,
            max_iter=20, scratch=None):
@@ -233,6 +241,12 @@ class BatchAnalyzer(_Handle):
         return pulses, lens, ovf, bool(em.value), bool(est.value)
 
     STAGES = ("baseline", "aggregate", "histogram", "model_init", "dme", "hist_reset", "labeler", "pulses")
+
+    def set_learned_init(self, net):
+        """Start every estimate from `net`'s proposal (a learned_init.Network,
+        kept alive by the caller); None restores the reference start."""
+        check(lib().hw_analyzer_set_learned_init(self._h, None if net is None else net._h))
+        self._net = net
 
     def profile(self, enable=True):
         check(lib().hw_analyzer_profile(self._h, 1 if enable else 0))

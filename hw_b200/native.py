@@ -58,6 +58,8 @@ def lib():
         "hw_dme_init_models": ([vp, vp, vp, vp], C.c_int),
         "hw_dme_estimate": ([vp, vp, vp, FI, FI, vp, vp, vp], C.c_int),
         "hw_dme_estimate_noalloc": ([PCFG, u32, vp, vp, FI, FI, vp, vp, vp], C.c_int),
+        "hw_dme_estimate_proposal": ([vp, vp, vp, FI, FI, vp, vp, vp, vp], C.c_int),
+        "hw_analyzer_set_learned_init": ([vp, vp], C.c_int),
         "hw_dme_em_fit_scratch_bytes": ([u32, C.POINTER(C.c_uint64)], C.c_int),
         "hw_dme_em_fit": ([PCFG, u32, vp, vp, FI, FI, vp, C.c_int, vp, vp, C.c_float, u32, vp, vp, vp, vp, vp],
                           C.c_int),

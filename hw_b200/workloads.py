@@ -97,3 +97,22 @@ def small_config():
     cfg.min_frames_for_estimate = 2048
     cfg.model_estimation_mode = abi.INITIAL_ESTIMATIONS
     return cfg
+
+
+def startup_chunks(cfg, pools, frames=512):
+    """Chunks of `frames` until every one of `pools` pools of the dynamic
+    schedule has entered its periodic estimation cycle: the baseliner's
+    start-up latency, the stagger of the last pool, the statistics
+    pre-accumulation and one estimation period."""
+    import ctypes as C
+    from . import native
+    b = C.c_void_p()
+    native.check(native.lib().hw_baseliner_create(C.byref(cfg), 0, 1, frames, C.byref(b)))
+    lat = C.c_uint32()
+    native.lib().hw_baseliner_startup_latency(b, C.byref(lat))
+    native.lib().hw_baseliner_destroy(b)
+    chunks_per_est = (max(cfg.min_frames_for_estimate, 1) + frames - 1) // frames
+    last_delay = ((pools - 1) % chunks_per_est) * frames
+    start = (lat.value + last_delay + frames - 1) // frames          # first chunk the last pool analyses
+    pre = (cfg.num_frames_pre_accum_stats + frames - 1) // frames    # histogram start-up
+    return start + pre + chunks_per_est

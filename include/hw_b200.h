@@ -333,6 +333,16 @@ int hw_dme_estimate(hw_dme* d, const hw_lane_histogram* d_hist, const hw_baselin
  * array: calls that overlap on the GPU (different streams, threads or
  * processes sharing a context) race.  Synchronous like hw_dme_estimate.
  * This entry point has no counterpart in the reference. */
+/* hw_dme_estimate from a learned EM start (no counterpart in the reference):
+ * d_proposal [lanes][15][64] (fractions, means, variances of the baseline and
+ * the four analogs, see hw_dme_em_fit) replaces the reference start for every
+ * ZMW whose proposal log-likelihood is not lower than the reference start's;
+ * everything else (lane-wide stopping rule, confidence, blend) is the
+ * reference's.  Synchronous like hw_dme_estimate. */
+int hw_dme_estimate_proposal(hw_dme* d, const hw_lane_histogram* d_hist, const hw_baseliner_stats* d_stats,
+                             hw_frame_interval hist_fi, hw_frame_interval model_fi, hw_lane_model* d_models,
+                             hw_dme_diag* d_diag, const float* d_proposal, void* stream);
+
 int hw_dme_estimate_noalloc(const hw_config* cfg, uint32_t lanes, const hw_lane_histogram* d_hist,
                             const hw_baseliner_stats* d_stats, hw_frame_interval hist_fi,
                             hw_frame_interval model_fi, hw_lane_model* d_models, hw_dme_diag* d_diag,
@@ -454,6 +464,10 @@ typedef struct hw_analyzer hw_analyzer;
 int hw_analyzer_create(const hw_config* cfg, uint32_t pool_id, uint32_t lanes, uint32_t frames_per_chunk,
                        hw_analyzer** out);
 int hw_analyzer_destroy(hw_analyzer* a);
+/* Makes an analyzer start every estimate from the network's proposal
+ * (hw_dme_estimate_proposal); NULL restores the reference start.  The network
+ * is not owned and must outlive its use. */
+int hw_analyzer_set_learned_init(hw_analyzer* a, hw_learned_init* net);
 /* BatchAnalyzer::operator(): d_trace[lanes][F][64] must be the next chunk
  * (first_frame == previous first_frame + F, starting at 0); otherwise
  * HW_ERR_FRAME_ORDER.  Pulses go to d_pulses[lanes][64][max_calls_per_zmw]

@@ -827,7 +827,8 @@ struct OraclePool
     }
 
     int Estimate(const hw_lane_histogram* h, const hw_baseliner_stats* stats, hw_frame_interval histFi_,
-                 hw_frame_interval modelFi, hw_lane_model* models, hw_dme_diag* diag);
+                 hw_frame_interval modelFi, hw_lane_model* models, hw_dme_diag* diag,
+                 const float* proposal = nullptr);
 
     // The DME's work before its EM iterations, for lane l (see the definition).
     using LaneEmRef = void*;
@@ -1068,6 +1069,39 @@ struct LaneEm
         }
     }
 
+    // The learned start: per ZMW, the proposal Q [15][64] replaces the current
+    // (reference) start unless `fallback` is set and the proposal's
+    // log-likelihood is lower (or not comparable).
+    void ChooseStart(const float* Q, bool fallback, int32_t* fellBack, float* llPlain, float* llStart)
+    {
+        float rho0[5][kLane], mu0[5][kLane], var0[5][kLane], s0[kLane], llProp[kLane];
+        EStep(llPlain);
+        std::memcpy(rho0, rho, sizeof(rho0));
+        std::memcpy(mu0, mu, sizeof(mu0));
+        std::memcpy(var0, var, sizeof(var0));
+        std::memcpy(s0, s, sizeof(s0));
+        FZ for (int k = 0; k < 5; ++k)
+        {
+            rho[k][z] = Q[k * kLane + z];
+            mu[k][z] = Q[(5 + k) * kLane + z];
+            var[k][z] = Q[(10 + k) * kLane + z];
+        }
+        SetScale();
+        EStep(llProp);
+        FZ
+        {
+            fellBack[z] = 0;
+            llStart[z] = llProp[z];
+            if (fallback && !(llProp[z] >= llPlain[z]))
+            {
+                for (int k = 0; k < 5; ++k) { rho[k][z] = rho0[k][z]; mu[k][z] = mu0[k][z]; var[k][z] = var0[k][z]; }
+                s[z] = s0[z];
+                fellBack[z] = 1;
+                llStart[z] = llPlain[z];
+            }
+        }
+    }
+
 private:
     float pref_[5][kLane];
 };
@@ -1197,7 +1231,7 @@ void OraclePool::DmePrelude(int64_t l, const hw_lane_histogram* hh, const hw_bas
 }
 
 int OraclePool::Estimate(const hw_lane_histogram* hh, const hw_baseliner_stats* stats, hw_frame_interval hfi,
-                         hw_frame_interval pfi, hw_lane_model* models, hw_dme_diag* diag)
+                         hw_frame_interval pfi, hw_lane_model* models, hw_dme_diag* diag, const float* proposal)
 {
     const DmeCtx c{&cfg, &d};
     int status = HW_OK;
@@ -1216,6 +1250,12 @@ int OraclePool::Estimate(const hw_lane_histogram* hh, const hw_baseliner_stats* 
             LaneEm& em = *emPtr;
             Model det;
             DmePrelude(l, hh, stats, hfi, pfi, models, det, &em);
+            if (proposal)
+            {
+                int32_t fb[kLane];
+                float l0[kLane], l1[kLane];
+                em.ChooseStart(proposal + (size_t)l * 15 * kLane, true, fb, l0, l1);
+            }
             UHist hist{&hh[l]};
             Model work;
             work.fi = hfi;
@@ -1413,38 +1453,15 @@ int OraclePool::EmFit(const hw_lane_histogram* hh, const hw_baseliner_stats* sta
             float* L = loglike + (size_t)l * 3 * kLane;
             const float* T = target ? target + (size_t)l * 15 * kLane : nullptr;
 
-            float llPlain[kLane], llProp[kLane], ll[kLane];
-            em.EStep(llPlain);
+            float llPlain[kLane], ll[kLane];
             int32_t fellBack[kLane], zStatus[kLane], tolIter[kLane], mIter[kLane], stepIter[kLane];
             float llStart[kLane];
-            FZ { fellBack[z] = 0; llStart[z] = llPlain[z]; }
             if (mode != 0)
+                em.ChooseStart(proposal + (size_t)l * 15 * kLane, mode == 2, fellBack, llPlain, llStart);
+            else
             {
-                float rho0[5][kLane], mu0[5][kLane], var0[5][kLane], s0[kLane];
-                std::memcpy(rho0, em.rho, sizeof(rho0));
-                std::memcpy(mu0, em.mu, sizeof(mu0));
-                std::memcpy(var0, em.var, sizeof(var0));
-                std::memcpy(s0, em.s, sizeof(s0));
-                const float* Q = proposal + (size_t)l * 15 * kLane;
-                FZ for (int k = 0; k < 5; ++k)
-                {
-                    em.rho[k][z] = Q[k * kLane + z];
-                    em.mu[k][z] = Q[(5 + k) * kLane + z];
-                    em.var[k][z] = Q[(10 + k) * kLane + z];
-                }
-                em.SetScale();
-                em.EStep(llProp);
-                FZ
-                {
-                    const bool usePlain = (mode == 2) && !(llProp[z] >= llPlain[z]);
-                    if (usePlain)
-                    {
-                        for (int k = 0; k < 5; ++k) { em.rho[k][z] = rho0[k][z]; em.mu[k][z] = mu0[k][z]; em.var[k][z] = var0[k][z]; }
-                        em.s[z] = s0[z];
-                        fellBack[z] = 1;
-                    }
-                    else llStart[z] = llProp[z];
-                }
+                em.EStep(llPlain);
+                FZ { fellBack[z] = 0; llStart[z] = llPlain[z]; }
             }
             float logLike[kLane], mLogLike[kLane], last[kLane];
             bool mConverged[kLane];
@@ -1916,6 +1933,12 @@ int or_label(void* p, const int16_t* tr, const hw_lane_model* m, int16_t* labels
 int or_pulses(void* p, const int16_t* labels, const int16_t* lat, const int16_t* tr, int32_t firstFrame,
               const hw_lane_model* m, hw_pulse* pulses, uint32_t* lens, uint32_t* ovf, hw_stat_accum_state* bs)
 { return static_cast<OraclePool*>(p)->Pulses(labels, lat, tr, firstFrame, m, pulses, lens, ovf, bs); }
+
+int or_dme_estimate_proposal(void* p, const hw_lane_histogram* h, const hw_baseliner_stats* s, hw_frame_interval hfi,
+                             hw_frame_interval mfi, hw_lane_model* m, hw_dme_diag* diag, const float* proposal)
+{
+    return static_cast<OraclePool*>(p)->Estimate(h, s, hfi, mfi, m, diag, proposal);
+}
 
 int or_em_fit(void* p, const hw_lane_histogram* h, const hw_baseliner_stats* s, hw_frame_interval hfi,
               hw_frame_interval mfi, const hw_lane_model* m, int mode, const float* proposal, const float* target,

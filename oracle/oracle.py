@@ -51,6 +51,7 @@ def lib():
         L.or_dme_estimate.argtypes = [vp, vp, vp, FI, FI, vp, vp]
         L.or_label.argtypes = [vp, vp, vp, vp, vp, vp]
         L.or_pulses.argtypes = [vp, vp, vp, vp, i32, vp, vp, vp, vp, vp]
+        L.or_dme_estimate_proposal.argtypes = [vp, vp, vp, FI, FI, vp, vp, vp]
         L.or_em_fit.argtypes = [vp, vp, vp, FI, FI, vp, C.c_int, vp, vp, C.c_float, u32, vp, vp, vp]
         L.or_static_model.argtypes = [C.POINTER(abi.Config), vp]
         L.or_extremum_stage.argtypes = [C.c_int, C.c_int, vp, C.c_int, C.c_int, vp]
@@ -153,6 +154,16 @@ class Pool:
         diag = np.zeros(self.lanes, abi.DME_DIAG_DT)
         _check(lib().or_dme_estimate(self.h, abi.ptr(hist), abi.ptr(stats), abi.FrameInterval(*hist_fi),
                                      abi.FrameInterval(*model_fi), abi.ptr(models), abi.ptr(diag)))
+        return models, diag
+
+    def estimate_proposal(self, hist, stats, hist_fi, model_fi, models, proposal):
+        """Estimate from a learned start (see hw_dme_estimate_proposal)."""
+        models = models.copy()
+        diag = np.zeros(self.lanes, abi.DME_DIAG_DT)
+        prop = np.ascontiguousarray(proposal, np.float32)
+        _check(lib().or_dme_estimate_proposal(self.h, abi.ptr(hist), abi.ptr(stats), abi.FrameInterval(*hist_fi),
+                                              abi.FrameInterval(*model_fi), abi.ptr(models), abi.ptr(diag),
+                                              abi.ptr(prop)))
         return models, diag
 
     def em_fit(self, hist, stats, hist_fi, model_fi, models, mode=0, proposal=None, target=None, tol=1e-4,

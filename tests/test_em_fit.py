@@ -106,3 +106,28 @@ def test_cuda_fit_matches_oracle(mode):
     assert np.array_equal(po.view(np.uint32), pg.cpu().numpy().view(np.uint32))
     assert np.array_equal(io, ig.cpu().numpy())
     assert np.array_equal(lo.view(np.uint32), lg.cpu().numpy().view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_cuda_estimate_from_proposal_matches_oracle():
+    """hw_dme_estimate_proposal: the reference estimate (lane-wide stop,
+    confidence, blend) from a learned start, bitwise against the oracle."""
+    import torch
+    from hw_b200 import abi, filters as Fl
+    cfg, be, (hist, stats, hfi, mfi, models) = _dme_inputs(seed=6)
+    lanes = hist.shape[0]
+    start, _, _ = be.p.em_fit(hist, stats, hfi, mfi, models, mode=0, max_iter=0)
+    ref, _, _ = be.p.em_fit(hist, stats, hfi, mfi, models, mode=0, max_iter=80)
+    prop = (0.7 * ref + 0.3 * start).astype(np.float32)
+    prop[:, 0:5] /= prop[:, 0:5].sum(1, keepdims=True)
+    mo, do = be.p.estimate_proposal(hist, stats, hfi, mfi, models, prop)
+    dme = Fl.DmeEmEstimator(cfg, 0, lanes)
+    m = Fl.numpy_to_struct(models)
+    d = dme.estimate_proposal(Fl.numpy_to_struct(hist), hfi, Fl.numpy_to_struct(stats), m, mfi,
+                              torch.from_numpy(prop).cuda())
+    assert np.array_equal(mo.view(np.uint8), Fl.struct_to_numpy(m, abi.LANE_MODEL_DT).view(np.uint8))
+    assert np.array_equal(do.view(np.uint8), Fl.struct_to_numpy(d, abi.DME_DIAG_DT).view(np.uint8))
+    # the reference start as proposal reproduces the reference estimate
+    mp, dp = be.p.estimate_proposal(hist, stats, hfi, mfi, models, start)
+    mr, dr = be.p.estimate(hist, stats, hfi, mfi, models)
+    assert np.array_equal(mp.view(np.uint8), mr.view(np.uint8))

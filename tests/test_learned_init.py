@@ -125,3 +125,31 @@ def test_training_beats_plain_start():
     assert m["step_criterion_iters_learned_mean"] <= m["step_criterion_iters_plain_mean"], m
     assert m["em_iters_learned_mean"] <= 1.05 * m["em_iters_plain_mean"], m
     assert m["fallback_rate"] < 0.5, m
+
+
+@pytest.mark.gpu
+def test_analyzer_with_learned_start_runs_dynamic_schedule():
+    """hw_analyzer_set_learned_init: a dynamic-estimation analyzer starts its
+    estimates from the network's proposal and still emits pulses and finite
+    models; detaching the network restores the reference start."""
+    import torch
+    from hw_b200 import abi, filters as Fl, learned_init as L, workloads
+    cfg = workloads.small_config()
+    cfg.model_estimation_mode = abi.DYNAMIC_ESTIMATIONS
+    net, _ = L.run(train_pools=1, eval_pools=1, lanes=256, fit_iters=200, epochs=5, batch=1024, seed=2)
+    lanes, F = 64, 512
+    gen = Fl.TraceGenerator(lanes, workload=1)
+    an = Fl.BatchAnalyzer(cfg, 0, lanes, F)
+    an.set_learned_init(net)
+    estimated = emitted = 0
+    for c in range(16):
+        _, lens, _, em, est = an(gen.next(c * F, F), c * F)
+        estimated += int(est)
+        emitted += int(em)
+    assert estimated >= 2 and emitted > 0 and int(lens.sum()) > 0
+    m, _ = an.models()
+    means = abi.f16_to_f32(Fl.struct_to_numpy(m, abi.LANE_MODEL_DT)["analogs"]["means"])
+    assert np.isfinite(means).all()
+    an.set_learned_init(None)
+    an(gen.next(16 * F, F), 16 * F)
+    torch.cuda.synchronize()
