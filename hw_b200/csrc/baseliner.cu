@@ -213,7 +213,7 @@ __global__ void BaselinerInitKernel(int16_t* st16, float* st32, int lanes)
 }
 
 template <int FT>
-__global__ void __launch_bounds__(64, 6) BaselinerKernel(BaselinerArgs a, KParams k)
+__global__ void __launch_bounds__(64, 7) BaselinerKernel(BaselinerArgs a, KParams k)
 {
     using Lay = FLayout<FT>;
     const int g = blockIdx.x * blockDim.x + threadIdx.x;

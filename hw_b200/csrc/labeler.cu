@@ -179,10 +179,9 @@ __device__ __forceinline__ int TraceSource(uint32_t w, int state)
 }
 
 
-constexpr int kMaxRoiWords = (1024 + 22 + 15) / 16;   // F up to 1024
 constexpr int kBatch = 8;                              // frames loaded ahead
 
-__global__ void __launch_bounds__(128) LabelerKernel(LabelerArgs A, KParams k)
+__global__ void __launch_bounds__(128, 5) LabelerKernel(LabelerArgs A, KParams k)
 {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= A.lanes * kLane) return;
@@ -195,7 +194,11 @@ __global__ void __launch_bounds__(128) LabelerKernel(LabelerArgs A, KParams k)
     const hw_lane_model& newM = A.models[l];
 
     // ---- ROI (ComputeRoi, FrameLabelerHost.cpp:267-309; RoiHost.h:110-249)
-    uint32_t roiw[kMaxRoiWords];
+    // 2-bit ROI codes, 16 per word, in dynamic shared memory [word][thread]
+    // (kept out of local memory, whose L1 share depends on other kernels'
+    // shared-memory carve-out).
+    extern __shared__ uint32_t roiSh[];
+    auto roiw = [&](int w) -> uint32_t& { return roiSh[w * blockDim.x + threadIdx.x]; };
     {
         const float inv1 = 1.0f / sqrtf(h2f(oldM.baseline.vars[z]));
         const float inv2 = 1.0f / sqrtf(h2f(newM.baseline.vars[z]));
@@ -213,7 +216,7 @@ __global__ void __launch_bounds__(128) LabelerKernel(LabelerArgs A, KParams k)
             const float thresh = (prevRoi & 1u) ? k.roiLower : k.roiUpper;
             const uint32_t v = ((mval >= thresh) ? 1u : 0u) | ((mval >= k.roiLower) ? 2u : 0u);
             word |= v << (2 * (ri & 15));
-            if ((ri & 15) == 15) { roiw[ri >> 4] = word; word = 0; }
+            if ((ri & 15) == 15) { roiw(ri >> 4) = word; word = 0; }
             ++ri;
             prevRoi = v;
             p0 = p1; p1 = p2; p2 = sn;
@@ -230,12 +233,12 @@ __global__ void __launch_bounds__(128) LabelerKernel(LabelerArgs A, KParams k)
                 process(mul_rn((float)y, inv2));
             }
         }
-        if (ri & 15) roiw[ri >> 4] = word;
+        if (ri & 15) roiw(ri >> 4) = word;
         // Backward recursion: 2-bit codes become 0/1 (in place, bit 0 of each code).
         uint32_t pr = 0;
         for (int wi = (nRoi - 1) >> 4; wi >= 0; --wi)
         {
-            uint32_t wv = roiw[wi];
+            uint32_t wv = roiw(wi);
             uint32_t outw = 0;
             const int hi = (wi == ((nRoi - 1) >> 4)) ? ((nRoi - 1) & 15) : 15;
             for (int j = hi; j >= 0; --j)
@@ -245,10 +248,10 @@ __global__ void __launch_bounds__(128) LabelerKernel(LabelerArgs A, KParams k)
                 pr = b;
                 outw |= b << (2 * j);
             }
-            roiw[wi] = outw;
+            roiw(wi) = outw;
         }
     }
-    auto roiBit = [&](int f) -> bool { return (roiw[f >> 4] >> (2 * (f & 15))) & 1u; };
+    auto roiBit = [&](int f) -> bool { return (roiw(f >> 4) >> (2 * (f & 15))) & 1u; };
 
     // ---- Viterbi (LabelBlock, FrameLabelerHost.cpp:314-448)
     float ll[kStates];
@@ -260,10 +263,10 @@ __global__ void __launch_bounds__(128) LabelerKernel(LabelerArgs A, KParams k)
     uint32_t* tb = A.tb + (size_t)l * (F + kLookback) * kLane + z;
     ZScorer sc;
     sc.Setup(k, oldM, z);
-    uint32_t roiWord = roiw[0];
+    uint32_t roiWord = roiw(0);
     for (int f = 0; f < kLatent; ++f)
     {
-        if ((f & 15) == 0) roiWord = roiw[f >> 4];
+        if ((f & 15) == 0) roiWord = roiw(f >> 4);
         const bool isRoi = (roiWord >> (2 * (f & 15))) & 1u;
         tb[(size_t)f * kLane] = ViterbiStep(k, sc, (float)pl[(size_t)f * kLane], isRoi, ll);
     }
@@ -288,7 +291,7 @@ __global__ void __launch_bounds__(128) LabelerKernel(LabelerArgs A, KParams k)
             for (int i = 0; i < kStates; ++i) anchorLL[i] = ll[i];
         }
         const int lf = f + kLatent;
-        if ((lf & 15) == 0) roiWord = roiw[lf >> 4];
+        if ((lf & 15) == 0) roiWord = roiw(lf >> 4);
         const bool isRoi = (roiWord >> (2 * (lf & 15))) & 1u;
         tb[(size_t)lf * kLane] = ViterbiStep(k, sc, (float)x, isRoi, ll);
     }
@@ -376,7 +379,8 @@ cudaError_t LaunchLabeler(const LabelerArgs& a, const KParams& k, cudaStream_t s
     if (a.F > 1024 || a.F % kBatch != 0) return cudaErrorInvalidValue;
     const int threads = 128;
     const int blocks = (a.lanes * kLane + threads - 1) / threads;
-    LabelerKernel<<<blocks, threads, 0, s>>>(a, k);
+    const int roiWords = (a.F + kLookback + kStitch + 15) / 16;
+    LabelerKernel<<<blocks, threads, (size_t)roiWords * threads * sizeof(uint32_t), s>>>(a, k);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const int n = a.lanes * (int)(sizeof(hw_lane_model) / 4);
