@@ -212,7 +212,7 @@ __global__ void BaselinerInitKernel(int16_t* st16, float* st32, int lanes)
     st32[(size_t)2 * nZmw + g] = 2.0f;     // blSigmaEma_ initial value
 }
 
-template <int FT>
+template <int FT, typename TIn>
 __global__ void __launch_bounds__(64, 7) BaselinerKernel(BaselinerArgs a, KParams k)
 {
     using Lay = FLayout<FT>;
@@ -254,7 +254,9 @@ __global__ void __launch_bounds__(64, 7) BaselinerKernel(BaselinerArgs a, KParam
     float b_m0 = 0, b_m1 = 0, b_m2 = 0, rawSum = 0;
     float g_m0 = 0, g_m1 = 0, g_m2 = 0;
 
-    const int16_t* tr = a.trace + (size_t)lane * a.F * kLane + z;
+    const TIn* tr;
+    if constexpr (std::is_same_v<TIn, uint8_t>) tr = a.trace8 + (size_t)lane * a.F * kLane + z;
+    else tr = a.trace + (size_t)lane * a.F * kLane + z;
     int16_t* out = a.out + (size_t)lane * a.F * kLane + z;
     const int16_t ped = (int16_t)k.pedestal;
     float sub = 0.0f;
@@ -263,12 +265,12 @@ __global__ void __launch_bounds__(64, 7) BaselinerKernel(BaselinerArgs a, KParam
     // block, the other even frames and the odd frames each get their own
     // specialisation of the frame body, with the trace loaded two frames ahead.
     static_assert(Lay::AggStride() == 16, "block size must be the aggregate stride");
-    int16_t xn0 = __ldg(tr), xn1 = __ldg(tr + kLane);
+    int16_t xn0 = (int16_t)__ldg(tr), xn1 = (int16_t)__ldg(tr + kLane);
     auto frame = [&](auto phaseTag, int t) {
         constexpr int Ph = decltype(phaseTag)::value;
         const int16_t x = xn0;
         xn0 = xn1;
-        if (t + 2 < a.F) xn1 = __ldg(tr + (size_t)(t + 2) * kLane);
+        if (t + 2 < a.F) xn1 = (int16_t)__ldg(tr + (size_t)(t + 2) * kLane);
         int16_t lo = 0, up = 0;
         const bool haveL = FeedFilter<FT, false, Ph>(x, mem, pc, lo);
         FeedFilter<FT, true, Ph>(x, mem, pc, up);
@@ -403,20 +405,31 @@ int BaselinerNumSlots16(int ft)
     return -1;
 }
 
-template <int FT>
-cudaError_t LaunchBaselinerT(const BaselinerArgs& a, const KParams& k, cudaStream_t s)
+template <int FT, typename TIn>
+cudaError_t LaunchBaselinerT2(const BaselinerArgs& a, const KParams& k, cudaStream_t s)
 {
     const int threads = kLane;
     const size_t smem = sizeof(int16_t) * FLayout<FT>::SmemSlots() * threads;
-    static bool attr = false;
-    if (!attr)
+    // the shared-memory limit is a per-device attribute of the kernel: set it
+    // once on each device
+    static bool attrSet[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64 || !attrSet[dev])
     {
-        cudaError_t e = cudaFuncSetAttribute(BaselinerKernel<FT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = cudaFuncSetAttribute(BaselinerKernel<FT, TIn>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        attr = true;
+        if (dev >= 0 && dev < 64) attrSet[dev] = true;
     }
-    BaselinerKernel<FT><<<a.lanes, threads, smem, s>>>(a, k);
+    BaselinerKernel<FT, TIn><<<a.lanes, threads, smem, s>>>(a, k);
     return cudaGetLastError();
+}
+
+template <int FT>
+cudaError_t LaunchBaselinerT(const BaselinerArgs& a, const KParams& k, cudaStream_t s)
+{
+    return a.trace8 ? LaunchBaselinerT2<FT, uint8_t>(a, k, s) : LaunchBaselinerT2<FT, int16_t>(a, k, s);
 }
 
 cudaError_t LaunchBaseliner(int ft, const BaselinerArgs& a, const KParams& k, cudaStream_t s)

@@ -242,6 +242,16 @@ int hw_baseliner_process(hw_baseliner* b, const int16_t* d_trace, int32_t first_
     return HW_OK;
 }
 
+int hw_baseliner_process_u8(hw_baseliner* b, const uint8_t* d_trace, int32_t first_frame, int16_t* d_out,
+                            hw_baseliner_stats* d_stats, void* stream)
+{
+    (void)first_frame;
+    if (!b || !d_trace || !d_out || !d_stats) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    BaselinerArgs a{nullptr, d_out, d_stats, b->st16, b->st32, (int)b->lanes, (int)b->F, d_trace};
+    HW_CUDA(LaunchBaseliner(b->cfg.filter_type, a, b->k, S(stream)), "hw_baseliner_process_u8");
+    return HW_OK;
+}
+
 // ---- Aggregator --------------------------------------------------------------
 
 int hw_blstats_aggregator_create(uint32_t pool_id, uint32_t lanes, hw_blstats_aggregator** out)
@@ -796,16 +806,154 @@ int hw_analyzer_set_learned_init(hw_analyzer* a, hw_learned_init* net)
     return HW_OK;
 }
 
+// ---- Checkpoints -----------------------------------------------------------------
+// The blob is a header (sizes, the schedule state kept on the host) followed
+// by every device buffer that carries state from one chunk to the next, in
+// a fixed order.  Per-chunk outputs and scratch are not saved.
+
+namespace {
+
+struct StateHeader
+{
+    char magic[8];
+    uint32_t version, lanes, F, poolId;
+    int32_t filterType, estimationMode;
+    uint64_t payload;
+    int32_t status, framesRemaining, initialized, fullEstimation, nextFrame, diagValid;
+    hw_frame_interval modelFi, aggFi, histFi;
+    int32_t histInitialized, pad_;
+};
+
+const char kStateMagic[8] = {'H', 'W', 'B', '2', '0', '0', 'S', 'T'};
+
+std::vector<std::pair<void*, size_t>> StateSegments(const hw_analyzer* a)
+{
+    const size_t n = (size_t)a->lanes * kLane;
+    return {
+        {a->bl->st16, (size_t)a->bl->slots16 * n * sizeof(int16_t)},
+        {a->bl->st32, 3 * n * sizeof(float)},
+        {a->agg->acc, a->lanes * sizeof(hw_baseliner_stats)},
+        {a->hist->hist, a->lanes * sizeof(hw_lane_histogram)},
+        {a->hist->edgePrev, n * sizeof(int16_t)},
+        {a->hist->edgeBits, n * sizeof(uint8_t)},
+        {a->lab->latModel, a->lanes * sizeof(hw_lane_model)},
+        {a->lab->latLabel, n * sizeof(int16_t)},
+        {a->lab->latRoi, n * sizeof(int16_t)},
+        {a->lab->latTrc, n * sizeof(int16_t)},
+        {a->lab->prevLat, (size_t)kLatent * n * sizeof(int16_t)},
+        {a->pa->segStart, n * sizeof(uint32_t)},
+        {a->pa->segFirst, n * sizeof(int16_t)},
+        {a->pa->segLast, n * sizeof(int16_t)},
+        {a->pa->segMax, n * sizeof(int16_t)},
+        {a->pa->segTotal, n * sizeof(float)},
+        {a->pa->segM2, n * sizeof(float)},
+        {a->pa->segLabel, n * sizeof(int16_t)},
+        {a->models, a->lanes * sizeof(hw_lane_model)},
+        {a->diag, a->lanes * sizeof(hw_dme_diag)},
+    };
+}
+
+uint64_t StatePayload(const hw_analyzer* a)
+{
+    uint64_t t = 0;
+    for (const auto& seg : StateSegments(a)) t += seg.second;
+    return t;
+}
+
+}   // namespace
+
+int hw_analyzer_state_size(const hw_analyzer* a, uint64_t* bytes)
+{
+    if (!a || !bytes) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    *bytes = sizeof(StateHeader) + StatePayload(a);
+    return HW_OK;
+}
+
+int hw_analyzer_state_export(const hw_analyzer* a, void* host_blob, uint64_t bytes, void* stream)
+{
+    if (!a || !host_blob) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    const uint64_t payload = StatePayload(a);
+    if (bytes < sizeof(StateHeader) + payload) return Fail(HW_ERR_INVALID_ARG, "state blob too small");
+    StateHeader h{};
+    memcpy(h.magic, kStateMagic, 8);
+    h.version = 1;
+    h.lanes = a->lanes;
+    h.F = a->F;
+    h.poolId = a->poolId;
+    h.filterType = a->cfg.filter_type;
+    h.estimationMode = a->cfg.model_estimation_mode;
+    h.payload = payload;
+    h.status = a->status;
+    h.framesRemaining = a->framesRemaining;
+    h.initialized = a->initialized;
+    h.fullEstimation = a->fullEstimation;
+    h.nextFrame = a->nextFrame;
+    h.diagValid = a->diagValid;
+    h.modelFi = a->modelFi;
+    h.aggFi = a->agg->fi;
+    h.histFi = a->hist->fi;
+    h.histInitialized = a->hist->initialized;
+    char* out = static_cast<char*>(host_blob);
+    memcpy(out, &h, sizeof(h));
+    size_t off = sizeof(h);
+    cudaStream_t s = S(stream);
+    for (const auto& seg : StateSegments(a))
+    {
+        HW_CUDA(cudaMemcpyAsync(out + off, seg.first, seg.second, cudaMemcpyDeviceToHost, s), "hw_analyzer_state_export");
+        off += seg.second;
+    }
+    HW_CUDA(cudaStreamSynchronize(s), "hw_analyzer_state_export");
+    return HW_OK;
+}
+
+int hw_analyzer_state_import(hw_analyzer* a, const void* host_blob, uint64_t bytes, void* stream)
+{
+    if (!a || !host_blob) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    if (bytes < sizeof(StateHeader)) return Fail(HW_ERR_INVALID_ARG, "state blob too small");
+    StateHeader h;
+    memcpy(&h, host_blob, sizeof(h));
+    if (memcmp(h.magic, kStateMagic, 8) != 0 || h.version != 1)
+        return Fail(HW_ERR_INVALID_ARG, "not an hw_analyzer state blob of version 1");
+    if (h.lanes != a->lanes || h.F != a->F || h.poolId != a->poolId || h.filterType != a->cfg.filter_type ||
+        h.estimationMode != a->cfg.model_estimation_mode)
+        return Fail(HW_ERR_INVALID_ARG, "state blob is for a different pool, size, filter or estimation mode");
+    const uint64_t payload = StatePayload(a);
+    if (h.payload != payload || bytes < sizeof(h) + payload)
+        return Fail(HW_ERR_INVALID_ARG, "state blob size does not match this analyzer");
+    const char* in = static_cast<const char*>(host_blob);
+    size_t off = sizeof(h);
+    cudaStream_t s = S(stream);
+    for (const auto& seg : StateSegments(a))
+    {
+        HW_CUDA(cudaMemcpyAsync(seg.first, in + off, seg.second, cudaMemcpyHostToDevice, s), "hw_analyzer_state_import");
+        off += seg.second;
+    }
+    HW_CUDA(cudaStreamSynchronize(s), "hw_analyzer_state_import");
+    a->status = h.status;
+    a->framesRemaining = h.framesRemaining;
+    a->initialized = h.initialized != 0;
+    a->fullEstimation = h.fullEstimation != 0;
+    a->nextFrame = h.nextFrame;
+    a->diagValid = h.diagValid != 0;
+    a->modelFi = h.modelFi;
+    a->agg->fi = h.aggFi;
+    a->hist->fi = h.histFi;
+    a->hist->initialized = h.histInitialized != 0;
+    return HW_OK;
+}
+
 int hw_analyzer_destroy(hw_analyzer* a)
 {
     delete a;
     return HW_OK;
 }
 
-int hw_analyzer_process(hw_analyzer* a, const int16_t* d_trace, int32_t first_frame, hw_pulse* d_pulses,
-                        uint32_t* d_lens, uint32_t* d_overflows, int32_t* emitted, int32_t* estimated, void* stream)
+static int AnalyzerProcess(hw_analyzer* a, const int16_t* d_trace, const uint8_t* d_trace8, int32_t first_frame,
+                           hw_pulse* d_pulses, uint32_t* d_lens, uint32_t* d_overflows, int32_t* emitted,
+                           int32_t* estimated, void* stream)
 {
-    if (!a || !d_trace || !d_pulses || !d_lens || !d_overflows) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    if (!a || !(d_trace || d_trace8) || !d_pulses || !d_lens || !d_overflows)
+        return Fail(HW_ERR_INVALID_ARG, "NULL argument");
     if (first_frame != a->nextFrame) return Fail(HW_ERR_FRAME_ORDER, "Bad frame ID.");
     cudaStream_t s = S(stream);
     int rc;
@@ -813,7 +961,8 @@ int hw_analyzer_process(hw_analyzer* a, const int16_t* d_trace, int32_t first_fr
     const size_t nZmw = (size_t)a->lanes * kLane;
     {
         const size_t t = a->Begin(HW_STAGE_BASELINE, s);
-        if ((rc = hw_baseliner_process(a->bl, d_trace, first_frame, a->bls, a->stats, s))) return rc;
+        if ((rc = d_trace8 ? hw_baseliner_process_u8(a->bl, d_trace8, first_frame, a->bls, a->stats, s)
+                           : hw_baseliner_process(a->bl, d_trace, first_frame, a->bls, a->stats, s))) return rc;
         a->End(t, s);
     }
     const hw_frame_interval fi{first_frame, first_frame + (int32_t)a->F};
@@ -857,6 +1006,19 @@ int hw_analyzer_process(hw_analyzer* a, const int16_t* d_trace, int32_t first_fr
     if (emitted) *emitted = emit ? 1 : 0;
     if (estimated) *estimated = ran ? 1 : 0;
     return HW_OK;
+}
+
+int hw_analyzer_process(hw_analyzer* a, const int16_t* d_trace, int32_t first_frame, hw_pulse* d_pulses,
+                        uint32_t* d_lens, uint32_t* d_overflows, int32_t* emitted, int32_t* estimated, void* stream)
+{
+    return AnalyzerProcess(a, d_trace, nullptr, first_frame, d_pulses, d_lens, d_overflows, emitted, estimated, stream);
+}
+
+int hw_analyzer_process_u8(hw_analyzer* a, const uint8_t* d_trace, int32_t first_frame, hw_pulse* d_pulses,
+                           uint32_t* d_lens, uint32_t* d_overflows, int32_t* emitted, int32_t* estimated,
+                           void* stream)
+{
+    return AnalyzerProcess(a, nullptr, d_trace, first_frame, d_pulses, d_lens, d_overflows, emitted, estimated, stream);
 }
 
 int hw_analyzer_models(const hw_analyzer* a, hw_lane_model* d_out, hw_frame_interval* fi, void* stream)

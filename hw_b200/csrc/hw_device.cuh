@@ -103,13 +103,16 @@ __device__ __forceinline__ float SignalCovar(const KParams& k, float cv2, float 
 
 struct BaselinerArgs
 {
-    const int16_t* trace;        // [lanes][F][64]
+    const int16_t* trace;        // [lanes][F][64] (int16 encoding)
     int16_t* out;                // [lanes][F][64]
     hw_baseliner_stats* stats;   // [lanes]
     int16_t* st16;               // [NumI16Slots][nZmw]
     float* st32;                 // [3][nZmw]
     int lanes;
     int F;
+    // uint8 encoding: [lanes][F][64], used instead of `trace` when not null;
+    // each value is widened to int16 first (BlockView::Extract, BatchData.h:160-180)
+    const uint8_t* trace8 = nullptr;
 };
 
 struct DmeArgs

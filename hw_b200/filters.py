@@ -75,11 +75,13 @@ class Baseliner(_Handle):
         return v.value
 
     def __call__(self, trace, first_frame, out=None, stats=None):
-        """Returns (baseline-subtracted traces, per-lane BaselinerStatAccumState)."""
-        assert trace.dtype == torch.int16 and trace.is_cuda and trace.is_contiguous()
-        out = torch.empty_like(trace) if out is None else out
+        """Returns (baseline-subtracted traces, per-lane BaselinerStatAccumState).
+        `trace` is int16 or uint8 (the two PacketLayout encodings)."""
+        assert trace.dtype in (torch.int16, torch.uint8) and trace.is_cuda and trace.is_contiguous()
+        out = torch.empty(trace.shape, dtype=torch.int16, device=trace.device) if out is None else out
         stats = struct_buffer(abi.BLSTATS_DT, self.lanes) if stats is None else stats
-        check(lib().hw_baseliner_process(self._h, _p(trace), int(first_frame), _p(out), _p(stats), _stream()))
+        fn = lib().hw_baseliner_process_u8 if trace.dtype == torch.uint8 else lib().hw_baseliner_process
+        check(fn(self._h, _p(trace), int(first_frame), _p(out), _p(stats), _stream()))
         return out, stats
 
 
@@ -236,11 +238,24 @@ class BatchAnalyzer(_Handle):
         lens = self.lens if lens is None else lens
         ovf = self.ovf if ovf is None else ovf
         em, est = C.c_int32(), C.c_int32()
-        check(lib().hw_analyzer_process(self._h, _p(trace), int(first_frame), _p(pulses), _p(lens), _p(ovf),
-                                        C.byref(em), C.byref(est), _stream()))
+        fn = lib().hw_analyzer_process_u8 if trace.dtype == torch.uint8 else lib().hw_analyzer_process
+        check(fn(self._h, _p(trace), int(first_frame), _p(pulses), _p(lens), _p(ovf), C.byref(em), C.byref(est),
+                 _stream()))
         return pulses, lens, ovf, bool(em.value), bool(est.value)
 
     STAGES = ("baseline", "aggregate", "histogram", "model_init", "dme", "hist_reset", "labeler", "pulses")
+
+    def export_state(self):
+        """Checkpoint of the pool's state as a numpy uint8 array."""
+        n = C.c_uint64()
+        check(lib().hw_analyzer_state_size(self._h, C.byref(n)))
+        blob = np.empty(n.value, np.uint8)
+        check(lib().hw_analyzer_state_export(self._h, abi.ptr(blob), n.value, _stream()))
+        return blob
+
+    def import_state(self, blob):
+        blob = np.ascontiguousarray(blob, np.uint8)
+        check(lib().hw_analyzer_state_import(self._h, abi.ptr(blob), blob.size, _stream()))
 
     def set_learned_init(self, net):
         """Start every estimate from `net`'s proposal (a learned_init.Network,

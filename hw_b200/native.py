@@ -42,6 +42,8 @@ def lib():
         "hw_baseliner_destroy": ([vp], C.c_int),
         "hw_baseliner_startup_latency": ([vp, C.POINTER(u32)], C.c_int),
         "hw_baseliner_process": ([vp, vp, i32, vp, vp, vp], C.c_int),
+        "hw_baseliner_process_u8": ([vp, vp, i32, vp, vp, vp], C.c_int),
+        "hw_analyzer_process_u8": ([vp, vp, i32, vp, vp, vp, C.POINTER(i32), C.POINTER(i32), vp], C.c_int),
         "hw_blstats_aggregator_create": ([u32, u32, PPV], C.c_int),
         "hw_blstats_aggregator_destroy": ([vp], C.c_int),
         "hw_blstats_aggregator_add": ([vp, vp, FI, vp], C.c_int),
@@ -60,6 +62,9 @@ def lib():
         "hw_dme_estimate_noalloc": ([PCFG, u32, vp, vp, FI, FI, vp, vp, vp], C.c_int),
         "hw_dme_estimate_proposal": ([vp, vp, vp, FI, FI, vp, vp, vp, vp], C.c_int),
         "hw_analyzer_set_learned_init": ([vp, vp], C.c_int),
+        "hw_analyzer_state_size": ([vp, C.POINTER(C.c_uint64)], C.c_int),
+        "hw_analyzer_state_export": ([vp, vp, C.c_uint64, vp], C.c_int),
+        "hw_analyzer_state_import": ([vp, vp, C.c_uint64, vp], C.c_int),
         "hw_dme_em_fit_scratch_bytes": ([u32, C.POINTER(C.c_uint64)], C.c_int),
         "hw_dme_em_fit": ([PCFG, u32, vp, vp, FI, FI, vp, C.c_int, vp, vp, C.c_float, u32, vp, vp, vp, vp, vp],
                           C.c_int),

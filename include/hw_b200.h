@@ -280,6 +280,11 @@ int hw_baseliner_startup_latency(const hw_baseliner* b, uint32_t* frames);
  * hw_baseliner_stats per lane.  first_frame must continue the previous call. */
 int hw_baseliner_process(hw_baseliner* b, const int16_t* d_trace, int32_t first_frame,
                          int16_t* d_out, hw_baseliner_stats* d_stats, void* stream);
+/* The same for chunks in the uint8 encoding (PacketLayout UINT8,
+ * DeviceMultiScaleBaseliner.cu:84-101): each value is widened to int16 before
+ * any arithmetic, as BlockView::Extract does (BatchData.h:160-180). */
+int hw_baseliner_process_u8(hw_baseliner* b, const uint8_t* d_trace, int32_t first_frame, int16_t* d_out,
+                            hw_baseliner_stats* d_stats, void* stream);
 
 /* ---- Baseline statistics aggregator (BaselineStatsAggregator.h:45-104) -- */
 typedef struct hw_blstats_aggregator hw_blstats_aggregator;
@@ -468,6 +473,18 @@ int hw_analyzer_destroy(hw_analyzer* a);
  * (hw_dme_estimate_proposal); NULL restores the reference start.  The network
  * is not owned and must outlive its use. */
 int hw_analyzer_set_learned_init(hw_analyzer* a, hw_learned_init* net);
+
+/* Checkpoints (the reference keeps pool state in stashable device
+ * allocations, analyzer/BatchAnalyzer.cpp:80; this saves and restores it to
+ * host memory).  The blob holds every buffer that carries state between
+ * chunks (filter windows, statistics, histogram, detection models, labeler
+ * latency state, open pulse segments) and the estimation schedule; an
+ * analyzer created with the same configuration, pool, lanes and chunk
+ * length continues exactly where the exporting one stopped.  Export and
+ * import are synchronous on `stream`. */
+int hw_analyzer_state_size(const hw_analyzer* a, uint64_t* bytes);
+int hw_analyzer_state_export(const hw_analyzer* a, void* host_blob, uint64_t bytes, void* stream);
+int hw_analyzer_state_import(hw_analyzer* a, const void* host_blob, uint64_t bytes, void* stream);
 /* BatchAnalyzer::operator(): d_trace[lanes][F][64] must be the next chunk
  * (first_frame == previous first_frame + F, starting at 0); otherwise
  * HW_ERR_FRAME_ORDER.  Pulses go to d_pulses[lanes][64][max_calls_per_zmw]
@@ -477,6 +494,11 @@ int hw_analyzer_set_learned_init(hw_analyzer* a, hw_learned_init* net);
 int hw_analyzer_process(hw_analyzer* a, const int16_t* d_trace, int32_t first_frame, hw_pulse* d_pulses,
                         uint32_t* d_lens, uint32_t* d_overflows, int32_t* emitted, int32_t* estimated,
                         void* stream);
+/* hw_analyzer_process for chunks in the uint8 encoding (see
+ * hw_baseliner_process_u8); an analyzer may receive either encoding. */
+int hw_analyzer_process_u8(hw_analyzer* a, const uint8_t* d_trace, int32_t first_frame, hw_pulse* d_pulses,
+                           uint32_t* d_lens, uint32_t* d_overflows, int32_t* emitted, int32_t* estimated,
+                           void* stream);
 /* Current detection models of the pool and their frame interval. */
 int hw_analyzer_models(const hw_analyzer* a, hw_lane_model* d_out, hw_frame_interval* fi, void* stream);
 /* Diagnostics of the most recent DME estimate (*valid = 0 if none yet). */

@@ -245,3 +245,37 @@ def test_generated_traces_bit_exact_chip_workload():
     tr = np.concatenate([gen.next(c * 512, 512).cpu().numpy() for c in range(12)], axis=1)
     _lockstep(cfg, tr[:2], 512, pool_id=0)
     _lockstep(cfg, tr[2:], 512, pool_id=1)
+
+
+def test_uint8_encoding_equals_its_int16_widening():
+    """A uint8 chunk (PacketLayout UINT8) goes through the chain exactly like
+    the same values widened to int16 (BatchData.h:160-180)."""
+    import torch
+    from hw_b200 import filters as Fl
+    cfg = workloads.small_config()
+    cfg.model_estimation_mode = abi.DYNAMIC_ESTIMATIONS
+    lanes, F, C = 2, 512, 12
+    tr = synth.traces(lanes, F * C, seed=41, baseline=60.0)
+    tr8 = np.clip(tr, 0, 255).astype(np.uint8)
+    a16 = Fl.BatchAnalyzer(cfg, 0, lanes, F)
+    a8 = Fl.BatchAnalyzer(cfg, 0, lanes, F)
+    b16 = Fl.Baseliner(cfg, 0, lanes, F)
+    b8 = Fl.Baseliner(cfg, 0, lanes, F)
+    for c in range(C):
+        x8 = torch.from_numpy(np.ascontiguousarray(tr8[:, c * F:(c + 1) * F])).cuda()
+        x16 = x8.to(torch.int16)
+        o16, s16 = b16(x16, c * F)
+        o8, s8 = b8(x8, c * F)
+        assert torch.equal(o16, o8) and torch.equal(s16, s8)
+        p16, l16, v16, e16, t16 = a16(x16, c * F)
+        p8, l8, v8, e8, t8 = a8(x8, c * F)
+        assert (e16, t16) == (e8, t8)
+        assert torch.equal(l16, l8) and torch.equal(v16, v8)
+        if e16:
+            q16 = Fl.struct_to_numpy(p16, abi.PULSE_DT).reshape(lanes, 64, cfg.max_calls_per_zmw)
+            q8 = Fl.struct_to_numpy(p8, abi.PULSE_DT).reshape(lanes, 64, cfg.max_calls_per_zmw)
+            n = l16.cpu().numpy()
+            for l in range(lanes):
+                for z in range(64):
+                    assert np.array_equal(q16[l, z, :n[l, z]].view(np.uint8), q8[l, z, :n[l, z]].view(np.uint8))
+    assert e16
