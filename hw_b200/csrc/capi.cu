@@ -1,5 +1,6 @@
 // C ABI of hw_b200: per-pool handles that own the device state of each filter
 // and launch the sm_100a kernels.  See include/hw_b200.h for the contract.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -1061,6 +1062,145 @@ int hw_analyzer_stage_times(hw_analyzer* a, double ms[HW_NUM_STAGES], uint32_t l
     }
     a->evMarks.clear();
     a->evUsed = 0;
+    return HW_OK;
+}
+
+}   // extern "C"
+
+// ---- Pool sets: uneven pools in shared launches ---------------------------------
+// Lanes are independent through the whole chain, and a pool's estimation
+// schedule depends only on its chunk length F and its stagger class
+// pool_id % chunksPerEstimate (BatchAnalyzer.cpp:96-117).  Pools that share
+// both are therefore run as one batched analyzer over all their lanes: each
+// stage is one launch for the whole class, with results identical to
+// separate per-pool analyzers.  The packed input holds the classes one after
+// the other, so every class's chunk is one contiguous slice.
+
+struct hw_pool_set
+{
+    struct Group
+    {
+        hw_analyzer* an = nullptr;
+        uint32_t lanes = 0, F = 0;
+        uint64_t inOffset = 0;                // int16 elements into the packed chunk
+        hw_pulse* pulses = nullptr;
+        uint32_t* lens = nullptr;
+        uint32_t* ovf = nullptr;
+        std::vector<uint32_t> pools;
+    };
+    uint32_t cap = 0;
+    std::vector<Group> groups;
+    std::vector<uint32_t> poolGroup, poolLaneOffset;
+    std::vector<uint64_t> poolInOffset;
+    uint64_t total = 0;
+
+    ~hw_pool_set()
+    {
+        for (auto& g : groups)
+        {
+            hw_analyzer_destroy(g.an);
+            cudaFree(g.pulses); cudaFree(g.lens); cudaFree(g.ovf);
+        }
+    }
+};
+
+extern "C" {
+
+int hw_pool_set_create(const hw_config* cfg, uint32_t n_pools, const uint32_t* lanes, const uint32_t* frames_per_chunk,
+                       hw_pool_set** out)
+{
+    if (!cfg || !lanes || !frames_per_chunk || !out || n_pools == 0) return Fail(HW_ERR_INVALID_ARG, "bad argument");
+    *out = nullptr;
+    auto ps = std::make_unique<hw_pool_set>();
+    ps->cap = cfg->max_calls_per_zmw;
+    ps->poolGroup.assign(n_pools, 0);
+    ps->poolLaneOffset.assign(n_pools, 0);
+    ps->poolInOffset.assign(n_pools, 0);
+    // class key: (F, stagger class); classes in order of first appearance
+    std::vector<std::pair<uint32_t, uint32_t>> keys;
+    for (uint32_t p = 0; p < n_pools; ++p)
+    {
+        if (lanes[p] == 0) return Fail(HW_ERR_INVALID_ARG, "every pool needs at least one lane");
+        const uint32_t F = frames_per_chunk[p];
+        if (F == 0) return Fail(HW_ERR_INVALID_ARG, "frames_per_chunk must be positive");
+        const uint32_t cpe = (std::max(cfg->min_frames_for_estimate, 1u) + F - 1) / F;
+        const std::pair<uint32_t, uint32_t> key{F, p % cpe};
+        size_t gi = 0;
+        while (gi < keys.size() && keys[gi] != key) ++gi;
+        if (gi == keys.size())
+        {
+            keys.push_back(key);
+            ps->groups.emplace_back();
+            ps->groups.back().F = F;
+        }
+        auto& g = ps->groups[gi];
+        ps->poolGroup[p] = (uint32_t)gi;
+        ps->poolLaneOffset[p] = g.lanes;
+        g.lanes += lanes[p];
+        g.pools.push_back(p);
+    }
+    uint64_t off = 0;
+    for (auto& g : ps->groups)
+    {
+        g.inOffset = off;
+        for (uint32_t p : g.pools) ps->poolInOffset[p] = off + (uint64_t)ps->poolLaneOffset[p] * g.F * kLane;
+        off += (uint64_t)g.lanes * g.F * kLane;
+        int rc = hw_analyzer_create(cfg, g.pools.front(), g.lanes, g.F, &g.an);
+        if (rc) return rc;
+        const size_t n = (size_t)g.lanes * kLane;
+        if ((rc = DevAlloc(&g.pulses, n * ps->cap, "hw_pool_set_create"))) return rc;
+        if ((rc = DevAlloc(&g.lens, n, "hw_pool_set_create"))) return rc;
+        if ((rc = DevAlloc(&g.ovf, n, "hw_pool_set_create"))) return rc;
+    }
+    ps->total = off;
+    *out = ps.release();
+    return HW_OK;
+}
+
+int hw_pool_set_destroy(hw_pool_set* s)
+{
+    delete s;
+    return HW_OK;
+}
+
+int hw_pool_set_layout(const hw_pool_set* s, uint64_t* in_offsets, uint64_t* total_elements, uint32_t* n_launch_groups)
+{
+    if (!s) return Fail(HW_ERR_INVALID_ARG, "NULL pool set");
+    if (in_offsets)
+        for (size_t p = 0; p < s->poolInOffset.size(); ++p) in_offsets[p] = s->poolInOffset[p];
+    if (total_elements) *total_elements = s->total;
+    if (n_launch_groups) *n_launch_groups = (uint32_t)s->groups.size();
+    return HW_OK;
+}
+
+int hw_pool_set_process(hw_pool_set* s, const int16_t* d_packed, int32_t step, int32_t* emitted, int32_t* estimated,
+                        void* stream)
+{
+    if (!s || !d_packed || step < 0) return Fail(HW_ERR_INVALID_ARG, "bad argument");
+    for (auto& g : s->groups)
+    {
+        int32_t em = 0, est = 0;
+        int rc = hw_analyzer_process(g.an, d_packed + g.inOffset, step * (int32_t)g.F, g.pulses, g.lens, g.ovf, &em,
+                                     &est, stream);
+        if (rc) return rc;
+        for (uint32_t p : g.pools)
+        {
+            if (emitted) emitted[p] = em;
+            if (estimated) estimated[p] = est;
+        }
+    }
+    return HW_OK;
+}
+
+int hw_pool_set_outputs(const hw_pool_set* s, uint32_t pool, hw_pulse** d_pulses, uint32_t** d_lens,
+                        uint32_t** d_overflows)
+{
+    if (!s || pool >= s->poolGroup.size()) return Fail(HW_ERR_INVALID_ARG, "bad pool");
+    const auto& g = s->groups[s->poolGroup[pool]];
+    const size_t z0 = (size_t)s->poolLaneOffset[pool] * kLane;
+    if (d_pulses) *d_pulses = g.pulses + z0 * s->cap;
+    if (d_lens) *d_lens = g.lens + z0;
+    if (d_overflows) *d_overflows = g.ovf + z0;
     return HW_OK;
 }
 

@@ -314,3 +314,61 @@ def default_config():
     cfg = abi.Config()
     check(lib().hw_config_default(C.byref(cfg)))
     return cfg
+
+
+class PoolSet(_Handle):
+    """Uneven pools in shared launches (hw_pool_set): pools with equal chunk
+    length and stagger class run as one batched analyzer."""
+    _destroy = "hw_pool_set_destroy"
+
+    def __init__(self, cfg, lanes, frames_per_chunk):
+        super().__init__()
+        n = len(lanes)
+        self.lanes = np.ascontiguousarray(lanes, np.uint32)
+        self.frames = np.ascontiguousarray(frames_per_chunk, np.uint32)
+        self.cap = cfg.max_calls_per_zmw
+        check(lib().hw_pool_set_create(C.byref(cfg), n, abi.ptr(self.lanes), abi.ptr(self.frames), C.byref(self._h)))
+        self.offsets = np.zeros(n, np.uint64)
+        total = C.c_uint64()
+        groups = C.c_uint32()
+        check(lib().hw_pool_set_layout(self._h, abi.ptr(self.offsets), C.byref(total), C.byref(groups)))
+        self.total, self.launch_groups = total.value, groups.value
+        self.packed = torch.empty(self.total, dtype=torch.int16, device="cuda")
+
+    def chunk(self, p):
+        """View of pool p's chunk [lanes][F][64] inside the packed input."""
+        o, L, F = int(self.offsets[p]), int(self.lanes[p]), int(self.frames[p])
+        return self.packed[o:o + L * F * abi.LANE].view(L, F, abi.LANE)
+
+    def process(self, step):
+        n = len(self.lanes)
+        em = np.zeros(n, np.int32)
+        est = np.zeros(n, np.int32)
+        check(lib().hw_pool_set_process(self._h, _p(self.packed), int(step), abi.ptr(em), abi.ptr(est), _stream()))
+        return em, est
+
+    def outputs(self, p):
+        """(pulses, lens, overflows) of pool p: CUDA tensors viewing the set's
+        buffers, overwritten by the next step."""
+        pp, pl, po = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        check(lib().hw_pool_set_outputs(self._h, p, C.byref(pp), C.byref(pl), C.byref(po)))
+        L = int(self.lanes[p])
+        n = L * abi.LANE
+        lens = _from_device(pl.value, n * 4).view(torch.int32).view(L, abi.LANE)
+        ovf = _from_device(po.value, n * 4).view(torch.int32).view(L, abi.LANE)
+        pulses = _from_device(pp.value, n * self.cap * abi.PULSE_DT.itemsize)
+        return pulses, lens, ovf
+
+
+class _DeviceBytes:
+    """Device memory owned by the library, exposed to torch without a copy."""
+
+    def __init__(self, ptr, nbytes):
+        self.__cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (ptr, False),
+                                         "version": 3, "strides": None}
+
+
+def _from_device(ptr, nbytes):
+    """uint8 CUDA tensor viewing nbytes of library-owned device memory at ptr
+    (valid while the owning handle lives)."""
+    return torch.as_tensor(_DeviceBytes(ptr, nbytes), device="cuda")

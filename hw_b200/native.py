@@ -62,6 +62,11 @@ def lib():
         "hw_dme_estimate_noalloc": ([PCFG, u32, vp, vp, FI, FI, vp, vp, vp], C.c_int),
         "hw_dme_estimate_proposal": ([vp, vp, vp, FI, FI, vp, vp, vp, vp], C.c_int),
         "hw_analyzer_set_learned_init": ([vp, vp], C.c_int),
+        "hw_pool_set_create": ([PCFG, u32, vp, vp, PPV], C.c_int),
+        "hw_pool_set_destroy": ([vp], C.c_int),
+        "hw_pool_set_layout": ([vp, vp, C.POINTER(C.c_uint64), C.POINTER(u32)], C.c_int),
+        "hw_pool_set_process": ([vp, vp, i32, vp, vp, vp], C.c_int),
+        "hw_pool_set_outputs": ([vp, u32, PPV, PPV, PPV], C.c_int),
         "hw_analyzer_state_size": ([vp, C.POINTER(C.c_uint64)], C.c_int),
         "hw_analyzer_state_export": ([vp, vp, C.c_uint64, vp], C.c_int),
         "hw_analyzer_state_import": ([vp, vp, C.c_uint64, vp], C.c_int),

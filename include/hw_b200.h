@@ -485,6 +485,31 @@ int hw_analyzer_set_learned_init(hw_analyzer* a, hw_learned_init* net);
 int hw_analyzer_state_size(const hw_analyzer* a, uint64_t* bytes);
 int hw_analyzer_state_export(const hw_analyzer* a, void* host_blob, uint64_t bytes, void* stream);
 int hw_analyzer_state_import(hw_analyzer* a, const void* host_blob, uint64_t bytes, void* stream);
+
+/* ---- Pool sets: uneven pools --------------------------
+ * No single reference counterpart: the reference runs one BatchAnalyzer per
+ * pool.  A pool set owns n_pools pools of any lane counts and chunk lengths
+ * (every chunk length a multiple of 16 frames, at most 1024).  Pools whose
+ * estimation schedules coincide -- same chunk length and same stagger class
+ * pool % ceil(MinFramesForEstimate / F) -- share one batched analyzer, so
+ * each stage of a step is one launch per class (hw_pool_set_layout reports
+ * how many classes), and every pool's results equal those of its own
+ * analyzer.  Each step processes one chunk of every pool from one packed
+ * device buffer of int16 traces: pool p's chunk [lanes_p][F_p][64] starts at
+ * element in_offsets[p].  Step s covers frames [s * F_p, (s + 1) * F_p). */
+typedef struct hw_pool_set hw_pool_set;
+int hw_pool_set_create(const hw_config* cfg, uint32_t n_pools, const uint32_t* lanes,
+                       const uint32_t* frames_per_chunk, hw_pool_set** out);
+int hw_pool_set_destroy(hw_pool_set* s);
+int hw_pool_set_layout(const hw_pool_set* s, uint64_t* in_offsets, uint64_t* total_elements,
+                       uint32_t* n_launch_groups);
+/* emitted / estimated: host arrays of n_pools flags (may be NULL). */
+int hw_pool_set_process(hw_pool_set* s, const int16_t* d_packed, int32_t step, int32_t* emitted,
+                        int32_t* estimated, void* stream);
+/* Device pointers to pool p's outputs of the last step (stable across steps):
+ * pulses [lanes_p][64][max_calls_per_zmw], lengths and overflows [lanes_p][64]. */
+int hw_pool_set_outputs(const hw_pool_set* s, uint32_t pool, hw_pulse** d_pulses, uint32_t** d_lens,
+                        uint32_t** d_overflows);
 /* BatchAnalyzer::operator(): d_trace[lanes][F][64] must be the next chunk
  * (first_frame == previous first_frame + F, starting at 0); otherwise
  * HW_ERR_FRAME_ORDER.  Pulses go to d_pulses[lanes][64][max_calls_per_zmw]

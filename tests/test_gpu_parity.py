@@ -279,3 +279,39 @@ def test_uint8_encoding_equals_its_int16_widening():
                 for z in range(64):
                     assert np.array_equal(q16[l, z, :n[l, z]].view(np.uint8), q8[l, z, :n[l, z]].view(np.uint8))
     assert e16
+
+
+def test_pool_set_equals_per_pool_analyzers():
+    """hw_pool_set: uneven pools (lane counts 1..5, chunk lengths 128/256/512)
+    batched by schedule class (12 pools in 10 classes) give exactly the
+    per-pool analyzers' pulses."""
+    import torch
+    from hw_b200 import filters as Fl
+    cfg = workloads.small_config()
+    cfg.model_estimation_mode = abi.DYNAMIC_ESTIMATIONS
+    lanes = [1, 3, 2, 5, 1, 2, 4, 1, 2, 3, 1, 2]
+    frames = [512] * 6 + [256] * 3 + [128] * 3
+    ps = Fl.PoolSet(cfg, lanes, frames)
+    assert ps.launch_groups < len(lanes)
+    ans = [Fl.BatchAnalyzer(cfg, p, L, F) for p, (L, F) in enumerate(zip(lanes, frames))]
+    gens = [Fl.TraceGenerator(L, workload=2, zmw_offset=1000 * p) for p, L in enumerate(lanes)]
+    emitted_any = False
+    for step in range(12):
+        for p, (g, F) in enumerate(zip(gens, frames)):
+            g.next(step * F, F, out=ps.chunk(p))
+        em, est = ps.process(step)
+        for p, (an, L) in enumerate(zip(ans, lanes)):
+            pulses, lens, ovf, e1, s1 = an(ps.chunk(p).clone(), step * frames[p])
+            assert (bool(em[p]), bool(est[p])) == (e1, s1)
+            if not e1:
+                continue
+            emitted_any = True
+            pp, pl, po = ps.outputs(p)
+            assert torch.equal(pl, lens) and torch.equal(po, ovf)
+            q0 = Fl.struct_to_numpy(pulses, abi.PULSE_DT).reshape(L, 64, cfg.max_calls_per_zmw)
+            q1 = Fl.struct_to_numpy(pp, abi.PULSE_DT).reshape(L, 64, cfg.max_calls_per_zmw)
+            n = lens.cpu().numpy()
+            for l in range(L):
+                for z in range(64):
+                    assert np.array_equal(q0[l, z, :n[l, z]].view(np.uint8), q1[l, z, :n[l, z]].view(np.uint8))
+    assert emitted_any
