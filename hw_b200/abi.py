@@ -157,6 +157,13 @@ DME_DIAG_DT = np.dtype([("iter_count", np.int32, (LANE,)), ("converged", np.int3
                         ("confidence", np.float32, (LANE,)), ("lane_iterations", np.int32),
                         ("pad_", np.int32, (15,))])
 
+# hw_pool_chunk: one pool's row of the hw_chunk_fused table (device pointers as integers)
+POOL_CHUNK_DT = np.dtype([("d_trace", np.uint64), ("d_trace8", np.uint64), ("d_pulses", np.uint64),
+                          ("d_lens", np.uint64), ("d_overflows", np.uint64), ("first_frame", np.int32),
+                          ("emitted", np.int32), ("estimated", np.int32), ("reserved", np.int32)])
+FUSED_TUNING_DT = np.dtype([("frames_per_chunk", np.uint32), ("fuse_label_pulses", np.uint32),
+                            ("labeler_lanes_per_cta", np.uint32), ("reserved", np.uint32)])
+
 SIZES = {
     "hw_stat_accum_state": (STAT_ACCUM_DT, 1024),
     "hw_autocorr_accum_state": (AUTOCORR_DT, 3456),
@@ -166,6 +173,8 @@ SIZES = {
     "hw_lane_hist_bounds": (HIST_BOUNDS_DT, 512),
     "hw_pulse": (PULSE_DT, 20),
     "hw_dme_diag": (DME_DIAG_DT, 1344),
+    "hw_pool_chunk": (POOL_CHUNK_DT, 56),
+    "hw_fused_tuning": (FUSED_TUNING_DT, 16),
 }
 
 

@@ -212,14 +212,20 @@ __global__ void BaselinerInitKernel(int16_t* st16, float* st32, int lanes)
     st32[(size_t)2 * nZmw + g] = 2.0f;     // blSigmaEma_ initial value
 }
 
-template <int FT, typename TIn>
+template <int FT, typename TIn, bool Mapped>
 __global__ void __launch_bounds__(64, 7) BaselinerKernel(BaselinerArgs a, KParams k)
 {
     using Lay = FLayout<FT>;
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    LaneMap map = a.map;
+    if (!Mapped) map.list = nullptr;      // the single-pool variant compiles without the lane list
+    const int gl = blockIdx.x * blockDim.x + threadIdx.x;
     const int nZmw = a.lanes * kLane;
-    if (g >= nZmw) return;     // whole lanes only: nZmw is a multiple of the block size
-    const int lane = g / kLane, z = g % kLane;
+    if (gl >= map.Lanes(a.lanes) * kLane) return;   // whole lanes only: the block is one lane
+    const int z = gl % kLane;
+    const int lane = map.Lane(gl / kLane);
+    const int g = lane * kLane + z;
+    const PoolStep* ps = map.On() ? &map.Pool(lane) : nullptr;
+    const int F = ps ? ps->F : a.F;
 
     // Window state: narrow windows in shared memory (one column per thread),
     // wide ones used in place in global memory.
@@ -255,9 +261,10 @@ __global__ void __launch_bounds__(64, 7) BaselinerKernel(BaselinerArgs a, KParam
     float g_m0 = 0, g_m1 = 0, g_m2 = 0;
 
     const TIn* tr;
-    if constexpr (std::is_same_v<TIn, uint8_t>) tr = a.trace8 + (size_t)lane * a.F * kLane + z;
-    else tr = a.trace + (size_t)lane * a.F * kLane + z;
-    int16_t* out = a.out + (size_t)lane * a.F * kLane + z;
+    const size_t inOff = ps ? (size_t)(lane - ps->lane0) * F * kLane : (size_t)lane * F * kLane;
+    if constexpr (std::is_same_v<TIn, uint8_t>) tr = (ps ? ps->trace8 : a.trace8) + inOff + z;
+    else tr = (ps ? ps->trace : a.trace) + inOff + z;
+    int16_t* out = a.out + map.Block(lane, F) + z;
     const int16_t ped = (int16_t)k.pedestal;
     float sub = 0.0f;
 
@@ -270,7 +277,7 @@ __global__ void __launch_bounds__(64, 7) BaselinerKernel(BaselinerArgs a, KParam
         constexpr int Ph = decltype(phaseTag)::value;
         const int16_t x = xn0;
         xn0 = xn1;
-        if (t + 2 < a.F) xn1 = (int16_t)__ldg(tr + (size_t)(t + 2) * kLane);
+        if (t + 2 < F) xn1 = (int16_t)__ldg(tr + (size_t)(t + 2) * kLane);
         int16_t lo = 0, up = 0;
         const bool haveL = FeedFilter<FT, false, Ph>(x, mem, pc, lo);
         FeedFilter<FT, true, Ph>(x, mem, pc, up);
@@ -329,7 +336,7 @@ __global__ void __launch_bounds__(64, 7) BaselinerKernel(BaselinerArgs a, KParam
         latData = bls;
     };
 #pragma unroll 1
-    for (int t0 = 0; t0 < a.F; t0 += 16)
+    for (int t0 = 0; t0 < F; t0 += 16)
     {
         frame(std::integral_constant<int, 0>{}, t0);
 #pragma unroll 1
@@ -405,8 +412,8 @@ int BaselinerNumSlots16(int ft)
     return -1;
 }
 
-template <int FT, typename TIn>
-cudaError_t LaunchBaselinerT2(const BaselinerArgs& a, const KParams& k, cudaStream_t s)
+template <int FT, typename TIn, bool Mapped>
+cudaError_t LaunchBaselinerT3(const BaselinerArgs& a, const KParams& k, cudaStream_t s)
 {
     const int threads = kLane;
     const size_t smem = sizeof(int16_t) * FLayout<FT>::SmemSlots() * threads;
@@ -418,18 +425,27 @@ cudaError_t LaunchBaselinerT2(const BaselinerArgs& a, const KParams& k, cudaStre
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64 || !attrSet[dev])
     {
-        e = cudaFuncSetAttribute(BaselinerKernel<FT, TIn>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = cudaFuncSetAttribute(BaselinerKernel<FT, TIn, Mapped>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < 64) attrSet[dev] = true;
     }
-    BaselinerKernel<FT, TIn><<<a.lanes, threads, smem, s>>>(a, k);
+    const int blocks = a.map.Lanes(a.lanes);
+    if (blocks == 0) return cudaSuccess;
+    BaselinerKernel<FT, TIn, Mapped><<<blocks, threads, smem, s>>>(a, k);
     return cudaGetLastError();
+}
+
+template <int FT, typename TIn>
+cudaError_t LaunchBaselinerT2(const BaselinerArgs& a, const KParams& k, cudaStream_t s)
+{
+    return a.map.On() ? LaunchBaselinerT3<FT, TIn, true>(a, k, s) : LaunchBaselinerT3<FT, TIn, false>(a, k, s);
 }
 
 template <int FT>
 cudaError_t LaunchBaselinerT(const BaselinerArgs& a, const KParams& k, cudaStream_t s)
 {
-    return a.trace8 ? LaunchBaselinerT2<FT, uint8_t>(a, k, s) : LaunchBaselinerT2<FT, int16_t>(a, k, s);
+    const bool u8 = a.map.On() ? a.u8 != 0 : a.trace8 != nullptr;
+    return u8 ? LaunchBaselinerT2<FT, uint8_t>(a, k, s) : LaunchBaselinerT2<FT, int16_t>(a, k, s);
 }
 
 cudaError_t LaunchBaseliner(int ft, const BaselinerArgs& a, const KParams& k, cudaStream_t s)

@@ -552,11 +552,23 @@ __device__ __forceinline__ int ChooseStart(const KParams& k, const EmHist& h, co
     return 0;
 }
 
+template <bool Mapped>
 __global__ void __launch_bounds__(kLane, 12) DmeEstimateKernel(DmeArgs A, KParams k)
 {
-    const int l = blockIdx.x;
+    LaneMap map = A.map;
+    if (!Mapped) map.list = nullptr;      // the single-pool variant compiles without the lane list
+    // scratch belongs to the launch lane, the rest to the (engine) lane
+    const int li = blockIdx.x;
+    const int l = map.Lane(li);
     const int z = threadIdx.x;
-    float* bpS = A.scratch + (size_t)l * 3 * (kBins + 1) * kLane;
+    int32_t tModel = A.tModel, tEst = A.tEst;
+    if (map.On())
+    {
+        const PoolStep& ps = map.Pool(l);
+        tModel = ps.tModel;
+        tEst = ps.tEst;
+    }
+    float* bpS = A.scratch + (size_t)li * 3 * (kBins + 1) * kLane;
     float* tau0S = bpS + (size_t)(kBins + 1) * kLane;
     float* facS = tau0S + (size_t)(kBins + 1) * kLane;
 
@@ -565,7 +577,7 @@ __global__ void __launch_bounds__(kLane, 12) DmeEstimateKernel(DmeArgs A, KParam
     ModelF det;
     EmVars v;
     EmReg r;
-    DmePrelude(k, A.models[l], A.stats[l], h, A.tModel, A.tEst, det, v, r);
+    DmePrelude(k, A.models[l], A.stats[l], h, tModel, tEst, det, v, r);
     if (A.proposal)
     {
         float llPlain, llStart;
@@ -705,7 +717,10 @@ __global__ void __launch_bounds__(kLane, 12) DmeEstimateKernel(DmeArgs A, KParam
 
 cudaError_t LaunchDmeEstimate(const DmeArgs& a, const KParams& k, cudaStream_t s)
 {
-    DmeEstimateKernel<<<a.lanes, kLane, 0, s>>>(a, k);
+    const int blocks = a.map.Lanes(a.lanes);
+    if (blocks == 0) return cudaSuccess;
+    if (a.map.On()) DmeEstimateKernel<true><<<blocks, kLane, 0, s>>>(a, k);
+    else DmeEstimateKernel<false><<<blocks, kLane, 0, s>>>(a, k);
     return cudaGetLastError();
 }
 

@@ -1,0 +1,651 @@
+// Fused chunk engine: every pool of a basecaller in one handle, each stage of
+// a chunk step one launch over a list of lanes (hw_chunk_fused).
+//
+// The reference runs one BatchAnalyzer per pool and chunk
+// (AN/BatchAnalyzer.cpp:119-375, AN = src/basecaller/basecaller/analyzer),
+// each of its filters launching over that pool's lanes.  Here the state of
+// all pools is packed lane after lane; per step the host walks every pool's
+// schedule (the DetectionModelEstimator state machine,
+// TA/DetectionModelEstimator.cpp:93-160, and the Fixed / SingleEstimate /
+// DynamicEstimate analyzers, AN/BatchAnalyzer.cpp:172-375) and appends the
+// pool's lanes to the list of every stage it takes.  The lists go to the
+// device with one copy each and every stage runs once over its list, so a
+// step is about a dozen launches however many pools there are and however
+// uneven they are.  Nothing in a step waits for the device: device-detected
+// failures travel back through a pinned word read two steps later.
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "hw_device.cuh"
+
+using namespace hwk;
+
+namespace {
+
+int Fail(int code, const std::string& msg) { return hwk::SetLastError(code, msg.c_str()); }
+
+#define HWF_CUDA(expr, where)                                                                     \
+    do {                                                                                          \
+        cudaError_t e_ = (expr);                                                                  \
+        if (e_ != cudaSuccess) return Fail(HW_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T>
+int Alloc(T** p, size_t count, const char* where)
+{
+    *p = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+    if (e != cudaSuccess) return Fail(HW_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+    return HW_OK;
+}
+
+template <typename T>
+int AllocZero(T** p, size_t count, const char* where)
+{
+    int rc = Alloc(p, count, where);
+    if (rc) return rc;
+    HWF_CUDA(cudaMemset(*p, 0, std::max<size_t>(count, 1) * sizeof(T)), where);
+    return HW_OK;
+}
+
+// The stage lists of one step, in launch order.
+enum List
+{
+    L_BASE16,     // baseline filter, int16 chunks
+    L_BASE8,      // baseline filter, uint8 chunks
+    L_AGG,        // BaselineStatsAggregator::AddMetrics
+    L_HIST,       // TraceHistogramAccumulator::AddBatch
+    L_INIT,       // CoreDMEstimator::InitDetectionModels
+    L_DME,        // CoreDMEstimator::Estimate
+    L_RESET,      // histogram reset from the aggregated statistics + aggregator reset
+    L_LABEL,      // frame labeler + pulse accumulator, separate kernels
+    L_LP,         // frame labeler + pulse accumulator, one kernel
+    L_ZERO,       // pools that emit nothing this step
+    kNumLists
+};
+
+// Per pool: hw_analyzer's schedule state.
+struct PoolRt
+{
+    enum Status { HIST_INIT = 0, DME_INIT = 1, SEQUENCING = 2 };
+    uint32_t id = 0, lanes = 0, F = 0, lane0 = 0;
+    int status = HIST_INIT;
+    int32_t framesRemaining = 0;
+    bool initialized = false, fullEstimation = false, histInitialized = false, diagValid = false;
+    int32_t blLatency = 0, poolDelay = 0, nextFrame = 0;
+    hw_frame_interval modelFi{0, 0}, aggFi{0, 0}, histFi{0, 0};
+};
+
+hw_frame_interval Merge(hw_frame_interval a, hw_frame_interval b)
+{
+    const bool aEmpty = a.lower == a.upper, bEmpty = b.lower == b.upper;
+    if (aEmpty) return b;
+    if (bEmpty) return a;
+    return hw_frame_interval{std::min(a.lower, b.lower), std::max(a.upper, b.upper)};
+}
+
+int32_t Center(hw_frame_interval fi) { return fi.lower + (fi.upper - fi.lower) / 2; }
+
+}   // namespace
+
+struct hw_fused
+{
+    hw_config cfg;
+    hwp::Derived d;
+    KParams k;
+    std::vector<PoolRt> pools;
+    uint32_t lanes = 0;
+    int maxF = 0;
+    // tuning per chunk length: {fuse label+pulses, labeler lanes per block}
+    std::map<uint32_t, std::pair<uint32_t, uint32_t>> tuning;
+
+    // device state, packed over the engine's lanes
+    int16_t* st16 = nullptr;
+    float* st32 = nullptr;
+    hw_baseliner_stats* stats = nullptr;
+    hw_baseliner_stats* acc = nullptr;
+    hw_lane_histogram* hist = nullptr;
+    int16_t* edgePrev = nullptr;
+    uint8_t* edgeBits = nullptr;
+    hw_lane_model* models = nullptr;
+    hw_dme_diag* diag = nullptr;
+    float* dmeScratch = nullptr;      // [launch lane][3][kBins + 1][64]
+    uint32_t dmeCap = 0;              // launch lanes the scratch holds
+    hw_lane_model* latModel = nullptr;
+    int16_t* latLabel = nullptr;
+    int16_t* latRoi = nullptr;
+    int16_t* latTrc = nullptr;
+    int16_t* prevLat = nullptr;
+    uint32_t* tb = nullptr;
+    int16_t* bls = nullptr;
+    int16_t* labels = nullptr;
+    int16_t* latent = nullptr;
+    float* score = nullptr;
+    hw_stat_accum_state* paStats = nullptr;
+    uint32_t* segStart = nullptr;
+    int16_t* segFirst = nullptr;
+    int16_t* segLast = nullptr;
+    int16_t* segMax = nullptr;
+    float* segTotal = nullptr;
+    float* segM2 = nullptr;
+    int16_t* segLabel = nullptr;
+    int* err = nullptr;
+
+    // lane tables and the per-step tables (pinned host copies, two in flight)
+    int32_t* dPoolOf = nullptr;
+    uint64_t* dFrameOff = nullptr;
+    PoolStep* dSteps = nullptr;
+    int32_t* dLists = nullptr;        // [kNumLists][lanes]
+    PoolStep* hSteps[2] = {nullptr, nullptr};
+    int32_t* hLists[2] = {nullptr, nullptr};
+    int* hErr[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    bool inFlight[2] = {false, false};
+    uint64_t step = 0;
+    int sticky = HW_OK;
+
+    // CUDA graphs per step plan, captured on a stream of the engine's own
+    // (the caller's stream may be the legacy default stream, which cannot be
+    // captured) and replayed on the caller's stream
+    bool graphs = false;
+    cudaStream_t capStream = nullptr;
+    std::map<std::vector<int64_t>, cudaGraphExec_t> graphCache;
+    std::map<std::vector<int64_t>, int> planSeen;
+    uint32_t lastLaunches = 0, lastGraphLaunches = 0;
+
+    ~hw_fused()
+    {
+        for (auto& g : graphCache) cudaGraphExecDestroy(g.second);
+        if (capStream) cudaStreamDestroy(capStream);
+        for (int b = 0; b < 2; ++b)
+        {
+            if (ev[b]) cudaEventDestroy(ev[b]);
+            cudaFreeHost(hSteps[b]);
+            cudaFreeHost(hLists[b]);
+            cudaFreeHost(hErr[b]);
+        }
+        void* bufs[] = {st16, st32, stats, acc, hist, edgePrev, edgeBits, models, diag, dmeScratch, latModel,
+                        latLabel, latRoi, latTrc, prevLat, tb, bls, labels, latent, score, paStats, segStart,
+                        segFirst, segLast, segMax, segTotal, segM2, segLabel, err, dPoolOf, dFrameOff, dSteps,
+                        dLists};
+        for (void* p : bufs) cudaFree(p);
+    }
+
+    int Launch(cudaStream_t s, const int32_t counts[kNumLists], const int maxFList[kNumLists], uint32_t* launches);
+    int Schedule(hw_pool_chunk* table, int b, int32_t counts[kNumLists], int maxFList[kNumLists]);
+};
+
+// Walks every pool's schedule for this step (host state only) and fills the
+// stage lists and per-pool step records of buffer b.
+int hw_fused::Schedule(hw_pool_chunk* table, int b, int32_t counts[kNumLists], int maxFList[kNumLists])
+{
+    for (int s = 0; s < kNumLists; ++s) { counts[s] = 0; maxFList[s] = 0; }
+    int32_t* lists = hLists[b];
+    const int minFrames = (int)cfg.min_frames_for_estimate;
+    for (size_t p = 0; p < pools.size(); ++p)
+    {
+        PoolRt& P = pools[p];
+        hw_pool_chunk& c = table[p];
+        const int32_t ff = c.first_frame;
+        PoolStep& st = hSteps[b][p];
+        st = PoolStep{c.d_trace, c.d_trace8, c.d_pulses, c.d_lens, c.d_overflows, ff, (int32_t)P.F, (int32_t)P.lane0,
+                      0, 0, 0};
+        auto append = [&](int s) {
+            int32_t* dst = lists + (size_t)s * lanes + counts[s];
+            for (uint32_t i = 0; i < P.lanes; ++i) dst[i] = (int32_t)(P.lane0 + i);
+            counts[s] += (int32_t)P.lanes;
+            maxFList[s] = std::max(maxFList[s], (int)P.F);
+        };
+        append(c.d_trace8 ? L_BASE8 : L_BASE16);
+        const hw_frame_interval fi{ff, ff + (int32_t)P.F};
+        bool ran = false, emit = false;
+        // DetectionModelEstimator::AddBatch (DetectionModelEstimator.cpp:93-160)
+        auto dmeAdd = [&]() -> int {
+            append(L_AGG);
+            P.aggFi = Merge(P.aggFi, fi);
+            if (P.status != PoolRt::HIST_INIT)
+            {
+                if (!P.histInitialized)
+                    return Fail(HW_ERR_NOT_INITIALIZED, "histogram used before its bounds were set");
+                append(L_HIST);
+                P.histFi = Merge(P.histFi, fi);
+            }
+            if (P.status != PoolRt::SEQUENCING)
+            {
+                append(L_INIT);
+                P.modelFi = P.aggFi;
+            }
+            P.framesRemaining -= (int32_t)P.F;
+            if (P.framesRemaining <= 0)
+            {
+                if (P.status == PoolRt::DME_INIT) P.status = PoolRt::SEQUENCING;
+                if (P.status == PoolRt::SEQUENCING)
+                {
+                    if (P.histFi.lower == P.histFi.upper || P.modelFi.lower == P.modelFi.upper)
+                        return Fail(HW_ERR_INVALID_ARG, "frame intervals must not be empty");
+                    ran = true;
+                    st.tModel = Center(P.modelFi);
+                    st.tEst = Center(P.histFi);
+                    append(L_DME);
+                    P.diagValid = true;
+                    P.modelFi = P.histFi;
+                }
+                append(L_RESET);
+                P.histInitialized = true;
+                P.histFi = hw_frame_interval{0, 0};
+                P.aggFi = hw_frame_interval{0, 0};
+                if (P.status == PoolRt::HIST_INIT) P.status = PoolRt::DME_INIT;
+                P.framesRemaining = minFrames;
+            }
+            return HW_OK;
+        };
+        auto labelAndPulse = [&]() {
+            auto t = tuning.find(P.F);
+            append((t != tuning.end() && t->second.first) ? L_LP : L_LABEL);
+        };
+        int rc = HW_OK;
+        if (cfg.model_estimation_mode == HW_FIXED_ESTIMATIONS)
+        {
+            // FixedModelBatchAnalyzer::AnalyzeImpl (BatchAnalyzer.cpp:172-207)
+            labelAndPulse();
+            emit = true;
+        }
+        else if (cfg.model_estimation_mode == HW_INITIAL_ESTIMATIONS)
+        {
+            // SingleEstimateBatchAnalyzer::AnalyzeImpl (BatchAnalyzer.cpp:177-256)
+            if (!P.initialized && ff > P.blLatency)
+            {
+                if ((rc = dmeAdd())) return rc;
+                P.initialized = ran;
+            }
+            if (P.initialized)
+            {
+                labelAndPulse();
+                emit = true;
+            }
+        }
+        else
+        {
+            // DynamicEstimateBatchAnalyzer::AnalyzeImpl (BatchAnalyzer.cpp:289-375)
+            if (ff >= P.blLatency + P.poolDelay)
+            {
+                if ((rc = dmeAdd())) return rc;
+                if (ran) P.fullEstimation = true;
+                labelAndPulse();
+                emit = P.fullEstimation;
+            }
+        }
+        if (!emit) append(L_ZERO);
+        P.nextFrame = ff + (int32_t)P.F;
+        c.emitted = emit ? 1 : 0;
+        c.estimated = ran ? 1 : 0;
+    }
+    return HW_OK;
+}
+
+// Enqueues the step's kernels over the device lists (also what a graph captures).
+int hw_fused::Launch(cudaStream_t s, const int32_t counts[kNumLists], const int maxFList[kNumLists],
+                     uint32_t* launches)
+{
+    uint32_t n = 0;
+    auto map = [&](int l) {
+        LaneMap m;
+        m.list = dLists + (size_t)l * lanes;
+        m.n = counts[l];
+        m.poolOf = dPoolOf;
+        m.frameOff = dFrameOff;
+        m.pools = dSteps;
+        return m;
+    };
+    const int L = (int)lanes;
+    for (int l : {L_BASE16, L_BASE8})
+        if (counts[l])
+        {
+            BaselinerArgs a{nullptr, bls, stats, st16, st32, L, maxFList[l]};
+            a.map = map(l);
+            a.u8 = l == L_BASE8;
+            HWF_CUDA(LaunchBaseliner(cfg.filter_type, a, k, s), "hw_chunk_fused: baseline filter");
+            ++n;
+        }
+    if (counts[L_AGG])
+    {
+        HWF_CUDA(LaunchAggMerge(acc, stats, L, s, map(L_AGG)), "hw_chunk_fused: statistics merge");
+        ++n;
+    }
+    if (counts[L_HIST])
+    {
+        HWF_CUDA(LaunchHistAdd(hist, edgePrev, edgeBits, bls, maxFList[L_HIST], models, L, s, map(L_HIST)),
+                 "hw_chunk_fused: histogram");
+        ++n;
+    }
+    if (counts[L_INIT])
+    {
+        HWF_CUDA(LaunchInitModels(models, acc, L, k, s, map(L_INIT)), "hw_chunk_fused: model initialisation");
+        ++n;
+    }
+    if (counts[L_DME])
+    {
+        DmeArgs a{hist, acc, models, diag, dmeScratch, err, L, 0, 0};
+        a.map = map(L_DME);
+        HWF_CUDA(LaunchDmeEstimate(a, k, s), "hw_chunk_fused: DME");
+        ++n;
+    }
+    if (counts[L_RESET])
+    {
+        HWF_CUDA(LaunchHistResetStats(hist, acc, L, k, err, s, map(L_RESET)), "hw_chunk_fused: histogram reset");
+        HWF_CUDA(LaunchAggReset(acc, L, s, map(L_RESET)), "hw_chunk_fused: aggregator reset");
+        n += 2;
+    }
+    if (counts[L_LABEL])
+    {
+        LabelerArgs la{bls, models, labels, latent, score, latModel, latLabel, latRoi, latTrc, prevLat, tb, L,
+                       maxFList[L_LABEL]};
+        la.map = map(L_LABEL);
+        HWF_CUDA(LaunchLabeler(la, k, s), "hw_chunk_fused: labeler");
+        PulseArgs pa{labels, latent, bls, models, nullptr, nullptr, nullptr, paStats, segStart, segFirst, segLast,
+                     segMax, segTotal, segM2, segLabel, L, maxFList[L_LABEL], 0};
+        pa.map = map(L_LABEL);
+        HWF_CUDA(LaunchPulses(pa, k, s), "hw_chunk_fused: pulse accumulator");
+        n += 3;
+    }
+    if (counts[L_LP])
+        return Fail(HW_ERR_UNSUPPORTED, "fused labeler and pulse kernel is not built");
+    if (counts[L_ZERO])
+    {
+        HWF_CUDA(LaunchZeroOutputs(map(L_ZERO), s), "hw_chunk_fused: empty outputs");
+        ++n;
+    }
+    *launches = n;
+    return HW_OK;
+}
+
+namespace {
+
+const char* kDeferredMsg =
+    "a device-side check failed in an earlier step (histogram bounds, UHistogramSimd.cpp:66-96, or a DME sanity "
+    "assertion); the analysis cannot continue";
+
+// Collects the failure word of buffer b's step once that step has finished.
+int Collect(hw_fused* f, int b)
+{
+    if (!f->inFlight[b]) return HW_OK;
+    HWF_CUDA(cudaEventSynchronize(f->ev[b]), "hw_chunk_fused");
+    f->inFlight[b] = false;
+    if (*f->hErr[b] != 0 && f->sticky == HW_OK) f->sticky = *f->hErr[b];
+    return HW_OK;
+}
+
+}   // namespace
+
+extern "C" {
+
+int hw_fused_create(const hw_config* cfg, uint32_t n_pools, const uint32_t* pool_ids, const uint32_t* lanes,
+                    const uint32_t* frames_per_chunk, hw_fused** out)
+{
+    if (!cfg || !lanes || !frames_per_chunk || !out || n_pools == 0) return Fail(HW_ERR_INVALID_ARG, "bad argument");
+    *out = nullptr;
+    auto f = std::make_unique<hw_fused>();
+    int rc = hwk::PrepareConfigNoAlloc(cfg, &f->d, &f->k);
+    if (rc) return rc;
+    f->cfg = *cfg;
+    const uint32_t stride = (uint32_t)f->d.aggStride;
+    const uint32_t minFrames = std::max(cfg->min_frames_for_estimate, 1u);
+    uint64_t total = 0, frameElems = 0;
+    std::vector<int32_t> poolOf;
+    std::vector<uint64_t> frameOff;
+    f->pools.resize(n_pools);
+    for (uint32_t p = 0; p < n_pools; ++p)
+    {
+        const uint32_t F = frames_per_chunk[p];
+        if (lanes[p] == 0) return Fail(HW_ERR_INVALID_ARG, "every pool needs at least one lane");
+        if (F % stride != 0 || F < (uint32_t)(kLatent + kLookback) || F > 1024)
+            return Fail(HW_ERR_INVALID_ARG,
+                        "frames_per_chunk must be a multiple of the filter's aggregate stride in [40, 1024]");
+        if (total + lanes[p] > (uint64_t)INT32_MAX / kLane) return Fail(HW_ERR_INVALID_ARG, "too many lanes");
+        PoolRt& P = f->pools[p];
+        P.id = pool_ids ? pool_ids[p] : p;
+        P.lanes = lanes[p];
+        P.F = F;
+        P.lane0 = (uint32_t)total;
+        P.framesRemaining = (int32_t)cfg->num_frames_pre_accum_stats;
+        P.blLatency = (int32_t)f->d.baselinerStartupLatency;
+        const uint32_t chunksPerEstimate = (minFrames + F - 1) / F;
+        P.poolDelay = (int32_t)((P.id % chunksPerEstimate) * F);
+        for (uint32_t i = 0; i < lanes[p]; ++i)
+        {
+            poolOf.push_back((int32_t)p);
+            frameOff.push_back(frameElems);
+            frameElems += (uint64_t)F * kLane;
+        }
+        total += lanes[p];
+        f->maxF = std::max(f->maxF, (int)F);
+    }
+    const uint32_t L = (uint32_t)total;
+    f->lanes = L;
+    const size_t nZmw = (size_t)L * kLane;
+    const char* where = "hw_fused_create";
+    const int slots16 = BaselinerNumSlots16(cfg->filter_type);
+    if ((rc = Alloc(&f->st16, (size_t)slots16 * nZmw, where))) return rc;
+    if ((rc = Alloc(&f->st32, 3 * nZmw, where))) return rc;
+    HWF_CUDA(LaunchBaselinerInit(cfg->filter_type, f->st16, f->st32, (int)L, 0), where);
+    if ((rc = AllocZero(&f->stats, L, where))) return rc;
+    if ((rc = Alloc(&f->acc, L, where))) return rc;
+    HWF_CUDA(LaunchAggReset(f->acc, (int)L, 0), where);
+    if ((rc = AllocZero(&f->hist, L, where))) return rc;
+    if ((rc = AllocZero(&f->edgePrev, nZmw, where))) return rc;
+    if ((rc = AllocZero(&f->edgeBits, nZmw, where))) return rc;
+    if ((rc = AllocZero(&f->models, L, where))) return rc;
+    if (cfg->model_estimation_mode == HW_FIXED_ESTIMATIONS)
+    {
+        // FixedModelBatchAnalyzer: the static model in every lane, from the start
+        hw_lane_model m;
+        hwp::StaticModel(*cfg, &m);
+        std::vector<hw_lane_model> host(L, m);
+        HWF_CUDA(cudaMemcpy(f->models, host.data(), sizeof(hw_lane_model) * L, cudaMemcpyHostToDevice), where);
+    }
+    if ((rc = AllocZero(&f->diag, L, where))) return rc;
+    if ((rc = Alloc(&f->latModel, L, where))) return rc;
+    {
+        // LatentViterbi ctor (FrameLabelerHost.cpp:58-70): baseline N(0, 50), analogs N(1000, 10).
+        hw_lane_model lm;
+        std::memset(&lm, 0, sizeof(lm));
+        for (int z = 0; z < kLane; ++z)
+        {
+            lm.baseline.means[z] = hwm::f32_to_f16_bits(0.0f);
+            lm.baseline.vars[z] = hwm::f32_to_f16_bits(50.0f);
+            for (int a = 0; a < kAnalogs; ++a)
+            {
+                lm.analogs[a].means[z] = hwm::f32_to_f16_bits(1000.0f);
+                lm.analogs[a].vars[z] = hwm::f32_to_f16_bits(10.0f);
+            }
+        }
+        std::vector<hw_lane_model> host(L, lm);
+        HWF_CUDA(cudaMemcpy(f->latModel, host.data(), sizeof(hw_lane_model) * L, cudaMemcpyHostToDevice), where);
+    }
+    if ((rc = AllocZero(&f->latLabel, nZmw, where))) return rc;
+    if ((rc = AllocZero(&f->latRoi, nZmw, where))) return rc;
+    if ((rc = AllocZero(&f->latTrc, nZmw, where))) return rc;
+    if ((rc = AllocZero(&f->prevLat, (size_t)kLatent * nZmw, where))) return rc;
+    if ((rc = Alloc(&f->tb, frameElems + (size_t)kLookback * nZmw, where))) return rc;
+    if ((rc = Alloc(&f->bls, frameElems, where))) return rc;
+    if ((rc = Alloc(&f->labels, frameElems, where))) return rc;
+    if ((rc = AllocZero(&f->latent, (size_t)kLatent * nZmw, where))) return rc;
+    if ((rc = AllocZero(&f->score, nZmw, where))) return rc;
+    if ((rc = AllocZero(&f->paStats, L, where))) return rc;
+    if ((rc = AllocZero(&f->segStart, nZmw, where))) return rc;
+    if ((rc = AllocZero(&f->segFirst, nZmw, where))) return rc;
+    if ((rc = AllocZero(&f->segLast, nZmw, where))) return rc;
+    if ((rc = AllocZero(&f->segMax, nZmw, where))) return rc;
+    if ((rc = AllocZero(&f->segTotal, nZmw, where))) return rc;
+    if ((rc = AllocZero(&f->segM2, nZmw, where))) return rc;
+    if ((rc = AllocZero(&f->segLabel, nZmw, where))) return rc;
+    if ((rc = AllocZero(&f->err, 1, where))) return rc;
+    if ((rc = Alloc(&f->dPoolOf, L, where))) return rc;
+    if ((rc = Alloc(&f->dFrameOff, L, where))) return rc;
+    HWF_CUDA(cudaMemcpy(f->dPoolOf, poolOf.data(), L * sizeof(int32_t), cudaMemcpyHostToDevice), where);
+    HWF_CUDA(cudaMemcpy(f->dFrameOff, frameOff.data(), L * sizeof(uint64_t), cudaMemcpyHostToDevice), where);
+    if ((rc = AllocZero(&f->dSteps, n_pools, where))) return rc;
+    if ((rc = AllocZero(&f->dLists, (size_t)kNumLists * L, where))) return rc;
+    for (int b = 0; b < 2; ++b)
+    {
+        HWF_CUDA(cudaMallocHost((void**)&f->hSteps[b], sizeof(PoolStep) * n_pools), where);
+        HWF_CUDA(cudaMallocHost((void**)&f->hLists[b], sizeof(int32_t) * kNumLists * (size_t)L), where);
+        HWF_CUDA(cudaMallocHost((void**)&f->hErr[b], sizeof(int)), where);
+        *f->hErr[b] = 0;
+        HWF_CUDA(cudaEventCreateWithFlags(&f->ev[b], cudaEventDisableTiming), where);
+    }
+    HWF_CUDA(cudaDeviceSynchronize(), where);
+    *out = f.release();
+    return HW_OK;
+}
+
+int hw_fused_destroy(hw_fused* f)
+{
+    if (f) cudaDeviceSynchronize();
+    delete f;
+    return HW_OK;
+}
+
+int hw_fused_use_graphs(hw_fused* f, int32_t enable)
+{
+    if (!f) return Fail(HW_ERR_INVALID_ARG, "NULL engine");
+    f->graphs = enable != 0;
+    return HW_OK;
+}
+
+int hw_fused_set_tuning(hw_fused* f, const hw_fused_tuning* t, uint32_t n)
+{
+    if (!f || (n && !t)) return Fail(HW_ERR_INVALID_ARG, "bad argument");
+    for (uint32_t i = 0; i < n; ++i)
+    {
+        const uint32_t lpc = t[i].labeler_lanes_per_cta;
+        if (lpc != 1 && lpc != 2 && lpc != 4) return Fail(HW_ERR_INVALID_ARG, "labeler_lanes_per_cta must be 1, 2 or 4");
+        if (t[i].fuse_label_pulses > 1) return Fail(HW_ERR_INVALID_ARG, "fuse_label_pulses must be 0 or 1");
+    }
+    for (uint32_t i = 0; i < n; ++i)
+        f->tuning[t[i].frames_per_chunk] = {t[i].fuse_label_pulses, t[i].labeler_lanes_per_cta};
+    return HW_OK;
+}
+
+int hw_chunk_fused(hw_fused* f, hw_pool_chunk* table, uint32_t n_pools, void* stream)
+{
+    if (!f || !table) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    if (n_pools != f->pools.size()) return Fail(HW_ERR_INVALID_ARG, "the table must list every pool of the engine");
+    for (uint32_t p = 0; p < n_pools; ++p)
+    {
+        const hw_pool_chunk& c = table[p];
+        if (!(c.d_trace || c.d_trace8) || !c.d_pulses || !c.d_lens || !c.d_overflows)
+            return Fail(HW_ERR_INVALID_ARG, "NULL buffer in the pool table");
+        if (c.first_frame != f->pools[p].nextFrame) return Fail(HW_ERR_FRAME_ORDER, "Bad frame ID.");
+    }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const int b = (int)(f->step & 1);
+    int rc;
+    // the step that last used buffer b must be done before its tables are rewritten
+    if ((rc = Collect(f, b))) return rc;
+    if (f->sticky) return Fail(f->sticky, kDeferredMsg);
+    int32_t counts[kNumLists];
+    int maxFList[kNumLists];
+    if ((rc = f->Schedule(table, b, counts, maxFList))) return rc;
+    if ((uint32_t)counts[L_DME] > f->dmeCap)
+    {
+        // grow the DME scratch (graphs hold the old pointer)
+        for (auto& g : f->graphCache) cudaGraphExecDestroy(g.second);
+        f->graphCache.clear();
+        HWF_CUDA(cudaFree(f->dmeScratch), "hw_chunk_fused");
+        f->dmeScratch = nullptr;
+        f->dmeCap = 0;
+        if ((rc = Alloc(&f->dmeScratch, (size_t)counts[L_DME] * 3 * (kBins + 1) * kLane, "hw_chunk_fused"))) return rc;
+        f->dmeCap = (uint32_t)counts[L_DME];
+    }
+    HWF_CUDA(cudaMemcpyAsync(f->dSteps, f->hSteps[b], sizeof(PoolStep) * n_pools, cudaMemcpyHostToDevice, s),
+             "hw_chunk_fused");
+    for (int l = 0; l < kNumLists; ++l)
+        if (counts[l])
+            HWF_CUDA(cudaMemcpyAsync(f->dLists + (size_t)l * f->lanes, f->hLists[b] + (size_t)l * f->lanes,
+                                     sizeof(int32_t) * counts[l], cudaMemcpyHostToDevice, s),
+                     "hw_chunk_fused");
+    uint32_t launches = 0, graphLaunches = 0;
+    if (f->graphs)
+    {
+        std::vector<int64_t> key;
+        for (int l = 0; l < kNumLists; ++l)
+        {
+            key.push_back(counts[l]);
+            key.push_back(maxFList[l]);
+        }
+        auto it = f->graphCache.find(key);
+        if (it == f->graphCache.end() && ++f->planSeen[key] >= 2)
+        {
+            // second sighting of this plan: capture it
+            if (!f->capStream)
+                HWF_CUDA(cudaStreamCreateWithFlags(&f->capStream, cudaStreamNonBlocking), "hw_chunk_fused: capture");
+            HWF_CUDA(cudaStreamBeginCapture(f->capStream, cudaStreamCaptureModeThreadLocal), "hw_chunk_fused: capture");
+            uint32_t n = 0;
+            rc = f->Launch(f->capStream, counts, maxFList, &n);
+            cudaGraph_t g = nullptr;
+            const cudaError_t ce = cudaStreamEndCapture(f->capStream, &g);
+            if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+            HWF_CUDA(ce, "hw_chunk_fused: capture");
+            cudaGraphExec_t ge = nullptr;
+            const cudaError_t ie = cudaGraphInstantiate(&ge, g, 0);
+            cudaGraphDestroy(g);
+            HWF_CUDA(ie, "hw_chunk_fused: graph instantiation");
+            it = f->graphCache.emplace(key, ge).first;
+        }
+        if (it != f->graphCache.end())
+        {
+            HWF_CUDA(cudaGraphLaunch(it->second, s), "hw_chunk_fused: graph launch");
+            graphLaunches = 1;
+        }
+    }
+    if (!graphLaunches && (rc = f->Launch(s, counts, maxFList, &launches))) return rc;
+    HWF_CUDA(cudaMemcpyAsync(f->hErr[b], f->err, sizeof(int), cudaMemcpyDeviceToHost, s), "hw_chunk_fused");
+    HWF_CUDA(cudaEventRecord(f->ev[b], s), "hw_chunk_fused");
+    f->inFlight[b] = true;
+    f->lastLaunches = launches;
+    f->lastGraphLaunches = graphLaunches;
+    ++f->step;
+    return HW_OK;
+}
+
+int hw_fused_finish(hw_fused* f, void* stream)
+{
+    if (!f) return Fail(HW_ERR_INVALID_ARG, "NULL engine");
+    (void)stream;
+    int rc;
+    for (int i = 0; i < 2; ++i)
+    {
+        // oldest step first
+        const int b = (int)((f->step + i) & 1);
+        if ((rc = Collect(f, b))) return rc;
+    }
+    if (f->sticky) return Fail(f->sticky, kDeferredMsg);
+    return HW_OK;
+}
+
+int hw_fused_models(const hw_fused* f, uint32_t pool, hw_lane_model* d_out, hw_frame_interval* fi, void* stream)
+{
+    if (!f || !d_out || pool >= f->pools.size()) return Fail(HW_ERR_INVALID_ARG, "bad argument");
+    const PoolRt& P = f->pools[pool];
+    HWF_CUDA(cudaMemcpyAsync(d_out, f->models + P.lane0, sizeof(hw_lane_model) * P.lanes, cudaMemcpyDeviceToDevice,
+                             reinterpret_cast<cudaStream_t>(stream)),
+             "hw_fused_models");
+    if (fi) *fi = P.modelFi;
+    return HW_OK;
+}
+
+int hw_fused_last_step(const hw_fused* f, uint32_t* launches, uint32_t* graph_launches)
+{
+    if (!f) return Fail(HW_ERR_INVALID_ARG, "NULL engine");
+    if (launches) *launches = f->lastLaunches;
+    if (graph_launches) *graph_launches = f->lastGraphLaunches;
+    return HW_OK;
+}
+
+}   // extern "C"

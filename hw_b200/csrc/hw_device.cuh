@@ -99,6 +99,63 @@ __device__ __forceinline__ float SignalCovar(const KParams& k, float cv2, float 
     return r;
 }
 
+// ---- lane lists (multi-pool launches) ----------------------------------------
+// A fused engine keeps the state of all its pools packed lane after lane and
+// runs each stage as one launch over a list of its lanes.  Per pool and
+// chunk step it publishes a PoolStep (the caller's buffers, the first frame
+// and the DME frame-interval centers).
+
+struct PoolStep
+{
+    const int16_t* trace;       // [lanes][F][64] int16 chunk, or null
+    const uint8_t* trace8;      // [lanes][F][64] uint8 chunk, or null
+    hw_pulse* pulses;           // [lanes][64][cap]
+    uint32_t* lens;             // [lanes][64]
+    uint32_t* ovf;              // [lanes][64]
+    int32_t firstFrame;         // of the trace chunk
+    int32_t F;
+    int32_t lane0;              // first engine lane of the pool
+    int32_t tModel, tEst;       // DME frame-interval centers
+    int32_t pad_;
+};
+
+struct LaneMap
+{
+    const int32_t* list = nullptr;     // launch lane -> engine lane; null: single-pool launch
+    int n = 0;                         // launch lanes when list is set
+    const int32_t* poolOf = nullptr;   // engine lane -> pool
+    const uint64_t* frameOff = nullptr;// engine lane -> element offset of its [F][64] block
+    const PoolStep* pools = nullptr;   // per pool, this chunk step
+
+    __host__ __device__ bool On() const { return list != nullptr; }
+    // launch lanes of a launch over `lanes` lanes
+    __host__ __device__ int Lanes(int lanes) const { return list ? n : lanes; }
+    __device__ __forceinline__ int Lane(int li) const { return list ? list[li] : li; }
+    __device__ __forceinline__ const PoolStep& Pool(int lane) const { return pools[poolOf[lane]]; }
+    // element offset of lane's [F][64] block in a per-chunk buffer
+    __device__ __forceinline__ size_t Block(int lane, int F) const
+    {
+        return list ? (size_t)frameOff[lane] : (size_t)lane * F * HW_LANE_SIZE;
+    }
+    // element offset of lane's [F + extra][64] block (extra frames per lane)
+    __device__ __forceinline__ size_t BlockX(int lane, int F, int extra) const
+    {
+        return list ? (size_t)frameOff[lane] + (size_t)lane * extra * HW_LANE_SIZE
+                    : (size_t)lane * (F + extra) * HW_LANE_SIZE;
+    }
+};
+
+// Thread -> (lane, ZMW) of a launch with one thread per ZMW; false past the
+// last launch lane.
+__device__ __forceinline__ bool ZmwOf(const LaneMap& m, int lanes, int& l, int& z)
+{
+    const int gl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gl >= m.Lanes(lanes) * kLane) return false;
+    z = gl % kLane;
+    l = m.Lane(gl / kLane);
+    return true;
+}
+
 // ---- kernel argument blocks and launchers ----------------------------------
 
 struct BaselinerArgs
@@ -113,6 +170,11 @@ struct BaselinerArgs
     // uint8 encoding: [lanes][F][64], used instead of `trace` when not null;
     // each value is widened to int16 first (BlockView::Extract, BatchData.h:160-180)
     const uint8_t* trace8 = nullptr;
+    // lane-list launch: input from map.Pool(lane).trace (or .trace8 when u8
+    // is set), `out` and the state packed over the engine's lanes (`lanes` =
+    // engine lanes)
+    LaneMap map{};
+    int u8 = 0;
 };
 
 struct DmeArgs
@@ -128,6 +190,9 @@ struct DmeArgs
     // Optional EM start [lanes][15][64] (fractions, means, variances), used
     // per ZMW unless its log-likelihood is below the reference start's.
     const float* proposal = nullptr;
+    // lane-list launch: frame-interval centers from map.Pool(lane); scratch
+    // indexed by launch lane
+    LaneMap map{};
 };
 
 struct LabelerArgs
@@ -146,6 +211,9 @@ struct LabelerArgs
     uint32_t* tb;                 // [lanes][F + 16][64] scratch
     int lanes;
     int F;
+    // lane-list launch: per-lane chunk lengths from map.Pool(lane).F, F = the
+    // launch's largest
+    LaneMap map{};
 };
 
 struct PulseArgs
@@ -169,21 +237,27 @@ struct PulseArgs
     int lanes;
     int F;
     uint32_t firstFrame;
+    // lane-list launch: outputs and first frame from map.Pool(lane)
+    LaneMap map{};
 };
 
 int BaselinerNumSlots16(int ft);
 cudaError_t LaunchBaseliner(int ft, const BaselinerArgs& a, const KParams& k, cudaStream_t s);
 cudaError_t LaunchBaselinerInit(int ft, int16_t* st16, float* st32, int lanes, cudaStream_t s);
-cudaError_t LaunchAggReset(hw_baseliner_stats* s, int lanes, cudaStream_t st);
-cudaError_t LaunchAggMerge(hw_baseliner_stats* acc, const hw_baseliner_stats* in, int lanes, cudaStream_t st);
+cudaError_t LaunchAggReset(hw_baseliner_stats* s, int lanes, cudaStream_t st, const LaneMap& map = LaneMap{});
+cudaError_t LaunchAggMerge(hw_baseliner_stats* acc, const hw_baseliner_stats* in, int lanes, cudaStream_t st,
+                           const LaneMap& map = LaneMap{});
 cudaError_t LaunchHistResetStats(hw_lane_histogram* h, const hw_baseliner_stats* s, int lanes, const KParams& k,
-                                 int* err, cudaStream_t st);
+                                 int* err, cudaStream_t st, const LaneMap& map = LaneMap{});
 cudaError_t LaunchHistResetBounds(hw_lane_histogram* h, const hw_lane_hist_bounds* b, int lanes, int* err,
                                   cudaStream_t st);
 cudaError_t LaunchHistAdd(hw_lane_histogram* h, int16_t* prev, uint8_t* bits, const int16_t* traces, int frames,
-                          const hw_lane_model* models, int lanes, cudaStream_t st);
+                          const hw_lane_model* models, int lanes, cudaStream_t st, const LaneMap& map = LaneMap{});
 cudaError_t LaunchInitModels(hw_lane_model* m, const hw_baseliner_stats* s, int lanes, const KParams& k,
-                             cudaStream_t st);
+                             cudaStream_t st, const LaneMap& map = LaneMap{});
+// Zeroes the pulse counts and overflow counters of the listed lanes (pools
+// that emit nothing this chunk).
+cudaError_t LaunchZeroOutputs(const LaneMap& map, cudaStream_t st);
 cudaError_t LaunchDmeEstimate(const DmeArgs& a, const KParams& k, cudaStream_t s);
 cudaError_t LaunchLabeler(const LabelerArgs& a, const KParams& k, cudaStream_t s);
 cudaError_t LaunchPulses(const PulseArgs& a, const KParams& k, cudaStream_t s);

@@ -181,14 +181,17 @@ __device__ __forceinline__ int TraceSource(uint32_t w, int state)
 
 constexpr int kBatch = 8;                              // frames loaded ahead
 
+template <bool Mapped>
 __global__ void __launch_bounds__(128, 5) LabelerKernel(LabelerArgs A, KParams k)
 {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= A.lanes * kLane) return;
-    const int l = g / kLane, z = g % kLane;
-    const int F = A.F;
+    LaneMap map = A.map;
+    if (!Mapped) map.list = nullptr;      // the single-pool variant compiles without the lane list
+    int l, z;
+    if (!ZmwOf(map, A.lanes, l, z)) return;
+    const int g = l * kLane + z;
+    const int F = map.On() ? map.Pool(l).F : A.F;
     const int nRoi = F + kLookback + kStitch;
-    const int16_t* chunk = A.trace + (size_t)l * F * kLane + z;
+    const int16_t* chunk = A.trace + map.Block(l, F) + z;
     int16_t* pl = A.prevLat + (size_t)l * kLatent * kLane + z;
     const hw_lane_model& oldM = A.latModel[l];
     const hw_lane_model& newM = A.models[l];
@@ -260,7 +263,7 @@ __global__ void __launch_bounds__(128, 5) LabelerKernel(LabelerArgs A, KParams k
 #pragma unroll
         for (int i = 0; i < kStates; ++i) ll[i] = (bc == i) ? 0.0f : -__int_as_float(0x7f800000);
     }
-    uint32_t* tb = A.tb + (size_t)l * (F + kLookback) * kLane + z;
+    uint32_t* tb = A.tb + map.BlockX(l, F, kLookback) + z;
     ZScorer sc;
     sc.Setup(k, oldM, z);
     uint32_t roiWord = roiw(0);
@@ -339,7 +342,7 @@ __global__ void __launch_bounds__(128, 5) LabelerKernel(LabelerArgs A, KParams k
     for (int i = 1; i < kStates; ++i) ret = (anchorState == i) ? anchorLL[i] : ret;
 
     int ts = anchorState;
-    int16_t* out = A.labels + (size_t)l * F * kLane + z;
+    int16_t* out = A.labels + map.Block(l, F) + z;
     for (int f0 = F - kBatch; f0 >= 0; f0 -= kBatch)
     {
         uint32_t w[kBatch];
@@ -367,24 +370,31 @@ __global__ void __launch_bounds__(128, 5) LabelerKernel(LabelerArgs A, KParams k
 }
 
 // The lane's old model is replaced by the new one after all its ZMWs used it.
-__global__ void LabelerModelCopyKernel(hw_lane_model* dst, const hw_lane_model* src, int lanes)
+__global__ void LabelerModelCopyKernel(hw_lane_model* dst, const hw_lane_model* src, int lanes, LaneMap map)
 {
-    const int n = lanes * (int)(sizeof(hw_lane_model) / 4);
+    constexpr int kWords = (int)(sizeof(hw_lane_model) / 4);
+    const int n = map.Lanes(lanes) * kWords;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) reinterpret_cast<uint32_t*>(dst)[i] = reinterpret_cast<const uint32_t*>(src)[i];
+    if (i >= n) return;
+    const size_t w = (size_t)map.Lane(i / kWords) * kWords + i % kWords;
+    reinterpret_cast<uint32_t*>(dst)[w] = reinterpret_cast<const uint32_t*>(src)[w];
 }
 
 cudaError_t LaunchLabeler(const LabelerArgs& a, const KParams& k, cudaStream_t s)
 {
     if (a.F > 1024 || a.F % kBatch != 0) return cudaErrorInvalidValue;
     const int threads = 128;
-    const int blocks = (a.lanes * kLane + threads - 1) / threads;
+    const int lanes = a.map.Lanes(a.lanes);
+    if (lanes == 0) return cudaSuccess;
+    const int blocks = (lanes * kLane + threads - 1) / threads;
     const int roiWords = (a.F + kLookback + kStitch + 15) / 16;
-    LabelerKernel<<<blocks, threads, (size_t)roiWords * threads * sizeof(uint32_t), s>>>(a, k);
+    const size_t smem = (size_t)roiWords * threads * sizeof(uint32_t);
+    if (a.map.On()) LabelerKernel<true><<<blocks, threads, smem, s>>>(a, k);
+    else LabelerKernel<false><<<blocks, threads, smem, s>>>(a, k);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    const int n = a.lanes * (int)(sizeof(hw_lane_model) / 4);
-    LabelerModelCopyKernel<<<(n + 255) / 256, 256, 0, s>>>(a.latModel, a.models, a.lanes);
+    const int n = lanes * (int)(sizeof(hw_lane_model) / 4);
+    LabelerModelCopyKernel<<<(n + 255) / 256, 256, 0, s>>>(a.latModel, a.models, a.lanes, a.map);
     return cudaGetLastError();
 }
 

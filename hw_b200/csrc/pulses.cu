@@ -15,10 +15,17 @@ __device__ __forceinline__ uint16_t ToFixed(float v) { return static_cast<uint16
 
 __global__ void __launch_bounds__(128) PulseKernel(PulseArgs A, KParams k)
 {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= A.lanes * kLane) return;
-    const int l = g / kLane, z = g % kLane;
+    int l, z;
+    if (!ZmwOf(A.map, A.lanes, l, z)) return;
+    const int g = l * kLane + z;
     const int cap = k.maxCalls;
+    // outputs, chunk length and first frame: the pool's own in a lane-list launch
+    const PoolStep* ps = A.map.On() ? &A.map.Pool(l) : nullptr;
+    const int F = ps ? ps->F : A.F;
+    const uint32_t firstFrame = ps ? (uint32_t)(ps->firstFrame - kLatent) : A.firstFrame;
+    const int go = ps ? (l - ps->lane0) * kLane + z : g;     // ZMW index in the output buffers
+    uint32_t* lensOut = ps ? ps->lens : A.lens;
+    uint32_t* ovfOut = ps ? ps->ovf : A.ovf;
     uint32_t start = A.segStart[g];
     int16_t first = A.segFirst[g], last = A.segLast[g], mx = A.segMax[g], label = A.segLabel[g];
     float total = A.segTotal[g], m2 = A.segM2[g];
@@ -26,13 +33,13 @@ __global__ void __launch_bounds__(128) PulseKernel(PulseArgs A, KParams k)
     const float maxSignal = 65535 * .1f;
     const float minSignal = 0.0f;
     uint32_t n = 0, over = 0;
-    hw_pulse* out = A.pulses + (size_t)g * cap;
+    hw_pulse* out = (ps ? ps->pulses : A.pulses) + (size_t)go * cap;
     float b0 = 0.0f, b1 = 0.0f, b2 = 0.0f;   // StatAccumulator of baseline frames (offset 0)
-    const int16_t* lab = A.labels + (size_t)l * A.F * kLane + z;
+    const int16_t* lab = A.labels + A.map.Block(l, F) + z;
     const int16_t* lat = A.latTrace + (size_t)l * kLatent * kLane + z;
-    const int16_t* tr = A.trace + (size_t)l * A.F * kLane + z;
+    const int16_t* tr = A.trace + A.map.Block(l, F) + z;
     constexpr int kB = 8;
-    for (int rel0 = 0; rel0 < A.F; rel0 += kB)
+    for (int rel0 = 0; rel0 < F; rel0 += kB)
     {
         // Load the next kB labels and signals ahead of use (F % 8 == 0).
         int16_t lbB[kB], sgB[kB];
@@ -47,7 +54,7 @@ __global__ void __launch_bounds__(128) PulseKernel(PulseArgs A, KParams k)
         for (int j = 0; j < kB; ++j)
         {
         const int rel = rel0 + j;
-        const uint32_t absF = (uint32_t)rel + A.firstFrame;
+        const uint32_t absF = (uint32_t)rel + firstFrame;
         const int16_t lb = lbB[j];
         const int16_t signal = sgB[j];
         const bool isUp = (lb > kAnalogs) & (lb <= 2 * kAnalogs);
@@ -96,8 +103,8 @@ __global__ void __launch_bounds__(128) PulseKernel(PulseArgs A, KParams k)
     }
     A.segStart[g] = start; A.segFirst[g] = first; A.segLast[g] = last; A.segMax[g] = mx;
     A.segTotal[g] = total; A.segM2[g] = m2; A.segLabel[g] = label;
-    A.lens[g] = n;
-    A.ovf[g] = over;
+    lensOut[go] = n;
+    ovfOut[go] = over;
     A.bls[l].offset[z] = 0.0f;
     A.bls[l].moment0[z] = b0;
     A.bls[l].moment1[z] = b1;
@@ -108,8 +115,27 @@ cudaError_t LaunchPulses(const PulseArgs& a, const KParams& k, cudaStream_t s)
 {
     if (a.F % 8 != 0) return cudaErrorInvalidValue;
     const int threads = 128;
-    const int blocks = (a.lanes * kLane + threads - 1) / threads;
+    const int lanes = a.map.Lanes(a.lanes);
+    if (lanes == 0) return cudaSuccess;
+    const int blocks = (lanes * kLane + threads - 1) / threads;
     PulseKernel<<<blocks, threads, 0, s>>>(a, k);
+    return cudaGetLastError();
+}
+
+__global__ void ZeroOutputsKernel(LaneMap map)
+{
+    int l, z;
+    if (!ZmwOf(map, 0, l, z)) return;
+    const PoolStep& ps = map.Pool(l);
+    const int go = (l - ps.lane0) * kLane + z;
+    ps.lens[go] = 0;
+    ps.ovf[go] = 0;
+}
+
+cudaError_t LaunchZeroOutputs(const LaneMap& map, cudaStream_t s)
+{
+    if (!map.On() || map.n == 0) return cudaSuccess;
+    ZeroOutputsKernel<<<(map.n * kLane + 127) / 128, 128, 0, s>>>(map);
     return cudaGetLastError();
 }
 

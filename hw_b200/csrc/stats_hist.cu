@@ -14,11 +14,10 @@ namespace hwk {
 
 // ---- BaselinerStatAccumulator::Merge -------------------------------------
 
-__global__ void AggResetKernel(hw_baseliner_stats* s, int lanes)
+__global__ void AggResetKernel(hw_baseliner_stats* s, int lanes, LaneMap map)
 {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= lanes * kLane) return;
-    const int l = g / kLane, z = g % kLane;
+    int l, z;
+    if (!ZmwOf(map, lanes, l, z)) return;
     hw_baseliner_stats& S = s[l];
     hw_stat_accum_state* st[3] = {&S.full_autocorr.basic_stats, &S.baseline_stats, &S.background_stats};
     for (auto* p : st) { p->offset[z] = 0; p->moment0[z] = 0; p->moment1[z] = 0; p->moment2[z] = 0; }
@@ -31,11 +30,10 @@ __global__ void AggResetKernel(hw_baseliner_stats* s, int lanes)
     S.raw_baseline_sum[z] = 0;
 }
 
-__global__ void AggMergeKernel(hw_baseliner_stats* acc, const hw_baseliner_stats* in, int lanes)
+__global__ void AggMergeKernel(hw_baseliner_stats* acc, const hw_baseliner_stats* in, int lanes, LaneMap map)
 {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= lanes * kLane) return;
-    const int l = g / kLane, z = g % kLane;
+    int l, z;
+    if (!ZmwOf(map, lanes, l, z)) return;
     hw_baseliner_stats& A = acc[l];
     const hw_baseliner_stats& B = in[l];
     auto mergeStat = [z](hw_stat_accum_state& a, const hw_stat_accum_state& b) {
@@ -107,11 +105,10 @@ __device__ __forceinline__ void HistClear(hw_lane_histogram& H, int z)
 
 // TraceHistogramAccumHost::ResetImpl(const BaselinerMetrics&), :96-126
 __global__ void HistResetStatsKernel(hw_lane_histogram* hist, const hw_baseliner_stats* stats, int lanes,
-                                     KParams k, int* err)
+                                     KParams k, int* err, LaneMap map)
 {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= lanes * kLane) return;
-    const int l = g / kLane, z = g % kLane;
+    int l, z;
+    if (!ZmwOf(map, lanes, l, z)) return;
     const hw_stat_accum_state& s = stats[l].baseline_stats;
     const bool suff = s.moment0[z] >= k.minFrameCount;
     const float mean = suff ? StatMean(s, z) : 0.0f;
@@ -128,11 +125,10 @@ __global__ void HistResetStatsKernel(hw_lane_histogram* hist, const hw_baseliner
 }
 
 // TraceHistogramAccumHost::ResetImpl(const UnifiedCudaArray<LaneHistBounds>&), :82-94
-__global__ void HistResetBoundsKernel(hw_lane_histogram* hist, const hw_lane_hist_bounds* b, int lanes, int* err)
+__global__ void HistResetBoundsKernel(hw_lane_histogram* hist, const hw_lane_hist_bounds* b, int lanes, int* err, LaneMap map)
 {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= lanes * kLane) return;
-    const int l = g / kLane, z = g % kLane;
+    int l, z;
+    if (!ZmwOf(map, lanes, l, z)) return;
     const float lo = b[l].lower_bounds[z], up = b[l].upper_bounds[z];
     const float bs = (up - lo) / static_cast<float>(kBins);
     hist[l].low_bound[z] = lo;
@@ -157,13 +153,15 @@ constexpr int kHistBatch = 8;
 // touches its own ZMW's column, so no atomics are needed).
 __global__ void __launch_bounds__(kLane * kHistLanesPerBlock)
 HistAddKernel(hw_lane_histogram* hist, EdgeState es, const int16_t* traces, int frames,
-              const hw_lane_model* models, int lanes)
+              const hw_lane_model* models, int lanes, LaneMap map)
 {
     extern __shared__ uint16_t histSmem[];
     auto cnt = reinterpret_cast<uint16_t (*)[kBins + 1][kLane]>(histSmem);
     const int ll = threadIdx.x / kLane, z = threadIdx.x % kLane;
-    const int l = blockIdx.x * kHistLanesPerBlock + ll;
-    if (l >= lanes) return;    // whole lanes only: no block-wide sync below
+    const int li = blockIdx.x * kHistLanesPerBlock + ll;
+    if (li >= map.Lanes(lanes)) return;    // whole lanes only: no block-wide sync below
+    const int l = map.Lane(li);
+    if (map.On()) frames = map.Pool(l).F;
     const int g = l * kLane + z;
     hw_lane_histogram& H = hist[l];
     for (int b = 0; b < kBins; ++b) cnt[ll][b][z] = H.bin_count[b][z];
@@ -176,7 +174,7 @@ HistAddKernel(hw_lane_histogram* hist, EdgeState es, const int16_t* traces, int 
     uint8_t bits = es.bits[g];
     bool b1 = bits & 1, b2 = (bits >> 1) & 1;
     int n = (bits >> 2) & 3;
-    const int16_t* tr = traces + (size_t)l * frames * kLane + z;
+    const int16_t* tr = traces + map.Block(l, frames) + z;
     auto step = [&](int16_t x) {
         const bool isBl = x < thr;
         const bool edge = (n == 2) ? (isBl ^ b2) : true;
@@ -212,11 +210,10 @@ HistAddKernel(hw_lane_histogram* hist, EdgeState es, const int16_t* traces, int 
 // ---- DmeEmHost::InitLaneDetModel (DmeEmHost.cpp:872-925) ------------------
 
 __global__ void InitModelsKernel(hw_lane_model* models, const hw_baseliner_stats* stats, int lanes, KParams k,
-                                 int fixedModel, float fixedMean, float fixedVar)
+                                 int fixedModel, float fixedMean, float fixedVar, LaneMap map)
 {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= lanes * kLane) return;
-    const int l = g / kLane, z = g % kLane;
+    int l, z;
+    if (!ZmwOf(map, lanes, l, z)) return;
     hw_lane_model& m = models[l];
     if (fixedModel)
     {
@@ -250,37 +247,43 @@ __global__ void InitModelsKernel(hw_lane_model* models, const hw_baseliner_stats
 
 static inline int Blocks(int lanes, int threads) { return (lanes * kLane + threads - 1) / threads; }
 
-cudaError_t LaunchAggReset(hw_baseliner_stats* s, int lanes, cudaStream_t st)
+cudaError_t LaunchAggReset(hw_baseliner_stats* s, int lanes, cudaStream_t st, const LaneMap& map)
 {
-    AggResetKernel<<<Blocks(lanes, 256), 256, 0, st>>>(s, lanes);
+    if (map.Lanes(lanes) == 0) return cudaSuccess;
+    AggResetKernel<<<Blocks(map.Lanes(lanes), 256), 256, 0, st>>>(s, lanes, map);
     return cudaGetLastError();
 }
 
-cudaError_t LaunchAggMerge(hw_baseliner_stats* acc, const hw_baseliner_stats* in, int lanes, cudaStream_t st)
+cudaError_t LaunchAggMerge(hw_baseliner_stats* acc, const hw_baseliner_stats* in, int lanes, cudaStream_t st,
+                           const LaneMap& map)
 {
-    AggMergeKernel<<<Blocks(lanes, 256), 256, 0, st>>>(acc, in, lanes);
+    if (map.Lanes(lanes) == 0) return cudaSuccess;
+    AggMergeKernel<<<Blocks(map.Lanes(lanes), 256), 256, 0, st>>>(acc, in, lanes, map);
     return cudaGetLastError();
 }
 
 cudaError_t LaunchHistResetStats(hw_lane_histogram* h, const hw_baseliner_stats* s, int lanes, const KParams& k,
-                                 int* err, cudaStream_t st)
+                                 int* err, cudaStream_t st, const LaneMap& map)
 {
-    HistResetStatsKernel<<<Blocks(lanes, 128), 128, 0, st>>>(h, s, lanes, k, err);
+    if (map.Lanes(lanes) == 0) return cudaSuccess;
+    HistResetStatsKernel<<<Blocks(map.Lanes(lanes), 128), 128, 0, st>>>(h, s, lanes, k, err, map);
     return cudaGetLastError();
 }
 
 cudaError_t LaunchHistResetBounds(hw_lane_histogram* h, const hw_lane_hist_bounds* b, int lanes, int* err,
                                   cudaStream_t st)
 {
-    HistResetBoundsKernel<<<Blocks(lanes, 128), 128, 0, st>>>(h, b, lanes, err);
+    HistResetBoundsKernel<<<Blocks(lanes, 128), 128, 0, st>>>(h, b, lanes, err, LaneMap{});
     return cudaGetLastError();
 }
 
 cudaError_t LaunchHistAdd(hw_lane_histogram* h, int16_t* prev, uint8_t* bits, const int16_t* traces, int frames,
-                          const hw_lane_model* models, int lanes, cudaStream_t st)
+                          const hw_lane_model* models, int lanes, cudaStream_t st, const LaneMap& map)
 {
     EdgeState es{prev, bits};
-    const int blocks = (lanes + kHistLanesPerBlock - 1) / kHistLanesPerBlock;
+    const int n = map.Lanes(lanes);
+    if (n == 0) return cudaSuccess;
+    const int blocks = (n + kHistLanesPerBlock - 1) / kHistLanesPerBlock;
     const size_t smem = sizeof(uint16_t) * kHistLanesPerBlock * (kBins + 1) * kLane;
     static bool attrSet = false;
     if (!attrSet)
@@ -289,14 +292,15 @@ cudaError_t LaunchHistAdd(hw_lane_histogram* h, int16_t* prev, uint8_t* bits, co
         if (e != cudaSuccess) return e;
         attrSet = true;
     }
-    HistAddKernel<<<blocks, kLane * kHistLanesPerBlock, smem, st>>>(h, es, traces, frames, models, lanes);
+    HistAddKernel<<<blocks, kLane * kHistLanesPerBlock, smem, st>>>(h, es, traces, frames, models, lanes, map);
     return cudaGetLastError();
 }
 
 cudaError_t LaunchInitModels(hw_lane_model* m, const hw_baseliner_stats* s, int lanes, const KParams& k,
-                             cudaStream_t st)
+                             cudaStream_t st, const LaneMap& map)
 {
-    InitModelsKernel<<<Blocks(lanes, 128), 128, 0, st>>>(m, s, lanes, k, 0, 0.0f, 0.0f);
+    if (map.Lanes(lanes) == 0) return cudaSuccess;
+    InitModelsKernel<<<Blocks(map.Lanes(lanes), 128), 128, 0, st>>>(m, s, lanes, k, 0, 0.0f, 0.0f, map);
     return cudaGetLastError();
 }
 

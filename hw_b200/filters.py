@@ -360,6 +360,83 @@ class PoolSet(_Handle):
         return pulses, lens, ovf
 
 
+class FusedEngine(_Handle):
+    """All pools of a basecaller in one handle (hw_chunk_fused): each stage of
+    a chunk step is one launch over the lanes of every pool that takes it.
+    Pool p's results equal those of BatchAnalyzer(cfg, pool_ids[p], lanes[p],
+    frames_per_chunk[p]); its outputs of the last step are in
+    outputs(p)."""
+    _destroy = "hw_fused_destroy"
+
+    def __init__(self, cfg, lanes, frames_per_chunk, pool_ids=None, graphs=False, tuning=None):
+        super().__init__()
+        self.lanes = np.ascontiguousarray(lanes, np.uint32)
+        self.frames = np.ascontiguousarray(frames_per_chunk, np.uint32)
+        n = len(self.lanes)
+        ids = None if pool_ids is None else np.ascontiguousarray(pool_ids, np.uint32)
+        self.cap = cfg.max_calls_per_zmw
+        check(lib().hw_fused_create(C.byref(cfg), n, abi.ptr(ids), abi.ptr(self.lanes), abi.ptr(self.frames),
+                                    C.byref(self._h)))
+        self.pulses, self.lens, self.ovf = [], [], []
+        self.table = np.zeros(n, abi.POOL_CHUNK_DT)
+        for p, L in enumerate(self.lanes):
+            z = int(L) * abi.LANE
+            self.pulses.append(torch.empty(z * self.cap * abi.PULSE_DT.itemsize, dtype=torch.uint8, device="cuda"))
+            self.lens.append(torch.empty((int(L), abi.LANE), dtype=torch.int32, device="cuda"))
+            self.ovf.append(torch.empty((int(L), abi.LANE), dtype=torch.int32, device="cuda"))
+            self.table["d_pulses"][p] = self.pulses[p].data_ptr()
+            self.table["d_lens"][p] = self.lens[p].data_ptr()
+            self.table["d_overflows"][p] = self.ovf[p].data_ptr()
+        self.next_frame = np.zeros(n, np.int64)
+        if graphs:
+            self.use_graphs(True)
+        if tuning:
+            self.set_tuning(tuning)
+
+    def use_graphs(self, enable=True):
+        check(lib().hw_fused_use_graphs(self._h, 1 if enable else 0))
+
+    def set_tuning(self, tuning):
+        """tuning: {frames_per_chunk: (fuse_label_pulses, labeler_lanes_per_cta)}."""
+        t = np.zeros(len(tuning), abi.FUSED_TUNING_DT)
+        for i, (F, (fuse, lpc)) in enumerate(sorted(tuning.items())):
+            t[i] = (F, fuse, lpc, 0)
+        check(lib().hw_fused_set_tuning(self._h, abi.ptr(t), len(t)))
+
+    def process(self, chunks):
+        """One step: chunks[p] is pool p's next chunk [lanes][F][64] (int16 or
+        uint8 CUDA tensor).  Returns (emitted, estimated) flags per pool."""
+        t = self.table
+        for p, c in enumerate(chunks):
+            if c.dtype == torch.uint8:
+                t["d_trace"][p], t["d_trace8"][p] = 0, c.data_ptr()
+            else:
+                t["d_trace"][p], t["d_trace8"][p] = c.data_ptr(), 0
+        t["first_frame"] = self.next_frame
+        check(lib().hw_chunk_fused(self._h, abi.ptr(t), len(t), _stream()))
+        self.next_frame += self.frames
+        return t["emitted"].copy(), t["estimated"].copy()
+
+    def finish(self):
+        check(lib().hw_fused_finish(self._h, _stream()))
+
+    def outputs(self, p):
+        """(pulses, lens, overflows) of pool p's last step."""
+        return self.pulses[p], self.lens[p], self.ovf[p]
+
+    def models(self, p):
+        out = struct_buffer(abi.LANE_MODEL_DT, int(self.lanes[p]))
+        fi = abi.FrameInterval()
+        check(lib().hw_fused_models(self._h, p, _p(out), C.byref(fi), _stream()))
+        return out, fi.tuple()
+
+    def last_step(self):
+        """(kernel launches, graph launches) of the last step."""
+        a, b = C.c_uint32(), C.c_uint32()
+        check(lib().hw_fused_last_step(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+
 class _DeviceBytes:
     """Device memory owned by the library, exposed to torch without a copy."""
 

@@ -67,6 +67,14 @@ def lib():
         "hw_pool_set_layout": ([vp, vp, C.POINTER(C.c_uint64), C.POINTER(u32)], C.c_int),
         "hw_pool_set_process": ([vp, vp, i32, vp, vp, vp], C.c_int),
         "hw_pool_set_outputs": ([vp, u32, PPV, PPV, PPV], C.c_int),
+        "hw_fused_create": ([PCFG, u32, vp, vp, vp, PPV], C.c_int),
+        "hw_fused_destroy": ([vp], C.c_int),
+        "hw_chunk_fused": ([vp, vp, u32, vp], C.c_int),
+        "hw_fused_finish": ([vp, vp], C.c_int),
+        "hw_fused_use_graphs": ([vp, i32], C.c_int),
+        "hw_fused_set_tuning": ([vp, vp, u32], C.c_int),
+        "hw_fused_models": ([vp, u32, vp, C.POINTER(FI), vp], C.c_int),
+        "hw_fused_last_step": ([vp, C.POINTER(u32), C.POINTER(u32)], C.c_int),
         "hw_analyzer_state_size": ([vp, C.POINTER(C.c_uint64)], C.c_int),
         "hw_analyzer_state_export": ([vp, vp, C.c_uint64, vp], C.c_int),
         "hw_analyzer_state_import": ([vp, vp, C.c_uint64, vp], C.c_int),

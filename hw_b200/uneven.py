@@ -4,15 +4,18 @@ uneven-pool generator (workload 2: per-ZMW lognormal amplitude factors with
 sigma 0.3, pulse rates uniform in 0.02-0.12 per frame), reference default
 analysis parameters with dynamic estimation.
 
-Two ways of running the same pools on the same traces are timed:
+Ways of running the same pools on the same traces, each timed on its own:
+  * fused engine (hw_chunk_fused): every stage of a step is one launch over
+    the lanes of all pools that take it; `fused_graphs` replays each step
+    plan as a CUDA graph;
   * pool set (hw_pool_set): pools that share chunk length and stagger class
     run as one batched analyzer, one launch per stage and class;
   * one analyzer per pool, each with its own launches (what a per-pool
     driver does).
 Reported: ZMW-frames/s of the timed steps (device time of the analysis,
-CUDA events; trace generation excluded) and the number of launch classes.
+CUDA events; trace generation excluded), launches per step.
 
-    python -m hw_b200.uneven [--pools 500] [--steps 4] [--warmup-steps N]
+    python -m hw_b200.uneven [--pools 500] [--steps 4] [--warmup-steps N] [--variants fused,per_pool]
 """
 import argparse
 import json
@@ -45,7 +48,19 @@ def _gens(lanes):
             for p, L in enumerate(lanes)]
 
 
-def run(n_pools=500, steps=4, warmup_steps=None, per_pool=True, seed=0):
+def _timed(process, gens, frames, warmup_steps, steps, stream, fill):
+    """Runs warmup + timed steps; fill(step) writes every pool's chunk and
+    returns the list of chunks; process(step, chunks) enqueues the analysis."""
+    t = 0.0
+    for step in range(warmup_steps + steps):
+        chunks = fill(step)
+        ms = _time(lambda: process(step, chunks), stream)
+        if step >= warmup_steps:
+            t += ms
+    return t / steps
+
+
+def run(n_pools=500, steps=4, warmup_steps=None, variants=("fused", "fused_graphs", "pool_set", "per_pool"), seed=0):
     cfg = workloads.chip_config()
     lanes, frames = pool_shapes(n_pools, seed)
     if warmup_steps is None:
@@ -53,53 +68,62 @@ def run(n_pools=500, steps=4, warmup_steps=None, per_pool=True, seed=0):
         warmup_steps = max(workloads.startup_chunks(cfg, n_pools, int(F)) for F in set(frames.tolist()))
     stream = torch.cuda.current_stream()
     zf_step = int((lanes.astype(np.int64) * frames.astype(np.int64)).sum()) * abi.LANE
-
-    # pool set: one launch per stage and schedule class
-    ps = Fl.PoolSet(cfg, lanes, frames)
-    gens = _gens(lanes)
-    t_set = 0.0
-    for step in range(warmup_steps + steps):
-        for p, (g, F) in enumerate(zip(gens, frames)):
-            g.next(step * int(F), int(F), out=ps.chunk(p))
-        ms = _time(lambda: ps.process(step), stream)
-        if step >= warmup_steps:
-            t_set += ms
-    classes = ps.launch_groups
-    ps.close()
-    for g in gens:
-        g.close()
-    torch.cuda.synchronize()
-    torch.cuda.empty_cache()
     out = {
         "pools": n_pools, "zmws": int(lanes.sum()) * abi.LANE, "lanes_min": int(lanes.min()),
         "lanes_max": int(lanes.max()), "chunk_lengths": sorted(set(int(f) for f in frames)),
-        "launch_classes": classes, "timed_steps": steps, "warmup_steps": warmup_steps,
-        "zmw_frames_per_step": zf_step,
-        "pool_set_zmw_frames_per_s": zf_step * steps / (t_set / 1e3),
-        "pool_set_ms_per_step": t_set / steps,
+        "timed_steps": steps, "warmup_steps": warmup_steps, "zmw_frames_per_step": zf_step,
     }
-    if not per_pool:
-        return out
 
-    # one analyzer per pool on the same traces
-    ans = [Fl.BatchAnalyzer(cfg, p, int(L), int(F)) for p, (L, F) in enumerate(zip(lanes, frames))]
-    gens = _gens(lanes)
-    bufs = [torch.empty((int(L), int(F), abi.LANE), dtype=torch.int16, device="cuda") for L, F in zip(lanes, frames)]
-    t_pool = 0.0
-    for step in range(warmup_steps + steps):
-        for p, (g, F) in enumerate(zip(gens, frames)):
-            g.next(step * int(F), int(F), out=bufs[p])
+    def per_pool_buffers():
+        return [torch.empty((int(L), int(F), abi.LANE), dtype=torch.int16, device="cuda") for L, F in zip(lanes, frames)]
 
-        def one_by_one():
-            for p, a in enumerate(ans):
-                a(bufs[p], step * int(frames[p]))
-        ms = _time(one_by_one, stream)
-        if step >= warmup_steps:
-            t_pool += ms
-    for a in ans:
-        a.close()
-    out["per_pool_zmw_frames_per_s"] = zf_step * steps / (t_pool / 1e3)
-    out["per_pool_ms_per_step"] = t_pool / steps
+    for v in variants:
+        gens = _gens(lanes)
+        if v in ("fused", "fused_graphs"):
+            eng = Fl.FusedEngine(cfg, lanes, frames, graphs=(v == "fused_graphs"))
+            bufs = per_pool_buffers()
+
+            def fill(step):
+                for p, (g, F) in enumerate(zip(gens, frames)):
+                    g.next(step * int(F), int(F), out=bufs[p])
+                return bufs
+            ms = _timed(lambda step, ch: eng.process(ch), gens, frames, warmup_steps, steps, stream, fill)
+            eng.finish()
+            out[v + "_launches_per_step"] = list(eng.last_step())
+            eng.close()
+            del bufs
+        elif v == "pool_set":
+            ps = Fl.PoolSet(cfg, lanes, frames)
+
+            def fill(step):
+                for p, (g, F) in enumerate(zip(gens, frames)):
+                    g.next(step * int(F), int(F), out=ps.chunk(p))
+                return None
+            ms = _timed(lambda step, ch: ps.process(step), gens, frames, warmup_steps, steps, stream, fill)
+            out["pool_set_launch_classes"] = ps.launch_groups
+            ps.close()
+        else:
+            ans = [Fl.BatchAnalyzer(cfg, p, int(L), int(F)) for p, (L, F) in enumerate(zip(lanes, frames))]
+            bufs = per_pool_buffers()
+
+            def fill(step):
+                for p, (g, F) in enumerate(zip(gens, frames)):
+                    g.next(step * int(F), int(F), out=bufs[p])
+                return bufs
+
+            def one_by_one(step, ch):
+                for p, a in enumerate(ans):
+                    a(ch[p], step * int(frames[p]))
+            ms = _timed(one_by_one, gens, frames, warmup_steps, steps, stream, fill)
+            for a in ans:
+                a.close()
+            del bufs
+        for g in gens:
+            g.close()
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        out[v + "_ms_per_step"] = ms
+        out[v + "_zmw_frames_per_s"] = zf_step / (ms / 1e3)
     return out
 
 
@@ -108,9 +132,9 @@ def main():
     ap.add_argument("--pools", type=int, default=500)
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup-steps", type=int, default=None)
-    ap.add_argument("--no-per-pool", action="store_true")
+    ap.add_argument("--variants", default="fused,fused_graphs,pool_set,per_pool")
     a = ap.parse_args()
-    print(json.dumps(run(a.pools, a.steps, a.warmup_steps, not a.no_per_pool)))
+    print(json.dumps(run(a.pools, a.steps, a.warmup_steps, tuple(a.variants.split(",")))))
 
 
 if __name__ == "__main__":

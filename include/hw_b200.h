@@ -510,6 +510,67 @@ int hw_pool_set_process(hw_pool_set* s, const int16_t* d_packed, int32_t step, i
  * pulses [lanes_p][64][max_calls_per_zmw], lengths and overflows [lanes_p][64]. */
 int hw_pool_set_outputs(const hw_pool_set* s, uint32_t pool, hw_pulse** d_pulses, uint32_t** d_lens,
                         uint32_t** d_overflows);
+
+/* ---- Fused chunk engine (hw_chunk_fused) ------------------------------------
+ * Replaces the per-pool BatchAnalyzer loop of the basecaller
+ * (AN/BatchAnalyzer.cpp:119-375 run once per pool and chunk by the
+ * basecaller's analysis threads, BC/appModules/Basecaller.h:246-250) with one
+ * call per chunk step for all pools.  The engine owns the state of every
+ * pool, packed lane after lane; each stage of a step (baseline filter,
+ * statistics merge, histogram, model initialisation, DME, histogram reset,
+ * labeler, pulse accumulator) is ONE launch over the list of lanes of all
+ * pools that take it this step, whatever their lane counts and chunk lengths.
+ * Each pool keeps hw_analyzer's schedule (estimation mode, stagger by
+ * pool_id % chunksPerEstimate) and its results equal those of an
+ * hw_analyzer(pool_ids[p], lanes[p], frames_per_chunk[p]).
+ *
+ * A step enqueues its work on `stream` without waiting for the device: a
+ * failure that only the device detects (the reference's histogram-bounds and
+ * DME sanity assertions) is returned by the second call after the failing
+ * step, or by hw_fused_finish, and from then on by every call (the
+ * reference throws and the analysis stops).  With graphs enabled, every
+ * step plan (which lanes take which stage) seen twice is captured as a CUDA
+ * graph and replayed from then on. */
+typedef struct hw_fused hw_fused;
+
+typedef struct hw_pool_chunk {
+    const int16_t* d_trace;     /* [lanes][F][64] int16 chunk, or NULL when d_trace8 is set */
+    const uint8_t* d_trace8;    /* [lanes][F][64] uint8 chunk, or NULL */
+    hw_pulse* d_pulses;         /* [lanes][64][max_calls_per_zmw] */
+    uint32_t* d_lens;           /* [lanes][64] */
+    uint32_t* d_overflows;      /* [lanes][64] */
+    int32_t first_frame;        /* must be the pool's next frame (0, F, 2F, ...) */
+    int32_t emitted;            /* out: 0 while the reference returns no pulses (start-up) */
+    int32_t estimated;          /* out: 1 when this step ran a full DME estimate */
+    int32_t reserved;
+} hw_pool_chunk;
+
+/* Kernel choices for the pools of one chunk length (see hw_fused_set_tuning). */
+typedef struct hw_fused_tuning {
+    uint32_t frames_per_chunk;      /* pools with this chunk length */
+    uint32_t fuse_label_pulses;     /* 1: labeler and pulse accumulator in one kernel */
+    uint32_t labeler_lanes_per_cta; /* 1, 2 or 4 lanes per labeler block */
+    uint32_t reserved;
+} hw_fused_tuning;
+
+/* pool_ids may be NULL (pool p gets id p).  Every chunk length must be a
+ * multiple of 16 frames in [48, 1024]. */
+int hw_fused_create(const hw_config* cfg, uint32_t n_pools, const uint32_t* pool_ids, const uint32_t* lanes,
+                    const uint32_t* frames_per_chunk, hw_fused** out);
+int hw_fused_destroy(hw_fused* f);
+/* Processes one chunk of every pool: table[n_pools], in creation order. */
+int hw_chunk_fused(hw_fused* f, hw_pool_chunk* table, uint32_t n_pools, void* stream);
+/* Waits for the enqueued steps and returns any failure they reported. */
+int hw_fused_finish(hw_fused* f, void* stream);
+int hw_fused_use_graphs(hw_fused* f, int32_t enable);
+/* Replaces the kernel choices of the listed chunk lengths (others keep the
+ * defaults: separate labeler and pulse kernels, 2 lanes per labeler block). */
+int hw_fused_set_tuning(hw_fused* f, const hw_fused_tuning* tuning, uint32_t n);
+/* Device copy of pool p's current models and their frame interval. */
+int hw_fused_models(const hw_fused* f, uint32_t pool, hw_lane_model* d_out, hw_frame_interval* fi, void* stream);
+/* Kernel launches and graph replays of the last step (graph nodes are not
+ * counted as launches). */
+int hw_fused_last_step(const hw_fused* f, uint32_t* launches, uint32_t* graph_launches);
 /* BatchAnalyzer::operator(): d_trace[lanes][F][64] must be the next chunk
  * (first_frame == previous first_frame + F, starting at 0); otherwise
  * HW_ERR_FRAME_ORDER.  Pulses go to d_pulses[lanes][64][max_calls_per_zmw]

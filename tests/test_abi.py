@@ -49,13 +49,15 @@ _PROBE = r"""
 int main(void) {
   S(hw_config) S(hw_analog) S(hw_stat_accum_state) S(hw_autocorr_accum_state) S(hw_baseliner_stats)
   S(hw_lane_analog_mode) S(hw_lane_model) S(hw_lane_histogram) S(hw_lane_hist_bounds) S(hw_pulse)
-  S(hw_dme_diag) S(hw_frame_interval) S(hw_gen_params)
+  S(hw_dme_diag) S(hw_frame_interval) S(hw_gen_params) S(hw_pool_chunk) S(hw_fused_tuning)
   O(hw_baseliner_stats, full_autocorr) O(hw_baseliner_stats, trace_min) O(hw_baseliner_stats, trace_max)
   O(hw_baseliner_stats, baseline_stats) O(hw_baseliner_stats, raw_baseline_sum) O(hw_baseliner_stats, background_stats)
   O(hw_lane_model, analogs) O(hw_lane_model, baseline) O(hw_lane_model, confidence)
   O(hw_lane_histogram, bin_count) O(hw_pulse, start) O(hw_pulse, width) O(hw_pulse, mean_signal)
   O(hw_pulse, mid_signal) O(hw_pulse, max_signal) O(hw_pulse, signal_m2) O(hw_pulse, label) O(hw_pulse, is_reject)
   O(hw_dme_diag, lane_iterations)
+  O(hw_pool_chunk, d_trace8) O(hw_pool_chunk, d_overflows) O(hw_pool_chunk, first_frame) O(hw_pool_chunk, estimated)
+  O(hw_fused_tuning, labeler_lanes_per_cta)
   O(hw_config, analogs) O(hw_config, filter_type) O(hw_config, max_calls_per_zmw) O(hw_config, xsp_amp_thresh)
   O(hw_config, model_estimation_mode) O(hw_config, static_baseline_variance)
   return 0;
@@ -97,7 +99,8 @@ def test_struct_offsets_match_python_mirrors(layout):
             continue
         dt = {"hw_baseliner_stats": abi.BLSTATS_DT, "hw_lane_model": abi.LANE_MODEL_DT,
               "hw_lane_histogram": abi.LANE_HIST_DT, "hw_pulse": abi.PULSE_DT,
-              "hw_dme_diag": abi.DME_DIAG_DT}[t]
+              "hw_dme_diag": abi.DME_DIAG_DT, "hw_pool_chunk": abi.POOL_CHUNK_DT,
+              "hw_fused_tuning": abi.FUSED_TUNING_DT}[t]
         assert dt.fields[m][1] == off, key
 
 
@@ -192,3 +195,17 @@ def test_no_cpu_fallback_without_device():
     rc = native.lib().hw_baseliner_create(C.byref(cfg), 0, 1, 512, C.byref(h))
     assert rc != 0
     assert b"CUDA" in native.lib().hw_last_error_string() or b"cuda" in native.lib().hw_last_error_string()
+
+
+def test_fused_engine_needs_a_device_and_checks_its_arguments():
+    """hw_fused_create rejects bad pool tables before touching the device and,
+    with no CUDA device, returns a CUDA status (no CPU path)."""
+    from hw_b200 import workloads
+    cfg = workloads.small_config()
+    h = C.c_void_p()
+    lanes = np.array([1, 2], np.uint32)
+    bad = np.array([512, 100], np.uint32)          # not a multiple of the aggregate stride
+    assert native.lib().hw_fused_create(C.byref(cfg), 2, None, abi.ptr(lanes), abi.ptr(bad), C.byref(h)) == 1
+    good = np.array([512, 128], np.uint32)
+    rc = native.lib().hw_fused_create(C.byref(cfg), 2, None, abi.ptr(lanes), abi.ptr(good), C.byref(h))
+    assert rc == 2 and b"CUDA" in native.lib().hw_last_error_string().upper()

@@ -1,0 +1,96 @@
+"""Fused chunk engine (hw_chunk_fused): uneven pools in one launch per stage
+give exactly the results of one hw_analyzer per pool."""
+import numpy as np
+import pytest
+
+from hw_b200 import abi, workloads
+
+pytestmark = pytest.mark.gpu
+
+LANES = [1, 3, 2, 5, 1, 2, 4, 1, 2, 3, 1, 2]
+FRAMES = [512] * 6 + [256] * 3 + [128] * 3
+
+
+def _chunks(gens, frames, step, u8):
+    import torch
+    out = []
+    for g, F in zip(gens, frames):
+        c = g.next(step * F, F)
+        out.append(c.clamp(0, 255).to(torch.uint8) if u8 else c)
+    return out
+
+
+def _same_pulses(cfg, L, a, b, lens):
+    from hw_b200 import filters as Fl
+    q0 = Fl.struct_to_numpy(a, abi.PULSE_DT).reshape(L, 64, cfg.max_calls_per_zmw)
+    q1 = Fl.struct_to_numpy(b, abi.PULSE_DT).reshape(L, 64, cfg.max_calls_per_zmw)
+    n = lens.cpu().numpy()
+    for l in range(L):
+        for z in range(64):
+            if not np.array_equal(q0[l, z, :n[l, z]].view(np.uint8), q1[l, z, :n[l, z]].view(np.uint8)):
+                return False
+    return True
+
+
+def _compare(mode, graphs, u8, steps, tuning=None):
+    import torch
+    from hw_b200 import filters as Fl
+    cfg = workloads.small_config()
+    cfg.model_estimation_mode = mode
+    ids = [3 * p + 1 for p in range(len(LANES))]      # stagger classes differ from the positions
+    eng = Fl.FusedEngine(cfg, LANES, FRAMES, pool_ids=ids, graphs=graphs, tuning=tuning)
+    ans = [Fl.BatchAnalyzer(cfg, i, L, F) for i, L, F in zip(ids, LANES, FRAMES)]
+    gens = [Fl.TraceGenerator(L, workload=2, zmw_offset=1000 * p) for p, L in enumerate(LANES)]
+    emitted = estimated = 0
+    graph_steps = 0
+    for step in range(steps):
+        chunks = _chunks(gens, FRAMES, step, u8)
+        em, est = eng.process(chunks)
+        graph_steps += eng.last_step()[1]
+        for p, (an, L) in enumerate(zip(ans, LANES)):
+            pulses, lens, ovf, e1, s1 = an(chunks[p], step * FRAMES[p])
+            assert (bool(em[p]), bool(est[p])) == (e1, s1), (step, p)
+            pp, pl, po = eng.outputs(p)
+            assert torch.equal(pl, lens) and torch.equal(po, ovf), (step, p)
+            if e1:
+                emitted += 1
+                assert _same_pulses(cfg, L, pulses, pp, lens), (step, p)
+            estimated += int(s1)
+    eng.finish()
+    for p, an in enumerate(ans):
+        m0, fi0 = an.models()
+        m1, fi1 = eng.models(p)
+        assert fi0 == fi1 and torch.equal(m0, m1), p
+    return emitted, estimated, graph_steps
+
+
+@pytest.mark.parametrize("mode", [abi.FIXED_ESTIMATIONS, abi.INITIAL_ESTIMATIONS, abi.DYNAMIC_ESTIMATIONS])
+def test_fused_equals_per_pool_analyzers(mode):
+    emitted, estimated, _ = _compare(mode, graphs=False, u8=False, steps=28)
+    assert emitted > 0
+    if mode != abi.FIXED_ESTIMATIONS:
+        assert estimated > 0
+
+
+def test_fused_graphs_replay_identically():
+    emitted, estimated, graph_steps = _compare(abi.DYNAMIC_ESTIMATIONS, graphs=True, u8=False, steps=28)
+    assert emitted > 0 and estimated > 0
+    assert graph_steps > 0
+
+
+def test_fused_uint8_chunks():
+    emitted, _, _ = _compare(abi.DYNAMIC_ESTIMATIONS, graphs=False, u8=True, steps=16)
+    assert emitted > 0
+
+
+def test_fused_rejects_out_of_order_chunks():
+    from hw_b200 import filters as Fl
+    from hw_b200.native import HwError
+    cfg = workloads.small_config()
+    eng = Fl.FusedEngine(cfg, [1, 2], [256, 512])
+    gens = [Fl.TraceGenerator(L, workload=2) for L in (1, 2)]
+    eng.process(_chunks(gens, [256, 512], 0, False))
+    eng.next_frame[1] += 512
+    with pytest.raises(HwError):
+        eng.process(_chunks(gens, [256, 512], 1, False))
+    eng.finish()
