@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned-init", action="store_true",
                     help="skip the learned DME initializer measurement (config 3)")
+    ap.add_argument("--engine", choices=["fused", "analyzers"], default="fused",
+                    help="fused: all pools through hw_chunk_fused; analyzers: one hw_analyzer per pool")
     return ap.parse_args()
 
 
@@ -209,15 +211,29 @@ def main():
             dist.destroy_process_group()
         return
 
-    analyzers = [Fl.BatchAnalyzer(cfg, p, args.lanes_per_pool, FRAMES) for p in range(args.pools)]
     from hw_b200.shard import zmw_offset
     gen = Fl.TraceGenerator(total_lanes, workload=1, zmw_offset=zmw_offset(rank, zmws))
     lpp = args.lanes_per_pool
     stream = torch.cuda.current_stream()
+    if args.engine == "fused":
+        # every pool in one engine: each stage is one launch over all lanes
+        engine = Fl.FusedEngine(cfg, [lpp] * args.pools, [FRAMES] * args.pools)
+        profiled = [engine]
+        outputs = [engine.outputs(p) for p in range(args.pools)]
+        lanes_per_launch = total_lanes
 
-    def run_chunk(chunk, c):
-        for p, a in enumerate(analyzers):
-            a(chunk[p * lpp:(p + 1) * lpp], c * FRAMES)
+        def run_chunk(chunk, c, outs=None):
+            engine.process([chunk[p * lpp:(p + 1) * lpp] for p in range(args.pools)], outs)
+    else:
+        analyzers = [Fl.BatchAnalyzer(cfg, p, lpp, FRAMES) for p in range(args.pools)]
+        profiled = analyzers
+        outputs = [(a.pulses, a.lens, a.ovf) for a in analyzers]
+        lanes_per_launch = lpp
+
+        def run_chunk(chunk, c, outs=None):
+            for p, a in enumerate(analyzers):
+                o = outs[p] if outs is not None else (None, None, None)
+                a(chunk[p * lpp:(p + 1) * lpp], c * FRAMES, *o)
 
     # Start-up and warm-up (untimed).
     n_start = startup_chunks(cfg, args.pools)
@@ -236,7 +252,7 @@ def main():
         t = torch.empty((total_lanes, FRAMES, 64), dtype=torch.int16, device="cuda")
         gen.next((c + k) * FRAMES, FRAMES, out=t)
         dev_chunks.append(t)
-    for a in analyzers:
+    for a in profiled:
         a.profile(True)
         a.stage_times()
     torch.cuda.synchronize()
@@ -265,18 +281,24 @@ def main():
     c += K
     del dev_chunks
     stage = {}
-    for a in analyzers:
+    for a in profiled:
         for kname, (t_ms, n) in a.stage_times().items():
             s = stage.setdefault(kname, [0.0, 0])
             s[0] += t_ms
             s[1] += n
         a.profile(False)
     launches = sum(n * KERNELS_PER_STAGE[k] for k, (_, n) in stage.items())
+    if args.engine == "fused":
+        launches += 2 * K      # per step: the step-table upload and the failure-word kernels
 
     zf_step = zmws * FRAMES
     value = zf_step * K * world / (ms / 1e3)
 
-    # End-to-end through the C ABI: pinned host chunk -> device, analyse, pulses -> host.
+    # End-to-end through the C ABI: every step copies its chunk from pinned
+    # host memory to the device, analyses it and copies all pulse outputs back
+    # to pinned host memory.  Copies run on their own streams, double-buffered
+    # against the analysis: step k's upload and step k-1's download overlap
+    # step k's kernels.
     e2e = None
     if not args.no_e2e:
         host_chunks = []
@@ -286,35 +308,58 @@ def main():
             h = torch.empty((total_lanes, FRAMES, 64), dtype=torch.int16, pin_memory=True)
             h.copy_(tmp)
             host_chunks.append(h)
-        cap = cfg.max_calls_per_zmw
-        host_out = [(torch.empty(a.pulses.numel(), dtype=torch.uint8, pin_memory=True),
-                     torch.empty(a.lens.shape, dtype=torch.int32, pin_memory=True),
-                     torch.empty(a.ovf.shape, dtype=torch.int32, pin_memory=True)) for a in analyzers]
+        del tmp
+        in_dev = [torch.empty((total_lanes, FRAMES, 64), dtype=torch.int16, device="cuda") for _ in range(2)]
+        out_dev = [[(torch.empty_like(dp), torch.empty_like(dl), torch.empty_like(do)) for dp, dl, do in outputs]
+                   for _ in range(2)]
+        host_out = [(torch.empty(dp.numel(), dtype=torch.uint8, pin_memory=True),
+                     torch.empty(dl.shape, dtype=torch.int32, pin_memory=True),
+                     torch.empty(do.shape, dtype=torch.int32, pin_memory=True)) for dp, dl, do in outputs]
+        s_h2d, s_d2h = torch.cuda.Stream(), torch.cuda.Stream()
+        ev_h2d = [torch.cuda.Event() for _ in range(2)]
+        ev_comp = [torch.cuda.Event() for _ in range(2)]
+        ev_d2h = [torch.cuda.Event() for _ in range(2)]
         torch.cuda.synchronize()
         barrier()
         e0.record(stream)
+        s_h2d.wait_stream(stream)
+        s_d2h.wait_stream(stream)
         for k in range(K):
-            tmp.copy_(host_chunks[k], non_blocking=True)
-            run_chunk(tmp, c + k)
-            for a, (hp, hl, ho) in zip(analyzers, host_out):
-                hl.copy_(a.lens, non_blocking=True)
-                ho.copy_(a.ovf, non_blocking=True)
-                hp.copy_(a.pulses, non_blocking=True)
+            b = k % 2
+            with torch.cuda.stream(s_h2d):
+                if k >= 2:
+                    s_h2d.wait_event(ev_comp[b])        # step k-2 has read in_dev[b]
+                in_dev[b].copy_(host_chunks[k], non_blocking=True)
+                ev_h2d[b].record(s_h2d)
+            stream.wait_event(ev_h2d[b])
+            if k >= 2:
+                stream.wait_event(ev_d2h[b])            # step k-2's outputs are on the host
+            run_chunk(in_dev[b], c + k, out_dev[b])
+            ev_comp[b].record(stream)
+            with torch.cuda.stream(s_d2h):
+                s_d2h.wait_event(ev_comp[b])
+                for (dp, dl, do), (hp, hl, ho) in zip(out_dev[b], host_out):
+                    hl.copy_(dl, non_blocking=True)
+                    ho.copy_(do, non_blocking=True)
+                    hp.copy_(dp, non_blocking=True)
+                ev_d2h[b].record(s_d2h)
+        stream.wait_stream(s_d2h)
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
         ms_e2e = max_over_ranks(e0.elapsed_time(e1))
         c += K
         h2d = total_lanes * FRAMES * 64 * 2
-        d2h = sum(a.pulses.numel() + a.lens.numel() * 4 + a.ovf.numel() * 4 for a in analyzers)
+        d2h = sum(dp.numel() + dl.numel() * 4 + do.numel() * 4 for dp, dl, do in outputs)
         e2e = {"value": zf_step * K * world / (ms_e2e / 1e3), "unit": "ZMW-frames/s",
-               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / K}
-        del host_chunks
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / K,
+               "overlap": "copies on their own streams, double-buffered against the analysis"}
+        del host_chunks, in_dev, out_dev
 
     # Roofline of the dominant kernel (the frame labeler) from the live stage timers.
     peaks = measured_peaks()
     lab_ms, lab_n = stage.get("labeler", (0.0, 0))
-    lab_bytes_launch = labeler_alg_bytes_per_zmw(FRAMES) * lpp * 64
+    lab_bytes_launch = labeler_alg_bytes_per_zmw(FRAMES) * lanes_per_launch * 64
     roof = None
     if lab_n:
         avg_s = lab_ms / lab_n / 1e3
@@ -323,7 +368,7 @@ def main():
         prof = labeler_dram_profile()
         traffic = None
         if prof:
-            traffic = prof["dram_bytes_per_zmw_frame"] * lpp * 64 * FRAMES
+            traffic = prof["dram_bytes_per_zmw_frame"] * lanes_per_launch * 64 * FRAMES
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
                 "kernel": "LabelerKernel", "launch_ms": lab_ms / lab_n,
@@ -340,7 +385,9 @@ def main():
                "sample": f"{args.cpu_lanes} lanes ({args.cpu_lanes * 64} ZMWs) x {args.cpu_steps} "
                          f"steady-state 512-frame chunks after start-up ({secs:.1f} s)"}
 
-    for a in analyzers:
+    if args.engine == "fused":
+        engine.finish()
+    for a in profiled:
         a.close()
     learned = None
     if rank == 0 and world == 1 and not args.no_learned_init:
@@ -360,7 +407,9 @@ def main():
             "config": {"workload": "chip: 1,048,576 ZMWs (16,384 lanes, 4 pools) x 512-frame chunks, "
                                    "reference default parameters, dynamic DME",
                        "zmws_per_gpu": zmws, "frames_per_chunk": FRAMES, "pools": args.pools,
-                       "startup_chunks": n_start, "inputs": "1 GiB chunk per step, larger than L2"},
+                       "startup_chunks": n_start, "inputs": "1 GiB chunk per step, larger than L2",
+                       "engine": "hw_chunk_fused (one launch per stage over all pools)" if args.engine == "fused"
+                                 else "one hw_analyzer per pool"},
             "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
             "clocks": clk,
             "stage_ms": {k: v[0] / K for k, v in stage.items()},

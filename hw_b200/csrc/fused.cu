@@ -91,6 +91,31 @@ hw_frame_interval Merge(hw_frame_interval a, hw_frame_interval b)
 
 int32_t Center(hw_frame_interval fi) { return fi.lower + (fi.upper - fi.lower) / 2; }
 
+// Step tables reach the device through a kernel that reads the pinned host
+// copy directly (not a copy-engine transfer, which would queue behind the
+// caller's large chunk uploads and hold up the analysis stream).
+constexpr int kMaxSegs = 1 + 10;
+struct TableCopy
+{
+    const uint32_t* src[kMaxSegs];
+    uint32_t* dst[kMaxSegs];
+    uint32_t words[kMaxSegs];
+    int n;
+};
+
+__global__ void TableCopyKernel(TableCopy t)
+{
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (int i = 0; i < t.n; ++i)
+        for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < t.words[i]; w += stride) t.dst[i][w] = t.src[i][w];
+}
+
+// The device failure word goes back the same way, into pinned host memory.
+__global__ void ErrorOutKernel(const int* err, int* hostErr)
+{
+    if (threadIdx.x == 0) *hostErr = *err;
+}
+
 }   // namespace
 
 struct hw_fused
@@ -144,6 +169,10 @@ struct hw_fused
     PoolStep* hSteps[2] = {nullptr, nullptr};
     int32_t* hLists[2] = {nullptr, nullptr};
     int* hErr[2] = {nullptr, nullptr};
+    // device addresses of the three pinned host buffers
+    PoolStep* mSteps[2] = {nullptr, nullptr};
+    int32_t* mLists[2] = {nullptr, nullptr};
+    int* mErr[2] = {nullptr, nullptr};
     cudaEvent_t ev[2] = {nullptr, nullptr};
     bool inFlight[2] = {false, false};
     uint64_t step = 0;
@@ -158,9 +187,36 @@ struct hw_fused
     std::map<std::vector<int64_t>, int> planSeen;
     uint32_t lastLaunches = 0, lastGraphLaunches = 0;
 
+    // Stage timers (as hw_analyzer_profile): event pairs around each stage's
+    // launches while profiling; steps are not replayed from graphs meanwhile.
+    bool profiling = false;
+    std::vector<cudaEvent_t> evPool;
+    size_t evUsed = 0;
+    std::vector<std::pair<int, size_t>> evMarks;   // (stage, index of start event)
+    size_t Begin(int stage, cudaStream_t s)
+    {
+        if (!profiling) return 0;
+        while (evPool.size() < evUsed + 2)
+        {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return 0;
+            evPool.push_back(e);
+        }
+        const size_t i = evUsed;
+        evUsed += 2;
+        cudaEventRecord(evPool[i], s);
+        evMarks.emplace_back(stage, i);
+        return i + 1;
+    }
+    void End(size_t tok, cudaStream_t s)
+    {
+        if (tok) cudaEventRecord(evPool[tok], s);
+    }
+
     ~hw_fused()
     {
         for (auto& g : graphCache) cudaGraphExecDestroy(g.second);
+        for (auto e : evPool) cudaEventDestroy(e);
         if (capStream) cudaStreamDestroy(capStream);
         for (int b = 0; b < 2; ++b)
         {
@@ -309,36 +365,48 @@ int hw_fused::Launch(cudaStream_t s, const int32_t counts[kNumLists], const int 
             BaselinerArgs a{nullptr, bls, stats, st16, st32, L, maxFList[l]};
             a.map = map(l);
             a.u8 = l == L_BASE8;
+            const size_t t = Begin(HW_STAGE_BASELINE, s);
             HWF_CUDA(LaunchBaseliner(cfg.filter_type, a, k, s), "hw_chunk_fused: baseline filter");
+            End(t, s);
             ++n;
         }
     if (counts[L_AGG])
     {
+        const size_t t = Begin(HW_STAGE_AGGREGATE, s);
         HWF_CUDA(LaunchAggMerge(acc, stats, L, s, map(L_AGG)), "hw_chunk_fused: statistics merge");
+        End(t, s);
         ++n;
     }
     if (counts[L_HIST])
     {
+        const size_t t = Begin(HW_STAGE_HISTOGRAM, s);
         HWF_CUDA(LaunchHistAdd(hist, edgePrev, edgeBits, bls, maxFList[L_HIST], models, L, s, map(L_HIST)),
                  "hw_chunk_fused: histogram");
+        End(t, s);
         ++n;
     }
     if (counts[L_INIT])
     {
+        const size_t t = Begin(HW_STAGE_MODEL_INIT, s);
         HWF_CUDA(LaunchInitModels(models, acc, L, k, s, map(L_INIT)), "hw_chunk_fused: model initialisation");
+        End(t, s);
         ++n;
     }
     if (counts[L_DME])
     {
         DmeArgs a{hist, acc, models, diag, dmeScratch, err, L, 0, 0};
         a.map = map(L_DME);
+        const size_t t = Begin(HW_STAGE_DME, s);
         HWF_CUDA(LaunchDmeEstimate(a, k, s), "hw_chunk_fused: DME");
+        End(t, s);
         ++n;
     }
     if (counts[L_RESET])
     {
+        const size_t t = Begin(HW_STAGE_HIST_RESET, s);
         HWF_CUDA(LaunchHistResetStats(hist, acc, L, k, err, s, map(L_RESET)), "hw_chunk_fused: histogram reset");
         HWF_CUDA(LaunchAggReset(acc, L, s, map(L_RESET)), "hw_chunk_fused: aggregator reset");
+        End(t, s);
         n += 2;
     }
     if (counts[L_LABEL])
@@ -346,11 +414,15 @@ int hw_fused::Launch(cudaStream_t s, const int32_t counts[kNumLists], const int 
         LabelerArgs la{bls, models, labels, latent, score, latModel, latLabel, latRoi, latTrc, prevLat, tb, L,
                        maxFList[L_LABEL]};
         la.map = map(L_LABEL);
+        size_t t = Begin(HW_STAGE_LABELER, s);
         HWF_CUDA(LaunchLabeler(la, k, s), "hw_chunk_fused: labeler");
+        End(t, s);
         PulseArgs pa{labels, latent, bls, models, nullptr, nullptr, nullptr, paStats, segStart, segFirst, segLast,
                      segMax, segTotal, segM2, segLabel, L, maxFList[L_LABEL], 0};
         pa.map = map(L_LABEL);
+        t = Begin(HW_STAGE_PULSES, s);
         HWF_CUDA(LaunchPulses(pa, k, s), "hw_chunk_fused: pulse accumulator");
+        End(t, s);
         n += 3;
     }
     if (counts[L_LP])
@@ -493,10 +565,15 @@ int hw_fused_create(const hw_config* cfg, uint32_t n_pools, const uint32_t* pool
     if ((rc = AllocZero(&f->dLists, (size_t)kNumLists * L, where))) return rc;
     for (int b = 0; b < 2; ++b)
     {
-        HWF_CUDA(cudaMallocHost((void**)&f->hSteps[b], sizeof(PoolStep) * n_pools), where);
-        HWF_CUDA(cudaMallocHost((void**)&f->hLists[b], sizeof(int32_t) * kNumLists * (size_t)L), where);
-        HWF_CUDA(cudaMallocHost((void**)&f->hErr[b], sizeof(int)), where);
+        // mapped: the step kernels read the tables and write the failure word in place
+        HWF_CUDA(cudaHostAlloc((void**)&f->hSteps[b], sizeof(PoolStep) * n_pools, cudaHostAllocMapped), where);
+        HWF_CUDA(cudaHostAlloc((void**)&f->hLists[b], sizeof(int32_t) * kNumLists * (size_t)L, cudaHostAllocMapped),
+                 where);
+        HWF_CUDA(cudaHostAlloc((void**)&f->hErr[b], sizeof(int), cudaHostAllocMapped), where);
         *f->hErr[b] = 0;
+        HWF_CUDA(cudaHostGetDevicePointer((void**)&f->mSteps[b], f->hSteps[b], 0), where);
+        HWF_CUDA(cudaHostGetDevicePointer((void**)&f->mLists[b], f->hLists[b], 0), where);
+        HWF_CUDA(cudaHostGetDevicePointer((void**)&f->mErr[b], f->hErr[b], 0), where);
         HWF_CUDA(cudaEventCreateWithFlags(&f->ev[b], cudaEventDisableTiming), where);
     }
     HWF_CUDA(cudaDeviceSynchronize(), where);
@@ -563,15 +640,28 @@ int hw_chunk_fused(hw_fused* f, hw_pool_chunk* table, uint32_t n_pools, void* st
         if ((rc = Alloc(&f->dmeScratch, (size_t)counts[L_DME] * 3 * (kBins + 1) * kLane, "hw_chunk_fused"))) return rc;
         f->dmeCap = (uint32_t)counts[L_DME];
     }
-    HWF_CUDA(cudaMemcpyAsync(f->dSteps, f->hSteps[b], sizeof(PoolStep) * n_pools, cudaMemcpyHostToDevice, s),
-             "hw_chunk_fused");
-    for (int l = 0; l < kNumLists; ++l)
-        if (counts[l])
-            HWF_CUDA(cudaMemcpyAsync(f->dLists + (size_t)l * f->lanes, f->hLists[b] + (size_t)l * f->lanes,
-                                     sizeof(int32_t) * counts[l], cudaMemcpyHostToDevice, s),
-                     "hw_chunk_fused");
+    {
+        TableCopy t{};
+        uint64_t words = sizeof(PoolStep) / 4 * (uint64_t)n_pools;
+        t.src[0] = reinterpret_cast<const uint32_t*>(f->mSteps[b]);
+        t.dst[0] = reinterpret_cast<uint32_t*>(f->dSteps);
+        t.words[0] = (uint32_t)words;
+        t.n = 1;
+        for (int l = 0; l < kNumLists; ++l)
+            if (counts[l])
+            {
+                t.src[t.n] = reinterpret_cast<const uint32_t*>(f->mLists[b] + (size_t)l * f->lanes);
+                t.dst[t.n] = reinterpret_cast<uint32_t*>(f->dLists + (size_t)l * f->lanes);
+                t.words[t.n] = (uint32_t)counts[l];
+                words += (uint64_t)counts[l];
+                ++t.n;
+            }
+        const int blocks = (int)std::min<uint64_t>(148 * 4, (words + 255) / 256);
+        TableCopyKernel<<<blocks, 256, 0, s>>>(t);
+        HWF_CUDA(cudaGetLastError(), "hw_chunk_fused: step tables");
+    }
     uint32_t launches = 0, graphLaunches = 0;
-    if (f->graphs)
+    if (f->graphs && !f->profiling)
     {
         std::vector<int64_t> key;
         for (int l = 0; l < kNumLists; ++l)
@@ -605,10 +695,11 @@ int hw_chunk_fused(hw_fused* f, hw_pool_chunk* table, uint32_t n_pools, void* st
         }
     }
     if (!graphLaunches && (rc = f->Launch(s, counts, maxFList, &launches))) return rc;
-    HWF_CUDA(cudaMemcpyAsync(f->hErr[b], f->err, sizeof(int), cudaMemcpyDeviceToHost, s), "hw_chunk_fused");
+    ErrorOutKernel<<<1, 32, 0, s>>>(f->err, f->mErr[b]);
+    HWF_CUDA(cudaGetLastError(), "hw_chunk_fused: failure word");
     HWF_CUDA(cudaEventRecord(f->ev[b], s), "hw_chunk_fused");
     f->inFlight[b] = true;
-    f->lastLaunches = launches;
+    f->lastLaunches = launches + 2;     // + the table and failure-word kernels
     f->lastGraphLaunches = graphLaunches;
     ++f->step;
     return HW_OK;
@@ -637,6 +728,30 @@ int hw_fused_models(const hw_fused* f, uint32_t pool, hw_lane_model* d_out, hw_f
                              reinterpret_cast<cudaStream_t>(stream)),
              "hw_fused_models");
     if (fi) *fi = P.modelFi;
+    return HW_OK;
+}
+
+int hw_fused_profile(hw_fused* f, int32_t enable)
+{
+    if (!f) return Fail(HW_ERR_INVALID_ARG, "NULL engine");
+    f->profiling = enable != 0;
+    return HW_OK;
+}
+
+int hw_fused_stage_times(hw_fused* f, double ms[HW_NUM_STAGES], uint32_t launches[HW_NUM_STAGES])
+{
+    if (!f || !ms || !launches) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    for (int i = 0; i < HW_NUM_STAGES; ++i) { ms[i] = 0.0; launches[i] = 0; }
+    for (const auto& m : f->evMarks)
+    {
+        HWF_CUDA(cudaEventSynchronize(f->evPool[m.second + 1]), "hw_fused_stage_times");
+        float t = 0.0f;
+        HWF_CUDA(cudaEventElapsedTime(&t, f->evPool[m.second], f->evPool[m.second + 1]), "hw_fused_stage_times");
+        ms[m.first] += t;
+        launches[m.first] += 1;
+    }
+    f->evMarks.clear();
+    f->evUsed = 0;
     return HW_OK;
 }
 

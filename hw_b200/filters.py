@@ -403,15 +403,20 @@ class FusedEngine(_Handle):
             t[i] = (F, fuse, lpc, 0)
         check(lib().hw_fused_set_tuning(self._h, abi.ptr(t), len(t)))
 
-    def process(self, chunks):
+    def process(self, chunks, outputs=None):
         """One step: chunks[p] is pool p's next chunk [lanes][F][64] (int16 or
-        uint8 CUDA tensor).  Returns (emitted, estimated) flags per pool."""
+        uint8 CUDA tensor).  outputs[p] = (pulses, lens, overflows) receives
+        pool p's results (default: the engine's own buffers, outputs(p)).
+        Returns (emitted, estimated) flags per pool."""
         t = self.table
         for p, c in enumerate(chunks):
             if c.dtype == torch.uint8:
                 t["d_trace"][p], t["d_trace8"][p] = 0, c.data_ptr()
             else:
                 t["d_trace"][p], t["d_trace8"][p] = c.data_ptr(), 0
+        outs = outputs if outputs is not None else [self.outputs(p) for p in range(len(t))]
+        for p, (pp, pl, po) in enumerate(outs):
+            t["d_pulses"][p], t["d_lens"][p], t["d_overflows"][p] = pp.data_ptr(), pl.data_ptr(), po.data_ptr()
         t["first_frame"] = self.next_frame
         check(lib().hw_chunk_fused(self._h, abi.ptr(t), len(t), _stream()))
         self.next_frame += self.frames
@@ -429,6 +434,16 @@ class FusedEngine(_Handle):
         fi = abi.FrameInterval()
         check(lib().hw_fused_models(self._h, p, _p(out), C.byref(fi), _stream()))
         return out, fi.tuple()
+
+    def profile(self, enable=True):
+        check(lib().hw_fused_profile(self._h, 1 if enable else 0))
+
+    def stage_times(self):
+        """{stage: (device ms, launches)} since the previous call (synchronises)."""
+        ms = np.zeros(len(BatchAnalyzer.STAGES), np.float64)
+        n = np.zeros(len(BatchAnalyzer.STAGES), np.uint32)
+        check(lib().hw_fused_stage_times(self._h, abi.ptr(ms), abi.ptr(n)))
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(BatchAnalyzer.STAGES)}
 
     def last_step(self):
         """(kernel launches, graph launches) of the last step."""

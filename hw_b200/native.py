@@ -75,6 +75,8 @@ def lib():
         "hw_fused_set_tuning": ([vp, vp, u32], C.c_int),
         "hw_fused_models": ([vp, u32, vp, C.POINTER(FI), vp], C.c_int),
         "hw_fused_last_step": ([vp, C.POINTER(u32), C.POINTER(u32)], C.c_int),
+        "hw_fused_profile": ([vp, i32], C.c_int),
+        "hw_fused_stage_times": ([vp, vp, vp], C.c_int),
         "hw_analyzer_state_size": ([vp, C.POINTER(C.c_uint64)], C.c_int),
         "hw_analyzer_state_export": ([vp, vp, C.c_uint64, vp], C.c_int),
         "hw_analyzer_state_import": ([vp, vp, C.c_uint64, vp], C.c_int),

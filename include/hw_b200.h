@@ -568,6 +568,11 @@ int hw_fused_use_graphs(hw_fused* f, int32_t enable);
 int hw_fused_set_tuning(hw_fused* f, const hw_fused_tuning* tuning, uint32_t n);
 /* Device copy of pool p's current models and their frame interval. */
 int hw_fused_models(const hw_fused* f, uint32_t pool, hw_lane_model* d_out, hw_frame_interval* fi, void* stream);
+/* Stage timers with the meaning of hw_analyzer_profile / _stage_times (the
+ * HW_STAGE_* indices; a fused labeler + pulse kernel counts as the labeler).
+ * While profiling, steps are launched kernel by kernel, not from graphs. */
+int hw_fused_profile(hw_fused* f, int32_t enable);
+int hw_fused_stage_times(hw_fused* f, double* ms, uint32_t* launches);
 /* Kernel launches and graph replays of the last step (graph nodes are not
  * counted as launches). */
 int hw_fused_last_step(const hw_fused* f, uint32_t* launches, uint32_t* graph_launches);
