@@ -63,11 +63,17 @@ enum List
     L_INIT,       // CoreDMEstimator::InitDetectionModels
     L_DME,        // CoreDMEstimator::Estimate
     L_RESET,      // histogram reset from the aggregated statistics + aggregator reset
-    L_LABEL,      // frame labeler + pulse accumulator, separate kernels
-    L_LP,         // frame labeler + pulse accumulator, one kernel
+    L_LABEL1,     // frame labeler + pulse accumulator, separate kernels, 1/2/4 lanes a labeler block
+    L_LABEL2,
+    L_LABEL4,
+    L_LP1,        // frame labeler + pulse accumulator in one kernel, 1/2/4 lanes a block
+    L_LP2,
+    L_LP4,
     L_ZERO,       // pools that emit nothing this step
     kNumLists
 };
+
+int LanesPerCta(int list) { return 1 << ((list - L_LABEL1) % 3); }
 
 // Per pool: hw_analyzer's schedule state.
 struct PoolRt
@@ -94,7 +100,7 @@ int32_t Center(hw_frame_interval fi) { return fi.lower + (fi.upper - fi.lower) /
 // Step tables reach the device through a kernel that reads the pinned host
 // copy directly (not a copy-engine transfer, which would queue behind the
 // caller's large chunk uploads and hold up the analysis stream).
-constexpr int kMaxSegs = 1 + 10;
+constexpr int kMaxSegs = 1 + kNumLists;
 struct TableCopy
 {
     const uint32_t* src[kMaxSegs];
@@ -301,8 +307,11 @@ int hw_fused::Schedule(hw_pool_chunk* table, int b, int32_t counts[kNumLists], i
             return HW_OK;
         };
         auto labelAndPulse = [&]() {
+            // kernel choice of this chunk length (default: separate kernels, 2 lanes a block)
+            uint32_t fuse = 0, lpc = 2;
             auto t = tuning.find(P.F);
-            append((t != tuning.end() && t->second.first) ? L_LP : L_LABEL);
+            if (t != tuning.end()) { fuse = t->second.first; lpc = t->second.second; }
+            append((fuse ? L_LP1 : L_LABEL1) + (lpc == 1 ? 0 : lpc == 2 ? 1 : 2));
         };
         int rc = HW_OK;
         if (cfg.model_estimation_mode == HW_FIXED_ESTIMATIONS)
@@ -409,24 +418,28 @@ int hw_fused::Launch(cudaStream_t s, const int32_t counts[kNumLists], const int 
         End(t, s);
         n += 2;
     }
-    if (counts[L_LABEL])
+    for (int l = L_LABEL1; l <= L_LP4; ++l)
     {
+        if (!counts[l]) continue;
+        const bool fuse = l >= L_LP1;
         LabelerArgs la{bls, models, labels, latent, score, latModel, latLabel, latRoi, latTrc, prevLat, tb, L,
-                       maxFList[L_LABEL]};
-        la.map = map(L_LABEL);
-        size_t t = Begin(HW_STAGE_LABELER, s);
-        HWF_CUDA(LaunchLabeler(la, k, s), "hw_chunk_fused: labeler");
-        End(t, s);
+                       maxFList[l]};
+        la.map = map(l);
         PulseArgs pa{labels, latent, bls, models, nullptr, nullptr, nullptr, paStats, segStart, segFirst, segLast,
-                     segMax, segTotal, segM2, segLabel, L, maxFList[L_LABEL], 0};
-        pa.map = map(L_LABEL);
-        t = Begin(HW_STAGE_PULSES, s);
-        HWF_CUDA(LaunchPulses(pa, k, s), "hw_chunk_fused: pulse accumulator");
+                     segMax, segTotal, segM2, segLabel, L, maxFList[l], 0};
+        pa.map = map(l);
+        size_t t = Begin(HW_STAGE_LABELER, s);
+        HWF_CUDA(LaunchLabeler(la, k, s, fuse ? &pa : nullptr, LanesPerCta(l)), "hw_chunk_fused: labeler");
         End(t, s);
-        n += 3;
+        n += 2;
+        if (!fuse)
+        {
+            t = Begin(HW_STAGE_PULSES, s);
+            HWF_CUDA(LaunchPulses(pa, k, s), "hw_chunk_fused: pulse accumulator");
+            End(t, s);
+            ++n;
+        }
     }
-    if (counts[L_LP])
-        return Fail(HW_ERR_UNSUPPORTED, "fused labeler and pulse kernel is not built");
     if (counts[L_ZERO])
     {
         HWF_CUDA(LaunchZeroOutputs(map(L_ZERO), s), "hw_chunk_fused: empty outputs");

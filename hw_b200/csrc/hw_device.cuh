@@ -259,7 +259,11 @@ cudaError_t LaunchInitModels(hw_lane_model* m, const hw_baseliner_stats* s, int 
 // that emit nothing this chunk).
 cudaError_t LaunchZeroOutputs(const LaneMap& map, cudaStream_t st);
 cudaError_t LaunchDmeEstimate(const DmeArgs& a, const KParams& k, cudaStream_t s);
-cudaError_t LaunchLabeler(const LabelerArgs& a, const KParams& k, cudaStream_t s);
+// fusedPulses: run the pulse accumulator in the labeler kernel (lane-list
+// launches only); lanesPerCta: 1, 2 or 4 lanes a block (2 for single-pool
+// launches).
+cudaError_t LaunchLabeler(const LabelerArgs& a, const KParams& k, cudaStream_t s,
+                          const PulseArgs* fusedPulses = nullptr, int lanesPerCta = 2);
 cudaError_t LaunchPulses(const PulseArgs& a, const KParams& k, cudaStream_t s);
 struct GenArgs;
 // Records the thread's last error message (capi.cu) and returns code.

@@ -17,7 +17,7 @@
 //      picks the anchor state and traces back F frames.
 // Traceback words live in a global scratch laid out [lane][frame][zmw] so
 // each warp writes and reads one 128-byte line per frame.
-#include "hw_device.cuh"
+#include "pulse_seg.cuh"
 
 namespace hwk {
 
@@ -181,8 +181,16 @@ __device__ __forceinline__ int TraceSource(uint32_t w, int state)
 
 constexpr int kBatch = 8;                              // frames loaded ahead
 
-template <bool Mapped>
-__global__ void __launch_bounds__(128, 5) LabelerKernel(LabelerArgs A, KParams k)
+// Blocks per SM the labeler variants are compiled for (96 registers a thread).
+constexpr int LabelerMinBlocks(int threads) { return threads == 64 ? 10 : threads == 128 ? 5 : 2; }
+
+// Mapped: lane-list launch.  Fuse: the pulse accumulator runs in the same
+// thread right after the traceback, on labels kept in shared memory (4 bits a
+// frame) instead of a labels batch in global memory.  Threads: 64 ZMWs (one
+// lane) per 64 threads.
+template <bool Mapped, bool Fuse, int Threads>
+__global__ void __launch_bounds__(Threads, LabelerMinBlocks(Threads)) LabelerKernel(LabelerArgs A, KParams k,
+                                                                                     PulseArgs P)
 {
     LaneMap map = A.map;
     if (!Mapped) map.list = nullptr;      // the single-pool variant compiles without the lane list
@@ -342,22 +350,68 @@ __global__ void __launch_bounds__(128, 5) LabelerKernel(LabelerArgs A, KParams k
     for (int i = 1; i < kStates; ++i) ret = (anchorState == i) ? anchorLL[i] : ret;
 
     int ts = anchorState;
-    int16_t* out = A.labels + map.Block(l, F) + z;
-    for (int f0 = F - kBatch; f0 >= 0; f0 -= kBatch)
+    if constexpr (Fuse)
     {
-        uint32_t w[kBatch];
-#pragma unroll
-        for (int j = 0; j < kBatch; ++j) w[j] = tb[(size_t)(f0 + j) * kLane];
-#pragma unroll
-        for (int j = kBatch - 1; j >= 0; --j)
+        // The ROI words are done with: the last ROI bit goes to the latent
+        // state first, then the traceback packs 8 labels a word into them.
+        A.latRoi[g] = (int16_t)roiBit(F - 1);
+        for (int f0 = F - kBatch; f0 >= 0; f0 -= kBatch)
         {
-            out[(size_t)(f0 + j) * kLane] = (int16_t)ts;
-            ts = TraceSource(w[j], ts);
+            uint32_t w[kBatch];
+#pragma unroll
+            for (int j = 0; j < kBatch; ++j) w[j] = tb[(size_t)(f0 + j) * kLane];
+            uint32_t word = 0;
+#pragma unroll
+            for (int j = kBatch - 1; j >= 0; --j)
+            {
+                word |= (uint32_t)ts << (4 * j);
+                ts = TraceSource(w[j], ts);
+            }
+            roiw(f0 / kBatch) = word;
         }
+        // Pulse accumulation over the labels batch (frames chunk start - 24
+        // .. chunk end - 24): the previous chunk's latent frames, then the
+        // chunk's first F - 24 frames.
+        const PoolStep& ps = map.Pool(l);
+        const int go = (l - ps.lane0) * kLane + z;
+        const uint32_t firstFrame = (uint32_t)(ps.firstFrame - kLatent);
+        PulseSeg seg;
+        seg.Load(P, g, h2f(newM.analogs[kAnalogs - 1].means[z]), ps.pulses + (size_t)go * k.maxCalls);
+        for (int r0 = 0; r0 < F; r0 += kBatch)
+        {
+            const uint32_t word = roiw(r0 / kBatch);
+            int16_t sg[kBatch];
+#pragma unroll
+            for (int j = 0; j < kBatch; ++j)
+            {
+                const int r = r0 + j;
+                sg[j] = (r < kLatent) ? pl[(size_t)r * kLane] : __ldg(chunk + (size_t)(r - kLatent) * kLane);
+            }
+#pragma unroll
+            for (int j = 0; j < kBatch; ++j)
+                seg.Frame(k, (uint32_t)(r0 + j) + firstFrame, (int16_t)((word >> (4 * j)) & 15u), sg[j]);
+        }
+        seg.Store(P, g, l, z, ps.lens, ps.ovf, go);
+    }
+    else
+    {
+        int16_t* out = A.labels + map.Block(l, F) + z;
+        for (int f0 = F - kBatch; f0 >= 0; f0 -= kBatch)
+        {
+            uint32_t w[kBatch];
+#pragma unroll
+            for (int j = 0; j < kBatch; ++j) w[j] = tb[(size_t)(f0 + j) * kLane];
+#pragma unroll
+            for (int j = kBatch - 1; j >= 0; --j)
+            {
+                out[(size_t)(f0 + j) * kLane] = (int16_t)ts;
+                ts = TraceSource(w[j], ts);
+            }
+        }
+        A.latRoi[g] = (int16_t)roiBit(F - 1);
     }
 
     // Latent state update.
-    A.latRoi[g] = (int16_t)roiBit(F - 1);
     A.latLabel[g] = (int16_t)anchorState;
     A.latTrc[g] = chunk[(size_t)(anchor - 1) * kLane];
     if (A.score) A.score[g] = ret;
@@ -380,18 +434,58 @@ __global__ void LabelerModelCopyKernel(hw_lane_model* dst, const hw_lane_model* 
     reinterpret_cast<uint32_t*>(dst)[w] = reinterpret_cast<const uint32_t*>(src)[w];
 }
 
-cudaError_t LaunchLabeler(const LabelerArgs& a, const KParams& k, cudaStream_t s)
+template <bool Mapped, bool Fuse, int Threads>
+cudaError_t LaunchLabelerT(const LabelerArgs& a, const KParams& k, const PulseArgs& p, int lanes, cudaStream_t s)
+{
+    const int blocks = (lanes * kLane + Threads - 1) / Threads;
+    // ROI words during the forward pass, packed labels after it (fused)
+    const int roiWords = (a.F + kLookback + kStitch + 15) / 16;
+    const int words = Fuse ? (roiWords > a.F / kBatch ? roiWords : a.F / kBatch) : roiWords;
+    const size_t smem = (size_t)words * Threads * sizeof(uint32_t);
+    static bool attrSet[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (smem > 48 * 1024 && (dev < 0 || dev >= 64 || !attrSet[dev]))
+    {
+        e = cudaFuncSetAttribute(LabelerKernel<Mapped, Fuse, Threads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(((1024 + kLookback + kStitch + 15) / 16 > 1024 / kBatch
+                                            ? (1024 + kLookback + kStitch + 15) / 16 : 1024 / kBatch) *
+                                       Threads * sizeof(uint32_t)));
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) attrSet[dev] = true;
+    }
+    LabelerKernel<Mapped, Fuse, Threads><<<blocks, Threads, smem, s>>>(a, k, p);
+    return cudaGetLastError();
+}
+
+cudaError_t LaunchLabeler(const LabelerArgs& a, const KParams& k, cudaStream_t s, const PulseArgs* fusedPulses,
+                          int lanesPerCta)
 {
     if (a.F > 1024 || a.F % kBatch != 0) return cudaErrorInvalidValue;
-    const int threads = 128;
     const int lanes = a.map.Lanes(a.lanes);
     if (lanes == 0) return cudaSuccess;
-    const int blocks = (lanes * kLane + threads - 1) / threads;
-    const int roiWords = (a.F + kLookback + kStitch + 15) / 16;
-    const size_t smem = (size_t)roiWords * threads * sizeof(uint32_t);
-    if (a.map.On()) LabelerKernel<true><<<blocks, threads, smem, s>>>(a, k);
-    else LabelerKernel<false><<<blocks, threads, smem, s>>>(a, k);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e;
+    const PulseArgs none{};
+    if (!a.map.On())
+    {
+        if (fusedPulses || lanesPerCta != 2) return cudaErrorInvalidValue;
+        e = LaunchLabelerT<false, false, 128>(a, k, none, lanes, s);
+    }
+    else if (fusedPulses)
+    {
+        if (lanesPerCta == 1) e = LaunchLabelerT<true, true, 64>(a, k, *fusedPulses, lanes, s);
+        else if (lanesPerCta == 2) e = LaunchLabelerT<true, true, 128>(a, k, *fusedPulses, lanes, s);
+        else if (lanesPerCta == 4) e = LaunchLabelerT<true, true, 256>(a, k, *fusedPulses, lanes, s);
+        else return cudaErrorInvalidValue;
+    }
+    else
+    {
+        if (lanesPerCta == 1) e = LaunchLabelerT<true, false, 64>(a, k, none, lanes, s);
+        else if (lanesPerCta == 2) e = LaunchLabelerT<true, false, 128>(a, k, none, lanes, s);
+        else if (lanesPerCta == 4) e = LaunchLabelerT<true, false, 256>(a, k, none, lanes, s);
+        else return cudaErrorInvalidValue;
+    }
     if (e != cudaSuccess) return e;
     const int n = lanes * (int)(sizeof(hw_lane_model) / 4);
     LabelerModelCopyKernel<<<(n + 255) / 256, 256, 0, s>>>(a.latModel, a.models, a.lanes, a.map);

@@ -6,12 +6,9 @@
 // (TA = src/basecaller/basecaller/traceAnalysis, DT = src/basecaller/dataTypes).
 // One thread per ZMW walks the chunk's labels; the open segment is carried
 // across chunks in device state.
-#include "hw_device.cuh"
+#include "pulse_seg.cuh"
 
 namespace hwk {
-
-
-__device__ __forceinline__ uint16_t ToFixed(float v) { return static_cast<uint16_t>(add_rn(v / .1f, 0.5f)); }
 
 __global__ void __launch_bounds__(128) PulseKernel(PulseArgs A, KParams k)
 {
@@ -24,17 +21,9 @@ __global__ void __launch_bounds__(128) PulseKernel(PulseArgs A, KParams k)
     const int F = ps ? ps->F : A.F;
     const uint32_t firstFrame = ps ? (uint32_t)(ps->firstFrame - kLatent) : A.firstFrame;
     const int go = ps ? (l - ps->lane0) * kLane + z : g;     // ZMW index in the output buffers
-    uint32_t* lensOut = ps ? ps->lens : A.lens;
-    uint32_t* ovfOut = ps ? ps->ovf : A.ovf;
-    uint32_t start = A.segStart[g];
-    int16_t first = A.segFirst[g], last = A.segLast[g], mx = A.segMax[g], label = A.segLabel[g];
-    float total = A.segTotal[g], m2 = A.segM2[g];
-    const float minMean = h2f(A.models[l].analogs[kAnalogs - 1].means[z]);
-    const float maxSignal = 65535 * .1f;
-    const float minSignal = 0.0f;
-    uint32_t n = 0, over = 0;
-    hw_pulse* out = (ps ? ps->pulses : A.pulses) + (size_t)go * cap;
-    float b0 = 0.0f, b1 = 0.0f, b2 = 0.0f;   // StatAccumulator of baseline frames (offset 0)
+    PulseSeg seg;
+    seg.Load(A, g, h2f(A.models[l].analogs[kAnalogs - 1].means[z]),
+             (ps ? ps->pulses : A.pulses) + (size_t)go * cap);
     const int16_t* lab = A.labels + A.map.Block(l, F) + z;
     const int16_t* lat = A.latTrace + (size_t)l * kLatent * kLane + z;
     const int16_t* tr = A.trace + A.map.Block(l, F) + z;
@@ -51,64 +40,9 @@ __global__ void __launch_bounds__(128) PulseKernel(PulseArgs A, KParams k)
             sgB[j] = (r < kLatent) ? __ldg(lat + (size_t)r * kLane) : __ldg(tr + (size_t)(r - kLatent) * kLane);
         }
 #pragma unroll
-        for (int j = 0; j < kB; ++j)
-        {
-        const int rel = rel0 + j;
-        const uint32_t absF = (uint32_t)rel + firstFrame;
-        const int16_t lb = lbB[j];
-        const int16_t signal = sgB[j];
-        const bool isUp = (lb > kAnalogs) & (lb <= 2 * kAnalogs);
-        const bool boundary = isUp | ((lb == 0) & (label != 0));
-        const bool pulseM = label != 0;
-        if (boundary & pulseM)
-        {
-            // LabelsSegment::ToPulse (HostPulseAccumulator.h:106-138)
-            const int width = (int)(absF - start);
-            const float rawMean = float(add_rn(add_rn(total, (float)last), (float)first)) / (float)width;
-            const float rawMid = total / (float)(width - 2);
-            const bool keep = ((float)width >= k.widthThresh) || (mul_rn(rawMean, (float)width) >= mul_rn(k.ampThresh, minMean));
-            hw_pulse p;
-            p.start = start;
-            p.width = (uint16_t)width;
-            p.mean_signal = ToFixed(fmin_std(maxSignal, fmax_std(minSignal, rawMean)));
-            p.mid_signal = ToFixed(width < 3 ? 0.0f : fmin_std(maxSignal, fmax_std(minSignal, rawMid)));
-            p.max_signal = ToFixed(fmin_std(maxSignal, fmax_std(minSignal, (float)mx)));
-            p.signal_m2 = m2;
-            int lbl = label;
-            if (lbl > 2 * kAnalogs) lbl -= 2 * kAnalogs;
-            if ((lbl > kAnalogs) & (lbl <= 2 * kAnalogs)) lbl -= kAnalogs;
-            p.label = k.analogMap[lbl - 1];
-            p.is_reject = keep ? 0 : 1;
-            p.pad_[0] = 0; p.pad_[1] = 0;
-            if (n < (uint32_t)cap) out[n++] = p;
-            else ++over;
-        }
-        if (boundary)
-        {
-            start = absF; first = signal; last = 0; mx = signal; total = 0.0f; m2 = 0.0f; label = lb;
-        }
-        else
-        {
-            total = add_rn(total, (float)last);
-            m2 = add_rn(m2, mul_rn((float)last, (float)last));
-            last = signal;
-            mx = signal > mx ? signal : mx;
-        }
-        if ((!pulseM) & (!boundary))
-        {
-            const float x = (float)signal;
-            b0 += 1.0f; b1 = add_rn(b1, x); b2 = add_rn(b2, mul_rn(x, x));
-        }
-            }
+        for (int j = 0; j < kB; ++j) seg.Frame(k, (uint32_t)(rel0 + j) + firstFrame, lbB[j], sgB[j]);
     }
-    A.segStart[g] = start; A.segFirst[g] = first; A.segLast[g] = last; A.segMax[g] = mx;
-    A.segTotal[g] = total; A.segM2[g] = m2; A.segLabel[g] = label;
-    lensOut[go] = n;
-    ovfOut[go] = over;
-    A.bls[l].offset[z] = 0.0f;
-    A.bls[l].moment0[z] = b0;
-    A.bls[l].moment1[z] = b1;
-    A.bls[l].moment2[z] = b2;
+    seg.Store(A, g, l, z, ps ? ps->lens : A.lens, ps ? ps->ovf : A.ovf, go);
 }
 
 cudaError_t LaunchPulses(const PulseArgs& a, const KParams& k, cudaStream_t s)

@@ -369,6 +369,8 @@ class FusedEngine(_Handle):
     _destroy = "hw_fused_destroy"
 
     def __init__(self, cfg, lanes, frames_per_chunk, pool_ids=None, graphs=False, tuning=None):
+        """tuning: {frames_per_chunk: (fuse_label_pulses, labeler_lanes_per_cta)},
+        or "auto" for the autotuner's cached choices on this device."""
         super().__init__()
         self.lanes = np.ascontiguousarray(lanes, np.uint32)
         self.frames = np.ascontiguousarray(frames_per_chunk, np.uint32)
@@ -390,6 +392,9 @@ class FusedEngine(_Handle):
         self.next_frame = np.zeros(n, np.int64)
         if graphs:
             self.use_graphs(True)
+        if isinstance(tuning, str) and tuning == "auto":
+            from . import autotune
+            tuning = autotune.load()
         if tuning:
             self.set_tuning(tuning)
 

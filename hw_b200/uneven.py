@@ -6,8 +6,8 @@ analysis parameters with dynamic estimation.
 
 Ways of running the same pools on the same traces, each timed on its own:
   * fused engine (hw_chunk_fused): every stage of a step is one launch over
-    the lanes of all pools that take it; `fused_graphs` replays each step
-    plan as a CUDA graph;
+    the lanes of all pools that take it; `fused_tuned` with the autotuner's
+    kernel choices, `fused_graphs` replaying each step plan as a CUDA graph;
   * pool set (hw_pool_set): pools that share chunk length and stagger class
     run as one batched analyzer, one launch per stage and class;
   * one analyzer per pool, each with its own launches (what a per-pool
@@ -60,7 +60,7 @@ def _timed(process, gens, frames, warmup_steps, steps, stream, fill):
     return t / steps
 
 
-def run(n_pools=500, steps=4, warmup_steps=None, variants=("fused", "fused_graphs", "pool_set", "per_pool"), seed=0):
+def run(n_pools=500, steps=4, warmup_steps=None, variants=("fused_tuned", "fused", "pool_set", "per_pool"), seed=0):
     cfg = workloads.chip_config()
     lanes, frames = pool_shapes(n_pools, seed)
     if warmup_steps is None:
@@ -79,8 +79,9 @@ def run(n_pools=500, steps=4, warmup_steps=None, variants=("fused", "fused_graph
 
     for v in variants:
         gens = _gens(lanes)
-        if v in ("fused", "fused_graphs"):
-            eng = Fl.FusedEngine(cfg, lanes, frames, graphs=(v == "fused_graphs"))
+        if v.startswith("fused"):
+            eng = Fl.FusedEngine(cfg, lanes, frames, graphs=(v == "fused_graphs"),
+                                 tuning="auto" if v == "fused_tuned" else None)
             bufs = per_pool_buffers()
 
             def fill(step):
@@ -132,7 +133,7 @@ def main():
     ap.add_argument("--pools", type=int, default=500)
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup-steps", type=int, default=None)
-    ap.add_argument("--variants", default="fused,fused_graphs,pool_set,per_pool")
+    ap.add_argument("--variants", default="fused_tuned,fused,pool_set,per_pool")
     a = ap.parse_args()
     print(json.dumps(run(a.pools, a.steps, a.warmup_steps, tuple(a.variants.split(",")))))
 

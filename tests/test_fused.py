@@ -94,3 +94,15 @@ def test_fused_rejects_out_of_order_chunks():
     with pytest.raises(HwError):
         eng.process(_chunks(gens, [256, 512], 1, False))
     eng.finish()
+
+
+@pytest.mark.parametrize("tuning", [
+    {512: (1, 2), 256: (1, 1), 128: (0, 4)},
+    {512: (0, 1), 256: (1, 4), 128: (1, 2)},
+    {512: (1, 4), 256: (0, 2), 128: (1, 1)},
+])
+def test_fused_kernel_variants_equal_per_pool_analyzers(tuning):
+    """Every labeler variant (fused with the pulse accumulator or not, 1, 2 or
+    4 lanes a block) gives the per-pool analyzers' results."""
+    emitted, estimated, _ = _compare(abi.DYNAMIC_ESTIMATIONS, graphs=False, u8=False, steps=28, tuning=tuning)
+    assert emitted > 0 and estimated > 0
