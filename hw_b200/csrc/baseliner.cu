@@ -57,6 +57,24 @@ template <int FT> struct FLayout
             }
         return t;
     }
+    static constexpr int NumGlobalStages()
+    {
+        int t = 0;
+        for (int k = 0; k < nStages; ++k) if (!InSmem(k)) ++t;
+        return 2 * t;
+    }
+    // index of a global stage among the global stages (lower first)
+    static constexpr int GIdx(bool upper, int k)
+    {
+        int t = 0;
+        for (int u = 0; u < 2; ++u)
+            for (int j = 0; j < nStages; ++j)
+            {
+                if (u == (upper ? 1 : 0) && j == k) return t;
+                if (!InSmem(j)) ++t;
+            }
+        return t;
+    }
     static constexpr int GlobalRingSlots()
     {
         int t = 0;
@@ -86,7 +104,7 @@ template <int FT> struct FLayout
 // extremum P of the current block and the current block's inputs B; the
 // output at block position c is op(S[c], P).  `base` points at S[0] of this
 // thread and `stride` separates consecutive array elements.
-template <int W, bool IsMax, bool Batched>
+template <int W, bool IsMax>
 __device__ __forceinline__ int16_t StageStep(int16_t* base, int stride, int16_t& P, int16_t& counter, int16_t x)
 {
     auto op = [](int16_t a, int16_t b) -> int16_t {
@@ -100,13 +118,48 @@ __device__ __forceinline__ int16_t StageStep(int16_t* base, int stride, int16_t&
     P = op(P, x);
     if (c + 1 == W)
     {
-        // New suffix extrema of the completed block.  For windows in global
-        // memory the inputs are read in batches of 4 before the batch's results
-        // are stored, so the loads overlap instead of each waiting behind the
-        // previous store.
+        // New suffix extrema of the completed block.
         int16_t acc = x;
         S[(W - 1) * stride] = acc;
-        constexpr int kBatch = Batched ? 4 : 1;
+#pragma unroll 1
+        for (int j = W - 2; j >= 0; --j)
+        {
+            acc = op(B[j * stride], acc);
+            S[j * stride] = acc;
+        }
+        P = IsMax ? (int16_t)-32768 : (int16_t)32767;
+        counter = 0;
+    }
+    else
+    {
+        counter = (int16_t)(c + 1);
+    }
+    return y;
+}
+
+// Global-memory window stage with S[counter] held in a register, loaded one
+// call ahead of its use (S changes only when a block completes), so the
+// stage never waits for memory on its critical path.  At a block's end the
+// inputs are read in batches of 4 before the batch's results are stored, so
+// the loads overlap instead of each waiting behind the previous store.
+template <int W, bool IsMax>
+__device__ __forceinline__ int16_t StageStepG(int16_t* base, int stride, int16_t& P, int16_t& counter,
+                                              int16_t& sNext, int16_t x)
+{
+    auto op = [](int16_t a, int16_t b) -> int16_t {
+        return IsMax ? (a > b ? a : b) : (a < b ? a : b);
+    };
+    int16_t* S = base;
+    int16_t* B = base + W * stride;
+    const int c = counter;
+    const int16_t y = op(sNext, P);
+    B[c * stride] = x;
+    P = op(P, x);
+    if (c + 1 == W)
+    {
+        int16_t acc = x;
+        S[(W - 1) * stride] = acc;
+        constexpr int kBatch = 4;
 #pragma unroll 1
         for (int j0 = W - 2; j0 >= 0; j0 -= kBatch)
         {
@@ -122,12 +175,14 @@ __device__ __forceinline__ int16_t StageStep(int16_t* base, int stride, int16_t&
                     S[(j0 - q) * stride] = acc;
                 }
         }
+        sNext = acc;      // S[0]
         P = IsMax ? (int16_t)-32768 : (int16_t)32767;
         counter = 0;
     }
     else
     {
         counter = (int16_t)(c + 1);
+        sNext = S[(c + 1) * stride];
     }
     return y;
 }
@@ -138,6 +193,7 @@ struct StageMem
     int sstride;       // blockDim.x
     int16_t* gmem;     // this ZMW's column of the global-resident arrays
     int gstride;       // nZmw
+    int16_t* sNext;    // per global stage: S[counter], loaded ahead
 };
 
 template <int FT, bool Upper, int K>
@@ -148,9 +204,28 @@ __device__ __forceinline__ int16_t Stage(const StageMem& m, int16_t* pc, int16_t
     constexpr int off = Lay::Offset(Upper, K);
     constexpr int i = Lay::Idx(Upper, K);
     if constexpr (Lay::InSmem(K))
-        return StageStep<W, Lay::IsMax(Upper, K), false>(m.smem + off * m.sstride, m.sstride, pc[2 * i], pc[2 * i + 1], x);
+        return StageStep<W, Lay::IsMax(Upper, K)>(m.smem + off * m.sstride, m.sstride, pc[2 * i], pc[2 * i + 1], x);
     else
-        return StageStep<W, Lay::IsMax(Upper, K), true>(m.gmem + (size_t)off * m.gstride, m.gstride, pc[2 * i], pc[2 * i + 1], x);
+        return StageStepG<W, Lay::IsMax(Upper, K)>(m.gmem + (size_t)off * m.gstride, m.gstride, pc[2 * i],
+                                                   pc[2 * i + 1], m.sNext[Lay::GIdx(Upper, K)], x);
+}
+
+// sNext of every global-memory stage of one filter from the saved state
+// (compile-time recursion: the stage layout tables are host constants).
+template <int FT, bool Upper, int K>
+__device__ __forceinline__ void LoadSNext(const StageMem& m, const int16_t* pc, int nZmw)
+{
+    using Lay = FLayout<FT>;
+    if constexpr (K < Lay::nStages)
+    {
+        if constexpr (!Lay::InSmem(K))
+        {
+            constexpr int i = Lay::Idx(Upper, K);
+            constexpr int off = Lay::Offset(Upper, K);
+            m.sNext[Lay::GIdx(Upper, K)] = m.gmem[((size_t)off + (size_t)pc[2 * i + 1]) * (size_t)nZmw];
+        }
+        LoadSNext<FT, Upper, K + 1>(m, pc, nZmw);
+    }
 }
 
 template <int FT, bool Upper, int Scale>
@@ -231,8 +306,11 @@ __global__ void __launch_bounds__(64, 7) BaselinerKernel(BaselinerArgs a, KParam
     // wide ones used in place in global memory.
     extern __shared__ int16_t blSmem[];
     constexpr int SS = Lay::SmemSlots();
-    const StageMem mem{blSmem + threadIdx.x, (int)blockDim.x, a.st16 + (size_t)Lay::SlotGlobal() * nZmw + g, nZmw};
-#pragma unroll 8
+    constexpr int NG = Lay::NumGlobalStages() > 0 ? Lay::NumGlobalStages() : 1;
+    int16_t sNext[NG];
+    const StageMem mem{blSmem + threadIdx.x, (int)blockDim.x, a.st16 + (size_t)Lay::SlotGlobal() * nZmw + g, nZmw,
+                       sNext};
+#pragma unroll 32
     for (int i = 0; i < SS; ++i) blSmem[i * blockDim.x + threadIdx.x] = a.st16[(size_t)(Lay::SlotSmem() + i) * nZmw + g];
     int16_t pc[4 * Lay::nStages];
 #pragma unroll
@@ -243,6 +321,9 @@ __global__ void __launch_bounds__(64, 7) BaselinerKernel(BaselinerArgs a, KParam
         pc[2 * i] = a.st16[(size_t)Lay::SlotPC(up, k) * nZmw + g];
         pc[2 * i + 1] = a.st16[(size_t)(Lay::SlotPC(up, k) + 1) * nZmw + g];
     }
+    // S[counter] of every global stage
+    LoadSNext<FT, false, 0>(mem, pc, nZmw);
+    LoadSNext<FT, true, 0>(mem, pc, nZmw);
     int16_t latData = a.st16[(size_t)Lay::SlotLatData() * nZmw + g];
     int16_t latRaw = a.st16[(size_t)(Lay::SlotLatData() + 1) * nZmw + g];
     const int16_t mbits = a.st16[(size_t)(Lay::SlotLatData() + 2) * nZmw + g];
@@ -271,13 +352,16 @@ __global__ void __launch_bounds__(64, 7) BaselinerKernel(BaselinerArgs a, KParam
     // Frames go in blocks of 16 (the aggregate stride): the first frame of a
     // block, the other even frames and the odd frames each get their own
     // specialisation of the frame body, with the trace loaded two frames ahead.
+    // Even frames take their value from xEven and odd frames from xOdd, each
+    // refilled right after use: no register is copied while its load is in
+    // flight (a rotation xn0 = xn1 would wait for the newest load every frame).
     static_assert(Lay::AggStride() == 16, "block size must be the aggregate stride");
-    int16_t xn0 = (int16_t)__ldg(tr), xn1 = (int16_t)__ldg(tr + kLane);
+    int16_t xEven = (int16_t)__ldg(tr), xOdd = (int16_t)__ldg(tr + kLane);
     auto frame = [&](auto phaseTag, int t) {
         constexpr int Ph = decltype(phaseTag)::value;
-        const int16_t x = xn0;
-        xn0 = xn1;
-        if (t + 2 < F) xn1 = (int16_t)__ldg(tr + (size_t)(t + 2) * kLane);
+        int16_t& slot = (Ph == 2) ? xOdd : xEven;      // phase 2 = odd frames
+        const int16_t x = slot;
+        if (t + 2 < F) slot = (int16_t)__ldg(tr + (size_t)(t + 2) * kLane);
         int16_t lo = 0, up = 0;
         const bool haveL = FeedFilter<FT, false, Ph>(x, mem, pc, lo);
         FeedFilter<FT, true, Ph>(x, mem, pc, up);
