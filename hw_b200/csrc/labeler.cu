@@ -181,6 +181,12 @@ __device__ __forceinline__ int TraceSource(uint32_t w, int state)
 
 constexpr int kBatch = 8;                              // frames loaded ahead
 
+// L1 prefetch of one address, no register result: used where the next loads
+// are needed sooner than one loop iteration can hide (the ROI pass spends ~30
+// instructions a frame) and for the traceback words read back in batches.
+__device__ __forceinline__ void PrefetchL1(const void* p) { asm volatile("prefetch.global.L1 [%0];" :: "l"(p)); }
+
+
 // Blocks per SM the labeler variants are compiled for (96 registers a thread).
 constexpr int LabelerMinBlocks(int threads) { return threads == 64 ? 10 : threads == 128 ? 5 : 2; }
 
@@ -238,6 +244,7 @@ __global__ void __launch_bounds__(Threads, LabelerMinBlocks(Threads)) LabelerKer
 #pragma unroll 2
             for (int i = 0; i < F; ++i)
             {
+                if (i + 8 < F) PrefetchL1(chunk + (size_t)(i + 8) * kLane);
                 const int16_t y = y0;
                 y0 = y1;
                 if (i + 2 < F) y1 = __ldg(chunk + (size_t)(i + 2) * kLane);
@@ -320,6 +327,7 @@ __global__ void __launch_bounds__(Threads, LabelerMinBlocks(Threads)) LabelerKer
 #pragma unroll
         for (int i = 0; i < kStates; ++i) prob[i] = mul_rn(prob[i], inv);
     }
+    for (int i = F + kLookback - 1; i > F - 1; --i) PrefetchL1(tb + (size_t)i * kLane);
     for (int i = F + kLookback - 1; i > F - 1; --i)
     {
         const uint32_t w = tb[(size_t)i * kLane];
@@ -360,6 +368,11 @@ __global__ void __launch_bounds__(Threads, LabelerMinBlocks(Threads)) LabelerKer
             uint32_t w[kBatch];
 #pragma unroll
             for (int j = 0; j < kBatch; ++j) w[j] = tb[(size_t)(f0 + j) * kLane];
+            if (f0 >= kBatch)
+            {
+#pragma unroll
+                for (int j = 0; j < kBatch; ++j) PrefetchL1(tb + (size_t)(f0 - kBatch + j) * kLane);
+            }
             uint32_t word = 0;
 #pragma unroll
             for (int j = kBatch - 1; j >= 0; --j)
@@ -401,6 +414,11 @@ __global__ void __launch_bounds__(Threads, LabelerMinBlocks(Threads)) LabelerKer
             uint32_t w[kBatch];
 #pragma unroll
             for (int j = 0; j < kBatch; ++j) w[j] = tb[(size_t)(f0 + j) * kLane];
+            if (f0 >= kBatch)
+            {
+#pragma unroll
+                for (int j = 0; j < kBatch; ++j) PrefetchL1(tb + (size_t)(f0 - kBatch + j) * kLane);
+            }
 #pragma unroll
             for (int j = kBatch - 1; j >= 0; --j)
             {
