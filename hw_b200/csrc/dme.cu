@@ -139,6 +139,9 @@ struct EmHist
     int z;
     float lb, binSize, varQuant, binProbMin, nSum;
     uint16_t inRange, nLowOut, total;
+    // occupied bins of the warp's ZMWs: every bin outside [wLo, wHi] is empty
+    // for all of them (wLo > wHi: no occupied bin)
+    int wLo, wHi;
     __device__ __forceinline__ float BinStart(int b) const { return add_rn(lb, mul_rn((float)b, binSize)); }
     __device__ __forceinline__ uint32_t Count(int b) const { return H->bin_count[b][z]; }
 };
@@ -149,12 +152,17 @@ __device__ __forceinline__ void LoadEmHist(const hw_lane_histogram& H, int z, Em
     h.z = z;
     uint16_t inRange = 0;
     float nSum = 0.0f;
+    int lo = kBins, hi = -1;
     for (int b = 0; b < kBins; ++b)
     {
         const uint16_t c = H.bin_count[b][z];
         inRange = (uint16_t)(inRange + c);
         nSum += (float)c;
+        lo = (c != 0 && b < lo) ? b : lo;
+        hi = (c != 0) ? b : hi;
     }
+    h.wLo = __reduce_min_sync(0xffffffffu, lo);
+    h.wHi = __reduce_max_sync(0xffffffffu, hi);
     h.inRange = inRange;
     h.nSum = nSum;
     h.nLowOut = H.outlier_count_low[z];
@@ -493,11 +501,23 @@ __device__ __forceinline__ void EmMStep(const KParams& k, const EmHist& h, const
     // loaded once, one bin ahead of its use.  Scratch slots of boundaries next
     // to empty bins hold stale values; they are loaded but only used for
     // occupied bins (or when !safe, where every boundary was written).
+    // Bins that are empty for every ZMW of the warp add +0 to every sum (see
+    // the E-step), so when all of the warp's ZMWs are `safe` the pass covers
+    // only the warp's occupied range.
     float mom2 = 0.0f;
     {
-        float bpj = bpS[z], t0j = tau0S[z];
-        uint32_t nj = h.Count(0);
-        for (int j = 0; j < kBins; ++j)
+        const bool narrow = __all_sync(0xffffffffu, safe);
+        const int j0 = narrow ? h.wLo : 0;
+        const int j1 = narrow ? h.wHi + 1 : kBins;
+        float bpj = 0.0f, t0j = 0.0f;
+        uint32_t nj = 0u;
+        if (j0 < j1)
+        {
+            bpj = bpS[(size_t)j0 * kLane + z];
+            t0j = tau0S[(size_t)j0 * kLane + z];
+            nj = h.Count(j0);
+        }
+        for (int j = j0; j < j1; ++j)
         {
             const float bpk = bpS[(size_t)(j + 1) * kLane + z], t0k = tau0S[(size_t)(j + 1) * kLane + z];
             const float fj = facS[(size_t)j * kLane + z];
