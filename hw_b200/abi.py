@@ -157,6 +157,20 @@ DME_DIAG_DT = np.dtype([("iter_count", np.int32, (LANE,)), ("converged", np.int3
                         ("confidence", np.float32, (LANE,)), ("lane_iterations", np.int32),
                         ("pad_", np.int32, (15,))])
 
+_L, _A = (LANE,), (NUM_ANALOGS, LANE)
+BASECALLING_METRICS_DT = np.dtype([
+    ("activity_label", np.uint8, _L), ("num_pulse_frames", np.uint16, _L), ("num_base_frames", np.uint16, _L),
+    ("num_sandwiches", np.uint16, _L), ("num_half_sandwiches", np.uint16, _L),
+    ("num_pulse_label_stutters", np.uint16, _L), ("num_bases", np.uint16, _L), ("num_pulses", np.uint16, _L),
+    ("pk_mid_signal", np.float32, _A), ("bp_zvar", np.float32, _A), ("pk_zvar", np.float32, _A),
+    ("pk_max", np.float32, _A), ("num_pk_mid_frames", np.uint16, _A), ("num_pk_mid_bases_by_analog", np.uint16, _A),
+    ("num_bases_by_analog", np.uint16, _A), ("num_pulses_by_analog", np.uint16, _A),
+    ("frame_baseline_dws", np.float32, _L), ("frame_baseline_variance_dws", np.float32, _L),
+    ("num_frames_baseline", np.uint16, _L), ("start_frame", np.uint32, _L), ("num_frames", np.uint16, _L),
+    ("autocorrelation", np.float32, _L), ("pulse_detection_score", np.float32, _L),
+    ("pixel_checksum", np.int16, _L)])
+HQRF_EMPTY, HQRF_SINGLE, HQRF_MULTI, HQRF_LOW = 0, 1, 2, 3
+
 # hw_pool_chunk: one pool's row of the hw_chunk_fused table (device pointers as integers)
 POOL_CHUNK_DT = np.dtype([("d_trace", np.uint64), ("d_trace8", np.uint64), ("d_pulses", np.uint64),
                           ("d_lens", np.uint64), ("d_overflows", np.uint64), ("first_frame", np.int32),
@@ -174,6 +188,7 @@ SIZES = {
     "hw_pulse": (PULSE_DT, 20),
     "hw_dme_diag": (DME_DIAG_DT, 1344),
     "hw_pool_chunk": (POOL_CHUNK_DT, 56),
+    "hw_basecalling_metrics": (BASECALLING_METRICS_DT, 8768),
     "hw_fused_tuning": (FUSED_TUNING_DT, 16),
 }
 

@@ -1031,6 +1031,23 @@ int hw_analyzer_models(const hw_analyzer* a, hw_lane_model* d_out, hw_frame_inte
     return HW_OK;
 }
 
+int hw_analyzer_chunk_metrics(const hw_analyzer* a, hw_baseliner_stats* d_baseliner_stats, float* d_viterbi_score,
+                              hw_stat_accum_state* d_pd_baseline_stats, void* stream)
+{
+    if (!a) return Fail(HW_ERR_INVALID_ARG, "NULL analyzer");
+    cudaStream_t s = S(stream);
+    if (d_baseliner_stats)
+        HW_CUDA(cudaMemcpyAsync(d_baseliner_stats, a->stats, sizeof(hw_baseliner_stats) * a->lanes,
+                                cudaMemcpyDeviceToDevice, s), "hw_analyzer_chunk_metrics");
+    if (d_viterbi_score)
+        HW_CUDA(cudaMemcpyAsync(d_viterbi_score, a->score, sizeof(float) * a->lanes * kLane, cudaMemcpyDeviceToDevice, s),
+                "hw_analyzer_chunk_metrics");
+    if (d_pd_baseline_stats)
+        HW_CUDA(cudaMemcpyAsync(d_pd_baseline_stats, a->paStats, sizeof(hw_stat_accum_state) * a->lanes,
+                                cudaMemcpyDeviceToDevice, s), "hw_analyzer_chunk_metrics");
+    return HW_OK;
+}
+
 int hw_analyzer_last_diag(const hw_analyzer* a, hw_dme_diag* d_out, int32_t* valid, void* stream)
 {
     if (!a || !d_out) return Fail(HW_ERR_INVALID_ARG, "NULL argument");

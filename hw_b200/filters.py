@@ -280,6 +280,15 @@ class BatchAnalyzer(_Handle):
         check(lib().hw_analyzer_models(self._h, _p(out), C.byref(fi), _stream()))
         return out, fi.tuple()
 
+    def chunk_metrics(self):
+        """(baseliner stats, Viterbi scores [lanes][64], pulse-detector baseline
+        stats) of the last chunk, as device buffers."""
+        bs = struct_buffer(abi.BLSTATS_DT, self.lanes)
+        vs = torch.empty((self.lanes, abi.LANE), dtype=torch.float32, device="cuda")
+        pd = struct_buffer(abi.STAT_ACCUM_DT, self.lanes)
+        check(lib().hw_analyzer_chunk_metrics(self._h, _p(bs), _p(vs), _p(pd), _stream()))
+        return bs, vs, pd
+
     def last_diag(self):
         out = struct_buffer(abi.DME_DIAG_DT, self.lanes)
         valid = C.c_int32()
@@ -455,6 +464,41 @@ class FusedEngine(_Handle):
         a, b = C.c_uint32(), C.c_uint32()
         check(lib().hw_fused_last_step(self._h, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+
+class HfMetrics(_Handle):
+    """HFMetricsFilter of one pool (hw_hfmetrics)."""
+    _destroy = "hw_hfmetrics_destroy"
+
+    def __init__(self, lanes, frames_per_block=4096, frame_rate=100.0, realtime_activity_labels=True, cart=None):
+        super().__init__()
+        self.lanes = lanes
+        check(lib().hw_hfmetrics_create(lanes, frames_per_block, float(frame_rate),
+                                        1 if realtime_activity_labels else 0, C.byref(self._h)))
+        self.out = struct_buffer(abi.BASECALLING_METRICS_DT, lanes)
+        if cart is not None:
+            self.set_cart(cart)
+
+    def set_cart(self, cart):
+        # converted copies held in locals until the call returns
+        left = np.ascontiguousarray(cart["children_left"], np.int16)
+        right = np.ascontiguousarray(cart["children_right"], np.int16)
+        feature = np.ascontiguousarray(cart["feature"], np.int8)
+        thr = np.ascontiguousarray(cart["threshold"], np.float32)
+        value = np.ascontiguousarray(cart["value"], np.int8)
+        hsw = np.ascontiguousarray(cart["hsw_curve"], np.float32)
+        check(lib().hw_hfmetrics_set_cart(self._h, abi.ptr(left), abi.ptr(right), abi.ptr(feature), abi.ptr(thr),
+                                          abi.ptr(value), len(left), abi.ptr(hsw),
+                                          float(np.asarray(cart["max_acceptable_halfsandwich_rate"]).reshape(-1)[0])))
+
+    def process(self, pulses, lens, cap, baseliner_stats, models, viterbi, pd_stats, first_frame, frames):
+        """One pulse batch (device buffers).  Returns the block's metrics
+        (device uint8 buffer of BASECALLING_METRICS_DT records) or None."""
+        em = C.c_int32()
+        check(lib().hw_hfmetrics_process(self._h, _p(pulses), _p(lens), int(cap), _p(baseliner_stats), _p(models),
+                                         _p(viterbi), _p(pd_stats), int(first_frame), int(frames), _p(self.out),
+                                         C.byref(em), _stream()))
+        return self.out if em.value else None
 
 
 class _DeviceBytes:

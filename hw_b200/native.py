@@ -76,6 +76,11 @@ def lib():
         "hw_fused_models": ([vp, u32, vp, C.POINTER(FI), vp], C.c_int),
         "hw_fused_last_step": ([vp, C.POINTER(u32), C.POINTER(u32)], C.c_int),
         "hw_fused_profile": ([vp, i32], C.c_int),
+        "hw_analyzer_chunk_metrics": ([vp, vp, vp, vp, vp], C.c_int),
+        "hw_hfmetrics_create": ([u32, u32, C.c_double, i32, PPV], C.c_int),
+        "hw_hfmetrics_destroy": ([vp], C.c_int),
+        "hw_hfmetrics_set_cart": ([vp, vp, vp, vp, vp, vp, u32, vp, C.c_float], C.c_int),
+        "hw_hfmetrics_process": ([vp, vp, vp, u32, vp, vp, vp, vp, i32, u32, vp, C.POINTER(i32), vp], C.c_int),
         "hw_fused_stage_times": ([vp, vp, vp], C.c_int),
         "hw_analyzer_state_size": ([vp, C.POINTER(C.c_uint64)], C.c_int),
         "hw_analyzer_state_export": ([vp, vp, C.c_uint64, vp], C.c_int),

@@ -486,6 +486,71 @@ int hw_analyzer_state_size(const hw_analyzer* a, uint64_t* bytes);
 int hw_analyzer_state_export(const hw_analyzer* a, void* host_blob, uint64_t bytes, void* stream);
 int hw_analyzer_state_import(hw_analyzer* a, const void* host_blob, uint64_t bytes, void* stream);
 
+/* ---- HF metrics (HFMetricsFilter) -------------------------------------------
+ * Replaces HFMetricsFilterHost / HFMetricsFilterDevice
+ * (traceAnalysis/HFMetricsFilter.h:43-105, HFMetricsFilterHost.cpp:40-121,
+ * dataTypes/BasecallingMetricsAccumulator.cpp:40-504): per ZMW, pulse and
+ * trace metrics accumulated over blocks of frames_per_block frames and
+ * emitted once a block is complete.
+ *
+ * hw_basecalling_metrics has the layout of Data::BasecallingMetrics
+ * (dataTypes/BasecallingMetrics.h:47-86, 137 bytes per ZMW). */
+typedef struct hw_basecalling_metrics {
+    uint8_t  activity_label[HW_LANE_SIZE];          /* HQRFPhysicalStates: 0 EMPTY, 1 SINGLE, 2 MULTI, 3 LOW */
+    uint16_t num_pulse_frames[HW_LANE_SIZE];
+    uint16_t num_base_frames[HW_LANE_SIZE];
+    uint16_t num_sandwiches[HW_LANE_SIZE];
+    uint16_t num_half_sandwiches[HW_LANE_SIZE];
+    uint16_t num_pulse_label_stutters[HW_LANE_SIZE];
+    uint16_t num_bases[HW_LANE_SIZE];
+    uint16_t num_pulses[HW_LANE_SIZE];
+    float    pk_mid_signal[HW_NUM_ANALOGS][HW_LANE_SIZE];
+    float    bp_zvar[HW_NUM_ANALOGS][HW_LANE_SIZE];
+    float    pk_zvar[HW_NUM_ANALOGS][HW_LANE_SIZE];
+    float    pk_max[HW_NUM_ANALOGS][HW_LANE_SIZE];
+    uint16_t num_pk_mid_frames[HW_NUM_ANALOGS][HW_LANE_SIZE];
+    uint16_t num_pk_mid_bases_by_analog[HW_NUM_ANALOGS][HW_LANE_SIZE];
+    uint16_t num_bases_by_analog[HW_NUM_ANALOGS][HW_LANE_SIZE];
+    uint16_t num_pulses_by_analog[HW_NUM_ANALOGS][HW_LANE_SIZE];
+    float    frame_baseline_dws[HW_LANE_SIZE];
+    float    frame_baseline_variance_dws[HW_LANE_SIZE];
+    uint16_t num_frames_baseline[HW_LANE_SIZE];
+    uint32_t start_frame[HW_LANE_SIZE];
+    uint16_t num_frames[HW_LANE_SIZE];
+    float    autocorrelation[HW_LANE_SIZE];
+    float    pulse_detection_score[HW_LANE_SIZE];
+    int16_t  pixel_checksum[HW_LANE_SIZE];
+} hw_basecalling_metrics;
+
+typedef struct hw_hfmetrics hw_hfmetrics;
+/* HFMetricsFilter::Configure(sandwichTolerance, framesPerHFMetricBlock,
+ * frameRate, realtimeActivityLabels) + a filter for one pool of `lanes`
+ * lanes.  Activity labels need the trained classifier (hw_hfmetrics_set_cart);
+ * until one is set they stay EMPTY, as with realtimeActivityLabels false. */
+int hw_hfmetrics_create(uint32_t lanes, uint32_t frames_per_block, double frame_rate,
+                        int32_t realtime_activity_labels, hw_hfmetrics** out);
+int hw_hfmetrics_destroy(hw_hfmetrics* h);
+/* The activity labeler's trained CART (ActivityLabeler::TrainedCart,
+ * dataTypes/TrainedCartParams.h:44-53): n_nodes nodes (children, feature
+ * index -- negative at a leaf --, threshold, leaf value), the half-sandwich
+ * rate curve (2 coefficients, highest degree first) and its cap.  Host
+ * arrays; copied. */
+int hw_hfmetrics_set_cart(hw_hfmetrics* h, const int16_t* children_left, const int16_t* children_right,
+                          const int8_t* feature, const float* threshold, const int8_t* value, uint32_t n_nodes,
+                          const float hsw_curve[2], float max_acceptable_halfsandwich_rate);
+/* HFMetricsFilter::operator() for one pulse batch of the pool: pulses
+ * [lanes][64][max_calls] with counts d_lens [lanes][64]; the chunk's
+ * baseliner metrics, models, frame-labeler Viterbi scores [lanes][64] and
+ * pulse-detector baseline statistics [lanes]; first_frame and frames of the
+ * pulse batch.  When the batch completes a block (last frame % block <
+ * frames), the block's metrics go to d_out[lanes] and *emitted = 1; otherwise
+ * d_out is untouched and *emitted = 0. */
+int hw_hfmetrics_process(hw_hfmetrics* h, const hw_pulse* d_pulses, const uint32_t* d_lens, uint32_t max_calls,
+                         const hw_baseliner_stats* d_baseliner_stats, const hw_lane_model* d_models,
+                         const float* d_viterbi_score, const hw_stat_accum_state* d_pd_baseline_stats,
+                         int32_t first_frame, uint32_t frames, hw_basecalling_metrics* d_out, int32_t* emitted,
+                         void* stream);
+
 /* ---- Pool sets: uneven pools --------------------------
  * No single reference counterpart: the reference runs one BatchAnalyzer per
  * pool.  A pool set owns n_pools pools of any lane counts and chunk lengths
@@ -592,6 +657,13 @@ int hw_analyzer_process_u8(hw_analyzer* a, const uint8_t* d_trace, int32_t first
                            void* stream);
 /* Current detection models of the pool and their frame interval. */
 int hw_analyzer_models(const hw_analyzer* a, hw_lane_model* d_out, hw_frame_interval* fi, void* stream);
+/* The last chunk's BaselinerMetrics (per-chunk baseliner statistics),
+ * FrameLabelerMetrics::viterbiScore [lanes][64] and
+ * PulseDetectorMetrics::baselineStats [lanes] -- the inputs of the HF metrics
+ * filter (hw_hfmetrics_process).  Valid after a chunk that ran the labeler;
+ * any pointer may be NULL. */
+int hw_analyzer_chunk_metrics(const hw_analyzer* a, hw_baseliner_stats* d_baseliner_stats, float* d_viterbi_score,
+                              hw_stat_accum_state* d_pd_baseline_stats, void* stream);
 /* Diagnostics of the most recent DME estimate (*valid = 0 if none yet). */
 int hw_analyzer_last_diag(const hw_analyzer* a, hw_dme_diag* d_out, int32_t* valid, void* stream);
 

@@ -1981,3 +1981,471 @@ uint16_t or_f32_to_f16(float x) { return f32_to_f16_bits(x); }
 int16_t or_to_i16(float x) { return to_i16_wrap(x); }
 
 }   // extern "C"
+
+// ===========================================================================
+// HF metrics: TA/HFMetricsFilterHost.cpp:40-121,
+// DT/BasecallingMetricsAccumulator.cpp:40-504, DT/TraceAnalysisMetrics.h:48-200,
+// CM/StatAccumulator.h:80-252 (offset-aware), CM/AutocorrAccumulator.cpp:42-67.
+// Lane-wide all()/any() conditions of the SIMD code are evaluated over the
+// 64 ZMWs of the lane, as the LaneArray code does.
+
+namespace {
+
+// StatAccumulator with a live offset (the trace metrics' baseline accumulator).
+struct HfStat
+{
+    float off[kLane], m0[kLane], m1[kLane], m2[kLane];
+    void Zero() { FZ { off[z] = 0; m0[z] = 0; m1[z] = 0; m2[z] = 0; } }
+    void ResetMoments() { FZ { m0[z] = 0; m1[z] = 0; m2[z] = 0; } }     // Reset(): offset kept
+    float Mean(int z) const { return m1[z] / m0[z] + off[z]; }
+    float Variance(int z) const
+    {
+        float var = m1[z] * m1[z] / m0[z];
+        var = (m2[z] - var) / (m0[z] - 1.0f);
+        var = fmax_sse(var, 0.0f);
+        return (m0[z] > 1.0f) ? var : kNaN;
+    }
+    // Offset(value), :234-246
+    void SetOffset(const float* value)
+    {
+        bool same = true;
+        FZ same &= (value[z] == off[z]);
+        if (same) return;
+        FZ
+        {
+            const float m1new = m1[z] + m0[z] * (off[z] - value[z]);
+            const float m2new = m2[z] + (m1new * m1new - m1[z] * m1[z]) / m0[z];
+            off[z] = value[z];
+            m1[z] = m1new;
+            m2[z] = (m0[z] == 0.0f) ? 0.0f : m2new;
+        }
+    }
+    // operator+=(StatAccumulator other), :144-166
+    void PlusEq(HfStat other)
+    {
+        bool allEmpty = true;
+        FZ allEmpty &= (other.m0[z] == 0.0f);
+        if (allEmpty) return;
+        bool anyNan = false;
+        FZ anyNan |= std::isnan(off[z]);
+        if (anyNan)
+        {
+            FZ if (std::isnan(off[z])) { m0[z] = 0; m1[z] = 0; m2[z] = 0; }
+            FZ off[z] = std::isnan(off[z]) ? 0.0f : off[z];
+        }
+        float offNew[kLane];
+        FZ
+        {
+            const float w = other.m0[z] / (m0[z] + other.m0[z]);
+            const float o = (1.0f - w) * off[z] + w * other.off[z];
+            offNew[z] = std::isnan(o) ? off[z] : o;
+        }
+        other.SetOffset(offNew);
+        SetOffset(offNew);
+        FZ { m0[z] += other.m0[z]; m1[z] += other.m1[z]; m2[z] += other.m2[z]; }
+    }
+};
+
+// AutocorrAccumulator::Autocorrelation, AutocorrAccumulator.cpp:42-67
+float Autocorrelation(const AutocorrAcc& a, int z)
+{
+    const float nmk = a.stats.m0[z] - 4.0f;
+    const float mu = a.stats.Mean(z) - a.stats.off[z];
+    float m1x2 = 2.0f * a.stats.m1[z];
+    for (int k = 0; k < 4; ++k) m1x2 -= a.fBuf[k][z] + a.bBuf[k][z];
+    float ac = mu * (m1x2 - nmk * mu);
+    ac = (a.m2[z] - ac) / ((nmk - 1.0f) * a.stats.Variance(z));
+    ac = fmin_sse(fmax_sse(ac, -1.0f), 1.0f);
+    return ((nmk < 1.0f) | std::isnan(ac)) ? kNaN : ac;
+}
+
+struct HfCart
+{
+    std::vector<int16_t> left, right;
+    std::vector<int8_t> feature, value;
+    std::vector<float> thr;
+    float hsw[2] = {0, 0};
+    float maxHsw = 0;
+};
+
+constexpr uint8_t kNoneLabel = 5;     // Pulse::NucleotideLabel::NONE
+
+// One lane's BasecallingMetricsAccumulator.
+struct HfLane
+{
+    uint16_t pulseFrames[kLane], baseFrames[kLane], sandwiches[kLane], halfSandwiches[kLane], stutters[kLane];
+    uint8_t activity[kLane];
+    float pkMid[4][kLane], bpZvar[4][kLane], pkZvar[4][kLane], pkMax[4][kLane];
+    float modelVar[4][kLane], modelMean[4][kLane];
+    uint16_t pkMidFrames[4][kLane], pkMidBases[4][kLane], basesBy[4][kLane], pulsesBy[4][kLane];
+    // TraceAnalysisMetrics
+    uint32_t startFrame[kLane], numFrames[kLane];
+    int16_t pixelChecksum[kLane];
+    float pdScore[kLane];
+    HfStat blStat;
+    AutocorrAcc corr;
+    hw_pulse prev[kLane], prevprev[kLane];
+
+    void Init()
+    {
+        FZ { startFrame[z] = 0; numFrames[z] = 0; pixelChecksum[z] = 0; }
+        blStat.Zero();
+        corr.Reset();
+        Reset();
+    }
+    // BasecallingMetricsAccumulator::Reset, :249-272 + TraceAnalysisMetrics::Reset
+    void Reset()
+    {
+        FZ
+        {
+            pulseFrames[z] = 0; baseFrames[z] = 0; sandwiches[z] = 0; halfSandwiches[z] = 0; stutters[z] = 0;
+            hw_pulse none{};
+            none.label = kNoneLabel;
+            prev[z] = none;
+            prevprev[z] = none;
+            activity[z] = 0;
+            for (int a = 0; a < 4; ++a)
+            {
+                pkMid[a][z] = 0; bpZvar[a][z] = 0; pkZvar[a][z] = 0; pkMax[a][z] = 0;
+                pkMidFrames[a][z] = 0; pkMidBases[a][z] = 0; basesBy[a][z] = 0; pulsesBy[a][z] = 0;
+            }
+        }
+        blStat.ResetMoments();
+        {
+            // AutocorrAccumulator::Reset keeps the offset
+            float off[kLane];
+            FZ off[z] = corr.stats.off[z];
+            corr.Reset();
+            FZ corr.stats.off[z] = off[z];
+        }
+        FZ { startFrame[z] = startFrame[z] + numFrames[z]; numFrames[z] = 0; pdScore[z] = 0.0f; }
+    }
+
+    static float MidSignal(const hw_pulse& p) { return p.width < 3 ? kNaN : (float)p.mid_signal * 0.1f; }
+    static float SignalM2(const hw_pulse& p) { return p.width < 3 ? kNaN : p.signal_m2; }
+
+    // Count, :348-412
+    void Count(const hw_pulse* pulses, const uint32_t* lens, uint32_t cap, uint32_t frames)
+    {
+        FZ numFrames[z] += frames;
+        FZ
+        {
+            const hw_pulse* pp = &prev[z];
+            const hw_pulse* ppp = &prevprev[z];
+            const hw_pulse* row = pulses + (size_t)z * cap;
+            for (uint32_t bi = 0; bi < lens[z]; ++bi)
+            {
+                const hw_pulse* p = &row[bi];
+                const uint8_t lb = p->label;
+                pulseFrames[z] = (uint16_t)(pulseFrames[z] + p->width);
+                pulsesBy[lb][z]++;
+                pkMax[lb][z] = std::max(pkMax[lb][z], (float)p->max_signal * 0.1f);
+                if (pp->label != kNoneLabel)
+                {
+                    if (pp->label == lb) stutters[z]++;
+                    const bool abutted = p->start == pp->start + pp->width;
+                    if (abutted && pp->label != lb) halfSandwiches[z]++;
+                    if (ppp->label != kNoneLabel)
+                    {
+                        const bool prevAbutted = pp->start == ppp->start + ppp->width;
+                        if (prevAbutted && abutted && ppp->label == lb && ppp->label != pp->label) sandwiches[z]++;
+                    }
+                }
+                if (!p->is_reject)
+                {
+                    baseFrames[z] = (uint16_t)(baseFrames[z] + p->width);
+                    basesBy[lb][z]++;
+                    if (!std::isnan(MidSignal(*p)))
+                    {
+                        pkMidBases[lb][z]++;
+                        const uint16_t midWidth = (uint16_t)(p->width - 2);
+                        pkMidFrames[lb][z] = (uint16_t)(pkMidFrames[lb][z] + midWidth);
+                        pkMid[lb][z] += MidSignal(*p) * midWidth;
+                        bpZvar[lb][z] += MidSignal(*p) * MidSignal(*p) * midWidth;
+                        pkZvar[lb][z] += SignalM2(*p);
+                    }
+                }
+                ppp = pp;
+                pp = p;
+            }
+            prev[z] = *pp;
+            prevprev[z] = *ppp;
+        }
+    }
+
+    // AddModels, :311-322
+    void AddModels(const hw_lane_model& m)
+    {
+        for (int a = 0; a < 4; ++a)
+            FZ { modelVar[a][z] = hwm::f16_bits_to_f32(m.analogs[a].vars[z]); modelMean[a][z] = hwm::f16_bits_to_f32(m.analogs[a].means[z]); }
+    }
+
+    // AddBatchMetrics, :324-340
+    void AddBatchMetrics(const hw_baseliner_stats& bs, const float* viterbi, const hw_stat_accum_state& pd)
+    {
+        AutocorrAcc sub;
+        sub.Load(bs.full_autocorr);
+        corr.Merge(sub);
+        FZ pdScore[z] += viterbi[z];
+        HfStat p;
+        FZ { p.off[z] = pd.offset[z]; p.m0[z] = pd.moment0[z]; p.m1[z] = pd.moment1[z]; p.m2[z] = pd.moment2[z]; }
+        FZ
+        {
+            const float bgMean = bs.background_stats.moment1[z] / bs.background_stats.moment0[z]
+                               + bs.background_stats.offset[z];
+            p.off[z] += bgMean;
+        }
+        blStat.PlusEq(p);
+    }
+
+    uint16_t NumBases(int z) const
+    {
+        uint16_t r = 0;
+        for (int a = 0; a < 4; ++a) r = (uint16_t)(r + basesBy[a][z]);
+        return r;
+    }
+    uint16_t NumPulses(int z) const
+    {
+        uint16_t r = 0;
+        for (int a = 0; a < 4; ++a) r = (uint16_t)(r + pulsesBy[a][z]);
+        return r;
+    }
+
+    // FinalizeMetrics, :414-500
+    void Finalize(bool realtime, float frameRate, const HfCart* cart)
+    {
+        for (int a = 0; a < 4; ++a)
+        {
+            bool allZero = true, allFewBases = true, allFewFrames = true;
+            FZ
+            {
+                allZero &= ((int16_t)pkMidBases[a][z] == 0);
+                allFewBases &= ((float)pkMidBases[a][z] < 2.0f);
+                allFewFrames &= ((float)pkMidFrames[a][z] < 2.0f);
+            }
+            if (allZero)
+            {
+                FZ { pkMid[a][z] = kNaN; bpZvar[a][z] = kNaN; pkZvar[a][z] = kNaN; }
+            }
+            else if (allFewBases || allFewFrames)
+            {
+                FZ { bpZvar[a][z] = kNaN; pkZvar[a][z] = kNaN; }
+            }
+            else
+            {
+                FZ
+                {
+                    float bp = bpZvar[a][z], pk = pkZvar[a][z], mid = pkMid[a][z];
+                    const float nf = (float)pkMidFrames[a][z];
+                    const float nb = (float)pkMidBases[a][z];
+                    bp = (bp - (mid * mid / nf)) / nf;
+                    bp = bp * nb / (nb - 1.0f);
+                    const float blVar = blStat.Variance(z);
+                    bp -= blVar / (nf / nb);
+                    pk = (pk - (mid * mid / nf)) / (nf - 1.0f);
+                    pk -= bp + blVar;
+                    const float mv = modelVar[a][z];
+                    bool mask = mv < blVar;
+                    pk /= mv - blVar;
+                    mask |= pk < 0.0f;
+                    pk = mask ? 0.0f : pk;
+                    const float pkm = mid / nf;
+                    mask = pkm < 0.0f;
+                    bp /= (pkm * pkm);
+                    mask |= bp < 0.0f;
+                    bp = mask ? kNaN : bp;
+                    const int16_t nbi = (int16_t)pkMidBases[a][z];
+                    bool m2 = nbi == 0;
+                    mid = m2 ? kNaN : mid;
+                    m2 |= nbi < 2;
+                    m2 |= (int16_t)pkMidFrames[a][z] < 2;
+                    bp = m2 ? kNaN : bp;
+                    pk = m2 ? kNaN : pk;
+                    pkMid[a][z] = mid; bpZvar[a][z] = bp; pkZvar[a][z] = pk;
+                }
+            }
+        }
+        FZ
+        {
+            float s = pdScore[z] / (float)numFrames[z];
+            pdScore[z] = std::isnan(s) ? 0.0f : s;
+        }
+        if (realtime && cart) LabelBlock(frameRate, *cart);
+    }
+
+    // LabelBlock, :65-201
+    void LabelBlock(float frameRate, const HfCart& cart)
+    {
+        FZ
+        {
+            float f[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+            const float stdDev = std::sqrt(blStat.Variance(z));
+            const float nBases = (float)NumBases(z);
+            const float nPulses = (float)NumPulses(z);
+            float pw = (float)pulseFrames[z] / nPulses;
+            pw = std::isnan(pw) ? 0.0f : pw;
+            float pkmid[4];
+            for (int a = 0; a < 4; ++a) pkmid[a] = pkMid[a][z] / (float)pkMidFrames[a][z];
+            const float seconds = (float)numFrames[z] / frameRate;
+            f[0] = nPulses / seconds;
+            f[1] = (float)sandwiches[z] / nPulses;
+            f[1] = std::isnan(f[1]) ? 0.0f : f[1];
+            float hswr = (float)halfSandwiches[z] / nPulses;
+            hswr = std::isnan(hswr) ? 0.0f : hswr;
+            float hswrExp = cart.hsw[0];
+            hswrExp = hswrExp * f[0] + cart.hsw[1];
+            hswrExp = (hswrExp > cart.maxHsw) ? cart.maxHsw : hswrExp;
+            f[2] = hswr - hswrExp;
+            f[3] = pdScore[z];
+            f[4] = pw;
+            f[5] = (float)stutters[z] / nPulses;
+            f[5] = std::isnan(f[5]) ? 0.0f : f[5];
+            float rel[4];
+            for (int a = 0; a < 4; ++a) rel[a] = modelMean[a][z];
+            float maxamp = rel[0];
+            for (int a = 1; a < 4; ++a) maxamp = fmax_sse(rel[a], maxamp);
+            for (int a = 0; a < 4; ++a) rel[a] /= maxamp;
+            unsigned lowIdx = 0;
+            float minamp = rel[0];
+            for (int a = 1; a < 4; ++a)
+            {
+                lowIdx = (rel[a] < minamp) ? (unsigned)a : lowIdx;
+                minamp = fmin_sse(rel[a], minamp);
+            }
+            for (int a = 0; a < 4; ++a)
+                f[6] += pkmid[a] / stdDev * (float)basesBy[a][z] / nBases * minamp / rel[a];
+            f[6] = std::isnan(f[6]) ? 0.0f : f[6];
+            for (int a = 0; a < 4; ++a) f[7] = fmax_sse(f[7], (pkMax[a][z] - pkmid[a]) / stdDev);
+            f[7] = std::isnan(f[7]) ? 0.0f : f[7];
+            f[8] = Autocorrelation(corr, z);
+            for (int a = 0; a < 4; ++a)
+            {
+                float t = bpZvar[a][z];
+                f[9] += (std::isnan(t) | (lowIdx == (unsigned)a)) ? 0.0f : t;
+                t = pkZvar[a][z];
+                f[10] += (std::isnan(t) | (lowIdx == (unsigned)a)) ? 0.0f : t;
+            }
+            f[9] /= 3.0f;
+            f[10] /= 3.0f;
+            size_t cur = 0;
+            while (cart.feature[cur] >= 0)
+                cur = (f[cart.feature[cur]] <= cart.thr[cur]) ? (size_t)cart.left[cur] : (size_t)cart.right[cur];
+            activity[z] = (uint8_t)cart.value[cur];
+        }
+    }
+
+    // PopulateBasecallingMetrics, :203-247
+    void Populate(hw_basecalling_metrics& m) const
+    {
+        FZ
+        {
+            float ac = Autocorrelation(corr, z);
+            ac = std::isnan(ac) ? 0.0f : ac;
+            m.activity_label[z] = activity[z];
+            m.num_pulse_frames[z] = pulseFrames[z];
+            m.num_base_frames[z] = baseFrames[z];
+            m.num_sandwiches[z] = sandwiches[z];
+            m.num_half_sandwiches[z] = halfSandwiches[z];
+            m.num_pulse_label_stutters[z] = stutters[z];
+            m.num_bases[z] = NumBases(z);
+            m.num_pulses[z] = NumPulses(z);
+            for (int a = 0; a < 4; ++a)
+            {
+                m.pk_mid_signal[a][z] = pkMid[a][z];
+                m.bp_zvar[a][z] = bpZvar[a][z];
+                m.pk_zvar[a][z] = pkZvar[a][z];
+                m.pk_max[a][z] = pkMax[a][z];
+                m.num_pk_mid_frames[a][z] = pkMidFrames[a][z];
+                m.num_pk_mid_bases_by_analog[a][z] = pkMidBases[a][z];
+                m.num_bases_by_analog[a][z] = basesBy[a][z];
+                m.num_pulses_by_analog[a][z] = pulsesBy[a][z];
+            }
+            m.frame_baseline_dws[z] = blStat.Mean(z);
+            m.frame_baseline_variance_dws[z] = blStat.Variance(z);
+            m.num_frames_baseline[z] = (uint16_t)blStat.m0[z];
+            m.start_frame[z] = startFrame[z];
+            m.num_frames[z] = (uint16_t)numFrames[z];
+            m.autocorrelation[z] = ac;
+            m.pulse_detection_score[z] = pdScore[z];
+            m.pixel_checksum[z] = pixelChecksum[z];
+        }
+    }
+};
+
+// HFMetricsFilterHost for one pool
+struct OracleHf
+{
+    std::vector<HfLane> lanes;
+    uint32_t block = 4096, framesSeen = 0;
+    float frameRate = 100.0f;
+    bool realtime = true;
+    bool haveCart = false;
+    HfCart cart;
+};
+
+}   // namespace
+
+extern "C" {
+
+void* or_hf_create(uint32_t lanes, uint32_t framesPerBlock, double frameRate, int32_t realtime)
+{
+    auto* h = new OracleHf;
+    h->lanes.resize(lanes);
+    for (auto& l : h->lanes) l.Init();
+    h->block = framesPerBlock;
+    h->frameRate = (float)frameRate;
+    h->realtime = realtime != 0;
+    return h;
+}
+
+void or_hf_destroy(void* p) { delete static_cast<OracleHf*>(p); }
+
+int or_hf_set_cart(void* p, const int16_t* left, const int16_t* right, const int8_t* feature, const float* thr,
+                   const int8_t* value, uint32_t n, const float* hsw, float maxHsw)
+{
+    auto* h = static_cast<OracleHf*>(p);
+    h->cart.left.assign(left, left + n);
+    h->cart.right.assign(right, right + n);
+    h->cart.feature.assign(feature, feature + n);
+    h->cart.thr.assign(thr, thr + n);
+    h->cart.value.assign(value, value + n);
+    h->cart.hsw[0] = hsw[0];
+    h->cart.hsw[1] = hsw[1];
+    h->cart.maxHsw = maxHsw;
+    h->haveCart = true;
+    return HW_OK;
+}
+
+// HFMetricsFilterHost::Process, :80-118
+int or_hf_process(void* p, const hw_pulse* pulses, const uint32_t* lens, uint32_t cap, const hw_baseliner_stats* bs,
+                  const hw_lane_model* models, const float* viterbi, const hw_stat_accum_state* pd,
+                  int32_t firstFrame, uint32_t frames, hw_basecalling_metrics* out, int32_t* emitted)
+{
+    auto* h = static_cast<OracleHf*>(p);
+    const size_t L = h->lanes.size();
+    if (h->framesSeen == 0)
+        for (auto& l : h->lanes) l.Reset();
+    for (size_t l = 0; l < L; ++l)
+    {
+        HfLane& m = h->lanes[l];
+        m.Count(pulses + l * kLane * cap, lens + l * kLane, cap, frames);
+        m.AddModels(models[l]);
+        m.AddBatchMetrics(bs[l], viterbi + l * kLane, pd[l]);
+    }
+    h->framesSeen += frames;
+    const uint32_t last = (uint32_t)(firstFrame + (int32_t)frames);
+    *emitted = 0;
+    if (last % h->block < frames)
+    {
+        for (size_t l = 0; l < L; ++l)
+        {
+            h->lanes[l].Finalize(h->realtime, h->frameRate, h->haveCart ? &h->cart : nullptr);
+            h->lanes[l].Populate(out[l]);
+        }
+        h->framesSeen = 0;
+        *emitted = 1;
+    }
+    return HW_OK;
+}
+
+}   // extern "C"

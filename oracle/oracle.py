@@ -63,6 +63,11 @@ def lib():
         L.or_f32_to_f16.restype = C.c_uint16
         L.or_to_i16.argtypes = [C.c_float]
         L.or_to_i16.restype = C.c_int16
+        L.or_hf_create.argtypes = [u32, u32, C.c_double, i32]
+        L.or_hf_create.restype = vp
+        L.or_hf_destroy.argtypes = [vp]
+        L.or_hf_set_cart.argtypes = [vp, vp, vp, vp, vp, vp, u32, vp, C.c_float]
+        L.or_hf_process.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp, i32, u32, vp, C.POINTER(i32)]
         _lib = L
     return _lib
 
@@ -195,8 +200,10 @@ class Pool:
         lens = np.zeros((self.lanes, abi.LANE), np.uint32)
         ovf = np.zeros((self.lanes, abi.LANE), np.uint32)
         bls = np.zeros(self.lanes, abi.STAT_ACCUM_DT)
-        _check(lib().or_pulses(self.h, abi.ptr(np.ascontiguousarray(labels)), abi.ptr(np.ascontiguousarray(latent)),
-                               abi.ptr(np.ascontiguousarray(traces)), first_frame, abi.ptr(models),
+        labels, latent, traces = (np.ascontiguousarray(labels), np.ascontiguousarray(latent),
+                                  np.ascontiguousarray(traces))      # held until the call returns
+        _check(lib().or_pulses(self.h, abi.ptr(labels), abi.ptr(latent),
+                               abi.ptr(traces), first_frame, abi.ptr(models),
                                abi.ptr(pulses), abi.ptr(lens), abi.ptr(ovf), abi.ptr(bls)))
         return pulses, lens, ovf, bls
 
@@ -223,3 +230,43 @@ def static_model(cfg, lanes):
     one = np.zeros(1, abi.LANE_MODEL_DT)
     _check(lib().or_static_model(C.byref(cfg), abi.ptr(one)))
     return np.repeat(one, lanes)
+
+
+class HfMetrics:
+    """HFMetricsFilterHost of one pool (oracle)."""
+
+    def __init__(self, lanes, frames_per_block=4096, frame_rate=100.0, realtime_activity_labels=True):
+        self.lanes = lanes
+        self.h = lib().or_hf_create(lanes, frames_per_block, frame_rate, int(bool(realtime_activity_labels)))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_hf_destroy(self.h)
+            self.h = None
+
+    def set_cart(self, cart):
+        """cart: mapping with children_left/right, feature, threshold, value,
+        hsw_curve, max_acceptable_halfsandwich_rate (tests/golden/trained_cart.npz)."""
+        self._cart = {k: np.ascontiguousarray(cart[k]) for k in cart}
+        c = self._cart
+        _check(lib().or_hf_set_cart(self.h, abi.ptr(c["children_left"]), abi.ptr(c["children_right"]),
+                                    abi.ptr(c["feature"]), abi.ptr(c["threshold"]), abi.ptr(c["value"]),
+                                    len(c["children_left"]), abi.ptr(c["hsw_curve"]),
+                                    float(np.asarray(c["max_acceptable_halfsandwich_rate"]).reshape(-1)[0])))
+
+    def process(self, pulses, lens, baseliner_stats, models, viterbi, pd_stats, first_frame, frames):
+        """Returns the block's metrics (numpy BASECALLING_METRICS_DT [lanes]) or None."""
+        # converted copies held in locals until the call returns
+        pulses = np.ascontiguousarray(pulses)
+        lens = np.ascontiguousarray(lens, np.uint32)
+        baseliner_stats = np.ascontiguousarray(baseliner_stats)
+        models = np.ascontiguousarray(models)
+        viterbi = np.ascontiguousarray(viterbi, np.float32)
+        pd_stats = np.ascontiguousarray(pd_stats)
+        cap = pulses.shape[-1]
+        out = np.zeros(self.lanes, abi.BASECALLING_METRICS_DT)
+        em = C.c_int32()
+        _check(lib().or_hf_process(self.h, abi.ptr(pulses), abi.ptr(lens), cap, abi.ptr(baseliner_stats),
+                                   abi.ptr(models), abi.ptr(viterbi), abi.ptr(pd_stats), int(first_frame),
+                                   int(frames), abi.ptr(out), C.byref(em)))
+        return out if em.value else None

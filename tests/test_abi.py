@@ -50,6 +50,7 @@ int main(void) {
   S(hw_config) S(hw_analog) S(hw_stat_accum_state) S(hw_autocorr_accum_state) S(hw_baseliner_stats)
   S(hw_lane_analog_mode) S(hw_lane_model) S(hw_lane_histogram) S(hw_lane_hist_bounds) S(hw_pulse)
   S(hw_dme_diag) S(hw_frame_interval) S(hw_gen_params) S(hw_pool_chunk) S(hw_fused_tuning)
+  S(hw_basecalling_metrics)
   O(hw_baseliner_stats, full_autocorr) O(hw_baseliner_stats, trace_min) O(hw_baseliner_stats, trace_max)
   O(hw_baseliner_stats, baseline_stats) O(hw_baseliner_stats, raw_baseline_sum) O(hw_baseliner_stats, background_stats)
   O(hw_lane_model, analogs) O(hw_lane_model, baseline) O(hw_lane_model, confidence)
@@ -58,6 +59,10 @@ int main(void) {
   O(hw_dme_diag, lane_iterations)
   O(hw_pool_chunk, d_trace8) O(hw_pool_chunk, d_overflows) O(hw_pool_chunk, first_frame) O(hw_pool_chunk, estimated)
   O(hw_fused_tuning, labeler_lanes_per_cta)
+  O(hw_basecalling_metrics, num_pulse_frames) O(hw_basecalling_metrics, pk_mid_signal)
+  O(hw_basecalling_metrics, num_pk_mid_frames) O(hw_basecalling_metrics, frame_baseline_dws)
+  O(hw_basecalling_metrics, start_frame) O(hw_basecalling_metrics, autocorrelation)
+  O(hw_basecalling_metrics, pixel_checksum)
   O(hw_config, analogs) O(hw_config, filter_type) O(hw_config, max_calls_per_zmw) O(hw_config, xsp_amp_thresh)
   O(hw_config, model_estimation_mode) O(hw_config, static_baseline_variance)
   return 0;
@@ -100,7 +105,7 @@ def test_struct_offsets_match_python_mirrors(layout):
         dt = {"hw_baseliner_stats": abi.BLSTATS_DT, "hw_lane_model": abi.LANE_MODEL_DT,
               "hw_lane_histogram": abi.LANE_HIST_DT, "hw_pulse": abi.PULSE_DT,
               "hw_dme_diag": abi.DME_DIAG_DT, "hw_pool_chunk": abi.POOL_CHUNK_DT,
-              "hw_fused_tuning": abi.FUSED_TUNING_DT}[t]
+              "hw_fused_tuning": abi.FUSED_TUNING_DT, "hw_basecalling_metrics": abi.BASECALLING_METRICS_DT}[t]
         assert dt.fields[m][1] == off, key
 
 
