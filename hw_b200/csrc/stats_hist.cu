@@ -159,12 +159,24 @@ HistAddKernel(hw_lane_histogram* hist, EdgeState es, const int16_t* traces, int 
     auto cnt = reinterpret_cast<uint16_t (*)[kBins + 1][kLane]>(histSmem);
     const int ll = threadIdx.x / kLane, z = threadIdx.x % kLane;
     const int li = blockIdx.x * kHistLanesPerBlock + ll;
-    if (li >= map.Lanes(lanes)) return;    // whole lanes only: no block-wide sync below
+    static_assert(kHistLanesPerBlock == 1, "the block-wide copies below need one lane per block");
+    if (li >= map.Lanes(lanes)) return;    // the whole block (one lane) returns together
     const int l = map.Lane(li);
     if (map.On()) frames = map.Pool(l).F;
     const int g = l * kLane + z;
     hw_lane_histogram& H = hist[l];
-    for (int b = 0; b < kBins; ++b) cnt[ll][b][z] = H.bin_count[b][z];
+    // The lane's counts [300][64] u16 are one contiguous 38,400-byte block in
+    // global and in shared memory: every thread issues its share of 16-byte
+    // asynchronous copies, all in flight together, then the block waits once.
+    constexpr int kChunks = kBins * kLane * 2 / 16;
+    {
+        const char* src = reinterpret_cast<const char*>(&H.bin_count[0][0]);
+        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&cnt[ll][0][0]);
+        for (int c = threadIdx.x; c < kChunks; c += blockDim.x)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(dst + 16 * c), "l"(src + 16 * c));
+        asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+        __syncthreads();
+    }
     uint16_t nLow = H.outlier_count_low[z], nHigh = H.outlier_count_high[z];
     const float lower = H.low_bound[z], binSize = H.bin_size[z];
     const float bm = h2f(models[l].baseline.means[z]);
@@ -190,17 +202,39 @@ HistAddKernel(hw_lane_histogram* hist, EdgeState es, const int16_t* traces, int 
         if ((!sel) | mLow | mHigh) bin = kBins;
         cnt[ll][bin][z] = (uint16_t)(cnt[ll][bin][z] + 1);
     };
+    // Trace values in two register batches of 8 frames that alternate: batch
+    // A is refilled while batch B is binned and vice versa, so loads are a
+    // batch ahead and no register is copied while its load is in flight.
     int f = 0;
-    for (; f + kHistBatch <= frames; f += kHistBatch)
     {
-        int16_t x[kHistBatch];
+        int16_t xa[kHistBatch], xb[kHistBatch];
+        if (frames >= 2 * kHistBatch)
+        {
 #pragma unroll
-        for (int j = 0; j < kHistBatch; ++j) x[j] = __ldg(tr + (size_t)(f + j) * kLane);
+            for (int j = 0; j < kHistBatch; ++j) xa[j] = __ldg(tr + (size_t)j * kLane);
+        }
+        for (; f + 2 * kHistBatch <= frames; f += 2 * kHistBatch)
+        {
 #pragma unroll
-        for (int j = 0; j < kHistBatch; ++j) step(x[j]);
+            for (int j = 0; j < kHistBatch; ++j) xb[j] = __ldg(tr + (size_t)(f + kHistBatch + j) * kLane);
+#pragma unroll
+            for (int j = 0; j < kHistBatch; ++j) step(xa[j]);
+            if (f + 3 * kHistBatch <= frames)
+            {
+#pragma unroll
+                for (int j = 0; j < kHistBatch; ++j) xa[j] = __ldg(tr + (size_t)(f + 2 * kHistBatch + j) * kLane);
+            }
+#pragma unroll
+            for (int j = 0; j < kHistBatch; ++j) step(xb[j]);
+        }
     }
     for (; f < frames; ++f) step(__ldg(tr + (size_t)f * kLane));
-    for (int b = 0; b < kBins; ++b) H.bin_count[b][z] = cnt[ll][b][z];
+    __syncthreads();
+    {
+        uint4* dst = reinterpret_cast<uint4*>(&H.bin_count[0][0]);
+        const uint4* src = reinterpret_cast<const uint4*>(&cnt[ll][0][0]);
+        for (int c = threadIdx.x; c < kChunks; c += blockDim.x) dst[c] = src[c];
+    }
     H.outlier_count_low[z] = nLow;
     H.outlier_count_high[z] = nHigh;
     es.prev[g] = prev;
