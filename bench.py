@@ -38,7 +38,7 @@ FRAMES = 512
 LANES_PER_POOL = 4096
 POOLS = 4
 KERNELS_PER_STAGE = {"baseline": 1, "aggregate": 1, "histogram": 1, "model_init": 1, "dme": 1,
-                     "hist_reset": 2, "labeler": 2, "pulses": 1}
+                     "hist_reset": 2, "labeler": 2, "pulses": 1, "metrics": 1}
 
 
 def parse():
@@ -216,8 +216,13 @@ def main():
     lpp = args.lanes_per_pool
     stream = torch.cuda.current_stream()
     if args.engine == "fused":
-        # every pool in one engine: each stage is one launch over all lanes
+        # every pool in one engine: each stage is one launch over all lanes,
+        # HF metrics included (4096-frame blocks, the reference's trained
+        # activity classifier when its table is in the checkout)
         engine = Fl.FusedEngine(cfg, [lpp] * args.pools, [FRAMES] * args.pools)
+        cart_file = os.path.join(ROOT, "tests", "golden", "trained_cart.npz")
+        cart = dict(np.load(cart_file)) if os.path.exists(cart_file) else None
+        engine.enable_hf_metrics(4096, cfg.frame_rate, True, cart)
         profiled = [engine]
         outputs = [engine.outputs(p) for p in range(args.pools)]
         lanes_per_launch = total_lanes
@@ -318,6 +323,9 @@ def main():
         host_out = [(torch.empty(dp.numel(), dtype=torch.uint8, pin_memory=True),
                      torch.empty(dl.shape, dtype=torch.int32, pin_memory=True),
                      torch.empty(do.shape, dtype=torch.int32, pin_memory=True)) for dp, dl, do in outputs]
+        hf_host = ([torch.empty(m.numel(), dtype=torch.uint8, pin_memory=True) for m in engine.metrics]
+                   if args.engine == "fused" else [])
+        metrics_bytes = 0
         s_h2d, s_d2h = torch.cuda.Stream(), torch.cuda.Stream()
         ev_h2d = [torch.cuda.Event() for _ in range(2)]
         ev_comp = [torch.cuda.Event() for _ in range(2)]
@@ -345,6 +353,12 @@ def main():
                     hl.copy_(dl, non_blocking=True)
                     ho.copy_(do, non_blocking=True)
                     hp.copy_(dp, non_blocking=True)
+                if args.engine == "fused":
+                    # HF metrics records of the pools that completed a block
+                    for p, em in enumerate(engine.metrics_emitted()):
+                        if em:
+                            hf_host[p].copy_(engine.metrics[p], non_blocking=True)
+                            metrics_bytes += engine.metrics[p].numel()
                 ev_d2h[b].record(s_d2h)
         stream.wait_stream(s_d2h)
         e1.record(stream)
@@ -353,7 +367,7 @@ def main():
         ms_e2e = max_over_ranks(e0.elapsed_time(e1))
         c += KE
         h2d = total_lanes * FRAMES * 64 * 2
-        d2h = sum(dp.numel() + dl.numel() * 4 + do.numel() * 4 for dp, dl, do in outputs)
+        d2h = sum(dp.numel() + dl.numel() * 4 + do.numel() * 4 for dp, dl, do in outputs) + metrics_bytes // KE
         e2e = {"value": zf_step * KE * world / (ms_e2e / 1e3), "unit": "ZMW-frames/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / KE, "steps": KE,
                "overlap": "copies on their own streams, double-buffered against the analysis"}

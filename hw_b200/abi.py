@@ -173,8 +173,9 @@ HQRF_EMPTY, HQRF_SINGLE, HQRF_MULTI, HQRF_LOW = 0, 1, 2, 3
 
 # hw_pool_chunk: one pool's row of the hw_chunk_fused table (device pointers as integers)
 POOL_CHUNK_DT = np.dtype([("d_trace", np.uint64), ("d_trace8", np.uint64), ("d_pulses", np.uint64),
-                          ("d_lens", np.uint64), ("d_overflows", np.uint64), ("first_frame", np.int32),
-                          ("emitted", np.int32), ("estimated", np.int32), ("reserved", np.int32)])
+                          ("d_lens", np.uint64), ("d_overflows", np.uint64), ("d_metrics", np.uint64),
+                          ("first_frame", np.int32), ("emitted", np.int32), ("estimated", np.int32),
+                          ("metrics_emitted", np.int32)])
 FUSED_TUNING_DT = np.dtype([("frames_per_chunk", np.uint32), ("fuse_label_pulses", np.uint32),
                             ("labeler_lanes_per_cta", np.uint32), ("reserved", np.uint32)])
 
@@ -187,7 +188,7 @@ SIZES = {
     "hw_lane_hist_bounds": (HIST_BOUNDS_DT, 512),
     "hw_pulse": (PULSE_DT, 20),
     "hw_dme_diag": (DME_DIAG_DT, 1344),
-    "hw_pool_chunk": (POOL_CHUNK_DT, 56),
+    "hw_pool_chunk": (POOL_CHUNK_DT, 64),
     "hw_basecalling_metrics": (BASECALLING_METRICS_DT, 8768),
     "hw_fused_tuning": (FUSED_TUNING_DT, 16),
 }

@@ -69,6 +69,7 @@ enum List
     L_LP1,        // frame labeler + pulse accumulator in one kernel, 1/2/4 lanes a block
     L_LP2,
     L_LP4,
+    L_HF,         // HF metrics filter
     L_ZERO,       // pools that emit nothing this step
     kNumLists
 };
@@ -85,6 +86,7 @@ struct PoolRt
     bool initialized = false, fullEstimation = false, histInitialized = false, diagValid = false;
     int32_t blLatency = 0, poolDelay = 0, nextFrame = 0;
     hw_frame_interval modelFi{0, 0}, aggFi{0, 0}, histFi{0, 0};
+    uint32_t hfSeen = 0;      // HFMetricsFilter::framesSeen_
 };
 
 hw_frame_interval Merge(hw_frame_interval a, hw_frame_interval b)
@@ -167,6 +169,20 @@ struct hw_fused
     int16_t* segLabel = nullptr;
     int* err = nullptr;
 
+    // HF metrics filter (hw_fused_enable_hf_metrics)
+    bool hf = false;
+    uint32_t hfBlock = 4096;
+    float hfFrameRate = 100.0f;
+    int hfRealtime = 1;
+    void* hfState = nullptr;
+    int16_t* hfLeft = nullptr;
+    int16_t* hfRight = nullptr;
+    int8_t* hfFeature = nullptr;
+    float* hfThr = nullptr;
+    int8_t* hfValue = nullptr;
+    int hfNodes = 0;
+    float hfHsw[2] = {0, 0}, hfMaxHsw = 0;
+
     // lane tables and the per-step tables (pinned host copies, two in flight)
     int32_t* dPoolOf = nullptr;
     uint64_t* dFrameOff = nullptr;
@@ -234,7 +250,7 @@ struct hw_fused
         void* bufs[] = {st16, st32, stats, acc, hist, edgePrev, edgeBits, models, diag, dmeScratch, latModel,
                         latLabel, latRoi, latTrc, prevLat, tb, bls, labels, latent, score, paStats, segStart,
                         segFirst, segLast, segMax, segTotal, segM2, segLabel, err, dPoolOf, dFrameOff, dSteps,
-                        dLists};
+                        dLists, hfState, hfLeft, hfRight, hfFeature, hfThr, hfValue};
         for (void* p : bufs) cudaFree(p);
     }
 
@@ -256,7 +272,7 @@ int hw_fused::Schedule(hw_pool_chunk* table, int b, int32_t counts[kNumLists], i
         const int32_t ff = c.first_frame;
         PoolStep& st = hSteps[b][p];
         st = PoolStep{c.d_trace, c.d_trace8, c.d_pulses, c.d_lens, c.d_overflows, ff, (int32_t)P.F, (int32_t)P.lane0,
-                      0, 0, 0};
+                      0, 0, 0, c.d_metrics};
         auto append = [&](int s) {
             int32_t* dst = lists + (size_t)s * lanes + counts[s];
             for (uint32_t i = 0; i < P.lanes; ++i) dst[i] = (int32_t)(P.lane0 + i);
@@ -346,6 +362,27 @@ int hw_fused::Schedule(hw_pool_chunk* table, int b, int32_t counts[kNumLists], i
             }
         }
         if (!emit) append(L_ZERO);
+        // HF metrics (BatchAnalyzer.cpp:201, 278, 368): every chunk for the
+        // fixed-model and single-estimate analyzers -- before the first
+        // estimate on an empty pulse batch with zero scores --, only emitting
+        // chunks for the dynamic one.  The pulse batch is the labels batch,
+        // 24 latent frames before the trace chunk.
+        c.metrics_emitted = 0;
+        if (hf)
+        {
+            const bool labeled = (cfg.model_estimation_mode == HW_FIXED_ESTIMATIONS)
+                              || (cfg.model_estimation_mode == HW_INITIAL_ESTIMATIONS ? P.initialized : emit);
+            const bool runs = cfg.model_estimation_mode != HW_DYNAMIC_ESTIMATIONS || emit;
+            if (runs)
+            {
+                const int64_t last = (int64_t)ff - kLatent + P.F;
+                const bool finalize = (uint32_t)(last % (int64_t)hfBlock) < P.F;
+                st.hfFlags = (P.hfSeen == 0 ? kHfReset : 0) | (finalize ? kHfFinalize : 0) | (labeled ? 0 : kHfEmpty);
+                P.hfSeen = finalize ? 0 : P.hfSeen + P.F;
+                c.metrics_emitted = finalize ? 1 : 0;
+                append(L_HF);
+            }
+        }
         P.nextFrame = ff + (int32_t)P.F;
         c.emitted = emit ? 1 : 0;
         c.estimated = ran ? 1 : 0;
@@ -439,6 +476,26 @@ int hw_fused::Launch(cudaStream_t s, const int32_t counts[kNumLists], const int 
             End(t, s);
             ++n;
         }
+    }
+    if (counts[L_HF])
+    {
+        HfEngineArgs a{};
+        a.map = map(L_HF);
+        a.state = hfState;
+        a.cap = (int)cfg.max_calls_per_zmw;
+        a.bs = stats;
+        a.models = models;
+        a.viterbi = score;
+        a.pd = paStats;
+        a.realtime = hfRealtime;
+        a.frameRate = hfFrameRate;
+        a.left = hfLeft; a.right = hfRight; a.feature = hfFeature; a.thr = hfThr; a.value = hfValue;
+        a.nodes = hfNodes;
+        a.hsw0 = hfHsw[0]; a.hsw1 = hfHsw[1]; a.maxHsw = hfMaxHsw;
+        const size_t t = Begin(HW_STAGE_METRICS, s);
+        HWF_CUDA(LaunchHfMapped(a, s), "hw_chunk_fused: HF metrics");
+        End(t, s);
+        ++n;
     }
     if (counts[L_ZERO])
     {
@@ -601,6 +658,62 @@ int hw_fused_destroy(hw_fused* f)
     return HW_OK;
 }
 
+int hw_fused_enable_hf_metrics(hw_fused* f, uint32_t frames_per_block, double frame_rate,
+                               int32_t realtime_activity_labels, const int16_t* children_left,
+                               const int16_t* children_right, const int8_t* feature, const float* threshold,
+                               const int8_t* value, uint32_t n_nodes, const float* hsw_curve,
+                               float max_acceptable_halfsandwich_rate)
+{
+    if (!f || frames_per_block == 0 || !(frame_rate > 0)) return Fail(HW_ERR_INVALID_ARG, "bad argument");
+    if (f->step != 0) return Fail(HW_ERR_INVALID_ARG, "HF metrics must be enabled before the first step");
+    const bool cart = children_left && children_right && feature && threshold && value && hsw_curve && n_nodes > 0;
+    if (cart)
+    {
+        if (n_nodes > 32767) return Fail(HW_ERR_INVALID_ARG, "too many CART nodes");
+        for (uint32_t i = 0; i < n_nodes; ++i)
+        {
+            if (feature[i] >= 11) return Fail(HW_ERR_INVALID_ARG, "CART feature index out of range");
+            if (feature[i] >= 0 && (children_left[i] < 0 || children_left[i] >= (int)n_nodes || children_right[i] < 0 ||
+                                    children_right[i] >= (int)n_nodes))
+                return Fail(HW_ERR_INVALID_ARG, "CART child index out of range");
+        }
+    }
+    const char* where = "hw_fused_enable_hf_metrics";
+    int rc;
+    if (!f->hfState)
+    {
+        const size_t bytes = HfLaneBytes() * f->lanes;
+        HWF_CUDA(cudaMalloc(&f->hfState, bytes), where);
+        HWF_CUDA(cudaMemset(f->hfState, 0, bytes), where);
+        HWF_CUDA(LaunchHfInit(f->hfState, (int)f->lanes, 0), where);
+    }
+    if (cart)
+    {
+        cudaFree(f->hfLeft); cudaFree(f->hfRight); cudaFree(f->hfFeature); cudaFree(f->hfThr); cudaFree(f->hfValue);
+        f->hfLeft = f->hfRight = nullptr; f->hfFeature = f->hfValue = nullptr; f->hfThr = nullptr;
+        if ((rc = Alloc(&f->hfLeft, n_nodes, where))) return rc;
+        if ((rc = Alloc(&f->hfRight, n_nodes, where))) return rc;
+        if ((rc = Alloc(&f->hfFeature, n_nodes, where))) return rc;
+        if ((rc = Alloc(&f->hfThr, n_nodes, where))) return rc;
+        if ((rc = Alloc(&f->hfValue, n_nodes, where))) return rc;
+        HWF_CUDA(cudaMemcpy(f->hfLeft, children_left, 2 * n_nodes, cudaMemcpyHostToDevice), where);
+        HWF_CUDA(cudaMemcpy(f->hfRight, children_right, 2 * n_nodes, cudaMemcpyHostToDevice), where);
+        HWF_CUDA(cudaMemcpy(f->hfFeature, feature, n_nodes, cudaMemcpyHostToDevice), where);
+        HWF_CUDA(cudaMemcpy(f->hfThr, threshold, 4 * n_nodes, cudaMemcpyHostToDevice), where);
+        HWF_CUDA(cudaMemcpy(f->hfValue, value, n_nodes, cudaMemcpyHostToDevice), where);
+        f->hfNodes = (int)n_nodes;
+        f->hfHsw[0] = hsw_curve[0];
+        f->hfHsw[1] = hsw_curve[1];
+        f->hfMaxHsw = max_acceptable_halfsandwich_rate;
+    }
+    HWF_CUDA(cudaDeviceSynchronize(), where);
+    f->hf = true;
+    f->hfBlock = frames_per_block;
+    f->hfFrameRate = (float)frame_rate;
+    f->hfRealtime = realtime_activity_labels != 0;
+    return HW_OK;
+}
+
 int hw_fused_use_graphs(hw_fused* f, int32_t enable)
 {
     if (!f) return Fail(HW_ERR_INVALID_ARG, "NULL engine");
@@ -629,7 +742,7 @@ int hw_chunk_fused(hw_fused* f, hw_pool_chunk* table, uint32_t n_pools, void* st
     for (uint32_t p = 0; p < n_pools; ++p)
     {
         const hw_pool_chunk& c = table[p];
-        if (!(c.d_trace || c.d_trace8) || !c.d_pulses || !c.d_lens || !c.d_overflows)
+        if (!(c.d_trace || c.d_trace8) || !c.d_pulses || !c.d_lens || !c.d_overflows || (f->hf && !c.d_metrics))
             return Fail(HW_ERR_INVALID_ARG, "NULL buffer in the pool table");
         if (c.first_frame != f->pools[p].nextFrame) return Fail(HW_ERR_FRAME_ORDER, "Bad frame ID.");
     }

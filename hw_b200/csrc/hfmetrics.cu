@@ -51,6 +51,24 @@ struct HfCartDev
     float hsw0, hsw1, maxHsw;
 };
 
+// One lane's inputs of one step.  viterbi / pd may be null: a pulse batch
+// with no frame labeler behind it (zero scores, no baseline frames).
+struct HfIn
+{
+    const hw_pulse* pulses;          // [64][cap] of the lane
+    const uint32_t* lens;            // [64], or null: no pulses
+    int cap;
+    const hw_baseliner_stats* bs;
+    const hw_lane_model* model;
+    const float* viterbi;            // [64] or null
+    const hw_stat_accum_state* pd;   // or null
+    uint32_t frames;
+    int reset, finalize, realtime;
+    float frameRate;
+    HfCartDev cart;                  // n == 0: no classifier
+    hw_basecalling_metrics* out;     // the lane's record
+};
+
 struct HfArgs
 {
     HfLane* state;
@@ -64,7 +82,7 @@ struct HfArgs
     uint32_t frames;
     int reset, finalize, realtime;
     float frameRate;
-    HfCartDev cart;      // n == 0: no classifier
+    HfCartDev cart;
     hw_basecalling_metrics* out;
 };
 
@@ -97,10 +115,10 @@ __device__ __forceinline__ float MidSignal(const hw_pulse& p)
     return p.width < 3 ? __int_as_float(0x7fffffff) : mul_rn((float)p.mid_signal, 0.1f);
 }
 
-__global__ void __launch_bounds__(kLane) HfStepKernel(HfArgs A)
+// One step of one lane (thread z = ZMW z; the whole 64-thread block takes part
+// in the votes).
+__device__ void HfStep(HfLane& S, const HfIn& A, int z)
 {
-    const int l = blockIdx.x, z = threadIdx.x;
-    HfLane& S = A.state[l];
     const float kNaN = __int_as_float(0x7fffffff);
 
     // BasecallingMetricsAccumulator::Reset + TraceAnalysisMetrics::Reset (first chunk of a block)
@@ -131,8 +149,8 @@ __global__ void __launch_bounds__(kLane) HfStepKernel(HfArgs A)
     S.numFrames[z] += A.frames;
     {
         hw_pulse pp = S.prev[z], ppp = S.prevprev[z];
-        const hw_pulse* row = A.pulses + ((size_t)l * kLane + z) * A.cap;
-        const uint32_t n = A.lens[l * kLane + z];
+        const hw_pulse* row = A.pulses + (size_t)z * A.cap;
+        const uint32_t n = A.lens ? A.lens[z] : 0u;
         for (uint32_t bi = 0; bi < n; ++bi)
         {
             const hw_pulse p = row[bi];
@@ -177,12 +195,12 @@ __global__ void __launch_bounds__(kLane) HfStepKernel(HfArgs A)
     // AddModels (:311-322)
     for (int a = 0; a < kAnalogs; ++a)
     {
-        S.modelVar[a][z] = h2f(A.models[l].analogs[a].vars[z]);
-        S.modelMean[a][z] = h2f(A.models[l].analogs[a].means[z]);
+        S.modelVar[a][z] = h2f(A.model->analogs[a].vars[z]);
+        S.modelMean[a][z] = h2f(A.model->analogs[a].means[z]);
     }
 
     // AddBatchMetrics (:324-340)
-    const hw_baseliner_stats& B = A.bs[l];
+    const hw_baseliner_stats& B = *A.bs;
     {
         // AutocorrAccumulator::Merge of the chunk's baseline-subtracted
         // statistics (AutocorrAccumulator.cpp:71-103); buffer indices as
@@ -208,12 +226,12 @@ __global__ void __launch_bounds__(kLane) HfStepKernel(HfArgs A)
         C.bidx[0][z] = (uint8_t)(fbi + n2);
         C.bidx[1][z] = (uint8_t)((bbi + (4 - n1)) % 4);
     }
-    S.pdScore[z] = add_rn(S.pdScore[z], A.viterbi[l * kLane + z]);
+    S.pdScore[z] = add_rn(S.pdScore[z], A.viterbi ? A.viterbi[z] : 0.0f);
     {
         // pulse-detector baseline statistics shifted by the background mean,
         // then StatAccumulator::operator+= (StatAccumulator.h:144-166)
-        const hw_stat_accum_state& P = A.pd[l];
-        float pOff = P.offset[z], pM0 = P.moment0[z], pM1 = P.moment1[z], pM2 = P.moment2[z];
+        float pOff = 0.0f, pM0 = 0.0f, pM1 = 0.0f, pM2 = 0.0f;
+        if (A.pd) { pOff = A.pd->offset[z]; pM0 = A.pd->moment0[z]; pM1 = A.pd->moment1[z]; pM2 = A.pd->moment2[z]; }
         const hw_stat_accum_state& bg = B.background_stats;
         pOff = add_rn(pOff, StatMean(bg.offset[z], bg.moment0[z], bg.moment1[z]));
         float off = S.blOff[z], m0 = S.blM0[z], m1 = S.blM1[z], m2 = S.blM2[z];
@@ -369,7 +387,7 @@ __global__ void __launch_bounds__(kLane) HfStepKernel(HfArgs A)
     }
 
     // PopulateBasecallingMetrics (:203-247)
-    hw_basecalling_metrics& M = A.out[l];
+    hw_basecalling_metrics& M = *A.out;
     M.activity_label[z] = S.activity[z];
     M.num_pulse_frames[z] = S.pulseFrames[z];
     M.num_base_frames[z] = S.baseFrames[z];
@@ -399,6 +417,33 @@ __global__ void __launch_bounds__(kLane) HfStepKernel(HfArgs A)
     M.pixel_checksum[z] = 0;
 }
 
+__global__ void __launch_bounds__(kLane) HfStepKernel(HfArgs A)
+{
+    const int l = blockIdx.x, z = threadIdx.x;
+    HfIn in{A.pulses + (size_t)l * kLane * A.cap, A.lens + (size_t)l * kLane, A.cap, A.bs + l, A.models + l,
+            A.viterbi + (size_t)l * kLane, A.pd + l, A.frames, A.reset, A.finalize, A.realtime, A.frameRate, A.cart,
+            A.out + l};
+    HfStep(A.state[l], in, z);
+}
+
+// Lane-list form for the fused engine: flags, outputs and the pulse batch of
+// each lane's pool come from its PoolStep.
+__global__ void __launch_bounds__(kLane) HfMappedKernel(HfEngineArgs A)
+{
+    const int li = blockIdx.x, z = threadIdx.x;
+    if (li >= A.map.n) return;          // the whole block returns together
+    const int l = A.map.Lane(li);
+    const PoolStep& ps = A.map.Pool(l);
+    const int lp = l - ps.lane0;         // lane within the pool
+    const bool empty = (ps.hfFlags & kHfEmpty) != 0;
+    HfIn in{ps.pulses + (size_t)lp * kLane * A.cap, empty ? nullptr : ps.lens + (size_t)lp * kLane, A.cap, A.bs + l,
+            A.models + l, empty ? nullptr : A.viterbi + (size_t)l * kLane, empty ? nullptr : A.pd + l,
+            (uint32_t)ps.F, (ps.hfFlags & kHfReset) != 0, (ps.hfFlags & kHfFinalize) != 0, A.realtime, A.frameRate,
+            HfCartDev{A.left, A.right, A.feature, A.thr, A.value, A.nodes, A.hsw0, A.hsw1, A.maxHsw},
+            ps.metrics + lp};
+    HfStep(static_cast<HfLane*>(A.state)[l], in, z);
+}
+
 __global__ void HfInitKernel(HfLane* state, int lanes)
 {
     const int l = blockIdx.x, z = threadIdx.x;
@@ -412,6 +457,22 @@ __global__ void HfInitKernel(HfLane* state, int lanes)
 int Fail(int code, const std::string& msg) { return hwk::SetLastError(code, msg.c_str()); }
 
 }   // namespace
+
+size_t hwk::HfLaneBytes() { return sizeof(HfLane); }
+
+cudaError_t hwk::LaunchHfInit(void* state, int lanes, cudaStream_t s)
+{
+    if (lanes == 0) return cudaSuccess;
+    HfInitKernel<<<lanes, kLane, 0, s>>>(static_cast<HfLane*>(state), lanes);
+    return cudaGetLastError();
+}
+
+cudaError_t hwk::LaunchHfMapped(const HfEngineArgs& a, cudaStream_t s)
+{
+    if (a.map.n == 0) return cudaSuccess;
+    HfMappedKernel<<<a.map.n, kLane, 0, s>>>(a);
+    return cudaGetLastError();
+}
 
 struct hw_hfmetrics
 {

@@ -116,8 +116,11 @@ struct PoolStep
     int32_t F;
     int32_t lane0;              // first engine lane of the pool
     int32_t tModel, tEst;       // DME frame-interval centers
-    int32_t pad_;
+    int32_t hfFlags;            // HF metrics step: kHfReset | kHfFinalize | kHfEmpty
+    hw_basecalling_metrics* metrics;   // the pool's HF metrics records [lanes]
 };
+
+constexpr int kHfReset = 1, kHfFinalize = 2, kHfEmpty = 4;
 
 struct LaneMap
 {
@@ -240,6 +243,31 @@ struct PulseArgs
     // lane-list launch: outputs and first frame from map.Pool(lane)
     LaneMap map{};
 };
+
+// HF metrics in the fused engine: per-lane accumulators (HfLaneBytes each)
+// and one lane-list launch per step.
+struct HfEngineArgs
+{
+    LaneMap map;
+    void* state;                     // [engine lanes] accumulators
+    int cap;
+    const hw_baseliner_stats* bs;    // [engine lanes]
+    const hw_lane_model* models;
+    const float* viterbi;            // [engine lanes][64]
+    const hw_stat_accum_state* pd;   // [engine lanes]
+    int realtime;
+    float frameRate;
+    const int16_t* left;
+    const int16_t* right;
+    const int8_t* feature;
+    const float* thr;
+    const int8_t* value;
+    int nodes;
+    float hsw0, hsw1, maxHsw;
+};
+size_t HfLaneBytes();
+cudaError_t LaunchHfInit(void* state, int lanes, cudaStream_t s);
+cudaError_t LaunchHfMapped(const HfEngineArgs& a, cudaStream_t s);
 
 int BaselinerNumSlots16(int ft);
 cudaError_t LaunchBaseliner(int ft, const BaselinerArgs& a, const KParams& k, cudaStream_t s);

@@ -243,7 +243,7 @@ class BatchAnalyzer(_Handle):
                  _stream()))
         return pulses, lens, ovf, bool(em.value), bool(est.value)
 
-    STAGES = ("baseline", "aggregate", "histogram", "model_init", "dme", "hist_reset", "labeler", "pulses")
+    STAGES = ("baseline", "aggregate", "histogram", "model_init", "dme", "hist_reset", "labeler", "pulses", "metrics")
 
     def export_state(self):
         """Checkpoint of the pool's state as a numpy uint8 array."""
@@ -409,6 +409,28 @@ class FusedEngine(_Handle):
 
     def use_graphs(self, enable=True):
         check(lib().hw_fused_use_graphs(self._h, 1 if enable else 0))
+
+    def enable_hf_metrics(self, frames_per_block=4096, frame_rate=100.0, realtime_activity_labels=True, cart=None):
+        """Adds the HF metrics filter; pool p's block metrics land in
+        self.metrics[p] on steps where metrics_emitted()[p] is set."""
+        arrs = [None] * 6
+        n, maxh = 0, 0.0
+        if cart is not None:
+            arrs = [np.ascontiguousarray(cart["children_left"], np.int16),
+                    np.ascontiguousarray(cart["children_right"], np.int16),
+                    np.ascontiguousarray(cart["feature"], np.int8), np.ascontiguousarray(cart["threshold"], np.float32),
+                    np.ascontiguousarray(cart["value"], np.int8), np.ascontiguousarray(cart["hsw_curve"], np.float32)]
+            n = len(arrs[0])
+            maxh = float(np.asarray(cart["max_acceptable_halfsandwich_rate"]).reshape(-1)[0])
+        ptrs = [abi.ptr(a) for a in arrs]
+        check(lib().hw_fused_enable_hf_metrics(self._h, frames_per_block, float(frame_rate),
+                                               1 if realtime_activity_labels else 0, *ptrs[:5], n, ptrs[5], maxh))
+        self.metrics = [struct_buffer(abi.BASECALLING_METRICS_DT, int(L)) for L in self.lanes]
+        for p, m in enumerate(self.metrics):
+            self.table["d_metrics"][p] = m.data_ptr()
+
+    def metrics_emitted(self):
+        return self.table["metrics_emitted"].copy()
 
     def set_tuning(self, tuning):
         """tuning: {frames_per_chunk: (fuse_label_pulses, labeler_lanes_per_cta)}."""

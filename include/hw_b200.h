@@ -604,11 +604,23 @@ typedef struct hw_pool_chunk {
     hw_pulse* d_pulses;         /* [lanes][64][max_calls_per_zmw] */
     uint32_t* d_lens;           /* [lanes][64] */
     uint32_t* d_overflows;      /* [lanes][64] */
+    hw_basecalling_metrics* d_metrics;  /* [lanes] HF metrics records (with hw_fused_enable_hf_metrics) */
     int32_t first_frame;        /* must be the pool's next frame (0, F, 2F, ...) */
     int32_t emitted;            /* out: 0 while the reference returns no pulses (start-up) */
     int32_t estimated;          /* out: 1 when this step ran a full DME estimate */
-    int32_t reserved;
+    int32_t metrics_emitted;    /* out: 1 when d_metrics holds a completed block */
 } hw_pool_chunk;
+
+/* Adds the HF metrics filter to every pool's step (HFMetricsFilter, called
+ * by the analyzers after the pulse accumulator, AN/BatchAnalyzer.cpp:201,
+ * 278, 368): one lane-list launch per step; each pool's block metrics go to
+ * its table row's d_metrics when a pulse batch ends a block.  The CART
+ * arrays may be NULL (no activity labels); see hw_hfmetrics_set_cart. */
+int hw_fused_enable_hf_metrics(hw_fused* f, uint32_t frames_per_block, double frame_rate,
+                               int32_t realtime_activity_labels, const int16_t* children_left,
+                               const int16_t* children_right, const int8_t* feature, const float* threshold,
+                               const int8_t* value, uint32_t n_nodes, const float* hsw_curve,
+                               float max_acceptable_halfsandwich_rate);
 
 /* Kernel choices for the pools of one chunk length (see hw_fused_set_tuning). */
 typedef struct hw_fused_tuning {
@@ -680,7 +692,8 @@ enum {
     HW_STAGE_HIST_RESET = 5,
     HW_STAGE_LABELER = 6,
     HW_STAGE_PULSES = 7,
-    HW_NUM_STAGES = 8
+    HW_STAGE_METRICS = 8,       /* HF metrics (hw_chunk_fused only) */
+    HW_NUM_STAGES = 9
 };
 int hw_analyzer_profile(hw_analyzer* a, int32_t enable);
 int hw_analyzer_stage_times(hw_analyzer* a, double ms[HW_NUM_STAGES], uint32_t launches[HW_NUM_STAGES]);

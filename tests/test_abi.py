@@ -57,7 +57,8 @@ int main(void) {
   O(hw_lane_histogram, bin_count) O(hw_pulse, start) O(hw_pulse, width) O(hw_pulse, mean_signal)
   O(hw_pulse, mid_signal) O(hw_pulse, max_signal) O(hw_pulse, signal_m2) O(hw_pulse, label) O(hw_pulse, is_reject)
   O(hw_dme_diag, lane_iterations)
-  O(hw_pool_chunk, d_trace8) O(hw_pool_chunk, d_overflows) O(hw_pool_chunk, first_frame) O(hw_pool_chunk, estimated)
+  O(hw_pool_chunk, d_trace8) O(hw_pool_chunk, d_overflows) O(hw_pool_chunk, d_metrics)
+  O(hw_pool_chunk, first_frame) O(hw_pool_chunk, estimated) O(hw_pool_chunk, metrics_emitted)
   O(hw_fused_tuning, labeler_lanes_per_cta)
   O(hw_basecalling_metrics, num_pulse_frames) O(hw_basecalling_metrics, pk_mid_signal)
   O(hw_basecalling_metrics, num_pk_mid_frames) O(hw_basecalling_metrics, frame_baseline_dws)

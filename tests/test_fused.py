@@ -1,5 +1,7 @@
 """Fused chunk engine (hw_chunk_fused): uneven pools in one launch per stage
 give exactly the results of one hw_analyzer per pool."""
+import os
+
 import numpy as np
 import pytest
 
@@ -106,3 +108,52 @@ def test_fused_kernel_variants_equal_per_pool_analyzers(tuning):
     4 lanes a block) gives the per-pool analyzers' results."""
     emitted, estimated, _ = _compare(abi.DYNAMIC_ESTIMATIONS, graphs=False, u8=False, steps=28, tuning=tuning)
     assert emitted > 0 and estimated > 0
+
+
+@pytest.mark.parametrize("mode", [abi.FIXED_ESTIMATIONS, abi.INITIAL_ESTIMATIONS, abi.DYNAMIC_ESTIMATIONS])
+def test_fused_hf_metrics_equal_standalone_filter(mode):
+    """HF metrics inside hw_chunk_fused equal a standalone hw_hfmetrics filter
+    fed by each pool's own analyzer, in the reference's calling pattern."""
+    import torch
+    from hw_b200 import filters as Fl
+    golden = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "trained_cart.npz")
+    cart = dict(np.load(golden))
+    cfg = workloads.small_config()
+    cfg.model_estimation_mode = mode
+    lanes, frames, block = [2, 1, 3], [512, 256, 128], 1024
+    eng = Fl.FusedEngine(cfg, lanes, frames)
+    eng.enable_hf_metrics(block, cfg.frame_rate, True, cart)
+    ans = [Fl.BatchAnalyzer(cfg, p, L, F) for p, (L, F) in enumerate(zip(lanes, frames))]
+    hfs = [Fl.HfMetrics(L, block, cfg.frame_rate, True, cart=cart) for L in lanes]
+    gens = [Fl.TraceGenerator(L, workload=2, zmw_offset=1000 * p) for p, L in enumerate(lanes)]
+    zeros = {L: (torch.zeros((L, 64), dtype=torch.int32, device="cuda"),
+                 torch.zeros((L, 64), dtype=torch.float32, device="cuda"),
+                 Fl.numpy_to_struct(np.zeros(L, abi.STAT_ACCUM_DT))) for L in set(lanes)}
+    blocks = 0
+    for step in range(24):
+        chunks = _chunks(gens, frames, step, False)
+        eng.process(chunks)
+        memit = eng.metrics_emitted()
+        for p, (an, L, F) in enumerate(zip(ans, lanes, frames)):
+            pulses, lens, ovf, em, est = an(chunks[p], step * F)
+            runs = mode != abi.DYNAMIC_ESTIMATIONS or em
+            if not runs:
+                assert memit[p] == 0
+                continue
+            bs, vit, pd = an.chunk_metrics()
+            models, _ = an.models()
+            if not em:
+                lens_in, vit, pd = zeros[L]
+            else:
+                lens_in = lens
+            got = hfs[p].process(pulses, lens_in, cfg.max_calls_per_zmw, bs, models, vit, pd,
+                                 step * F - abi.LATENT_FRAMES, F)
+            assert (got is not None) == bool(memit[p]), (step, p)
+            if got is not None:
+                blocks += 1
+                a = Fl.struct_to_numpy(got, abi.BASECALLING_METRICS_DT)
+                b = Fl.struct_to_numpy(eng.metrics[p], abi.BASECALLING_METRICS_DT)
+                for name in abi.BASECALLING_METRICS_DT.names:
+                    assert np.array_equal(a[name], b[name], equal_nan=a[name].dtype.kind == "f"), (step, p, name)
+    eng.finish()
+    assert blocks > 0
