@@ -171,6 +171,11 @@ BASECALLING_METRICS_DT = np.dtype([
     ("pixel_checksum", np.int16, _L)])
 HQRF_EMPTY, HQRF_SINGLE, HQRF_MULTI, HQRF_LOW = 0, 1, 2, 3
 
+# hw_sensor_packet (repacker input descriptor)
+SENSOR_PACKET_DT = np.dtype([("data_offset", np.uint64), ("start_zmw", np.uint32), ("start_frame", np.int32),
+                             ("num_frames", np.uint32), ("block_width", np.uint32), ("num_blocks", np.uint32),
+                             ("reserved", np.uint32)])
+
 # hw_pool_chunk: one pool's row of the hw_chunk_fused table (device pointers as integers)
 POOL_CHUNK_DT = np.dtype([("d_trace", np.uint64), ("d_trace8", np.uint64), ("d_pulses", np.uint64),
                           ("d_lens", np.uint64), ("d_overflows", np.uint64), ("d_metrics", np.uint64),
@@ -190,6 +195,7 @@ SIZES = {
     "hw_dme_diag": (DME_DIAG_DT, 1344),
     "hw_pool_chunk": (POOL_CHUNK_DT, 64),
     "hw_basecalling_metrics": (BASECALLING_METRICS_DT, 8768),
+    "hw_sensor_packet": (SENSOR_PACKET_DT, 32),
     "hw_fused_tuning": (FUSED_TUNING_DT, 16),
 }
 

@@ -523,6 +523,36 @@ class HfMetrics(_Handle):
         return self.out if em.value else None
 
 
+class Repacker(_Handle):
+    """Ingest repacking (hw_repacker): sensor packets of one chunk of frames
+    gathered into the pools' TraceBatch chunks."""
+    _destroy = "hw_repacker_destroy"
+
+    def __init__(self, num_zmw, lanes_per_pool, frames_per_chunk, encoding="int16"):
+        super().__init__()
+        self.num_zmw, self.lanes_per_pool, self.F = num_zmw, lanes_per_pool, frames_per_chunk
+        self.dtype = torch.int16 if encoding == "int16" else torch.uint8
+        check(lib().hw_repacker_create(num_zmw, lanes_per_pool, frames_per_chunk, 0 if encoding == "int16" else 1,
+                                       C.byref(self._h)))
+        n = C.c_uint32()
+        check(lib().hw_repacker_num_pools(self._h, C.byref(n)))
+        self.n_pools = n.value
+        lanes = num_zmw // abi.LANE
+        self.pool_lanes = [min(lanes_per_pool, lanes - p * lanes_per_pool) for p in range(self.n_pools)]
+
+    def new_chunks(self):
+        return [torch.zeros((L, self.F, abi.LANE), dtype=self.dtype, device="cuda") for L in self.pool_lanes]
+
+    def __call__(self, packets, packet_data, chunk_first_frame, chunks):
+        """packets: numpy SENSOR_PACKET_DT table; packet_data: CUDA uint8
+        tensor holding the packets; chunks: per-pool CUDA tensors (written)."""
+        packets = np.ascontiguousarray(packets, abi.SENSOR_PACKET_DT)
+        ptrs = (C.c_void_p * len(chunks))(*[c.data_ptr() for c in chunks])
+        check(lib().hw_repack_chunk(self._h, abi.ptr(packets), len(packets), _p(packet_data), int(chunk_first_frame),
+                                    ptrs, _stream()))
+        return chunks
+
+
 class _DeviceBytes:
     """Device memory owned by the library, exposed to torch without a copy."""
 

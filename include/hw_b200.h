@@ -551,6 +551,40 @@ int hw_hfmetrics_process(hw_hfmetrics* h, const hw_pulse* d_pulses, const uint32
                          int32_t first_frame, uint32_t frames, hw_basecalling_metrics* d_out, int32_t* emitted,
                          void* stream);
 
+/* ---- Ingest repacking (BlockRepacker) ---------------------------------------
+ * Replaces the data shuffle of BlockRepacker
+ * (appModules/BlockRepacker.cpp:200-345, BatchFiller::Process): sensor
+ * packets -- num_blocks blocks of block_width ZMWs, each block stored
+ * [num_frames][block_width] -- are gathered into the pools' TraceBatch
+ * chunks [lanes][frames_per_chunk][64].  Pools cover ZMWs [0, num_zmw) in
+ * order, lanes_per_pool lanes each (the last pool may have fewer).  One call
+ * handles the packets of one chunk of frames; each packet's frames lie inside
+ * that chunk and its block width is a multiple of 32 ZMWs (int16) or 64 ZMWs
+ * (uint8), the reference's cache-line granularity. */
+typedef struct hw_sensor_packet {
+    uint64_t data_offset;       /* bytes from d_packet_data to the packet's first block */
+    uint32_t start_zmw;
+    int32_t  start_frame;
+    uint32_t num_frames;
+    uint32_t block_width;       /* ZMWs per block */
+    uint32_t num_blocks;
+    uint32_t reserved;
+} hw_sensor_packet;
+
+typedef struct hw_repacker hw_repacker;
+/* encoding: 0 = int16, 1 = uint8 (PacketLayout::INT16 / UINT8). */
+int hw_repacker_create(uint32_t num_zmw, uint32_t lanes_per_pool, uint32_t frames_per_chunk, int32_t encoding,
+                       hw_repacker** out);
+int hw_repacker_destroy(hw_repacker* r);
+int hw_repacker_num_pools(const hw_repacker* r, uint32_t* n_pools);
+/* Gathers the packets (host descriptors, data in device memory) into the
+ * pools' chunks of frames [chunk_first_frame, chunk_first_frame +
+ * frames_per_chunk): d_pool_chunks[n_pools] are device pointers.  Packets
+ * must lie in the chunk and in [0, num_zmw); every covered element is
+ * written, others are left unchanged. */
+int hw_repack_chunk(hw_repacker* r, const hw_sensor_packet* packets, uint32_t n_packets, const void* d_packet_data,
+                    int32_t chunk_first_frame, void* const* d_pool_chunks, void* stream);
+
 /* ---- Pool sets: uneven pools --------------------------
  * No single reference counterpart: the reference runs one BatchAnalyzer per
  * pool.  A pool set owns n_pools pools of any lane counts and chunk lengths

@@ -2449,3 +2449,43 @@ int or_hf_process(void* p, const hw_pulse* pulses, const uint32_t* lens, uint32_
 }
 
 }   // extern "C"
+
+// ===========================================================================
+// Ingest repacking: appModules/BlockRepacker.cpp:252-345 (BatchFiller::Process),
+// every cache line of every packet block copied to its pool / lane / frame.
+
+extern "C" {
+
+int or_repack(uint32_t numZmw, uint32_t lanesPerPool, uint32_t F, int32_t encoding, const hw_sensor_packet* packets,
+              uint32_t nPackets, const uint8_t* data, int32_t chunkFirstFrame, uint8_t* const* poolChunks)
+{
+    const size_t e = encoding == 0 ? 2 : 1;
+    const size_t cacheLineZmw = encoding == 0 ? 32 : 64;
+    const size_t laneWidth = kLane;
+    for (uint32_t i = 0; i < nPackets; ++i)
+    {
+        const hw_sensor_packet& p = packets[i];
+        const size_t W = p.block_width;
+        for (size_t blk = 0; blk < p.num_blocks; ++blk)
+        {
+            const size_t blockZmw = p.start_zmw + blk * W;
+            const uint8_t* blockData = data + p.data_offset + blk * p.num_frames * W * e;
+            for (size_t f = 0; f < p.num_frames; ++f)
+            {
+                const size_t batchFrame = (size_t)(p.start_frame - chunkFirstFrame) + f;
+                for (size_t zi = 0; zi < W; zi += cacheLineZmw)
+                {
+                    const size_t zmw = blockZmw + zi;
+                    if (zmw >= numZmw) break;
+                    const size_t lane = zmw / laneWidth;
+                    const size_t pool = lane / lanesPerPool, lip = lane % lanesPerPool;
+                    uint8_t* dst = poolChunks[pool] + ((lip * F + batchFrame) * laneWidth + (zmw - lane * laneWidth)) * e;
+                    std::memcpy(dst, blockData + (f * W + zi) * e, cacheLineZmw * e);
+                }
+            }
+        }
+    }
+    return HW_OK;
+}
+
+}   // extern "C"

@@ -68,6 +68,7 @@ def lib():
         L.or_hf_destroy.argtypes = [vp]
         L.or_hf_set_cart.argtypes = [vp, vp, vp, vp, vp, vp, u32, vp, C.c_float]
         L.or_hf_process.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp, i32, u32, vp, C.POINTER(i32)]
+        L.or_repack.argtypes = [u32, u32, u32, i32, vp, u32, vp, i32, vp]
         _lib = L
     return _lib
 
@@ -270,3 +271,13 @@ class HfMetrics:
                                    abi.ptr(models), abi.ptr(viterbi), abi.ptr(pd_stats), int(first_frame),
                                    int(frames), abi.ptr(out), C.byref(em)))
         return out if em.value else None
+
+
+def repack(num_zmw, lanes_per_pool, frames_per_chunk, encoding, packets, data, chunk_first_frame, pool_chunks):
+    """BatchFiller::Process over a chunk's packets (abi.SENSOR_PACKET_DT table,
+    uint8 packet data); pool_chunks: list of numpy arrays updated in place."""
+    packets = np.ascontiguousarray(packets, abi.SENSOR_PACKET_DT)
+    data = np.ascontiguousarray(data, np.uint8)
+    ptrs = (C.c_void_p * len(pool_chunks))(*[c.ctypes.data for c in pool_chunks])
+    _check(lib().or_repack(num_zmw, lanes_per_pool, frames_per_chunk, encoding, abi.ptr(packets), len(packets),
+                           abi.ptr(data), int(chunk_first_frame), ptrs))

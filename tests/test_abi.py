@@ -50,7 +50,7 @@ int main(void) {
   S(hw_config) S(hw_analog) S(hw_stat_accum_state) S(hw_autocorr_accum_state) S(hw_baseliner_stats)
   S(hw_lane_analog_mode) S(hw_lane_model) S(hw_lane_histogram) S(hw_lane_hist_bounds) S(hw_pulse)
   S(hw_dme_diag) S(hw_frame_interval) S(hw_gen_params) S(hw_pool_chunk) S(hw_fused_tuning)
-  S(hw_basecalling_metrics)
+  S(hw_basecalling_metrics) S(hw_sensor_packet)
   O(hw_baseliner_stats, full_autocorr) O(hw_baseliner_stats, trace_min) O(hw_baseliner_stats, trace_max)
   O(hw_baseliner_stats, baseline_stats) O(hw_baseliner_stats, raw_baseline_sum) O(hw_baseliner_stats, background_stats)
   O(hw_lane_model, analogs) O(hw_lane_model, baseline) O(hw_lane_model, confidence)
@@ -64,6 +64,7 @@ int main(void) {
   O(hw_basecalling_metrics, num_pk_mid_frames) O(hw_basecalling_metrics, frame_baseline_dws)
   O(hw_basecalling_metrics, start_frame) O(hw_basecalling_metrics, autocorrelation)
   O(hw_basecalling_metrics, pixel_checksum)
+  O(hw_sensor_packet, start_zmw) O(hw_sensor_packet, num_blocks)
   O(hw_config, analogs) O(hw_config, filter_type) O(hw_config, max_calls_per_zmw) O(hw_config, xsp_amp_thresh)
   O(hw_config, model_estimation_mode) O(hw_config, static_baseline_variance)
   return 0;
@@ -106,7 +107,8 @@ def test_struct_offsets_match_python_mirrors(layout):
         dt = {"hw_baseliner_stats": abi.BLSTATS_DT, "hw_lane_model": abi.LANE_MODEL_DT,
               "hw_lane_histogram": abi.LANE_HIST_DT, "hw_pulse": abi.PULSE_DT,
               "hw_dme_diag": abi.DME_DIAG_DT, "hw_pool_chunk": abi.POOL_CHUNK_DT,
-              "hw_fused_tuning": abi.FUSED_TUNING_DT, "hw_basecalling_metrics": abi.BASECALLING_METRICS_DT}[t]
+              "hw_fused_tuning": abi.FUSED_TUNING_DT, "hw_basecalling_metrics": abi.BASECALLING_METRICS_DT,
+              "hw_sensor_packet": abi.SENSOR_PACKET_DT}[t]
         assert dt.fields[m][1] == off, key
 
 
@@ -192,6 +194,15 @@ def test_version_string():
 
 @pytest.mark.skipif("torch" in sys.modules and __import__("torch").cuda.is_available(),
                     reason="checks the no-device failure path")
+def _has_device():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_has_device(), reason="checks the behaviour without a CUDA device")
 def test_no_cpu_fallback_without_device():
     """With no CUDA device the handles cannot be created: the call returns a
     CUDA status instead of computing on the CPU."""
@@ -203,6 +214,7 @@ def test_no_cpu_fallback_without_device():
     assert b"CUDA" in native.lib().hw_last_error_string() or b"cuda" in native.lib().hw_last_error_string()
 
 
+@pytest.mark.skipif(_has_device(), reason="checks the behaviour without a CUDA device")
 def test_fused_engine_needs_a_device_and_checks_its_arguments():
     """hw_fused_create rejects bad pool tables before touching the device and,
     with no CUDA device, returns a CUDA status (no CPU path)."""
