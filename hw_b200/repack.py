@@ -5,7 +5,7 @@ memory) gathered into 4 pools of 4096 lanes.  Device time with CUDA events
 over K calls; the rate is bytes moved (every byte read once and written once)
 per second, against the measured HBM copy bandwidth.
 
-    python -m hw_b200.repack [--steps 20]
+    python -m hw_b200.repack [--steps 20] [--zmw 1048576]
 """
 import argparse
 import json
@@ -31,8 +31,8 @@ def chip_packets(num_zmw=1 << 20, frames=512, block_width=128, blocks=256):
     return np.array(rows, abi.SENSOR_PACKET_DT), off
 
 
-def run(steps=20, warmup=3):
-    num_zmw, F, lpp = 1 << 20, 512, 4096
+def run(steps=20, warmup=3, num_zmw=1 << 20):
+    F, lpp = 512, 4096
     table, nbytes = chip_packets(num_zmw, F)
     data = torch.randint(0, 255, (nbytes,), dtype=torch.uint8, device="cuda")
     rp = Fl.Repacker(num_zmw, lpp, F)
@@ -64,8 +64,9 @@ def run(steps=20, warmup=3):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--zmw", type=int, default=1 << 20)
     a = ap.parse_args()
-    print(json.dumps(run(a.steps)))
+    print(json.dumps(run(a.steps, num_zmw=a.zmw)))
 
 
 if __name__ == "__main__":
