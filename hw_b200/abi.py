@@ -15,6 +15,7 @@ NUM_STATES = 13
 LATENT_FRAMES = 24          # ViterbiStitchLookback + ROI lookForward + stitchFrames
 
 HW_OK = 0
+HW_ERR_OUT_OF_MEMORY = 8
 STATUS_NAMES = {
     0: "HW_OK", 1: "HW_ERR_INVALID_ARG", 2: "HW_ERR_CUDA", 3: "HW_ERR_BAD_POOL",
     4: "HW_ERR_FRAME_ORDER", 5: "HW_ERR_NOT_INITIALIZED", 6: "HW_ERR_UNSUPPORTED",
@@ -181,6 +182,14 @@ POOL_CHUNK_DT = np.dtype([("d_trace", np.uint64), ("d_trace8", np.uint64), ("d_p
                           ("d_lens", np.uint64), ("d_overflows", np.uint64), ("d_metrics", np.uint64),
                           ("first_frame", np.int32), ("emitted", np.int32), ("estimated", np.int32),
                           ("metrics_emitted", np.int32)])
+# hw_baz_field (one field of a BAZ pulse encoding)
+BAZ_FIELD_DT = np.dtype([(n, np.int32) for n in ("name", "store_signed", "transform", "scale", "transform_bytes",
+                                                  "serialize", "num_bits", "overflow_bytes")])
+BAZ_LABEL, BAZ_START_FRAME, BAZ_PULSE_WIDTH, BAZ_IS_BASE, BAZ_PKMAX, BAZ_PKMID, BAZ_PKMEAN, BAZ_PKVAR = range(8)
+BAZ_NOOP, BAZ_DELTA, BAZ_FLOAT_FIXED = range(3)
+BAZ_TRUNCATE, BAZ_SIMPLE_OVERFLOW, BAZ_COMPACT_OVERFLOW = range(3)
+BAZ_PRODUCTION, BAZ_INTERNAL = 0, 1
+
 FUSED_TUNING_DT = np.dtype([("frames_per_chunk", np.uint32), ("fuse_label_pulses", np.uint32),
                             ("labeler_lanes_per_cta", np.uint32), ("reserved", np.uint32)])
 
@@ -197,6 +206,7 @@ SIZES = {
     "hw_basecalling_metrics": (BASECALLING_METRICS_DT, 8768),
     "hw_sensor_packet": (SENSOR_PACKET_DT, 32),
     "hw_fused_tuning": (FUSED_TUNING_DT, 16),
+    "hw_baz_field": (BAZ_FIELD_DT, 32),
 }
 
 

@@ -553,6 +553,48 @@ class Repacker(_Handle):
         return chunks
 
 
+def baz_preset(which):
+    """(fields, skip_rejects) of a basecaller pulse encoding: abi.BAZ_PRODUCTION
+    or abi.BAZ_INTERNAL (PulseGroups.h)."""
+    fields = np.zeros(16, abi.BAZ_FIELD_DT)
+    n, skip = C.c_uint32(), C.c_int32()
+    check(lib().hw_baz_preset(int(which), abi.ptr(fields), C.byref(n), C.byref(skip)))
+    return fields[:n.value].copy(), bool(skip.value)
+
+
+class BazEncoder(_Handle):
+    """BAZ pulse encoding (hw_baz_encoder): each chunk's pulses of every ZMW
+    become that ZMW's bytes (PrelimHQFilter + PacketBuffer::AddZmw).  The
+    start-frame delta state of each ZMW carries over between chunks."""
+    _destroy = "hw_baz_encoder_destroy"
+
+    def __init__(self, num_zmw, fields=None, skip_rejects=None, preset=abi.BAZ_PRODUCTION):
+        super().__init__()
+        if fields is None:
+            fields, skip = baz_preset(preset)
+            skip_rejects = skip if skip_rejects is None else skip_rejects
+        self.fields = np.ascontiguousarray(fields, abi.BAZ_FIELD_DT)
+        self.num_zmw = num_zmw
+        check(lib().hw_baz_encoder_create(abi.ptr(self.fields), len(self.fields), int(bool(skip_rejects)), num_zmw,
+                                          C.byref(self._h)))
+        self.offsets = torch.zeros(num_zmw + 1, dtype=torch.int64, device="cuda")
+        self.bytes = torch.empty(0, dtype=torch.uint8, device="cuda")
+
+    def __call__(self, pulses, lens, max_calls):
+        """pulses: CUDA buffer of [num_zmw][max_calls] hw_pulse; lens: CUDA
+        uint32/int32 counts.  Returns (bytes, offsets): the chunk's bytes (a
+        view of the encoder's buffer) and the ZMW offsets [num_zmw + 1]."""
+        total = C.c_uint64()
+        for _ in range(2):
+            rc = lib().hw_baz_encode(self._h, _p(pulses), _p(lens), int(max_calls), _p(self.bytes),
+                                     self.bytes.numel(), _p(self.offsets), C.byref(total), _stream())
+            if rc != abi.HW_ERR_OUT_OF_MEMORY:
+                break
+            self.bytes = torch.empty(max(total.value, 2 * self.bytes.numel()), dtype=torch.uint8, device="cuda")
+        check(rc)
+        return self.bytes[:total.value], self.offsets
+
+
 class _DeviceBytes:
     """Device memory owned by the library, exposed to torch without a copy."""
 

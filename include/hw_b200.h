@@ -585,6 +585,55 @@ int hw_repacker_num_pools(const hw_repacker* r, uint32_t* n_pools);
 int hw_repack_chunk(hw_repacker* r, const hw_sensor_packet* packets, uint32_t n_packets, const void* d_packet_data,
                     int32_t chunk_first_frame, void* const* d_pool_chunks, void* stream);
 
+/* ---- BAZ pulse encoding (bazio/encoding) ------------------------------------
+ * Replaces the pulse serialization of the BAZ writer path
+ * (PrelimHQFilter.cpp:63-120 + PacketBuffer::AddZmw, bazio/writing/PacketBuffer.h:143-210,
+ * with the field machinery of bazio/encoding/ObjectToBaz.h,
+ * FieldTransforms.h and FieldSerializers.h): each ZMW's pulses of a chunk
+ * become a byte string, appended per ZMW.  A pulse encoding is a list of
+ * fields; consecutive fields are packed little-endian into groups of at most
+ * 64 bits, a new group starting when the current one is a whole number of
+ * bytes or the next field would not fit (ObjectToBaz.h:373-393), and each
+ * group's overflow bytes follow its main bytes in field order. */
+enum {
+    HW_BAZ_LABEL = 0, HW_BAZ_START_FRAME = 1, HW_BAZ_PULSE_WIDTH = 2, HW_BAZ_IS_BASE = 3,
+    HW_BAZ_PKMAX = 4, HW_BAZ_PKMID = 5, HW_BAZ_PKMEAN = 6, HW_BAZ_PKVAR = 7
+};
+enum { HW_BAZ_NOOP = 0, HW_BAZ_DELTA = 1, HW_BAZ_FLOAT_FIXED = 2 };                 /* transforms */
+enum { HW_BAZ_TRUNCATE = 0, HW_BAZ_SIMPLE_OVERFLOW = 1, HW_BAZ_COMPACT_OVERFLOW = 2 }; /* serializers */
+typedef struct hw_baz_field {
+    int32_t name;             /* HW_BAZ_LABEL ... HW_BAZ_PKVAR */
+    int32_t store_signed;
+    int32_t transform;        /* HW_BAZ_NOOP, HW_BAZ_DELTA, HW_BAZ_FLOAT_FIXED */
+    int32_t scale;            /* FloatFixedCodec FixedPointScale */
+    int32_t transform_bytes;  /* FloatFixedCodec NumBytes */
+    int32_t serialize;        /* HW_BAZ_TRUNCATE, HW_BAZ_SIMPLE_OVERFLOW, HW_BAZ_COMPACT_OVERFLOW */
+    int32_t num_bits;         /* main-portion bits (1..30) */
+    int32_t overflow_bytes;   /* SimpleOverflow NumBytes */
+} hw_baz_field;
+
+/* The basecaller's two encodings (basecaller/dataTypes/PulseGroups.h:42-96):
+ * 0 = ProductionPulses (3 fields, 2 nominal bytes, rejected pulses left
+ * out), 1 = InternalPulses (8 fields, 6 nominal bytes, every pulse). */
+int hw_baz_preset(int32_t which, hw_baz_field* fields, uint32_t* n_fields, int32_t* skip_rejects);
+
+typedef struct hw_baz_encoder hw_baz_encoder;
+/* An encoder for num_zmw ZMWs; the start-frame delta state of each ZMW is
+ * kept across calls (the per-ZMW serializers of PrelimHQFilter). */
+int hw_baz_encoder_create(const hw_baz_field* fields, uint32_t n_fields, int32_t skip_rejects, uint32_t num_zmw,
+                          hw_baz_encoder** out);
+int hw_baz_encoder_destroy(hw_baz_encoder* e);
+/* Encodes one chunk: pulses [num_zmw][max_calls] with counts d_lens[num_zmw]
+ * (counts above max_calls read as max_calls).
+ * d_offsets[num_zmw + 1] receives each ZMW's byte range in d_bytes (capacity
+ * bytes_capacity); *total_bytes the bytes written.  Returns
+ * HW_ERR_OUT_OF_MEMORY (nothing written, state unchanged) when the chunk
+ * needs more than bytes_capacity.  Synchronises the stream once (to learn
+ * the total). */
+int hw_baz_encode(hw_baz_encoder* e, const hw_pulse* d_pulses, const uint32_t* d_lens, uint32_t max_calls,
+                  uint8_t* d_bytes, uint64_t bytes_capacity, uint64_t* d_offsets, uint64_t* total_bytes,
+                  void* stream);
+
 /* ---- Pool sets: uneven pools --------------------------
  * No single reference counterpart: the reference runs one BatchAnalyzer per
  * pool.  A pool set owns n_pools pools of any lane counts and chunk lengths

@@ -2489,3 +2489,391 @@ int or_repack(uint32_t numZmw, uint32_t lanesPerPool, uint32_t F, int32_t encodi
 }
 
 }   // extern "C"
+
+// ===========================================================================
+// BAZ pulse encoding: bazio/encoding/ObjectToBaz.h:60-150 (GroupEncoder),
+// :373-393 (grouping), FieldSerializers.h:56-364, FieldTransforms.h (NoOp,
+// FloatFixedCodec, DeltaCompression), basecaller/dataTypes/PulseFieldAccessors.h
+// (field values of a pulse).  The fields are a runtime list here.
+
+namespace {
+
+struct BazPulse          // the field values of one pulse
+{
+    uint8_t label;
+    uint32_t start;
+    uint16_t width;
+    uint8_t isBase;
+    float pkmax, pkmid, pkmean, pkvar;
+};
+
+constexpr uint64_t kFfNan = 0, kFfInf = 1, kFfNinf = 2, kFfOffset = 3;
+
+struct BazOracle
+{
+    std::vector<hw_baz_field> f;
+    std::vector<std::vector<int>> groups;      // field indices per group
+    std::vector<int> groupBytes;
+
+    explicit BazOracle(const hw_baz_field* fields, uint32_t n) : f(fields, fields + n)
+    {
+        int cur = 0;
+        std::vector<int> g;
+        for (uint32_t i = 0; i < n; ++i)
+        {
+            const int bits = f[i].num_bits;
+            const bool even = cur % 8 == 0 && cur > 0;
+            if (even || cur + bits > 64)
+            {
+                groups.push_back(g); groupBytes.push_back((cur + 7) / 8);
+                g.clear(); cur = 0;
+            }
+            g.push_back((int)i); cur += bits;
+        }
+        groups.push_back(g); groupBytes.push_back((cur + 7) / 8);
+    }
+
+    static uint64_t FloatFixed(float v, bool sgn, int scale, int bytes)
+    {
+        float scaled = std::round(v * (float)scale);
+        if (sgn)
+        {
+            const int64_t mx = (int64_t)((1ull << (8 * bytes - 1)) - 1 - kFfOffset);
+            if ((float)(-mx) <= scaled && (float)mx >= scaled)
+            {
+                if (scaled >= 0) scaled += (float)kFfOffset;
+                return (uint64_t)(int64_t)scaled;
+            }
+        }
+        else
+        {
+            // 8 bytes: the largest code less the offset (a shift by 64 is undefined)
+            const uint64_t mx = (bytes >= 8 ? ~0ull : (1ull << (8 * bytes)) - 1) - kFfOffset;
+            if (0 <= scaled && (float)mx >= scaled)
+            {
+                scaled += (float)kFfOffset;
+                return (uint64_t)scaled;
+            }
+        }
+        if (std::isnan(v)) return kFfNan;
+        if (scaled < 0) return kFfNinf;
+        return kFfInf;
+    }
+
+    // the transformed value of field i (DeltaCompression updates last[i])
+    uint64_t Value(int i, const BazPulse& p, uint64_t* last) const
+    {
+        const hw_baz_field& d = f[i];
+        if (d.transform == HW_BAZ_FLOAT_FIXED)
+        {
+            const float v = d.name == HW_BAZ_PKMAX ? p.pkmax : d.name == HW_BAZ_PKMID ? p.pkmid
+                          : d.name == HW_BAZ_PKMEAN ? p.pkmean : p.pkvar;
+            return FloatFixed(v, d.store_signed != 0, d.scale, d.transform_bytes);
+        }
+        const uint64_t raw = d.name == HW_BAZ_LABEL ? p.label : d.name == HW_BAZ_START_FRAME ? p.start
+                           : d.name == HW_BAZ_PULSE_WIDTH ? p.width : p.isBase;
+        if (d.transform == HW_BAZ_DELTA)
+        {
+            const uint64_t r = raw - last[i];
+            last[i] = raw;
+            return r;
+        }
+        return raw;
+    }
+
+    static bool SimpleNeeds(uint64_t v, bool sgn, int bits)
+    {
+        if (sgn) v += (1ull << (bits - 1)) - 1;
+        return v >= (1ull << bits) - 1;
+    }
+
+    static size_t CompactOverflowBytes(uint64_t t, bool sgn, int bits)
+    {
+        if (sgn)
+        {
+            const int discard = __builtin_clrsbl((long)t);
+            const int keep = 64 - discard - (bits - 1);
+            return (size_t)((keep + 6) / 7);
+        }
+        t >>= (bits - 1);
+        size_t r = 0;
+        while (t) { ++r; t >>= 7; }
+        return r;
+    }
+
+    size_t OverflowBytes(int i, uint64_t v) const
+    {
+        const hw_baz_field& d = f[i];
+        if (d.serialize == HW_BAZ_SIMPLE_OVERFLOW)
+            return SimpleNeeds(v, d.store_signed != 0, d.num_bits) ? (size_t)d.overflow_bytes : 0;
+        if (d.serialize == HW_BAZ_COMPACT_OVERFLOW) return CompactOverflowBytes(v, d.store_signed != 0, d.num_bits);
+        return 0;
+    }
+
+    uint64_t ToBinary(int i, uint64_t v, uint8_t*& ptr) const
+    {
+        const hw_baz_field& d = f[i];
+        const int bits = d.num_bits;
+        if (d.serialize == HW_BAZ_SIMPLE_OVERFLOW)
+        {
+            if (SimpleNeeds(v, d.store_signed != 0, bits))
+            {
+                std::memcpy(ptr, &v, (size_t)d.overflow_bytes);
+                ptr += d.overflow_bytes;
+                return (1ull << bits) - 1;
+            }
+            if (d.store_signed) v += (1ull << (bits - 1)) - 1;
+            return v;
+        }
+        if (d.serialize == HW_BAZ_COMPACT_OVERFLOW)
+        {
+            const uint64_t cmask = 1ull << (bits - 1), vmask = cmask - 1;
+            size_t n = CompactOverflowBytes(v, d.store_signed != 0, bits);
+            uint64_t first = v & vmask;
+            v >>= (bits - 1);
+            if (n) first |= cmask;
+            while (n)
+            {
+                uint8_t b = (uint8_t)(v & 0x7f);
+                v >>= 7;
+                --n;
+                if (n) b |= 0x80;
+                *ptr++ = b;
+            }
+            return first;
+        }
+        return v;
+    }
+
+    // BytesRequired + Serialize of one pulse (PacketBuffer::AddZmw)
+    size_t Bytes(const BazPulse& p, uint64_t* last) const
+    {
+        size_t n = 0;
+        for (size_t g = 0; g < groups.size(); ++g)
+        {
+            n += (size_t)groupBytes[g];
+            for (int i : groups[g]) n += OverflowBytes(i, Value(i, p, last));
+        }
+        return n;
+    }
+
+    uint8_t* Encode(const BazPulse& p, uint8_t* ptr, uint64_t* last) const
+    {
+        for (size_t g = 0; g < groups.size(); ++g)
+        {
+            uint64_t data = 0;
+            uint8_t* ptr2 = ptr + groupBytes[g];
+            size_t pos = 0;
+            for (int i : groups[g])
+            {
+                const int bits = f[i].num_bits;
+                const uint64_t v = ToBinary(i, Value(i, p, last), ptr2);
+                data |= (v & (uint64_t)((1 << bits) - 1)) << pos;
+                pos += (size_t)bits;
+            }
+            std::memcpy(ptr, &data, (size_t)groupBytes[g]);
+            ptr = ptr2;
+        }
+        return ptr;
+    }
+
+    // FieldSerializers.h FromBinary: the main bits `val` plus overflow bytes at ptr
+    uint64_t FromBinary(int i, uint64_t val, const uint8_t*& ptr) const
+    {
+        const hw_baz_field& d = f[i];
+        const int bits = d.num_bits;
+        const bool sgn = d.store_signed != 0;
+        uint64_t ret = val;
+        if (d.serialize == HW_BAZ_TRUNCATE)
+        {
+            if (sgn && (val & (1ull << (bits - 1)))) ret |= (~0ull << bits);
+        }
+        else if (d.serialize == HW_BAZ_SIMPLE_OVERFLOW)
+        {
+            if (val == (1ull << bits) - 1)
+            {
+                ret = 0;
+                std::memcpy(&ret, ptr, (size_t)d.overflow_bytes);
+                ptr += d.overflow_bytes;
+                const int sb = 8 * d.overflow_bytes;
+                if (sgn && (ret & (1ull << (sb - 1)))) ret |= (~0ull << (sb - 1));
+            }
+            else if (sgn) ret = val - ((1ull << (bits - 1)) - 1);
+        }
+        else
+        {
+            const uint64_t cmask = 1ull << (bits - 1);
+            ret = val & (cmask - 1);
+            bool cont = (val & cmask) != 0;
+            int cur = bits - 1;
+            while (cont)
+            {
+                const uint64_t b = *ptr++;
+                cont = (b & 0x80) != 0;
+                ret |= (b & 0x7f) << cur;
+                cur += 7;
+            }
+            if (sgn && (ret & (1ull << (cur - 1)))) ret |= ~0ull << cur;
+        }
+        return ret;
+    }
+
+    // FloatFixedCodec::Revert
+    static float FloatFixedRevert(uint64_t ret, bool sgn, int scale)
+    {
+        if (ret == kFfNan) return kNaN;
+        if (ret == kFfInf) return std::numeric_limits<float>::infinity();
+        if (ret == kFfNinf) return -std::numeric_limits<float>::infinity();
+        if (sgn)
+        {
+            int64_t s = (int64_t)ret;
+            if (s >= 0) s -= (int64_t)kFfOffset;
+            return (float)s / (float)scale;
+        }
+        return (float)(ret - kFfOffset) / (float)scale;
+    }
+
+    // Decode (for round trips)
+    const uint8_t* Decode(const uint8_t* ptr, BazPulse& p, uint64_t* last) const
+    {
+        for (size_t g = 0; g < groups.size(); ++g)
+        {
+            uint64_t data = 0;
+            std::memcpy(&data, ptr, (size_t)groupBytes[g]);
+            ptr += groupBytes[g];
+            for (int i : groups[g])
+            {
+                const hw_baz_field& d = f[i];
+                const int bits = d.num_bits;
+                const uint64_t val = data & (uint64_t)((1 << bits) - 1);
+                data >>= bits;
+                uint64_t ret = FromBinary(i, val, ptr);
+                // the transforms' Revert
+                if (d.transform == HW_BAZ_DELTA) { last[i] += ret; ret = last[i]; }
+                if (d.transform == HW_BAZ_FLOAT_FIXED)
+                {
+                    const float fv = FloatFixedRevert(ret, d.store_signed != 0, d.scale);
+                    if (d.name == HW_BAZ_PKMAX) p.pkmax = fv;
+                    else if (d.name == HW_BAZ_PKMID) p.pkmid = fv;
+                    else if (d.name == HW_BAZ_PKMEAN) p.pkmean = fv;
+                    else p.pkvar = fv;
+                    continue;
+                }
+                if (d.name == HW_BAZ_LABEL) p.label = (uint8_t)ret;
+                else if (d.name == HW_BAZ_START_FRAME) p.start = (uint32_t)ret;
+                else if (d.name == HW_BAZ_PULSE_WIDTH) p.width = (uint16_t)ret;
+                else p.isBase = (uint8_t)ret;
+            }
+        }
+        return ptr;
+    }
+};
+
+// PulseFieldAccessors.h:43-68 on the basecaller's Pulse (signals in 0.1 DN steps)
+BazPulse FromHwPulse(const hw_pulse& p)
+{
+    BazPulse b;
+    b.label = p.label;
+    b.start = p.start;
+    b.width = p.width;
+    b.isBase = p.is_reject ? 0 : 1;
+    b.pkmax = (float)p.max_signal * 0.1f;
+    b.pkmid = p.width < 3 ? kNaN : (float)p.mid_signal * 0.1f;
+    b.pkmean = (float)p.mean_signal * 0.1f;
+    b.pkvar = p.width < 3 ? kNaN : p.signal_m2;
+    return b;
+}
+
+}   // namespace
+
+extern "C" {
+
+// One serializer alone (FieldSerializers.h): ToBinary of val, the main bits
+// masked to num_bits when mask is set, then FromBinary.  *overflow receives
+// OverflowBytes(val); the return value is the decoded value.
+uint64_t or_baz_serializer_roundtrip(int32_t serialize, int32_t numBits, int32_t overflowBytes, int32_t sgn,
+                                     uint64_t val, int32_t mask, uint64_t* overflow)
+{
+    hw_baz_field d{};
+    d.serialize = serialize;
+    d.num_bits = numBits;
+    d.overflow_bytes = overflowBytes;
+    d.store_signed = sgn;
+    BazOracle o(&d, 1);
+    *overflow = o.OverflowBytes(0, val);
+    uint8_t buf[16] = {};
+    uint8_t* w = buf;
+    uint64_t main = o.ToBinary(0, val, w);
+    if (mask) main &= (1ull << numBits) - 1;
+    const uint8_t* r = buf;
+    return o.FromBinary(0, main, r);
+}
+
+// FloatFixedCodec Apply then Revert; *code receives the transformed value.
+float or_baz_float_fixed_roundtrip(float v, int32_t sgn, int32_t scale, int32_t bytes, uint64_t* code)
+{
+    *code = BazOracle::FloatFixed(v, sgn != 0, scale, bytes);
+    return BazOracle::FloatFixedRevert(*code, sgn != 0, scale);
+}
+
+// One ZMW's pulse sequence (field values), encoded with `last` (one uint64 per
+// field) carried in and out.  Returns the byte count; writes at most cap.
+int64_t or_baz_encode_values(const hw_baz_field* fields, uint32_t nf, const void* pulses, uint32_t n, uint8_t* out,
+                             uint64_t cap, uint64_t* last)
+{
+    BazOracle o(fields, nf);
+    const BazPulse* p = static_cast<const BazPulse*>(pulses);
+    std::vector<uint64_t> copy(last, last + nf);
+    size_t need = 0;
+    for (uint32_t i = 0; i < n; ++i) need += o.Bytes(p[i], copy.data());
+    if (need > cap) return -1;
+    uint8_t* ptr = out;
+    for (uint32_t i = 0; i < n; ++i) ptr = o.Encode(p[i], ptr, last);
+    return (int64_t)(ptr - out);
+}
+
+int or_baz_decode_values(const hw_baz_field* fields, uint32_t nf, const uint8_t* bytes, uint32_t n, void* pulses,
+                         uint64_t* last, uint64_t* consumed)
+{
+    BazOracle o(fields, nf);
+    BazPulse* p = static_cast<BazPulse*>(pulses);
+    const uint8_t* ptr = bytes;
+    for (uint32_t i = 0; i < n; ++i)
+    {
+        p[i] = BazPulse{};
+        ptr = o.Decode(ptr, p[i], last);
+    }
+    *consumed = (uint64_t)(ptr - bytes);
+    return HW_OK;
+}
+
+// PrelimHQFilter + PacketBuffer::AddZmw over a chunk of the basecaller's
+// pulses: per ZMW the kept pulses in order, bytes appended to out;
+// offsets[numZmw + 1].  last[numZmw][nf] carries the delta state.
+int or_baz_encode_chunk(const hw_baz_field* fields, uint32_t nf, int32_t skipRejects, uint32_t numZmw,
+                        const hw_pulse* pulses, const uint32_t* lens, uint32_t cap, uint8_t* out, uint64_t outCap,
+                        uint64_t* offsets, uint64_t* last)
+{
+    BazOracle o(fields, nf);
+    uint64_t pos = 0;
+    for (uint32_t z = 0; z < numZmw; ++z)
+    {
+        offsets[z] = pos;
+        const uint32_t n = std::min(lens[z], cap);
+        for (uint32_t i = 0; i < n; ++i)
+        {
+            const hw_pulse& hp = pulses[(size_t)z * cap + i];
+            if (skipRejects && hp.is_reject) continue;
+            const BazPulse b = FromHwPulse(hp);
+            std::vector<uint64_t> copy(last + (size_t)z * nf, last + (size_t)(z + 1) * nf);
+            const size_t need = o.Bytes(b, copy.data());
+            if (pos + need > outCap) return HW_ERR_OUT_OF_MEMORY;
+            uint8_t* end = o.Encode(b, out + pos, last + (size_t)z * nf);
+            pos = (uint64_t)(end - out);
+        }
+    }
+    offsets[numZmw] = pos;
+    return HW_OK;
+}
+
+}   // extern "C"

@@ -69,6 +69,14 @@ def lib():
         L.or_hf_set_cart.argtypes = [vp, vp, vp, vp, vp, vp, u32, vp, C.c_float]
         L.or_hf_process.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp, i32, u32, vp, C.POINTER(i32)]
         L.or_repack.argtypes = [u32, u32, u32, i32, vp, u32, vp, i32, vp]
+        L.or_baz_encode_values.argtypes = [vp, u32, vp, u32, vp, C.c_uint64, vp]
+        L.or_baz_encode_values.restype = C.c_int64
+        L.or_baz_decode_values.argtypes = [vp, u32, vp, u32, vp, vp, C.POINTER(C.c_uint64)]
+        L.or_baz_serializer_roundtrip.argtypes = [i32, i32, i32, i32, C.c_uint64, i32, C.POINTER(C.c_uint64)]
+        L.or_baz_serializer_roundtrip.restype = C.c_uint64
+        L.or_baz_float_fixed_roundtrip.argtypes = [C.c_float, i32, i32, i32, C.POINTER(C.c_uint64)]
+        L.or_baz_float_fixed_roundtrip.restype = C.c_float
+        L.or_baz_encode_chunk.argtypes = [vp, u32, i32, u32, vp, vp, u32, vp, C.c_uint64, vp, vp]
         _lib = L
     return _lib
 
@@ -281,3 +289,73 @@ def repack(num_zmw, lanes_per_pool, frames_per_chunk, encoding, packets, data, c
     ptrs = (C.c_void_p * len(pool_chunks))(*[c.ctypes.data for c in pool_chunks])
     _check(lib().or_repack(num_zmw, lanes_per_pool, frames_per_chunk, encoding, abi.ptr(packets), len(packets),
                            abi.ptr(data), int(chunk_first_frame), ptrs))
+
+
+# the field values of one pulse (struct BazPulse of the oracle)
+BAZ_PULSE_DT = np.dtype([("label", np.uint8), ("start", np.uint32), ("width", np.uint16), ("is_base", np.uint8),
+                         ("pkmax", np.float32), ("pkmid", np.float32), ("pkmean", np.float32),
+                         ("pkvar", np.float32)], align=True)
+
+
+def baz_encode_values(fields, pulses, last=None):
+    """One ZMW's pulses (BAZ_PULSE_DT) encoded with the field list; `last`
+    (uint64 per field, delta state) is updated.  Returns the bytes."""
+    fields = np.ascontiguousarray(fields, abi.BAZ_FIELD_DT)
+    pulses = np.ascontiguousarray(pulses, BAZ_PULSE_DT)
+    last = np.zeros(len(fields), np.uint64) if last is None else last
+    cap = 64 * len(pulses) * len(fields) + 64
+    out = np.zeros(cap, np.uint8)
+    n = lib().or_baz_encode_values(abi.ptr(fields), len(fields), abi.ptr(pulses), len(pulses), abi.ptr(out), cap,
+                                   abi.ptr(last))
+    if n < 0:
+        raise RuntimeError("oracle: BAZ buffer too small")
+    return out[:n].copy()
+
+
+def baz_serializer_roundtrip(serialize, num_bits, overflow_bytes, signed, value, mask=True):
+    """One serializer: (decoded value as uint64, overflow bytes of the value)."""
+    ov = C.c_uint64()
+    r = lib().or_baz_serializer_roundtrip(serialize, num_bits, overflow_bytes, int(signed), value & (2**64 - 1),
+                                          int(mask), C.byref(ov))
+    return r, ov.value
+
+
+def baz_float_fixed_roundtrip(v, signed, scale, nbytes):
+    """FloatFixedCodec: (reverted float, code)."""
+    code = C.c_uint64()
+    r = lib().or_baz_float_fixed_roundtrip(float(v), int(signed), scale, nbytes, C.byref(code))
+    return np.float32(r), code.value
+
+
+def baz_decode_values(fields, data, n, last=None):
+    """Inverse of baz_encode_values: (pulses, bytes consumed)."""
+    fields = np.ascontiguousarray(fields, abi.BAZ_FIELD_DT)
+    data = np.ascontiguousarray(data, np.uint8)
+    last = np.zeros(len(fields), np.uint64) if last is None else last
+    out = np.zeros(n, BAZ_PULSE_DT)
+    used = C.c_uint64()
+    _check(lib().or_baz_decode_values(abi.ptr(fields), len(fields), abi.ptr(data), n, abi.ptr(out), abi.ptr(last),
+                                      C.byref(used)))
+    return out, used.value
+
+
+class BazEncoder:
+    """PrelimHQFilter + PacketBuffer::AddZmw over chunks of the basecaller's
+    pulses ([num_zmw][cap] abi.PULSE_DT); per-ZMW delta state kept."""
+
+    def __init__(self, fields, skip_rejects, num_zmw):
+        self.fields = np.ascontiguousarray(fields, abi.BAZ_FIELD_DT)
+        self.skip = int(bool(skip_rejects))
+        self.num_zmw = num_zmw
+        self.last = np.zeros((num_zmw, len(self.fields)), np.uint64)
+
+    def __call__(self, pulses, lens, cap):
+        pulses = np.ascontiguousarray(pulses, abi.PULSE_DT)
+        lens = np.ascontiguousarray(lens, np.uint32)
+        out_cap = int(lens.sum()) * (8 * len(self.fields) + 8) + 16
+        out = np.zeros(out_cap, np.uint8)
+        offsets = np.zeros(self.num_zmw + 1, np.uint64)
+        _check(lib().or_baz_encode_chunk(abi.ptr(self.fields), len(self.fields), self.skip, self.num_zmw,
+                                         abi.ptr(pulses), abi.ptr(lens), int(cap), abi.ptr(out), out_cap,
+                                         abi.ptr(offsets), abi.ptr(self.last)))
+        return out[:int(offsets[-1])].copy(), offsets
