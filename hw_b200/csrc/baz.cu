@@ -8,14 +8,22 @@
 // the per-ZMW append of PrelimHQFilter / PacketBuffer::AddZmw
 // (basecaller/appModules/PrelimHQFilter.cpp:95-118, bazio/writing/PacketBuffer.h:143-210).
 //
-// One thread per ZMW.  Pass 1 sizes every ZMW's bytes for the chunk (on a
-// copy of its delta state), an exclusive scan places the ZMWs one after the
-// other, pass 2 encodes each ZMW's pulses at its offset and advances the
-// state.
+// One launch, pulse-parallel.  A CTA takes a tile of 128 ZMWs (tiles handed
+// out in launch order by a ticket); each of its 256 threads takes a
+// contiguous run of the tile's pulses.  A pulse's bytes depend only on the
+// pulse and, for delta-coded fields, on the previous kept pulse of its ZMW
+// (or the ZMW's state from the previous chunk), so a run is sized on its
+// own.  Sweep 1 sizes the runs (pulses loaded four at a time); one block
+// scan places the runs in the tile; a decoupled look-back over the tiles
+// before it places the tile in the output; sweep 2 writes every run at its
+// place (the pulses come from L1/L2 the second time).  The delta state is
+// double-buffered: a call reads one copy and writes the other, and the call's
+// last tile switches copies when the whole chunk fit in the buffer.
+#include <atomic>
 #include <string>
-#include <vector>
 
-#include <cub/device/device_scan.cuh>
+#include <cub/block/block_reduce.cuh>
+#include <cub/block/block_scan.cuh>
 
 #include "hw_device.cuh"
 
@@ -24,38 +32,101 @@ using namespace hwk;
 namespace {
 
 constexpr int kMaxFields = 16;
+constexpr int kTileRows = 128;       // ZMWs a tile
+constexpr int kThreads = 256;        // runs of pulses a tile
 constexpr uint64_t kFfNan = 0, kFfInf = 1, kFfNinf = 2, kFfOffset = 3;   // FloatFixedCodec codes
+// look-back flags (top two bits of a tile's word): count published, inclusive total published
+constexpr unsigned long long kFlagAgg = 1ull << 62, kFlagInc = 2ull << 62;
+constexpr int kSpinLimit = 1 << 22;  // polls of a predecessor's status (about 0.4 s) before giving up
 
 struct BazSpec
 {
     hw_baz_field f[kMaxFields];
     int groupEnd[kMaxFields];     // 1: the field closes its group
     int groupBytes[kMaxFields];   // nominal bytes of the group a field opens (0 elsewhere)
+    int slot[kMaxFields];         // delta-state slot of a delta-coded field
     int n;
     int skipRejects;
+    int slots;                    // delta-coded fields
 };
 
-struct BazPulseVals
+// ---- field lists: the runtime one, and the basecaller's two as constants ----
+
+struct RtFields
 {
-    uint32_t label, start, width, isBase;
-    float pkmax, pkmid, pkmean, pkvar;
+    const BazSpec& S;
+    __device__ explicit RtFields(const BazSpec& s) : S(s) {}
+    __device__ int n() const { return S.n; }
+    __device__ hw_baz_field f(int i) const { return S.f[i]; }
+    __device__ int groupBytes(int i) const { return S.groupBytes[i]; }
+    __device__ bool groupEnd(int i) const { return S.groupEnd[i] != 0; }
+    __device__ int slot(int i) const { return S.slot[i]; }
+    __device__ bool skip() const { return S.skipRejects != 0; }
+    __device__ bool hasDelta() const { return S.slots > 0; }
 };
 
-__device__ __forceinline__ BazPulseVals Values(const hw_pulse& p)
+// PulseGroups.h:42-53
+struct ProductionFields
 {
-    const float nan = __int_as_float(0x7fc00000);
-    BazPulseVals v;
-    v.label = p.label;
-    v.start = p.start;
-    v.width = p.width;
-    v.isBase = p.is_reject ? 0u : 1u;
-    v.pkmax = __fmul_rn((float)p.max_signal, 0.1f);
-    v.pkmid = p.width < 3 ? nan : __fmul_rn((float)p.mid_signal, 0.1f);
-    v.pkmean = __fmul_rn((float)p.mean_signal, 0.1f);
-    v.pkvar = p.width < 3 ? nan : p.signal_m2;
-    return v;
+    __device__ explicit ProductionFields(const BazSpec&) {}
+    __host__ __device__ static constexpr int n() { return 3; }
+    __host__ __device__ static constexpr hw_baz_field f(int i)
+    {
+        return i == 0 ? hw_baz_field{HW_BAZ_LABEL, 0, HW_BAZ_NOOP, 0, 0, HW_BAZ_TRUNCATE, 2, 0}
+             : i == 1 ? hw_baz_field{HW_BAZ_PULSE_WIDTH, 0, HW_BAZ_NOOP, 0, 0, HW_BAZ_COMPACT_OVERFLOW, 7, 0}
+                      : hw_baz_field{HW_BAZ_START_FRAME, 0, HW_BAZ_DELTA, 0, 0, HW_BAZ_COMPACT_OVERFLOW, 7, 0};
+    }
+    __host__ __device__ static constexpr int groupBytes(int i) { return i == 0 ? 2 : 0; }
+    __host__ __device__ static constexpr bool groupEnd(int i) { return i == 2; }
+    __host__ __device__ static constexpr int slot(int) { return 0; }
+    __host__ __device__ static constexpr bool skip() { return true; }
+    __host__ __device__ static constexpr bool hasDelta() { return true; }
+};
+
+// PulseGroups.h:55-94
+struct InternalFields
+{
+    __device__ explicit InternalFields(const BazSpec&) {}
+    __host__ __device__ static constexpr int n() { return 8; }
+    __host__ __device__ static constexpr hw_baz_field f(int i)
+    {
+        return i < 3 ? ProductionFields::f(i)
+             : i == 3 ? hw_baz_field{HW_BAZ_PKMAX, 1, HW_BAZ_FLOAT_FIXED, 10, 2, HW_BAZ_SIMPLE_OVERFLOW, 8, 2}
+             : i == 4 ? hw_baz_field{HW_BAZ_PKMID, 1, HW_BAZ_FLOAT_FIXED, 10, 2, HW_BAZ_SIMPLE_OVERFLOW, 8, 2}
+             : i == 5 ? hw_baz_field{HW_BAZ_PKMEAN, 1, HW_BAZ_FLOAT_FIXED, 10, 2, HW_BAZ_SIMPLE_OVERFLOW, 8, 2}
+             : i == 6 ? hw_baz_field{HW_BAZ_PKVAR, 0, HW_BAZ_FLOAT_FIXED, 10, 2, HW_BAZ_SIMPLE_OVERFLOW, 7, 2}
+                      : hw_baz_field{HW_BAZ_IS_BASE, 0, HW_BAZ_NOOP, 0, 0, HW_BAZ_TRUNCATE, 1, 0};
+    }
+    // groups: {Label, PulseWidth, StartFrame} 2 bytes, {Pkmax}, {Pkmid}, {Pkmean}, {Pkvar, IsBase} 1 byte each
+    __host__ __device__ static constexpr int groupBytes(int i) { return i == 0 ? 2 : (i >= 3 && i <= 6) ? 1 : 0; }
+    __host__ __device__ static constexpr bool groupEnd(int i) { return i == 2 || i == 3 || i == 4 || i == 5 || i == 7; }
+    __host__ __device__ static constexpr int slot(int) { return 0; }
+    __host__ __device__ static constexpr bool skip() { return false; }
+    __host__ __device__ static constexpr bool hasDelta() { return true; }
+};
+
+// ---- one field: value, transform, serializer ----------------------------------
+
+__device__ __forceinline__ uint64_t RawField(int name, const hw_pulse& p)
+{
+    return name == HW_BAZ_LABEL ? (uint64_t)p.label
+         : name == HW_BAZ_START_FRAME ? (uint64_t)p.start
+         : name == HW_BAZ_PULSE_WIDTH ? (uint64_t)p.width
+                                      : (uint64_t)(p.is_reject ? 0u : 1u);
 }
 
+// Pulse::MaxSignal / MidSignal / MeanSignal / SignalM2 (Pulse.h:105-127):
+// fixed-point signals in 0.1 steps, NaN mid signal and M2 below width 3
+__device__ __forceinline__ float FloatField(int name, const hw_pulse& p)
+{
+    const float nan = __int_as_float(0x7fc00000);
+    if (name == HW_BAZ_PKMAX) return __fmul_rn((float)p.max_signal, 0.1f);
+    if (name == HW_BAZ_PKMID) return p.width < 3 ? nan : __fmul_rn((float)p.mid_signal, 0.1f);
+    if (name == HW_BAZ_PKMEAN) return __fmul_rn((float)p.mean_signal, 0.1f);
+    return p.width < 3 ? nan : p.signal_m2;
+}
+
+// FloatFixedCodec::Apply (FieldTransforms.h:207-251)
 __device__ __forceinline__ uint64_t FloatFixed(float v, bool sgn, int scale, int bytes)
 {
     float scaled = roundf(__fmul_rn(v, (float)scale));
@@ -77,24 +148,12 @@ __device__ __forceinline__ uint64_t FloatFixed(float v, bool sgn, int scale, int
     return scaled < 0 ? kFfNinf : kFfInf;
 }
 
-// Transformed value of field i; the delta state of the field advances.
-__device__ __forceinline__ uint64_t FieldValue(const hw_baz_field& d, const BazPulseVals& p, uint64_t& last)
+__device__ __forceinline__ uint64_t FieldValue(const hw_baz_field& d, const hw_pulse& p, uint64_t prev)
 {
     if (d.transform == HW_BAZ_FLOAT_FIXED)
-    {
-        const float v = d.name == HW_BAZ_PKMAX ? p.pkmax : d.name == HW_BAZ_PKMID ? p.pkmid
-                      : d.name == HW_BAZ_PKMEAN ? p.pkmean : p.pkvar;
-        return FloatFixed(v, d.store_signed != 0, d.scale, d.transform_bytes);
-    }
-    const uint64_t raw = d.name == HW_BAZ_LABEL ? p.label : d.name == HW_BAZ_START_FRAME ? p.start
-                       : d.name == HW_BAZ_PULSE_WIDTH ? p.width : p.isBase;
-    if (d.transform == HW_BAZ_DELTA)
-    {
-        const uint64_t r = raw - last;
-        last = raw;
-        return r;
-    }
-    return raw;
+        return FloatFixed(FloatField(d.name, p), d.store_signed != 0, d.scale, d.transform_bytes);
+    const uint64_t raw = RawField(d.name, p);
+    return d.transform == HW_BAZ_DELTA ? raw - prev : raw;   // DeltaCompression::Apply
 }
 
 __device__ __forceinline__ bool SimpleNeeds(uint64_t v, bool sgn, int bits)
@@ -109,14 +168,12 @@ __device__ __forceinline__ int CompactBytes(uint64_t t, bool sgn, int bits)
     {
         // leading bits equal to the sign bit, beyond the first
         const uint64_t u = ((int64_t)t < 0) ? ~t : t;
-        const int discard = __clzll(u) - 1;
-        const int keep = 64 - discard - (bits - 1);
+        const int keep = 64 - (__clzll(u) - 1) - (bits - 1);
         return (keep + 6) / 7;
     }
-    t >>= (bits - 1);
-    int r = 0;
-    while (t) { ++r; t >>= 7; }
-    return r;
+    // 7-bit groups of the bits above the main portion
+    const int above = 64 - __clzll(t >> (bits - 1));
+    return (above + 6) / 7;
 }
 
 __device__ __forceinline__ int OverflowBytes(const hw_baz_field& d, uint64_t v)
@@ -161,86 +218,434 @@ __device__ __forceinline__ uint64_t ToBinary(const hw_baz_field& d, uint64_t v, 
     return v;
 }
 
-__device__ __forceinline__ int PulseBytes(const BazSpec& S, const BazPulseVals& p, uint64_t* last)
+// ---- one pulse -----------------------------------------------------------------
+
+template <class Spec>
+__device__ __forceinline__ uint32_t PulseBytes(const Spec& F, const hw_pulse& p, const uint64_t (&prev)[kMaxFields])
 {
-    int n = 0;
-    for (int i = 0; i < S.n; ++i) n += S.groupBytes[i] + OverflowBytes(S.f[i], FieldValue(S.f[i], p, last[i]));
+    uint32_t n = 0;
+#pragma unroll
+    for (int i = 0; i < kMaxFields; ++i)
+    {
+        if (i >= F.n()) break;
+        const hw_baz_field d = F.f(i);
+        n += (uint32_t)F.groupBytes(i) + (uint32_t)OverflowBytes(d, FieldValue(d, p, prev[i]));
+    }
     return n;
 }
 
-__device__ __forceinline__ uint8_t* EncodePulse(const BazSpec& S, const BazPulseVals& p, uint8_t* ptr, uint64_t* last)
+// Groups in order: main bytes little-endian, then the group's overflow bytes
+// in field order (ObjectToBaz.h GroupEncoder::Encode).
+template <class Spec>
+__device__ __forceinline__ uint8_t* EncodePulse(const Spec& F, const hw_pulse& p, const uint64_t (&prev)[kMaxFields],
+                                                uint8_t* ptr)
 {
     uint64_t data = 0;
     int pos = 0, gBytes = 0;
     uint8_t* main = ptr;
     uint8_t* ov = ptr;
-    for (int i = 0; i < S.n; ++i)
+#pragma unroll
+    for (int i = 0; i < kMaxFields; ++i)
     {
-        if (S.groupBytes[i])
+        if (i >= F.n()) break;
+        const hw_baz_field d = F.f(i);
+        if (F.groupBytes(i))
         {
-            // a new group: main bytes first, overflow bytes after them
             main = ov;
-            gBytes = S.groupBytes[i];
+            gBytes = F.groupBytes(i);
             ov = main + gBytes;
             data = 0;
             pos = 0;
         }
-        const int bits = S.f[i].num_bits;
-        const uint64_t v = ToBinary(S.f[i], FieldValue(S.f[i], p, last[i]), ov);
-        data |= (v & (uint64_t)((1 << bits) - 1)) << pos;
-        pos += bits;
-        if (S.groupEnd[i])
+        const uint64_t v = ToBinary(d, FieldValue(d, p, prev[i]), ov);
+        data |= (v & (uint64_t)((1 << d.num_bits) - 1)) << pos;
+        pos += d.num_bits;
+        if (F.groupEnd(i))
             for (int b = 0; b < gBytes; ++b) main[b] = (uint8_t)(data >> (8 * b));
     }
     return ov;
 }
 
-// Pass 1: offsets[z] = the bytes of ZMW z this chunk (on a copy of its
-// delta state); offsets[numZmw] = 0, so the exclusive scan that follows
-// leaves the total there.
-__global__ void BazSizeKernel(BazSpec S, const hw_pulse* pulses, const uint32_t* lens, int cap, int numZmw,
-                              const uint64_t* state, uint64_t* offsets)
+template <class Spec>
+__device__ __forceinline__ void KeepPrev(const Spec& F, const hw_pulse& p, uint64_t (&prev)[kMaxFields])
 {
-    const int z = blockIdx.x * blockDim.x + threadIdx.x;
-    if (z == 0) offsets[numZmw] = 0;
-    if (z >= numZmw) return;
-    uint64_t last[kMaxFields];
-    for (int i = 0; i < S.n; ++i) last[i] = state[(size_t)z * kMaxFields + i];
-    uint64_t bytes = 0;
-    const hw_pulse* row = pulses + (size_t)z * cap;
-    const uint32_t n = min(lens[z], (uint32_t)cap);   // counts past the slots are clamped
-    for (uint32_t k = 0; k < n; ++k)
+#pragma unroll
+    for (int i = 0; i < kMaxFields; ++i)
     {
-        const hw_pulse p = row[k];
-        if (S.skipRejects && p.is_reject) continue;
-        bytes += (uint64_t)PulseBytes(S, Values(p), last);
+        if (i >= F.n()) break;
+        const hw_baz_field d = F.f(i);
+        if (d.transform == HW_BAZ_DELTA) prev[i] = RawField(d.name, p);
     }
-    offsets[z] = bytes;
 }
 
-// Pass 2: each ZMW's pulses at its offset; the delta state advances.  When
-// the chunk needs more than `capacity` bytes nothing is written and the
-// state stays.  The total goes to the mapped host word.
-__global__ void BazEncodeKernel(BazSpec S, const hw_pulse* pulses, const uint32_t* lens, int cap, int numZmw,
-                                uint64_t* state, const uint64_t* offsets, uint8_t* out, uint64_t capacity,
-                                volatile uint64_t* hostTotal)
+struct TileArgs
 {
-    const int z = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint64_t total = offsets[numZmw];
-    if (z == 0) *hostTotal = total;
-    if (z >= numZmw || total > capacity) return;
-    uint64_t last[kMaxFields];
-    for (int i = 0; i < S.n; ++i) last[i] = state[(size_t)z * kMaxFields + i];
-    uint8_t* ptr = out + offsets[z];
-    const hw_pulse* row = pulses + (size_t)z * cap;
-    const uint32_t n = min(lens[z], (uint32_t)cap);   // counts past the slots are clamped
-    for (uint32_t k = 0; k < n; ++k)
+    const hw_pulse* pulses;
+    const uint32_t* lens;
+    uint32_t cap, numZmw, numTiles;
+    uint32_t zmwStride;               // ZMWs of a lane encoded: every zmwStride-th
+    uint64_t* state;                  // [2][slots][numZmw]; *cur names the copy this call reads
+    uint32_t* cur;
+    uint64_t* offsets;                // [numZmw + 1]
+    uint8_t* out;
+    uint64_t capacity;
+    unsigned long long* status;       // [numTiles] look-back words
+    unsigned long long* ticket;
+    unsigned long long ticketBase;    // tickets taken by earlier calls
+    unsigned long long epoch;         // this call's tag in the look-back words
+    volatile uint64_t* host;          // mapped: [0] total bytes, [1] look-back gave up, [2] encoded
+};
+
+// look-back words: flag (2 bits) | call epoch (20 bits) | byte count (42 bits)
+constexpr int kEpochShift = 42;
+constexpr unsigned long long kCountMask = (1ull << kEpochShift) - 1;
+
+__device__ __forceinline__ void StoreRelease(unsigned long long* p, unsigned long long v)
+{
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ void StoreRelaxed(unsigned long long* p, unsigned long long v)
+{
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Relaxed: the counts are the only data the tiles exchange, and an acquire
+// load would drop the pulses this SM holds in L1.
+__device__ __forceinline__ unsigned long long LoadRelaxed(const unsigned long long* p)
+{
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// The tile's byte count, published as soon as it is known (the first tile's
+// is its inclusive total).  Release: the tile read the state-copy word
+// before, which the last tile may switch once it has seen every count.
+__device__ __forceinline__ void PublishCount(const TileArgs& a, uint32_t tile, uint64_t agg)
+{
+    const unsigned long long tag = a.epoch << kEpochShift;
+    StoreRelease(a.status + tile, (tile == 0 ? kFlagInc : kFlagAgg) | tag | agg);
+}
+
+// Decoupled look-back by one warp: sum the counts of the tiles before this
+// one back to the nearest one whose inclusive total is known, publish this
+// tile's inclusive total.  Words of earlier calls (another epoch) read as
+// not ready.  Tiles are taken in ticket order, so every tile waited on has
+// started and publishes its count without waiting; the polls are bounded
+// all the same.
+__device__ uint64_t LookBack(const TileArgs& a, uint32_t tile, uint64_t agg, bool& gaveUp)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned long long tag = a.epoch << kEpochShift;
+    gaveUp = false;
+    if (tile == 0) return 0;
+    uint64_t excl = 0;
+    int hi = (int)tile - 1;
+    int spins = 0;
+    while (true)
     {
-        const hw_pulse p = row[k];
-        if (S.skipRejects && p.is_reject) continue;
-        ptr = EncodePulse(S, Values(p), ptr, last);
+        const int idx = hi - lane;
+        unsigned long long w = idx >= 0 ? LoadRelaxed(a.status + idx) : (kFlagInc | tag);
+        const bool mine = ((w >> kEpochShift) & 0xfffff) == a.epoch;
+        const int flag = mine ? (int)(w >> 62) : 0;
+        if (__ballot_sync(~0u, flag == 0))
+        {
+            if (++spins > kSpinLimit)
+            {
+                gaveUp = true;
+                if (lane == 0) a.host[1] = 1;
+                break;
+            }
+            __nanosleep(100);
+            continue;
+        }
+        const uint32_t inc = __ballot_sync(~0u, flag == 2);
+        const int stop = inc ? __ffs(inc) - 1 : 31;
+        uint64_t v = lane <= stop ? (w & kCountMask) : 0;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(~0u, v, o);
+        excl += v;
+        if (inc) break;
+        hi -= 32;
     }
-    for (int i = 0; i < S.n; ++i) state[(size_t)z * kMaxFields + i] = last[i];
+    if (lane == 0) StoreRelaxed(a.status + tile, kFlagInc | tag | (excl + agg));
+    return excl;
+}
+
+constexpr int kPulseStage = 2048;   // pulses of a tile held in shared memory
+
+// Bytes of shared memory for a tile's encoded bytes (tiles with more are
+// written straight to the output); a production pulse is about 2 bytes.
+template <class Spec> struct OutStage { static constexpr int bytes = 24 * 1024; };
+template <> struct OutStage<ProductionFields> { static constexpr int bytes = 8 * 1024; };
+
+template <class Spec>
+constexpr int DynSmem() { return kPulseStage * (int)sizeof(hw_pulse) + OutStage<Spec>::bytes + 32; }
+
+__device__ __forceinline__ void CpAsync4(void* dst, const void* src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+
+__device__ __forceinline__ void CpAsync8(void* dst, const void* src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+
+struct TileView
+{
+    const TileArgs& a;
+    uint32_t z0;
+    const uint32_t* rowStart;    // [kTileRows + 1]
+    const hw_pulse* pstage;      // the tile's first kPulseStage pulses
+    const uint64_t* state0;      // slot 0 of each ZMW's delta state
+    const uint64_t* stateCur;
+    uint64_t* stateNext;
+    // pulse i of the tile, slot k of its ZMW r
+    __device__ __forceinline__ hw_pulse At(uint32_t i, int r, int k) const
+    {
+        return i < (uint32_t)kPulseStage ? pstage[i] : a.pulses[(size_t)(z0 + r) * a.cap + k];
+    }
+    __device__ __forceinline__ uint64_t State(int slot, int r) const
+    {
+        return slot == 0 ? state0[r] : stateCur[(size_t)slot * a.numZmw + z0 + r];
+    }
+};
+
+// One thread's contiguous run of the tile's pulses [i0, i1): sized, with
+// the run-relative byte offset of each ZMW starting in it and the delta
+// state after each ZMW ending in it (sweep 1), or written at `out` (sweep
+// 2).  Returns the run's bytes.
+template <class Spec, bool Write>
+__device__ __forceinline__ uint32_t Run(const Spec& F, const TileView& t, uint32_t i0, uint32_t i1, uint8_t* out,
+                                        uint32_t* rowLocal)
+{
+    if (i0 >= i1) return 0;
+    int lo = 0, hi = kTileRows;   // the ZMW of pulse i0: the last with rowStart <= i0
+    while (hi - lo > 1)
+    {
+        const int mid = (lo + hi) >> 1;
+        if (t.rowStart[mid] <= i0) lo = mid; else hi = mid;
+    }
+    int r = lo, k = (int)(i0 - t.rowStart[lo]);
+    uint32_t rowLen = t.rowStart[r + 1] - t.rowStart[r];
+    uint64_t prev[kMaxFields];
+    if (F.hasDelta())
+    {
+        // the kept pulse before the run in its ZMW, or the ZMW's state
+        int j = k - 1;
+        hw_pulse q;
+        while (j >= 0)
+        {
+            q = t.At(i0 - (uint32_t)(k - j), r, j);
+            if (!(F.skip() && q.is_reject)) break;
+            --j;
+        }
+#pragma unroll
+        for (int f = 0; f < kMaxFields; ++f)
+        {
+            if (f >= F.n()) break;
+            const hw_baz_field d = F.f(f);
+            if (d.transform == HW_BAZ_DELTA) prev[f] = j >= 0 ? RawField(d.name, q) : t.State(F.slot(f), r);
+        }
+    }
+    uint32_t bytes = 0;
+    for (uint32_t i = i0; i < i1; ++i)
+    {
+        const hw_pulse p = t.At(i, r, k);
+        if (k == 0)
+        {
+            if (!Write) rowLocal[r] = bytes;
+#pragma unroll
+            for (int f = 0; f < kMaxFields; ++f)
+            {
+                if (f >= F.n()) break;
+                const hw_baz_field d = F.f(f);
+                if (d.transform == HW_BAZ_DELTA) prev[f] = t.State(F.slot(f), r);
+            }
+        }
+        if (!(F.skip() && p.is_reject))
+        {
+            if (Write) bytes = (uint32_t)(EncodePulse(F, p, prev, out + bytes) - out);
+            else bytes += PulseBytes(F, p, prev);
+            KeepPrev(F, p, prev);
+        }
+        if ((uint32_t)++k == rowLen)
+        {
+            if (!Write)
+            {
+                // the ZMW's last pulse: the next chunk's delta state (the last
+                // kept pulse's values, or the state it came in with)
+#pragma unroll
+                for (int f = 0; f < kMaxFields; ++f)
+                {
+                    if (f >= F.n()) break;
+                    const hw_baz_field d = F.f(f);
+                    if (d.transform == HW_BAZ_DELTA)
+                        t.stateNext[(size_t)F.slot(f) * t.a.numZmw + t.z0 + r] = prev[f];
+                }
+            }
+            // the next ZMW with pulses
+            do { ++r; } while (r < kTileRows && t.rowStart[r + 1] == t.rowStart[r]);
+            k = 0;
+            rowLen = r < kTileRows ? t.rowStart[r + 1] - t.rowStart[r] : 0;
+        }
+    }
+    return bytes;
+}
+
+template <class Spec>
+__global__ void __launch_bounds__(kThreads) BazTileKernel(const __grid_constant__ BazSpec S, const TileArgs a)
+{
+    using Scan = cub::BlockScan<uint32_t, kThreads>;
+    constexpr int kOut = OutStage<Spec>::bytes;
+    __shared__ typename Scan::TempStorage scanTmp;
+    __shared__ uint32_t rowStart[kTileRows + 1];   // tile pulse index of each ZMW's first pulse
+    __shared__ uint32_t rowLocal[kTileRows];       // byte offset of a ZMW's first pulse in its run
+    __shared__ uint32_t runOffSh[kThreads];        // tile byte offset of each thread's run
+    __shared__ uint64_t state0[kTileRows];         // slot 0 of the delta state
+    __shared__ uint32_t tileSh, curSh;
+    __shared__ uint64_t prefixSh;
+    __shared__ int gaveUpSh;
+    extern __shared__ __align__(16) uint8_t dyn[];
+    hw_pulse* pstage = reinterpret_cast<hw_pulse*>(dyn);
+    uint32_t* ostage = reinterpret_cast<uint32_t*>(dyn + kPulseStage * sizeof(hw_pulse));   // then 32 bytes of slack
+    const Spec F(S);
+    const int tid = threadIdx.x;
+    if (tid == 0)
+    {
+        tileSh = (uint32_t)(atomicAdd(a.ticket, 1ull) - a.ticketBase);
+        curSh = *a.cur;
+    }
+    __syncthreads();
+    const uint32_t tile = tileSh;
+    const uint32_t z0 = tile * kTileRows;
+    const size_t plane = (size_t)(S.slots ? S.slots : 1) * a.numZmw;
+    const uint64_t* stateCur = a.state + curSh * plane;
+    uint64_t* stateNext = a.state + (1 - curSh) * plane;
+    uint32_t cnt = 0;
+    if (tid < kTileRows && z0 + tid < a.numZmw && ((z0 + tid) & 63) % a.zmwStride == 0)
+        cnt = min(a.lens[z0 + tid], a.cap);   // counts past the slots clamp
+    uint32_t excl, P;
+    Scan(scanTmp).ExclusiveSum(cnt, excl, P);
+    if (tid < kTileRows)
+    {
+        rowStart[tid] = excl;
+        if (z0 + tid < a.numZmw && F.hasDelta()) CpAsync8(&state0[tid], stateCur + z0 + tid);
+        if (z0 + tid < a.numZmw && cnt == 0)
+        {
+            // no pulses this chunk: the state carries over
+#pragma unroll
+            for (int f = 0; f < kMaxFields; ++f)
+            {
+                if (f >= F.n()) break;
+                const hw_baz_field d = F.f(f);
+                if (d.transform != HW_BAZ_DELTA) continue;
+                const size_t s = (size_t)F.slot(f) * a.numZmw + z0 + tid;
+                stateNext[s] = stateCur[s];
+            }
+        }
+    }
+    if (tid == 0) rowStart[kTileRows] = P;
+    __syncthreads();
+    {
+        // the tile's pulses (up to kPulseStage) into shared memory, each
+        // warp a ZMW at a time in 4-byte words: 128 contiguous bytes a step
+        const int warp = tid >> 5, lane = tid & 31;
+        constexpr int kWords = sizeof(hw_pulse) / 4;
+        for (int r = warp; r < kTileRows; r += kThreads / 32)
+        {
+            const uint32_t first = rowStart[r];
+            if (first >= (uint32_t)kPulseStage) break;
+            const uint32_t n = min(rowStart[r + 1], (uint32_t)kPulseStage) - first;
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(a.pulses + (size_t)(z0 + r) * a.cap);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(pstage + first);
+            for (uint32_t w = lane; w < n * kWords; w += 32) CpAsync4(dst + w, src + w);
+        }
+        asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+    }
+    __syncthreads();
+    const TileView tv{a, z0, rowStart, pstage, state0, stateCur, stateNext};
+
+    // sweep 1: each thread sizes a contiguous run of the tile's pulses
+    const uint32_t per = (P + kThreads - 1) / kThreads;
+    const uint32_t i0 = min(P, tid * per), i1 = min(P, i0 + per);
+    const uint32_t mine = Run<Spec, false>(F, tv, i0, i1, nullptr, rowLocal);
+    uint32_t runOff, tileBytes;
+    Scan(scanTmp).ExclusiveSum(mine, runOff, tileBytes);
+    runOffSh[tid] = runOff;
+    if (tid == 0) PublishCount(a, tile, tileBytes);
+    // sweep 2 into shared memory before the look-back, when the tile fits
+    const bool staged = tileBytes <= (uint32_t)kOut;
+    if (staged) Run<Spec, true>(F, tv, i0, i1, reinterpret_cast<uint8_t*>(ostage) + runOff, nullptr);
+    if (tid < 32)
+    {
+        bool gaveUp;
+        const uint64_t prefix = LookBack(a, tile, tileBytes, gaveUp);
+        if (tid == 0)
+        {
+            prefixSh = prefix;
+            gaveUpSh = gaveUp;
+        }
+    }
+    __syncthreads();
+    const uint64_t prefix = prefixSh;
+    const bool fits = prefix + tileBytes <= a.capacity;   // else nothing of this tile is written
+    if (fits && staged && tileBytes)
+    {
+        // out in 16-byte stores at 16-byte boundaries; the two ends, shared
+        // with the neighbouring tiles, byte by byte
+        const uint32_t mis = (uint32_t)(reinterpret_cast<uintptr_t>(a.out + prefix) & 15);
+        uint8_t* base = a.out + prefix - mis;
+        const uint32_t end = mis + tileBytes;
+        const uint8_t* sb = reinterpret_cast<const uint8_t*>(ostage);
+        for (uint32_t lo = tid * 16; lo < end; lo += kThreads * 16)
+        {
+            if (lo >= mis && lo + 16 <= end)
+            {
+                const uint32_t src = lo - mis, w = src >> 2, sh = (src & 3) * 8;
+                const uint32_t x0 = ostage[w], x1 = ostage[w + 1], x2 = ostage[w + 2], x3 = ostage[w + 3],
+                               x4 = ostage[w + 4];
+                uint4 v;
+                v.x = __funnelshift_r(x0, x1, sh);
+                v.y = __funnelshift_r(x1, x2, sh);
+                v.z = __funnelshift_r(x2, x3, sh);
+                v.w = __funnelshift_r(x3, x4, sh);
+                *reinterpret_cast<uint4*>(base + lo) = v;
+            }
+            else
+            {
+                for (uint32_t b = max(lo, mis); b < min(lo + 16, end); ++b) base[b] = sb[b - mis];
+            }
+        }
+    }
+    else if (fits && !staged)
+    {
+        Run<Spec, true>(F, tv, i0, i1, a.out + prefix + runOff, nullptr);
+    }
+
+    if (tid < kTileRows && z0 + tid < a.numZmw)
+    {
+        // a ZMW without pulses starts where the next one with pulses does
+        int r = tid;
+        while (r < kTileRows && rowStart[r] == rowStart[r + 1]) ++r;
+        a.offsets[z0 + tid] = prefix + (r < kTileRows ? runOffSh[rowStart[r] / per] + rowLocal[r] : tileBytes);
+    }
+    if (tile == a.numTiles - 1 && tid == 0)
+    {
+        // every tile read *cur before it published its count, and every
+        // count has been seen
+        __threadfence();
+        const uint64_t total = prefix + tileBytes;
+        const bool ok = total <= a.capacity && !gaveUpSh && a.host[1] == 0;
+        a.offsets[a.numZmw] = total;
+        a.host[0] = total;
+        a.host[2] = ok ? 1 : 0;
+        if (ok) *a.cur = 1 - curSh;
+    }
 }
 
 int Fail(int code, const std::string& msg) { return hwk::SetLastError(code, msg.c_str()); }
@@ -272,42 +677,122 @@ int CheckFields(const hw_baz_field* f, uint32_t n)
     return HW_OK;
 }
 
+// Does the list equal a constant one (same fields, groups and reject rule)?
+template <class Spec>
+bool SameAs(const BazSpec& S)
+{
+    if (S.n != Spec::n() || (S.skipRejects != 0) != Spec::skip()) return false;
+    for (int i = 0; i < S.n; ++i)
+    {
+        const hw_baz_field a = S.f[i], b = Spec::f(i);
+        if (a.name != b.name || a.store_signed != b.store_signed || a.transform != b.transform ||
+            a.serialize != b.serialize || a.num_bits != b.num_bits ||
+            (a.transform == HW_BAZ_FLOAT_FIXED && (a.scale != b.scale || a.transform_bytes != b.transform_bytes)) ||
+            (a.serialize == HW_BAZ_SIMPLE_OVERFLOW && a.overflow_bytes != b.overflow_bytes) ||
+            S.groupBytes[i] != Spec::groupBytes(i) || (S.groupEnd[i] != 0) != Spec::groupEnd(i) ||
+            (a.transform == HW_BAZ_DELTA && S.slot[i] != Spec::slot(i)))
+            return false;
+    }
+    return true;
+}
+
 }   // namespace
 
 struct hw_baz_encoder
 {
     BazSpec spec{};
-    uint32_t numZmw = 0;
-    uint64_t* state = nullptr;     // [numZmw][kMaxFields] delta state
-    void* scanTmp = nullptr;
-    size_t scanTmpBytes = 0;
-    uint64_t* hostTotal = nullptr;  // mapped pinned word
-    uint64_t* devTotal = nullptr;   // its device address
-    ~hw_baz_encoder() { cudaFree(state); cudaFree(scanTmp); cudaFreeHost(hostTotal); }
+    int kind = 0;                  // 0 runtime list, 1 production, 2 internal
+    uint32_t numZmw = 0, numTiles = 0, zmwStride = 1;
+    uint64_t* state = nullptr;     // [2][slots][numZmw] delta state
+    uint32_t* cur = nullptr;       // device: the state copy the next call reads
+    unsigned long long* status = nullptr;   // [numTiles] look-back words, then the ticket counter
+    unsigned long long tickets = 0;         // tickets taken by earlier calls
+    unsigned long long epoch = 0;           // the last call's tag (20 bits; 0 never used)
+    uint64_t* host = nullptr;      // mapped pinned words
+    uint64_t* hostDev = nullptr;
+    ~hw_baz_encoder() { cudaFree(state); cudaFree(status); cudaFreeHost(host); }
 };
+
+namespace {
+
+template <class Spec>
+cudaError_t Launch(uint32_t tiles, const BazSpec& spec, const TileArgs& a, cudaStream_t s)
+{
+    static std::atomic<uint64_t> devicesSet{0};   // the shared memory above 48 KB, set once a device
+    int dev = 0;
+    cudaError_t ce = cudaGetDevice(&dev);
+    if (ce != cudaSuccess) return ce;
+    const uint64_t bit = 1ull << (dev & 63);
+    if (!(devicesSet.load() & bit))
+    {
+        ce = cudaFuncSetAttribute(BazTileKernel<Spec>, cudaFuncAttributeMaxDynamicSharedMemorySize, DynSmem<Spec>());
+        if (ce != cudaSuccess) return ce;
+        devicesSet.fetch_or(bit);
+    }
+    BazTileKernel<Spec><<<tiles, kThreads, DynSmem<Spec>(), s>>>(spec, a);
+    return cudaGetLastError();
+}
+
+// Enqueues one chunk's encoding.
+int Enqueue(hw_baz_encoder* e, const hw_pulse* d_pulses, const uint32_t* d_lens, uint32_t max_calls,
+            uint8_t* d_bytes, uint64_t bytes_capacity, uint64_t* d_offsets, cudaStream_t s)
+{
+    if (!d_bytes) bytes_capacity = 0;
+    cudaError_t ce = cudaSuccess;
+    if (++e->epoch == (1ull << 20))
+    {
+        // the tags wrap: clear the words so no word of an old call reads as this one's
+        ce = cudaMemsetAsync(e->status, 0, sizeof(unsigned long long) * (e->numTiles + 1), s);
+        e->epoch = 1;
+        e->tickets = 0;
+    }
+    TileArgs a;
+    a.pulses = d_pulses;
+    a.lens = d_lens;
+    a.cap = max_calls;
+    a.numZmw = e->numZmw;
+    a.numTiles = e->numTiles;
+    a.zmwStride = e->zmwStride;
+    a.state = e->state;
+    a.cur = e->cur;
+    a.offsets = d_offsets;
+    a.out = d_bytes;
+    a.capacity = bytes_capacity;
+    a.status = e->status;
+    a.ticket = e->status + e->numTiles;
+    a.ticketBase = e->tickets;
+    a.epoch = e->epoch;
+    a.host = e->hostDev;
+    if (ce == cudaSuccess)
+    {
+        if (e->kind == 1) ce = Launch<ProductionFields>(e->numTiles, e->spec, a, s);
+        else if (e->kind == 2) ce = Launch<InternalFields>(e->numTiles, e->spec, a, s);
+        else ce = Launch<RtFields>(e->numTiles, e->spec, a, s);
+    }
+    if (ce != cudaSuccess) return Fail(HW_ERR_CUDA, std::string("hw_baz_encode: ") + cudaGetErrorString(ce));
+    e->tickets += e->numTiles;
+    return HW_OK;
+}
+
+int Result(hw_baz_encoder* e, uint64_t* total_bytes)
+{
+    volatile uint64_t* h = e->host;
+    *total_bytes = h[0];
+    if (h[1]) return Fail(HW_ERR_TIMEOUT, "hw_baz_encode: a tile's look-back gave up waiting");
+    if (!h[2]) return Fail(HW_ERR_OUT_OF_MEMORY, "hw_baz_encode: the chunk needs more than bytes_capacity");
+    return HW_OK;
+}
+
+}   // namespace
 
 extern "C" {
 
 int hw_baz_preset(int32_t which, hw_baz_field* fields, uint32_t* n_fields, int32_t* skip_rejects)
 {
     if (!fields || !n_fields || (which != 0 && which != 1)) return Fail(HW_ERR_INVALID_ARG, "bad argument");
-    // PulseGroups.h:42-53 ProductionPulses, :55-94 InternalPulses
-    const hw_baz_field label{HW_BAZ_LABEL, 0, HW_BAZ_NOOP, 0, 0, HW_BAZ_TRUNCATE, 2, 0};
-    const hw_baz_field width{HW_BAZ_PULSE_WIDTH, 0, HW_BAZ_NOOP, 0, 0, HW_BAZ_COMPACT_OVERFLOW, 7, 0};
-    const hw_baz_field start{HW_BAZ_START_FRAME, 0, HW_BAZ_DELTA, 0, 0, HW_BAZ_COMPACT_OVERFLOW, 7, 0};
-    uint32_t n = 0;
-    fields[n++] = label;
-    fields[n++] = width;
-    fields[n++] = start;
-    if (which == 1)
-    {
-        fields[n++] = hw_baz_field{HW_BAZ_PKMAX, 1, HW_BAZ_FLOAT_FIXED, 10, 2, HW_BAZ_SIMPLE_OVERFLOW, 8, 2};
-        fields[n++] = hw_baz_field{HW_BAZ_PKMID, 1, HW_BAZ_FLOAT_FIXED, 10, 2, HW_BAZ_SIMPLE_OVERFLOW, 8, 2};
-        fields[n++] = hw_baz_field{HW_BAZ_PKMEAN, 1, HW_BAZ_FLOAT_FIXED, 10, 2, HW_BAZ_SIMPLE_OVERFLOW, 8, 2};
-        fields[n++] = hw_baz_field{HW_BAZ_PKVAR, 0, HW_BAZ_FLOAT_FIXED, 10, 2, HW_BAZ_SIMPLE_OVERFLOW, 7, 2};
-        fields[n++] = hw_baz_field{HW_BAZ_IS_BASE, 0, HW_BAZ_NOOP, 0, 0, HW_BAZ_TRUNCATE, 1, 0};
-    }
-    *n_fields = n;
+    const int n = which == 0 ? ProductionFields::n() : InternalFields::n();
+    for (int i = 0; i < n; ++i) fields[i] = which == 0 ? ProductionFields::f(i) : InternalFields::f(i);
+    *n_fields = (uint32_t)n;
     if (skip_rejects) *skip_rejects = which == 0 ? 1 : 0;   // PrelimHQFilter.cpp:116
     return HW_OK;
 }
@@ -321,6 +806,7 @@ int hw_baz_encoder_create(const hw_baz_field* fields, uint32_t n_fields, int32_t
     if (rc) return rc;
     auto e = new hw_baz_encoder;
     e->numZmw = num_zmw;
+    e->numTiles = (num_zmw + kTileRows - 1) / kTileRows;
     BazSpec& S = e->spec;
     S.n = (int)n_fields;
     S.skipRejects = skip_rejects != 0;
@@ -342,16 +828,19 @@ int hw_baz_encoder_create(const hw_baz_field* fields, uint32_t n_fields, int32_t
             cur = 0;
         }
         cur += bits;
+        if (fields[i].transform == HW_BAZ_DELTA) S.slot[i] = S.slots++;
     }
     S.groupEnd[n_fields - 1] = 1;
     S.groupBytes[open] = (cur + 7) / 8;
-    cudaError_t ce = cudaMalloc((void**)&e->state, sizeof(uint64_t) * kMaxFields * num_zmw);
-    if (ce == cudaSuccess) ce = cudaMemset(e->state, 0, sizeof(uint64_t) * kMaxFields * num_zmw);
-    if (ce == cudaSuccess) ce = cudaHostAlloc((void**)&e->hostTotal, sizeof(uint64_t), cudaHostAllocMapped);
-    if (ce == cudaSuccess) ce = cudaHostGetDevicePointer((void**)&e->devTotal, e->hostTotal, 0);
-    if (ce == cudaSuccess)
-        ce = cub::DeviceScan::ExclusiveSum(nullptr, e->scanTmpBytes, e->state, e->state, (int)num_zmw + 1);
-    if (ce == cudaSuccess) ce = cudaMalloc(&e->scanTmp, e->scanTmpBytes);
+    e->kind = SameAs<ProductionFields>(S) ? 1 : SameAs<InternalFields>(S) ? 2 : 0;
+    const size_t stateBytes = sizeof(uint64_t) * 2 * (size_t)(S.slots ? S.slots : 1) * num_zmw;
+    cudaError_t ce = cudaMalloc((void**)&e->state, stateBytes + sizeof(uint64_t));
+    if (ce == cudaSuccess) ce = cudaMemset(e->state, 0, stateBytes + sizeof(uint64_t));
+    if (ce == cudaSuccess) e->cur = reinterpret_cast<uint32_t*>(e->state + stateBytes / sizeof(uint64_t));
+    if (ce == cudaSuccess) ce = cudaMalloc((void**)&e->status, sizeof(unsigned long long) * (e->numTiles + 1));
+    if (ce == cudaSuccess) ce = cudaMemset(e->status, 0, sizeof(unsigned long long) * (e->numTiles + 1));
+    if (ce == cudaSuccess) ce = cudaHostAlloc((void**)&e->host, 4 * sizeof(uint64_t), cudaHostAllocMapped);
+    if (ce == cudaSuccess) ce = cudaHostGetDevicePointer((void**)&e->hostDev, e->host, 0);
     if (ce != cudaSuccess)
     {
         delete e;
@@ -367,33 +856,41 @@ int hw_baz_encoder_destroy(hw_baz_encoder* e)
     return HW_OK;
 }
 
+int hw_baz_encoder_set_zmw_stride(hw_baz_encoder* e, uint32_t stride)
+{
+    if (!e || stride == 0 || 64 % stride != 0)
+        return Fail(HW_ERR_INVALID_ARG, "hw_baz_encoder_set_zmw_stride: the stride must divide 64");
+    e->zmwStride = stride;
+    return HW_OK;
+}
+
 int hw_baz_encode(hw_baz_encoder* e, const hw_pulse* d_pulses, const uint32_t* d_lens, uint32_t max_calls,
                   uint8_t* d_bytes, uint64_t bytes_capacity, uint64_t* d_offsets, uint64_t* total_bytes,
                   void* stream)
 {
     if (!e || !d_pulses || !d_lens || !d_offsets || !total_bytes || max_calls == 0)
         return Fail(HW_ERR_INVALID_ARG, "hw_baz_encode: bad argument");
-    if (!d_bytes) bytes_capacity = 0;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    const int n = (int)e->numZmw;
-    const int threads = 128, blocks = (n + threads - 1) / threads;
-    BazSizeKernel<<<blocks, threads, 0, s>>>(e->spec, d_pulses, d_lens, (int)max_calls, n, e->state, d_offsets);
-    cudaError_t ce = cudaGetLastError();
-    if (ce == cudaSuccess)
-        ce = cub::DeviceScan::ExclusiveSum(e->scanTmp, e->scanTmpBytes, d_offsets, d_offsets, n + 1, s);
-    if (ce == cudaSuccess)
-    {
-        BazEncodeKernel<<<blocks, threads, 0, s>>>(e->spec, d_pulses, d_lens, (int)max_calls, n, e->state, d_offsets,
-                                                   d_bytes, bytes_capacity, e->devTotal);
-        ce = cudaGetLastError();
-    }
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    int rc = Enqueue(e, d_pulses, d_lens, max_calls, d_bytes, bytes_capacity, d_offsets, s);
+    if (rc) return rc;
+    const cudaError_t ce = cudaStreamSynchronize(s);
     if (ce != cudaSuccess) return Fail(HW_ERR_CUDA, std::string("hw_baz_encode: ") + cudaGetErrorString(ce));
-    const uint64_t total = *(volatile uint64_t*)e->hostTotal;
-    *total_bytes = total;
-    if (total > bytes_capacity)
-        return Fail(HW_ERR_OUT_OF_MEMORY, "hw_baz_encode: the chunk needs more than bytes_capacity");
-    return HW_OK;
+    return Result(e, total_bytes);
+}
+
+int hw_baz_encode_async(hw_baz_encoder* e, const hw_pulse* d_pulses, const uint32_t* d_lens, uint32_t max_calls,
+                        uint8_t* d_bytes, uint64_t bytes_capacity, uint64_t* d_offsets, void* stream)
+{
+    if (!e || !d_pulses || !d_lens || !d_offsets || max_calls == 0)
+        return Fail(HW_ERR_INVALID_ARG, "hw_baz_encode_async: bad argument");
+    return Enqueue(e, d_pulses, d_lens, max_calls, d_bytes, bytes_capacity, d_offsets,
+                   reinterpret_cast<cudaStream_t>(stream));
+}
+
+int hw_baz_encode_result(hw_baz_encoder* e, uint64_t* total_bytes)
+{
+    if (!e || !total_bytes) return Fail(HW_ERR_INVALID_ARG, "hw_baz_encode_result: bad argument");
+    return Result(e, total_bytes);
 }
 
 }   // extern "C"

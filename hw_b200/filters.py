@@ -568,7 +568,7 @@ class BazEncoder(_Handle):
     start-frame delta state of each ZMW carries over between chunks."""
     _destroy = "hw_baz_encoder_destroy"
 
-    def __init__(self, num_zmw, fields=None, skip_rejects=None, preset=abi.BAZ_PRODUCTION):
+    def __init__(self, num_zmw, fields=None, skip_rejects=None, preset=abi.BAZ_PRODUCTION, zmw_stride=1):
         super().__init__()
         if fields is None:
             fields, skip = baz_preset(preset)
@@ -577,6 +577,8 @@ class BazEncoder(_Handle):
         self.num_zmw = num_zmw
         check(lib().hw_baz_encoder_create(abi.ptr(self.fields), len(self.fields), int(bool(skip_rejects)), num_zmw,
                                           C.byref(self._h)))
+        if zmw_stride != 1:
+            check(lib().hw_baz_encoder_set_zmw_stride(self._h, zmw_stride))
         self.offsets = torch.zeros(num_zmw + 1, dtype=torch.int64, device="cuda")
         self.bytes = torch.empty(0, dtype=torch.uint8, device="cuda")
 
@@ -593,6 +595,18 @@ class BazEncoder(_Handle):
             self.bytes = torch.empty(max(total.value, 2 * self.bytes.numel()), dtype=torch.uint8, device="cuda")
         check(rc)
         return self.bytes[:total.value], self.offsets
+
+    def enqueue(self, pulses, lens, max_calls, out, offsets):
+        """hw_baz_encode_async into caller buffers (a CUDA uint8 tensor and an
+        int64 tensor of num_zmw + 1); offsets[-1] is the chunk's bytes."""
+        check(lib().hw_baz_encode_async(self._h, _p(pulses), _p(lens), int(max_calls), _p(out), out.numel(),
+                                        _p(offsets), _stream()))
+
+    def result(self):
+        """Status of the last finished enqueue (after synchronising): its bytes."""
+        total = C.c_uint64()
+        check(lib().hw_baz_encode_result(self._h, C.byref(total)))
+        return total.value
 
 
 class _DeviceBytes:

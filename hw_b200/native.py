@@ -83,7 +83,10 @@ def lib():
         "hw_baz_preset": ([i32, vp, C.POINTER(u32), C.POINTER(i32)], C.c_int),
         "hw_baz_encoder_create": ([vp, u32, i32, u32, PPV], C.c_int),
         "hw_baz_encoder_destroy": ([vp], C.c_int),
+        "hw_baz_encoder_set_zmw_stride": ([vp, u32], C.c_int),
         "hw_baz_encode": ([vp, vp, vp, u32, vp, C.c_uint64, vp, C.POINTER(C.c_uint64), vp], C.c_int),
+        "hw_baz_encode_async": ([vp, vp, vp, u32, vp, C.c_uint64, vp, vp], C.c_int),
+        "hw_baz_encode_result": ([vp, C.POINTER(C.c_uint64)], C.c_int),
         "hw_fused_enable_hf_metrics": ([vp, u32, C.c_double, i32, vp, vp, vp, vp, vp, u32, vp, C.c_float], C.c_int),
         "hw_analyzer_chunk_metrics": ([vp, vp, vp, vp, vp], C.c_int),
         "hw_hfmetrics_create": ([u32, u32, C.c_double, i32, PPV], C.c_int),

@@ -623,16 +623,32 @@ typedef struct hw_baz_encoder hw_baz_encoder;
 int hw_baz_encoder_create(const hw_baz_field* fields, uint32_t n_fields, int32_t skip_rejects, uint32_t num_zmw,
                           hw_baz_encoder** out);
 int hw_baz_encoder_destroy(hw_baz_encoder* e);
+/* Encode only ZMW 0, stride, 2 x stride, ... of every lane (PrelimHQConfig
+ * zmwOutputStride, PrelimHQFilter.cpp:107-118); the others get empty byte
+ * ranges and keep their state.  stride divides 64 (default 1). */
+int hw_baz_encoder_set_zmw_stride(hw_baz_encoder* e, uint32_t stride);
 /* Encodes one chunk: pulses [num_zmw][max_calls] with counts d_lens[num_zmw]
  * (counts above max_calls read as max_calls).
  * d_offsets[num_zmw + 1] receives each ZMW's byte range in d_bytes (capacity
- * bytes_capacity); *total_bytes the bytes written.  Returns
- * HW_ERR_OUT_OF_MEMORY (nothing written, state unchanged) when the chunk
- * needs more than bytes_capacity.  Synchronises the stream once (to learn
- * the total). */
+ * bytes_capacity); *total_bytes the chunk's bytes.  When the chunk needs
+ * more than bytes_capacity (or d_bytes is NULL) the call returns
+ * HW_ERR_OUT_OF_MEMORY with the offsets and *total_bytes set, the delta
+ * state unchanged and the contents of d_bytes unspecified, so the same call
+ * with a larger buffer encodes the chunk.  One launch (tiles of 128 ZMWs
+ * placed by a decoupled look-back whose polls are bounded: HW_ERR_TIMEOUT if
+ * one gives up); synchronises the stream once, to learn the total. */
 int hw_baz_encode(hw_baz_encoder* e, const hw_pulse* d_pulses, const uint32_t* d_lens, uint32_t max_calls,
                   uint8_t* d_bytes, uint64_t bytes_capacity, uint64_t* d_offsets, uint64_t* total_bytes,
                   void* stream);
+/* hw_baz_encode without the synchronisation: enqueues the chunk on the
+ * stream and returns.  d_offsets[num_zmw] holds the chunk's bytes once the
+ * stream reaches it; calls in a row are ordered on the stream and each one
+ * continues the delta state of the last one that fit in its buffer.  After
+ * synchronising, hw_baz_encode_result reports the last finished call as
+ * hw_baz_encode would have (HW_OK, HW_ERR_OUT_OF_MEMORY, HW_ERR_TIMEOUT). */
+int hw_baz_encode_async(hw_baz_encoder* e, const hw_pulse* d_pulses, const uint32_t* d_lens, uint32_t max_calls,
+                        uint8_t* d_bytes, uint64_t bytes_capacity, uint64_t* d_offsets, void* stream);
+int hw_baz_encode_result(hw_baz_encoder* e, uint64_t* total_bytes);
 
 /* ---- Pool sets: uneven pools --------------------------
  * No single reference counterpart: the reference runs one BatchAnalyzer per

@@ -2850,15 +2850,18 @@ int or_baz_decode_values(const hw_baz_field* fields, uint32_t nf, const uint8_t*
 // PrelimHQFilter + PacketBuffer::AddZmw over a chunk of the basecaller's
 // pulses: per ZMW the kept pulses in order, bytes appended to out;
 // offsets[numZmw + 1].  last[numZmw][nf] carries the delta state.
+// zmwStride: only ZMW 0, stride, 2 x stride ... of each lane of 64
+// (PrelimHQFilter.cpp:107-118).
 int or_baz_encode_chunk(const hw_baz_field* fields, uint32_t nf, int32_t skipRejects, uint32_t numZmw,
-                        const hw_pulse* pulses, const uint32_t* lens, uint32_t cap, uint8_t* out, uint64_t outCap,
-                        uint64_t* offsets, uint64_t* last)
+                        uint32_t zmwStride, const hw_pulse* pulses, const uint32_t* lens, uint32_t cap, uint8_t* out,
+                        uint64_t outCap, uint64_t* offsets, uint64_t* last)
 {
     BazOracle o(fields, nf);
     uint64_t pos = 0;
     for (uint32_t z = 0; z < numZmw; ++z)
     {
         offsets[z] = pos;
+        if ((z % 64) % zmwStride != 0) continue;
         const uint32_t n = std::min(lens[z], cap);
         for (uint32_t i = 0; i < n; ++i)
         {

@@ -76,7 +76,7 @@ def lib():
         L.or_baz_serializer_roundtrip.restype = C.c_uint64
         L.or_baz_float_fixed_roundtrip.argtypes = [C.c_float, i32, i32, i32, C.POINTER(C.c_uint64)]
         L.or_baz_float_fixed_roundtrip.restype = C.c_float
-        L.or_baz_encode_chunk.argtypes = [vp, u32, i32, u32, vp, vp, u32, vp, C.c_uint64, vp, vp]
+        L.or_baz_encode_chunk.argtypes = [vp, u32, i32, u32, u32, vp, vp, u32, vp, C.c_uint64, vp, vp]
         _lib = L
     return _lib
 
@@ -343,10 +343,11 @@ class BazEncoder:
     """PrelimHQFilter + PacketBuffer::AddZmw over chunks of the basecaller's
     pulses ([num_zmw][cap] abi.PULSE_DT); per-ZMW delta state kept."""
 
-    def __init__(self, fields, skip_rejects, num_zmw):
+    def __init__(self, fields, skip_rejects, num_zmw, zmw_stride=1):
         self.fields = np.ascontiguousarray(fields, abi.BAZ_FIELD_DT)
         self.skip = int(bool(skip_rejects))
         self.num_zmw = num_zmw
+        self.stride = zmw_stride
         self.last = np.zeros((num_zmw, len(self.fields)), np.uint64)
 
     def __call__(self, pulses, lens, cap):
@@ -356,6 +357,6 @@ class BazEncoder:
         out = np.zeros(out_cap, np.uint8)
         offsets = np.zeros(self.num_zmw + 1, np.uint64)
         _check(lib().or_baz_encode_chunk(abi.ptr(self.fields), len(self.fields), self.skip, self.num_zmw,
-                                         abi.ptr(pulses), abi.ptr(lens), int(cap), abi.ptr(out), out_cap,
+                                         self.stride, abi.ptr(pulses), abi.ptr(lens), int(cap), abi.ptr(out), out_cap,
                                          abi.ptr(offsets), abi.ptr(self.last)))
         return out[:int(offsets[-1])].copy(), offsets

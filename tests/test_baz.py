@@ -331,6 +331,22 @@ def test_oracle_chunk_equals_per_zmw_encoding(which):
             assert data[off[z]:off[z + 1]].tobytes() == want.tobytes(), (chunk, z)
 
 
+def test_oracle_zmw_stride_leaves_other_zmws_empty():
+    """zmwOutputStride (PrelimHQFilter.cpp:107-118): ZMW 0, 4, 8 ... of each
+    lane encoded, the others empty."""
+    import oracle
+    f, skip = preset(abi.BAZ_PRODUCTION)
+    rng = np.random.default_rng(5)
+    p, lens = random_pulses(rng, 256, 16)
+    lens[:] = np.maximum(lens, 1)
+    every = oracle.BazEncoder(f, skip, 256)(p, lens, 16)
+    data, off = oracle.BazEncoder(f, skip, 256, zmw_stride=4)(p, lens, 16)
+    for z in range(256):
+        got = data[off[z]:off[z + 1]].tobytes()
+        want = every[0][every[1][z]:every[1][z + 1]].tobytes() if z % 4 == 0 else b""
+        assert got == want, z
+
+
 def test_encoder_rejects_bad_field_lists():
     """Checked before any device work: no GPU needed."""
     from hw_b200 import native
@@ -370,13 +386,13 @@ CUSTOM = [
 ]
 
 
-def _gpu_vs_oracle(f, skip, chunks, nz, cap, seed, max_len=None):
+def _gpu_vs_oracle(f, skip, chunks, nz, cap, seed, max_len=None, stride=1):
     import torch
     import oracle
     from hw_b200 import filters as Fl
     rng = np.random.default_rng(seed)
-    gpu = Fl.BazEncoder(nz, fields=f, skip_rejects=skip)
-    ref = oracle.BazEncoder(f, skip, nz)
+    gpu = Fl.BazEncoder(nz, fields=f, skip_rejects=skip, zmw_stride=stride)
+    ref = oracle.BazEncoder(f, skip, nz, zmw_stride=stride)
     total = 0
     for _ in range(chunks):
         p, lens = random_pulses(rng, nz, cap, max_len)
@@ -394,8 +410,9 @@ def _gpu_vs_oracle(f, skip, chunks, nz, cap, seed, max_len=None):
 @pytest.mark.gpu
 @pytest.mark.parametrize("which", [abi.BAZ_PRODUCTION, abi.BAZ_INTERNAL])
 def test_gpu_encoder_matches_oracle_on_presets(which):
+    """160 tiles of 128 ZMWs: the look-back crosses several 32-tile windows."""
     f, skip = preset(which)
-    assert _gpu_vs_oracle(f, skip, chunks=4, nz=1000, cap=48, seed=11) > 0
+    assert _gpu_vs_oracle(f, skip, chunks=3, nz=20400, cap=24, seed=11) > 0
 
 
 @pytest.mark.gpu
@@ -407,8 +424,8 @@ def test_gpu_encoder_matches_oracle_on_custom_fields(make, skip):
 
 @pytest.mark.gpu
 def test_gpu_encoder_edges():
-    """Empty chunks, a single ZMW, ZMW counts off the block size, and a too
-    small buffer (HW_ERR_OUT_OF_MEMORY, state unchanged)."""
+    """Empty chunks, a single ZMW, ZMW counts off the tile size, and a too
+    small buffer (HW_ERR_OUT_OF_MEMORY with the offsets set, state unchanged)."""
     import torch
     import oracle
     from hw_b200 import filters as Fl, native
@@ -431,11 +448,34 @@ def test_gpu_encoder_edges():
                                     C.c_void_p(small.data_ptr()), 4, C.c_void_p(gpu.offsets.data_ptr()),
                                     C.byref(total), None)
     assert rc == abi.HW_ERR_OUT_OF_MEMORY and total.value > 4
-    assert small.sum().item() == 0
-    for _ in range(2):                  # the retry and the next chunk match the oracle from the start
-        want, _ = ref(p, lens, cap)
-        got, _ = gpu(d_p, d_l, cap)
-        assert got.cpu().numpy().tobytes() == want.tobytes()
+    want, woff = ref(p, lens, cap)
+    assert gpu.offsets.cpu().numpy().astype(np.uint64).tolist() == woff.tolist()
+    # a buffer of exactly the chunk's bytes; then the next chunk: the state
+    # was left as it was by the refused call
+    exact = torch.zeros(total.value, dtype=torch.uint8, device="cuda")
+    rc = native.lib().hw_baz_encode(gpu._h, C.c_void_p(d_p.data_ptr()), C.c_void_p(d_l.data_ptr()), cap,
+                                    C.c_void_p(exact.data_ptr()), total.value, C.c_void_p(gpu.offsets.data_ptr()),
+                                    C.byref(total), None)
+    assert rc == 0 and exact.cpu().numpy().tobytes() == want.tobytes()
+    want, _ = ref(p, lens, cap)
+    got, _ = gpu(d_p, d_l, cap)
+    assert got.cpu().numpy().tobytes() == want.tobytes()
+
+
+@pytest.mark.gpu
+def test_gpu_encoder_zmw_stride():
+    f, skip = preset(abi.BAZ_PRODUCTION)
+    assert _gpu_vs_oracle(f, skip, chunks=3, nz=1000, cap=24, seed=13, stride=4) > 0
+
+
+@pytest.mark.gpu
+def test_gpu_encoder_production_fields_keeping_rejects():
+    """The production fields with rejected pulses kept: the general field
+    path of the kernel (the constant production path skips rejects)."""
+    f, _ = preset(abi.BAZ_PRODUCTION)
+    assert _gpu_vs_oracle(f, False, chunks=3, nz=900, cap=40, seed=8) > 0
+    f, _ = preset(abi.BAZ_INTERNAL)
+    assert _gpu_vs_oracle(f, True, chunks=3, nz=900, cap=40, seed=9) > 0
 
 
 @pytest.mark.gpu
@@ -477,3 +517,35 @@ def test_gpu_encoder_on_chain_pulses_round_trip():
                 assert back[k].tolist() == kept[k].tolist()
             decoded += len(kept)
     assert decoded > 1000
+
+
+@pytest.mark.gpu
+def test_gpu_encoder_async_calls_in_a_row():
+    """Encodings enqueued back to back: each continues the state of the last
+    one that fit; a call whose buffer is too small leaves the state, and the
+    result call reports the last one."""
+    import torch
+    import oracle
+    from hw_b200 import filters as Fl
+    f, skip = preset(abi.BAZ_PRODUCTION)
+    nz, cap = 3000, 24
+    rng = np.random.default_rng(21)
+    chunks = [random_pulses(rng, nz, cap) for _ in range(4)]
+    ref = oracle.BazEncoder(f, skip, nz)
+    want = [ref(*chunks[0], cap)[0], None, ref(*chunks[2], cap)[0], ref(*chunks[3], cap)[0]]
+    gpu = Fl.BazEncoder(nz, fields=f, skip_rejects=skip)
+    outs, offs, keep = [], [], []
+    for c, (p, lens) in enumerate(chunks):
+        d_p = torch.from_numpy(p.view(np.uint8).reshape(-1).copy()).cuda()
+        d_l = torch.from_numpy(lens.view(np.int32)).cuda()
+        size = 8 if c == 1 else len(want[c]) + 64
+        outs.append(torch.zeros(size, dtype=torch.uint8, device="cuda"))
+        offs.append(torch.zeros(nz + 1, dtype=torch.int64, device="cuda"))
+        keep.append((d_p, d_l))
+        gpu.enqueue(d_p, d_l, cap, outs[-1], offs[-1])
+    torch.cuda.synchronize()
+    assert gpu.result() == len(want[3])
+    for c in (0, 2, 3):
+        n = int(offs[c][-1].item())
+        assert n == len(want[c])
+        assert outs[c][:n].cpu().numpy().tobytes() == want[c].tobytes(), c
