@@ -190,6 +190,14 @@ BAZ_NOOP, BAZ_DELTA, BAZ_FLOAT_FIXED = range(3)
 BAZ_TRUNCATE, BAZ_SIMPLE_OVERFLOW, BAZ_COMPACT_OVERFLOW = range(3)
 BAZ_PRODUCTION, BAZ_INTERNAL = 0, 1
 
+# hw_prelim_hq_config and hw_baz_checkpoint
+PRELIM_HQ_CONFIG_DT = np.dtype([("chunks_per_block", np.uint32), ("lookback_blocks", np.uint32),
+                                ("enable_prehq", np.int32), ("hq_throttle_fraction", np.float32),
+                                ("zmw_stride", np.uint32), ("reserved", np.uint32)])
+BAZ_CHECKPOINT_DT = np.dtype([("d_bytes", np.uint64), ("total_bytes", np.uint64), ("d_offsets", np.uint64),
+                              ("d_events", np.uint64), ("d_hq", np.uint64), ("num_hq", np.uint32),
+                              ("block", np.uint32)])
+
 FUSED_TUNING_DT = np.dtype([("frames_per_chunk", np.uint32), ("fuse_label_pulses", np.uint32),
                             ("labeler_lanes_per_cta", np.uint32), ("reserved", np.uint32)])
 
@@ -207,6 +215,8 @@ SIZES = {
     "hw_sensor_packet": (SENSOR_PACKET_DT, 32),
     "hw_fused_tuning": (FUSED_TUNING_DT, 16),
     "hw_baz_field": (BAZ_FIELD_DT, 32),
+    "hw_prelim_hq_config": (PRELIM_HQ_CONFIG_DT, 24),
+    "hw_baz_checkpoint": (BAZ_CHECKPOINT_DT, 48),
 }
 
 

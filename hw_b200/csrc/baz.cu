@@ -287,6 +287,7 @@ struct TileArgs
     uint64_t* state;                  // [2][slots][numZmw]; *cur names the copy this call reads
     uint32_t* cur;
     uint64_t* offsets;                // [numZmw + 1]
+    uint32_t* events;                 // [numZmw] pulses encoded, or null
     uint8_t* out;
     uint64_t capacity;
     unsigned long long* status;       // [numTiles] look-back words
@@ -421,7 +422,7 @@ struct TileView
 // 2).  Returns the run's bytes.
 template <class Spec, bool Write>
 __device__ __forceinline__ uint32_t Run(const Spec& F, const TileView& t, uint32_t i0, uint32_t i1, uint8_t* out,
-                                        uint32_t* rowLocal)
+                                        uint32_t* rowLocal, uint32_t* rowEvents)
 {
     if (i0 >= i1) return 0;
     int lo = 0, hi = kTileRows;   // the ZMW of pulse i0: the last with rowStart <= i0
@@ -452,7 +453,7 @@ __device__ __forceinline__ uint32_t Run(const Spec& F, const TileView& t, uint32
             if (d.transform == HW_BAZ_DELTA) prev[f] = j >= 0 ? RawField(d.name, q) : t.State(F.slot(f), r);
         }
     }
-    uint32_t bytes = 0;
+    uint32_t bytes = 0, seg = 0;   // seg: pulses kept in this ZMW's part of the run
     for (uint32_t i = i0; i < i1; ++i)
     {
         const hw_pulse p = t.At(i, r, k);
@@ -472,11 +473,13 @@ __device__ __forceinline__ uint32_t Run(const Spec& F, const TileView& t, uint32
             if (Write) bytes = (uint32_t)(EncodePulse(F, p, prev, out + bytes) - out);
             else bytes += PulseBytes(F, p, prev);
             KeepPrev(F, p, prev);
+            ++seg;
         }
         if ((uint32_t)++k == rowLen)
         {
             if (!Write)
             {
+                if (seg) atomicAdd(&rowEvents[r], seg);
                 // the ZMW's last pulse: the next chunk's delta state (the last
                 // kept pulse's values, or the state it came in with)
 #pragma unroll
@@ -491,9 +494,11 @@ __device__ __forceinline__ uint32_t Run(const Spec& F, const TileView& t, uint32
             // the next ZMW with pulses
             do { ++r; } while (r < kTileRows && t.rowStart[r + 1] == t.rowStart[r]);
             k = 0;
+            seg = 0;
             rowLen = r < kTileRows ? t.rowStart[r + 1] - t.rowStart[r] : 0;
         }
     }
+    if (!Write && seg) atomicAdd(&rowEvents[r], seg);   // the run ends inside a ZMW
     return bytes;
 }
 
@@ -505,6 +510,7 @@ __global__ void __launch_bounds__(kThreads) BazTileKernel(const __grid_constant_
     __shared__ typename Scan::TempStorage scanTmp;
     __shared__ uint32_t rowStart[kTileRows + 1];   // tile pulse index of each ZMW's first pulse
     __shared__ uint32_t rowLocal[kTileRows];       // byte offset of a ZMW's first pulse in its run
+    __shared__ uint32_t rowEvents[kTileRows];      // pulses encoded of each ZMW
     __shared__ uint32_t runOffSh[kThreads];        // tile byte offset of each thread's run
     __shared__ uint64_t state0[kTileRows];         // slot 0 of the delta state
     __shared__ uint32_t tileSh, curSh;
@@ -534,6 +540,7 @@ __global__ void __launch_bounds__(kThreads) BazTileKernel(const __grid_constant_
     if (tid < kTileRows)
     {
         rowStart[tid] = excl;
+        rowEvents[tid] = 0;
         if (z0 + tid < a.numZmw && F.hasDelta()) CpAsync8(&state0[tid], stateCur + z0 + tid);
         if (z0 + tid < a.numZmw && cnt == 0)
         {
@@ -573,14 +580,14 @@ __global__ void __launch_bounds__(kThreads) BazTileKernel(const __grid_constant_
     // sweep 1: each thread sizes a contiguous run of the tile's pulses
     const uint32_t per = (P + kThreads - 1) / kThreads;
     const uint32_t i0 = min(P, tid * per), i1 = min(P, i0 + per);
-    const uint32_t mine = Run<Spec, false>(F, tv, i0, i1, nullptr, rowLocal);
+    const uint32_t mine = Run<Spec, false>(F, tv, i0, i1, nullptr, rowLocal, rowEvents);
     uint32_t runOff, tileBytes;
     Scan(scanTmp).ExclusiveSum(mine, runOff, tileBytes);
     runOffSh[tid] = runOff;
     if (tid == 0) PublishCount(a, tile, tileBytes);
     // sweep 2 into shared memory before the look-back, when the tile fits
     const bool staged = tileBytes <= (uint32_t)kOut;
-    if (staged) Run<Spec, true>(F, tv, i0, i1, reinterpret_cast<uint8_t*>(ostage) + runOff, nullptr);
+    if (staged) Run<Spec, true>(F, tv, i0, i1, reinterpret_cast<uint8_t*>(ostage) + runOff, nullptr, nullptr);
     if (tid < 32)
     {
         bool gaveUp;
@@ -624,7 +631,7 @@ __global__ void __launch_bounds__(kThreads) BazTileKernel(const __grid_constant_
     }
     else if (fits && !staged)
     {
-        Run<Spec, true>(F, tv, i0, i1, a.out + prefix + runOff, nullptr);
+        Run<Spec, true>(F, tv, i0, i1, a.out + prefix + runOff, nullptr, nullptr);
     }
 
     if (tid < kTileRows && z0 + tid < a.numZmw)
@@ -633,6 +640,7 @@ __global__ void __launch_bounds__(kThreads) BazTileKernel(const __grid_constant_
         int r = tid;
         while (r < kTileRows && rowStart[r] == rowStart[r + 1]) ++r;
         a.offsets[z0 + tid] = prefix + (r < kTileRows ? runOffSh[rowStart[r] / per] + rowLocal[r] : tileBytes);
+        if (a.events) a.events[z0 + tid] = rowEvents[tid];
     }
     if (tile == a.numTiles - 1 && tid == 0)
     {
@@ -735,7 +743,7 @@ cudaError_t Launch(uint32_t tiles, const BazSpec& spec, const TileArgs& a, cudaS
 
 // Enqueues one chunk's encoding.
 int Enqueue(hw_baz_encoder* e, const hw_pulse* d_pulses, const uint32_t* d_lens, uint32_t max_calls,
-            uint8_t* d_bytes, uint64_t bytes_capacity, uint64_t* d_offsets, cudaStream_t s)
+            uint8_t* d_bytes, uint64_t bytes_capacity, uint64_t* d_offsets, uint32_t* d_events, cudaStream_t s)
 {
     if (!d_bytes) bytes_capacity = 0;
     cudaError_t ce = cudaSuccess;
@@ -756,6 +764,7 @@ int Enqueue(hw_baz_encoder* e, const hw_pulse* d_pulses, const uint32_t* d_lens,
     a.state = e->state;
     a.cur = e->cur;
     a.offsets = d_offsets;
+    a.events = d_events;
     a.out = d_bytes;
     a.capacity = bytes_capacity;
     a.status = e->status;
@@ -865,13 +874,13 @@ int hw_baz_encoder_set_zmw_stride(hw_baz_encoder* e, uint32_t stride)
 }
 
 int hw_baz_encode(hw_baz_encoder* e, const hw_pulse* d_pulses, const uint32_t* d_lens, uint32_t max_calls,
-                  uint8_t* d_bytes, uint64_t bytes_capacity, uint64_t* d_offsets, uint64_t* total_bytes,
-                  void* stream)
+                  uint8_t* d_bytes, uint64_t bytes_capacity, uint64_t* d_offsets, uint32_t* d_events,
+                  uint64_t* total_bytes, void* stream)
 {
     if (!e || !d_pulses || !d_lens || !d_offsets || !total_bytes || max_calls == 0)
         return Fail(HW_ERR_INVALID_ARG, "hw_baz_encode: bad argument");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    int rc = Enqueue(e, d_pulses, d_lens, max_calls, d_bytes, bytes_capacity, d_offsets, s);
+    int rc = Enqueue(e, d_pulses, d_lens, max_calls, d_bytes, bytes_capacity, d_offsets, d_events, s);
     if (rc) return rc;
     const cudaError_t ce = cudaStreamSynchronize(s);
     if (ce != cudaSuccess) return Fail(HW_ERR_CUDA, std::string("hw_baz_encode: ") + cudaGetErrorString(ce));
@@ -879,11 +888,12 @@ int hw_baz_encode(hw_baz_encoder* e, const hw_pulse* d_pulses, const uint32_t* d
 }
 
 int hw_baz_encode_async(hw_baz_encoder* e, const hw_pulse* d_pulses, const uint32_t* d_lens, uint32_t max_calls,
-                        uint8_t* d_bytes, uint64_t bytes_capacity, uint64_t* d_offsets, void* stream)
+                        uint8_t* d_bytes, uint64_t bytes_capacity, uint64_t* d_offsets, uint32_t* d_events,
+                        void* stream)
 {
     if (!e || !d_pulses || !d_lens || !d_offsets || max_calls == 0)
         return Fail(HW_ERR_INVALID_ARG, "hw_baz_encode_async: bad argument");
-    return Enqueue(e, d_pulses, d_lens, max_calls, d_bytes, bytes_capacity, d_offsets,
+    return Enqueue(e, d_pulses, d_lens, max_calls, d_bytes, bytes_capacity, d_offsets, d_events,
                    reinterpret_cast<cudaStream_t>(stream));
 }
 

@@ -580,27 +580,30 @@ class BazEncoder(_Handle):
         if zmw_stride != 1:
             check(lib().hw_baz_encoder_set_zmw_stride(self._h, zmw_stride))
         self.offsets = torch.zeros(num_zmw + 1, dtype=torch.int64, device="cuda")
+        self.events = torch.zeros(num_zmw, dtype=torch.int32, device="cuda")
         self.bytes = torch.empty(0, dtype=torch.uint8, device="cuda")
 
     def __call__(self, pulses, lens, max_calls):
         """pulses: CUDA buffer of [num_zmw][max_calls] hw_pulse; lens: CUDA
         uint32/int32 counts.  Returns (bytes, offsets): the chunk's bytes (a
-        view of the encoder's buffer) and the ZMW offsets [num_zmw + 1]."""
+        view of the encoder's buffer) and the ZMW offsets [num_zmw + 1]; the
+        pulses encoded of each ZMW are in self.events."""
         total = C.c_uint64()
         for _ in range(2):
             rc = lib().hw_baz_encode(self._h, _p(pulses), _p(lens), int(max_calls), _p(self.bytes),
-                                     self.bytes.numel(), _p(self.offsets), C.byref(total), _stream())
+                                     self.bytes.numel(), _p(self.offsets), _p(self.events), C.byref(total),
+                                     _stream())
             if rc != abi.HW_ERR_OUT_OF_MEMORY:
                 break
             self.bytes = torch.empty(max(total.value, 2 * self.bytes.numel()), dtype=torch.uint8, device="cuda")
         check(rc)
         return self.bytes[:total.value], self.offsets
 
-    def enqueue(self, pulses, lens, max_calls, out, offsets):
+    def enqueue(self, pulses, lens, max_calls, out, offsets, events=None):
         """hw_baz_encode_async into caller buffers (a CUDA uint8 tensor and an
         int64 tensor of num_zmw + 1); offsets[-1] is the chunk's bytes."""
         check(lib().hw_baz_encode_async(self._h, _p(pulses), _p(lens), int(max_calls), _p(out), out.numel(),
-                                        _p(offsets), _stream()))
+                                        _p(offsets), _p(events), _stream()))
 
     def result(self):
         """Status of the last finished enqueue (after synchronising): its bytes."""
@@ -621,3 +624,54 @@ def _from_device(ptr, nbytes):
     """uint8 CUDA tensor viewing nbytes of library-owned device memory at ptr
     (valid while the owning handle lives)."""
     return torch.as_tensor(_DeviceBytes(ptr, nbytes), device="cuda")
+
+
+class PrelimHq(_Handle):
+    """Preliminary HQ stage (hw_prelim_hq): BAZ-encodes every chunk, keeps the
+    last `lookback` metric blocks on the device and produces one checkpoint a
+    metric block (PrelimHQFilterBody with the BazAggregator packet side)."""
+    _destroy = "hw_prelim_hq_destroy"
+
+    def __init__(self, num_zmw, preset=abi.BAZ_PRODUCTION, fields=None, skip_rejects=None, chunks_per_block=8,
+                 lookback=10, enable=False, throttle=0.10, zmw_stride=1):
+        super().__init__()
+        if fields is None:
+            fields, skip = baz_preset(preset)
+            skip_rejects = skip if skip_rejects is None else skip_rejects
+        self.fields = np.ascontiguousarray(fields, abi.BAZ_FIELD_DT)
+        self.num_zmw = num_zmw
+        cfg = np.zeros(1, abi.PRELIM_HQ_CONFIG_DT)
+        check(lib().hw_prelim_hq_config_default(abi.ptr(cfg)))
+        cfg["chunks_per_block"], cfg["lookback_blocks"] = chunks_per_block, lookback
+        cfg["enable_prehq"], cfg["hq_throttle_fraction"], cfg["zmw_stride"] = int(bool(enable)), throttle, zmw_stride
+        check(lib().hw_prelim_hq_create(abi.ptr(self.fields), len(self.fields), int(bool(skip_rejects)), num_zmw,
+                                        abi.ptr(cfg), C.byref(self._h)))
+        self._res = np.zeros(1, abi.BAZ_CHECKPOINT_DT)
+
+    def _checkpoint(self):
+        r = self._res[0]
+        n = self.num_zmw
+        return {"bytes": _from_device(int(r["d_bytes"]), int(r["total_bytes"])) if r["total_bytes"] else
+                torch.empty(0, dtype=torch.uint8, device="cuda"),
+                "offsets": _from_device(int(r["d_offsets"]), 8 * (n + 1)).view(torch.int64),
+                "events": _from_device(int(r["d_events"]), 4 * n).view(torch.int32),
+                "hq": _from_device(int(r["d_hq"]), n),
+                "num_hq": int(r["num_hq"]), "block": int(r["block"])}
+
+    def process(self, pulses, lens, max_calls, metrics=None, marks=None):
+        """One chunk; the block's checkpoint (views of the stage's device
+        buffers, valid until the next call) when it ends a metric block."""
+        produced = C.c_int32()
+        check(lib().hw_prelim_hq_process(self._h, _p(pulses), _p(lens), int(max_calls), _p(metrics), _p(marks),
+                                         C.byref(produced), abi.ptr(self._res), _stream()))
+        return self._checkpoint() if produced.value else None
+
+    def flush(self):
+        produced = C.c_int32()
+        check(lib().hw_prelim_hq_flush(self._h, C.byref(produced), abi.ptr(self._res), _stream()))
+        return self._checkpoint()
+
+    def activity(self):
+        out = torch.empty(self.num_zmw, dtype=torch.uint8, device="cuda")
+        check(lib().hw_prelim_hq_activity(self._h, _p(out), _stream()))
+        return out

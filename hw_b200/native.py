@@ -84,8 +84,14 @@ def lib():
         "hw_baz_encoder_create": ([vp, u32, i32, u32, PPV], C.c_int),
         "hw_baz_encoder_destroy": ([vp], C.c_int),
         "hw_baz_encoder_set_zmw_stride": ([vp, u32], C.c_int),
-        "hw_baz_encode": ([vp, vp, vp, u32, vp, C.c_uint64, vp, C.POINTER(C.c_uint64), vp], C.c_int),
-        "hw_baz_encode_async": ([vp, vp, vp, u32, vp, C.c_uint64, vp, vp], C.c_int),
+        "hw_prelim_hq_config_default": ([vp], C.c_int),
+        "hw_prelim_hq_create": ([vp, u32, i32, u32, vp, PPV], C.c_int),
+        "hw_prelim_hq_destroy": ([vp], C.c_int),
+        "hw_prelim_hq_process": ([vp, vp, vp, u32, vp, vp, C.POINTER(i32), vp, vp], C.c_int),
+        "hw_prelim_hq_flush": ([vp, C.POINTER(i32), vp, vp], C.c_int),
+        "hw_prelim_hq_activity": ([vp, vp, vp], C.c_int),
+        "hw_baz_encode": ([vp, vp, vp, u32, vp, C.c_uint64, vp, vp, C.POINTER(C.c_uint64), vp], C.c_int),
+        "hw_baz_encode_async": ([vp, vp, vp, u32, vp, C.c_uint64, vp, vp, vp], C.c_int),
         "hw_baz_encode_result": ([vp, C.POINTER(C.c_uint64)], C.c_int),
         "hw_fused_enable_hf_metrics": ([vp, u32, C.c_double, i32, vp, vp, vp, vp, vp, u32, vp, C.c_float], C.c_int),
         "hw_analyzer_chunk_metrics": ([vp, vp, vp, vp, vp], C.c_int),

@@ -630,7 +630,8 @@ int hw_baz_encoder_set_zmw_stride(hw_baz_encoder* e, uint32_t stride);
 /* Encodes one chunk: pulses [num_zmw][max_calls] with counts d_lens[num_zmw]
  * (counts above max_calls read as max_calls).
  * d_offsets[num_zmw + 1] receives each ZMW's byte range in d_bytes (capacity
- * bytes_capacity); *total_bytes the chunk's bytes.  When the chunk needs
+ * bytes_capacity), d_events[num_zmw] (may be NULL) its pulses encoded (the
+ * PacketBuffer event count); *total_bytes the chunk's bytes.  When the chunk needs
  * more than bytes_capacity (or d_bytes is NULL) the call returns
  * HW_ERR_OUT_OF_MEMORY with the offsets and *total_bytes set, the delta
  * state unchanged and the contents of d_bytes unspecified, so the same call
@@ -638,8 +639,8 @@ int hw_baz_encoder_set_zmw_stride(hw_baz_encoder* e, uint32_t stride);
  * placed by a decoupled look-back whose polls are bounded: HW_ERR_TIMEOUT if
  * one gives up); synchronises the stream once, to learn the total. */
 int hw_baz_encode(hw_baz_encoder* e, const hw_pulse* d_pulses, const uint32_t* d_lens, uint32_t max_calls,
-                  uint8_t* d_bytes, uint64_t bytes_capacity, uint64_t* d_offsets, uint64_t* total_bytes,
-                  void* stream);
+                  uint8_t* d_bytes, uint64_t bytes_capacity, uint64_t* d_offsets, uint32_t* d_events,
+                  uint64_t* total_bytes, void* stream);
 /* hw_baz_encode without the synchronisation: enqueues the chunk on the
  * stream and returns.  d_offsets[num_zmw] holds the chunk's bytes once the
  * stream reaches it; calls in a row are ordered on the stream and each one
@@ -647,8 +648,67 @@ int hw_baz_encode(hw_baz_encoder* e, const hw_pulse* d_pulses, const uint32_t* d
  * synchronising, hw_baz_encode_result reports the last finished call as
  * hw_baz_encode would have (HW_OK, HW_ERR_OUT_OF_MEMORY, HW_ERR_TIMEOUT). */
 int hw_baz_encode_async(hw_baz_encoder* e, const hw_pulse* d_pulses, const uint32_t* d_lens, uint32_t max_calls,
-                        uint8_t* d_bytes, uint64_t bytes_capacity, uint64_t* d_offsets, void* stream);
+                        uint8_t* d_bytes, uint64_t bytes_capacity, uint64_t* d_offsets, uint32_t* d_events,
+                        void* stream);
 int hw_baz_encode_result(hw_baz_encoder* e, uint64_t* total_bytes);
+
+/* ---- Preliminary HQ stage (PrelimHQFilterBody + BazAggregator packets) ------
+ * Replaces basecaller/appModules/PrelimHQFilter.cpp:63-230 with the packet
+ * side of bazio/writing/BazAggregator.h (PacketBufferManager.cpp:43-176).
+ * Each chunk's pulses are BAZ-encoded and kept on the device for the last
+ * lookback_blocks metric blocks.  At each metric block's end (every
+ * chunks_per_block chunks) the stage marks ZMWs HQ -- the reference's
+ * placeholder rule (PrelimHQFilter.cpp:163-215: all ZMWs when enable_prehq is
+ * 0; otherwise, from the lookback_blocks-th block on, every
+ * round(1 / hq_throttle_fraction)-th ZMW still pre-HQ, in ZMW order), or the
+ * caller's marks -- and produces the block's checkpoint (BazAggregator::
+ * ProduceBazBuffer): no bytes for a pre-HQ ZMW, its bytes of the block for an
+ * HQ ZMW, and for a ZMW marked HQ at this block every block of the window,
+ * oldest first; older data is dropped.  The metric side of the aggregator
+ * (metric-block lookback and aggregation) is not covered. */
+typedef struct hw_prelim_hq_config {
+    uint32_t chunks_per_block;      /* ceil(framesPerHFMetricBlock / frames per chunk) */
+    uint32_t lookback_blocks;       /* PrelimHQConfig lookbackSize (>= 1) */
+    int32_t  enable_prehq;          /* PrelimHQConfig enablePreHQ */
+    float    hq_throttle_fraction;  /* PrelimHQConfig hqThrottleFraction */
+    uint32_t zmw_stride;            /* PrelimHQConfig zmwOutputStride (divides 64) */
+    uint32_t reserved;
+} hw_prelim_hq_config;
+
+/* A checkpoint: device buffers owned by the stage, valid until its next call. */
+typedef struct hw_baz_checkpoint {
+    const uint8_t*  d_bytes;        /* total_bytes, ZMW after ZMW */
+    uint64_t        total_bytes;
+    const uint64_t* d_offsets;      /* [num_zmw + 1] */
+    const uint32_t* d_events;       /* [num_zmw] pulses in each ZMW's bytes */
+    const uint8_t*  d_hq;           /* [num_zmw] 1: HQ after this block */
+    uint32_t        num_hq;
+    uint32_t        block;          /* the metric block (from 0) */
+} hw_baz_checkpoint;
+
+/* Reference defaults: 8 chunks (4096-frame metric blocks of 512-frame
+ * chunks), lookback 10, preliminary HQ off, throttle 0.10, stride 1. */
+int hw_prelim_hq_config_default(hw_prelim_hq_config* cfg);
+typedef struct hw_prelim_hq hw_prelim_hq;
+/* fields/n_fields/skip_rejects: the pulse encoding, as hw_baz_encoder_create. */
+int hw_prelim_hq_create(const hw_baz_field* fields, uint32_t n_fields, int32_t skip_rejects, uint32_t num_zmw,
+                        const hw_prelim_hq_config* cfg, hw_prelim_hq** out);
+int hw_prelim_hq_destroy(hw_prelim_hq* h);
+/* One chunk of pulses of all num_zmw ZMWs (as hw_baz_encode).  d_metrics:
+ * the HF metrics of a block that ended with this chunk (ceil(num_zmw / 64)
+ * lanes, NULL otherwise); each ZMW's most recent activity label is kept
+ * (MetricBufferManager::GetRecentActivityLabel).  d_marks: NULL for the
+ * placeholder rule, or per ZMW 1 = mark HQ at this block's end.  When the
+ * chunk ends a metric block, *produced = 1 and *out describes the
+ * checkpoint.  Synchronises the stream (once a chunk, twice more at a
+ * block's end). */
+int hw_prelim_hq_process(hw_prelim_hq* h, const hw_pulse* d_pulses, const uint32_t* d_lens, uint32_t max_calls,
+                         const hw_basecalling_metrics* d_metrics, const uint8_t* d_marks, int32_t* produced,
+                         hw_baz_checkpoint* out, void* stream);
+/* BazAggregator::Flush: the HQ ZMWs' bytes of the chunks of the unfinished block. */
+int hw_prelim_hq_flush(hw_prelim_hq* h, int32_t* produced, hw_baz_checkpoint* out, void* stream);
+/* Each ZMW's most recent activity label (HQRFPhysicalStates; 4 before any). */
+int hw_prelim_hq_activity(hw_prelim_hq* h, uint8_t* d_out, void* stream);
 
 /* ---- Pool sets: uneven pools --------------------------
  * No single reference counterpart: the reference runs one BatchAnalyzer per

@@ -23,6 +23,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <deque>
 #include <limits>
 #include <memory>
 #include <string>
@@ -2877,6 +2878,166 @@ int or_baz_encode_chunk(const hw_baz_field* fields, uint32_t nf, int32_t skipRej
     }
     offsets[numZmw] = pos;
     return HW_OK;
+}
+
+}   // extern "C"
+
+// ---- Preliminary HQ stage -------------------------------------------------------
+// bazio/writing/PacketBufferManager.cpp:43-176 (what a checkpoint holds for
+// each ZMW: nothing while it is pre-HQ, its data of the current metric block
+// once HQ, and on the block it is marked HQ every block of the lookback
+// window, oldest first; data older than the window is dropped) and
+// basecaller/appModules/PrelimHQFilter.cpp:133-215 (DetectHQ: every ZMW marked
+// HQ when the preliminary HQ step is off; otherwise, from the lookbackSize-th
+// metric block on, every round(1/hqThrottleFraction)-th ZMW still pre-HQ, in
+// ZMW order).  Each ZMW keeps a list of per-block (bytes, events), the
+// current block last.
+
+namespace {
+
+struct PreHqOracle
+{
+    uint32_t numZmw, lookback;
+    bool enable;
+    size_t stride;
+    size_t seen = 0;
+    std::vector<uint8_t> hq;
+    std::vector<std::deque<std::pair<std::vector<uint8_t>, uint32_t>>> blocks;
+
+    PreHqOracle(uint32_t n, uint32_t lb, bool en, float throttle)
+        : numZmw(n), lookback(lb), enable(en), stride((size_t)std::round(1 / throttle)), hq(n, 0), blocks(n)
+    {
+        for (auto& d : blocks) d.emplace_back();
+    }
+
+    void Add(const uint8_t* bytes, const uint64_t* offsets, const uint32_t* events)
+    {
+        for (uint32_t z = 0; z < numZmw; ++z)
+        {
+            auto& b = blocks[z].back();
+            b.first.insert(b.first.end(), bytes + offsets[z], bytes + offsets[z + 1]);
+            b.second += events[z];
+        }
+    }
+
+    // the ZMWs newly HQ at this block's end
+    std::vector<uint8_t> Mark(const uint8_t* marks)
+    {
+        std::vector<uint8_t> newly(numZmw, 0);
+        if (marks)
+        {
+            for (uint32_t z = 0; z < numZmw; ++z) newly[z] = !hq[z] && marks[z];
+            ++seen;
+            return newly;
+        }
+        if (!enable)
+        {
+            for (uint32_t z = 0; z < numZmw; ++z) newly[z] = !hq[z];
+            return newly;
+        }
+        if (++seen < lookback) return newly;
+        size_t counter = 0;
+        for (uint32_t z = 0; z < numZmw; ++z)
+        {
+            if (hq[z]) continue;
+            if (counter % stride == 0) newly[z] = 1;
+            ++counter;
+        }
+        return newly;
+    }
+
+    // the checkpoint's bytes; false when they pass cap (nothing changes then)
+    int64_t Output(const std::vector<uint8_t>& newly, bool flush, uint8_t* out, uint64_t cap, uint64_t* offsets,
+                   uint32_t* events, uint8_t* hqOut)
+    {
+        uint64_t pos = 0;
+        std::vector<std::pair<uint64_t, uint32_t>> sizes(numZmw);
+        for (uint32_t z = 0; z < numZmw; ++z)
+        {
+            uint64_t n = 0;
+            uint32_t ev = 0;
+            if (hq[z])
+            {
+                n = blocks[z].back().first.size();
+                ev = blocks[z].back().second;
+            }
+            else if (!flush && newly[z])
+                for (const auto& b : blocks[z])
+                {
+                    n += b.first.size();
+                    ev += b.second;
+                }
+            sizes[z] = {n, ev};
+            pos += n;
+        }
+        if (pos > cap) return -1;
+        pos = 0;
+        for (uint32_t z = 0; z < numZmw; ++z)
+        {
+            offsets[z] = pos;
+            events[z] = sizes[z].second;
+            if (hq[z] || (!flush && newly[z]))
+            {
+                const size_t from = hq[z] ? blocks[z].size() - 1 : 0;
+                for (size_t i = from; i < blocks[z].size(); ++i)
+                {
+                    const auto& b = blocks[z][i].first;
+                    std::copy(b.begin(), b.end(), out + pos);
+                    pos += b.size();
+                }
+            }
+        }
+        offsets[numZmw] = pos;
+        if (!flush)
+            for (uint32_t z = 0; z < numZmw; ++z)
+            {
+                if (hq[z] || newly[z])
+                {
+                    hq[z] = 1;
+                    blocks[z].clear();
+                }
+                blocks[z].emplace_back();
+                if (blocks[z].size() > lookback) blocks[z].pop_front();
+            }
+        for (uint32_t z = 0; z < numZmw; ++z) hqOut[z] = hq[z];
+        return (int64_t)pos;
+    }
+};
+
+}   // namespace
+
+extern "C" {
+
+void* or_prehq_create(uint32_t numZmw, uint32_t lookback, int32_t enable, float throttle)
+{
+    return new PreHqOracle(numZmw, lookback, enable != 0, throttle);
+}
+
+void or_prehq_destroy(void* h) { delete static_cast<PreHqOracle*>(h); }
+
+void or_prehq_add(void* h, const uint8_t* bytes, const uint64_t* offsets, const uint32_t* events)
+{
+    static_cast<PreHqOracle*>(h)->Add(bytes, offsets, events);
+}
+
+// End of a metric block: marks (the placeholder rule, or `marks` when not
+// null), then the checkpoint.  Returns its bytes, or -1 when they pass cap
+// (the marks are then discarded and nothing changes).
+int64_t or_prehq_end_block(void* h, const uint8_t* marks, uint8_t* out, uint64_t cap, uint64_t* offsets,
+                           uint32_t* events, uint8_t* hq)
+{
+    auto* o = static_cast<PreHqOracle*>(h);
+    const size_t seen = o->seen;
+    const auto newly = o->Mark(marks);
+    const int64_t n = o->Output(newly, false, out, cap, offsets, events, hq);
+    if (n < 0) o->seen = seen;
+    return n;
+}
+
+int64_t or_prehq_flush(void* h, uint8_t* out, uint64_t cap, uint64_t* offsets, uint32_t* events, uint8_t* hq)
+{
+    auto* o = static_cast<PreHqOracle*>(h);
+    return o->Output(std::vector<uint8_t>(o->numZmw, 0), true, out, cap, offsets, events, hq);
 }
 
 }   // extern "C"

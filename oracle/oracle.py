@@ -76,6 +76,14 @@ def lib():
         L.or_baz_serializer_roundtrip.restype = C.c_uint64
         L.or_baz_float_fixed_roundtrip.argtypes = [C.c_float, i32, i32, i32, C.POINTER(C.c_uint64)]
         L.or_baz_float_fixed_roundtrip.restype = C.c_float
+        L.or_prehq_create.argtypes = [u32, u32, i32, C.c_float]
+        L.or_prehq_create.restype = vp
+        L.or_prehq_destroy.argtypes = [vp]
+        L.or_prehq_add.argtypes = [vp, vp, vp, vp]
+        L.or_prehq_end_block.argtypes = [vp, vp, vp, C.c_uint64, vp, vp, vp]
+        L.or_prehq_end_block.restype = C.c_int64
+        L.or_prehq_flush.argtypes = [vp, vp, C.c_uint64, vp, vp, vp]
+        L.or_prehq_flush.restype = C.c_int64
         L.or_baz_encode_chunk.argtypes = [vp, u32, i32, u32, u32, vp, vp, u32, vp, C.c_uint64, vp, vp]
         _lib = L
     return _lib
@@ -360,3 +368,44 @@ class BazEncoder:
                                          self.stride, abi.ptr(pulses), abi.ptr(lens), int(cap), abi.ptr(out), out_cap,
                                          abi.ptr(offsets), abi.ptr(self.last)))
         return out[:int(offsets[-1])].copy(), offsets
+
+
+class PrelimHq:
+    """PacketBufferManager checkpoints + DummyPreHQ marking (the preliminary HQ
+    stage) over per-chunk encoded bytes: add() a chunk's (bytes, offsets,
+    events), end_block() at each metric block's end."""
+
+    def __init__(self, num_zmw, lookback, enable, throttle=0.1):
+        self.n = num_zmw
+        self.h = lib().or_prehq_create(num_zmw, lookback, int(bool(enable)), float(throttle))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_prehq_destroy(self.h)
+            self.h = None
+
+    def add(self, data, offsets, events):
+        data = np.ascontiguousarray(data, np.uint8)
+        offsets = np.ascontiguousarray(offsets, np.uint64)
+        events = np.ascontiguousarray(events, np.uint32)
+        lib().or_prehq_add(self.h, abi.ptr(data) if len(data) else None, abi.ptr(offsets), abi.ptr(events))
+
+    def _out(self, fn, *args):
+        cap = 1 << 16
+        while True:
+            out = np.zeros(cap, np.uint8)
+            off = np.zeros(self.n + 1, np.uint64)
+            ev = np.zeros(self.n, np.uint32)
+            hq = np.zeros(self.n, np.uint8)
+            n = fn(self.h, *args, abi.ptr(out), cap, abi.ptr(off), abi.ptr(ev), abi.ptr(hq))
+            if n >= 0:
+                return out[:n].copy(), off, ev, hq
+            cap *= 4
+
+    def end_block(self, marks=None):
+        """(bytes, offsets[n + 1], events[n], hq[n]) of the block's checkpoint."""
+        m = None if marks is None else np.ascontiguousarray(marks, np.uint8)
+        return self._out(lib().or_prehq_end_block, abi.ptr(m) if m is not None else None)
+
+    def flush(self):
+        return self._out(lib().or_prehq_flush)

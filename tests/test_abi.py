@@ -50,7 +50,7 @@ int main(void) {
   S(hw_config) S(hw_analog) S(hw_stat_accum_state) S(hw_autocorr_accum_state) S(hw_baseliner_stats)
   S(hw_lane_analog_mode) S(hw_lane_model) S(hw_lane_histogram) S(hw_lane_hist_bounds) S(hw_pulse)
   S(hw_dme_diag) S(hw_frame_interval) S(hw_gen_params) S(hw_pool_chunk) S(hw_fused_tuning)
-  S(hw_basecalling_metrics) S(hw_sensor_packet) S(hw_baz_field)
+  S(hw_basecalling_metrics) S(hw_sensor_packet) S(hw_baz_field) S(hw_prelim_hq_config) S(hw_baz_checkpoint)
   O(hw_baseliner_stats, full_autocorr) O(hw_baseliner_stats, trace_min) O(hw_baseliner_stats, trace_max)
   O(hw_baseliner_stats, baseline_stats) O(hw_baseliner_stats, raw_baseline_sum) O(hw_baseliner_stats, background_stats)
   O(hw_lane_model, analogs) O(hw_lane_model, baseline) O(hw_lane_model, confidence)
@@ -66,6 +66,8 @@ int main(void) {
   O(hw_basecalling_metrics, pixel_checksum)
   O(hw_sensor_packet, start_zmw) O(hw_sensor_packet, num_blocks)
   O(hw_baz_field, transform) O(hw_baz_field, num_bits) O(hw_baz_field, overflow_bytes)
+  O(hw_prelim_hq_config, hq_throttle_fraction) O(hw_prelim_hq_config, zmw_stride)
+  O(hw_baz_checkpoint, d_hq) O(hw_baz_checkpoint, num_hq) O(hw_baz_checkpoint, block)
   O(hw_config, analogs) O(hw_config, filter_type) O(hw_config, max_calls_per_zmw) O(hw_config, xsp_amp_thresh)
   O(hw_config, model_estimation_mode) O(hw_config, static_baseline_variance)
   return 0;
@@ -109,7 +111,8 @@ def test_struct_offsets_match_python_mirrors(layout):
               "hw_lane_histogram": abi.LANE_HIST_DT, "hw_pulse": abi.PULSE_DT,
               "hw_dme_diag": abi.DME_DIAG_DT, "hw_pool_chunk": abi.POOL_CHUNK_DT,
               "hw_fused_tuning": abi.FUSED_TUNING_DT, "hw_basecalling_metrics": abi.BASECALLING_METRICS_DT,
-              "hw_sensor_packet": abi.SENSOR_PACKET_DT, "hw_baz_field": abi.BAZ_FIELD_DT}[t]
+              "hw_sensor_packet": abi.SENSOR_PACKET_DT, "hw_baz_field": abi.BAZ_FIELD_DT,
+              "hw_prelim_hq_config": abi.PRELIM_HQ_CONFIG_DT, "hw_baz_checkpoint": abi.BAZ_CHECKPOINT_DT}[t]
         assert dt.fields[m][1] == off, key
 
 

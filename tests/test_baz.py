@@ -402,6 +402,11 @@ def _gpu_vs_oracle(f, skip, chunks, nz, cap, seed, max_len=None, stride=1):
         got, goff = gpu(d_p, d_l, cap)
         assert goff.cpu().numpy().astype(np.uint64).tolist() == woff.tolist()
         assert got.cpu().numpy().tobytes() == want.tobytes()
+        kept = np.minimum(lens, cap)[:, None] > np.arange(cap)[None, :]
+        if skip:
+            kept &= p["is_reject"] == 0
+        kept[(np.arange(nz) % 64) % stride != 0] = False
+        assert (gpu.events.cpu().numpy() == kept.sum(axis=1)).all()
         total += len(want)
     gpu.close()
     return total
@@ -445,7 +450,7 @@ def test_gpu_encoder_edges():
     small = torch.zeros(4, dtype=torch.uint8, device="cuda")
     total = C.c_uint64()
     rc = native.lib().hw_baz_encode(gpu._h, C.c_void_p(d_p.data_ptr()), C.c_void_p(d_l.data_ptr()), cap,
-                                    C.c_void_p(small.data_ptr()), 4, C.c_void_p(gpu.offsets.data_ptr()),
+                                    C.c_void_p(small.data_ptr()), 4, C.c_void_p(gpu.offsets.data_ptr()), None,
                                     C.byref(total), None)
     assert rc == abi.HW_ERR_OUT_OF_MEMORY and total.value > 4
     want, woff = ref(p, lens, cap)
@@ -455,7 +460,7 @@ def test_gpu_encoder_edges():
     exact = torch.zeros(total.value, dtype=torch.uint8, device="cuda")
     rc = native.lib().hw_baz_encode(gpu._h, C.c_void_p(d_p.data_ptr()), C.c_void_p(d_l.data_ptr()), cap,
                                     C.c_void_p(exact.data_ptr()), total.value, C.c_void_p(gpu.offsets.data_ptr()),
-                                    C.byref(total), None)
+                                    None, C.byref(total), None)
     assert rc == 0 and exact.cpu().numpy().tobytes() == want.tobytes()
     want, _ = ref(p, lens, cap)
     got, _ = gpu(d_p, d_l, cap)
