@@ -554,3 +554,38 @@ def test_gpu_encoder_async_calls_in_a_row():
         n = int(offs[c][-1].item())
         assert n == len(want[c])
         assert outs[c][:n].cpu().numpy().tobytes() == want[c].tobytes(), c
+
+
+@pytest.mark.gpu
+def test_gpu_encoder_chip_size_properties():
+    """1,048,576 ZMWs (8192 tiles): offsets rise by each ZMW's bytes, event
+    counts equal the kept pulses, and a sample of ZMWs spread over the whole
+    chip decodes back to their pulses' labels, widths and starts (delta state
+    from the previous chunk carried)."""
+    import torch
+    import oracle
+    from hw_b200 import filters as Fl
+    nz, cap = 1 << 20, 12
+    f, skip = preset(abi.BAZ_PRODUCTION)
+    rng = np.random.default_rng(17)
+    gpu = Fl.BazEncoder(nz, fields=f, skip_rejects=skip)
+    sample = np.sort(rng.choice(nz, 512, replace=False))
+    last = np.zeros((nz, len(f)), np.uint64)
+    for chunk in range(2):
+        p, lens = random_pulses(rng, nz, cap)
+        d_p = torch.from_numpy(p.view(np.uint8).reshape(-1)).cuda()
+        d_l = torch.from_numpy(lens.view(np.int32)).cuda()
+        data, off = gpu(d_p, d_l, cap)
+        off = off.cpu().numpy().astype(np.uint64)
+        data = data.cpu().numpy()
+        kept = (np.minimum(lens, cap)[:, None] > np.arange(cap)[None, :]) & (p["is_reject"] == 0)
+        n_kept = kept.sum(axis=1)
+        assert (gpu.events.cpu().numpy() == n_kept).all()
+        assert off[0] == 0 and (np.diff(off.astype(np.int64)) >= 0).all() and off[-1] == len(data)
+        for z in sample:
+            k = p[z, :lens[z]]
+            k = k[k["is_reject"] == 0]
+            back, used = oracle.baz_decode_values(f, data[off[z]:off[z + 1]], len(k), last[z])
+            assert used == off[z + 1] - off[z]
+            for name in ("label", "width", "start"):
+                assert back[name].tolist() == k[name].tolist(), (chunk, z, name)
