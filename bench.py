@@ -19,6 +19,9 @@ scaling, no data exchange).
           host memory and the pulse output copied back inside the timed region
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl hw|reference]
+       python bench.py --next-rows    (the stages after and before the chain:
+           HF metrics, ingest repacking, BAZ encoding, preliminary HQ -- each
+           timed on the GPU and its CPU restatement on a bounded sample)
 """
 import argparse
 import json
@@ -52,6 +55,8 @@ def parse():
     ap.add_argument("--cpu-lanes", type=int, default=512, help="lanes in the CPU-baseline sample")
     ap.add_argument("--cpu-steps", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--next-rows", action="store_true",
+                    help="time the HF metrics, repacking, BAZ and preliminary HQ stages, GPU and CPU")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned-init", action="store_true",
                     help="skip the learned DME initializer measurement (config 3)")
@@ -172,6 +177,118 @@ def cpu_baseline(cfg, lanes, steps, warmup, threads):
     return zf / t_timed, t_timed
 
 
+def next_rows(threads):
+    """The four stages beside the chain, each on the GPU (CUDA events, chip
+    sizes) and as the CPU restatement (the oracle, one host thread: these
+    restatements are sequential, on a bounded sample of the same inputs).
+    One JSON line."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from hw_b200 import abi, filters as Fl, workloads
+    from hw_b200 import baz as bazm, prehq as prehqm, repack as repackm
+    oracle.set_threads(threads)
+    out = {"metric": "next rows: GPU and CPU rates", "cpu_cores": 1}
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    # HF metrics on the chain's own chunk outputs (a 4096-lane pool, small configuration)
+    lanes, F = 4096, FRAMES
+    cfg = workloads.small_config()
+    an = Fl.BatchAnalyzer(cfg, 0, lanes, F)
+    gen = Fl.TraceGenerator(lanes, workload=1)
+    cart = dict(np.load(os.path.join(ROOT, "tests", "golden", "trained_cart.npz")))
+    inputs = []
+    for c in range(16):
+        pulses, lens, ovf, em, est = an(gen.next(c * F, F), c * F)
+        if em:
+            bs, vit, pd = an.chunk_metrics()
+            models, _ = an.models()
+            inputs.append((pulses.clone(), lens.clone(), bs.clone(), models.clone(), vit.clone(), pd.clone(),
+                           c * F - abi.LATENT_FRAMES))
+    cap = cfg.max_calls_per_zmw
+    hf = Fl.HfMetrics(lanes, 4096, cfg.frame_rate, True, cart=cart)
+    for x in inputs[:2]:
+        hf.process(x[0], x[1], cap, *x[2:6], x[6], F)
+    torch.cuda.synchronize()
+    ev0.record()
+    for x in inputs[2:]:
+        hf.process(x[0], x[1], cap, *x[2:6], x[6], F)
+    ev1.record()
+    ev1.synchronize()
+    n = len(inputs) - 2
+    gpu_rate = lanes * 64 * F * n / (ev0.elapsed_time(ev1) / 1e3)
+    sl = lanes   # CPU sample: the whole pool
+    ref = oracle.HfMetrics(sl, 4096, cfg.frame_rate, True)
+    ref.set_cart(cart)
+    host = [(Fl.struct_to_numpy(x[0], abi.PULSE_DT).reshape(lanes, 64, cap)[:sl].copy(),
+             x[1].cpu().numpy().astype(np.uint32).reshape(lanes, 64)[:sl].copy(),
+             Fl.struct_to_numpy(x[2], abi.BLSTATS_DT)[:sl].copy(), Fl.struct_to_numpy(x[3], abi.LANE_MODEL_DT)[:sl].copy(),
+             x[4].cpu().numpy().reshape(lanes, 64)[:sl].copy(), Fl.struct_to_numpy(x[5], abi.STAT_ACCUM_DT)[:sl].copy(),
+             x[6]) for x in inputs]
+    t0 = time.perf_counter()
+    for h in host:
+        ref.process(*h[:6], h[6], F)
+    cpu_s = time.perf_counter() - t0
+    out["hf_metrics"] = {"unit": "ZMW-frames/s", "gpu": gpu_rate,
+                         "cpu": sl * 64 * F * len(host) / cpu_s,
+                         "gpu_workload": f"{lanes} lanes, {n} chunks of {F} frames of the chain's outputs",
+                         "cpu_sample": f"{sl} lanes, {len(host)} chunks ({cpu_s:.2f} s)"}
+    del an, inputs, host
+
+    # ingest repacking: the chip chunk on the GPU; 16,384 ZMWs of it on the CPU
+    r = repackm.run(steps=10)
+    nz_s = 131072
+    table, nbytes = repackm.chip_packets(nz_s, F)
+    data = np.random.default_rng(1).integers(0, 255, nbytes, dtype=np.uint8)
+    chunks = [np.zeros((nz_s // 64, F, 64), np.int16)]
+    t0 = time.perf_counter()
+    for _ in range(10):
+        oracle.repack(nz_s, nz_s // 64, F, 0, table, data, 0, chunks)
+    cpu_s = (time.perf_counter() - t0) / 10
+    out["repack"] = {"unit": "ZMW-frames/s", "gpu": r["zmw_frames_per_s"], "cpu": nz_s * F / cpu_s,
+                     "gpu_workload": r["workload"], "cpu_sample": f"{nz_s} ZMWs x {F} frames ({cpu_s:.3f} s a chunk)"}
+
+    # BAZ encoding: consecutive chip chunks on the GPU; 32,768 ZMWs of them on the CPU
+    b = bazm.run(steps=5, warmup=3)
+    pool_chunks, cap = bazm.chain_pulses(3)
+    nz_s = 262144
+    fields, skip = Fl.baz_preset(abi.BAZ_PRODUCTION)
+    enc = oracle.BazEncoder(fields, skip, nz_s)
+    host = [(Fl.struct_to_numpy(p, abi.PULSE_DT).reshape(-1, cap)[:nz_s].copy(),
+             l.cpu().numpy().astype(np.uint32).reshape(-1)[:nz_s].copy()) for p, l in pool_chunks]
+    t0 = time.perf_counter()
+    npul = 0
+    for p, l in host:
+        enc(p, l, cap)
+        npul += int(l.sum())
+    cpu_s = time.perf_counter() - t0
+    nz_s = 32768
+    host = [(p[:nz_s].copy(), l[:nz_s].copy()) for p, l in host]
+    out["baz_encoding"] = {"unit": "pulses/s", "gpu": b["pulses_per_s"], "cpu": npul / cpu_s,
+                           "gpu_workload": b["workload"], "cpu_sample": f"262144 ZMWs x {len(host)} chunks, "
+                                                                        f"{npul} pulses ({cpu_s:.2f} s)"}
+
+    # preliminary HQ: the chip stage on the GPU; 32,768 ZMWs through encoding + stage on the CPU
+    q = prehqm.run(blocks=2, warmup_blocks=11)
+    st = oracle.PrelimHq(nz_s, 10, True, 0.10)
+    enc = oracle.BazEncoder(fields, skip, nz_s)
+    t0 = time.perf_counter()
+    nchunks = 0
+    for blk in range(13):
+        for c in range(8):
+            p, l = host[(blk * 8 + c) % len(host)]
+            d, off = enc(p, l, cap)
+            kept = (np.minimum(l, cap)[:, None] > np.arange(cap)[None, :]) & (p["is_reject"] == 0)
+            st.add(d, off, kept.sum(axis=1).astype(np.uint32))
+            nchunks += 1
+        st.end_block()
+    cpu_s = time.perf_counter() - t0
+    out["prelim_hq"] = {"unit": "ZMW-frames/s", "gpu": q["zmw_frames_per_s"], "cpu": nz_s * F * nchunks / cpu_s,
+                        "gpu_workload": q["workload"],
+                        "cpu_sample": f"{nz_s} ZMWs x {nchunks} chunks, encoding included ({cpu_s:.2f} s)"}
+    print(json.dumps(out))
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup()
@@ -183,6 +300,10 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
     from hw_b200 import filters as Fl, workloads
+    if args.next_rows:
+        if rank == 0:
+            next_rows(os.cpu_count() or 1)
+        return
     cfg = workloads.chip_config()
     total_lanes = args.lanes_per_pool * args.pools
     zmws = total_lanes * 64
