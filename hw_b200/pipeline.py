@@ -38,8 +38,11 @@ def packets_from_traces(tr):
     return tr.view(lanes // 2, 2, F, 64).permute(0, 2, 1, 3).contiguous().view(torch.uint8).reshape(-1)
 
 
-def run(steps=24, warmup_steps=40, n_inputs=8):
-    cfg = workloads.chip_config()
+def run(steps=24, warmup_steps=40, n_inputs=8, pools=POOLS, lanes=LANES, cfg=None, collect=None):
+    """collect: a list that receives (step, pool, checkpoint copy) for every
+    checkpoint (tests)."""
+    POOLS, LANES = pools, lanes
+    cfg = workloads.chip_config() if cfg is None else cfg
     nz = POOLS * LANES * 64
     gen = Fl.TraceGenerator(POOLS * LANES, workload=1)
     table, nbytes = chip_packets(nz, F)
@@ -56,7 +59,7 @@ def run(steps=24, warmup_steps=40, n_inputs=8):
     hq = [Fl.PrelimHq(LANES * 64, chunks_per_block=8, lookback=10, enable=False) for _ in range(POOLS)]
     # each pool's checkpoints land in its own pinned buffer, copied on a side
     # stream that overlaps the next steps' analysis
-    host = [torch.empty(256 << 20, dtype=torch.uint8, pin_memory=True) for _ in range(POOLS)]
+    host = [torch.empty(min(256 << 20, LANES * 64 * 8 * 64), dtype=torch.uint8, pin_memory=True) for _ in range(POOLS)]
     copy_stream = torch.cuda.Stream()
     copied = [None] * POOLS
     s = torch.cuda.current_stream()
@@ -88,10 +91,14 @@ def run(steps=24, warmup_steps=40, n_inputs=8):
             pulses, lens, _ = eng.outputs(p)
             out = hq[p].process(pulses, lens, cfg.max_calls_per_zmw,
                                 metrics=eng.metrics[p] if m_em[p] else None)
+            if out is not None and collect is not None:
+                collect.append((c, p, {k: (v.clone() if torch.is_tensor(v) else v) for k, v in out.items()}))
             if out is not None:
                 n = out["bytes"].numel()
                 if copied[p] is not None:
                     copied[p].synchronize()   # the pool's previous checkpoint is out
+                if n > host[p].numel():
+                    host[p] = torch.empty(n + n // 4, dtype=torch.uint8, pin_memory=True)
                 ready = torch.cuda.Event()
                 ready.record(s)
                 with torch.cuda.stream(copy_stream):
