@@ -525,6 +525,9 @@ __global__ void __launch_bounds__(kThreads) BazTileKernel(const __grid_constant_
     {
         tileSh = (uint32_t)(atomicAdd(a.ticket, 1ull) - a.ticketBase);
         curSh = *a.cur;
+        // the first tile clears the look-back failure word of an earlier call
+        // (a tile can only give up long after every tile has started)
+        if (tileSh == 0) a.host[1] = 0;
     }
     __syncthreads();
     const uint32_t tile = tileSh;
@@ -849,6 +852,8 @@ int hw_baz_encoder_create(const hw_baz_field* fields, uint32_t n_fields, int32_t
     if (ce == cudaSuccess) ce = cudaMalloc((void**)&e->status, sizeof(unsigned long long) * (e->numTiles + 1));
     if (ce == cudaSuccess) ce = cudaMemset(e->status, 0, sizeof(unsigned long long) * (e->numTiles + 1));
     if (ce == cudaSuccess) ce = cudaHostAlloc((void**)&e->host, 4 * sizeof(uint64_t), cudaHostAllocMapped);
+    if (ce == cudaSuccess)
+        for (int i = 0; i < 4; ++i) e->host[i] = 0;   // pinned memory comes uninitialised
     if (ce == cudaSuccess) ce = cudaHostGetDevicePointer((void**)&e->hostDev, e->host, 0);
     if (ce != cudaSuccess)
     {
