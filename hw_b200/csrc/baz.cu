@@ -292,7 +292,7 @@ struct TileArgs
     uint64_t capacity;
     unsigned long long* status;       // [numTiles] look-back words
     unsigned long long* ticket;
-    unsigned long long ticketBase;    // tickets taken by earlier calls
+    unsigned long long ticketBase;    // the ticket counter's value at launch (0: reset by the call)
     unsigned long long epoch;         // this call's tag in the look-back words
     volatile uint64_t* host;          // mapped: [0] total bytes, [1] look-back gave up, [2] encoded
 };
@@ -717,7 +717,6 @@ struct hw_baz_encoder
     uint64_t* state = nullptr;     // [2][slots][numZmw] delta state
     uint32_t* cur = nullptr;       // device: the state copy the next call reads
     unsigned long long* status = nullptr;   // [numTiles] look-back words, then the ticket counter
-    unsigned long long tickets = 0;         // tickets taken by earlier calls
     unsigned long long epoch = 0;           // the last call's tag (20 bits; 0 never used)
     uint64_t* host = nullptr;      // mapped pinned words
     uint64_t* hostDev = nullptr;
@@ -740,6 +739,7 @@ cudaError_t Launch(uint32_t tiles, const BazSpec& spec, const TileArgs& a, cudaS
         if (ce != cudaSuccess) return ce;
         devicesSet.fetch_or(bit);
     }
+    (void)cudaGetLastError();   // an earlier, unrelated failure is not this launch's
     BazTileKernel<Spec><<<tiles, kThreads, DynSmem<Spec>(), s>>>(spec, a);
     return cudaGetLastError();
 }
@@ -753,10 +753,11 @@ int Enqueue(hw_baz_encoder* e, const hw_pulse* d_pulses, const uint32_t* d_lens,
     if (++e->epoch == (1ull << 20))
     {
         // the tags wrap: clear the words so no word of an old call reads as this one's
-        ce = cudaMemsetAsync(e->status, 0, sizeof(unsigned long long) * (e->numTiles + 1), s);
+        ce = cudaMemsetAsync(e->status, 0, sizeof(unsigned long long) * e->numTiles, s);
         e->epoch = 1;
-        e->tickets = 0;
     }
+    // tickets count from 0 every call, whatever became of earlier launches
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(e->status + e->numTiles, 0, sizeof(unsigned long long), s);
     TileArgs a;
     a.pulses = d_pulses;
     a.lens = d_lens;
@@ -772,7 +773,7 @@ int Enqueue(hw_baz_encoder* e, const hw_pulse* d_pulses, const uint32_t* d_lens,
     a.capacity = bytes_capacity;
     a.status = e->status;
     a.ticket = e->status + e->numTiles;
-    a.ticketBase = e->tickets;
+    a.ticketBase = 0;
     a.epoch = e->epoch;
     a.host = e->hostDev;
     if (ce == cudaSuccess)
@@ -782,7 +783,6 @@ int Enqueue(hw_baz_encoder* e, const hw_pulse* d_pulses, const uint32_t* d_lens,
         else ce = Launch<RtFields>(e->numTiles, e->spec, a, s);
     }
     if (ce != cudaSuccess) return Fail(HW_ERR_CUDA, std::string("hw_baz_encode: ") + cudaGetErrorString(ce));
-    e->tickets += e->numTiles;
     return HW_OK;
 }
 
