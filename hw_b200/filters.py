@@ -675,3 +675,29 @@ class PrelimHq(_Handle):
         out = torch.empty(self.num_zmw, dtype=torch.uint8, device="cuda")
         check(lib().hw_prelim_hq_activity(self._h, _p(out), _stream()))
         return out
+
+
+class PulseCompactor(_Handle):
+    """hw_pulses_compact: the valid pulse records packed ZMW after ZMW, for
+    the download of a chunk's results."""
+    _destroy = "hw_pulse_compactor_destroy"
+
+    def __init__(self, num_zmw):
+        super().__init__()
+        self.num_zmw = num_zmw
+        check(lib().hw_pulse_compactor_create(num_zmw, C.byref(self._h)))
+
+    def __call__(self, pulses, lens, max_calls, out, offsets):
+        """Enqueues the packing into out (CUDA uint8 tensor of num_zmw x
+        max_calls records) and offsets (int64, num_zmw + 1); returns the
+        mapped slot that will hold the total."""
+        slot = C.c_uint32()
+        check(lib().hw_pulses_compact(self._h, _p(pulses), _p(lens), int(max_calls), _p(out), _p(offsets),
+                                      C.byref(slot), _stream()))
+        return slot.value
+
+    def total(self, slot):
+        """Records packed by the call that used `slot` (once the stream passed it)."""
+        t = C.c_uint64()
+        check(lib().hw_pulse_compactor_total(self._h, int(slot), C.byref(t)))
+        return t.value

@@ -652,6 +652,21 @@ int hw_baz_encode_async(hw_baz_encoder* e, const hw_pulse* d_pulses, const uint3
                         void* stream);
 int hw_baz_encode_result(hw_baz_encoder* e, uint64_t* total_bytes);
 
+/* ---- Pulse compaction (for the download of a chunk's results) --------------
+ * The pulse accumulator's output keeps max_calls slots a ZMW (BatchVectors,
+ * DT/BatchVectors.h); hw_pulses_compact packs the valid records ZMW after
+ * ZMW: d_out[d_offsets[z] .. d_offsets[z + 1]) are ZMW z's min(d_lens[z],
+ * max_calls) pulses, d_offsets[num_zmw] their total.  The total is also
+ * left in one of two mapped host slots (*slot says which), readable with
+ * hw_pulse_compactor_total once the stream has passed the call, so a caller
+ * can size the copy of one call's records while the next call is queued. */
+typedef struct hw_pulse_compactor hw_pulse_compactor;
+int hw_pulse_compactor_create(uint32_t num_zmw, hw_pulse_compactor** out);
+int hw_pulse_compactor_destroy(hw_pulse_compactor* h);
+int hw_pulses_compact(hw_pulse_compactor* h, const hw_pulse* d_pulses, const uint32_t* d_lens, uint32_t max_calls,
+                      hw_pulse* d_out, uint64_t* d_offsets, uint32_t* slot, void* stream);
+int hw_pulse_compactor_total(const hw_pulse_compactor* h, uint32_t slot, uint64_t* total);
+
 /* ---- Preliminary HQ stage (PrelimHQFilterBody + BazAggregator packets) ------
  * Replaces basecaller/appModules/PrelimHQFilter.cpp:63-230 with the packet
  * side of bazio/writing/BazAggregator.h (PacketBufferManager.cpp:43-176).
