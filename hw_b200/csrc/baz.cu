@@ -37,7 +37,7 @@ constexpr int kThreads = 256;        // runs of pulses a tile
 constexpr uint64_t kFfNan = 0, kFfInf = 1, kFfNinf = 2, kFfOffset = 3;   // FloatFixedCodec codes
 // look-back flags (top two bits of a tile's word): count published, inclusive total published
 constexpr unsigned long long kFlagAgg = 1ull << 62, kFlagInc = 2ull << 62;
-constexpr int kSpinLimit = 1 << 22;  // polls of a predecessor's status (about 0.4 s) before giving up
+constexpr uint32_t kSpinLimit = 1u << 22;  // default bound on polls of a predecessor's status (about 0.4 s)
 
 struct BazSpec
 {
@@ -294,6 +294,8 @@ struct TileArgs
     unsigned long long* ticket;
     unsigned long long ticketBase;    // the ticket counter's value at launch (0: reset by the call)
     unsigned long long epoch;         // this call's tag in the look-back words
+    uint32_t spinLimit;               // polls of a predecessor's word before giving up
+    int32_t withhold;                 // tests: this tile never publishes (-1: none)
     volatile uint64_t* host;          // mapped: [0] total bytes, [1] look-back gave up, [2] encoded
 };
 
@@ -340,10 +342,10 @@ __device__ uint64_t LookBack(const TileArgs& a, uint32_t tile, uint64_t agg, boo
     const int lane = threadIdx.x & 31;
     const unsigned long long tag = a.epoch << kEpochShift;
     gaveUp = false;
-    if (tile == 0) return 0;
+    if (tile == 0 || (int32_t)tile == a.withhold) return 0;
     uint64_t excl = 0;
     int hi = (int)tile - 1;
-    int spins = 0;
+    uint32_t spins = 0;
     while (true)
     {
         const int idx = hi - lane;
@@ -352,7 +354,7 @@ __device__ uint64_t LookBack(const TileArgs& a, uint32_t tile, uint64_t agg, boo
         const int flag = mine ? (int)(w >> 62) : 0;
         if (__ballot_sync(~0u, flag == 0))
         {
-            if (++spins > kSpinLimit)
+            if ((uint32_t)++spins > a.spinLimit)
             {
                 gaveUp = true;
                 if (lane == 0) a.host[1] = 1;
@@ -587,7 +589,7 @@ __global__ void __launch_bounds__(kThreads) BazTileKernel(const __grid_constant_
     uint32_t runOff, tileBytes;
     Scan(scanTmp).ExclusiveSum(mine, runOff, tileBytes);
     runOffSh[tid] = runOff;
-    if (tid == 0) PublishCount(a, tile, tileBytes);
+    if (tid == 0 && (int32_t)tile != a.withhold) PublishCount(a, tile, tileBytes);
     // sweep 2 into shared memory before the look-back, when the tile fits
     const bool staged = tileBytes <= (uint32_t)kOut;
     if (staged) Run<Spec, true>(F, tv, i0, i1, reinterpret_cast<uint8_t*>(ostage) + runOff, nullptr, nullptr);
@@ -718,6 +720,8 @@ struct hw_baz_encoder
     uint32_t* cur = nullptr;       // device: the state copy the next call reads
     unsigned long long* status = nullptr;   // [numTiles] look-back words, then the ticket counter
     unsigned long long epoch = 0;           // the last call's tag (20 bits; 0 never used)
+    uint32_t spinLimit = kSpinLimit;        // look-back polls before a tile gives up
+    int32_t withhold = -1;                  // tests: a tile that never publishes
     uint64_t* host = nullptr;      // mapped pinned words
     uint64_t* hostDev = nullptr;
     ~hw_baz_encoder() { cudaFree(state); cudaFree(status); cudaFreeHost(host); }
@@ -775,6 +779,8 @@ int Enqueue(hw_baz_encoder* e, const hw_pulse* d_pulses, const uint32_t* d_lens,
     a.ticket = e->status + e->numTiles;
     a.ticketBase = 0;
     a.epoch = e->epoch;
+    a.spinLimit = e->spinLimit;
+    a.withhold = e->withhold;
     a.host = e->hostDev;
     if (ce == cudaSuccess)
     {
@@ -867,6 +873,14 @@ int hw_baz_encoder_create(const hw_baz_field* fields, uint32_t n_fields, int32_t
 int hw_baz_encoder_destroy(hw_baz_encoder* e)
 {
     delete e;
+    return HW_OK;
+}
+
+int hw_baz_encoder_set_wait_limit(hw_baz_encoder* e, uint32_t polls, int32_t withhold_tile)
+{
+    if (!e || polls == 0) return Fail(HW_ERR_INVALID_ARG, "hw_baz_encoder_set_wait_limit: bad argument");
+    e->spinLimit = polls;
+    e->withhold = withhold_tile;
     return HW_OK;
 }
 

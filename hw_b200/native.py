@@ -84,6 +84,7 @@ def lib():
         "hw_baz_encoder_create": ([vp, u32, i32, u32, PPV], C.c_int),
         "hw_baz_encoder_destroy": ([vp], C.c_int),
         "hw_baz_encoder_set_zmw_stride": ([vp, u32], C.c_int),
+        "hw_baz_encoder_set_wait_limit": ([vp, u32, i32], C.c_int),
         "hw_pulse_compactor_create": ([u32, PPV], C.c_int),
         "hw_pulse_compactor_destroy": ([vp], C.c_int),
         "hw_pulses_compact": ([vp, vp, vp, u32, vp, vp, C.POINTER(u32), vp], C.c_int),

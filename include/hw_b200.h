@@ -627,6 +627,12 @@ int hw_baz_encoder_destroy(hw_baz_encoder* e);
  * zmwOutputStride, PrelimHQFilter.cpp:107-118); the others get empty byte
  * ranges and keep their state.  stride divides 64 (default 1). */
 int hw_baz_encoder_set_zmw_stride(hw_baz_encoder* e, uint32_t stride);
+/* The bound on a tile's look-back: after `polls` reads of a predecessor's
+ * word that is not ready (about 100 ns apart; default 4,194,304) the tile
+ * gives up and the call returns HW_ERR_TIMEOUT with the delta state
+ * unchanged.  withhold_tile >= 0 makes that tile never publish its count --
+ * for tests of the bounded wait only; -1 for normal use. */
+int hw_baz_encoder_set_wait_limit(hw_baz_encoder* e, uint32_t polls, int32_t withhold_tile);
 /* Encodes one chunk: pulses [num_zmw][max_calls] with counts d_lens[num_zmw]
  * (counts above max_calls read as max_calls).
  * d_offsets[num_zmw + 1] receives each ZMW's byte range in d_bytes (capacity

@@ -589,3 +589,32 @@ def test_gpu_encoder_chip_size_properties():
             assert used == off[z + 1] - off[z]
             for name in ("label", "width", "start"):
                 assert back[name].tolist() == k[name].tolist(), (chunk, z, name)
+
+
+@pytest.mark.gpu
+def test_gpu_encoder_bounded_wait_reports_timeout():
+    """A tile that never publishes its count (a test hook): the tiles after
+    it stop waiting after the poll bound, the call returns HW_ERR_TIMEOUT
+    with the delta state unchanged, and the next call encodes the chunk as
+    the oracle does -- the context stays usable, nothing faults or hangs."""
+    import torch
+    import oracle
+    from hw_b200 import filters as Fl, native
+    f, skip = preset(abi.BAZ_PRODUCTION)
+    nz, cap = 128 * 40, 16
+    rng = np.random.default_rng(31)
+    p, lens = random_pulses(rng, nz, cap)
+    gpu = Fl.BazEncoder(nz, fields=f, skip_rejects=skip)
+    ref = oracle.BazEncoder(f, skip, nz)
+    d_p = torch.from_numpy(p.view(np.uint8).reshape(-1).copy()).cuda()
+    d_l = torch.from_numpy(lens.view(np.int32)).cuda()
+    lib = native.lib()
+    assert lib.hw_baz_encoder_set_wait_limit(gpu._h, 4096, 5) == 0
+    with pytest.raises(native.HwError) as err:
+        gpu(d_p, d_l, cap)
+    assert err.value.code == 7 and "HW_ERR_TIMEOUT" in str(err.value)
+    assert lib.hw_baz_encoder_set_wait_limit(gpu._h, 1 << 22, -1) == 0
+    want, woff = ref(p, lens, cap)
+    got, goff = gpu(d_p, d_l, cap)
+    assert goff.cpu().numpy().astype(np.uint64).tolist() == woff.tolist()
+    assert got.cpu().numpy().tobytes() == want.tobytes()
