@@ -896,6 +896,7 @@ int hw_baz_encode(hw_baz_encoder* e, const hw_pulse* d_pulses, const uint32_t* d
                   uint8_t* d_bytes, uint64_t bytes_capacity, uint64_t* d_offsets, uint32_t* d_events,
                   uint64_t* total_bytes, void* stream)
 {
+    const NvtxRange range("hw_baz_encode");
     if (!e || !d_pulses || !d_lens || !d_offsets || !total_bytes || max_calls == 0)
         return Fail(HW_ERR_INVALID_ARG, "hw_baz_encode: bad argument");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);

@@ -1012,6 +1012,7 @@ static int AnalyzerProcess(hw_analyzer* a, const int16_t* d_trace, const uint8_t
 int hw_analyzer_process(hw_analyzer* a, const int16_t* d_trace, int32_t first_frame, hw_pulse* d_pulses,
                         uint32_t* d_lens, uint32_t* d_overflows, int32_t* emitted, int32_t* estimated, void* stream)
 {
+    const hwk::NvtxRange range("hw_analyzer_process");
     return AnalyzerProcess(a, d_trace, nullptr, first_frame, d_pulses, d_lens, d_overflows, emitted, estimated, stream);
 }
 

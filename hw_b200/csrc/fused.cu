@@ -737,6 +737,7 @@ int hw_fused_set_tuning(hw_fused* f, const hw_fused_tuning* t, uint32_t n)
 
 int hw_chunk_fused(hw_fused* f, hw_pool_chunk* table, uint32_t n_pools, void* stream)
 {
+    const hwk::NvtxRange range("hw_chunk_fused");
     if (!f || !table) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
     if (n_pools != f->pools.size()) return Fail(HW_ERR_INVALID_ARG, "the table must list every pool of the engine");
     for (uint32_t p = 0; p < n_pools; ++p)

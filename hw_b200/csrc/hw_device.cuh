@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
 #include "../../include/hw_b200.h"
@@ -296,6 +297,16 @@ cudaError_t LaunchPulses(const PulseArgs& a, const KParams& k, cudaStream_t s);
 struct GenArgs;
 // Records the thread's last error message (capi.cu) and returns code.
 int SetLastError(int code, const char* msg);
+
+// A named NVTX range for the life of the object (header-only NVTX3: nothing
+// happens unless a profiler is attached).
+struct NvtxRange
+{
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 // Configuration checks and derived constants without heap allocation on success.
 int PrepareConfigNoAlloc(const hw_config* cfg, hwp::Derived* d, KParams* k);
 cudaError_t LaunchGen(const GenArgs& a, cudaStream_t s);

@@ -464,6 +464,7 @@ int hw_prelim_hq_process(hw_prelim_hq* h, const hw_pulse* d_pulses, const uint32
                          const hw_basecalling_metrics* d_metrics, const uint8_t* d_marks, int32_t* produced,
                          hw_baz_checkpoint* out, void* stream)
 {
+    const NvtxRange range("hw_prelim_hq_process");
     if (!h || !d_pulses || !d_lens || !produced || !out || max_calls == 0)
         return Fail(HW_ERR_INVALID_ARG, "hw_prelim_hq_process: bad argument");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
