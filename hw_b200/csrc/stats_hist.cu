@@ -146,6 +146,7 @@ struct EdgeState
 
 constexpr int kHistLanesPerBlock = 1;
 constexpr int kHistBatch = 8;
+constexpr int kHistPairBatch = 4;   // frames of each half loaded ahead
 
 // AddBlock (TraceHistogramAccumHost.cpp:140-169): edge scrubbing with the fp16
 // baseline mode, then UHistogramSimd::AddDatum.  Counts of the lane are held
@@ -202,11 +203,93 @@ HistAddKernel(hw_lane_histogram* hist, EdgeState es, const int16_t* traces, int 
         if ((!sel) | mLow | mHigh) bin = kBins;
         cnt[ll][bin][z] = (uint16_t)(cnt[ll][bin][z] + 1);
     };
-    // Trace values in two register batches of 8 frames that alternate: batch
-    // A is refilled while batch B is binned and vice versa, so loads are a
-    // batch ahead and no register is copied while its load is in flight.
     int f = 0;
+    if (frames >= 4 * kHistPairBatch && frames % (4 * kHistPairBatch) == 0)
     {
+        // Two halves of the chunk at once, each with its own edge-classifier
+        // state: the classifier looks back two frames only, so the second
+        // half starts exactly from frames S-2 and S-1.  Two independent
+        // divide / count chains are in flight; when both frames land in the
+        // same bin the count is bumped by two once, so the counts equal the
+        // one-stream ones.  Loads run a batch ahead in alternating registers.
+        const int S = frames / 2;
+        const int16_t xm2 = __ldg(tr + (size_t)(S - 2) * kLane), xm1 = __ldg(tr + (size_t)(S - 1) * kLane);
+        int16_t prevB = xm1;
+        bool b1B = xm1 < thr, b2B = xm2 < thr;
+        uint16_t nLowB = 0, nHighB = 0;
+        auto binOf = [&](int16_t x, int16_t& pv, bool& c1, bool& c2, int& cn, uint16_t& lo, uint16_t& hi) {
+            const bool isBl = x < thr;
+            const bool edge = (cn == 2) ? (isBl ^ c2) : true;
+            const float xv = (float)pv;
+            pv = x;
+            c2 = c1; c1 = isBl; cn = (cn < 2) ? cn + 1 : 2;
+            const bool sel = !edge;
+            int bin = floor_cast_i32((xv - lower) / binSize);
+            const bool mLow = sel & (bin < 0);
+            const bool mHigh = sel & (bin >= kBins);
+            lo = (uint16_t)(lo + (mLow ? 1 : 0));
+            hi = (uint16_t)(hi + (mHigh ? 1 : 0));
+            if ((!sel) | mLow | mHigh) bin = kBins;
+            return bin;
+        };
+        int nB = 2;
+        auto pair = [&](int16_t xA, int16_t xB) {
+            const int ba = binOf(xA, prev, b1, b2, n, nLow, nHigh);
+            const int bb = binOf(xB, prevB, b1B, b2B, nB, nLowB, nHighB);
+            const uint16_t ca = cnt[ll][ba][z], cb = cnt[ll][bb][z];
+            if (ba == bb)
+                cnt[ll][ba][z] = (uint16_t)(ca + 2);
+            else
+            {
+                cnt[ll][ba][z] = (uint16_t)(ca + 1);
+                cnt[ll][bb][z] = (uint16_t)(cb + 1);
+            }
+        };
+        int16_t aA[kHistPairBatch], aB[kHistPairBatch], bA[kHistPairBatch], bB[kHistPairBatch];
+#pragma unroll
+        for (int j = 0; j < kHistPairBatch; ++j)
+        {
+            aA[j] = __ldg(tr + (size_t)j * kLane);
+            aB[j] = __ldg(tr + (size_t)(S + j) * kLane);
+        }
+        int i = 0;
+        for (; i + 2 * kHistPairBatch <= S; i += 2 * kHistPairBatch)
+        {
+#pragma unroll
+            for (int j = 0; j < kHistPairBatch; ++j)
+            {
+                bA[j] = __ldg(tr + (size_t)(i + kHistPairBatch + j) * kLane);
+                bB[j] = __ldg(tr + (size_t)(S + i + kHistPairBatch + j) * kLane);
+            }
+#pragma unroll
+            for (int j = 0; j < kHistPairBatch; ++j) pair(aA[j], aB[j]);
+            if (i + 3 * kHistPairBatch <= S)
+            {
+#pragma unroll
+                for (int j = 0; j < kHistPairBatch; ++j)
+                {
+                    aA[j] = __ldg(tr + (size_t)(i + 2 * kHistPairBatch + j) * kLane);
+                    aB[j] = __ldg(tr + (size_t)(S + i + 2 * kHistPairBatch + j) * kLane);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < kHistPairBatch; ++j) pair(bA[j], bB[j]);
+        }
+        // S is a multiple of 2 x kHistPairBatch: nothing is left over
+        nLow = (uint16_t)(nLow + nLowB);
+        nHigh = (uint16_t)(nHigh + nHighB);
+        prev = prevB;
+        b1 = b1B;
+        b2 = b2B;
+        n = nB;
+        f = frames;
+    }
+    else
+    {
+        // Trace values in two register batches of 8 frames that alternate:
+        // batch A is refilled while batch B is binned and vice versa, so
+        // loads are a batch ahead and no register is copied while its load
+        // is in flight.
         int16_t xa[kHistBatch], xb[kHistBatch];
         if (frames >= 2 * kHistBatch)
         {
