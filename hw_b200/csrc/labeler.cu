@@ -403,6 +403,7 @@ __global__ void __launch_bounds__(Threads, LabelerMinBlocks(Threads)) LabelerKer
 #pragma unroll
             for (int j = 0; j < kBatch; ++j)
                 seg.Frame(k, (uint32_t)(r0 + j) + firstFrame, (int16_t)((word >> (4 * j)) & 15u), sg[j]);
+            seg.Flush(k);
         }
         seg.Store(P, g, l, z, ps.lens, ps.ovf, go);
     }

@@ -23,6 +23,12 @@ struct PulseSeg
     float b0, b1, b2;       // StatAccumulator of baseline frames (offset 0)
     float minMean;
     hw_pulse* out;
+    // a closed pulse not yet converted (LabelsSegment fields at its end)
+    bool pend;
+    uint32_t pStart;
+    int pWidth;
+    float pNum, pTotal, pM2;       // (total + last) + first, total, m2
+    int16_t pMx, pLabel;
 
     __device__ __forceinline__ void Load(const PulseArgs& A, int g, float minMeanIn, hw_pulse* outIn)
     {
@@ -33,37 +39,66 @@ struct PulseSeg
         b0 = 0.0f; b1 = 0.0f; b2 = 0.0f;
         minMean = minMeanIn;
         out = outIn;
+        pend = false;
+    }
+
+    // LabelsSegment::ToPulse (HostPulseAccumulator.h:106-138) of the pending
+    // pulse, appended to the ZMW's bounded pulse vector.
+    __device__ __forceinline__ void Emit(const KParams& k)
+    {
+        constexpr float maxSignal = 65535 * .1f;
+        constexpr float minSignal = 0.0f;
+        const int width = pWidth;
+        const float rawMean = pNum / (float)width;
+        const float rawMid = pTotal / (float)(width - 2);
+        const bool keep = ((float)width >= k.widthThresh) || (mul_rn(rawMean, (float)width) >= mul_rn(k.ampThresh, minMean));
+        hw_pulse p;
+        p.start = pStart;
+        p.width = (uint16_t)width;
+        p.mean_signal = ToFixed(fmin_std(maxSignal, fmax_std(minSignal, rawMean)));
+        p.mid_signal = ToFixed(width < 3 ? 0.0f : fmin_std(maxSignal, fmax_std(minSignal, rawMid)));
+        p.max_signal = ToFixed(fmin_std(maxSignal, fmax_std(minSignal, (float)pMx)));
+        p.signal_m2 = pM2;
+        int lbl = pLabel;
+        if (lbl > 2 * kAnalogs) lbl -= 2 * kAnalogs;
+        if ((lbl > kAnalogs) & (lbl <= 2 * kAnalogs)) lbl -= kAnalogs;
+        p.label = k.analogMap[lbl - 1];
+        p.is_reject = keep ? 0 : 1;
+        p.pad_[0] = 0; p.pad_[1] = 0;
+        if (n < (uint32_t)k.maxCalls) out[n++] = p;
+        else ++over;
+    }
+
+    // Converts the pending pulse, if any: called after each frame batch and
+    // before Store.
+    __device__ __forceinline__ void Flush(const KParams& k)
+    {
+        if (pend)
+        {
+            Emit(k);
+            pend = false;
+        }
     }
 
     __device__ __forceinline__ void Frame(const KParams& k, uint32_t absF, int16_t lb, int16_t signal)
     {
-        constexpr float maxSignal = 65535 * .1f;
-        constexpr float minSignal = 0.0f;
         const bool isUp = (lb > kAnalogs) & (lb <= 2 * kAnalogs);
         const bool boundary = isUp | ((lb == 0) & (label != 0));
         const bool pulseM = label != 0;
         if (boundary & pulseM)
         {
-            // LabelsSegment::ToPulse (HostPulseAccumulator.h:106-138)
-            const int width = (int)(absF - start);
-            const float rawMean = float(add_rn(add_rn(total, (float)last), (float)first)) / (float)width;
-            const float rawMid = total / (float)(width - 2);
-            const bool keep = ((float)width >= k.widthThresh) || (mul_rn(rawMean, (float)width) >= mul_rn(k.ampThresh, minMean));
-            hw_pulse p;
-            p.start = start;
-            p.width = (uint16_t)width;
-            p.mean_signal = ToFixed(fmin_std(maxSignal, fmax_std(minSignal, rawMean)));
-            p.mid_signal = ToFixed(width < 3 ? 0.0f : fmin_std(maxSignal, fmax_std(minSignal, rawMid)));
-            p.max_signal = ToFixed(fmin_std(maxSignal, fmax_std(minSignal, (float)mx)));
-            p.signal_m2 = m2;
-            int lbl = label;
-            if (lbl > 2 * kAnalogs) lbl -= 2 * kAnalogs;
-            if ((lbl > kAnalogs) & (lbl <= 2 * kAnalogs)) lbl -= kAnalogs;
-            p.label = k.analogMap[lbl - 1];
-            p.is_reject = keep ? 0 : 1;
-            p.pad_[0] = 0; p.pad_[1] = 0;
-            if (n < (uint32_t)k.maxCalls) out[n++] = p;
-            else ++over;
+            // The pulse's raw sums wait in the pending slot; ToPulse runs at
+            // the end of the frame batch, once for the whole warp, instead of
+            // at every frame where some lane of the warp closes a pulse.
+            if (pend) Emit(k);
+            pend = true;
+            pStart = start;
+            pWidth = (int)(absF - start);
+            pNum = add_rn(add_rn(total, (float)last), (float)first);
+            pTotal = total;
+            pM2 = m2;
+            pMx = mx;
+            pLabel = label;
         }
         if (boundary)
         {

@@ -41,6 +41,7 @@ __global__ void __launch_bounds__(128) PulseKernel(PulseArgs A, KParams k)
         }
 #pragma unroll
         for (int j = 0; j < kB; ++j) seg.Frame(k, (uint32_t)(rel0 + j) + firstFrame, lbB[j], sgB[j]);
+        seg.Flush(k);
     }
     seg.Store(A, g, l, z, ps ? ps->lens : A.lens, ps ? ps->ovf : A.ovf, go);
 }
