@@ -196,7 +196,7 @@ def next_rows(threads):
     cfg = workloads.small_config()
     an = Fl.BatchAnalyzer(cfg, 0, lanes, F)
     gen = Fl.TraceGenerator(lanes, workload=1)
-    cart = dict(np.load(os.path.join(ROOT, "tests", "golden", "trained_cart.npz")))
+    cart = dict(np.load(os.path.join(ROOT, "hw_b200", "data", "trained_cart.npz")))
     inputs = []
     for c in range(16):
         pulses, lens, ovf, em, est = an(gen.next(c * F, F), c * F)
@@ -341,7 +341,7 @@ def main():
         # HF metrics included (4096-frame blocks, the reference's trained
         # activity classifier when its table is in the checkout)
         engine = Fl.FusedEngine(cfg, [lpp] * args.pools, [FRAMES] * args.pools)
-        cart_file = os.path.join(ROOT, "tests", "golden", "trained_cart.npz")
+        cart_file = os.path.join(ROOT, "hw_b200", "data", "trained_cart.npz")
         cart = dict(np.load(cart_file)) if os.path.exists(cart_file) else None
         engine.enable_hf_metrics(4096, cfg.frame_rate, True, cart)
         profiled = [engine]

@@ -36,7 +36,9 @@ constexpr int kTileRows = 128;       // ZMWs a tile
 constexpr int kThreads = 256;        // runs of pulses a tile
 constexpr uint64_t kFfNan = 0, kFfInf = 1, kFfNinf = 2, kFfOffset = 3;   // FloatFixedCodec codes
 // look-back flags (top two bits of a tile's word): count published, inclusive total published
-constexpr unsigned long long kFlagAgg = 1ull << 62, kFlagInc = 2ull << 62;
+// kFlagFail: an inclusive word whose prefix is not valid (the tile, or a tile
+// before it, gave up waiting); successors stop at it and carry it forward.
+constexpr unsigned long long kFlagAgg = 1ull << 62, kFlagInc = 2ull << 62, kFlagFail = 3ull << 62;
 constexpr uint32_t kSpinLimit = 1u << 22;  // default bound on polls of a predecessor's status (about 0.4 s)
 
 struct BazSpec
@@ -336,7 +338,11 @@ __device__ __forceinline__ void PublishCount(const TileArgs& a, uint32_t tile, u
 // tile's inclusive total.  Words of earlier calls (another epoch) read as
 // not ready.  Tiles are taken in ticket order, so every tile waited on has
 // started and publishes its count without waiting; the polls are bounded
-// all the same.
+// all the same.  A tile that gives up, or whose nearest inclusive word is a
+// failed one, publishes kFlagFail instead, so every later tile (the call's
+// last one included) learns that its prefix is invalid from the status word
+// itself; the mapped failure word is written and fenced to system scope
+// before that publish.
 __device__ uint64_t LookBack(const TileArgs& a, uint32_t tile, uint64_t agg, bool& gaveUp)
 {
     const int lane = threadIdx.x & 31;
@@ -346,6 +352,7 @@ __device__ uint64_t LookBack(const TileArgs& a, uint32_t tile, uint64_t agg, boo
     uint64_t excl = 0;
     int hi = (int)tile - 1;
     uint32_t spins = 0;
+    bool failed = false;
     while (true)
     {
         const int idx = hi - lane;
@@ -356,23 +363,32 @@ __device__ uint64_t LookBack(const TileArgs& a, uint32_t tile, uint64_t agg, boo
         {
             if ((uint32_t)++spins > a.spinLimit)
             {
-                gaveUp = true;
-                if (lane == 0) a.host[1] = 1;
+                failed = true;
+                if (lane == 0)
+                {
+                    a.host[1] = 1;
+                    __threadfence_system();
+                }
                 break;
             }
             __nanosleep(100);
             continue;
         }
-        const uint32_t inc = __ballot_sync(~0u, flag == 2);
+        const uint32_t inc = __ballot_sync(~0u, flag >= 2);
         const int stop = inc ? __ffs(inc) - 1 : 31;
         uint64_t v = lane <= stop ? (w & kCountMask) : 0;
 #pragma unroll
         for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(~0u, v, o);
         excl += v;
-        if (inc) break;
+        if (inc)
+        {
+            failed = __shfl_sync(~0u, flag, stop) == 3;
+            break;
+        }
         hi -= 32;
     }
-    if (lane == 0) StoreRelaxed(a.status + tile, kFlagInc | tag | (excl + agg));
+    gaveUp = failed;
+    if (lane == 0) StoreRelaxed(a.status + tile, (failed ? kFlagFail : kFlagInc) | tag | ((excl + agg) & kCountMask));
     return excl;
 }
 

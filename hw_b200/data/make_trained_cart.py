@@ -1,10 +1,10 @@
-"""Generates tests/golden/trained_cart.npz: the activity labeler's trained
+"""Generates hw_b200/data/trained_cart.npz: the activity labeler's trained
 CART as the reference ships it (ActivityLabeler::TrainedCart,
 src/basecaller/dataTypes/TrainedCartParams.cpp), read from the reference
-checkout.  The HF-metrics tests pass these arrays through
+checkout.  The HF-metrics tests and the benchmark pass these arrays through
 hw_hfmetrics_set_cart, as an integrating basecaller passes its own table.
 
-    python tests/golden/make_trained_cart.py [reference root]
+    python hw_b200/data/make_trained_cart.py <reference project root>
 """
 import os
 import re
@@ -34,7 +34,9 @@ def parse(path):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_trained_cart.py <reference project root>")
+    root = sys.argv[1]
     arrays = parse(os.path.join(root, "src/basecaller/dataTypes/TrainedCartParams.cpp"))
     np.savez(os.path.join(HERE, "trained_cart.npz"), **arrays)
     print({k: v.shape for k, v in arrays.items()})

@@ -54,7 +54,7 @@ def run(steps=24, warmup_steps=40, n_inputs=8, pools=POOLS, lanes=LANES, cfg=Non
     rp = Fl.Repacker(nz, LANES, F)
     chunks = rp.new_chunks()
     eng = Fl.FusedEngine(cfg, [LANES] * POOLS, [F] * POOLS, tuning="auto")
-    cart = dict(np.load(os.path.join(ROOT, "tests", "golden", "trained_cart.npz")))
+    cart = dict(np.load(os.path.join(ROOT, "hw_b200", "data", "trained_cart.npz")))
     eng.enable_hf_metrics(4096, cfg.frame_rate, True, cart)
     hq = [Fl.PrelimHq(LANES * 64, chunks_per_block=8, lookback=10, enable=False) for _ in range(POOLS)]
     # each pool's checkpoints land in its own pinned buffer, copied on a side

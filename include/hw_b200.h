@@ -327,17 +327,6 @@ int hw_dme_estimate(hw_dme* d, const hw_lane_histogram* d_hist, const hw_baselin
                     hw_frame_interval hist_fi, hw_frame_interval model_fi,
                     hw_lane_model* d_models, hw_dme_diag* d_diag, void* stream);
 
-/* Same estimate as hw_dme_estimate for callers that cannot allocate device
- * memory (for example code that runs inside a custom allocator or a
- * pre-sized real-time pipeline).  It needs no handle: the EM scratch is a
- * fixed file-scope device array of about 28 MiB that every GPU loading the
- * library holds until the process exits, so at most 128 lanes are accepted
- * per call (HW_ERR_INVALID_ARG above that; split a pool into sub-ranges).
- * The first call on each device looks up the array's device address, so
- * make that first call before any stream capture.  All calls share the one
- * array: calls that overlap on the GPU (different streams, threads or
- * processes sharing a context) race.  Synchronous like hw_dme_estimate.
- * This entry point has no counterpart in the reference. */
 /* hw_dme_estimate from a learned EM start (no counterpart in the reference):
  * d_proposal [lanes][15][64] (fractions, means, variances of the baseline and
  * the four analogs, see hw_dme_em_fit) replaces the reference start for every
@@ -348,6 +337,31 @@ int hw_dme_estimate_proposal(hw_dme* d, const hw_lane_histogram* d_hist, const h
                              hw_frame_interval hist_fi, hw_frame_interval model_fi, hw_lane_model* d_models,
                              hw_dme_diag* d_diag, const float* d_proposal, void* stream);
 
+/* Same estimate as hw_dme_estimate for callers that cannot allocate device
+ * memory: code that runs inside a custom allocator's callbacks (where a
+ * cudaMalloc would re-enter the allocator), or a real-time pipeline whose
+ * device memory is sized once at start-up.  No counterpart in the reference.
+ *
+ * It needs no handle: the EM scratch is a fixed file-scope device array of
+ * about 28 MiB (128 lanes x 3 x 301 x 64 floats) that every GPU loading the
+ * library holds until the process exits.
+ *   - At most 128 lanes per call (HW_ERR_INVALID_ARG above that): split a
+ *     larger pool into sub-ranges of at most 128 lanes.
+ *   - Synchronous: it returns after the estimate finished on `stream`.
+ *   - All calls on a device share the one scratch array and its error word,
+ *     so calls must not overlap on the GPU: callers serialise them (one
+ *     host thread, one stream, or their own lock).  Overlapping calls (two
+ *     host threads, two streams, or processes sharing a context) overwrite
+ *     each other's scratch and can clear each other's error word, which
+ *     gives wrong models without an error.
+ *   - The first call on each device looks up the array's device address
+ *     (once per device, with that device current), so make it before any
+ *     stream capture.  With CUDA's default lazy module loading the first use
+ *     of the library's DME code on a device loads the module, and that load
+ *     allocates the array: warm the library up once per device outside the
+ *     no-allocation region (any hw_dme_* call, or a first
+ *     hw_dme_estimate_noalloc call), or load with CUDA_MODULE_LOADING=EAGER.
+ *   - The looked-up addresses are not valid after cudaDeviceReset. */
 int hw_dme_estimate_noalloc(const hw_config* cfg, uint32_t lanes, const hw_lane_histogram* d_hist,
                             const hw_baseliner_stats* d_stats, hw_frame_interval hist_fi,
                             hw_frame_interval model_fi, hw_lane_model* d_models, hw_dme_diag* d_diag,

@@ -263,7 +263,7 @@ class HfMetrics:
 
     def set_cart(self, cart):
         """cart: mapping with children_left/right, feature, threshold, value,
-        hsw_curve, max_acceptable_halfsandwich_rate (tests/golden/trained_cart.npz)."""
+        hsw_curve, max_acceptable_halfsandwich_rate (hw_b200/data/trained_cart.npz)."""
         self._cart = {k: np.ascontiguousarray(cart[k]) for k in cart}
         c = self._cart
         _check(lib().or_hf_set_cart(self.h, abi.ptr(c["children_left"]), abi.ptr(c["children_right"]),

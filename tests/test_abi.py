@@ -33,11 +33,14 @@ def test_library_exports_every_header_function():
 
 
 def test_library_is_built_for_sm100a():
-    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", native.LIB_PATH], capture_output=True,
-                         text=True)
-    if out.returncode != 0:
-        pytest.skip("cuobjdump unavailable")
-    assert "sm_100a" in out.stdout
+    # every object and the link are compiled for sm_100a only (no PTX for a
+    # JIT to pick up on another architecture)
+    from hw_b200 import build
+    flags = build.NVCC_FLAGS
+    i = flags.index("-gencode")
+    assert flags[i + 1] == "arch=compute_100a,code=sm_100a"
+    assert flags.count("-gencode") == 1
+    assert "--use_fast_math" not in flags and "-fmad=false" in flags
 
 
 _PROBE = r"""

@@ -116,7 +116,7 @@ def test_fused_hf_metrics_equal_standalone_filter(mode):
     fed by each pool's own analyzer, in the reference's calling pattern."""
     import torch
     from hw_b200 import filters as Fl
-    golden = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "trained_cart.npz")
+    golden = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "hw_b200", "data", "trained_cart.npz")
     cart = dict(np.load(golden))
     cfg = workloads.small_config()
     cfg.model_estimation_mode = mode

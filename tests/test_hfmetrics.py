@@ -16,7 +16,7 @@ F, BLOCK, LANES, CAP = 512, 4096, 2, 48
 
 
 def cart():
-    return dict(np.load(os.path.join(HERE, "golden", "trained_cart.npz")))
+    return dict(np.load(os.path.join(HERE, "..", "hw_b200", "data", "trained_cart.npz")))
 
 
 def fixed(v):
