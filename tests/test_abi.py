@@ -180,16 +180,6 @@ def test_config_validation_rejects_bad_analogs():
     assert native.lib().hw_config_validate(C.byref(c)) == 1
 
 
-def test_transition_matrix_matches_oracle():
-    import oracle
-    from hw_b200 import workloads
-    for cfg in (_default(), workloads.chip_config(), workloads.small_config()):
-        t = np.zeros((abi.NUM_STATES, abi.NUM_STATES), np.float32)
-        native.check(native.lib().hw_transition_matrix(C.byref(cfg), abi.ptr(t)))
-        assert np.array_equal(t, oracle.transition_matrix(cfg))
-        assert np.isfinite(t).any()
-
-
 def test_latent_frames():
     assert native.lib().hw_labeler_latent_frames() == abi.LATENT_FRAMES == 24
 
