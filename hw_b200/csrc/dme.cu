@@ -67,6 +67,14 @@ __device__ __forceinline__ float XsnCoeffCVSq(const KParams& k, float mean, floa
     return r;
 }
 
+// EvolveConfidence (DetectionModelHost.h:189-201): the confidence decays by
+// half every `halfLife` frames between the interval centres.
+__device__ __forceinline__ float EvolveConfidence(float conf, int tFrom, int tTo, float halfLife)
+{
+    const float tDiff = static_cast<float>(tTo - tFrom);
+    return mul_rn(conf, exp2_d(-fabsf(tDiff) / halfLife));
+}
+
 // DetectionModelHost::Update(other, fraction), Update0/1/2
 __device__ void ModelUpdateFrac(const KParams& k, ModelF& t, const ModelF& o, float fraction)
 {
@@ -212,8 +220,7 @@ __device__ __forceinline__ void DmePrelude(const KParams& k, const hw_lane_model
         const float thl = mul_rn(0.5f, (float)(tModel + tEst));
         const float t0 = 56160.0f, t1 = 168480.0f;
         const float hl = add_rn(k.halfLife0, mul_rn(k.halfLife1 - k.halfLife0, satlin_std(t0, t1, thl)));
-        const float tDiff = static_cast<float>(tEst - tModel);
-        det.conf = mul_rn(det.conf, exp2_d(-fabsf(tDiff) / hl));
+        det.conf = EvolveConfidence(det.conf, tModel, tEst, hl);
     }
 
     // PrelimEstimate (DmeEmHost.cpp:161-214)
@@ -975,4 +982,95 @@ extern "C" int hw_dme_em_fit(const hw_config* cfg, uint32_t lanes, const hw_lane
     const cudaError_t ce = cudaGetLastError();
     if (ce != cudaSuccess) return SetLastError(HW_ERR_CUDA, cudaGetErrorString(ce));
     return HW_OK;
+}
+
+// ---- DetectionModelHost <-> LaneDetectionModel ------------------------------
+// The float model the estimator works on and the fp16 lane model it exports
+// (DetectionModelHost(ldm, fi), DetectionModelHost.cpp:47-60; ExportTo,
+// DetectionModelHost.cpp:226-234, 277-285), with the DME's own conversion
+// functions, so the conversion can be checked on its own.  Float parameters
+// are [lane][16][64]: baseline weight, mean, variance; each analog's weight,
+// mean, variance; confidence.
+
+namespace hwk {
+
+__global__ void ModelImportKernel(const hw_lane_model* m, float* p, int lanes)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= lanes * kLane) return;
+    const int l = g / kLane, z = g % kLane;
+    ModelF f;
+    LoadModel(m[l], z, f);
+    float* o = p + (size_t)l * 16 * kLane + z;
+    o[0 * kLane] = f.bw; o[1 * kLane] = f.bm; o[2 * kLane] = f.bv;
+    for (int a = 0; a < kAnalogs; ++a)
+    {
+        o[(3 + 3 * a) * kLane] = f.aw[a];
+        o[(4 + 3 * a) * kLane] = f.am[a];
+        o[(5 + 3 * a) * kLane] = f.av[a];
+    }
+    o[15 * kLane] = f.conf;
+}
+
+__global__ void ModelExportKernel(const float* p, hw_lane_model* m, int lanes)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= lanes * kLane) return;
+    const int l = g / kLane, z = g % kLane;
+    const float* i = p + (size_t)l * 16 * kLane + z;
+    ModelF f;
+    f.bw = i[0 * kLane]; f.bm = i[1 * kLane]; f.bv = i[2 * kLane];
+    for (int a = 0; a < kAnalogs; ++a)
+    {
+        f.aw[a] = i[(3 + 3 * a) * kLane];
+        f.am[a] = i[(4 + 3 * a) * kLane];
+        f.av[a] = i[(5 + 3 * a) * kLane];
+    }
+    f.conf = i[15 * kLane];
+    StoreModel(f, z, m[l]);
+}
+
+__global__ void ModelEvolveKernel(float* p, int lanes, int tFrom, int tTo, float halfLife)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= lanes * kLane) return;
+    float* c = p + ((size_t)(g / kLane) * 16 + 15) * kLane + g % kLane;
+    *c = EvolveConfidence(*c, tFrom, tTo, halfLife);
+}
+
+inline int32_t CenterInt(const hw_frame_interval& fi) { return fi.lower + (fi.upper - fi.lower) / 2; }
+
+}   // namespace hwk
+
+extern "C" int hw_detection_model_import(const hw_lane_model* d_models, uint32_t lanes, float* d_params, void* stream)
+{
+    using namespace hwk;
+    if (!d_models || !d_params || lanes == 0) return SetLastError(HW_ERR_INVALID_ARG, "NULL argument or no lanes");
+    ModelImportKernel<<<(lanes * kLane + 127) / 128, 128, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        d_models, d_params, (int)lanes);
+    const cudaError_t ce = cudaGetLastError();
+    return ce == cudaSuccess ? HW_OK : SetLastError(HW_ERR_CUDA, cudaGetErrorString(ce));
+}
+
+extern "C" int hw_detection_model_export(const float* d_params, uint32_t lanes, hw_lane_model* d_models, void* stream)
+{
+    using namespace hwk;
+    if (!d_models || !d_params || lanes == 0) return SetLastError(HW_ERR_INVALID_ARG, "NULL argument or no lanes");
+    ModelExportKernel<<<(lanes * kLane + 127) / 128, 128, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        d_params, d_models, (int)lanes);
+    const cudaError_t ce = cudaGetLastError();
+    return ce == cudaSuccess ? HW_OK : SetLastError(HW_ERR_CUDA, cudaGetErrorString(ce));
+}
+
+extern "C" int hw_detection_model_evolve_confidence(float* d_params, uint32_t lanes, hw_frame_interval from,
+                                                    hw_frame_interval to, float half_life, void* stream)
+{
+    using namespace hwk;
+    if (!d_params || lanes == 0) return SetLastError(HW_ERR_INVALID_ARG, "NULL argument or no lanes");
+    if (from.lower >= from.upper || to.lower >= to.upper)
+        return SetLastError(HW_ERR_INVALID_ARG, "frame intervals must not be empty");
+    ModelEvolveKernel<<<(lanes * kLane + 127) / 128, 128, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        d_params, (int)lanes, CenterInt(from), CenterInt(to), half_life);
+    const cudaError_t ce = cudaGetLastError();
+    return ce == cudaSuccess ? HW_OK : SetLastError(HW_ERR_CUDA, cudaGetErrorString(ce));
 }

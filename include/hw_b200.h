@@ -337,6 +337,19 @@ int hw_dme_estimate_proposal(hw_dme* d, const hw_lane_histogram* d_hist, const h
                              hw_frame_interval hist_fi, hw_frame_interval model_fi, hw_lane_model* d_models,
                              hw_dme_diag* d_diag, const float* d_proposal, void* stream);
 
+/* DetectionModelHost <-> LaneDetectionModel<PBHalf> (DetectionModelHost.h:
+ * constructor from a LaneDetectionModel, ExportTo; DetectionModelHost.cpp:
+ * 47-60, 226-234, 277-285) with the estimator's own conversion code: the
+ * float model the EM works on, d_params [lanes][16][64] = baseline weight,
+ * mean, variance, each analog's weight, mean, variance, confidence, and the
+ * fp16 lane model (variances clamped to half(65000) on export). */
+int hw_detection_model_import(const hw_lane_model* d_models, uint32_t lanes, float* d_params, void* stream);
+int hw_detection_model_export(const float* d_params, uint32_t lanes, hw_lane_model* d_models, void* stream);
+/* EvolveConfidence (DetectionModelHost.h:189-201): the confidence row of
+ * d_params decays by exp2(-|center(to) - center(from)| / half_life). */
+int hw_detection_model_evolve_confidence(float* d_params, uint32_t lanes, hw_frame_interval from,
+                                         hw_frame_interval to, float half_life, void* stream);
+
 /* Same estimate as hw_dme_estimate for callers that cannot allocate device
  * memory: code that runs inside a custom allocator's callbacks (where a
  * cudaMalloc would re-enter the allocator), or a real-time pipeline whose

@@ -447,6 +447,13 @@ void ModelFromLane(const hw_lane_model& l, hw_frame_interval fi, Model& m)
     m.fi = fi;
 }
 
+// EvolveConfidence, DetectionModelHost.h:189-201 (interval centres t0, t1)
+void EvolveConfidence(Model& m, int32_t t0, int32_t t1, float halfLife)
+{
+    const float tDiff = static_cast<float>(t1 - t0);
+    FZ { const float f = exp2_f(-std::abs(tDiff) / halfLife); m.conf[z] *= f; }
+}
+
 // ExportTo, DetectionModelHost.cpp:226-234, 277-285
 void ModelToLane(const Model& m, hw_lane_model& l)
 {
@@ -1132,8 +1139,7 @@ void OraclePool::DmePrelude(int64_t l, const hw_lane_histogram* hh, const hw_bas
         const float hl0 = cfg.confidence_half_life[0], hl1 = cfg.confidence_half_life[1];
         const float hl = hl0 + (hl1 - hl0) * satlin_std(t0, t1, thl);
         // EvolveConfidence, DetectionModelHost.h:166-177
-        const float tDiff = static_cast<float>(CenterInt(hfi) - CenterInt(det.fi));
-        FZ { const float m = exp2_f(-std::abs(tDiff) / hl); det.conf[z] *= m; }
+        EvolveConfidence(det, CenterInt(det.fi), CenterInt(hfi), hl);
         det.fi = hfi;
     }
 
@@ -1980,6 +1986,76 @@ float or_expf(float x) { return hw_expf(x); }
 float or_logf(float x) { return hw_logf(x); }
 uint16_t or_f32_to_f16(float x) { return f32_to_f16_bits(x); }
 int16_t or_to_i16(float x) { return to_i16_wrap(x); }
+
+// DetectionModelHost(ldm, fi) and ExportTo on [lanes][16][64] float
+// parameters (baseline weight, mean, variance; analog weight, mean, variance
+// each; confidence), and EvolveConfidence on their confidence row.
+static void ParamsToModel(const float* p, Model& m)
+{
+    FZ
+    {
+        m.bw[z] = p[0 * kLane + z]; m.bm[z] = p[1 * kLane + z]; m.bv[z] = p[2 * kLane + z];
+        for (int a = 0; a < kAnalogs; ++a)
+        {
+            m.aw[a][z] = p[(3 + 3 * a) * kLane + z];
+            m.am[a][z] = p[(4 + 3 * a) * kLane + z];
+            m.av[a][z] = p[(5 + 3 * a) * kLane + z];
+        }
+        m.conf[z] = p[15 * kLane + z];
+    }
+}
+
+static void ModelToParams(const Model& m, float* p)
+{
+    FZ
+    {
+        p[0 * kLane + z] = m.bw[z]; p[1 * kLane + z] = m.bm[z]; p[2 * kLane + z] = m.bv[z];
+        for (int a = 0; a < kAnalogs; ++a)
+        {
+            p[(3 + 3 * a) * kLane + z] = m.aw[a][z];
+            p[(4 + 3 * a) * kLane + z] = m.am[a][z];
+            p[(5 + 3 * a) * kLane + z] = m.av[a][z];
+        }
+        p[15 * kLane + z] = m.conf[z];
+    }
+}
+
+int or_detection_model_import(const hw_lane_model* models, uint32_t lanes, float* params)
+{
+    for (uint32_t l = 0; l < lanes; ++l)
+    {
+        Model m;
+        ModelFromLane(models[l], hw_frame_interval{0, 1}, m);
+        ModelToParams(m, params + (size_t)l * 16 * kLane);
+    }
+    return HW_OK;
+}
+
+int or_detection_model_export(const float* params, uint32_t lanes, hw_lane_model* models)
+{
+    for (uint32_t l = 0; l < lanes; ++l)
+    {
+        Model m;
+        ParamsToModel(params + (size_t)l * 16 * kLane, m);
+        ModelToLane(m, models[l]);
+    }
+    return HW_OK;
+}
+
+int or_detection_model_evolve_confidence(float* params, uint32_t lanes, hw_frame_interval from,
+                                         hw_frame_interval to, float halfLife)
+{
+    if (from.lower >= from.upper || to.lower >= to.upper) { g_err = "empty frame interval"; return HW_ERR_INVALID_ARG; }
+    for (uint32_t l = 0; l < lanes; ++l)
+    {
+        Model m;
+        float* p = params + (size_t)l * 16 * kLane;
+        ParamsToModel(p, m);
+        EvolveConfidence(m, CenterInt(from), CenterInt(to), halfLife);
+        ModelToParams(m, p);
+    }
+    return HW_OK;
+}
 
 }   // extern "C"
 

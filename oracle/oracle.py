@@ -61,6 +61,9 @@ def lib():
         L.or_logf.restype = C.c_float
         L.or_f32_to_f16.argtypes = [C.c_float]
         L.or_f32_to_f16.restype = C.c_uint16
+        L.or_detection_model_import.argtypes = [vp, u32, vp]
+        L.or_detection_model_export.argtypes = [vp, u32, vp]
+        L.or_detection_model_evolve_confidence.argtypes = [vp, u32, FI, FI, C.c_float]
         L.or_to_i16.argtypes = [C.c_float]
         L.or_to_i16.restype = C.c_int16
         L.or_hf_create.argtypes = [u32, u32, C.c_double, i32]
@@ -104,6 +107,29 @@ def transition_matrix(cfg):
     out = np.zeros((abi.NUM_STATES, abi.NUM_STATES), np.float32)
     lib().or_transition_matrix(C.byref(cfg), abi.ptr(out))
     return out
+
+
+def detection_model_import(models):
+    """DetectionModelHost(ldm): fp16 lane models -> float [lanes][16][64]."""
+    models = np.ascontiguousarray(models)
+    out = np.zeros((len(models), 16, abi.LANE), np.float32)
+    _check(lib().or_detection_model_import(abi.ptr(models), len(models), abi.ptr(out)))
+    return out
+
+
+def detection_model_export(params):
+    """ExportTo: float [lanes][16][64] -> fp16 lane models."""
+    params = np.ascontiguousarray(params, np.float32)
+    out = np.zeros(len(params), abi.LANE_MODEL_DT)
+    _check(lib().or_detection_model_export(abi.ptr(params), len(params), abi.ptr(out)))
+    return out
+
+
+def detection_model_evolve_confidence(params, fi_from, fi_to, half_life):
+    params = np.ascontiguousarray(params, np.float32).copy()
+    _check(lib().or_detection_model_evolve_confidence(abi.ptr(params), len(params), abi.FrameInterval(*fi_from),
+                                                      abi.FrameInterval(*fi_to), half_life))
+    return params
 
 
 def set_threads(n):
