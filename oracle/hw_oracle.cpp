@@ -26,6 +26,7 @@
 #include <deque>
 #include <limits>
 #include <memory>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -1986,6 +1987,50 @@ float or_expf(float x) { return hw_expf(x); }
 float or_logf(float x) { return hw_logf(x); }
 uint16_t or_f32_to_f16(float x) { return f32_to_f16_bits(x); }
 int16_t or_to_i16(float x) { return to_i16_wrap(x); }
+
+// PicketFenceGenerator::GenerateSignal (appModules/SimulatedDataSource.cpp:
+// 252-323, config SimulatedDataSource.h:176-212): the reference baseliner
+// tests' traces.  Signal `idx` seeds its own std::mt19937 (seedFunc = the
+// identity); an inter-pulse run of baseline frames floor(N(level, sigma)) +
+// pedestal, then a pulse run of the same plus (a uniformly chosen pulse level
+// - the baseline level); every run draws from a fresh normal_distribution,
+// so no cached second polar value crosses runs.  Run lengths are fixed or
+// ceil(exponential(rate)).  The C++ standard library's engine and
+// distributions are the reference's own.
+int or_picket_fence(uint32_t numFrames, uint64_t idx, int poisson, uint16_t pulseWidth, uint16_t pulseIpd,
+                    float widthRate, float ipdRate, int16_t blLevel, int16_t blSigma, const int16_t* levels,
+                    int nLevels, int16_t pedestal, int16_t* out)
+{
+    if (nLevels < 1 || !out) { g_err = "picket fence: no pulse levels"; return HW_ERR_INVALID_ARG; }
+    std::mt19937 gen((std::mt19937::result_type)idx);
+    auto baseline = [&](uint16_t frames, std::vector<short>& v) {
+        std::normal_distribution<> rng(blLevel, blSigma);
+        v.clear();
+        for (size_t f = 0; f < frames; ++f) v.push_back((short)(std::floor(rng(gen)) + pedestal));
+    };
+    auto width = [&]() -> uint16_t {
+        if (poisson) { std::exponential_distribution<> rng(widthRate); return (uint16_t)std::ceil(rng(gen)); }
+        return pulseWidth;
+    };
+    auto ipd = [&]() -> uint16_t {
+        if (poisson) { std::exponential_distribution<> rng(ipdRate); return (uint16_t)std::ceil(rng(gen)); }
+        return pulseIpd;
+    };
+    size_t frame = 0;
+    std::vector<short> run;
+    while (frame < numFrames)
+    {
+        const uint16_t nIpd = (uint16_t)std::min<size_t>(numFrames - frame, ipd());
+        baseline(nIpd, run);
+        for (short v : run) out[frame++] = v;
+        const uint16_t nPw = (uint16_t)std::min<size_t>(numFrames - frame, width());
+        std::uniform_int_distribution<> pick(0, nLevels - 1);
+        const int level = levels[pick(gen)] - blLevel;
+        baseline(nPw, run);
+        for (short v : run) out[frame++] = (short)(v + level);
+    }
+    return HW_OK;
+}
 
 // DetectionModelHost(ldm, fi) and ExportTo on [lanes][16][64] float
 // parameters (baseline weight, mean, variance; analog weight, mean, variance

@@ -64,6 +64,8 @@ def lib():
         L.or_detection_model_import.argtypes = [vp, u32, vp]
         L.or_detection_model_export.argtypes = [vp, u32, vp]
         L.or_detection_model_evolve_confidence.argtypes = [vp, u32, FI, FI, C.c_float]
+        L.or_picket_fence.argtypes = [u32, C.c_uint64, C.c_int, C.c_uint16, C.c_uint16, C.c_float, C.c_float,
+                                      C.c_int16, C.c_int16, vp, C.c_int, C.c_int16, vp]
         L.or_to_i16.argtypes = [C.c_float]
         L.or_to_i16.restype = C.c_int16
         L.or_hf_create.argtypes = [u32, u32, C.c_double, i32]
@@ -130,6 +132,17 @@ def detection_model_evolve_confidence(params, fi_from, fi_to, half_life):
     _check(lib().or_detection_model_evolve_confidence(abi.ptr(params), len(params), abi.FrameInterval(*fi_from),
                                                       abi.FrameInterval(*fi_to), half_life))
     return params
+
+
+def picket_fence(num_frames, idx, poisson=True, pulse_width=5, pulse_ipd=10, width_rate=0.2, ipd_rate=0.1,
+                 baseline_level=200, baseline_sigma=20, levels=(200,), pedestal=0):
+    """The reference's PicketFenceGenerator signal `idx` (int16, num_frames);
+    defaults are its Config defaults."""
+    lv = np.ascontiguousarray(levels, np.int16)
+    out = np.zeros(num_frames, np.int16)
+    _check(lib().or_picket_fence(num_frames, idx, int(poisson), pulse_width, pulse_ipd, width_rate, ipd_rate,
+                                 baseline_level, baseline_sigma, abi.ptr(lv), len(lv), pedestal, abi.ptr(out)))
+    return out
 
 
 def set_threads(n):
