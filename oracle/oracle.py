@@ -171,6 +171,8 @@ class Pool:
 
     def baseline(self, trace, first_frame):
         trace = np.ascontiguousarray(trace, dtype=np.int16)
+        if trace.shape != (self.lanes, self.F, abi.LANE):
+            raise ValueError(f"oracle baseline: trace {trace.shape} for {self.lanes} lanes of {self.F} frames")
         out = np.empty_like(trace)
         stats = np.zeros(self.lanes, abi.BLSTATS_DT)
         _check(lib().or_baseline(self.h, abi.ptr(trace), first_frame, abi.ptr(out), abi.ptr(stats)))
@@ -243,6 +245,9 @@ class Pool:
 
     def label(self, traces, models):
         traces = np.ascontiguousarray(traces, dtype=np.int16)
+        if traces.shape != (self.lanes, self.F, abi.LANE) or len(models) != self.lanes:
+            raise ValueError(f"oracle label: traces {traces.shape}, {len(models)} models for "
+                             f"{self.lanes} lanes of {self.F} frames")
         labels = np.empty_like(traces)
         lat = np.empty((self.lanes, abi.LATENT_FRAMES, abi.LANE), np.int16)
         score = np.empty((self.lanes, abi.LANE), np.float32)

@@ -1,0 +1,152 @@
+"""Frame labels against synthetic ground truth, mirroring the reference's
+CompareVsGroundTruth test (src/basecaller/basecaller/test/
+TestFrameLabeler.cpp:104-251).
+
+The reference test labels a simulated SNR-40 trace file (missing from the
+reference checkout) with a fixed model and the movie's kinetics, then
+classifies every labelled frame against the file's ground truth: equal
+labels are matches; unequal ones where either label is a sub-frame state
+(up or down, > 4) are sub-frame confusions; the rest are mismatches.  It
+requires matches > 97%, sub-frame confusions < 2% and mismatches < 1%.
+
+Here the traces come from tests/synth.py:labeled_traces, drawn from the same
+movie (analog kinetics with two-step pulse widths, the test's fixed model:
+analog means 227.13 / 154.45 / 97.67 / 61.32, variances 776 / 426 / 226 /
+132, baseline 0 with variance 33) with sub-frame pulse starts and ends, and
+the same layout: 2 pools of 2 lanes, 64 chunks of 128 frames, labels lagging
+the chunk by the 24 latent frames.  The oracle's labeler must meet the
+reference's thresholds; a shifted truth or swapped analog means must not
+(the check has teeth).  On the GPU the library's labeler must produce the
+oracle's labels, latent traces and Viterbi scores bit for bit and so meet
+the same thresholds.
+"""
+import numpy as np
+import pytest
+
+import synth
+from hw_b200 import abi, workloads
+
+LANES_PER_POOL, POOLS = 2, 2
+BLOCK_LEN, N_BLOCKS = 128, 64
+LATENT = abi.LATENT_FRAMES
+
+
+def movie_config():
+    cfg = workloads.chip_config()
+    for i in range(4):
+        cfg.analogs[i].ipd_s = synth.LABELER_TEST_IPD_S[i]
+        cfg.analogs[i].pulse_width_s = synth.LABELER_TEST_PW_S[i]
+        cfg.analogs[i].ipd2_slow_step_ratio = 0.0
+        cfg.analogs[i].pw2_slow_step_ratio = synth.LABELER_TEST_PW_RATIO
+    cfg.frame_rate = 100.0
+    return cfg
+
+
+def fixed_model(lanes, means=synth.LABELER_TEST_MEANS):
+    h = lambda x: np.float16(x).view(np.uint16)
+    m = np.zeros(lanes, abi.LANE_MODEL_DT)
+    m["baseline"]["means"] = h(0.0)
+    m["baseline"]["vars"] = h(synth.LABELER_TEST_BL_VAR)
+    m["baseline"]["weights"] = h(0.5)
+    for i in range(4):
+        m["analogs"][:, i]["means"] = h(means[i])
+        m["analogs"][:, i]["vars"] = h(synth.LABELER_TEST_VARS[i])
+        m["analogs"][:, i]["weights"] = h(0.125)
+    return m
+
+
+class OracleLabeler:
+    def __init__(self, cfg, pool_id, lanes):
+        import oracle
+        self.p = oracle.Pool(cfg, lanes, BLOCK_LEN, pool_id)
+
+    def __call__(self, chunk, models):
+        return self.p.label(chunk, models)
+
+
+class GpuLabeler:
+    def __init__(self, cfg, pool_id, lanes):
+        import torch
+        from hw_b200 import filters as Fl
+        self.torch, self.Fl = torch, Fl
+        self.lab = Fl.FrameLabeler(cfg, pool_id, lanes, BLOCK_LEN)
+
+    def __call__(self, chunk, models):
+        labels, lat, score = self.lab(self.torch.from_numpy(chunk).cuda(), self.Fl.numpy_to_struct(models))
+        return labels.cpu().numpy(), lat.cpu().numpy(), score.cpu().numpy()
+
+
+def run(make, traces, means=synth.LABELER_TEST_MEANS):
+    """Label every chunk of every pool; returns the per-chunk outputs."""
+    cfg = movie_config()
+    out = []
+    for p in range(POOLS):
+        lab = make(cfg, p, LANES_PER_POOL)
+        models = fixed_model(LANES_PER_POOL, means)
+        tr = traces[p * LANES_PER_POOL:(p + 1) * LANES_PER_POOL]
+        out.append([lab(np.ascontiguousarray(tr[:, c * BLOCK_LEN:(c + 1) * BLOCK_LEN]), models)
+                    for c in range(tr.shape[1] // BLOCK_LEN)])
+    return out
+
+
+def score(outputs, truth, shift=0):
+    """LabelValidator counts (TestFrameLabeler.cpp:200-205): labels batch
+    frame j of a chunk starting at frame c * 128 is trace frame c * 128 + j -
+    24; frames before 0 are skipped."""
+    matches = sub = mism = 0
+    nf = truth.shape[1]
+    for p, chunks in enumerate(outputs):
+        t = truth[p * LANES_PER_POOL:(p + 1) * LANES_PER_POOL]
+        for c, (labels, _, _) in enumerate(chunks):
+            for j in range(BLOCK_LEN):
+                frame = c * BLOCK_LEN + j - LATENT + shift
+                if frame < 0 or frame >= nf:
+                    continue
+                a, e = labels[:, j, :], t[:, frame, :]
+                eq = a == e
+                sf = ~eq & ((a > 4) | (e > 4))
+                matches += int(eq.sum())
+                sub += int(sf.sum())
+                mism += int((~eq & ~sf).sum())
+    total = matches + sub + mism
+    return matches / total, sub / total, mism / total
+
+
+@pytest.fixture(scope="module")
+def data():
+    return synth.labeled_traces(LANES_PER_POOL * POOLS, BLOCK_LEN * N_BLOCKS, seed=40)
+
+
+@pytest.fixture(scope="module")
+def oracle_out(data):
+    return run(OracleLabeler, data[0])
+
+
+def test_oracle_meets_reference_thresholds(data, oracle_out):
+    m, s, x = score(oracle_out, data[1])
+    assert m > 0.97 and s < 0.02 and x < 0.01, (m, s, x)
+
+
+def test_thresholds_catch_a_shifted_truth(data, oracle_out):
+    m, s, x = score(oracle_out, data[1], shift=1)
+    assert not (m > 0.97 and s < 0.02 and x < 0.01), (m, s, x)
+
+
+def test_thresholds_catch_swapped_analogs(data):
+    means = list(synth.LABELER_TEST_MEANS)
+    means[0], means[1] = means[1], means[0]
+    out = run(OracleLabeler, data[0][:, :BLOCK_LEN * 16], means)
+    m, s, x = score(out, data[1][:, :BLOCK_LEN * 16])
+    assert not (m > 0.97 and s < 0.02 and x < 0.01), (m, s, x)
+
+
+@pytest.mark.gpu
+def test_gpu_labels_equal_oracle_and_meet_thresholds(data, oracle_out):
+    got = run(GpuLabeler, data[0])
+    for p in range(POOLS):
+        for c in range(N_BLOCKS):
+            for k, what in enumerate(("labels", "latent", "viterbi score")):
+                a, b = got[p][c][k], oracle_out[p][c][k]
+                assert np.array_equal(np.asarray(a).view(np.uint8), np.asarray(b).view(np.uint8)), (p, c, what)
+    m, s, x = score(got, data[1])
+    assert m > 0.97 and s < 0.02 and x < 0.01, (m, s, x)
