@@ -144,6 +144,7 @@ struct hw_labeler
     int16_t* latTrc = nullptr;
     int16_t* prevLat = nullptr;
     uint32_t* tb = nullptr;
+    float* gap = nullptr;     // decision gaps, allocated on the first call that asks for margins
 };
 
 struct hw_pulse_accumulator
@@ -517,16 +518,25 @@ int hw_labeler_destroy(hw_labeler* l)
     cudaFree(l->latTrc);
     cudaFree(l->prevLat);
     cudaFree(l->tb);
+    cudaFree(l->gap);
     delete l;
     return HW_OK;
 }
 
 int hw_labeler_process(hw_labeler* l, const int16_t* d_traces, const hw_lane_model* d_models, int16_t* d_labels,
-                       int16_t* d_latent_out, float* d_viterbi_score, void* stream)
+                       int16_t* d_latent_out, float* d_viterbi_score, float* d_margin_or_null, void* stream)
 {
     if (!l || !d_traces || !d_models || !d_labels) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    if (d_margin_or_null && !l->gap)
+    {
+        int rc = DevAlloc(&l->gap, (size_t)l->lanes * (l->F + hwp::kViterbiStitchLookback) * kStates * kLane,
+                          "hw_labeler_process (margin scratch)");
+        if (rc) return rc;
+    }
     LabelerArgs a{d_traces, d_models, d_labels, d_latent_out, d_viterbi_score, l->latModel, l->latLabel, l->latRoi,
                   l->latTrc, l->prevLat, l->tb, (int)l->lanes, (int)l->F};
+    a.margin = d_margin_or_null;
+    a.gap = l->gap;
     HW_CUDA(LaunchLabeler(a, l->k, S(stream)), "hw_labeler_process");
     return HW_OK;
 }
@@ -733,7 +743,7 @@ struct hw_analyzer
     {
         int rc;
         size_t t = Begin(HW_STAGE_LABELER, s);
-        if ((rc = hw_labeler_process(lab, bls, models, labels, latent, score, s))) return rc;
+        if ((rc = hw_labeler_process(lab, bls, models, labels, latent, score, nullptr, s))) return rc;
         End(t, s);
         t = Begin(HW_STAGE_PULSES, s);
         // The labels batch starts hw_labeler_latent_frames() before the trace

@@ -215,6 +215,9 @@ struct LabelerArgs
     uint32_t* tb;                 // [lanes][F + 16][64] scratch
     int lanes;
     int F;
+    // best-path decision margin of every label, or null; needs `gap`
+    float* margin = nullptr;      // [lanes][F][64]
+    float* gap = nullptr;         // [lanes][F + 16][13][64] scratch
     // lane-list launch: per-lane chunk lengths from map.Pool(lane).F, F = the
     // launch's largest
     LaneMap map{};

@@ -111,8 +111,11 @@ struct ZScorer
 // 9-way rows (baseline, pulse-up) code source s as 0 for state 0 and s - 4
 // for states 5..12 in 4 bits; 2-way rows (full, down) code the second source
 // as a single bit, which is just the outcome of the one comparison.
-template <int R>
-__device__ __forceinline__ float ViterbiRow(const KParams& k, float score, const float* ll, uint32_t& code)
+// With Margin, `gap` receives the row's decision gap: the winning candidate
+// less the best other one (0 on a tie, +inf when only one is finite).
+template <int R, bool Margin>
+__device__ __forceinline__ float ViterbiRow(const KParams& k, float score, const float* ll, uint32_t& code,
+                                            float& gap)
 {
     constexpr bool nineWay = (R == 0 || (R >= 5 && R <= 8));
     constexpr int first = nineWay ? 0 : (R <= 4 ? R : R - 8);
@@ -120,43 +123,55 @@ __device__ __forceinline__ float ViterbiRow(const KParams& k, float score, const
     constexpr int se = nineWay ? 13 : sb + 1;
     constexpr int shift = (R == 0) ? 0 : (R <= 4 ? 20 + R - 1 : (R <= 8 ? 4 + 4 * (R - 5) : 24 + R - 9));
     float mv = add_rn(add_rn(score, k.trans[R][first]), ll[first]);
+    float sv = -__int_as_float(0x7f800000);
     uint32_t c = 0u;
 #pragma unroll
     for (int p = sb; p < se; ++p)
     {
         const float v = add_rn(add_rn(score, k.trans[R][p]), ll[p]);
         const bool ge = v >= mv;
+        if constexpr (Margin) sv = ge ? mv : ((v > sv) ? v : sv);
         mv = ge ? v : mv;
         c = ge ? ((uint32_t)(nineWay ? p - 4 : 1) << shift) : c;
     }
     code = c;
+    if constexpr (Margin) gap = mv - sv;
     return mv;
 }
 
-// One Viterbi recursion step; returns the packed traceback word.
-__device__ __forceinline__ uint32_t ViterbiStep(const KParams& k, const ZScorer& sc, float data, bool isRoi, float* ll)
+// One Viterbi recursion step; returns the packed traceback word.  With
+// Margin, gap[r] receives row r's decision gap.
+template <bool Margin = false>
+__device__ __forceinline__ uint32_t ViterbiStep(const KParams& k, const ZScorer& sc, float data, bool isRoi, float* ll,
+                                                float* gap = nullptr)
 {
     float sco[9];
     sc.Scores(data, sco);
     float nl[kStates];
     uint32_t cd[kStates];
-    nl[0] = ViterbiRow<0>(k, sco[0], ll, cd[0]);
-    nl[1] = ViterbiRow<1>(k, sco[1], ll, cd[1]);
-    nl[2] = ViterbiRow<2>(k, sco[2], ll, cd[2]);
-    nl[3] = ViterbiRow<3>(k, sco[3], ll, cd[3]);
-    nl[4] = ViterbiRow<4>(k, sco[4], ll, cd[4]);
-    nl[5] = ViterbiRow<5>(k, sco[5], ll, cd[5]);
-    nl[6] = ViterbiRow<6>(k, sco[6], ll, cd[6]);
-    nl[7] = ViterbiRow<7>(k, sco[7], ll, cd[7]);
-    nl[8] = ViterbiRow<8>(k, sco[8], ll, cd[8]);
-    nl[9] = ViterbiRow<9>(k, sco[5], ll, cd[9]);
-    nl[10] = ViterbiRow<10>(k, sco[6], ll, cd[10]);
-    nl[11] = ViterbiRow<11>(k, sco[7], ll, cd[11]);
-    nl[12] = ViterbiRow<12>(k, sco[8], ll, cd[12]);
+    float gl[kStates];
+    nl[0] = ViterbiRow<0, Margin>(k, sco[0], ll, cd[0], gl[0]);
+    nl[1] = ViterbiRow<1, Margin>(k, sco[1], ll, cd[1], gl[1]);
+    nl[2] = ViterbiRow<2, Margin>(k, sco[2], ll, cd[2], gl[2]);
+    nl[3] = ViterbiRow<3, Margin>(k, sco[3], ll, cd[3], gl[3]);
+    nl[4] = ViterbiRow<4, Margin>(k, sco[4], ll, cd[4], gl[4]);
+    nl[5] = ViterbiRow<5, Margin>(k, sco[5], ll, cd[5], gl[5]);
+    nl[6] = ViterbiRow<6, Margin>(k, sco[6], ll, cd[6], gl[6]);
+    nl[7] = ViterbiRow<7, Margin>(k, sco[7], ll, cd[7], gl[7]);
+    nl[8] = ViterbiRow<8, Margin>(k, sco[8], ll, cd[8], gl[8]);
+    nl[9] = ViterbiRow<9, Margin>(k, sco[5], ll, cd[9], gl[9]);
+    nl[10] = ViterbiRow<10, Margin>(k, sco[6], ll, cd[10], gl[10]);
+    nl[11] = ViterbiRow<11, Margin>(k, sco[7], ll, cd[11], gl[11]);
+    nl[12] = ViterbiRow<12, Margin>(k, sco[8], ll, cd[12], gl[12]);
     const float pen = isRoi ? 0.0f : __int_as_float(0x7f800000);
     ll[0] = nl[0];
 #pragma unroll
     for (int r = 1; r < kStates; ++r) ll[r] = nl[r] - pen;
+    if constexpr (Margin)
+    {
+#pragma unroll
+        for (int r = 0; r < kStates; ++r) gap[r] = gl[r];
+    }
     return ((cd[0] | cd[1] | cd[2]) | (cd[3] | cd[4] | cd[5])) | ((cd[6] | cd[7] | cd[8]) | (cd[9] | cd[10] | cd[11])) | cd[12];
 }
 
@@ -194,10 +209,14 @@ constexpr int LabelerMinBlocks(int threads) { return threads == 64 ? 10 : thread
 // thread right after the traceback, on labels kept in shared memory (4 bits a
 // frame) instead of a labels batch in global memory.  Threads: 64 ZMWs (one
 // lane) per 64 threads.
-template <bool Mapped, bool Fuse, int Threads>
+// Margin (single-pool launch only): the decision gaps of every frame and
+// state go to the scratch A.gap [lanes][F + 16][13][64], and the traceback
+// writes each label's best-path margin to A.margin.
+template <bool Mapped, bool Fuse, int Threads, bool Margin = false>
 __global__ void __launch_bounds__(Threads, LabelerMinBlocks(Threads)) LabelerKernel(LabelerArgs A, KParams k,
                                                                                      PulseArgs P)
 {
+    static_assert(!Margin || (!Mapped && !Fuse), "margins come from the single-pool labeler");
     LaneMap map = A.map;
     if (!Mapped) map.list = nullptr;      // the single-pool variant compiles without the lane list
     int l, z;
@@ -279,14 +298,31 @@ __global__ void __launch_bounds__(Threads, LabelerMinBlocks(Threads)) LabelerKer
         for (int i = 0; i < kStates; ++i) ll[i] = (bc == i) ? 0.0f : -__int_as_float(0x7f800000);
     }
     uint32_t* tb = A.tb + map.BlockX(l, F, kLookback) + z;
+    // decision gap of state r at frame lf
+    auto gapAt = [&](int lf, int r) -> float& {
+        return A.gap[(((size_t)l * (F + kLookback) + lf) * kStates + r) * kLane + z];
+    };
     ZScorer sc;
+    auto step = [&](int lf, float x, bool isRoi) {
+        if constexpr (Margin)
+        {
+            float g[kStates];
+            tb[(size_t)lf * kLane] = ViterbiStep<true>(k, sc, x, isRoi, ll, g);
+#pragma unroll
+            for (int r = 0; r < kStates; ++r) gapAt(lf, r) = g[r];
+        }
+        else
+        {
+            tb[(size_t)lf * kLane] = ViterbiStep(k, sc, x, isRoi, ll);
+        }
+    };
     sc.Setup(k, oldM, z);
     uint32_t roiWord = roiw(0);
     for (int f = 0; f < kLatent; ++f)
     {
         if ((f & 15) == 0) roiWord = roiw(f >> 4);
         const bool isRoi = (roiWord >> (2 * (f & 15))) & 1u;
-        tb[(size_t)f * kLane] = ViterbiStep(k, sc, (float)pl[(size_t)f * kLane], isRoi, ll);
+        step(f, (float)pl[(size_t)f * kLane], isRoi);
     }
     sc.Setup(k, newM, z);
     const int anchor = F - kLatent;
@@ -311,7 +347,7 @@ __global__ void __launch_bounds__(Threads, LabelerMinBlocks(Threads)) LabelerKer
         const int lf = f + kLatent;
         if ((lf & 15) == 0) roiWord = roiw(lf >> 4);
         const bool isRoi = (roiWord >> (2 * (lf & 15))) & 1u;
-        tb[(size_t)lf * kLane] = ViterbiStep(k, sc, (float)x, isRoi, ll);
+        step(lf, (float)x, isRoi);
     }
 
     // Normalize (FrameLabelerHost.cpp:186-205) and back-propagation.
@@ -407,6 +443,27 @@ __global__ void __launch_bounds__(Threads, LabelerMinBlocks(Threads)) LabelerKer
         }
         seg.Store(P, g, l, z, ps.lens, ps.ovf, go);
     }
+    else if constexpr (Margin)
+    {
+        // Traceback with the best path's decision margin of every label: the
+        // last label's is the anchor choice's probability gap, label f's the
+        // gap that frame f + 1 recorded for the path's state there.
+        int16_t* out = A.labels + map.Block(l, F) + z;
+        float* mg = A.margin + map.Block(l, F) + z;
+        float second = -__int_as_float(0x7f800000);
+#pragma unroll
+        for (int i = 0; i < kStates; ++i) second = (i != anchorState && prob[i] > second) ? prob[i] : second;
+        mg[(size_t)(F - 1) * kLane] = maxP - second;
+        int next = anchorState;
+        for (int f = F - 1; f >= 0; --f)
+        {
+            out[(size_t)f * kLane] = (int16_t)ts;
+            if (f < F - 1) mg[(size_t)f * kLane] = gapAt(f + 1, next);
+            next = ts;
+            ts = TraceSource(tb[(size_t)f * kLane], ts);
+        }
+        A.latRoi[g] = (int16_t)roiBit(F - 1);
+    }
     else
     {
         int16_t* out = A.labels + map.Block(l, F) + z;
@@ -453,7 +510,7 @@ __global__ void LabelerModelCopyKernel(hw_lane_model* dst, const hw_lane_model* 
     reinterpret_cast<uint32_t*>(dst)[w] = reinterpret_cast<const uint32_t*>(src)[w];
 }
 
-template <bool Mapped, bool Fuse, int Threads>
+template <bool Mapped, bool Fuse, int Threads, bool Margin = false>
 cudaError_t LaunchLabelerT(const LabelerArgs& a, const KParams& k, const PulseArgs& p, int lanes, cudaStream_t s)
 {
     const int blocks = (lanes * kLane + Threads - 1) / Threads;
@@ -467,14 +524,14 @@ cudaError_t LaunchLabelerT(const LabelerArgs& a, const KParams& k, const PulseAr
     if (e != cudaSuccess) return e;
     if (smem > 48 * 1024 && (dev < 0 || dev >= 64 || !attrSet[dev]))
     {
-        e = cudaFuncSetAttribute(LabelerKernel<Mapped, Fuse, Threads>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(LabelerKernel<Mapped, Fuse, Threads, Margin>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(((1024 + kLookback + kStitch + 15) / 16 > 1024 / kBatch
                                             ? (1024 + kLookback + kStitch + 15) / 16 : 1024 / kBatch) *
                                        Threads * sizeof(uint32_t)));
         if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < 64) attrSet[dev] = true;
     }
-    LabelerKernel<Mapped, Fuse, Threads><<<blocks, Threads, smem, s>>>(a, k, p);
+    LabelerKernel<Mapped, Fuse, Threads, Margin><<<blocks, Threads, smem, s>>>(a, k, p);
     return cudaGetLastError();
 }
 
@@ -489,7 +546,13 @@ cudaError_t LaunchLabeler(const LabelerArgs& a, const KParams& k, cudaStream_t s
     if (!a.map.On())
     {
         if (fusedPulses || lanesPerCta != 2) return cudaErrorInvalidValue;
-        e = LaunchLabelerT<false, false, 128>(a, k, none, lanes, s);
+        if (a.margin && !a.gap) return cudaErrorInvalidValue;
+        e = a.margin ? LaunchLabelerT<false, false, 128, true>(a, k, none, lanes, s)
+                     : LaunchLabelerT<false, false, 128>(a, k, none, lanes, s);
+    }
+    else if (a.margin)
+    {
+        return cudaErrorInvalidValue;     // margins come from the single-pool labeler
     }
     else if (fusedPulses)
     {

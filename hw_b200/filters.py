@@ -189,13 +189,16 @@ class FrameLabeler(_Handle):
         self.latent_frames = lib().hw_labeler_latent_frames()
         check(lib().hw_labeler_create(C.byref(cfg), pool_id, lanes, frames_per_chunk, C.byref(self._h)))
 
-    def __call__(self, traces, models):
-        """Returns (labels [lanes,F,64] lagging 24 frames, latent traces [lanes,24,64], viterbi score)."""
+    def __call__(self, traces, models, margin=False):
+        """Returns (labels [lanes,F,64] lagging 24 frames, latent traces [lanes,24,64], viterbi score), and
+        with margin=True also each label's best-path decision margin [lanes,F,64] (see hw_labeler_process)."""
         labels = torch.empty_like(traces)
         lat = torch.empty((self.lanes, self.latent_frames, abi.LANE), dtype=torch.int16, device=traces.device)
         score = torch.empty((self.lanes, abi.LANE), dtype=torch.float32, device=traces.device)
-        check(lib().hw_labeler_process(self._h, _p(traces), _p(models), _p(labels), _p(lat), _p(score), _stream()))
-        return labels, lat, score
+        mg = torch.empty(traces.shape, dtype=torch.float32, device=traces.device) if margin else None
+        check(lib().hw_labeler_process(self._h, _p(traces), _p(models), _p(labels), _p(lat), _p(score),
+                                       _p(mg) if margin else None, _stream()))
+        return (labels, lat, score, mg) if margin else (labels, lat, score)
 
 
 class PulseAccumulator(_Handle):

@@ -128,7 +128,7 @@ def lib():
                                        C.c_int),
         "hw_labeler_create": ([PCFG, u32, u32, u32, PPV], C.c_int),
         "hw_labeler_destroy": ([vp], C.c_int),
-        "hw_labeler_process": ([vp, vp, vp, vp, vp, vp, vp], C.c_int),
+        "hw_labeler_process": ([vp, vp, vp, vp, vp, vp, vp, vp], C.c_int),
         "hw_pulse_accumulator_create": ([PCFG, u32, u32, u32, PPV], C.c_int),
         "hw_pulse_accumulator_destroy": ([vp], C.c_int),
         "hw_pulse_accumulator_process": ([vp, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp], C.c_int),

@@ -462,10 +462,18 @@ int hw_labeler_destroy(hw_labeler* l);
 /* Labels lag the traces by hw_labeler_latent_frames() (24) frames.
  * d_labels[lanes][F][64] int16; d_latent_out[lanes][24][64] receives the
  * traces the first 24 labels belong to (LabelsBatch::LatentTrace);
- * d_viterbi_score[lanes][64] the anchor log-likelihood. */
+ * d_viterbi_score[lanes][64] the anchor log-likelihood.
+ * d_margin_or_null[lanes][F][64] float, if not NULL, receives the best path's
+ * decision margin of every label: for label f < F - 1, the gap between the
+ * winning and the best other candidate of the path state's row in the
+ * Viterbi step of frame f + 1 (which chose label f; 0 on a tie, +inf when
+ * only one candidate is finite); for the last label, the gap between the
+ * largest and the next back-propagated end-state probability (the anchor
+ * choice, FrameLabelerHost.cpp:410-418).  The first call with a margin
+ * buffer allocates the handle's gap scratch (13 floats per frame and ZMW). */
 int hw_labeler_process(hw_labeler* l, const int16_t* d_traces, const hw_lane_model* d_models,
                        int16_t* d_labels, int16_t* d_latent_out, float* d_viterbi_score,
-                       void* stream);
+                       float* d_margin_or_null, void* stream);
 uint32_t hw_labeler_latent_frames(void);
 
 /* ---- Pulse accumulator (PulseAccumulator.h:68-74, HostPulseAccumulator) - */

@@ -849,7 +849,8 @@ struct OraclePool
               hw_frame_interval pfi, const hw_lane_model* models, int mode, const float* proposal,
               const float* target, float tol, uint32_t maxIter, float* params, int32_t* iters, float* loglike);
 
-    int Label(const int16_t* traces, const hw_lane_model* models, int16_t* labels, int16_t* latOut, float* score);
+    int Label(const int16_t* traces, const hw_lane_model* models, int16_t* labels, int16_t* latOut, float* score,
+              float* margin);
 
     int Pulses(const int16_t* labels, const int16_t* latTrace, const int16_t* trace, int32_t firstFrame,
                const hw_lane_model* models, hw_pulse* pulses, uint32_t* lens, uint32_t* ovf,
@@ -1644,8 +1645,15 @@ struct Scorer
 
 }   // namespace
 
+// margin (optional, [lanes][F][64]): the best path's decision margin of each
+// label.  Label f < F - 1 is the arg-max source that the Viterbi step of frame
+// f + 1 recorded for the path's state there; its margin is that step's gap
+// between the winning candidate and the best other one of the state's row
+// (0 on a tie, +inf with a single finite candidate).  The last label is the
+// anchor state; its margin is the gap between the largest back-propagated
+// end-state probability and the next largest.
 int OraclePool::Label(const int16_t* traces, const hw_lane_model* models, int16_t* labels,
-                      int16_t* latOut, float* score)
+                      int16_t* latOut, float* score, float* margin)
 {
     const int L = hwp::kLatentFrames;
     const int LB = hwp::kViterbiStitchLookback;
@@ -1657,6 +1665,7 @@ int OraclePool::Label(const int16_t* traces, const hw_lane_model* models, int16_
 #pragma omp parallel
     {
         std::vector<uint16_t> tb((size_t)(F + LB) * kStates);   // traceback per frame per state
+        std::vector<float> gap(margin ? (size_t)(F + LB) * kStates : 0);   // decision gap per frame per state
         std::vector<uint8_t> roi(nRoi);
         std::vector<float> tr((size_t)(F + L));
 #pragma omp for schedule(dynamic, 1)
@@ -1720,16 +1729,19 @@ int OraclePool::Label(const int16_t* traces, const hw_lane_model* models, int16_
                         const float score = sco[r];
                         int idx = sp.first[r];
                         float mv = score + d.trans[r][idx] + ll[idx];
+                        float sv = -kInf;     // best of the other candidates
                         for (int p = sp.segBegin[r]; p < sp.segEnd[r]; ++p)
                         {
                             const float v = score + d.trans[r][p] + ll[p];
                             const bool cnd = v >= mv;
+                            sv = cnd ? mv : ((v > sv) ? v : sv);
                             mv = cnd ? v : mv;
                             idx = cnd ? p : idx;
                         }
                         const float penalty = (r == 0 || isRoi) ? 0.0f : kInf;
                         la[r] = mv - penalty;
                         tb[(size_t)lf * kStates + r] = (uint16_t)idx;
+                        if (margin) gap[(size_t)lf * kStates + r] = mv - sv;
                     }
                     for (int r = 0; r < kStates; ++r) ll[r] = la[r];
                 };
@@ -1769,9 +1781,19 @@ int OraclePool::Label(const int16_t* traces, const hw_lane_model* models, int16_
                 }
                 int ts = anchorState;
                 int16_t* out = labels + (size_t)l * F * kLane;
+                float* mg = margin ? margin + (size_t)l * F * kLane : nullptr;
+                if (mg)
+                {
+                    float second = -kInf;
+                    for (int i = 0; i < kStates; ++i)
+                        if (i != anchorState) second = (prob[i] > second) ? prob[i] : second;
+                    mg[(size_t)(F - 1) * kLane + z] = maxP - second;
+                }
                 for (int f = (int)F - 1; f >= 0; --f)
                 {
                     out[(size_t)f * kLane + z] = (int16_t)ts;
+                    if (mg && f < (int)F - 1)
+                        mg[(size_t)f * kLane + z] = gap[(size_t)(f + 1) * kStates + out[(size_t)(f + 1) * kLane + z]];
                     ts = tb[(size_t)f * kStates + ts];
                 }
                 latRoi[(size_t)l * kLane + z] = roi[F - 1];
@@ -1935,8 +1957,9 @@ int or_dme_estimate(void* p, const hw_lane_histogram* h, const hw_baseliner_stat
                     hw_frame_interval mfi, hw_lane_model* m, hw_dme_diag* diag)
 { return static_cast<OraclePool*>(p)->Estimate(h, s, hfi, mfi, m, diag); }
 
-int or_label(void* p, const int16_t* tr, const hw_lane_model* m, int16_t* labels, int16_t* latOut, float* score)
-{ return static_cast<OraclePool*>(p)->Label(tr, m, labels, latOut, score); }
+int or_label(void* p, const int16_t* tr, const hw_lane_model* m, int16_t* labels, int16_t* latOut, float* score,
+             float* margin)
+{ return static_cast<OraclePool*>(p)->Label(tr, m, labels, latOut, score, margin); }
 
 int or_pulses(void* p, const int16_t* labels, const int16_t* lat, const int16_t* tr, int32_t firstFrame,
               const hw_lane_model* m, hw_pulse* pulses, uint32_t* lens, uint32_t* ovf, hw_stat_accum_state* bs)

@@ -49,7 +49,7 @@ def lib():
         L.or_hist_get.argtypes = [vp, vp, C.POINTER(FI)]
         L.or_dme_init_models.argtypes = [vp, vp, vp]
         L.or_dme_estimate.argtypes = [vp, vp, vp, FI, FI, vp, vp]
-        L.or_label.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.or_label.argtypes = [vp, vp, vp, vp, vp, vp, vp]
         L.or_pulses.argtypes = [vp, vp, vp, vp, i32, vp, vp, vp, vp, vp]
         L.or_dme_estimate_proposal.argtypes = [vp, vp, vp, FI, FI, vp, vp, vp]
         L.or_em_fit.argtypes = [vp, vp, vp, FI, FI, vp, C.c_int, vp, vp, C.c_float, u32, vp, vp, vp]
@@ -243,7 +243,9 @@ class Pool:
                                float(tol), int(max_iter), abi.ptr(params), abi.ptr(iters), abi.ptr(ll)))
         return params, iters, ll
 
-    def label(self, traces, models):
+    def label(self, traces, models, margin=False):
+        """FrameLabeler: labels, latent trace, Viterbi score (and, with
+        margin=True, the best path's decision margin of every label)."""
         traces = np.ascontiguousarray(traces, dtype=np.int16)
         if traces.shape != (self.lanes, self.F, abi.LANE) or len(models) != self.lanes:
             raise ValueError(f"oracle label: traces {traces.shape}, {len(models)} models for "
@@ -251,9 +253,10 @@ class Pool:
         labels = np.empty_like(traces)
         lat = np.empty((self.lanes, abi.LATENT_FRAMES, abi.LANE), np.int16)
         score = np.empty((self.lanes, abi.LANE), np.float32)
+        mg = np.empty(traces.shape, np.float32) if margin else None
         _check(lib().or_label(self.h, abi.ptr(traces), abi.ptr(models), abi.ptr(labels), abi.ptr(lat),
-                              abi.ptr(score)))
-        return labels, lat, score
+                              abi.ptr(score), abi.ptr(mg) if margin else None))
+        return (labels, lat, score, mg) if margin else (labels, lat, score)
 
     def pulses(self, labels, latent, traces, first_frame, models):
         cap = self.cfg.max_calls_per_zmw

@@ -56,32 +56,35 @@ def fixed_model(lanes, means=synth.LABELER_TEST_MEANS):
 
 
 class OracleLabeler:
-    def __init__(self, cfg, pool_id, lanes):
+    def __init__(self, cfg, pool_id, lanes, margin=False):
         import oracle
         self.p = oracle.Pool(cfg, lanes, BLOCK_LEN, pool_id)
+        self.margin = margin
 
     def __call__(self, chunk, models):
-        return self.p.label(chunk, models)
+        return self.p.label(chunk, models, self.margin)
 
 
 class GpuLabeler:
-    def __init__(self, cfg, pool_id, lanes):
+    def __init__(self, cfg, pool_id, lanes, margin=False):
         import torch
         from hw_b200 import filters as Fl
         self.torch, self.Fl = torch, Fl
         self.lab = Fl.FrameLabeler(cfg, pool_id, lanes, BLOCK_LEN)
+        self.margin = margin
 
     def __call__(self, chunk, models):
-        labels, lat, score = self.lab(self.torch.from_numpy(chunk).cuda(), self.Fl.numpy_to_struct(models))
-        return labels.cpu().numpy(), lat.cpu().numpy(), score.cpu().numpy()
+        out = self.lab(self.torch.from_numpy(chunk).cuda(), self.Fl.numpy_to_struct(models), self.margin)
+        self.torch.cuda.synchronize()
+        return tuple(t.cpu().numpy() for t in out)
 
 
-def run(make, traces, means=synth.LABELER_TEST_MEANS):
+def run(make, traces, means=synth.LABELER_TEST_MEANS, margin=False):
     """Label every chunk of every pool; returns the per-chunk outputs."""
     cfg = movie_config()
     out = []
     for p in range(POOLS):
-        lab = make(cfg, p, LANES_PER_POOL)
+        lab = make(cfg, p, LANES_PER_POOL, margin)
         models = fixed_model(LANES_PER_POOL, means)
         tr = traces[p * LANES_PER_POOL:(p + 1) * LANES_PER_POOL]
         out.append([lab(np.ascontiguousarray(tr[:, c * BLOCK_LEN:(c + 1) * BLOCK_LEN]), models)
@@ -97,7 +100,8 @@ def score(outputs, truth, shift=0):
     nf = truth.shape[1]
     for p, chunks in enumerate(outputs):
         t = truth[p * LANES_PER_POOL:(p + 1) * LANES_PER_POOL]
-        for c, (labels, _, _) in enumerate(chunks):
+        for c, res in enumerate(chunks):
+            labels = res[0]
             for j in range(BLOCK_LEN):
                 frame = c * BLOCK_LEN + j - LATENT + shift
                 if frame < 0 or frame >= nf:
@@ -119,12 +123,40 @@ def data():
 
 @pytest.fixture(scope="module")
 def oracle_out(data):
-    return run(OracleLabeler, data[0])
+    return run(OracleLabeler, data[0], margin=True)
+
+
+def agree_except_small_margin(a, b, margin, tol=1e-5):
+    """The parity rule for labels: equal except where the decision that
+    chose the label was closer than `tol`."""
+    return bool(np.all((a == b) | (margin < tol)))
 
 
 def test_oracle_meets_reference_thresholds(data, oracle_out):
     m, s, x = score(oracle_out, data[1])
     assert m > 0.97 and s < 0.02 and x < 0.01, (m, s, x)
+
+
+def test_oracle_margins(oracle_out):
+    """Margins are gaps between the winning and the next candidate: never
+    negative or NaN; the last label's is a probability gap in [0, 1]
+    (up to rounding);
+    the margin option leaves labels, latent traces and scores unchanged."""
+    for chunks in oracle_out:
+        for labels, lat, score, mg in chunks:
+            assert not np.isnan(mg).any() and (mg >= 0).all()
+            assert (mg[:, -1, :] <= np.float32(1 + 1e-6)).all()     # normalised in float: may round above 1
+    import oracle
+    cfg = movie_config()
+    a = oracle.Pool(cfg, 1, BLOCK_LEN)
+    b = oracle.Pool(cfg, 1, BLOCK_LEN)
+    tr, _ = synth.labeled_traces(1, BLOCK_LEN * 4, seed=3)
+    m = fixed_model(1)
+    for c in range(4):
+        chunk = np.ascontiguousarray(tr[:, c * BLOCK_LEN:(c + 1) * BLOCK_LEN])
+        ra, rb = a.label(chunk, m), b.label(chunk, m, True)
+        for x, y in zip(ra, rb[:3]):
+            assert np.array_equal(x.view(np.uint8), y.view(np.uint8))
 
 
 def test_thresholds_catch_a_shifted_truth(data, oracle_out):
@@ -150,3 +182,18 @@ def test_gpu_labels_equal_oracle_and_meet_thresholds(data, oracle_out):
                 assert np.array_equal(np.asarray(a).view(np.uint8), np.asarray(b).view(np.uint8)), (p, c, what)
     m, s, x = score(got, data[1])
     assert m > 0.97 and s < 0.02 and x < 0.01, (m, s, x)
+
+
+@pytest.mark.gpu
+def test_gpu_margins_equal_oracle(data, oracle_out):
+    """hw_labeler_process with a margin buffer: labels, latent traces,
+    scores and every label's margin equal the oracle's bit for bit, so the
+    rule 'labels equal except where the margin is under 1e-5' can be
+    evaluated at the C ABI."""
+    got = run(GpuLabeler, data[0], margin=True)
+    for p in range(POOLS):
+        for c in range(N_BLOCKS):
+            for k, what in enumerate(("labels", "latent", "viterbi score", "margin")):
+                a, b = got[p][c][k], oracle_out[p][c][k]
+                assert np.array_equal(np.asarray(a).view(np.uint8), np.asarray(b).view(np.uint8)), (p, c, what)
+            assert agree_except_small_margin(got[p][c][0], oracle_out[p][c][0], oracle_out[p][c][3])
