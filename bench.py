@@ -2,21 +2,29 @@
 """Throughput of the smrt-basecaller trace-analysis chain on B200.
 
 Workload (chip scale): 1,048,576 ZMWs = 16,384 lanes of 64, as 4 pools of 4096
-lanes, 512-frame int16 chunks from the device trace generator (lognormal gain
-sigma 0.2, 15% empty ZMWs, 0.05 DN/frame baseline random walk), reference
-default analysis parameters (MultiScaleLarge baseliner, dynamic estimation:
-every pool re-estimates its detection models every 4000 frames, staggered by
+lanes, 512-frame int16 chunks from the trace generator (lognormal gain sigma
+0.2, 15% empty ZMWs, 0.05 DN/frame baseline random walk), reference default
+analysis parameters (MultiScaleLarge baseliner, dynamic estimation: every
+pool re-estimates its detection models every 4000 frames, staggered by
 pool).  The run first streams the start-up chunks (untimed) until every pool
 is in its periodic estimation cycle; a step is then one chunk of the whole
 chip through baseliner -> statistics -> histogram -> (EM when due) ->
-labeler -> pulses.  The default K = 8 steps covers exactly one 8-chunk
-estimation cycle, so every pool runs its EM once inside the timed region.
-With --gpus N each rank analyses its own chip-sized ZMW range (weak
-scaling, no data exchange).
+labeler -> pulses (+ HF metrics), all pools in one hw_chunk_fused call.  The
+8-step estimation cycle runs one EM per pool, so K steps from a given phase
+of the cycle hold a phase-dependent number of EMs; both timed legs below
+start at the same phase and run the same K steps.  With --gpus N each rank
+analyses its own chip-sized ZMW range (weak scaling, no data exchange).
 
   value : ZMW-frames/s with the chunks already in HBM
-  e2e   : same through hw_analyzer_process with the chunk copied from pinned
-          host memory and the pulse output copied back inside the timed region
+  e2e   : the same K steps through hw_chunk_fused with every step's chunk
+          copied from pinned host memory and all pulse outputs copied back
+          inside the timed region (copies on their own streams, double
+          buffered; the first upload and the last download overlap nothing)
+
+--impl reference times the oracle (the CPU restatement of the reference's
+Host* path) on the host cores over a lane sample of the same workload, with
+traces from the oracle's host copy of the generator: nothing of the CUDA
+library is loaded on that arm.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl hw|reference]
        python bench.py --next-rows    (the stages after and before the chain:
@@ -40,6 +48,8 @@ sys.path.insert(0, ROOT)
 FRAMES = 512
 LANES_PER_POOL = 4096
 POOLS = 4
+WORKLOAD = ("chip: 1,048,576 ZMWs (16,384 lanes, 4 pools) x 512-frame int16 chunks, trace generator "
+            "workload 1, reference default parameters, dynamic DME")
 KERNELS_PER_STAGE = {"baseline": 1, "aggregate": 1, "histogram": 1, "model_init": 1, "dme": 1,
                      "hist_reset": 2, "labeler": 2, "pulses": 1, "metrics": 1}
 
@@ -153,21 +163,23 @@ def labeler_alg_bytes_per_zmw(F):
 
 
 def cpu_baseline(cfg, lanes, steps, warmup, threads):
-    """The oracle (CPU restatement of the reference Host* path) on a sample of lanes."""
-    import torch
+    """The oracle (CPU restatement of the reference Host* path) on a sample of
+    lanes of the chip workload, traces from the oracle's host generator (the
+    CUDA library is not loaded).  Returns (ZMW-frames/s, seconds timed)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    from hw_b200 import filters as Fl
+    from hw_b200 import workloads
     oracle.set_threads(threads)
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from harness import OracleBackend, Pipeline
-    pipe = Pipeline(OracleBackend(cfg, lanes, FRAMES, 0), cfg, 0)
-    gen = Fl.TraceGenerator(lanes, workload=1, zmw_offset=0)
-    n0 = startup_chunks(cfg, 1) + warmup
+    backend = OracleBackend(cfg, lanes, FRAMES, 0)
+    pipe = Pipeline(backend, cfg, 0)
+    gen = oracle.TraceGenerator(lanes, workload=1, zmw_offset=0)
+    n0 = workloads.startup_chunks(cfg, 1, FRAMES, latency=backend.startup_latency()) + warmup
     total = n0 + steps
     t_timed = 0.0
     for c in range(total):
-        chunk = gen.next(c * FRAMES, FRAMES).cpu().numpy()
+        chunk = gen.next(c * FRAMES, FRAMES)
         t0 = time.perf_counter()
         pipe.process(chunk, c * FRAMES)
         dt = time.perf_counter() - t0
@@ -292,6 +304,33 @@ def next_rows(threads):
 def main():
     args = parse()
     world, rank, local = dist_setup()
+    from hw_b200 import workloads
+    cfg = workloads.chip_config()
+    total_lanes = args.lanes_per_pool * args.pools
+    zmws = total_lanes * 64
+    threads = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        # The reference path on the host cores: rank 0 alone, no CUDA and no
+        # collective (the other ranks exit at once).
+        if rank == 0:
+            rate, secs = cpu_baseline(cfg, args.cpu_lanes, max(args.steps, 1), args.warmup, threads)
+            sample = (f"{args.cpu_lanes} lanes ({args.cpu_lanes * 64} ZMWs) of the workload x {args.steps} "
+                      f"steady-state 512-frame chunks after start-up, {secs:.1f} s of CPU time")
+            zf_step = args.cpu_lanes * 64 * FRAMES
+            out = {"metric": "ZMW-frames/s", "value": rate, "unit": "ZMW-frames/s", "impl": "reference",
+                   "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                   "ms_per_step": zf_step / rate * 1e3, "higher_is_better": True, "scaling": "weak",
+                   "vs_baseline": None, "dtype": "int16+f32", "data": "synthetic",
+                   "config": {"workload": WORKLOAD, "zmws_per_gpu": zmws, "frames_per_chunk": FRAMES,
+                              "pools": args.pools, "cpu_sample_lanes": args.cpu_lanes},
+                   "cpu_baseline": {"value": rate, "unit": "ZMW-frames/s", "cores": threads, "kind": "port",
+                                    "sample": sample},
+                   "e2e": {"value": rate, "unit": "ZMW-frames/s", "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}}
+            print(json.dumps(out), flush=True)
+        return
+
     import torch
     torch.cuda.set_device(local)
     if world > 1:
@@ -299,37 +338,10 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
-    from hw_b200 import filters as Fl, workloads
+    from hw_b200 import filters as Fl
     if args.next_rows:
         if rank == 0:
             next_rows(os.cpu_count() or 1)
-        return
-    cfg = workloads.chip_config()
-    total_lanes = args.lanes_per_pool * args.pools
-    zmws = total_lanes * 64
-    threads = os.cpu_count() or 1
-
-    if args.impl == "reference":
-        out = None
-        if rank == 0:
-            rate, secs = cpu_baseline(cfg, args.cpu_lanes, max(args.steps, 1), args.warmup, threads)
-            sample = (f"{args.cpu_lanes} lanes ({args.cpu_lanes * 64} ZMWs) x {args.steps} steady-state "
-                      f"512-frame chunks after start-up, {secs:.1f} s of CPU time")
-            out = {"metric": "ZMW-frames/s", "value": rate, "unit": "ZMW-frames/s", "impl": "reference",
-                   "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-                   "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                   "dtype": "int16+f32", "data": "synthetic",
-                   "config": {"workload": "chip: 1,048,576 ZMWs x 512-frame chunks (sampled on CPU)",
-                              "lanes": total_lanes, "frames_per_chunk": FRAMES, "pools": args.pools},
-                   "cpu_baseline": {"value": rate, "unit": "ZMW-frames/s", "cores": threads, "kind": "port",
-                                    "sample": sample},
-                   "e2e": {"value": rate, "unit": "ZMW-frames/s", "h2d_bytes_per_step": 0,
-                           "d2h_bytes_per_step": 0}}
-            print(json.dumps(out), flush=True)
-        if world > 1:
-            import torch.distributed as dist
-            dist.barrier()
-            dist.destroy_process_group()
         return
 
     from hw_b200.shard import zmw_offset
@@ -373,6 +385,7 @@ def main():
 
     # Device-resident timed region.
     K = args.steps
+    c_dev0 = c
     dev_chunks = []
     for k in range(K):
         t = torch.empty((total_lanes, FRAMES, 64), dtype=torch.int16, device="cuda")
@@ -434,11 +447,18 @@ def main():
     # step k's kernels.
     e2e = None
     if not args.no_e2e:
-        # at least 64 steps: the first upload and the last download (~20 ms
-        # each, overlapped with no analysis) are a one-off of a stream, and
-        # over 16 steps they weighed 7% of the rate.  16 distinct pinned
-        # chunks, uploaded in turn (every step still moves its 1 GiB).
-        KE = max(K, 64)
+        # The same K steps from the same phase of the estimation cycle as
+        # the device-resident leg (so both run the same number of EMs): the
+        # engine first streams untimed chunks up to that phase.  Up to 16
+        # distinct pinned chunks are uploaded in turn (every step still moves
+        # its 1 GiB).
+        cycle = (max(int(cfg.min_frames_for_estimate), 1) + FRAMES - 1) // FRAMES
+        while (c - c_dev0) % cycle:
+            gen.next(c * FRAMES, FRAMES, out=buf)
+            run_chunk(buf, c)
+            c += 1
+        torch.cuda.synchronize()
+        KE = K
         host_chunks = []
         tmp = torch.empty((total_lanes, FRAMES, 64), dtype=torch.int16, device="cuda")
         for k in range(min(KE, 16)):
@@ -500,7 +520,9 @@ def main():
         d2h = sum(dp.numel() + dl.numel() * 4 + do.numel() * 4 for dp, dl, do in outputs) + metrics_bytes // KE
         e2e = {"value": zf_step * KE * world / (ms_e2e / 1e3), "unit": "ZMW-frames/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / KE, "steps": KE,
-               "overlap": "copies on their own streams, double-buffered against the analysis"}
+               "phase": "same K steps of the estimation cycle as value",
+               "overlap": "copies on their own streams, double-buffered against the analysis; the first "
+                          "upload and the last download overlap no analysis"}
         del host_chunks, in_dev, out_dev
 
     # Roofline of the dominant kernel (the frame labeler) from the live stage timers.
@@ -551,8 +573,7 @@ def main():
             "metric": "ZMW-frames/s", "value": value, "unit": "ZMW-frames/s", "n_gpus": world,
             "steps": K, "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int16+f32", "data": "synthetic",
-            "config": {"workload": "chip: 1,048,576 ZMWs (16,384 lanes, 4 pools) x 512-frame chunks, "
-                                   "reference default parameters, dynamic DME",
+            "config": {"workload": WORKLOAD,
                        "zmws_per_gpu": zmws, "frames_per_chunk": FRAMES, "pools": args.pools,
                        "startup_chunks": n_start, "inputs": "1 GiB chunk per step, larger than L2",
                        "engine": "hw_chunk_fused (one launch per stage over all pools)" if args.engine == "fused"

@@ -99,20 +99,23 @@ def small_config():
     return cfg
 
 
-def startup_chunks(cfg, pools, frames=512):
+def startup_chunks(cfg, pools, frames=512, latency=None):
     """Chunks of `frames` until every one of `pools` pools of the dynamic
     schedule has entered its periodic estimation cycle: the baseliner's
-    start-up latency, the stagger of the last pool, the statistics
-    pre-accumulation and one estimation period."""
-    import ctypes as C
-    from . import native
-    b = C.c_void_p()
-    native.check(native.lib().hw_baseliner_create(C.byref(cfg), 0, 1, frames, C.byref(b)))
-    lat = C.c_uint32()
-    native.lib().hw_baseliner_startup_latency(b, C.byref(lat))
-    native.lib().hw_baseliner_destroy(b)
+    start-up latency (`latency` frames, or the library's value for `cfg`),
+    the stagger of the last pool, the statistics pre-accumulation and one
+    estimation period."""
+    if latency is None:
+        import ctypes as C
+        from . import native
+        b = C.c_void_p()
+        native.check(native.lib().hw_baseliner_create(C.byref(cfg), 0, 1, frames, C.byref(b)))
+        lat = C.c_uint32()
+        native.lib().hw_baseliner_startup_latency(b, C.byref(lat))
+        native.lib().hw_baseliner_destroy(b)
+        latency = lat.value
     chunks_per_est = (max(cfg.min_frames_for_estimate, 1) + frames - 1) // frames
     last_delay = ((pools - 1) % chunks_per_est) * frames
-    start = (lat.value + last_delay + frames - 1) // frames          # first chunk the last pool analyses
+    start = (latency + last_delay + frames - 1) // frames            # first chunk the last pool analyses
     pre = (cfg.num_frames_pre_accum_stats + frames - 1) // frames    # histogram start-up
     return start + pre + chunks_per_est

@@ -2011,6 +2011,158 @@ float or_logf(float x) { return hw_logf(x); }
 uint16_t or_f32_to_f16(float x) { return f32_to_f16_bits(x); }
 int16_t or_to_i16(float x) { return to_i16_wrap(x); }
 
+// The workloads' synthetic trace generator (hw_b200/csrc/gen.cu) on the host:
+// the same counter-based hash per (seed, ZMW, frame, slot), polar normals and
+// float arithmetic, so a chunk is byte-identical to the device generator's.
+// It lets the CPU baseline draw its traces without the CUDA library.  The
+// workload defaults restate hw_gen_params_default; a test checks both.
+namespace {
+inline uint64_t GenMix64(uint64_t x)
+{
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+inline uint64_t GenDraw(uint64_t key, uint64_t ctr) { return GenMix64(key ^ GenMix64(ctr)); }
+inline float GenU24(uint64_t r, int half)
+{
+    const uint32_t v = half ? (uint32_t)(r >> 40) : (uint32_t)((r >> 8) & 0xFFFFFFu);
+    return (float)v * 5.9604644775390625e-08f;
+}
+inline float GenNormal(uint64_t key, uint64_t ctrBase)
+{
+    for (int a = 0; a < 8; ++a)
+    {
+        const uint64_t r = GenDraw(key, ctrBase + a);
+        const float u = 2.0f * GenU24(r, 0) - 1.0f, v = 2.0f * GenU24(r, 1) - 1.0f;
+        const float s = u * u + v * v;
+        if (s > 0.0f && s < 1.0f) return u * std::sqrt(-2.0f * hw_logf(s) / s);
+    }
+    return 0.0f;
+}
+
+struct OracleGen
+{
+    hw_gen_params p;
+    uint32_t lanes;
+    uint64_t zmwOffset;
+    std::vector<uint8_t> inPulse;
+    std::vector<float> amp, walk;
+};
+}   // namespace
+
+extern "C" {
+
+int or_gen_params_default(int workload, hw_gen_params* p)
+{
+    if (!p) return HW_ERR_INVALID_ARG;
+    std::memset(p, 0, sizeof(*p));
+    p->seed = 0x5eed0000ull + (uint64_t)workload;
+    p->baseline_mean = 200.0f;
+    p->baseline_sigma = 8.0f;
+    const float amps[4] = {80.0f, 50.0f, 32.0f, 20.0f};
+    for (int a = 0; a < 4; ++a) p->amplitudes[a] = amps[a];
+    p->amp_cv = 0.1f;
+    p->pulse_width_mean = 8.0f;
+    p->ipd_mean = 14.0f;
+    p->shot_coeff = 0.5f;
+    p->step_frame = -1;
+    switch (workload)
+    {
+    case 0: break;
+    case 1: p->gain_sigma = 0.2f; p->empty_fraction = 0.15f; p->walk_sigma = 0.05f; break;
+    case 2: p->amp_scale_sigma = 0.3f; p->rate_min = 0.02f; p->rate_max = 0.12f; p->pulse_width_mean = 4.0f; break;
+    case 4:
+        p->gain_sigma = 0.2f; p->empty_fraction = 0.15f; p->walk_sigma = 0.05f;
+        p->decay_fraction = 0.2f; p->decay_frames = 128 * 512;
+        p->step_frame = 64 * 512; p->step_dn = 15.0f; p->step_fraction = 0.01f;
+        break;
+    default: return HW_ERR_INVALID_ARG;
+    }
+    return HW_OK;
+}
+
+void* or_gen_create(const hw_gen_params* p, uint32_t lanes, uint64_t zmwOffset)
+{
+    if (!p || lanes == 0) return nullptr;
+    auto g = new OracleGen{*p, lanes, zmwOffset, {}, {}, {}};
+    const size_t n = (size_t)lanes * kLane;
+    g->inPulse.assign(n, 0);
+    g->amp.assign(n, 0.0f);
+    g->walk.assign(n, 0.0f);
+    return g;
+}
+
+void or_gen_destroy(void* g) { delete static_cast<OracleGen*>(g); }
+
+// Frames [firstFrame, firstFrame + frames) of every lane into out[lanes][frames][64].
+int or_gen_next(void* gp, int16_t* out, int64_t firstFrame, uint32_t frames)
+{
+    OracleGen& G = *static_cast<OracleGen*>(gp);
+    const hw_gen_params& P = G.p;
+    const int64_t n = (int64_t)G.lanes * kLane;
+#pragma omp parallel for schedule(static)
+    for (int64_t g = 0; g < n; ++g)
+    {
+        const int64_t l = g / kLane, z = g % kLane;
+        const uint64_t zmw = G.zmwOffset + (uint64_t)g;
+        const uint64_t key = GenMix64(P.seed ^ GenMix64(zmw * 0x2545F4914F6CDD1Dull + 1));
+        const float gain = (P.gain_sigma > 0.0f) ? hw_expf(P.gain_sigma * GenNormal(key, 0)) : 1.0f;
+        const float ampScale = (P.amp_scale_sigma > 0.0f) ? hw_expf(P.amp_scale_sigma * GenNormal(key, 8)) : 1.0f;
+        const uint64_t rz = GenDraw(key, 16);
+        const bool empty = GenU24(rz, 0) < P.empty_fraction;
+        const bool stepped = GenU24(rz, 1) < P.step_fraction;
+        float startHazard = 1.0f / P.ipd_mean;
+        if (P.rate_max > 0.0f)
+        {
+            const float rate = P.rate_min + (P.rate_max - P.rate_min) * GenU24(GenDraw(key, 17), 0);
+            const float gap = std::fmax(1.0f / rate - P.pulse_width_mean, 1.0f);
+            startHazard = 1.0f / gap;
+        }
+        const float endHazard = 1.0f / P.pulse_width_mean;
+        bool inp = G.inPulse[g] != 0;
+        float amp = G.amp[g];
+        float walk = G.walk[g];
+        int16_t* o = out + (size_t)l * frames * kLane + z;
+        for (uint32_t t = 0; t < frames; ++t)
+        {
+            const int64_t f = firstFrame + t;
+            const uint64_t base = (uint64_t)(f + 1) * 32;
+            const uint64_t r0 = GenDraw(key, base);
+            const float u = GenU24(r0, 0);
+            if (inp)
+            {
+                if (u < endHazard) inp = false;
+            }
+            else if (!empty && u < startHazard)
+            {
+                inp = true;
+                int a = (int)(GenU24(r0, 1) * 4.0f);
+                a = a > 3 ? 3 : a;
+                float decay = 1.0f;
+                if (P.decay_frames > 0)
+                    decay = 1.0f - P.decay_fraction * std::fmin((float)f / (float)P.decay_frames, 1.0f);
+                const float an = GenNormal(key, base + 1);
+                amp = std::fmax(P.amplitudes[a] * gain * ampScale * decay * (1.0f + P.amp_cv * an), 0.0f);
+            }
+            if (P.walk_sigma > 0.0f) walk += P.walk_sigma * GenNormal(key, base + 9);
+            const float sig = inp ? amp : 0.0f;
+            float level = P.baseline_mean + walk + sig;
+            if (stepped && P.step_frame >= 0 && f >= P.step_frame) level += P.step_dn;
+            const float sd = std::sqrt(P.baseline_sigma * P.baseline_sigma + P.shot_coeff * sig);
+            const float v = std::rint(level + sd * GenNormal(key, base + 17));
+            o[(size_t)t * kLane] = (int16_t)std::fmin(std::fmax(v, -32768.0f), 32767.0f);
+        }
+        G.inPulse[g] = inp ? 1 : 0;
+        G.amp[g] = amp;
+        G.walk[g] = walk;
+    }
+    return HW_OK;
+}
+
+}   // extern "C"
+
 // PicketFenceGenerator::GenerateSignal (appModules/SimulatedDataSource.cpp:
 // 252-323, config SimulatedDataSource.h:176-212): the reference baseliner
 // tests' traces.  Signal `idx` seeds its own std::mt19937 (seedFunc = the

@@ -66,6 +66,11 @@ def lib():
         L.or_detection_model_evolve_confidence.argtypes = [vp, u32, FI, FI, C.c_float]
         L.or_picket_fence.argtypes = [u32, C.c_uint64, C.c_int, C.c_uint16, C.c_uint16, C.c_float, C.c_float,
                                       C.c_int16, C.c_int16, vp, C.c_int, C.c_int16, vp]
+        L.or_gen_params_default.argtypes = [C.c_int, C.POINTER(abi.GenParams)]
+        L.or_gen_create.argtypes = [C.POINTER(abi.GenParams), u32, C.c_uint64]
+        L.or_gen_create.restype = vp
+        L.or_gen_destroy.argtypes = [vp]
+        L.or_gen_next.argtypes = [vp, vp, C.c_int64, u32]
         L.or_to_i16.argtypes = [C.c_float]
         L.or_to_i16.restype = C.c_int16
         L.or_hf_create.argtypes = [u32, u32, C.c_double, i32]
@@ -143,6 +148,34 @@ def picket_fence(num_frames, idx, poisson=True, pulse_width=5, pulse_ipd=10, wid
     _check(lib().or_picket_fence(num_frames, idx, int(poisson), pulse_width, pulse_ipd, width_rate, ipd_rate,
                                  baseline_level, baseline_sigma, abi.ptr(lv), len(lv), pedestal, abi.ptr(out)))
     return out
+
+
+def gen_params_default(workload):
+    p = abi.GenParams()
+    _check(lib().or_gen_params_default(int(workload), C.byref(p)))
+    return p
+
+
+class TraceGenerator:
+    """The workloads' trace generator on the host (byte-identical to
+    hw_trace_generator): chunks [lanes][frames][64] int16, in order."""
+
+    def __init__(self, lanes, workload=1, zmw_offset=0, params=None):
+        self.lanes = lanes
+        self.params = gen_params_default(workload) if params is None else params
+        self.h = lib().or_gen_create(C.byref(self.params), lanes, zmw_offset)
+        if not self.h:
+            raise RuntimeError("oracle generator create failed")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_gen_destroy(self.h)
+            self.h = None
+
+    def next(self, first_frame, frames):
+        out = np.empty((self.lanes, frames, abi.LANE), np.int16)
+        _check(lib().or_gen_next(self.h, abi.ptr(out), int(first_frame), int(frames)))
+        return out
 
 
 def set_threads(n):
