@@ -357,6 +357,10 @@ __device__ __forceinline__ float EmEStep(const KParams& k, const EmHist& h, cons
                                          float* bpS, float* tau0S, float* facS, float ci[5], float mom1[5],
                                          float varinv[5], bool& safeOut)
 {
+    // Modes 0/1 and 2/3 run as packed pairs (hw_expf2, f32x2 arithmetic:
+    // each component rounds exactly as the scalar operation), mode 4 alone.
+    // Subtractions are additions of the exactly negated operand, and
+    // pref - ((0.5 y) y) vinv is pref + ((-0.5 y) y) vinv: the same bits.
     const int z = h.z;
     const float halfLog2pi = mul_rn(0.5f, k.logTwoPi);
     float pref[5];
@@ -366,9 +370,6 @@ __device__ __forceinline__ float EmEStep(const KParams& k, const EmHist& h, cons
         varinv[i] = 1.0f / v.var[i];
         pref[i] = (hw_logf(v.rho[i]) - mul_rn(0.5f, hw_logf(v.var[i]))) - halfLog2pi;
     }
-    float probSum = 0.0f, wps = 0.0f;
-#pragma unroll
-    for (int i = 0; i < 5; ++i) { ci[i] = 0.0f; mom1[i] = 0.0f; }
     bool safe = true;
     {
         float pmax = pref[0];
@@ -380,7 +381,16 @@ __device__ __forceinline__ float EmEStep(const KParams& k, const EmHist& h, cons
         }
         safe &= pmax < 80.0f;
     }
-    float tauPrev[5] = {0, 0, 0, 0, 0}, bpPrev = 0.0f, xPrev = 0.0f;
+    const float2 pref01 = f2(pref[0], pref[1]), pref23 = f2(pref[2], pref[3]);
+    const float2 vinv01 = f2(varinv[0], varinv[1]), vinv23 = f2(varinv[2], varinv[3]);
+    const float2 nmu01 = f2(-v.mu[0], -v.mu[1]), nmu23 = f2(-v.mu[2], -v.mu[3]);
+    const float pref4 = pref[4], vinv4 = varinv[4], mu4 = v.mu[4];
+    const float2 nz = f2(k.negZero);
+    float probSum = 0.0f, wps = 0.0f;
+    float2 ci01 = f2(0.0f), ci23 = f2(0.0f), m01 = f2(0.0f), m23 = f2(0.0f);
+    float ci4 = 0.0f, m4 = 0.0f;
+    float2 tp01 = f2(0.0f), tp23 = f2(0.0f);
+    float tp4 = 0.0f, bpPrev = 0.0f, xPrev = 0.0f;
     uint32_t nPrev = 0;
     // bin counts are loaded one boundary ahead of their use
     uint32_t nNext = h.Count(0);
@@ -388,47 +398,51 @@ __device__ __forceinline__ float EmEStep(const KParams& k, const EmHist& h, cons
     {
         // cornerComp(b)
         const float x = h.BinStart(b);
-        float t[5];
-#pragma unroll
-        for (int i = 0; i < 5; ++i)
+        const float2 x2 = f2(x);
+        float2 y = add2(x2, nmu01);
+        const float2 t01 = add2(pref01, mulz2(mul2(mul2(f2(-0.5f), y), y), vinv01, nz));
+        y = add2(x2, nmu23);
+        const float2 t23 = add2(pref23, mulz2(mul2(mul2(f2(-0.5f), y), y), vinv23, nz));
+        float t4;
         {
-            const float y = x - v.mu[i];
-            t[i] = pref[i] - mul_rn(mul_rn(mul_rn(0.5f, y), y), varinv[i]);
+            const float y4 = x - mu4;
+            t4 = pref4 - mul_rn(mul_rn(mul_rn(0.5f, y4), y4), vinv4);
         }
-        float tmax = t[0];
-#pragma unroll
-        for (int i = 1; i < 5; ++i) tmax = fmax_sse(tmax, t[i]);
+        float tmax = t01.x;
+        tmax = fmax_sse(tmax, t01.y);
+        tmax = fmax_sse(tmax, t23.x);
+        tmax = fmax_sse(tmax, t23.y);
+        tmax = fmax_sse(tmax, t4);
         const uint32_t nCur = nNext;
         nNext = (b + 1 < kBins) ? h.Count(b + 1) : 0u;
         const bool needTau = (nPrev != 0u) | (nCur != 0u) | !safe;
         // Far tails: with every t finite and below -106, llb = tmax +
         // log(se) with 1 <= se <= 5 stays below -104.3, where hw_expf
         // returns exactly 0, so bp is 0 without evaluating it.
-        bool allFinite = true;
-#pragma unroll
-        for (int i = 0; i < 5; ++i) allFinite &= isfinite(t[i]);
+        const bool allFinite = isfinite(t01.x) & isfinite(t01.y) & isfinite(t23.x) & isfinite(t23.y) & isfinite(t4);
         const bool tail = !needTau & allFinite & (tmax < -106.0f);
         float bp = 0.0f, llb = 0.0f;
         if (!tail)
         {
-            float se = hw_expf(t[0] - tmax);
-#pragma unroll
-            for (int i = 1; i < 5; ++i) se = add_rn(se, hw_expf(t[i] - tmax));
+            const float2 ntmax = f2(-tmax);
+            const float2 e01 = hw_expf2(add2(t01, ntmax), nz), e23 = hw_expf2(add2(t23, ntmax), nz);
+            float se = add_rn(e01.x, e01.y);
+            se = add_rn(se, e23.x);
+            se = add_rn(se, e23.y);
+            se = add_rn(se, hw_expf(t4 - tmax));
             llb = add_rn(tmax, hw_logf(se));
             bp = hw_expf(llb);
         }
-        float tau[5];
+        float2 tau01 = f2(0.0f), tau23 = f2(0.0f);
+        float tau4 = 0.0f;
         if (needTau)
         {
-#pragma unroll
-            for (int i = 0; i < 5; ++i) tau[i] = hw_expf(t[i] - llb);
+            const float2 nllb = f2(-llb);
+            tau01 = hw_expf2(add2(t01, nllb), nz);
+            tau23 = hw_expf2(add2(t23, nllb), nz);
+            tau4 = hw_expf(t4 - llb);
             bpS[(size_t)b * kLane + z] = bp;
-            tau0S[(size_t)b * kLane + z] = tau[0];
-        }
-        else
-        {
-#pragma unroll
-            for (int i = 0; i < 5; ++i) tau[i] = 0.0f;
+            tau0S[(size_t)b * kLane + z] = tau01.x;
         }
         if (b > 0)
         {
@@ -442,25 +456,33 @@ __device__ __forceinline__ float EmEStep(const KParams& k, const EmHist& h, cons
                 wps = add_rn(wps, mul_rn(njb, hw_logf(bpr)));
                 const float factor = njb / bpr;
                 facS[(size_t)c * kLane + z] = factor;
-#pragma unroll
-                for (int m = 0; m < 5; ++m)
-                {
-                    const float tmp1 = mul_rn(bpPrev, tauPrev[m]);
-                    const float tmp2 = mul_rn(bp, tau[m]);
-                    ci[m] = add_rn(ci[m], mul_rn(add_rn(tmp1, tmp2), factor));
-                    mom1[m] = add_rn(mom1[m], mul_rn(add_rn(mul_rn(tmp1, xPrev), mul_rn(tmp2, x)), factor));
-                }
+                const float2 fac = f2(factor), bpp = f2(bpPrev), bpc = f2(bp), xp = f2(xPrev);
+                float2 tmp1 = mulz2(bpp, tp01, nz), tmp2 = mulz2(bpc, tau01, nz);
+                ci01 = add2(ci01, mulz2(add2(tmp1, tmp2), fac, nz));
+                m01 = add2(m01, mulz2(add2(mulz2(tmp1, xp, nz), mulz2(tmp2, x2, nz)), fac, nz));
+                tmp1 = mulz2(bpp, tp23, nz);
+                tmp2 = mulz2(bpc, tau23, nz);
+                ci23 = add2(ci23, mulz2(add2(tmp1, tmp2), fac, nz));
+                m23 = add2(m23, mulz2(add2(mulz2(tmp1, xp, nz), mulz2(tmp2, x2, nz)), fac, nz));
+                const float s1 = mul_rn(bpPrev, tp4), s2 = mul_rn(bp, tau4);
+                ci4 = add_rn(ci4, mul_rn(add_rn(s1, s2), factor));
+                m4 = add_rn(m4, mul_rn(add_rn(mul_rn(s1, xPrev), mul_rn(s2, x)), factor));
             }
         }
-#pragma unroll
-        for (int i = 0; i < 5; ++i) tauPrev[i] = tau[i];
+        tp01 = tau01;
+        tp23 = tau23;
+        tp4 = tau4;
         bpPrev = bp;
         xPrev = x;
         nPrev = nCur;
     }
-    const float hb = mul_rn(0.5f, h.binSize);
-#pragma unroll
-    for (int m = 0; m < 5; ++m) { ci[m] = mul_rn(ci[m], hb); mom1[m] = mul_rn(mom1[m], hb); }
+    const float2 hb = f2(mul_rn(0.5f, h.binSize));
+    ci01 = mulz2(ci01, hb, nz);
+    ci23 = mulz2(ci23, hb, nz);
+    m01 = mulz2(m01, hb, nz);
+    m23 = mulz2(m23, hb, nz);
+    ci[0] = ci01.x; ci[1] = ci01.y; ci[2] = ci23.x; ci[3] = ci23.y; ci[4] = mul_rn(ci4, hb.x);
+    mom1[0] = m01.x; mom1[1] = m01.y; mom1[2] = m23.x; mom1[3] = m23.y; mom1[4] = mul_rn(m4, hb.x);
     float ll = wps - mul_rn(h.nSum, hw_logf(probSum));
     const float ds = v.s - r.sExpect;
     ll = ll - mul_rn(mul_rn(0.5f, mul_rn(ds, ds)), r.sExpectW);
@@ -580,7 +602,7 @@ __device__ __forceinline__ int ChooseStart(const KParams& k, const EmHist& h, co
 }
 
 template <bool Mapped>
-__global__ void __launch_bounds__(kLane, 12) DmeEstimateKernel(DmeArgs A, KParams k)
+__global__ void __launch_bounds__(kLane, 10) DmeEstimateKernel(DmeArgs A, KParams k)
 {
     LaneMap map = A.map;
     if (!Mapped) map.list = nullptr;      // the single-pool variant compiles without the lane list
@@ -771,6 +793,7 @@ struct DmeFitArgs
     float* loglike;            // [lanes][3][64]
     int lanes, tModel, tEst, mode, maxIter;
     float tol;
+    float* atStop = nullptr;   // [lanes][15][64] or null: parameters at the first converged iteration
 };
 
 // Largest relative distance of the parameters from a target column, with
@@ -846,6 +869,18 @@ __global__ void __launch_bounds__(kLane, 12) DmeEmFitKernel(DmeFitArgs A, KParam
         bool cv = (delta >= 0) & (delta < convTol);
         cv &= (ll >= mLogLike);
         mIter = (cv & !mConverged) ? it : mIter;
+        if (A.atStop && cv && !mConverged)
+        {
+            // the estimate the reference keeps at its first converged iteration
+            float* S = A.atStop + (size_t)l * 15 * kLane;
+#pragma unroll
+            for (int i = 0; i < 5; ++i)
+            {
+                S[i * kLane + z] = v.rho[i];
+                S[(5 + i) * kLane + z] = v.mu[i];
+                S[(10 + i) * kLane + z] = v.var[i];
+            }
+        }
         mLogLike = cv ? ll : mLogLike;
         mConverged |= cv;
         last = ll;
@@ -854,6 +889,12 @@ __global__ void __launch_bounds__(kLane, 12) DmeEmFitKernel(DmeFitArgs A, KParam
         if (stepIter < 0 && EmStep(v, before) <= A.tol) stepIter = it + 1;
     }
     if (T && tolIter < 0 && EmDistance(v, T, z) <= A.tol) tolIter = A.maxIter;
+    if (A.atStop && !mConverged)
+    {
+        float* S = A.atStop + (size_t)l * 15 * kLane;
+#pragma unroll
+        for (int i = 0; i < 15; ++i) S[i * kLane + z] = __int_as_float(0x7fffffff);
+    }
 
     float* P = A.params + (size_t)l * 15 * kLane;
 #pragma unroll
@@ -958,7 +999,8 @@ extern "C" int hw_dme_em_fit(const hw_config* cfg, uint32_t lanes, const hw_lane
                              const hw_baseliner_stats* d_stats, hw_frame_interval hist_fi,
                              hw_frame_interval model_fi, const hw_lane_model* d_models, int start,
                              const float* d_proposal, const float* d_target, float tol, uint32_t max_iter,
-                             float* d_scratch, float* d_params, int32_t* d_iters, float* d_loglike, void* stream)
+                             float* d_scratch, float* d_params, int32_t* d_iters, float* d_loglike,
+                             float* d_params_at_stop, void* stream)
 {
     using namespace hwk;
     if (!cfg || !d_hist || !d_stats || !d_models || !d_scratch || !d_params || !d_iters || !d_loglike)
@@ -978,6 +1020,7 @@ extern "C" int hw_dme_em_fit(const hw_config* cfg, uint32_t lanes, const hw_lane
     DmeFitArgs a{d_hist, d_stats, d_models, d_proposal, d_target, d_scratch, d_params, d_iters, d_loglike,
                  (int)lanes, model_fi.lower + (model_fi.upper - model_fi.lower) / 2,
                  hist_fi.lower + (hist_fi.upper - hist_fi.lower) / 2, start, (int)max_iter, tol};
+    a.atStop = d_params_at_stop;
     DmeEmFitKernel<<<lanes, kLane, 0, reinterpret_cast<cudaStream_t>(stream)>>>(a, k);
     const cudaError_t ce = cudaGetLastError();
     if (ce != cudaSuccess) return SetLastError(HW_ERR_CUDA, cudaGetErrorString(ce));

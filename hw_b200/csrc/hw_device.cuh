@@ -25,6 +25,79 @@ constexpr int kStitch = hwp::kRoiStitchFrames;
 __device__ __forceinline__ float h2f(uint16_t b) { return __half2float(__ushort_as_half(b)); }
 __device__ __forceinline__ uint16_t f2h(float f) { return __half_as_ushort(__float2half_rn(f)); }
 
+// ---- Packed pairs (sm_100 f32x2 arithmetic) --------------------------------
+// add.rn / mul.rn / fma.rn .f32x2 round each component exactly as the scalar
+// .rn instruction does, so a pair of independent scalar chains can be
+// evaluated as one packed chain with identical bits and half the issued
+// floating-point instructions.  One caution, measured: the code generator
+// fuses a packed multiply and a packed add that consumes it into one packed
+// fma (one rounding instead of two) even with the explicit .rn and the
+// build's -fmad=false, which only holds for scalar arithmetic.  A product
+// that feeds an addition is therefore written mulz2(a, b, nz) = fma2(a, b,
+// nz) with nz = (-0, -0) read at run time (KParams::negZero): a * b + (-0)
+// rounds exactly as a * b (also for a zero product), and an fma is not fused
+// with a following add.
+__device__ __forceinline__ float2 f2(float x, float y) { return make_float2(x, y); }
+__device__ __forceinline__ float2 f2(float x) { return make_float2(x, x); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b)
+{
+    float2 r;
+    asm("{\n\t.reg .b64 pa, pb, pr;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+        "add.rn.f32x2 pr, pa, pb;\n\tmov.b64 {%0, %1}, pr;\n\t}"
+        : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b)
+{
+    float2 r;
+    asm("{\n\t.reg .b64 pa, pb, pr;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+        "mul.rn.f32x2 pr, pa, pb;\n\tmov.b64 {%0, %1}, pr;\n\t}"
+        : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c)
+{
+    float2 r;
+    asm("{\n\t.reg .b64 pa, pb, pc, pr;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+        "mov.b64 pc, {%6, %7};\n\tfma.rn.f32x2 pr, pa, pb, pc;\n\tmov.b64 {%0, %1}, pr;\n\t}"
+        : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return r;
+}
+// a * b with the rounding of mul.rn, for products that feed an addition
+// (see above); nz holds (-0, -0) from a run-time value.
+__device__ __forceinline__ float2 mulz2(float2 a, float2 b, float2 nz) { return fma2(a, b, nz); }
+
+// hw_expf (hw_math.h) of both components: the special-case selects and the
+// integer scaling per component, the reduction and the polynomial packed
+// (each multiply there feeds an fma, never a packed add).
+__device__ __forceinline__ float2 hw_expf2(float2 x, float2 nz)
+{
+    const bool nanX = x.x != x.x, hiX = x.x > 88.72283935546875f, loX = x.x < -103.97208404541016f;
+    const bool nanY = x.y != x.y, hiY = x.y > 88.72283935546875f, loY = x.y < -103.97208404541016f;
+    const float2 xc = f2((nanX | hiX | loX) ? 0.0f : x.x, (nanY | hiY | loY) ? 0.0f : x.y);
+    const float2 zf = fma2(xc, f2(1.44269504088896341f), f2(0.5f));
+    const float2 z = f2(floorf(zf.x), floorf(zf.y));
+    float2 r = fma2(z, f2(-0.693359375f), xc);
+    r = fma2(z, f2(2.12194440e-4f), r);
+    float2 p = fma2(f2(1.9875691500e-4f), r, f2(1.3981999507e-3f));
+    p = fma2(p, r, f2(8.3334519073e-3f));
+    p = fma2(p, r, f2(4.1665795894e-2f));
+    p = fma2(p, r, f2(1.6666665459e-1f));
+    p = fma2(p, r, f2(5.0000001201e-1f));
+    const float2 r2 = mul2(r, r);
+    const float2 y = add2(fma2(p, r2, r), f2(1.0f));
+    const int nx = (int)z.x, ny = (int)z.y;
+    const int nx1 = nx >> 1, ny1 = ny >> 1;
+    float2 out = mulz2(mul2(y, f2(pow2i(nx1), pow2i(ny1))), f2(pow2i(nx - nx1), pow2i(ny - ny1)), nz);
+    out.x = loX ? 0.0f : out.x;
+    out.y = loY ? 0.0f : out.y;
+    out.x = hiX ? __int_as_float(0x7f800000) : out.x;
+    out.y = hiY ? __int_as_float(0x7f800000) : out.y;
+    out.x = nanX ? x.x : out.x;
+    out.y = nanY ? x.y : out.y;
+    return out;
+}
+
 // Device error word shared by the kernels of one launch: the first failing
 // check stores its code; the host reads it after the launch.
 struct ErrWord
@@ -57,6 +130,8 @@ struct KParams
     float ampThresh, widthThresh;
     int maxCalls;
     uint8_t analogMap[kAnalogs];
+    // -0.0f, read at run time by the packed products (mulz2)
+    float negZero;
 };
 
 inline void FillParams(const hw_config& cfg, const hwp::Derived& d, KParams* k)
@@ -89,6 +164,7 @@ inline void FillParams(const hw_config& cfg, const hwp::Derived& d, KParams* k)
     k->sqrtHalfPi = d.sqrtHalfPi; k->sqrt2 = d.sqrt2; k->sqrt3 = d.sqrt3;
     k->roiUpper = cfg.roi_upper_threshold; k->roiLower = cfg.roi_lower_threshold;
     k->ampThresh = d.ampThresh; k->widthThresh = d.widthThresh; k->maxCalls = (int)cfg.max_calls_per_zmw;
+    k->negZero = -0.0f;
 }
 
 // ModelSignalCovar, DetectionModelHost.cpp:237-245

@@ -105,74 +105,126 @@ struct ZScorer
     }
 };
 
-// Max over a row: first entry, then the contiguous segment; ties go to the
-// later entry (Recursion, FrameLabelerHost.cpp:214-264).  Instead of the
-// source state the row returns its traceback code already shifted into place:
-// 9-way rows (baseline, pulse-up) code source s as 0 for state 0 and s - 4
-// for states 5..12 in 4 bits; 2-way rows (full, down) code the second source
-// as a single bit, which is just the outcome of the one comparison.
-// With Margin, `gap` receives the row's decision gap: the winning candidate
-// less the best other one (0 on a tie, +inf when only one is finite).
+// Log-likelihoods of the 13 states between Viterbi steps: state 0 alone,
+// states 1..12 in the pairs (1,2) (3,4) (5,6) (7,8) (9,10) (11,12) that the
+// rows add as one f32x2 operation (every row reads its sources pairwise:
+// the 9-way rows (5,6) .. (11,12), the 2-way rows of states r and r + 1 read
+// (r, r + 1) and (r + 4, r + 5) or (r - 8, r - 7) and (r - 4, r - 3)).
+struct StateLL
+{
+    float s0;
+    float2 p[6];
+    __device__ __forceinline__ float Get(int i) const
+    {
+        return i == 0 ? s0 : (((i - 1) & 1) ? p[(i - 1) >> 1].y : p[(i - 1) >> 1].x);
+    }
+    __device__ __forceinline__ void Set(int i, float v)
+    {
+        if (i == 0) s0 = v;
+        else if ((i - 1) & 1) p[(i - 1) >> 1].y = v;
+        else p[(i - 1) >> 1].x = v;
+    }
+};
+
+// Arg-max over a row's candidates in the reference's order (first entry,
+// then the contiguous segment); ties go to the later entry (Recursion,
+// FrameLabelerHost.cpp:214-264).  The candidate values are
+// (score + T[row][src]) + ll[src]: the first addition per candidate, the
+// second pairwise.  Instead of the source state a row returns its traceback
+// code already shifted into place: 9-way rows (baseline, pulse-up) code
+// source s as 0 for state 0 and s - 4 for states 5..12 in 4 bits; 2-way
+// rows (full, down) code the second source as one bit, the outcome of their
+// single comparison.  With Margin, `gap` receives the row's decision gap:
+// the winning candidate less the best other one (0 on a tie, +inf when only
+// one is finite).
+template <bool Margin>
+__device__ __forceinline__ void Pick(float v, uint32_t cv, float& mv, float& sv, uint32_t& c)
+{
+    const bool ge = v >= mv;
+    if constexpr (Margin) sv = ge ? mv : ((v > sv) ? v : sv);
+    mv = ge ? v : mv;
+    c = ge ? cv : c;
+}
+
 template <int R, bool Margin>
-__device__ __forceinline__ float ViterbiRow(const KParams& k, float score, const float* ll, uint32_t& code,
+__device__ __forceinline__ float NineWayRow(const KParams& k, float score, const StateLL& ll, uint32_t& code,
                                             float& gap)
 {
-    constexpr bool nineWay = (R == 0 || (R >= 5 && R <= 8));
-    constexpr int first = nineWay ? 0 : (R <= 4 ? R : R - 8);
-    constexpr int sb = nineWay ? 5 : (R <= 4 ? R + 4 : R - 4);
-    constexpr int se = nineWay ? 13 : sb + 1;
-    constexpr int shift = (R == 0) ? 0 : (R <= 4 ? 20 + R - 1 : (R <= 8 ? 4 + 4 * (R - 5) : 24 + R - 9));
-    float mv = add_rn(add_rn(score, k.trans[R][first]), ll[first]);
+    constexpr int shift = (R == 0) ? 0 : 4 + 4 * (R - 5);
+    float mv = add_rn(add_rn(score, k.trans[R][0]), ll.s0);
     float sv = -__int_as_float(0x7f800000);
     uint32_t c = 0u;
 #pragma unroll
-    for (int p = sb; p < se; ++p)
+    for (int q = 2; q < 6; ++q)
     {
-        const float v = add_rn(add_rn(score, k.trans[R][p]), ll[p]);
-        const bool ge = v >= mv;
-        if constexpr (Margin) sv = ge ? mv : ((v > sv) ? v : sv);
-        mv = ge ? v : mv;
-        c = ge ? ((uint32_t)(nineWay ? p - 4 : 1) << shift) : c;
+        const int p0 = 2 * q + 1;          // sources p0, p0 + 1
+        const float2 v = add2(f2(add_rn(score, k.trans[R][p0]), add_rn(score, k.trans[R][p0 + 1])), ll.p[q]);
+        Pick<Margin>(v.x, (uint32_t)(p0 - 4) << shift, mv, sv, c);
+        Pick<Margin>(v.y, (uint32_t)(p0 - 3) << shift, mv, sv, c);
     }
     code = c;
     if constexpr (Margin) gap = mv - sv;
     return mv;
 }
 
+// Two 2-way rows, R and R + 1, with scores s.x, s.y: their first sources are
+// the pair qa, their second the pair qb.
+template <int R, int qa, int qb, bool Margin>
+__device__ __forceinline__ float2 TwoWayRows(const KParams& k, float2 s, const StateLL& ll, uint32_t& code,
+                                             float& gap0, float& gap1)
+{
+    constexpr int shift = (R <= 4) ? 20 + R - 1 : 24 + R - 9;
+    constexpr int a0 = 2 * qa + 1, b0 = 2 * qb + 1;
+    const float2 first = add2(f2(add_rn(s.x, k.trans[R][a0]), add_rn(s.y, k.trans[R + 1][a0 + 1])), ll.p[qa]);
+    const float2 second = add2(f2(add_rn(s.x, k.trans[R][b0]), add_rn(s.y, k.trans[R + 1][b0 + 1])), ll.p[qb]);
+    const bool gx = second.x >= first.x, gy = second.y >= first.y;
+    if constexpr (Margin)
+    {
+        const float ninf = -__int_as_float(0x7f800000);
+        const float sx = gx ? first.x : ((second.x > ninf) ? second.x : ninf);
+        const float sy = gy ? first.y : ((second.y > ninf) ? second.y : ninf);
+        gap0 = (gx ? second.x : first.x) - sx;
+        gap1 = (gy ? second.y : first.y) - sy;
+    }
+    code = (gx ? 1u << shift : 0u) | (gy ? 2u << shift : 0u);
+    return f2(gx ? second.x : first.x, gy ? second.y : first.y);
+}
+
 // One Viterbi recursion step; returns the packed traceback word.  With
 // Margin, gap[r] receives row r's decision gap.
 template <bool Margin = false>
-__device__ __forceinline__ uint32_t ViterbiStep(const KParams& k, const ZScorer& sc, float data, bool isRoi, float* ll,
-                                                float* gap = nullptr)
+__device__ __forceinline__ uint32_t ViterbiStep(const KParams& k, const ZScorer& sc, float data, bool isRoi,
+                                                StateLL& ll, float* gap = nullptr)
 {
     float sco[9];
     sc.Scores(data, sco);
-    float nl[kStates];
-    uint32_t cd[kStates];
+    uint32_t cd[9];
     float gl[kStates];
-    nl[0] = ViterbiRow<0, Margin>(k, sco[0], ll, cd[0], gl[0]);
-    nl[1] = ViterbiRow<1, Margin>(k, sco[1], ll, cd[1], gl[1]);
-    nl[2] = ViterbiRow<2, Margin>(k, sco[2], ll, cd[2], gl[2]);
-    nl[3] = ViterbiRow<3, Margin>(k, sco[3], ll, cd[3], gl[3]);
-    nl[4] = ViterbiRow<4, Margin>(k, sco[4], ll, cd[4], gl[4]);
-    nl[5] = ViterbiRow<5, Margin>(k, sco[5], ll, cd[5], gl[5]);
-    nl[6] = ViterbiRow<6, Margin>(k, sco[6], ll, cd[6], gl[6]);
-    nl[7] = ViterbiRow<7, Margin>(k, sco[7], ll, cd[7], gl[7]);
-    nl[8] = ViterbiRow<8, Margin>(k, sco[8], ll, cd[8], gl[8]);
-    nl[9] = ViterbiRow<9, Margin>(k, sco[5], ll, cd[9], gl[9]);
-    nl[10] = ViterbiRow<10, Margin>(k, sco[6], ll, cd[10], gl[10]);
-    nl[11] = ViterbiRow<11, Margin>(k, sco[7], ll, cd[11], gl[11]);
-    nl[12] = ViterbiRow<12, Margin>(k, sco[8], ll, cd[12], gl[12]);
-    const float pen = isRoi ? 0.0f : __int_as_float(0x7f800000);
-    ll[0] = nl[0];
-#pragma unroll
-    for (int r = 1; r < kStates; ++r) ll[r] = nl[r] - pen;
+    const float n0 = NineWayRow<0, Margin>(k, sco[0], ll, cd[0], gl[0]);
+    const float n5 = NineWayRow<5, Margin>(k, sco[5], ll, cd[1], gl[5]);
+    const float n6 = NineWayRow<6, Margin>(k, sco[6], ll, cd[2], gl[6]);
+    const float n7 = NineWayRow<7, Margin>(k, sco[7], ll, cd[3], gl[7]);
+    const float n8 = NineWayRow<8, Margin>(k, sco[8], ll, cd[4], gl[8]);
+    // full rows: (r, r + 4); down rows: (r - 8, r - 4)
+    const float2 n12 = TwoWayRows<1, 0, 2, Margin>(k, f2(sco[1], sco[2]), ll, cd[5], gl[1], gl[2]);
+    const float2 n34 = TwoWayRows<3, 1, 3, Margin>(k, f2(sco[3], sco[4]), ll, cd[6], gl[3], gl[4]);
+    const float2 n9a = TwoWayRows<9, 0, 2, Margin>(k, f2(sco[5], sco[6]), ll, cd[7], gl[9], gl[10]);
+    const float2 nbc = TwoWayRows<11, 1, 3, Margin>(k, f2(sco[7], sco[8]), ll, cd[8], gl[11], gl[12]);
+    // non-ROI frames: every state but the baseline gets -inf (x - inf)
+    const float2 npen = f2(isRoi ? -0.0f : -__int_as_float(0x7f800000));
+    ll.s0 = n0;
+    ll.p[0] = add2(n12, npen);
+    ll.p[1] = add2(n34, npen);
+    ll.p[2] = add2(f2(n5, n6), npen);
+    ll.p[3] = add2(f2(n7, n8), npen);
+    ll.p[4] = add2(n9a, npen);
+    ll.p[5] = add2(nbc, npen);
     if constexpr (Margin)
     {
 #pragma unroll
         for (int r = 0; r < kStates; ++r) gap[r] = gl[r];
     }
-    return ((cd[0] | cd[1] | cd[2]) | (cd[3] | cd[4] | cd[5])) | ((cd[6] | cd[7] | cd[8]) | (cd[9] | cd[10] | cd[11])) | cd[12];
+    return ((cd[0] | cd[1] | cd[2]) | (cd[3] | cd[4])) | ((cd[5] | cd[6]) | (cd[7] | cd[8]));
 }
 
 // Source state of `state` recorded in traceback word `w`.
@@ -291,11 +343,11 @@ __global__ void __launch_bounds__(Threads, LabelerMinBlocks(Threads)) LabelerKer
     auto roiBit = [&](int f) -> bool { return (roiw(f >> 4) >> (2 * (f & 15))) & 1u; };
 
     // ---- Viterbi (LabelBlock, FrameLabelerHost.cpp:314-448)
-    float ll[kStates];
+    StateLL ll;
     {
         const int bc = A.latLabel[g];
 #pragma unroll
-        for (int i = 0; i < kStates; ++i) ll[i] = (bc == i) ? 0.0f : -__int_as_float(0x7f800000);
+        for (int i = 0; i < kStates; ++i) ll.Set(i, (bc == i) ? 0.0f : -__int_as_float(0x7f800000));
     }
     uint32_t* tb = A.tb + map.BlockX(l, F, kLookback) + z;
     // decision gap of state r at frame lf
@@ -342,7 +394,7 @@ __global__ void __launch_bounds__(Threads, LabelerMinBlocks(Threads)) LabelerKer
         if (f == anchor)
         {
 #pragma unroll
-            for (int i = 0; i < kStates; ++i) anchorLL[i] = ll[i];
+            for (int i = 0; i < kStates; ++i) anchorLL[i] = ll.Get(i);
         }
         const int lf = f + kLatent;
         if ((lf & 15) == 0) roiWord = roiw(lf >> 4);
@@ -353,12 +405,12 @@ __global__ void __launch_bounds__(Threads, LabelerMinBlocks(Threads)) LabelerKer
     // Normalize (FrameLabelerHost.cpp:186-205) and back-propagation.
     float prob[kStates];
     {
-        float mx = ll[0];
+        float mx = ll.Get(0);
 #pragma unroll
-        for (int i = 1; i < kStates; ++i) mx = fmax_sse(ll[i], mx);
+        for (int i = 1; i < kStates; ++i) mx = fmax_sse(ll.Get(i), mx);
         float sum = 0.0f;
 #pragma unroll
-        for (int i = 0; i < kStates; ++i) { prob[i] = hw_expf(ll[i] - mx); sum = add_rn(sum, prob[i]); }
+        for (int i = 0; i < kStates; ++i) { prob[i] = hw_expf(ll.Get(i) - mx); sum = add_rn(sum, prob[i]); }
         const float inv = 1.0f / sum;
 #pragma unroll
         for (int i = 0; i < kStates; ++i) prob[i] = mul_rn(prob[i], inv);

@@ -162,12 +162,14 @@ class DmeEmEstimator(_Handle):
 
 
 def em_fit(cfg, lanes, hist, stats, hist_fi, model_fi, models, start=0, proposal=None, target=None, tol=1e-4,
-           max_iter=20, scratch=None):
+           max_iter=20, scratch=None, at_stop=False):
     """Single-ZMW EM fit (hw_dme_em_fit) on device buffers; returns
     (params [lanes][15][64] float32, iters [lanes][5][64] int32,
-    loglike [lanes][3][64] float32) as CUDA tensors."""
+    loglike [lanes][3][64] float32) as CUDA tensors, and with at_stop=True
+    also the parameters at the first converged iteration [lanes][15][64]."""
     dev = "cuda"
     params = torch.empty((lanes, 15, abi.LANE), dtype=torch.float32, device=dev)
+    stop = torch.empty((lanes, 15, abi.LANE), dtype=torch.float32, device=dev) if at_stop else None
     iters = torch.empty((lanes, 5, abi.LANE), dtype=torch.int32, device=dev)
     ll = torch.empty((lanes, 3, abi.LANE), dtype=torch.float32, device=dev)
     if scratch is None:
@@ -176,8 +178,9 @@ def em_fit(cfg, lanes, hist, stats, hist_fi, model_fi, models, start=0, proposal
         scratch = torch.empty(nbytes.value // 4, dtype=torch.float32, device=dev)
     check(lib().hw_dme_em_fit(C.byref(cfg), lanes, _p(hist), _p(stats), abi.FrameInterval(*hist_fi),
                               abi.FrameInterval(*model_fi), _p(models), int(start), _p(proposal), _p(target),
-                              float(tol), int(max_iter), _p(scratch), _p(params), _p(iters), _p(ll), _stream()))
-    return params, iters, ll
+                              float(tol), int(max_iter), _p(scratch), _p(params), _p(iters), _p(ll), _p(stop),
+                              _stream()))
+    return (params, iters, ll, stop) if at_stop else (params, iters, ll)
 
 
 class FrameLabeler(_Handle):

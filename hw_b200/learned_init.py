@@ -104,11 +104,12 @@ def estimate_inputs(cfg, lanes, pool_id=0, seed=None, frames_per_chunk=512, work
     raise RuntimeError("estimate never became due")
 
 
-def fit(pool, start=0, proposal=None, target=None, tol=1e-4, max_iter=1000):
+def fit(pool, start=0, proposal=None, target=None, tol=1e-4, max_iter=1000, at_stop=False):
     """hw_dme_em_fit on a Pool: (params [lanes][15][64], iters [lanes][5][64],
-    loglike [lanes][3][64]) CUDA tensors."""
+    loglike [lanes][3][64]) CUDA tensors, and with at_stop=True the
+    parameters at the first iteration that passes the reference's test."""
     return Fl.em_fit(pool.cfg, pool.lanes, pool.hist, pool.stats, pool.hist_fi, pool.model_fi, pool.models,
-                     start=start, proposal=proposal, target=target, tol=tol, max_iter=max_iter)
+                     start=start, proposal=proposal, target=target, tol=tol, max_iter=max_iter, at_stop=at_stop)
 
 
 def features(pool):
@@ -258,12 +259,23 @@ def evaluate(net, pools, fixed, fit_iters, tol=1e-4, settle=100):
     least `settle` iterations before the end of the budget."""
     plain_it, learned_it, fell, final_ok, conv_plain, conv_learned, resolved_all = [], [], [], [], [], [], []
     step_plain, step_learned = [], []
+    both_conv, stop_agree, stop_plain_fixed, stop_learned_fixed = [], [], [], []
     for p, tgt in zip(pools, fixed):
-        _, ip, _ = fit(p, start=0, target=tgt, tol=tol, max_iter=fit_iters)
+        _, ip, _, sp = fit(p, start=0, target=tgt, tol=tol, max_iter=fit_iters, at_stop=True)
         out = net.forward(features(p))
         prop = net.proposal(p, out)
-        pl, il, _ = fit(p, start=abi.EM_START_BETTER, proposal=prop, target=tgt, tol=tol, max_iter=fit_iters)
+        pl, il, _, sl = fit(p, start=abi.EM_START_BETTER, proposal=prop, target=tgt, tol=tol, max_iter=fit_iters,
+                            at_stop=True)
         ip, il = ip.cpu().numpy(), il.cpu().numpy()
+        # the reference's stopping rule: iterations to it from either start,
+        # and how close the estimates kept there are to each other and to
+        # the plain fixed point
+        sp, sl, tg = sp.cpu().numpy(), sl.cpu().numpy(), tgt.cpu().numpy()
+        both = (ip[:, 0] >= 0) & (il[:, 0] >= 0)
+        both_conv.append(both.ravel())
+        stop_agree.append((param_distance(sl, sp) <= tol)[both])
+        stop_plain_fixed.append((param_distance(sp, tg) <= tol)[both])
+        stop_learned_fixed.append((param_distance(sl, tg) <= tol)[both])
         res = (ip[:, 1] >= 0) & (ip[:, 1] <= fit_iters - settle)
         resolved_all.append(res.ravel())
         plain_it.append(ip[:, 1][res])
@@ -290,6 +302,21 @@ def evaluate(net, pools, fixed, fit_iters, tol=1e-4, settle=100):
         "reference_criterion_iters_learned_mean": float(cat(conv_learned).mean()),
         "step_criterion_iters_plain_mean": float(cat(step_plain).mean()),
         "step_criterion_iters_learned_mean": float(cat(step_learned).mean()),
+        # both north-star figures on one criterion at a time
+        "criteria": {
+            "reference_stopping_rule": {
+                "iters_ratio": float(cat(conv_plain).mean() / max(cat(conv_learned).mean(), 1e-9)),
+                "within_tol_of_plain_fraction": float(cat(stop_agree).mean()),
+                "plain_stop_within_tol_of_fixed_point": float(cat(stop_plain_fixed).mean()),
+                "learned_stop_within_tol_of_fixed_point": float(cat(stop_learned_fixed).mean()),
+                "zmws_both_converged_fraction": float(cat(both_conv).mean()),
+            },
+            "distance_to_plain_fixed_point": {
+                "iters_ratio": float(pi.mean() / max(li.mean(), 1e-9)),
+                "within_tol_of_plain_fraction": float(cat(final_ok).mean()),
+                "resolved_fraction": float(cat(resolved_all).mean()),
+            },
+        },
     }
 
 

@@ -112,7 +112,7 @@ def lib():
         "hw_analyzer_state_export": ([vp, vp, C.c_uint64, vp], C.c_int),
         "hw_analyzer_state_import": ([vp, vp, C.c_uint64, vp], C.c_int),
         "hw_dme_em_fit_scratch_bytes": ([u32, C.POINTER(C.c_uint64)], C.c_int),
-        "hw_dme_em_fit": ([PCFG, u32, vp, vp, FI, FI, vp, C.c_int, vp, vp, C.c_float, u32, vp, vp, vp, vp, vp],
+        "hw_dme_em_fit": ([PCFG, u32, vp, vp, FI, FI, vp, C.c_int, vp, vp, C.c_float, u32, vp, vp, vp, vp, vp, vp],
                           C.c_int),
         "hw_learned_init_create": ([u32, C.c_uint64, PPV], C.c_int),
         "hw_learned_init_destroy": ([vp], C.c_int),

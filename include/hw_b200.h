@@ -400,7 +400,10 @@ int hw_dme_estimate_noalloc(const hw_config* cfg, uint32_t lanes, const hw_lane_
  * iterations after which one update first changed the parameters by at most
  * `tol` (same relative measure; -1 if never); d_loglike [3][64] = log-
  * likelihood of the plain start, of the start used, and of the last
- * iteration.  d_target may be NULL.  d_scratch holds
+ * iteration.  d_params_at_stop [15][64] (may be NULL) receives the
+ * parameters at the first iteration that passes the reference's convergence
+ * test, the estimate the reference keeps when it stops there (NaN where no
+ * iteration passes).  d_target may be NULL.  d_scratch holds
  * hw_dme_em_fit_scratch_bytes(lanes) bytes.  Asynchronous. */
 typedef enum hw_em_start {
     HW_EM_START_PLAIN = 0,
@@ -412,7 +415,7 @@ int hw_dme_em_fit(const hw_config* cfg, uint32_t lanes, const hw_lane_histogram*
                   const hw_baseliner_stats* d_stats, hw_frame_interval hist_fi, hw_frame_interval model_fi,
                   const hw_lane_model* d_models, int start, const float* d_proposal, const float* d_target,
                   float tol, uint32_t max_iter, float* d_scratch, float* d_params, int32_t* d_iters,
-                  float* d_loglike, void* stream);
+                  float* d_loglike, float* d_params_at_stop, void* stream);
 
 /* ---- Learned DME initializer (no counterpart in the reference) ----------
  * A 302 -> 256 -> 256 -> 19 MLP with BF16 weights and activations, FP32

@@ -847,7 +847,8 @@ struct OraclePool
 
     int EmFit(const hw_lane_histogram* hh, const hw_baseliner_stats* stats, hw_frame_interval hfi,
               hw_frame_interval pfi, const hw_lane_model* models, int mode, const float* proposal,
-              const float* target, float tol, uint32_t maxIter, float* params, int32_t* iters, float* loglike);
+              const float* target, float tol, uint32_t maxIter, float* params, int32_t* iters, float* loglike,
+              float* atStop);
 
     int Label(const int16_t* traces, const hw_lane_model* models, int16_t* labels, int16_t* latOut, float* score,
               float* margin);
@@ -1438,7 +1439,7 @@ static float EmDistance(const float rho[5][kLane], const float mu[5][kLane], con
 int OraclePool::EmFit(const hw_lane_histogram* hh, const hw_baseliner_stats* stats, hw_frame_interval hfi,
                       hw_frame_interval pfi, const hw_lane_model* models, int mode, const float* proposal,
                       const float* target, float tol, uint32_t maxIter, float* params, int32_t* iters,
-                      float* loglike)
+                      float* loglike, float* atStop)
 {
     if (mode < 0 || mode > 2 || (mode != 0 && !proposal))
     { g_err = "EmFit: bad start mode or missing proposal"; return HW_ERR_INVALID_ARG; }
@@ -1496,6 +1497,16 @@ int OraclePool::EmFit(const hw_lane_histogram* hh, const hw_baseliner_stats* sta
                     bool cv = (delta >= 0) & (delta < convTol);
                     cv &= (ll[z] >= mLogLike[z]);
                     mIter[z] = (cv & !mConverged[z]) ? (int32_t)it : mIter[z];
+                    if (atStop && cv && !mConverged[z])
+                    {
+                        float* S = atStop + (size_t)l * 15 * kLane;
+                        for (int k = 0; k < 5; ++k)
+                        {
+                            S[k * kLane + z] = em.rho[k][z];
+                            S[(5 + k) * kLane + z] = em.mu[k][z];
+                            S[(10 + k) * kLane + z] = em.var[k][z];
+                        }
+                    }
                     mLogLike[z] = cv ? ll[z] : mLogLike[z];
                     mConverged[z] |= cv;
                     last[z] = ll[z];
@@ -1519,6 +1530,9 @@ int OraclePool::EmFit(const hw_lane_histogram* hh, const hw_baseliner_stats* sta
             }
             if (T)
                 FZ if (tolIter[z] < 0 && EmDistance(em.rho, em.mu, em.var, T, z) <= tol) tolIter[z] = (int32_t)maxIter;
+            if (atStop)
+                FZ if (!mConverged[z])
+                    for (int k = 0; k < 15; ++k) atStop[(size_t)l * 15 * kLane + k * kLane + z] = std::nanf("");
             FZ
             {
                 for (int k = 0; k < 5; ++k)
@@ -1973,10 +1987,10 @@ int or_dme_estimate_proposal(void* p, const hw_lane_histogram* h, const hw_basel
 
 int or_em_fit(void* p, const hw_lane_histogram* h, const hw_baseliner_stats* s, hw_frame_interval hfi,
               hw_frame_interval mfi, const hw_lane_model* m, int mode, const float* proposal, const float* target,
-              float tol, uint32_t maxIter, float* params, int32_t* iters, float* loglike)
+              float tol, uint32_t maxIter, float* params, int32_t* iters, float* loglike, float* atStop)
 {
     return static_cast<OraclePool*>(p)->EmFit(h, s, hfi, mfi, m, mode, proposal, target, tol, maxIter, params,
-                                              iters, loglike);
+                                              iters, loglike, atStop);
 }
 
 // The fixed detection model of FixedModelBatchAnalyzer, one lane.

@@ -52,7 +52,7 @@ def lib():
         L.or_label.argtypes = [vp, vp, vp, vp, vp, vp, vp]
         L.or_pulses.argtypes = [vp, vp, vp, vp, i32, vp, vp, vp, vp, vp]
         L.or_dme_estimate_proposal.argtypes = [vp, vp, vp, FI, FI, vp, vp, vp]
-        L.or_em_fit.argtypes = [vp, vp, vp, FI, FI, vp, C.c_int, vp, vp, C.c_float, u32, vp, vp, vp]
+        L.or_em_fit.argtypes = [vp, vp, vp, FI, FI, vp, C.c_int, vp, vp, C.c_float, u32, vp, vp, vp, vp]
         L.or_static_model.argtypes = [C.POINTER(abi.Config), vp]
         L.or_extremum_stage.argtypes = [C.c_int, C.c_int, vp, C.c_int, C.c_int, vp]
         L.or_expf.argtypes = [C.c_float]
@@ -263,9 +263,11 @@ class Pool:
         return models, diag
 
     def em_fit(self, hist, stats, hist_fi, model_fi, models, mode=0, proposal=None, target=None, tol=1e-4,
-               max_iter=20):
+               max_iter=20, at_stop=False):
         """Single-ZMW EM fit (see hw_dme_em_fit): returns params [lanes][15][64],
-        iters [lanes][5][64] and log-likelihoods [lanes][3][64]."""
+        iters [lanes][5][64] and log-likelihoods [lanes][3][64], and with
+        at_stop=True the parameters at the first converged iteration."""
+        stop = np.zeros((self.lanes, 15, abi.LANE), np.float32) if at_stop else None
         params = np.zeros((self.lanes, 15, abi.LANE), np.float32)
         iters = np.zeros((self.lanes, 5, abi.LANE), np.int32)
         ll = np.zeros((self.lanes, 3, abi.LANE), np.float32)
@@ -273,8 +275,9 @@ class Pool:
         tgt = None if target is None else np.ascontiguousarray(target, np.float32)
         _check(lib().or_em_fit(self.h, abi.ptr(hist), abi.ptr(stats), abi.FrameInterval(*hist_fi),
                                abi.FrameInterval(*model_fi), abi.ptr(models), int(mode), abi.ptr(prop), abi.ptr(tgt),
-                               float(tol), int(max_iter), abi.ptr(params), abi.ptr(iters), abi.ptr(ll)))
-        return params, iters, ll
+                               float(tol), int(max_iter), abi.ptr(params), abi.ptr(iters), abi.ptr(ll),
+                               abi.ptr(stop)))
+        return (params, iters, ll, stop) if at_stop else (params, iters, ll)
 
     def label(self, traces, models, margin=False):
         """FrameLabeler: labels, latent trace, Viterbi score (and, with

@@ -97,15 +97,21 @@ def test_cuda_fit_matches_oracle(mode):
     prop[:, 0:5] = np.abs(prop[:, 0:5]) / np.abs(prop[:, 0:5]).sum(1, keepdims=True)
     prop[:, 10:15] = np.abs(prop[:, 10:15])
     args = dict(target=ref, tol=1e-3, max_iter=25)
-    po, io, lo = be.p.em_fit(hist, stats, hfi, mfi, models, mode=mode, proposal=None if mode == 0 else prop, **args)
+    po, io, lo, so = be.p.em_fit(hist, stats, hfi, mfi, models, mode=mode, proposal=None if mode == 0 else prop,
+                                 at_stop=True, **args)
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
-    pg, ig, lg = Fl.em_fit(cfg, lanes, Fl.numpy_to_struct(hist), Fl.numpy_to_struct(stats), hfi, mfi,
-                           Fl.numpy_to_struct(models), start=mode, proposal=None if mode == 0 else t(prop),
-                           target=t(ref), tol=1e-3, max_iter=25)
+    pg, ig, lg, sg = Fl.em_fit(cfg, lanes, Fl.numpy_to_struct(hist), Fl.numpy_to_struct(stats), hfi, mfi,
+                               Fl.numpy_to_struct(models), start=mode, proposal=None if mode == 0 else t(prop),
+                               target=t(ref), tol=1e-3, max_iter=25, at_stop=True)
     torch.cuda.synchronize()
     assert np.array_equal(po.view(np.uint32), pg.cpu().numpy().view(np.uint32))
     assert np.array_equal(io, ig.cpu().numpy())
     assert np.array_equal(lo.view(np.uint32), lg.cpu().numpy().view(np.uint32))
+    sg = sg.cpu().numpy()
+    assert np.array_equal(np.isnan(so), np.isnan(sg))
+    assert np.array_equal(so[~np.isnan(so)].view(np.uint32), sg[~np.isnan(sg)].view(np.uint32))
+    # NaN exactly where no iteration passed the reference's test
+    assert np.array_equal(np.isnan(so).all(1), io[:, 0] < 0)
 
 
 @pytest.mark.gpu
