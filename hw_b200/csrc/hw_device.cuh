@@ -126,6 +126,7 @@ struct KParams
     // labeler
     float trans[kStates][kStates];
     float sqrtHalfPi, sqrt2, sqrt3, roiUpper, roiLower;
+    float rcpSqrt2, rcpSqrt3;    // RN(1 / sqrt2), RN(1 / sqrt3)
     // pulses
     float ampThresh, widthThresh;
     int maxCalls;
@@ -162,6 +163,7 @@ inline void FillParams(const hw_config& cfg, const hwp::Derived& d, KParams* k)
     for (int r = 0; r < kStates; ++r)
         for (int c = 0; c < kStates; ++c) k->trans[r][c] = d.trans[r][c];
     k->sqrtHalfPi = d.sqrtHalfPi; k->sqrt2 = d.sqrt2; k->sqrt3 = d.sqrt3;
+    k->rcpSqrt2 = 1.0f / d.sqrt2; k->rcpSqrt3 = 1.0f / d.sqrt3;
     k->roiUpper = cfg.roi_upper_threshold; k->roiLower = cfg.roi_lower_threshold;
     k->ampThresh = d.ampThresh; k->widthThresh = d.widthThresh; k->maxCalls = (int)cfg.max_calls_per_zmw;
     k->negZero = -0.0f;

@@ -21,12 +21,18 @@
 
 namespace hwk {
 
-// BlockStateSubframeScorer for one ZMW (SubframeScorer.h:152-318).
+// BlockStateSubframeScorer for one ZMW (SubframeScorer.h:152-318).  The
+// scores of analogs 0/1 and 2/3 are evaluated as packed pairs with the
+// reference's operation order (see the f32x2 helpers); constants the
+// reference recomputes per frame from per-ZMW values (-0.5 times the inverse
+// variances, the negated caps, means and log means, the dimmest analog's
+// fallback condition) are formed once in Setup, with the same roundings.
 struct ZScorer
 {
-    float bgMean, bInvVar, bgFixed, x0;
-    float ffMean[4], pInvVar[4], ffFixed[4], logPMean[4], x1[4];
+    float bgMean, bInvVar, bgFixed, x0, nhBInv;
+    float2 negMean[2], pInv[2], ffFixed[2], nhPInv[2], negX1[2], negLogP[2], x1[2];
     float fbMean, fbNormTerm, fbScale;
+    bool fbUse;     // x0 > x1 of the dimmest analog: its up/down score is the normal fallback
 
     __device__ __forceinline__ void Setup(const KParams& k, const hw_lane_model& m, int z)
     {
@@ -37,20 +43,34 @@ struct ZScorer
         const float bSigma = sqrtf(bVar);
         x0 = add_rn(bMean, mul_rn(bSigma, k.sqrtHalfPi));
         bInvVar = 1.0f / bVar;
+        nhBInv = mul_rn(nhalf, bInvVar);
+        float aM[kAnalogs], pI[kAnalogs], fx[kAnalogs], lp[kAnalogs], xx[kAnalogs];
 #pragma unroll
         for (int a = 0; a < kAnalogs; ++a)
         {
             const float aMean = h2f(m.analogs[a].means[z]);
-            logPMean[a] = hw_logf(aMean - bMean);
+            lp[a] = hw_logf(aMean - bMean);
             const float aVar = h2f(m.analogs[a].vars[z]);
             const float aSigma = sqrtf(aVar);
-            x1[a] = aMean - mul_rn(aSigma, k.sqrtHalfPi);
-            pInvVar[a] = 1.0f / aVar;
-            ffFixed[a] = mul_rn(nhalf, hw_logf(aVar)) - log2pi_f / 2.0f;
-            ffMean[a] = aMean;
+            xx[a] = aMean - mul_rn(aSigma, k.sqrtHalfPi);
+            pI[a] = 1.0f / aVar;
+            fx[a] = mul_rn(nhalf, hw_logf(aVar)) - log2pi_f / 2.0f;
+            aM[a] = aMean;
+        }
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+        {
+            const int a = 2 * q;
+            negMean[q] = f2(-aM[a], -aM[a + 1]);
+            pInv[q] = f2(pI[a], pI[a + 1]);
+            ffFixed[q] = f2(fx[a], fx[a + 1]);
+            nhPInv[q] = f2(mul_rn(nhalf, pI[a]), mul_rn(nhalf, pI[a + 1]));
+            negX1[q] = f2(-xx[a], -xx[a + 1]);
+            x1[q] = f2(xx[a], xx[a + 1]);
+            negLogP[q] = f2(-lp[a], -lp[a + 1]);
         }
         {
-            const float aMean = ffMean[3];
+            const float aMean = aM[3];
             const float aVar = h2f(m.analogs[3].vars[z]);
             const float eMean = mul_rn(halfVal, bMean + aMean);
             float eVar = mul_rn(oneSixth, aMean - bMean);
@@ -60,47 +80,46 @@ struct ZScorer
             fbNormTerm = mul_rn(-0.5f, add_rn(log2pi_f, hw_logf(eVar)));
             fbScale = 0.5f / eVar;
         }
+        fbUse = !(x0 <= xx[3]);
         bgFixed = mul_rn(nhalf, hw_logf(bVar)) - log2pi_f / 2.0f;
         bgMean = bMean;
     }
 
-    __device__ __forceinline__ float Subframe(int a, float val) const
-    {
-        const bool lowExtrema = val < x0;
-        const float cap = lowExtrema ? x0 : x1[a];
-        float fixedTerm = lowExtrema ? bInvVar : pInvVar[a];
-        fixedTerm = mul_rn(-0.5f, fixedTerm);
-        const bool extrema = lowExtrema | (val > x1[a]);
-        const float dv = val - cap;
-        float s = (extrema ? mul_rn(fixedTerm, mul_rn(dv, dv)) : 0.0f) - logPMean[a];
-        if (a == kAnalogs - 1)
-        {
-            const float dm = val - fbMean;
-            const float fb = fbNormTerm - mul_rn(mul_rn(dm, dm), fbScale);
-            s = (x0 <= x1[a]) ? s : fb;
-        }
-        return s;
-    }
-
     // StateScores for states 0..8 (states 9..12 repeat 5..8).
-    __device__ __forceinline__ void Scores(float data, float* out) const
+    __device__ __forceinline__ void Scores(float data, float* out, float2 nz) const
     {
         {
             const float y = data - bgMean;
             out[0] = add_rn(mul_rn(mul_rn(mul_rn(-0.5f, y), bInvVar), y), bgFixed);
         }
+        const float2 d2 = f2(data);
+        const bool low = data < x0;
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int q = 0; q < 2; ++q)
         {
-            const float y = data - ffMean[i];
-            out[1 + i] = add_rn(mul_rn(mul_rn(mul_rn(-0.5f, y), pInvVar[i]), y), ffFixed[i]);
-        }
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-        {
-            float score = Subframe(i, data);
-            score = (data > ffMean[i]) ? fmin_sse(fmin_sse(score, out[1 + i] - 1.0f), 0.0f) : score;
-            out[5 + i] = score;
+            // full frame: ((-0.5 y) / var) y + fixed, y = data - mean
+            const float2 y = add2(d2, negMean[q]);
+            const float2 full = add2(mulz2(mul2(mul2(f2(-0.5f), y), pInv[q]), y, nz), ffFixed[q]);
+            // sub-frame Gauss cap: (extrema ? (-0.5 / var) dv^2 : 0) - log(mean - baseline mean)
+            const float2 negCap = low ? f2(-x0) : negX1[q];
+            const float2 fixedTerm = low ? f2(nhBInv) : nhPInv[q];
+            const float2 dv = add2(d2, negCap);
+            const float2 prod = mulz2(fixedTerm, mul2(dv, dv), nz);
+            const bool ex = low | (data > x1[q].x), ey = low | (data > x1[q].y);
+            float2 sub = add2(f2(ex ? prod.x : 0.0f, ey ? prod.y : 0.0f), negLogP[q]);
+            if (q == 1 && fbUse)
+            {
+                const float dm = data - fbMean;
+                sub.y = fbNormTerm - mul_rn(mul_rn(dm, dm), fbScale);
+            }
+            // clamp above the full-frame mean
+            const float2 fm1 = add2(full, f2(-1.0f));
+            sub.x = (data > -negMean[q].x) ? fmin_sse(fmin_sse(sub.x, fm1.x), 0.0f) : sub.x;
+            sub.y = (data > -negMean[q].y) ? fmin_sse(fmin_sse(sub.y, fm1.y), 0.0f) : sub.y;
+            out[1 + 2 * q] = full.x;
+            out[2 + 2 * q] = full.y;
+            out[5 + 2 * q] = sub.x;
+            out[6 + 2 * q] = sub.y;
         }
     }
 };
@@ -197,7 +216,7 @@ __device__ __forceinline__ uint32_t ViterbiStep(const KParams& k, const ZScorer&
                                                 StateLL& ll, float* gap = nullptr)
 {
     float sco[9];
-    sc.Scores(data, sco);
+    sc.Scores(data, sco, f2(k.negZero));
     uint32_t cd[9];
     float gl[kStates];
     const float n0 = NineWayRow<0, Margin>(k, sco[0], ll, cd[0], gl[0]);
@@ -245,6 +264,22 @@ __device__ __forceinline__ int TraceSource(uint32_t w, int state)
     return b ? state - 4 : state - 8;
 }
 
+
+// x / c, correctly rounded, for the ROI's constants c = sqrt(2) and sqrt(3):
+// q = x * RN(1/c) corrected once with the exact remainder x - q c (Markstein's
+// correction); zero and non-finite quotients pass through.  An exhaustive
+// check over every float x gives the IEEE quotient for both constants
+// whenever |x| >= 2^-124 (the quotient is then a normal number), and for
+// zero, infinite and NaN x; only smaller x can differ, and the ROI never
+// divides one (its dividends are 0 or sums of int16 trace values times an
+// inverse sigma of at least 1/256, so their magnitude is 0 or above 2^-33).
+__device__ __forceinline__ float DivByConst(float x, float c, float rcp)
+{
+    const float q = mul_rn(x, rcp);
+    const float r = fma_rn(-q, c, x);
+    const float q2 = fma_rn(r, rcp, q);
+    return (isfinite(q) && q != 0.0f) ? q2 : q;
+}
 
 constexpr int kBatch = 8;                              // frames loaded ahead
 
@@ -298,8 +333,8 @@ __global__ void __launch_bounds__(Threads, LabelerMinBlocks(Threads)) LabelerKer
         int ri = 0;
         auto process = [&](float sn) {
             float mval = p1;
-            mval = fmax_sse(mval, (p0 + p1) / k.sqrt2);
-            mval = fmax_sse(mval, add_rn(p0 + p1, p2) / k.sqrt3);
+            mval = fmax_sse(mval, DivByConst(p0 + p1, k.sqrt2, k.rcpSqrt2));
+            mval = fmax_sse(mval, DivByConst(add_rn(p0 + p1, p2), k.sqrt3, k.rcpSqrt3));
             mval = fmax_sse(mval, add_rn(add_rn(p0 + p1, p2), sn) / 2.0f);
             const float thresh = (prevRoi & 1u) ? k.roiLower : k.roiUpper;
             const uint32_t v = ((mval >= thresh) ? 1u : 0u) | ((mval >= k.roiLower) ? 2u : 0u);
