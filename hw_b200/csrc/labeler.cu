@@ -269,8 +269,8 @@ __device__ __forceinline__ int TraceSource(uint32_t w, int state)
 // q = x * RN(1/c) corrected once with the exact remainder x - q c (Markstein's
 // correction); zero and non-finite quotients pass through.  An exhaustive
 // check over every float x gives the IEEE quotient for both constants
-// whenever |x| >= 2^-124 (the quotient is then a normal number), and for
-// zero, infinite and NaN x; only smaller x can differ, and the ROI never
+// whenever |x| >= 2^-100 (the largest x that differs is below 2^-102), and
+// for zero, infinite and NaN x; only smaller x can differ, and the ROI never
 // divides one (its dividends are 0 or sums of int16 trace values times an
 // inverse sigma of at least 1/256, so their magnitude is 0 or above 2^-33).
 __device__ __forceinline__ float DivByConst(float x, float c, float rcp)
