@@ -130,6 +130,7 @@ struct hw_dme
     uint32_t poolId = 0, lanes = 0;
     float* scratch = nullptr;
     int* err = nullptr;
+    long long* phases = nullptr;     // per-lane phase clock when profiling
 };
 
 struct hw_labeler
@@ -419,7 +420,35 @@ int hw_dme_destroy(hw_dme* d)
     if (!d) return HW_OK;
     cudaFree(d->scratch);
     cudaFree(d->err);
+    cudaFree(d->phases);
     delete d;
+    return HW_OK;
+}
+
+int hw_dme_profile_phases(hw_dme* d, int enable)
+{
+    if (!d) return Fail(HW_ERR_INVALID_ARG, "NULL handle");
+    if (enable && !d->phases)
+    {
+        int rc = DevAlloc(&d->phases, (size_t)d->lanes * 8, "hw_dme_profile_phases");
+        if (rc) return rc;
+        HW_CUDA(cudaMemset(d->phases, 0, (size_t)d->lanes * 8 * sizeof(long long)), "hw_dme_profile_phases");
+    }
+    else if (!enable && d->phases)
+    {
+        cudaFree(d->phases);
+        d->phases = nullptr;
+    }
+    return HW_OK;
+}
+
+int hw_dme_phase_cycles(const hw_dme* d, int64_t* host_out, void* stream)
+{
+    if (!d || !host_out) return Fail(HW_ERR_INVALID_ARG, "NULL argument");
+    if (!d->phases) return Fail(HW_ERR_INVALID_ARG, "hw_dme_phase_cycles: phase profiling is off");
+    HW_CUDA(cudaMemcpyAsync(host_out, d->phases, (size_t)d->lanes * 8 * sizeof(long long), cudaMemcpyDeviceToHost,
+                            S(stream)), "hw_dme_phase_cycles");
+    HW_CUDA(cudaStreamSynchronize(S(stream)), "hw_dme_phase_cycles");
     return HW_OK;
 }
 
@@ -440,6 +469,7 @@ int hw_dme_estimate(hw_dme* d, const hw_lane_histogram* d_hist, const hw_baselin
     DmeArgs a{d_hist, d_stats, d_models, d_diag, d->scratch, d->err, (int)d->lanes,
               model_fi.lower + (model_fi.upper - model_fi.lower) / 2,
               hist_fi.lower + (hist_fi.upper - hist_fi.lower) / 2};
+    a.phases = d->phases;
     HW_CUDA(LaunchDmeEstimate(a, d->k, S(stream)), "hw_dme_estimate");
     int e = TakeDeviceError(d->err, S(stream), "hw_dme_estimate");
     if (e) return Fail(e, "DME: a reference sanity assertion failed (non-finite estimate or bad SNR-drop threshold)");
@@ -456,6 +486,7 @@ int hw_dme_estimate_proposal(hw_dme* d, const hw_lane_histogram* d_hist, const h
     DmeArgs a{d_hist, d_stats, d_models, d_diag, d->scratch, d->err, (int)d->lanes,
               model_fi.lower + (model_fi.upper - model_fi.lower) / 2,
               hist_fi.lower + (hist_fi.upper - hist_fi.lower) / 2, d_proposal};
+    a.phases = d->phases;
     HW_CUDA(LaunchDmeEstimate(a, d->k, S(stream)), "hw_dme_estimate_proposal");
     int e = TakeDeviceError(d->err, S(stream), "hw_dme_estimate_proposal");
     if (e) return Fail(e, "DME: a reference sanity assertion failed (non-finite estimate or bad SNR-drop threshold)");

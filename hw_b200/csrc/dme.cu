@@ -621,17 +621,33 @@ __global__ void __launch_bounds__(kLane, 10) DmeEstimateKernel(DmeArgs A, KParam
     float* tau0S = bpS + (size_t)(kBins + 1) * kLane;
     float* facS = tau0S + (size_t)(kBins + 1) * kLane;
 
+    // phase clock (thread 0, when asked for): see DmeArgs::phases
+    const bool clk = A.phases != nullptr && z == 0;
+    long long tc[5] = {0, 0, 0, 0, 0};
+    long long tMark = clk ? clock64() : 0;
+    const long long tBegin = tMark;
+    auto lap = [&](int phase) {
+        if (clk)
+        {
+            const long long t = clock64();
+            tc[phase] += t - tMark;
+            tMark = t;
+        }
+    };
+
     EmHist h;
     LoadEmHist(A.hist[l], z, h);
     ModelF det;
     EmVars v;
     EmReg r;
     DmePrelude(k, A.models[l], A.stats[l], h, tModel, tEst, det, v, r);
+    lap(0);
     if (A.proposal)
     {
         float llPlain, llStart;
         ChooseStart(k, h, r, A.proposal + (size_t)l * 15 * kLane, true, bpS, tau0S, facS, v, llPlain, llStart);
     }
+    lap(1);
 
     // Values needed only before and after the EM iterations (the prior model
     // and the estimates at the latest converged iteration) wait in per-thread
@@ -678,8 +694,10 @@ __global__ void __launch_bounds__(kLane, 10) DmeEstimateKernel(DmeArgs A, KParam
             for (int i = 0; i < 5; ++i) { rhoEst(i) = v.rho[i]; muEst(i) = v.mu[i]; varEst(i) = v.var[i]; }
         }
         const int allDone = __syncthreads_and(mConverged | (zStatus != 0));
+        lap(2);
         if (!k.iterToLimit && allDone) break;
         EmMStep(k, h, r, safe, bpS, tau0S, facS, ci, mom1, varinv, v, zStatus);
+        lap(3);
     }
     const int laneIters = it + 1 < iterLimit ? it + 1 : iterLimit;
 
@@ -761,6 +779,18 @@ __global__ void __launch_bounds__(kLane, 10) DmeEstimateKernel(DmeArgs A, KParam
         D.confidence[z] = conf;
         if (z == 0) D.lane_iterations = laneIters;
         if (z < 15) D.pad_[z] = 0;
+    }
+    if (clk)
+    {
+        lap(4);
+        long long* P = A.phases + (size_t)li * 8;
+#pragma unroll
+        for (int i = 0; i < 5; ++i) P[i] = tc[i];
+        P[5] = laneIters;
+        P[6] = tMark - tBegin;
+        unsigned smid;
+        asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+        P[7] = smid;
     }
 }
 

@@ -275,6 +275,10 @@ struct DmeArgs
     // lane-list launch: frame-interval centers from map.Pool(lane); scratch
     // indexed by launch lane
     LaneMap map{};
+    // Optional per-lane phase clock [lanes][8] (SM cycles, thread 0 of the
+    // lane): prelude, start choice, E-steps, M-steps, confidence and blend,
+    // lane iterations, whole lane, SM id.
+    long long* phases = nullptr;
 };
 
 struct LabelerArgs

@@ -160,6 +160,16 @@ class DmeEmEstimator(_Handle):
                                              _stream()))
         return d
 
+    def profile_phases(self, enable=True):
+        check(lib().hw_dme_profile_phases(self._h, 1 if enable else 0))
+
+    def phase_cycles(self):
+        """[lanes][8] int64 per-lane phase clock of the last estimate (see
+        hw_dme_profile_phases)."""
+        out = np.zeros((self.lanes, 8), np.int64)
+        check(lib().hw_dme_phase_cycles(self._h, abi.ptr(out), _stream()))
+        return out
+
 
 def em_fit(cfg, lanes, hist, stats, hist_fi, model_fi, models, start=0, proposal=None, target=None, tol=1e-4,
            max_iter=20, scratch=None, at_stop=False):

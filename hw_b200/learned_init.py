@@ -320,6 +320,48 @@ def evaluate(net, pools, fixed, fit_iters, tol=1e-4, settle=100):
     }
 
 
+def dme_phases(net, pool, pool_id=0, sm_mhz=None):
+    """Where the DME's time goes, plain start against the learned start, on
+    one pool's estimate (the product's lane-wide estimate, hw_dme_estimate /
+    hw_dme_estimate_proposal): launch time (CUDA events), the network's own
+    time (features, forward pass, proposal columns), lane EM iterations
+    (mean, max, share of lanes at the iteration limit) and the per-lane phase
+    clock summed over lanes as a share of all lane cycles.  The launch time
+    follows the slowest lanes of each SM's lane waves, not the mean."""
+    cfg, lanes = pool.cfg, pool.lanes
+    names = ["setup", "start_choice", "e_steps", "m_steps", "confidence_blend"]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+
+    def one(use_net):
+        dme = Fl.DmeEmEstimator(cfg, pool_id, lanes)
+        dme.profile_phases(True)
+        models = pool.models.clone()
+        torch.cuda.synchronize()
+        ev[0].record()
+        prop = None
+        if use_net:
+            prop = net.proposal(pool, net.forward(features(pool)))
+        ev[1].record()
+        if use_net:
+            dme.estimate_proposal(pool.hist, pool.hist_fi, pool.stats, models, pool.model_fi, prop, diag=False)
+        else:
+            dme.estimate(pool.hist, pool.hist_fi, pool.stats, models, pool.model_fi, diag=False)
+        ev[2].record()
+        ev[2].synchronize()
+        ph = dme.phase_cycles()
+        dme.close()
+        it = ph[:, 5].astype(np.float64)
+        tot = ph[:, :5].sum()
+        out = {"network_ms": ev[0].elapsed_time(ev[1]), "estimate_ms": ev[1].elapsed_time(ev[2]),
+               "lane_iterations_mean": float(it.mean()), "lane_iterations_max": int(it.max()),
+               "lanes_at_iteration_limit": float((it >= cfg.em_iteration_limit).mean()),
+               "phase_share": {n: float(ph[:, i].sum() / tot) for i, n in enumerate(names)},
+               "lane_cycles_mean": float(ph[:, 6].mean()), "lane_cycles_max": int(ph[:, 6].max())}
+        return out
+
+    return {"lanes": lanes, "plain": one(False), "learned": one(True)}
+
+
 def run(train_pools=8, eval_pools=1, lanes=4096, fit_iters=1000, epochs=40, batch=4096, lr=1e-3, seed=7, log=None):
     """Generate, label, train and evaluate; returns (network, metrics)."""
     cfg = data_config()
@@ -333,6 +375,7 @@ def run(train_pools=8, eval_pools=1, lanes=4096, fit_iters=1000, epochs=40, batc
     held = _pools(cfg, eval_pools, lanes, 1000, seed)
     fixed = [fit(p, start=0, max_iter=fit_iters)[0] for p in held]
     metrics = evaluate(net, held, fixed, fit_iters)
+    metrics["dme_phases"] = dme_phases(net, held[0], pool_id=1000)
     metrics["train_zmws"] = train_pools * lanes * abi.LANE
     metrics["final_train_loss"] = history[-1] if history else None
     return net, metrics

@@ -60,6 +60,8 @@ def lib():
         "hw_dme_init_models": ([vp, vp, vp, vp], C.c_int),
         "hw_dme_estimate": ([vp, vp, vp, FI, FI, vp, vp, vp], C.c_int),
         "hw_dme_estimate_noalloc": ([PCFG, u32, vp, vp, FI, FI, vp, vp, vp], C.c_int),
+        "hw_dme_profile_phases": ([vp, C.c_int], C.c_int),
+        "hw_dme_phase_cycles": ([vp, vp, vp], C.c_int),
         "hw_detection_model_import": ([vp, u32, vp, vp], C.c_int),
         "hw_detection_model_export": ([vp, u32, vp, vp], C.c_int),
         "hw_detection_model_evolve_confidence": ([vp, u32, FI, FI, C.c_float, vp], C.c_int),

@@ -337,6 +337,18 @@ int hw_dme_estimate_proposal(hw_dme* d, const hw_lane_histogram* d_hist, const h
                              hw_frame_interval hist_fi, hw_frame_interval model_fi, hw_lane_model* d_models,
                              hw_dme_diag* d_diag, const float* d_proposal, void* stream);
 
+/* Per-lane phase clock of the next estimates (no counterpart in the
+ * reference): with profiling on, every hw_dme_estimate /
+ * hw_dme_estimate_proposal records for each lane, in SM clock cycles of the
+ * lane's first thread: [0] model evolution, preliminary estimate and EM
+ * set-up, [1] the start choice of a proposal (its two E-steps), [2] the
+ * E-steps with the lane-wide convergence vote, [3] the M-steps, [4] the
+ * confidence, blend and export, [5] the lane's EM iterations, [6] the whole
+ * lane, [7] the SM the lane ran on.  hw_dme_phase_cycles copies the
+ * [lanes][8] int64 table to host memory (synchronous). */
+int hw_dme_profile_phases(hw_dme* d, int enable);
+int hw_dme_phase_cycles(const hw_dme* d, int64_t* host_out, void* stream);
+
 /* DetectionModelHost <-> LaneDetectionModel<PBHalf> (DetectionModelHost.h:
  * constructor from a LaneDetectionModel, ExportTo; DetectionModelHost.cpp:
  * 47-60, 226-234, 277-285) with the estimator's own conversion code: the
