@@ -193,10 +193,23 @@ BAZ_PRODUCTION, BAZ_INTERNAL = 0, 1
 # hw_prelim_hq_config and hw_baz_checkpoint
 PRELIM_HQ_CONFIG_DT = np.dtype([("chunks_per_block", np.uint32), ("lookback_blocks", np.uint32),
                                 ("enable_prehq", np.int32), ("hq_throttle_fraction", np.float32),
-                                ("zmw_stride", np.uint32), ("reserved", np.uint32)])
+                                ("zmw_stride", np.uint32), ("metrics", np.uint32)])
 BAZ_CHECKPOINT_DT = np.dtype([("d_bytes", np.uint64), ("total_bytes", np.uint64), ("d_offsets", np.uint64),
                               ("d_events", np.uint64), ("d_hq", np.uint64), ("num_hq", np.uint32),
                               ("block", np.uint32)])
+
+# hw_spider_metric_block (Primary::SpiderMetricBlock) and hw_metric_checkpoint
+_N4 = (NUM_ANALOGS,)
+SPIDER_METRIC_BLOCK_DT = np.dtype([
+    ("num_frames", np.uint32), ("num_pulses", np.uint32), ("pulse_width", np.uint32), ("base_width", np.uint32),
+    ("num_sandwiches", np.uint32), ("num_half_sandwiches", np.uint32), ("num_pulse_label_stutters", np.uint32),
+    ("pulse_detection_score", np.float32), ("trace_autocorr", np.float32), ("pixel_checksum", np.int16),
+    ("dme_status", np.uint8), ("activity_label", np.uint8), ("pkmid", np.float32, _N4),
+    ("num_pkmid_frames", np.uint32, _N4), ("pkmax", np.float32, _N4), ("num_bases", np.uint32, _N4),
+    ("num_pkmid_bases", np.uint32, _N4), ("bpzvar", np.float32, _N4), ("pkzvar", np.float32, _N4),
+    ("baseline", np.float32), ("baseline_sd", np.float32), ("num_baseline_frames", np.uint32)])
+METRIC_CHECKPOINT_DT = np.dtype([("d_blocks", np.uint64), ("total_blocks", np.uint64), ("d_offsets", np.uint64),
+                                 ("block", np.uint32), ("reserved", np.uint32)])
 
 FUSED_TUNING_DT = np.dtype([("frames_per_chunk", np.uint32), ("fuse_label_pulses", np.uint32),
                             ("labeler_lanes_per_cta", np.uint32), ("reserved", np.uint32)])
@@ -217,6 +230,8 @@ SIZES = {
     "hw_baz_field": (BAZ_FIELD_DT, 32),
     "hw_prelim_hq_config": (PRELIM_HQ_CONFIG_DT, 24),
     "hw_baz_checkpoint": (BAZ_CHECKPOINT_DT, 48),
+    "hw_spider_metric_block": (SPIDER_METRIC_BLOCK_DT, 164),
+    "hw_metric_checkpoint": (METRIC_CHECKPOINT_DT, 32),
 }
 
 

@@ -23,7 +23,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 HOST_CXX = "/usr/bin/g++"
 
 SOURCES = ["baseliner.cu", "stats_hist.cu", "dme.cu", "labeler.cu", "pulses.cu", "gen.cu", "mlp.cu", "capi.cu", "fused.cu", "hfmetrics.cu", "repack.cu", "baz.cu", "prehq.cu", "compact.cu"]
-HEADERS = ["hw_device.cuh", "hw_math.h", "hw_params.h", "../../include/hw_b200.h"]
+HEADERS = ["hw_device.cuh", "hw_math.h", "hw_params.h", "metric_blocks.cuh", "../../include/hw_b200.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

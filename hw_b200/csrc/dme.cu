@@ -575,14 +575,15 @@ __device__ __forceinline__ void EmMStep(const KParams& k, const EmHist& h, const
 
 // The learned start: replaces the reference start v by the proposal column Q
 // unless the proposal's log-likelihood is lower (or not comparable); returns
-// 1 when it kept the reference start.  Reports both log-likelihoods.
+// 1 when it kept the reference start.  Reports both log-likelihoods.  When
+// the proposal is kept, ci/mom1/varinv/safe and the per-bin scratch hold its
+// E-step, which is the first EM iteration's E-step from that start.
 __device__ __forceinline__ int ChooseStart(const KParams& k, const EmHist& h, const EmReg& r, const float* Q, bool fallback,
                                            float* bpS, float* tau0S, float* facS, EmVars& v, float& llPlain,
-                                           float& llStart)
+                                           float& llStart, float (&ci)[5], float (&mom1)[5], float (&varinv)[5],
+                                           bool& safe)
 {
     const int z = h.z;
-    float ci[5], mom1[5], varinv[5];
-    bool safe;
     llPlain = EmEStep(k, h, v, r, bpS, tau0S, facS, ci, mom1, varinv, safe);
     llStart = llPlain;
     EmVars p;
@@ -642,10 +643,17 @@ __global__ void __launch_bounds__(kLane, 10) DmeEstimateKernel(DmeArgs A, KParam
     EmReg r;
     DmePrelude(k, A.models[l], A.stats[l], h, tModel, tEst, det, v, r);
     lap(0);
+    // With a learned start that is kept, its E-step in ChooseStart is the
+    // first iteration's E-step (same start, same histogram), so the loop
+    // takes it instead of computing it again.
+    float ci[5], mom1[5], varinv[5];
+    bool safe = false, haveE = false;
+    float llE = 0.0f;
     if (A.proposal)
     {
-        float llPlain, llStart;
-        ChooseStart(k, h, r, A.proposal + (size_t)l * 15 * kLane, true, bpS, tau0S, facS, v, llPlain, llStart);
+        float llPlain;
+        haveE = !ChooseStart(k, h, r, A.proposal + (size_t)l * 15 * kLane, true, bpS, tau0S, facS, v, llPlain, llE,
+                             ci, mom1, varinv, safe);
     }
     lap(1);
 
@@ -676,9 +684,8 @@ __global__ void __launch_bounds__(kLane, 10) DmeEstimateKernel(DmeArgs A, KParam
     int it = 0;
     for (; it < iterLimit; ++it)
     {
-        float ci[5], mom1[5], varinv[5];
-        bool safe;
-        const float ll = EmEStep(k, h, v, r, bpS, tau0S, facS, ci, mom1, varinv, safe);
+        const float ll = haveE ? llE : EmEStep(k, h, v, r, bpS, tau0S, facS, ci, mom1, varinv, safe);
+        haveE = false;
         const float prev = logLike;
         logLike = ll;
         const float delta = ll - prev;
@@ -877,7 +884,7 @@ __global__ void __launch_bounds__(kLane, 12) DmeEmFitKernel(DmeFitArgs A, KParam
     int fellBack = 0;
     if (A.mode != HW_EM_START_PLAIN)
         fellBack = ChooseStart(k, h, r, A.proposal + (size_t)l * 15 * kLane, A.mode == HW_EM_START_BETTER, bpS, tau0S,
-                               facS, v, llPlain, llStart);
+                               facS, v, llPlain, llStart, ci, mom1, varinv, safe);
     else
     {
         llPlain = EmEStep(k, h, v, r, bpS, tau0S, facS, ci, mom1, varinv, safe);

@@ -23,6 +23,7 @@
 #include <cub/device/device_scan.cuh>
 
 #include "hw_device.cuh"
+#include "metric_blocks.cuh"
 
 using namespace hwk;
 
@@ -237,11 +238,13 @@ __global__ void PromoteKernel(uint8_t* hq, const uint8_t* newly, uint32_t n, uns
     if ((threadIdx.x & 31) == 0 && votes) atomicAdd(count, (unsigned long long)votes);
 }
 
-// The most recent activity label of each ZMW from a block's HF metrics.
-__global__ void ActivityKernel(const hw_basecalling_metrics* metrics, uint8_t* activity, uint32_t n)
+// The most recent activity label of each ZMW the aggregator is given
+// metrics for (z % stride == 0, PrelimHQFilter.cpp:107-118) from a block's
+// HF metrics.
+__global__ void ActivityKernel(const hw_basecalling_metrics* metrics, uint8_t* activity, uint32_t n, uint32_t stride)
 {
     const uint32_t z = blockIdx.x * blockDim.x + threadIdx.x;
-    if (z < n) activity[z] = metrics[z / kLane].activity_label[z % kLane];
+    if (z < n && z % stride == 0) activity[z] = metrics[z / kLane].activity_label[z % kLane];
 }
 
 int Fail(int code, const std::string& msg) { return hwk::SetLastError(code, msg.c_str()); }
@@ -282,6 +285,12 @@ struct hw_prelim_hq
     unsigned long long* numHq = nullptr;
     void* scanTmp = nullptr;
     size_t scanBytes = 0;
+    // metric side (cfg.metrics)
+    MetricSide ms{};
+    hw_spider_metric_block* mOut = nullptr;
+    uint64_t mCap = 0, mTotal = 0;
+    uint64_t* mOffsets = nullptr;      // [numZmw + 1]
+    uint32_t mBlock = 0;
 
     ~hw_prelim_hq()
     {
@@ -305,6 +314,45 @@ struct hw_prelim_hq
         cudaFree(outEvents);
         cudaFree(numHq);
         cudaFree(scanTmp);
+        cudaFree(ms.ring);
+        cudaFree(ms.agg);
+        cudaFree(ms.pending);
+        cudaFree(ms.pendingCount);
+        cudaFree(mOut);
+        cudaFree(mOffsets);
+    }
+
+    // The metric side of the checkpoint: before the promotion of the ZMWs
+    // marked now (hq = HQ before this block's end).
+    int MetricCheckpoint(bool flush, cudaStream_t s)
+    {
+        const uint32_t n = numZmw, threads = 256, blocks = (n + threads - 1) / threads;
+        const int mode = flush ? 1 : 0;
+        MetricCountKernel<<<blocks, threads, 0, s>>>(ms, hq, newly, block, mode, mOffsets);
+        int rc = Cuda(cudaGetLastError(), "hw_prelim_hq metrics");
+        if (!rc)
+            rc = Cuda(cub::DeviceScan::ExclusiveSum(scanTmp, scanBytes, mOffsets, mOffsets, (int)n + 1, s),
+                      "hw_prelim_hq metrics");
+        uint64_t total = 0;
+        if (!rc) rc = Cuda(cudaMemcpyAsync(&total, mOffsets + n, sizeof(total), cudaMemcpyDeviceToHost, s),
+                           "hw_prelim_hq metrics");
+        if (!rc) rc = Cuda(cudaStreamSynchronize(s), "hw_prelim_hq metrics");
+        if (rc) return rc;
+        if (total > mCap)
+        {
+            cudaFree(mOut);
+            mOut = nullptr;
+            mCap = 0;
+            const uint64_t cap = std::max<uint64_t>(total + total / 4, 1024);
+            if ((rc = Cuda(cudaMalloc((void**)&mOut, cap * sizeof(hw_spider_metric_block)), "hw_prelim_hq metrics")))
+                return rc;
+            mCap = cap;
+        }
+        MetricWriteKernel<<<blocks, threads, 0, s>>>(ms, hq, newly, block, mode, mOffsets, mOut);
+        if ((rc = Cuda(cudaGetLastError(), "hw_prelim_hq metrics"))) return rc;
+        mTotal = total;
+        mBlock = block;
+        return HW_OK;
     }
 
     int UploadSlots()
@@ -361,6 +409,7 @@ struct hw_prelim_hq
         CheckpointCopyKernel<<<std::min<uint32_t>((n + 255) / 256, 148 * 8), 256, 0, s>>>(v, hq, newly, flush,
                                                                                            outOffsets, out, n);
         if ((rc = Cuda(cudaGetLastError(), "hw_prelim_hq"))) return rc;
+        if (cfg.metrics && (rc = MetricCheckpoint(flush, s))) return rc;
         if (!flush)
         {
             PromoteKernel<<<blocks, threads, 0, s>>>(hq, newly, n, numHq);
@@ -435,6 +484,27 @@ int hw_prelim_hq_create(const hw_baz_field* fields, uint32_t n_fields, int32_t s
     alloc((void**)&h->outEvents, sizeof(uint32_t) * num_zmw);
     alloc((void**)&h->numHq, sizeof(unsigned long long));
     if (!rc) rc = Cuda(cudaMemset(h->activity, 4, num_zmw), "hw_prelim_hq_create");   // NUM_PHYS_STATES: none yet
+    if (cfg->metrics)
+    {
+        MetricSide& m = h->ms;
+        m.numZmw = num_zmw;
+        m.lookback = cfg->lookback_blocks;
+        m.stride = cfg->zmw_stride;
+        m.production = cfg->enable_prehq != 0;
+        if (m.production)
+        {
+            alloc((void**)&m.ring, sizeof(MetricBlk) * (size_t)cfg->lookback_blocks * num_zmw);
+            alloc((void**)&m.agg, sizeof(AggBlk) * (size_t)num_zmw);
+        }
+        alloc((void**)&m.pending, sizeof(hw_spider_metric_block) * (size_t)num_zmw);
+        alloc((void**)&m.pendingCount, num_zmw);
+        alloc((void**)&h->mOffsets, sizeof(uint64_t) * (num_zmw + 1));
+        if (!rc)
+        {
+            MetricInitKernel<<<(num_zmw + 255) / 256, 256>>>(m);
+            rc = Cuda(cudaGetLastError(), "hw_prelim_hq_create");
+        }
+    }
     if (!rc)
     {
         size_t a = 0, b = 0;
@@ -495,8 +565,13 @@ int hw_prelim_hq_process(hw_prelim_hq* h, const hw_pulse* d_pulses, const uint32
     if ((rc = Cuda(cudaGetLastError(), "hw_prelim_hq_process"))) return rc;
     if (d_metrics)
     {
-        ActivityKernel<<<blocks, threads, 0, s>>>(d_metrics, h->activity, n);
+        ActivityKernel<<<blocks, threads, 0, s>>>(d_metrics, h->activity, n, h->cfg.zmw_stride);
         if ((rc = Cuda(cudaGetLastError(), "hw_prelim_hq_process"))) return rc;
+        if (h->cfg.metrics)
+        {
+            MetricAddKernel<<<blocks, threads, 0, s>>>(h->ms, d_metrics, h->hq, h->block);
+            if ((rc = Cuda(cudaGetLastError(), "hw_prelim_hq_process"))) return rc;
+        }
     }
     if (++h->chunk < h->cfg.chunks_per_block) return HW_OK;
     rc = h->Checkpoint(d_marks, false, out, s);
@@ -514,6 +589,18 @@ int hw_prelim_hq_flush(hw_prelim_hq* h, int32_t* produced, hw_baz_checkpoint* ou
     const int rc = h->Checkpoint(nullptr, true, out, reinterpret_cast<cudaStream_t>(stream));
     if (rc) return rc;
     *produced = 1;
+    return HW_OK;
+}
+
+int hw_prelim_hq_metrics(const hw_prelim_hq* h, hw_metric_checkpoint* out)
+{
+    if (!h || !out) return Fail(HW_ERR_INVALID_ARG, "hw_prelim_hq_metrics: bad argument");
+    if (!h->cfg.metrics) return Fail(HW_ERR_INVALID_ARG, "hw_prelim_hq_metrics: the stage runs no metric side");
+    *out = hw_metric_checkpoint{};
+    out->d_blocks = h->mOut;
+    out->total_blocks = h->mTotal;
+    out->d_offsets = h->mOffsets;
+    out->block = h->mBlock;
     return HW_OK;
 }
 

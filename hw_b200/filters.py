@@ -649,7 +649,7 @@ class PrelimHq(_Handle):
     _destroy = "hw_prelim_hq_destroy"
 
     def __init__(self, num_zmw, preset=abi.BAZ_PRODUCTION, fields=None, skip_rejects=None, chunks_per_block=8,
-                 lookback=10, enable=False, throttle=0.10, zmw_stride=1):
+                 lookback=10, enable=False, throttle=0.10, zmw_stride=1, metrics=False):
         super().__init__()
         if fields is None:
             fields, skip = baz_preset(preset)
@@ -660,6 +660,7 @@ class PrelimHq(_Handle):
         check(lib().hw_prelim_hq_config_default(abi.ptr(cfg)))
         cfg["chunks_per_block"], cfg["lookback_blocks"] = chunks_per_block, lookback
         cfg["enable_prehq"], cfg["hq_throttle_fraction"], cfg["zmw_stride"] = int(bool(enable)), throttle, zmw_stride
+        cfg["metrics"] = int(bool(metrics))
         check(lib().hw_prelim_hq_create(abi.ptr(self.fields), len(self.fields), int(bool(skip_rejects)), num_zmw,
                                         abi.ptr(cfg), C.byref(self._h)))
         self._res = np.zeros(1, abi.BAZ_CHECKPOINT_DT)
@@ -691,6 +692,20 @@ class PrelimHq(_Handle):
         out = torch.empty(self.num_zmw, dtype=torch.uint8, device="cuda")
         check(lib().hw_prelim_hq_activity(self._h, _p(out), _stream()))
         return out
+
+    def metric_checkpoint(self):
+        """The metric side of the last checkpoint (hw_prelim_hq_metrics):
+        {"blocks": uint8 CUDA tensor of total * 164 bytes (abi.
+        SPIDER_METRIC_BLOCK_DT records), "offsets": int64 [n + 1], "block"}."""
+        r = np.zeros(1, abi.METRIC_CHECKPOINT_DT)
+        check(lib().hw_prelim_hq_metrics(self._h, abi.ptr(r)))
+        r = r[0]
+        n, total = self.num_zmw, int(r["total_blocks"])
+        size = abi.SPIDER_METRIC_BLOCK_DT.itemsize
+        return {"blocks": _from_device(int(r["d_blocks"]), total * size) if total else
+                torch.empty(0, dtype=torch.uint8, device="cuda"),
+                "offsets": _from_device(int(r["d_offsets"]), 8 * (n + 1)).view(torch.int64),
+                "total": total, "block": int(r["block"])}
 
 
 class PulseCompactor(_Handle):

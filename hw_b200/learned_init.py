@@ -359,6 +359,7 @@ def dme_phases(net, pool, pool_id=0, sm_mhz=None):
                "lane_cycles_mean": float(ph[:, 6].mean()), "lane_cycles_max": int(ph[:, 6].max())}
         return out
 
+    one(False), one(True)   # warm-up: module loading and first-launch costs
     return {"lanes": lanes, "plain": one(False), "learned": one(True)}
 
 

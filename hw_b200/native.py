@@ -100,6 +100,7 @@ def lib():
         "hw_prelim_hq_process": ([vp, vp, vp, u32, vp, vp, C.POINTER(i32), vp, vp], C.c_int),
         "hw_prelim_hq_flush": ([vp, C.POINTER(i32), vp, vp], C.c_int),
         "hw_prelim_hq_activity": ([vp, vp, vp], C.c_int),
+        "hw_prelim_hq_metrics": ([vp, vp], C.c_int),
         "hw_baz_encode": ([vp, vp, vp, u32, vp, C.c_uint64, vp, vp, C.POINTER(C.c_uint64), vp], C.c_int),
         "hw_baz_encode_async": ([vp, vp, vp, u32, vp, C.c_uint64, vp, vp, vp], C.c_int),
         "hw_baz_encode_result": ([vp, C.POINTER(C.c_uint64)], C.c_int),

@@ -735,15 +735,17 @@ int hw_pulse_compactor_total(const hw_pulse_compactor* h, uint32_t slot, uint64_
  * caller's marks -- and produces the block's checkpoint (BazAggregator::
  * ProduceBazBuffer): no bytes for a pre-HQ ZMW, its bytes of the block for an
  * HQ ZMW, and for a ZMW marked HQ at this block every block of the window,
- * oldest first; older data is dropped.  The metric side of the aggregator
- * (metric-block lookback and aggregation) is not covered. */
+ * oldest first; older data is dropped.  With `metrics` set the stage also
+ * runs the aggregator's metric side (bazio/writing/MetricBufferManager.h:
+ * 70-357) on the HF metrics passed in; hw_prelim_hq_metrics reports each
+ * checkpoint's metric blocks. */
 typedef struct hw_prelim_hq_config {
     uint32_t chunks_per_block;      /* ceil(framesPerHFMetricBlock / frames per chunk) */
     uint32_t lookback_blocks;       /* PrelimHQConfig lookbackSize (>= 1) */
     int32_t  enable_prehq;          /* PrelimHQConfig enablePreHQ */
     float    hq_throttle_fraction;  /* PrelimHQConfig hqThrottleFraction */
     uint32_t zmw_stride;            /* PrelimHQConfig zmwOutputStride (divides 64) */
-    uint32_t reserved;
+    uint32_t metrics;               /* 1: run the metric side; 0: keep only the activity labels */
 } hw_prelim_hq_config;
 
 /* A checkpoint: device buffers owned by the stage, valid until its next call. */
@@ -780,6 +782,60 @@ int hw_prelim_hq_process(hw_prelim_hq* h, const hw_pulse* d_pulses, const uint32
 int hw_prelim_hq_flush(hw_prelim_hq* h, int32_t* produced, hw_baz_checkpoint* out, void* stream);
 /* Each ZMW's most recent activity label (HQRFPhysicalStates; 4 before any). */
 int hw_prelim_hq_activity(hw_prelim_hq* h, uint8_t* d_out, void* stream);
+
+/* One metric block of one ZMW as the BAZ file takes it: Primary::
+ * SpiderMetricBlock (bazio/MetricBlock.h:58-124, MetricBlock<float, 1>), its
+ * fields in the same order.  Its count setters take uint16_t
+ * (bazio/MetricBlock.h:153-310), so aggregated counts arrive modulo 65536;
+ * num_baseline_frames keeps 32 bits.  pixel_checksum and dme_status are never
+ * set on this path (0). */
+typedef struct hw_spider_metric_block {
+    uint32_t num_frames, num_pulses, pulse_width, base_width;
+    uint32_t num_sandwiches, num_half_sandwiches, num_pulse_label_stutters;
+    float    pulse_detection_score, trace_autocorr;
+    int16_t  pixel_checksum;
+    uint8_t  dme_status, activity_label;
+    float    pkmid[HW_NUM_ANALOGS];               /* A, C, G, T */
+    uint32_t num_pkmid_frames[HW_NUM_ANALOGS];
+    float    pkmax[HW_NUM_ANALOGS];
+    uint32_t num_bases[HW_NUM_ANALOGS];
+    uint32_t num_pkmid_bases[HW_NUM_ANALOGS];
+    float    bpzvar[HW_NUM_ANALOGS];
+    float    pkzvar[HW_NUM_ANALOGS];
+    float    baseline, baseline_sd;
+    uint32_t num_baseline_frames;
+} hw_spider_metric_block;
+
+/* The metric side of a checkpoint: device buffers owned by the stage, valid
+ * until its next call.  ZMW z's blocks are d_blocks[d_offsets[z] ..
+ * d_offsets[z + 1]). */
+typedef struct hw_metric_checkpoint {
+    const hw_spider_metric_block* d_blocks;
+    uint64_t        total_blocks;
+    const uint64_t* d_offsets;      /* [num_zmw + 1] */
+    uint32_t        block;          /* the metric block (from 0), as the checkpoint's */
+    uint32_t        reserved;
+} hw_metric_checkpoint;
+
+/* The metric blocks of the checkpoint that the last hw_prelim_hq_process or
+ * hw_prelim_hq_flush produced (BazAggregator::ProduceBazBuffer / Flush ->
+ * MetricBufferManager::GetMetrics; the stage must have been created with
+ * `metrics` set).  Preliminary HQ off (CompleteMetricsGroup,
+ * PrelimHQFilter.cpp:232-290, MetricBufferManager.h:240-250): one block per
+ * ZMW per metric block, CompleteMetrics<uint16_t, half> converted as it
+ * arrives.  Preliminary HQ on (ProductionMetricsGroup): a pre-HQ ZMW's blocks
+ * wait in the lookback window and the oldest are aggregated into its pre-HQ
+ * block; a ZMW marked HQ emits its pre-HQ block and the window's blocks
+ * aggregated by runs of equal activity label, the last run kept open; an HQ
+ * ZMW emits an aggregate each time the label changes; the flush emits every
+ * open aggregate with data.  The reference aggregates an HQ ZMW into the
+ * open aggregate at its stale lookback index (MetricBufferManager.h:263) and
+ * walks a newly-HQ ZMW's window reading each buffer at the index of the
+ * buffer before it (:318); both read other ZMWs' entries, or memory never
+ * written, once ZMWs below were marked HQ inside the window.  The stage
+ * follows each ZMW's own entries and aggregate, which equals the reference
+ * wherever those slips are no-ops. */
+int hw_prelim_hq_metrics(const hw_prelim_hq* h, hw_metric_checkpoint* out);
 
 /* ---- Pool sets: uneven pools --------------------------
  * No single reference counterpart: the reference runs one BatchAnalyzer per

@@ -3351,3 +3351,625 @@ int64_t or_prehq_flush(void* h, uint8_t* out, uint64_t cap, uint64_t* offsets, u
 }
 
 }   // extern "C"
+
+// ---- Metric side of the preliminary HQ stage ------------------------------------
+// basecaller/dataTypes/Metrics.h:36-366 (ProductionMetrics and
+// CompleteMetrics: construction from BasecallingMetrics :53-70 / :212-228,
+// Aggregate :73-118 / :230-286, Convert :121-146 / :288-318) and
+// bazio/writing/MetricBufferManager.h:70-357 (AddZmw, MarkAsHQ, Flush,
+// UpdateLookback, AddProductionMetrics, NumTransitionsInLookbackWindow,
+// AddLookbackWindowMetricBlocks), restated over the same data structures: a
+// window of per-block buffers whose entries are linked by next-buffer
+// indices, per-ZMW (hqStarted, currentIndex, recentIndex) and one open
+// aggregate per ZMW.  AddZmw is called for ZMWs z with z % stride == 0
+// (PrelimHQFilter.cpp:107-118); entries never written read as
+// default-constructed blocks (the reference reads uninitialised memory
+// there), and a newly-HQ ZMW whose window holds fewer label runs than blocks
+// it writes keeps only the first NumTransitions of them (the reference
+// writes the rest past the end of its output view).
+//
+// Two index slips of the reference are kept apart under `literal`:
+// AddProductionMetrics aggregates an HQ ZMW into the open aggregate at its
+// stale window index instead of its own (MetricBufferManager.h:263), and
+// AddLookbackWindowMetricBlocks reads each buffer after the front at the
+// index of the buffer before it (:318, the index advances after the read).
+// Both are no-ops while no ZMW below the one concerned was marked HQ in the
+// blocks its indices span; past that the reference reads other ZMWs'
+// entries and, where its index runs past a buffer or through an entry that
+// was never linked, memory it never wrote (read here as a default block and
+// index 0).  With `literal` off the oracle follows each ZMW's own entries
+// and aggregate, which is what the stage computes.
+//
+// The half type is the `half` library 2.1.0 (half.sourceforge.net; pinned by
+// basecaller/nexus-versions/Fetchhalf.cmake:3 and not in the reference tree):
+// float -> half rounds to nearest with ties to even (its default round
+// style), half -> float is exact, and half sqrt is correctly rounded, which
+// equals rounding the correctly-rounded float sqrt to half (24 >= 2*11 + 2
+// bits).  NaN converts to the quiet NaN 0x7fff / 0xffff.
+
+namespace {
+
+uint16_t HalfBits(float f)
+{
+    uint32_t x;
+    std::memcpy(&x, &f, 4);
+    const uint16_t sign = (uint16_t)((x >> 16) & 0x8000u);
+    const uint32_t ax = x & 0x7fffffffu;
+    if (ax > 0x7f800000u) return (uint16_t)(sign | 0x7fffu);    // NaN
+    if (ax >= 0x477ff000u) return (uint16_t)(sign | 0x7c00u);   // >= 65520 (and inf) -> inf
+    if (ax < 0x38800000u)                                        // below 2^-14: subnormal or zero
+    {
+        const int e = (int)(ax >> 23);
+        const int shift = 126 - e;                               // value = m * 2^(e-150); unit 2^-24
+        if (shift > 24) return sign;
+        const uint32_t m = (ax & 0x7fffffu) | 0x800000u;
+        uint32_t h = m >> shift;
+        const uint32_t rem = m & ((1u << shift) - 1u), half = 1u << (shift - 1);
+        if (rem > half || (rem == half && (h & 1u))) ++h;
+        return (uint16_t)(sign | h);
+    }
+    uint32_t h = (ax - 0x38000000u) >> 13;                       // rebias 127 -> 15
+    const uint32_t rem = ax & 0x1fffu;
+    if (rem > 0x1000u || (rem == 0x1000u && (h & 1u))) ++h;
+    return (uint16_t)(sign | h);
+}
+
+float HalfFloat(uint16_t h)
+{
+    const uint32_t sign = (uint32_t)(h & 0x8000u) << 16;
+    const uint32_t e = (h >> 10) & 0x1fu, m = h & 0x3ffu;
+    uint32_t x;
+    if (e == 0x1f) x = sign | 0x7f800000u | (m << 13);
+    else if (e) x = sign | ((e + 112u) << 23) | (m << 13);
+    else if (!m) x = sign;
+    else
+    {
+        int k = 0;
+        uint32_t mm = m;
+        while (!(mm & 0x400u)) { mm <<= 1; ++k; }
+        x = sign | ((uint32_t)(113 - k) << 23) | ((mm & 0x3ffu) << 13);
+    }
+    float f;
+    std::memcpy(&f, &x, 4);
+    return f;
+}
+
+struct Half
+{
+    uint16_t bits = 0;
+    Half() = default;
+    Half(float f) : bits(HalfBits(f)) {}
+    operator float() const { return HalfFloat(bits); }
+};
+
+float SqrtOf(float v) { return std::sqrt(v); }
+float SqrtOf(Half v) { return Half(std::sqrt((float)v)); }
+
+constexpr uint8_t kNoLabel = 4;   // HQRFPhysicalStates::NUM_PHYS_STATES
+
+template <typename U, typename F>
+struct ProdBlock
+{
+    U numFrames = 0, pulseWidth = 0, baseWidth = 0, numPulses = 0, numBases = 0;
+    F pkmid[4] = {F(0.f), F(0.f), F(0.f), F(0.f)};
+    U numPkmidFrames[4] = {0, 0, 0, 0};
+    U numBasesByAnalog[4] = {0, 0, 0, 0};
+    F baselineVar = F(0.f), baselineMean = F(0.f);
+    U numBaselineFrames = 0;
+    uint8_t label = kNoLabel;
+
+    ProdBlock() = default;
+    ProdBlock(const hw_basecalling_metrics& bm, int z)
+        : numFrames(bm.num_frames[z]), pulseWidth(bm.num_pulse_frames[z]), baseWidth(bm.num_base_frames[z]),
+          numPulses(bm.num_pulses[z]), numBases(bm.num_bases[z]), baselineVar(F(bm.frame_baseline_variance_dws[z])),
+          baselineMean(F(bm.frame_baseline_dws[z])), numBaselineFrames(bm.num_frames_baseline[z]),
+          label(bm.activity_label[z])
+    {
+        for (int a = 0; a < 4; ++a)
+        {
+            numPkmidFrames[a] = bm.num_pk_mid_frames[a][z];
+            const float v = numPkmidFrames[a] > 0 ? bm.pk_mid_signal[a][z] / (float)numPkmidFrames[a] : 0.0f;
+            pkmid[a] = F(v);
+            numBasesByAnalog[a] = bm.num_bases_by_analog[a][z];
+        }
+    }
+
+    bool HasData() const { return numFrames != 0; }
+
+    // Metrics.h:73-118, every product and sum in float
+    template <typename U2, typename F2>
+    void Aggregate(const ProdBlock<U2, F2>& b)
+    {
+        const U nbf = (U)(numBaselineFrames + b.numBaselineFrames);
+        float mean = (float)numBaselineFrames * (float)baselineMean;
+        mean = mean + (float)b.numBaselineFrames * (float)b.baselineMean;
+        baselineMean = F(mean);
+        if (nbf > 0)
+        {
+            baselineMean = F((float)baselineMean / (float)nbf);
+            float bv = 0.0f;
+            U nk = nbf;
+            auto pooled = [&](uint64_t n0, float var) {
+                const uint64_t n = n0 > 1 ? n0 - 1 : n0;
+                bv = bv + (float)n * var;
+                return n0 > 0;
+            };
+            if (pooled(numBaselineFrames, (float)baselineVar)) --nk;
+            if (pooled(b.numBaselineFrames, (float)b.baselineVar)) --nk;
+            baselineVar = F(bv / (float)nk);
+            numBaselineFrames = nbf;
+        }
+        for (int a = 0; a < 4; ++a)
+        {
+            float p = (float)numPkmidFrames[a] * (float)pkmid[a];
+            p = p + (float)b.numPkmidFrames[a] * (float)b.pkmid[a];
+            numPkmidFrames[a] = (U)(numPkmidFrames[a] + b.numPkmidFrames[a]);
+            if (numPkmidFrames[a] > 0) p = p / (float)numPkmidFrames[a];
+            pkmid[a] = F(p);
+            numBasesByAnalog[a] = (U)(numBasesByAnalog[a] + b.numBasesByAnalog[a]);
+        }
+        numFrames = (U)(numFrames + b.numFrames);
+        pulseWidth = (U)(pulseWidth + b.pulseWidth);
+        baseWidth = (U)(baseWidth + b.baseWidth);
+        numPulses = (U)(numPulses + b.numPulses);
+        numBases = (U)(numBases + b.numBases);
+        label = b.label;
+    }
+
+    // Metrics.h:121-146 through the uint16_t setters of bazio/MetricBlock.h
+    void Convert(hw_spider_metric_block& sm) const
+    {
+        sm.num_frames = (uint16_t)numFrames;
+        sm.pulse_width = (uint16_t)pulseWidth;
+        sm.base_width = (uint16_t)baseWidth;
+        sm.num_pulses = (uint16_t)numPulses;
+        for (int a = 0; a < 4; ++a)
+        {
+            sm.pkmid[a] = (float)pkmid[a];
+            sm.num_pkmid_frames[a] = (uint16_t)numPkmidFrames[a];
+            sm.num_bases[a] = (uint16_t)numBasesByAnalog[a];
+        }
+        sm.baseline = (float)baselineMean;
+        sm.baseline_sd = (float)SqrtOf(baselineVar);
+        sm.num_baseline_frames = (uint32_t)numBaselineFrames;
+        sm.activity_label = label;
+    }
+};
+
+template <typename U, typename F>
+struct CompleteBlock
+{
+    ProdBlock<U, F> prod;
+    U numHalfSandwiches = 0, numSandwiches = 0, numPulseLabelStutters = 0;
+    F pulseDetectionScore = F(0.f), traceAutoCorrelation = F(0.f);
+    F pkmax[4] = {F(0.f), F(0.f), F(0.f), F(0.f)};
+    U numPkmidBases[4] = {0, 0, 0, 0};
+    F bpzvar[4] = {F(0.f), F(0.f), F(0.f), F(0.f)};
+    F pkzvar[4] = {F(0.f), F(0.f), F(0.f), F(0.f)};
+
+    CompleteBlock() = default;
+    CompleteBlock(const hw_basecalling_metrics& bm, int z)
+        : prod(bm, z), numHalfSandwiches(bm.num_half_sandwiches[z]), numSandwiches(bm.num_sandwiches[z]),
+          numPulseLabelStutters(bm.num_pulse_label_stutters[z]), pulseDetectionScore(F(bm.pulse_detection_score[z])),
+          traceAutoCorrelation(F(bm.autocorrelation[z]))
+    {
+        for (int a = 0; a < 4; ++a)
+        {
+            pkmax[a] = F(bm.pk_max[a][z]);
+            numPkmidBases[a] = bm.num_pk_mid_bases_by_analog[a][z];
+            bpzvar[a] = F(bm.bp_zvar[a][z]);
+            pkzvar[a] = F(bm.pk_zvar[a][z]);
+        }
+    }
+
+    // Metrics.h:230-286 (only the reference's own known-answer test
+    // aggregates complete metrics; the stage converts them as they arrive)
+    template <typename U2, typename F2>
+    void Aggregate(const CompleteBlock<U2, F2>& b)
+    {
+        numHalfSandwiches = (U)(numHalfSandwiches + b.numHalfSandwiches);
+        numSandwiches = (U)(numSandwiches + b.numSandwiches);
+        numPulseLabelStutters = (U)(numPulseLabelStutters + b.numPulseLabelStutters);
+        float pk[4], pkz[4] = {0, 0, 0, 0}, bpz[4] = {0, 0, 0, 0};
+        U npf[4], npb[4];
+        for (int a = 0; a < 4; ++a)
+        {
+            const float pa = (float)prod.pkmid[a], pb = (float)b.prod.pkmid[a];
+            pk[a] = (float)prod.numPkmidFrames[a] * pa + (float)b.prod.numPkmidFrames[a] * pb;
+            npf[a] = (U)(prod.numPkmidFrames[a] + b.prod.numPkmidFrames[a]);
+            if (npf[a] > 0) pk[a] = pk[a] / (float)npf[a];
+            if (prod.numPkmidFrames[a] > 1) pkz[a] = pkz[a] + (float)prod.numPkmidFrames[a] * (float)pkzvar[a];
+            if (b.prod.numPkmidFrames[a] > 1) pkz[a] = pkz[a] + (float)b.prod.numPkmidFrames[a] * (float)b.pkzvar[a];
+            npb[a] = (U)(numPkmidBases[a] + b.numPkmidBases[a]);
+            if (numPkmidBases[a] > 1) bpz[a] = bpz[a] + (float)bpzvar[a] * pa * pa * (float)numPkmidBases[a];
+            if (b.numPkmidBases[a] > 1) bpz[a] = bpz[a] + (float)b.bpzvar[a] * pb * pb * (float)b.numPkmidBases[a];
+        }
+        for (int a = 0; a < 4; ++a)
+        {
+            float v = pkz[a];
+            if (npf[a] > 1) v = v / (float)npf[a];
+            pkzvar[a] = F(v);
+            float w = bpz[a];
+            numPkmidBases[a] = npb[a];
+            if (npf[a] > 0 && numPkmidBases[a] > 1) w = w / ((float)numPkmidBases[a] * pk[a] * pk[a]);
+            bpzvar[a] = F(w);
+            pkmax[a] = F(std::max((float)pkmax[a], (float)b.pkmax[a]));
+        }
+        const U nf = (U)(prod.numFrames + b.prod.numFrames);
+        float pds = (float)prod.numFrames * (float)pulseDetectionScore + (float)b.prod.numFrames * (float)b.pulseDetectionScore;
+        float tac = (float)prod.numFrames * (float)traceAutoCorrelation + (float)b.prod.numFrames * (float)b.traceAutoCorrelation;
+        if (nf > 0)
+        {
+            pds = pds / (float)nf;
+            tac = tac / (float)nf;
+        }
+        pulseDetectionScore = F(pds);
+        traceAutoCorrelation = F(tac);
+        prod.Aggregate(b.prod);
+    }
+
+    void Convert(hw_spider_metric_block& sm) const
+    {
+        prod.Convert(sm);
+        sm.num_half_sandwiches = (uint16_t)numHalfSandwiches;
+        sm.num_sandwiches = (uint16_t)numSandwiches;
+        sm.num_pulse_label_stutters = (uint16_t)numPulseLabelStutters;
+        sm.pulse_detection_score = (float)pulseDetectionScore;
+        sm.trace_autocorr = (float)traceAutoCorrelation;
+        for (int a = 0; a < 4; ++a)
+        {
+            sm.pkmax[a] = (float)pkmax[a];
+            sm.num_pkmid_bases[a] = (uint16_t)numPkmidBases[a];
+            sm.bpzvar[a] = (float)bpzvar[a];
+            sm.pkzvar[a] = (float)pkzvar[a];
+        }
+    }
+};
+
+hw_spider_metric_block EmptySpider()
+{
+    hw_spider_metric_block sm;
+    std::memset(&sm, 0, sizeof(sm));
+    return sm;
+}
+
+// MetricBufferManager over ProductionMetricsGroup (preliminary HQ on) or
+// CompleteMetricsGroup (off).
+struct MetricSideOracle
+{
+    using MetricT = ProdBlock<uint16_t, Half>;
+    using AggT = ProdBlock<uint32_t, float>;
+    struct Buffer
+    {
+        std::vector<MetricT> data;
+        std::vector<uint32_t> next;
+        explicit Buffer(size_t n) : data(n), next(n, 0) {}
+    };
+    struct Info
+    {
+        bool hqStarted = false;
+        uint32_t current = 0, recent = 0;
+    };
+
+    uint32_t numZmw, maxLookBack, stride;
+    bool production, literal;
+    std::vector<uint8_t> recentLabel;
+    std::vector<Info> info;
+    std::vector<uint8_t> newHq;
+    size_t numHq = 0;
+    std::vector<AggT> agg;
+    std::deque<Buffer> window;
+    std::vector<std::vector<hw_spider_metric_block>> out;
+
+    MetricSideOracle(uint32_t n, uint32_t lookback, bool prehq, uint32_t zmwStride, bool lit)
+        : numZmw(n), maxLookBack(lookback), stride(zmwStride), production(prehq), literal(lit),
+          recentLabel(n, kNoLabel), info(n), newHq(n, 0), agg(n), out(n)
+    {
+        for (uint32_t z = 0; z < n; ++z) info[z].current = info[z].recent = z;
+        if (production) window.emplace_back(n);
+    }
+
+    // MetricBufferManager.h:142-149, 240-287
+    void AddZmw(uint32_t z, const hw_basecalling_metrics& bm, int lz)
+    {
+        recentLabel[z] = bm.activity_label[lz];
+        if (!production)
+        {
+            hw_spider_metric_block sm = EmptySpider();
+            CompleteBlock<uint16_t, Half>(bm, lz).Convert(sm);
+            out[z] = {sm};
+            return;
+        }
+        const MetricT m(bm, lz);
+        if (!info[z].hqStarted)
+        {
+            window.back().data[info[z].recent] = m;
+            return;
+        }
+        AggT& a = agg[literal ? info[z].current : z];
+        if (m.label == a.label)
+        {
+            a.Aggregate(m);
+            return;
+        }
+        if (a.label != kNoLabel)
+        {
+            hw_spider_metric_block sm = EmptySpider();
+            a.Convert(sm);
+            out[z] = {sm};
+        }
+        a = AggT();
+        a.Aggregate(m);
+    }
+
+    void Add(const hw_basecalling_metrics* lanes)
+    {
+        for (uint32_t z = 0; z < numZmw; z += stride) AddZmw(z, lanes[z / HW_LANE_SIZE], (int)(z % HW_LANE_SIZE));
+    }
+
+    // MetricBufferManager.h:151-159
+    void MarkAsHq(uint32_t z)
+    {
+        if (!production || info[z].hqStarted || newHq[z]) return;
+        ++numHq;
+        newHq[z] = 1;
+    }
+
+    // MetricBufferManager.h:289-305
+    size_t Transitions(uint32_t z) const
+    {
+        uint32_t idx = info[z].current;
+        size_t n = 0;
+        uint8_t cur = kNoLabel;
+        for (const Buffer& b : window)
+        {
+            const MetricT& m = b.data[idx];
+            if (m.label != cur)
+            {
+                ++n;
+                cur = m.label;
+            }
+            idx = b.next[idx];
+        }
+        return n;
+    }
+
+    // MetricBufferManager.h:180-233 with :307-333
+    void UpdateLookback()
+    {
+        if (!production) return;
+        uint32_t lookbackIdx = 0;
+        for (uint32_t z = 0; z < numZmw; ++z)
+        {
+            Info& in = info[z];
+            if (in.hqStarted || newHq[z])
+            {
+                in.hqStarted = true;
+                if (!newHq[z]) continue;
+                const size_t n = Transitions(z);
+                std::vector<hw_spider_metric_block> o(n, EmptySpider());
+                auto put = [&](size_t i, const AggT& a) {
+                    if (i < n) a.Convert(o[i]);
+                };
+                put(0, agg[z]);
+                uint32_t idx = in.current;
+                const MetricT& front = window.front().data[idx];
+                uint8_t cur = front.label;
+                AggT amb;
+                amb.Aggregate(front);
+                size_t k = 1;
+                for (size_t w = 1; w < window.size(); ++w)
+                {
+                    const Buffer& b = window[w];
+                    MetricT mb;
+                    if (literal)
+                    {
+                        if (idx < b.data.size()) mb = b.data[idx];
+                        idx = idx < b.next.size() ? b.next[idx] : 0;
+                    }
+                    else
+                    {
+                        idx = window[w - 1].next[idx];
+                        mb = b.data[idx];
+                    }
+                    if (mb.label != cur)
+                    {
+                        put(k++, amb);
+                        cur = mb.label;
+                        amb = AggT();
+                    }
+                    amb.Aggregate(mb);
+                }
+                out[z] = std::move(o);
+                agg[z] = AggT();
+                agg[z].Aggregate(amb);
+            }
+            else
+            {
+                window.back().next[in.recent] = lookbackIdx;
+                in.recent = lookbackIdx++;
+                if (window.size() == maxLookBack)
+                {
+                    const Buffer& f = window.front();
+                    agg[z].Aggregate(f.data[in.current]);
+                    in.current = f.next[in.current];
+                }
+            }
+        }
+        if (maxLookBack > 0)
+        {
+            window.emplace_back(numZmw - numHq);
+            if (window.size() > maxLookBack) window.pop_front();
+        }
+        std::fill(newHq.begin(), newHq.end(), 0);
+    }
+
+    // MetricBufferManager.h:161-178
+    void Flush()
+    {
+        if (!production) return;
+        for (uint32_t z = 0; z < numZmw; ++z)
+            if (agg[z].HasData())
+            {
+                hw_spider_metric_block sm = EmptySpider();
+                agg[z].Convert(sm);
+                out[z] = {sm};
+            }
+    }
+
+    // GetMetrics; -1 (nothing taken) when the blocks pass cap
+    int64_t Take(hw_spider_metric_block* dst, uint64_t cap, uint64_t* offsets)
+    {
+        uint64_t total = 0;
+        for (const auto& o : out) total += o.size();
+        if (total > cap) return -1;
+        uint64_t pos = 0;
+        for (uint32_t z = 0; z < numZmw; ++z)
+        {
+            offsets[z] = pos;
+            for (const auto& b : out[z]) dst[pos++] = b;
+            out[z].clear();
+        }
+        offsets[numZmw] = pos;
+        return (int64_t)pos;
+    }
+};
+
+}   // namespace
+
+extern "C" {
+
+// literal: keep the reference's two index slips (see above).
+void* or_metrics_create(uint32_t numZmw, uint32_t lookback, int32_t enablePrehq, uint32_t zmwStride, int32_t literal)
+{
+    if (numZmw == 0 || lookback == 0 || zmwStride == 0 || 64 % zmwStride) return nullptr;
+    return new MetricSideOracle(numZmw, lookback, enablePrehq != 0, zmwStride, literal != 0);
+}
+
+void or_metrics_destroy(void* h) { delete static_cast<MetricSideOracle*>(h); }
+
+// AddMetrics of every ZMW z with z % stride == 0 from one block's HF metrics
+// (ceil(numZmw / 64) lanes).
+void or_metrics_add(void* h, const hw_basecalling_metrics* lanes) { static_cast<MetricSideOracle*>(h)->Add(lanes); }
+
+// End of a metric block: MarkAsHQ(z) for newly[z] != 0, UpdateLookback,
+// GetMetrics.  Returns the blocks written (or -1 when they pass cap: the
+// caller retries the GetMetrics with or_metrics_take).
+int64_t or_metrics_end_block(void* h, const uint8_t* newly, hw_spider_metric_block* out, uint64_t cap,
+                             uint64_t* offsets)
+{
+    auto* o = static_cast<MetricSideOracle*>(h);
+    if (newly)
+        for (uint32_t z = 0; z < o->numZmw; ++z)
+            if (newly[z]) o->MarkAsHq(z);
+    o->UpdateLookback();
+    return o->Take(out, cap, offsets);
+}
+
+int64_t or_metrics_take(void* h, hw_spider_metric_block* out, uint64_t cap, uint64_t* offsets)
+{
+    return static_cast<MetricSideOracle*>(h)->Take(out, cap, offsets);
+}
+
+// BazAggregator::Flush: MetricBufferManager::Flush then GetMetrics.
+int64_t or_metrics_flush(void* h, hw_spider_metric_block* out, uint64_t cap, uint64_t* offsets)
+{
+    auto* o = static_cast<MetricSideOracle*>(h);
+    o->Flush();
+    return o->Take(out, cap, offsets);
+}
+
+void or_metrics_activity(void* h, uint8_t* out)
+{
+    auto* o = static_cast<MetricSideOracle*>(h);
+    std::copy(o->recentLabel.begin(), o->recentLabel.end(), out);
+}
+
+void or_half_bits(const float* x, uint64_t n, uint16_t* out)
+{
+    for (uint64_t i = 0; i < n; ++i) out[i] = HalfBits(x[i]);
+}
+
+void or_half_float(const uint16_t* x, uint64_t n, float* out)
+{
+    for (uint64_t i = 0; i < n; ++i) out[i] = HalfFloat(x[i]);
+}
+
+// One metric block of ZMW z of a lane through the reference's metric types:
+// kind 0 ProductionMetrics<uint16_t, half>, 1 CompleteMetrics<uint16_t,
+// half>, 2 ProductionMetrics<uint32_t, float>, 3 CompleteMetrics<uint32_t,
+// float>, converted.
+void or_metric_block_convert(const hw_basecalling_metrics* lane, int32_t z, int32_t kind, hw_spider_metric_block* out)
+{
+    *out = EmptySpider();
+    switch (kind)
+    {
+    case 0: ProdBlock<uint16_t, Half>(*lane, z).Convert(*out); break;
+    case 1: CompleteBlock<uint16_t, Half>(*lane, z).Convert(*out); break;
+    case 2: ProdBlock<uint32_t, float>(*lane, z).Convert(*out); break;
+    default: CompleteBlock<uint32_t, float>(*lane, z).Convert(*out); break;
+    }
+}
+
+// Aggregation sequences of the reference's known-answer tests
+// (basecaller/dataTypes/test/TestMetrics.cpp:60-146) on ZMWs z0, z1 of a lane.
+// test 0 (Production): ProductionMetrics<uint32_t, float>{z0} aggregating
+// {z1}; test 1 (Production, half): an empty ProductionMetrics<uint32_t,
+// float> aggregating ProductionMetrics<uint16_t, half>{z0} `reps` times;
+// test 2 (Aggregate): an empty ProductionMetrics<uint32_t, float> aggregating
+// ProductionMetrics<uint16_t, float> {z0} then {z1}; test 3 (Complete):
+// CompleteMetrics<uint32_t, float>{z0} aggregating {z1}.  The result is
+// converted, and its uncapped counts and aggregate fields are returned in
+// raw[0..]: numFrames, pulseWidth, baseWidth, numPulses, numBases,
+// numBaselineFrames, numPkmidFrames[0], baselineMean, baselineVar, pkmid[0],
+// pkmid[3]; complete: numSandwiches, numHalfSandwiches,
+// numPulseLabelStutters, pulseDetectionScore, traceAutoCorrelation,
+// pkmax[0], numPkmidBases[0], pkzvar[0], bpzvar[0].
+void or_metrics_kat(const hw_basecalling_metrics* lane, int32_t test, int32_t z0, int32_t z1, int32_t reps,
+                    hw_spider_metric_block* out, double* raw)
+{
+    *out = EmptySpider();
+    auto prodRaw = [&](const ProdBlock<uint32_t, float>& p) {
+        const double v[] = {(double)p.numFrames, (double)p.pulseWidth, (double)p.baseWidth, (double)p.numPulses,
+                            (double)p.numBases, (double)p.numBaselineFrames, (double)p.numPkmidFrames[0],
+                            (double)p.baselineMean, (double)p.baselineVar, (double)p.pkmid[0], (double)p.pkmid[3]};
+        std::copy(v, v + 11, raw);
+    };
+    if (test == 0)
+    {
+        ProdBlock<uint32_t, float> m1(*lane, z0), m2(*lane, z1);
+        m1.Aggregate(m2);
+        m1.Convert(*out);
+        prodRaw(m1);
+    }
+    else if (test == 1)
+    {
+        ProdBlock<uint16_t, Half> m3(*lane, z0);
+        ProdBlock<uint32_t, float> m4;
+        for (int i = 0; i < reps; ++i) m4.Aggregate(m3);
+        m4.Convert(*out);
+        prodRaw(m4);
+    }
+    else if (test == 2)
+    {
+        ProdBlock<uint32_t, float> b1;
+        ProdBlock<uint16_t, float> b2(*lane, z0), b3(*lane, z1);
+        b1.Aggregate(b2);
+        b1.Aggregate(b3);
+        b1.Convert(*out);
+        prodRaw(b1);
+    }
+    else
+    {
+        CompleteBlock<uint32_t, float> c1(*lane, z0), c2(*lane, z1);
+        c1.Aggregate(c2);
+        c1.Convert(*out);
+        prodRaw(c1.prod);
+        const double v[] = {(double)c1.numSandwiches, (double)c1.numHalfSandwiches, (double)c1.numPulseLabelStutters,
+                            (double)c1.pulseDetectionScore, (double)c1.traceAutoCorrelation, (double)c1.pkmax[0],
+                            (double)c1.numPkmidBases[0], (double)c1.pkzvar[0], (double)c1.bpzvar[0]};
+        std::copy(v, v + 9, raw + 11);
+    }
+}
+
+}   // extern "C"

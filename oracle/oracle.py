@@ -94,6 +94,22 @@ def lib():
         L.or_prehq_end_block.restype = C.c_int64
         L.or_prehq_flush.argtypes = [vp, vp, C.c_uint64, vp, vp, vp]
         L.or_prehq_flush.restype = C.c_int64
+        u64 = C.c_uint64
+        L.or_metrics_create.argtypes = [u32, u32, i32, u32, i32]
+        L.or_metrics_create.restype = vp
+        L.or_metrics_destroy.argtypes = [vp]
+        L.or_metrics_add.argtypes = [vp, vp]
+        L.or_metrics_end_block.argtypes = [vp, vp, vp, u64, vp]
+        L.or_metrics_end_block.restype = C.c_int64
+        L.or_metrics_take.argtypes = [vp, vp, u64, vp]
+        L.or_metrics_take.restype = C.c_int64
+        L.or_metrics_flush.argtypes = [vp, vp, u64, vp]
+        L.or_metrics_flush.restype = C.c_int64
+        L.or_metrics_activity.argtypes = [vp, vp]
+        L.or_half_bits.argtypes = [vp, u64, vp]
+        L.or_half_float.argtypes = [vp, u64, vp]
+        L.or_metric_block_convert.argtypes = [vp, i32, i32, vp]
+        L.or_metrics_kat.argtypes = [vp, i32, i32, i32, i32, vp, vp]
         L.or_baz_encode_chunk.argtypes = [vp, u32, i32, u32, u32, vp, vp, u32, vp, C.c_uint64, vp, vp]
         _lib = L
     return _lib
@@ -492,3 +508,87 @@ class PrelimHq:
 
     def flush(self):
         return self._out(lib().or_prehq_flush)
+
+
+def half_bits(x):
+    """float32 -> IEEE half bits as the reference's half type rounds them."""
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.empty(x.shape, np.uint16)
+    lib().or_half_bits(abi.ptr(x), x.size, abi.ptr(out))
+    return out
+
+
+def half_float(bits):
+    bits = np.ascontiguousarray(bits, np.uint16)
+    out = np.empty(bits.shape, np.float32)
+    lib().or_half_float(abi.ptr(bits), bits.size, abi.ptr(out))
+    return out
+
+
+METRIC_KINDS = {"production_half": 0, "complete_half": 1, "production_float": 2, "complete_float": 3}
+
+
+def metric_block(lane, z, kind):
+    """One ZMW of a lane's BasecallingMetrics (abi.BASECALLING_METRICS_DT)
+    through one of the reference's metric types, converted."""
+    lane = np.ascontiguousarray(lane, abi.BASECALLING_METRICS_DT)
+    out = np.zeros(1, abi.SPIDER_METRIC_BLOCK_DT)
+    lib().or_metric_block_convert(abi.ptr(lane), int(z), METRIC_KINDS[kind], abi.ptr(out))
+    return out[0]
+
+
+def metrics_kat(lane, test, z0=0, z1=1, reps=1):
+    """The aggregation sequences of the reference's metric known-answer
+    tests (or_metrics_kat): (converted block, raw aggregate fields)."""
+    lane = np.ascontiguousarray(lane, abi.BASECALLING_METRICS_DT)
+    out = np.zeros(1, abi.SPIDER_METRIC_BLOCK_DT)
+    raw = np.zeros(20, np.float64)
+    lib().or_metrics_kat(abi.ptr(lane), int(test), int(z0), int(z1), int(reps), abi.ptr(out), abi.ptr(raw))
+    return out[0], raw
+
+
+class MetricSide:
+    """MetricBufferManager of the preliminary HQ stage: add() one block's HF
+    metrics (lanes of abi.BASECALLING_METRICS_DT), end_block(newly) at each
+    metric block's end, flush() at the end.  `literal` keeps the reference's
+    two index slips (see hw_oracle.cpp)."""
+
+    def __init__(self, num_zmw, lookback, enable_prehq, zmw_stride=1, literal=False):
+        self.n = num_zmw
+        self.h = lib().or_metrics_create(num_zmw, lookback, int(bool(enable_prehq)), zmw_stride, int(bool(literal)))
+        if not self.h:
+            raise ValueError("or_metrics_create: bad argument")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_metrics_destroy(self.h)
+            self.h = None
+
+    def add(self, lanes):
+        lanes = np.ascontiguousarray(lanes, abi.BASECALLING_METRICS_DT)
+        assert len(lanes) * abi.LANE >= self.n
+        lib().or_metrics_add(self.h, abi.ptr(lanes))
+
+    def _take(self, fn, *args):
+        cap = max(1024, self.n * 2)
+        off = np.zeros(self.n + 1, np.uint64)
+        while True:
+            out = np.zeros(cap, abi.SPIDER_METRIC_BLOCK_DT)
+            k = fn(self.h, *args, abi.ptr(out), cap, abi.ptr(off))
+            if k >= 0:
+                return out[:k].copy(), off
+            fn, args = lib().or_metrics_take, ()
+            cap *= 4
+
+    def end_block(self, newly=None):
+        """(blocks, offsets[n + 1]) of the block's metric checkpoint."""
+        m = None if newly is None else np.ascontiguousarray(newly, np.uint8)
+        return self._take(lib().or_metrics_end_block, abi.ptr(m) if m is not None else None)
+
+    def flush(self):
+        return self._take(lib().or_metrics_flush)
+
+    def activity(self):
+        out = np.zeros(self.n, np.uint8)
+        lib().or_metrics_activity(self.h, abi.ptr(out))
+        return out

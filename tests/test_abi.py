@@ -54,6 +54,7 @@ int main(void) {
   S(hw_lane_analog_mode) S(hw_lane_model) S(hw_lane_histogram) S(hw_lane_hist_bounds) S(hw_pulse)
   S(hw_dme_diag) S(hw_frame_interval) S(hw_gen_params) S(hw_pool_chunk) S(hw_fused_tuning)
   S(hw_basecalling_metrics) S(hw_sensor_packet) S(hw_baz_field) S(hw_prelim_hq_config) S(hw_baz_checkpoint)
+  S(hw_spider_metric_block) S(hw_metric_checkpoint)
   O(hw_baseliner_stats, full_autocorr) O(hw_baseliner_stats, trace_min) O(hw_baseliner_stats, trace_max)
   O(hw_baseliner_stats, baseline_stats) O(hw_baseliner_stats, raw_baseline_sum) O(hw_baseliner_stats, background_stats)
   O(hw_lane_model, analogs) O(hw_lane_model, baseline) O(hw_lane_model, confidence)
@@ -71,6 +72,9 @@ int main(void) {
   O(hw_baz_field, transform) O(hw_baz_field, num_bits) O(hw_baz_field, overflow_bytes)
   O(hw_prelim_hq_config, hq_throttle_fraction) O(hw_prelim_hq_config, zmw_stride)
   O(hw_baz_checkpoint, d_hq) O(hw_baz_checkpoint, num_hq) O(hw_baz_checkpoint, block)
+  O(hw_prelim_hq_config, metrics) O(hw_spider_metric_block, pulse_detection_score)
+  O(hw_spider_metric_block, activity_label) O(hw_spider_metric_block, pkmid) O(hw_spider_metric_block, pkzvar)
+  O(hw_spider_metric_block, num_baseline_frames) O(hw_metric_checkpoint, d_offsets) O(hw_metric_checkpoint, block)
   O(hw_config, analogs) O(hw_config, filter_type) O(hw_config, max_calls_per_zmw) O(hw_config, xsp_amp_thresh)
   O(hw_config, model_estimation_mode) O(hw_config, static_baseline_variance)
   return 0;
@@ -115,7 +119,9 @@ def test_struct_offsets_match_python_mirrors(layout):
               "hw_dme_diag": abi.DME_DIAG_DT, "hw_pool_chunk": abi.POOL_CHUNK_DT,
               "hw_fused_tuning": abi.FUSED_TUNING_DT, "hw_basecalling_metrics": abi.BASECALLING_METRICS_DT,
               "hw_sensor_packet": abi.SENSOR_PACKET_DT, "hw_baz_field": abi.BAZ_FIELD_DT,
-              "hw_prelim_hq_config": abi.PRELIM_HQ_CONFIG_DT, "hw_baz_checkpoint": abi.BAZ_CHECKPOINT_DT}[t]
+              "hw_prelim_hq_config": abi.PRELIM_HQ_CONFIG_DT, "hw_baz_checkpoint": abi.BAZ_CHECKPOINT_DT,
+              "hw_spider_metric_block": abi.SPIDER_METRIC_BLOCK_DT,
+              "hw_metric_checkpoint": abi.METRIC_CHECKPOINT_DT}[t]
         assert dt.fields[m][1] == off, key
 
 
