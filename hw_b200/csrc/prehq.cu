@@ -503,6 +503,7 @@ int hw_prelim_hq_create(const hw_baz_field* fields, uint32_t n_fields, int32_t s
         {
             MetricInitKernel<<<(num_zmw + 255) / 256, 256>>>(m);
             rc = Cuda(cudaGetLastError(), "hw_prelim_hq_create");
+            if (!rc) rc = Cuda(cudaStreamSynchronize(0), "hw_prelim_hq_create");
         }
     }
     if (!rc)
