@@ -23,6 +23,16 @@ constexpr int kHidden = 256;
 constexpr int kOut = 32;            // 19 outputs, padded
 constexpr int kOutUsed = 19;
 
+// Parameter layout (floats): W1 [256][304], b1 [256], W2 [256][256], b2 [256],
+// W3 [32][256], b3 [32].  Rows 19..31 of W3 and b3 stay 0.
+constexpr size_t kOffW1 = 0;
+constexpr size_t kOffB1 = kOffW1 + (size_t)kHidden * kFeat;
+constexpr size_t kOffW2 = kOffB1 + kHidden;
+constexpr size_t kOffB2 = kOffW2 + (size_t)kHidden * kHidden;
+constexpr size_t kOffW3 = kOffB2 + kHidden;
+constexpr size_t kOffB3 = kOffW3 + (size_t)kOut * kHidden;
+constexpr size_t kParams = kOffB3 + kOut;
+
 // ---- features, targets, proposals -------------------------------------------
 
 // Per ZMW: sqrt of each bin's share of the in-range counts, then the baseline
@@ -240,6 +250,286 @@ __global__ void __launch_bounds__(128) GemmKernel(const TA* __restrict__ A, long
             }
 }
 
+// ---- Fused forward pass on the sm_100 tensor cores (tcgen05 + TMEM) ------------
+// One CTA of 128 threads per 128 rows runs all three layers: the
+// standardised BF16 input tile and each layer's BF16 weights are staged in
+// shared memory as canonical K-major core matrices (8 rows x 16 bytes,
+// no swizzle: rows 16 bytes apart, the next 8-column group 128 bytes on,
+// the next 8-row group K * 16 bytes on); one thread issues
+// tcgen05.mma.cta_group::1.kind::f16 (M = 128, K = 16 a step) into a
+// 256-column FP32 accumulator in tensor memory and commits to an mbarrier;
+// the four warps read their 32 rows back (tcgen05.ld 32x32b), add the bias,
+// apply GELU and write the BF16 activations over the input tile as the next
+// layer's A operand.  Layer 1 runs as two N = 128 halves so that a weight
+// half (76 KB) and the input tile (76 KB) fit beside each other; layer 2
+// takes all of W2 (128 KB).  Rounding points are those of the mma.sync
+// path (BF16 inputs and activations, FP32 accumulation and epilogue); only
+// the order of the FP32 accumulation differs.  Every wait on the mbarrier
+// is bounded: past about a second the CTA writes NaN rows (a proposal the
+// DME's fallback test rejects), sets *err and returns.
+constexpr int kTcRows = 128;
+constexpr int kTcThreads = 128;
+constexpr uint32_t kTcCols = 256;                                      // TMEM columns
+constexpr int kTcA = kTcRows * kFeat * 2;                             // 77,824 B: input tile, then activations
+constexpr int kTcW = kHidden * kHidden * 2;                           // 131,072 B: the largest weight block
+constexpr int kTcSmem = kTcA + kTcW;
+
+__device__ __forceinline__ uint32_t SmemU32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// K-major, no-swizzle UMMA shared-memory descriptor (sm_100 version bit 46).
+__device__ __forceinline__ uint64_t UmmaDesc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor: BF16 x BF16 -> FP32, both K-major, M = 128.
+__host__ __device__ constexpr uint32_t UmmaIdesc(int n)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kTcRows >> 4) << 24);
+}
+
+__device__ __forceinline__ void UmmaBf16(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
+{
+    asm volatile("{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                 :: "r"(d), "l"(a), "l"(b), "r"(idesc), "r"(acc) : "memory");
+}
+
+__device__ __forceinline__ bool MbarTryWait(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+    return ok != 0;
+}
+
+// All threads: wait for the MMAs committed to `bar` (phase `parity`); false
+// (for every thread) when any thread gave up.
+__device__ __forceinline__ bool WaitMmas(uint32_t bar, uint32_t parity)
+{
+    const long long t0 = clock64();
+    bool ok = false;
+    while (!(ok = MbarTryWait(bar, parity)))
+        if (clock64() - t0 > 4000000000ll) break;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    return !__syncthreads_or(!ok);
+}
+
+// Issued by one thread: D[tmem] (+)= A (128 x K) . B (N x K)^T over K / 16 steps.
+__device__ __forceinline__ void MmaChain(uint32_t d, uint32_t a, uint32_t b, int k, int n, uint32_t bar)
+{
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t sbo = (uint32_t)k * 16u, idesc = UmmaIdesc(n);
+    for (int s = 0; s < k / 16; ++s)
+        UmmaBf16(d, UmmaDesc(a + s * 256u, 128u, sbo), UmmaDesc(b + s * 256u, 128u, sbo), idesc, s > 0);
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" :: "r"(bar)
+                 : "memory");
+}
+
+// Byte offset of 16-byte chunk c (columns 8c..8c+7) of row r in a K-column tile.
+__device__ __forceinline__ uint32_t CoreOffset(int r, int c, int k)
+{
+    return (uint32_t)((r >> 3) * k * 16 + c * 128 + (r & 7) * 16);
+}
+
+// rows x k BF16 weights (row stride k) into the canonical layout, 32 bytes a task.
+__device__ __forceinline__ void StageWeights(const __nv_bfloat16* __restrict__ w, int rows, int k, uint8_t* dst)
+{
+    const int pairs = k / 16;
+    for (int t = threadIdx.x; t < rows * pairs; t += kTcThreads)
+    {
+        const int r8 = t & 7, rest = t >> 3, c2 = rest % pairs, g = rest / pairs, r = g * 8 + r8;
+        const uint4* src = reinterpret_cast<const uint4*>(w + (size_t)r * k + c2 * 16);
+        const uint4 lo = __ldg(src), hi = __ldg(src + 1);
+        *reinterpret_cast<uint4*>(dst + CoreOffset(r, 2 * c2, k)) = lo;
+        *reinterpret_cast<uint4*>(dst + CoreOffset(r, 2 * c2 + 1, k)) = hi;
+    }
+}
+
+// The standardised input tile (rows past n are 0), as InputKernel rounds it.
+__device__ __forceinline__ void StageInput(const float* __restrict__ feat, long row0, long n,
+                                           const float* __restrict__ mean, const float* __restrict__ scale,
+                                           uint8_t* dst)
+{
+    const int pairs = kFeat / 16;
+    for (int t = threadIdx.x; t < kTcRows * pairs; t += kTcThreads)
+    {
+        const int r8 = t & 7, rest = t >> 3, c2 = rest % pairs, g = rest / pairs, r = g * 8 + r8;
+        uint32_t packed[8];
+        if (row0 + r < n)
+        {
+            const float4* src = reinterpret_cast<const float4*>(feat + (row0 + r) * kFeat + c2 * 16);
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+            {
+                const float4 v = __ldg(src + q);
+                const int c = c2 * 16 + q * 4;
+                const __nv_bfloat16 a = __float2bfloat16_rn((v.x - mean[c]) / scale[c]);
+                const __nv_bfloat16 b = __float2bfloat16_rn((v.y - mean[c + 1]) / scale[c + 1]);
+                const __nv_bfloat16 e = __float2bfloat16_rn((v.z - mean[c + 2]) / scale[c + 2]);
+                const __nv_bfloat16 f = __float2bfloat16_rn((v.w - mean[c + 3]) / scale[c + 3]);
+                packed[2 * q] = Pack2(a, b);
+                packed[2 * q + 1] = Pack2(e, f);
+            }
+        }
+        else
+        {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) packed[q] = 0;
+        }
+        *reinterpret_cast<uint4*>(dst + CoreOffset(r, 2 * c2, kFeat)) =
+            make_uint4(packed[0], packed[1], packed[2], packed[3]);
+        *reinterpret_cast<uint4*>(dst + CoreOffset(r, 2 * c2 + 1, kFeat)) =
+            make_uint4(packed[4], packed[5], packed[6], packed[7]);
+    }
+}
+
+// Generic-proxy shared-memory writes made visible to the tensor cores, then a
+// CTA barrier (with the TMEM reads before it ordered).
+__device__ __forceinline__ void PublishShared()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+}
+
+// 32 accumulator columns [col, col + 32) of this thread's row.
+__device__ __forceinline__ void TmemLoad32(uint32_t taddr, float (&v)[32])
+{
+    uint32_t r[32];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                 "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                 "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                   "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                   "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                   "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Hidden-layer epilogue: bias, GELU, BF16 into the A tile (K = 256 layout).
+__device__ __forceinline__ void HiddenEpilogue(uint32_t tbase, const float* __restrict__ bias, uint8_t* a)
+{
+    const int warp = threadIdx.x >> 5, r = threadIdx.x;
+    for (int c0 = 0; c0 < kHidden; c0 += 32)
+    {
+        float v[32];
+        TmemLoad32(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+        {
+            uint32_t p[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                const int c = c0 + q * 8 + 2 * j;
+                const float z0 = v[q * 8 + 2 * j] + bias[c], z1 = v[q * 8 + 2 * j + 1] + bias[c + 1];
+                p[j] = Pack2(__float2bfloat16_rn(GeluTanh(z0)), __float2bfloat16_rn(GeluTanh(z1)));
+            }
+            *reinterpret_cast<uint4*>(a + CoreOffset(r, c0 / 8 + q, kHidden)) = make_uint4(p[0], p[1], p[2], p[3]);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1) ForwardTcKernel(const float* __restrict__ feat, long n,
+                                                                 const float* __restrict__ inMean,
+                                                                 const float* __restrict__ inScale,
+                                                                 const __nv_bfloat16* __restrict__ wb,
+                                                                 const float* __restrict__ master,
+                                                                 float* __restrict__ out, int* err)
+{
+    extern __shared__ __align__(1024) uint8_t tcSmem[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmemSlot;
+    uint8_t* A = tcSmem;
+    uint8_t* W = tcSmem + kTcA;
+    const uint32_t aAddr = SmemU32(A), wAddr = SmemU32(W), barAddr = SmemU32(&bar);
+    const int warp = threadIdx.x >> 5;
+    const long row0 = (long)blockIdx.x * kTcRows;
+    const long myRow = row0 + threadIdx.x;
+
+    if (warp == 0)
+    {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(SmemU32(&tmemSlot)), "r"(kTcCols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (threadIdx.x == 0)
+    {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(barAddr) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    StageInput(feat, row0, n, inMean, inScale, A);
+    StageWeights(wb + kOffW1, kHidden / 2, kFeat, W);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    PublishShared();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tbase = tmemSlot;
+
+    bool ok = true;
+    uint32_t parity = 0;
+    // layer 1, columns 0..127 then 128..255
+    for (int half = 0; half < 2 && ok; ++half)
+    {
+        if (half)
+        {
+            StageWeights(wb + kOffW1 + (size_t)(kHidden / 2) * kFeat, kHidden / 2, kFeat, W);
+            PublishShared();
+        }
+        if (threadIdx.x == 0) MmaChain(tbase + (uint32_t)(half * 128), aAddr, wAddr, kFeat, 128, barAddr);
+        ok = WaitMmas(barAddr, parity);
+        parity ^= 1;
+    }
+    // layer 2
+    if (ok)
+    {
+        HiddenEpilogue(tbase, master + kOffB1, A);
+        StageWeights(wb + kOffW2, kHidden, kHidden, W);
+        PublishShared();
+        if (threadIdx.x == 0) MmaChain(tbase, aAddr, wAddr, kHidden, kHidden, barAddr);
+        ok = WaitMmas(barAddr, parity);
+        parity ^= 1;
+    }
+    // layer 3
+    if (ok)
+    {
+        HiddenEpilogue(tbase, master + kOffB2, A);
+        StageWeights(wb + kOffW3, kOut, kHidden, W);
+        PublishShared();
+        if (threadIdx.x == 0) MmaChain(tbase, aAddr, wAddr, kHidden, kOut, barAddr);
+        ok = WaitMmas(barAddr, parity);
+    }
+    if (ok)
+    {
+        float v[32];
+        TmemLoad32(tbase + ((uint32_t)(warp * 32) << 16), v);
+        if (myRow < n)
+        {
+            float4* o = reinterpret_cast<float4*>(out + myRow * kOut);
+            const float* b3 = master + kOffB3;
+#pragma unroll
+            for (int q = 0; q < kOut / 4; ++q)
+                o[q] = make_float4(v[4 * q] + b3[4 * q], v[4 * q + 1] + b3[4 * q + 1], v[4 * q + 2] + b3[4 * q + 2],
+                                   v[4 * q + 3] + b3[4 * q + 3]);
+        }
+    }
+    else
+    {
+        if (threadIdx.x == 0) atomicCAS(err, 0, HW_ERR_TIMEOUT);
+        if (myRow < n)
+            for (int q = 0; q < kOut; ++q) out[myRow * kOut + q] = __int_as_float(0x7fc00000);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tbase), "r"(kTcCols) : "memory");
+}
+
 // ---- training helpers ---------------------------------------------------------
 
 // Network input: rows idx[i] (or i) of the features, standardised, as bf16.
@@ -340,16 +630,6 @@ namespace {
 
 using namespace hwk;
 
-// Parameter layout (floats): W1 [256][304], b1 [256], W2 [256][256], b2 [256],
-// W3 [32][256], b3 [32].  Rows 19..31 of W3 and b3 stay 0.
-constexpr size_t kOffW1 = 0;
-constexpr size_t kOffB1 = kOffW1 + (size_t)kHidden * kFeat;
-constexpr size_t kOffW2 = kOffB1 + kHidden;
-constexpr size_t kOffB2 = kOffW2 + (size_t)kHidden * kHidden;
-constexpr size_t kOffW3 = kOffB2 + kHidden;
-constexpr size_t kOffB3 = kOffW3 + (size_t)kOut * kHidden;
-constexpr size_t kParams = kOffB3 + kOut;
-
 int Cuda(cudaError_t e, const char* where)
 {
     if (e == cudaSuccess) return HW_OK;
@@ -390,6 +670,7 @@ struct hw_learned_init
     float* dY = nullptr;
     float* dA = nullptr;       // [maxBatch][256] hidden gradient
     float* loss = nullptr;
+    int* err = nullptr;        // set by the tensor-core forward pass when a wait timed out
 
     float* InMean() const { return norm; }
     float* InScale() const { return norm + kFeat; }
@@ -400,7 +681,7 @@ struct hw_learned_init
     {
         cudaFree(master); cudaFree(grad); cudaFree(m); cudaFree(v); cudaFree(wb); cudaFree(norm);
         cudaFree(X); cudaFree(Z1); cudaFree(H1); cudaFree(Z2); cudaFree(H2); cudaFree(Y); cudaFree(T);
-        cudaFree(dY); cudaFree(dA); cudaFree(loss);
+        cudaFree(dY); cudaFree(dA); cudaFree(loss); cudaFree(err);
     }
 
     // Forward pass of n <= maxBatch rows (rows idx[i], or i, of feat): outputs in Y.
@@ -465,7 +746,8 @@ int hw_learned_init_create(uint32_t max_batch, uint64_t seed, hw_learned_init** 
     alloc(&h->wb, kParams); alloc(&h->norm, 2 * kFeat + 2 * kOut);
     alloc(&h->X, B * kFeat); alloc(&h->Z1, B * kHidden); alloc(&h->H1, B * kHidden); alloc(&h->Z2, B * kHidden);
     alloc(&h->H2, B * kHidden); alloc(&h->Y, B * kOut); alloc(&h->T, B * kOut); alloc(&h->dY, B * kOut);
-    alloc(&h->dA, B * kHidden); alloc(&h->loss, 1);
+    alloc(&h->dA, B * kHidden); alloc(&h->loss, 1); alloc(&h->err, 1);
+    if (!rc) rc = Cuda(cudaMemset(h->err, 0, sizeof(int)), "hw_learned_init_create");
     if (rc) { delete h; return rc; }
     // He-normal weights (std sqrt(2 / fan_in)) from a seeded host generator,
     // zero biases, zero rows for the unused outputs.
@@ -557,14 +839,31 @@ int hw_learned_init_targets(const hw_config* cfg, uint32_t lanes, const float* d
 int hw_learned_init_forward(hw_learned_init* h, const float* d_features, uint32_t n, float* d_out, void* stream)
 {
     if (!h || !d_features || !d_out) return SetLastError(HW_ERR_INVALID_ARG, "bad argument");
+    if (n == 0) return HW_OK;
     cudaStream_t s = (cudaStream_t)stream;
-    for (uint32_t i0 = 0; i0 < n; i0 += h->maxBatch)
+    static bool attr = false;
+    if (!attr)
     {
-        const int b = (int)std::min(h->maxBatch, n - i0);
-        int rc = Cuda(h->Forward(d_features + (size_t)i0 * kFeat, nullptr, b, s), "hw_learned_init_forward");
-        if (!rc) rc = Cuda(cudaMemcpyAsync(d_out + (size_t)i0 * kOut, h->Y, (size_t)b * kOut * 4,
-                                           cudaMemcpyDeviceToDevice, s), "hw_learned_init_forward");
+        const int rc = Cuda(cudaFuncSetAttribute(ForwardTcKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem),
+                            "hw_learned_init_forward");
         if (rc) return rc;
+        attr = true;
+    }
+    ForwardTcKernel<<<(n + kTcRows - 1) / kTcRows, kTcThreads, kTcSmem, s>>>(
+        d_features, (long)n, h->InMean(), h->InScale(), h->wb, h->master, d_out, h->err);
+    return Cuda(cudaGetLastError(), "hw_learned_init_forward");
+}
+
+int hw_learned_init_forward_status(hw_learned_init* h)
+{
+    if (!h) return SetLastError(HW_ERR_INVALID_ARG, "bad argument");
+    int e = 0;
+    int rc = Cuda(cudaMemcpy(&e, h->err, sizeof(int), cudaMemcpyDeviceToHost), "hw_learned_init_forward_status");
+    if (rc) return rc;
+    if (e)
+    {
+        cudaMemset(h->err, 0, sizeof(int));
+        return SetLastError(e, "hw_learned_init_forward: a tensor-core wait timed out (rows written as NaN)");
     }
     return HW_OK;
 }

@@ -187,6 +187,11 @@ class Network:
         check(lib().hw_learned_init_forward(self._h, Fl._p(feats), feats.shape[0], Fl._p(out), Fl._stream()))
         return out
 
+    def forward_status(self):
+        """Raises if a forward pass since the last call gave up a bounded
+        tensor-core wait (its rows are NaN)."""
+        check(lib().hw_learned_init_forward_status(self._h))
+
     def proposal(self, pool, out):
         P = torch.empty((pool.lanes, 15, abi.LANE), dtype=torch.float32, device="cuda")
         check(lib().hw_learned_init_proposal(self._h, pool.lanes, Fl._p(out), Fl._p(pool.hist), Fl._p(P),

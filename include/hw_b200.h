@@ -455,8 +455,14 @@ int hw_learned_init_features(uint32_t lanes, const hw_lane_histogram* d_hist, co
 /* Targets from fitted parameters d_params [lanes][15][64] (hw_dme_em_fit layout). */
 int hw_learned_init_targets(const hw_config* cfg, uint32_t lanes, const float* d_params,
                             const hw_lane_histogram* d_hist, float* d_targets, void* stream);
-/* Standardised outputs of n rows (processed max_batch rows at a time). */
+/* Standardised outputs d_out [n][32] of n rows (any n): one fused launch of
+ * 128-row tiles on the tensor cores (tcgen05, accumulators in tensor memory;
+ * BF16 inputs and activations, FP32 accumulation).  Asynchronous. */
 int hw_learned_init_forward(hw_learned_init* h, const float* d_features, uint32_t n, float* d_out, void* stream);
+/* Synchronous: HW_ERR_TIMEOUT (and the flag cleared) when a forward pass
+ * since the last call gave up a bounded tensor-core wait -- its rows were
+ * written as NaN, which the learned start's fallback test rejects. */
+int hw_learned_init_forward_status(hw_learned_init* h);
 /* EM start [lanes][15][64] from the outputs of lanes * 64 rows. */
 int hw_learned_init_proposal(const hw_learned_init* h, uint32_t lanes, const float* d_out,
                              const hw_lane_histogram* d_hist, float* d_proposal, void* stream);

@@ -93,6 +93,7 @@ def test_forward_and_gradients_match_reference():
     feat = rng.standard_normal((n, R.FEAT)).astype(np.float32)
     tgt = rng.standard_normal((n, R.OUT)).astype(np.float32)
     y = net.forward(_dev(feat)).cpu().numpy()
+    net.forward_status()
     y_ref, _ = R.forward(p, norm, feat)
     err = np.abs(y - y_ref)
     assert err.max() <= 2e-2 * np.abs(y_ref).max() and np.median(err) <= 2e-3 * np.abs(y_ref).mean()
