@@ -661,8 +661,6 @@ struct hw_analyzer
     bool diagValid = false;
     // learned EM start (hw_analyzer_set_learned_init), not owned
     hw_learned_init* net = nullptr;
-    float* lFeat = nullptr;     // [lanes * 64][304]
-    float* lOut = nullptr;      // [lanes * 64][32]
     float* lProp = nullptr;     // [lanes][15][64]
     hw_frame_interval modelFi{0, 0};
     int status = HIST_INIT;
@@ -715,7 +713,7 @@ struct hw_analyzer
         hw_pulse_accumulator_destroy(pa);
         cudaFree(bls); cudaFree(stats); cudaFree(models); cudaFree(labels); cudaFree(latent);
         cudaFree(score); cudaFree(paStats); cudaFree(diag);
-        cudaFree(lFeat); cudaFree(lOut); cudaFree(lProp);
+        cudaFree(lProp);
     }
 
     // DetectionModelEstimator::AddBatch
@@ -749,9 +747,7 @@ struct hw_analyzer
                 t = Begin(HW_STAGE_DME, s);
                 if (net)
                 {
-                    if ((rc = hw_learned_init_features(lanes, hist->hist, agg->acc, lFeat, s))) return rc;
-                    if ((rc = hw_learned_init_forward(net, lFeat, lanes * kLane, lOut, s))) return rc;
-                    if ((rc = hw_learned_init_proposal(net, lanes, lOut, hist->hist, lProp, s))) return rc;
+                    if ((rc = hw_learned_init_propose(net, lanes, hist->hist, agg->acc, lProp, s))) return rc;
                     if ((rc = hw_dme_estimate_proposal(dme, hist->hist, agg->acc, hist->fi, modelFi, models, diag,
                                                        lProp, s))) return rc;
                 }
@@ -836,13 +832,10 @@ int hw_analyzer_create(const hw_config* cfg, uint32_t pool_id, uint32_t lanes, u
 int hw_analyzer_set_learned_init(hw_analyzer* a, hw_learned_init* net)
 {
     if (!a) return Fail(HW_ERR_INVALID_ARG, "NULL analyzer");
-    if (net && !a->lFeat)
+    if (net && !a->lProp)
     {
-        const size_t n = (size_t)a->lanes * kLane;
-        int rc;
-        if ((rc = DevAlloc(&a->lFeat, n * 304, "hw_analyzer_set_learned_init"))) return rc;
-        if ((rc = DevAlloc(&a->lOut, n * 32, "hw_analyzer_set_learned_init"))) return rc;
-        if ((rc = DevAlloc(&a->lProp, (size_t)a->lanes * 15 * kLane, "hw_analyzer_set_learned_init"))) return rc;
+        const int rc = DevAlloc(&a->lProp, (size_t)a->lanes * 15 * kLane, "hw_analyzer_set_learned_init");
+        if (rc) return rc;
     }
     a->net = net;
     return HW_OK;

@@ -353,6 +353,10 @@ __device__ __forceinline__ void DmePrelude(const KParams& k, const hw_lane_model
 // density finite: llb <= max(pref) + log(5), so finite prefactors, means and
 // inverse variances with max(pref) < 80 guarantee it (`safe`).  Otherwise the
 // reference path runs.
+//
+// kFull = false computes the log-likelihood alone (the same bits): no
+// responsibilities, sums or scratch, for the start that is only compared.
+template <bool kFull = true>
 __device__ __forceinline__ float EmEStep(const KParams& k, const EmHist& h, const EmVars& v, const EmReg& r,
                                          float* bpS, float* tau0S, float* facS, float ci[5], float mom1[5],
                                          float varinv[5], bool& safeOut)
@@ -415,7 +419,7 @@ __device__ __forceinline__ float EmEStep(const KParams& k, const EmHist& h, cons
         tmax = fmax_sse(tmax, t4);
         const uint32_t nCur = nNext;
         nNext = (b + 1 < kBins) ? h.Count(b + 1) : 0u;
-        const bool needTau = (nPrev != 0u) | (nCur != 0u) | !safe;
+        const bool needTau = kFull & ((nPrev != 0u) | (nCur != 0u) | !safe);
         // Far tails: with every t finite and below -106, llb = tmax +
         // log(se) with 1 <= se <= 5 stays below -104.3, where hw_expf
         // returns exactly 0, so bp is 0 without evaluating it.
@@ -450,7 +454,9 @@ __device__ __forceinline__ float EmEStep(const KParams& k, const EmHist& h, cons
             const int c = b - 1;
             const float bpr = fmax_sse(mul_rn(mul_rn(0.5f, h.binSize), add_rn(bpPrev, bp)), h.binProbMin);
             probSum = add_rn(probSum, bpr);
-            if ((nPrev != 0u) | !safe)
+            if (!kFull && ((nPrev != 0u) | !safe))
+                wps = add_rn(wps, mul_rn((float)nPrev, hw_logf(bpr)));
+            if (kFull && ((nPrev != 0u) | !safe))
             {
                 const float njb = (float)nPrev;
                 wps = add_rn(wps, mul_rn(njb, hw_logf(bpr)));
@@ -575,17 +581,17 @@ __device__ __forceinline__ void EmMStep(const KParams& k, const EmHist& h, const
 
 // The learned start: replaces the reference start v by the proposal column Q
 // unless the proposal's log-likelihood is lower (or not comparable); returns
-// 1 when it kept the reference start.  Reports both log-likelihoods.  When
-// the proposal is kept, ci/mom1/varinv/safe and the per-bin scratch hold its
-// E-step, which is the first EM iteration's E-step from that start.
+// 1 when it kept the reference start.  Reports both log-likelihoods.  The
+// proposal's E-step is the full one and the reference start's only its
+// log-likelihood, so when the proposal is kept, ci/mom1/varinv/safe and the
+// per-bin scratch hold its E-step, which is the first EM iteration's E-step
+// from that start.
 __device__ __forceinline__ int ChooseStart(const KParams& k, const EmHist& h, const EmReg& r, const float* Q, bool fallback,
                                            float* bpS, float* tau0S, float* facS, EmVars& v, float& llPlain,
                                            float& llStart, float (&ci)[5], float (&mom1)[5], float (&varinv)[5],
                                            bool& safe)
 {
     const int z = h.z;
-    llPlain = EmEStep(k, h, v, r, bpS, tau0S, facS, ci, mom1, varinv, safe);
-    llStart = llPlain;
     EmVars p;
 #pragma unroll
     for (int i = 0; i < 5; ++i)
@@ -596,6 +602,12 @@ __device__ __forceinline__ int ChooseStart(const KParams& k, const EmHist& h, co
     }
     p.s = EmScale(k, p.mu);
     const float llProp = EmEStep(k, h, p, r, bpS, tau0S, facS, ci, mom1, varinv, safe);
+    {
+        float ciX[5], momX[5], vinvX[5];
+        bool safeX;
+        llPlain = EmEStep<false>(k, h, v, r, bpS, tau0S, facS, ciX, momX, vinvX, safeX);
+    }
+    llStart = llPlain;
     if (fallback && !(llProp >= llPlain)) return 1;
     v = p;
     llStart = llProp;
@@ -649,11 +661,13 @@ __global__ void __launch_bounds__(kLane, 10) DmeEstimateKernel(DmeArgs A, KParam
     float ci[5], mom1[5], varinv[5];
     bool safe = false, haveE = false;
     float llE = 0.0f;
+    int fellBack = 0;
     if (A.proposal)
     {
         float llPlain;
         haveE = !ChooseStart(k, h, r, A.proposal + (size_t)l * 15 * kLane, true, bpS, tau0S, facS, v, llPlain, llE,
                              ci, mom1, varinv, safe);
+        fellBack = __syncthreads_count(!haveE);
     }
     lap(1);
 
@@ -795,9 +809,7 @@ __global__ void __launch_bounds__(kLane, 10) DmeEstimateKernel(DmeArgs A, KParam
         for (int i = 0; i < 5; ++i) P[i] = tc[i];
         P[5] = laneIters;
         P[6] = tMark - tBegin;
-        unsigned smid;
-        asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
-        P[7] = smid;
+        P[7] = fellBack;
     }
 }
 

@@ -277,7 +277,7 @@ struct DmeArgs
     LaneMap map{};
     // Optional per-lane phase clock [lanes][8] (SM cycles, thread 0 of the
     // lane): prelude, start choice, E-steps, M-steps, confidence and blend,
-    // lane iterations, whole lane, SM id.
+    // lane iterations, whole lane, ZMWs that kept the reference start.
     long long* phases = nullptr;
 };
 

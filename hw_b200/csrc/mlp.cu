@@ -45,6 +45,33 @@ constexpr size_t kParams = kOffB3 + kOut;
 // consecutive threads write consecutive addresses.
 constexpr int kFeatThreads = 256;
 
+// Per ZMW: the inverse of the in-range count total and the two baseline
+// features (shared by the features kernel and the fused proposal).
+__device__ __forceinline__ void FeatureRow(const hw_lane_histogram& H, const hw_baseliner_stats& st, int z,
+                                           float& inv, float& fMean, float& fVar)
+{
+    float total = 0.0f;
+    for (int b = 0; b < kBins; ++b) total += (float)H.bin_count[b][z];
+    inv = total > 0.0f ? 1.0f / total : 0.0f;
+    const float lb = H.low_bound[z], bs = H.bin_size[z];
+    const hw_stat_accum_state& S = st.baseline_stats;
+    const float m0 = S.moment0[z], m1 = S.moment1[z], m2 = S.moment2[z];
+    const float mean = m0 > 0.0f ? m1 / m0 + S.offset[z] : lb;
+    const float var = m0 > 1.0f ? fmaxf((m2 - m1 * m1 / m0) / (m0 - 1.0f), 0.0f) : bs * bs;
+    const float fm = (mean - lb) / bs, fv = var / (bs * bs);
+    fMean = isfinite(fm) ? fm : 0.0f;
+    fVar = isfinite(fv) ? fv : 0.0f;
+}
+
+__device__ __forceinline__ float FeatureValue(const hw_lane_histogram& H, int z, int b, float inv, float fMean,
+                                              float fVar)
+{
+    if (b < kBins) return sqrtf((float)H.bin_count[b][z] * inv);
+    if (b == kBins) return fMean;
+    if (b == kBins + 1) return fVar;
+    return 0.0f;
+}
+
 __global__ void __launch_bounds__(kFeatThreads) FeaturesKernel(const hw_lane_histogram* __restrict__ hist,
                                                                const hw_baseliner_stats* __restrict__ st,
                                                                float* __restrict__ out)
@@ -52,32 +79,13 @@ __global__ void __launch_bounds__(kFeatThreads) FeaturesKernel(const hw_lane_his
     const int l = blockIdx.x, tid = threadIdx.x;
     const hw_lane_histogram& H = hist[l];
     __shared__ float inv[kLane], fMean[kLane], fVar[kLane];
-    if (tid < kLane)
-    {
-        const int z = tid;
-        float total = 0.0f;
-        for (int b = 0; b < kBins; ++b) total += (float)H.bin_count[b][z];
-        inv[z] = total > 0.0f ? 1.0f / total : 0.0f;
-        const float lb = H.low_bound[z], bs = H.bin_size[z];
-        const hw_stat_accum_state& S = st[l].baseline_stats;
-        const float m0 = S.moment0[z], m1 = S.moment1[z], m2 = S.moment2[z];
-        const float mean = m0 > 0.0f ? m1 / m0 + S.offset[z] : lb;
-        const float var = m0 > 1.0f ? fmaxf((m2 - m1 * m1 / m0) / (m0 - 1.0f), 0.0f) : bs * bs;
-        const float fm = (mean - lb) / bs, fv = var / (bs * bs);
-        fMean[z] = isfinite(fm) ? fm : 0.0f;
-        fVar[z] = isfinite(fv) ? fv : 0.0f;
-    }
+    if (tid < kLane) FeatureRow(H, st[l], tid, inv[tid], fMean[tid], fVar[tid]);
     __syncthreads();
     float* f = out + (size_t)l * kLane * kFeat;
     for (int e = tid; e < kLane * kFeat; e += kFeatThreads)
     {
         const int z = e / kFeat, b = e % kFeat;
-        float v;
-        if (b < kBins) v = sqrtf((float)H.bin_count[b][z] * inv[z]);
-        else if (b == kBins) v = fMean[z];
-        else if (b == kBins + 1) v = fVar[z];
-        else v = 0.0f;
-        f[e] = v;
+        f[e] = FeatureValue(H, z, b, inv[z], fMean[z], fVar[z]);
     }
 }
 
@@ -112,15 +120,11 @@ __global__ void TargetsKernel(const float* __restrict__ params, const hw_lane_hi
 // EM start from network outputs y [n][32] (standardised; mean/scale undo
 // the standardisation): the inverse of TargetsKernel, with fractions floored
 // at 0.001 and renormalised and variances floored at 1e-3 squared bins.
-__global__ void ProposalKernel(const float* __restrict__ y, const float* __restrict__ mean,
-                               const float* __restrict__ scale, const hw_lane_histogram* __restrict__ hist,
-                               float* __restrict__ proposal)
+__device__ __forceinline__ void ProposalFromOutputs(const float* Y, const float* __restrict__ mean,
+                                                    const float* __restrict__ scale, float lb, float bs, float* P,
+                                                    int z)
 {
-    const int l = blockIdx.x, z = threadIdx.x;
-    const float* Y = y + ((size_t)l * kLane + z) * kOut;
     auto o = [&](int i) { return Y[i] * scale[i] + mean[i]; };
-    const float lb = hist[l].low_bound[z], bs = hist[l].bin_size[z];
-    float* P = proposal + (size_t)l * 15 * kLane;
     float rs = 0.0f, r[5];
     for (int i = 0; i < 5; ++i) { r[i] = fmaxf(o(10 + i), 0.001f); rs += r[i]; }
     for (int i = 0; i < 5; ++i) P[i * kLane + z] = r[i] / rs;
@@ -131,6 +135,15 @@ __global__ void ProposalKernel(const float* __restrict__ y, const float* __restr
         P[(6 + a) * kLane + z] = lb + o(2 + a) * bs;
         P[(11 + a) * kLane + z] = bs * bs * fmaxf(expf(fminf(o(6 + a), 30.0f)), 1e-3f);
     }
+}
+
+__global__ void ProposalKernel(const float* __restrict__ y, const float* __restrict__ mean,
+                               const float* __restrict__ scale, const hw_lane_histogram* __restrict__ hist,
+                               float* __restrict__ proposal)
+{
+    const int l = blockIdx.x, z = threadIdx.x;
+    ProposalFromOutputs(y + ((size_t)l * kLane + z) * kOut, mean, scale, hist[l].low_bound[z], hist[l].bin_size[z],
+                        proposal + (size_t)l * 15 * kLane, z);
 }
 
 // ---- BF16 tensor-core GEMM ----------------------------------------------------
@@ -385,6 +398,53 @@ __device__ __forceinline__ void StageInput(const float* __restrict__ feat, long 
     }
 }
 
+// The same tile computed from the lanes' histograms and baseliner statistics
+// (FeatureRow / FeatureValue, as FeaturesKernel): rows are ZMWs of the lanes
+// row0 / 64 and the next.
+__device__ __forceinline__ void StageInputFromHist(const hw_lane_histogram* __restrict__ hist,
+                                                   const hw_baseliner_stats* __restrict__ st, long row0, long n,
+                                                   const float* __restrict__ mean, const float* __restrict__ scale,
+                                                   uint8_t* dst, float* rowInv, float* rowMean, float* rowVar)
+{
+    {
+        const long row = row0 + threadIdx.x;
+        if (row < n)
+            FeatureRow(hist[row / kLane], st[row / kLane], (int)(row % kLane), rowInv[threadIdx.x],
+                       rowMean[threadIdx.x], rowVar[threadIdx.x]);
+    }
+    __syncthreads();
+    const int pairs = kFeat / 16;
+    for (int t = threadIdx.x; t < kTcRows * pairs; t += kTcThreads)
+    {
+        const int r8 = t & 7, rest = t >> 3, c2 = rest % pairs, g = rest / pairs, r = g * 8 + r8;
+        uint32_t packed[8];
+        const long row = row0 + r;
+        if (row < n)
+        {
+            const hw_lane_histogram& H = hist[row / kLane];
+            const int z = (int)(row % kLane);
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+            {
+                const int c = c2 * 16 + 2 * q;
+                const float f0 = FeatureValue(H, z, c, rowInv[r], rowMean[r], rowVar[r]);
+                const float f1 = FeatureValue(H, z, c + 1, rowInv[r], rowMean[r], rowVar[r]);
+                packed[q] = Pack2(__float2bfloat16_rn((f0 - mean[c]) / scale[c]),
+                                  __float2bfloat16_rn((f1 - mean[c + 1]) / scale[c + 1]));
+            }
+        }
+        else
+        {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) packed[q] = 0;
+        }
+        *reinterpret_cast<uint4*>(dst + CoreOffset(r, 2 * c2, kFeat)) =
+            make_uint4(packed[0], packed[1], packed[2], packed[3]);
+        *reinterpret_cast<uint4*>(dst + CoreOffset(r, 2 * c2 + 1, kFeat)) =
+            make_uint4(packed[4], packed[5], packed[6], packed[7]);
+    }
+}
+
 // Generic-proxy shared-memory writes made visible to the tensor cores, then a
 // CTA barrier (with the TMEM reads before it ordered).
 __device__ __forceinline__ void PublishShared()
@@ -436,16 +496,34 @@ __device__ __forceinline__ void HiddenEpilogue(uint32_t tbase, const float* __re
     }
 }
 
-__global__ void __launch_bounds__(kTcThreads, 1) ForwardTcKernel(const float* __restrict__ feat, long n,
-                                                                 const float* __restrict__ inMean,
-                                                                 const float* __restrict__ inScale,
-                                                                 const __nv_bfloat16* __restrict__ wb,
-                                                                 const float* __restrict__ master,
-                                                                 float* __restrict__ out, int* err)
+struct TcArgs
+{
+    const float* feat;                 // [n][304] features, or
+    const hw_lane_histogram* hist;     // the lanes' histograms and statistics (n = lanes * 64)
+    const hw_baseliner_stats* stats;
+    long n;
+    const float* inMean;
+    const float* inScale;
+    const float* outMean;
+    const float* outScale;
+    const __nv_bfloat16* wb;
+    const float* master;
+    float* out;                        // [n][32] standardised outputs, or
+    float* proposal;                   // [lanes][15][64] EM starts
+    int* err;
+};
+
+// kHist: features from the histograms and the proposal written directly.
+template <bool kHist>
+__global__ void __launch_bounds__(kTcThreads, 1) ForwardTcKernel(TcArgs p)
 {
     extern __shared__ __align__(1024) uint8_t tcSmem[];
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tmemSlot;
+    __shared__ float rowInv[kTcRows], rowMean[kTcRows], rowVar[kTcRows];
+    const long n = p.n;
+    const __nv_bfloat16* __restrict__ wb = p.wb;
+    const float* __restrict__ master = p.master;
     uint8_t* A = tcSmem;
     uint8_t* W = tcSmem + kTcA;
     const uint32_t aAddr = SmemU32(A), wAddr = SmemU32(W), barAddr = SmemU32(&bar);
@@ -464,7 +542,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) ForwardTcKernel(const float* __
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(barAddr) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    StageInput(feat, row0, n, inMean, inScale, A);
+    if (kHist) StageInputFromHist(p.hist, p.stats, row0, n, p.inMean, p.inScale, A, rowInv, rowMean, rowVar);
+    else StageInput(p.feat, row0, n, p.inMean, p.inScale, A);
     StageWeights(wb + kOffW1, kHidden / 2, kFeat, W);
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     PublishShared();
@@ -508,21 +587,37 @@ __global__ void __launch_bounds__(kTcThreads, 1) ForwardTcKernel(const float* __
     {
         float v[32];
         TmemLoad32(tbase + ((uint32_t)(warp * 32) << 16), v);
+        const float* b3 = master + kOffB3;
+#pragma unroll
+        for (int q = 0; q < kOut; ++q) v[q] = v[q] + b3[q];
         if (myRow < n)
         {
-            float4* o = reinterpret_cast<float4*>(out + myRow * kOut);
-            const float* b3 = master + kOffB3;
+            if (kHist)
+            {
+                const long l = myRow / kLane;
+                const int z = (int)(myRow % kLane);
+                ProposalFromOutputs(v, p.outMean, p.outScale, p.hist[l].low_bound[z], p.hist[l].bin_size[z],
+                                    p.proposal + l * 15 * kLane, z);
+            }
+            else
+            {
+                float4* o = reinterpret_cast<float4*>(p.out + myRow * kOut);
 #pragma unroll
-            for (int q = 0; q < kOut / 4; ++q)
-                o[q] = make_float4(v[4 * q] + b3[4 * q], v[4 * q + 1] + b3[4 * q + 1], v[4 * q + 2] + b3[4 * q + 2],
-                                   v[4 * q + 3] + b3[4 * q + 3]);
+                for (int q = 0; q < kOut / 4; ++q) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            }
         }
     }
     else
     {
-        if (threadIdx.x == 0) atomicCAS(err, 0, HW_ERR_TIMEOUT);
+        if (threadIdx.x == 0) atomicCAS(p.err, 0, HW_ERR_TIMEOUT);
         if (myRow < n)
-            for (int q = 0; q < kOut; ++q) out[myRow * kOut + q] = __int_as_float(0x7fc00000);
+        {
+            const float nan = __int_as_float(0x7fc00000);
+            if (kHist)
+                for (int q = 0; q < 15; ++q) p.proposal[(myRow / kLane) * 15 * kLane + q * kLane + myRow % kLane] = nan;
+            else
+                for (int q = 0; q < kOut; ++q) p.out[myRow * kOut + q] = nan;
+        }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -684,6 +779,29 @@ struct hw_learned_init
         cudaFree(dY); cudaFree(dA); cudaFree(loss); cudaFree(err);
     }
 
+    // The fused tensor-core forward pass over a.n rows.
+    template <bool kHist>
+    int LaunchTc(TcArgs a, cudaStream_t s, const char* where)
+    {
+        static bool attr = false;
+        if (!attr)
+        {
+            const int rc = Cuda(cudaFuncSetAttribute(ForwardTcKernel<kHist>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     kTcSmem), where);
+            if (rc) return rc;
+            attr = true;
+        }
+        a.inMean = InMean();
+        a.inScale = InScale();
+        a.outMean = OutMean();
+        a.outScale = OutScale();
+        a.wb = wb;
+        a.master = master;
+        a.err = err;
+        ForwardTcKernel<kHist><<<(unsigned)((a.n + kTcRows - 1) / kTcRows), kTcThreads, kTcSmem, s>>>(a);
+        return Cuda(cudaGetLastError(), where);
+    }
+
     // Forward pass of n <= maxBatch rows (rows idx[i], or i, of feat): outputs in Y.
     cudaError_t Forward(const float* feat, const int32_t* idx, int n, cudaStream_t s)
     {
@@ -840,18 +958,24 @@ int hw_learned_init_forward(hw_learned_init* h, const float* d_features, uint32_
 {
     if (!h || !d_features || !d_out) return SetLastError(HW_ERR_INVALID_ARG, "bad argument");
     if (n == 0) return HW_OK;
-    cudaStream_t s = (cudaStream_t)stream;
-    static bool attr = false;
-    if (!attr)
-    {
-        const int rc = Cuda(cudaFuncSetAttribute(ForwardTcKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem),
-                            "hw_learned_init_forward");
-        if (rc) return rc;
-        attr = true;
-    }
-    ForwardTcKernel<<<(n + kTcRows - 1) / kTcRows, kTcThreads, kTcSmem, s>>>(
-        d_features, (long)n, h->InMean(), h->InScale(), h->wb, h->master, d_out, h->err);
-    return Cuda(cudaGetLastError(), "hw_learned_init_forward");
+    TcArgs a{};
+    a.feat = d_features;
+    a.n = n;
+    a.out = d_out;
+    return h->LaunchTc<false>(a, (cudaStream_t)stream, "hw_learned_init_forward");
+}
+
+int hw_learned_init_propose(hw_learned_init* h, uint32_t lanes, const hw_lane_histogram* d_hist,
+                            const hw_baseliner_stats* d_stats, float* d_proposal, void* stream)
+{
+    if (!h || !d_hist || !d_stats || !d_proposal) return SetLastError(HW_ERR_INVALID_ARG, "bad argument");
+    if (lanes == 0) return HW_OK;
+    TcArgs a{};
+    a.hist = d_hist;
+    a.stats = d_stats;
+    a.n = (long)lanes * kLane;
+    a.proposal = d_proposal;
+    return h->LaunchTc<true>(a, (cudaStream_t)stream, "hw_learned_init_propose");
 }
 
 int hw_learned_init_forward_status(hw_learned_init* h)

@@ -192,6 +192,14 @@ class Network:
         tensor-core wait (its rows are NaN)."""
         check(lib().hw_learned_init_forward_status(self._h))
 
+    def propose(self, pool):
+        """Features, forward pass and EM start in one launch
+        (hw_learned_init_propose); equals proposal(pool, forward(features(pool)))."""
+        P = torch.empty((pool.lanes, 15, abi.LANE), dtype=torch.float32, device="cuda")
+        check(lib().hw_learned_init_propose(self._h, pool.lanes, Fl._p(pool.hist), Fl._p(pool.stats), Fl._p(P),
+                                            Fl._stream()))
+        return P
+
     def proposal(self, pool, out):
         P = torch.empty((pool.lanes, 15, abi.LANE), dtype=torch.float32, device="cuda")
         check(lib().hw_learned_init_proposal(self._h, pool.lanes, Fl._p(out), Fl._p(pool.hist), Fl._p(P),
@@ -345,7 +353,7 @@ def dme_phases(net, pool, pool_id=0, sm_mhz=None):
         ev[0].record()
         prop = None
         if use_net:
-            prop = net.proposal(pool, net.forward(features(pool)))
+            prop = net.propose(pool)
         ev[1].record()
         if use_net:
             dme.estimate_proposal(pool.hist, pool.hist_fi, pool.stats, models, pool.model_fi, prop, diag=False)
@@ -362,6 +370,9 @@ def dme_phases(net, pool, pool_id=0, sm_mhz=None):
                "lanes_at_iteration_limit": float((it >= cfg.em_iteration_limit).mean()),
                "phase_share": {n: float(ph[:, i].sum() / tot) for i, n in enumerate(names)},
                "lane_cycles_mean": float(ph[:, 6].mean()), "lane_cycles_max": int(ph[:, 6].max())}
+        if use_net:
+            out["zmws_kept_reference_start"] = float(ph[:, 7].sum() / (lanes * abi.LANE))
+            out["lanes_with_a_kept_reference_start"] = float((ph[:, 7] > 0).mean())
         return out
 
     one(False), one(True)   # warm-up: module loading and first-launch costs

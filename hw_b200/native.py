@@ -126,6 +126,7 @@ def lib():
         "hw_learned_init_targets": ([PCFG, u32, vp, vp, vp, vp], C.c_int),
         "hw_learned_init_forward": ([vp, vp, u32, vp, vp], C.c_int),
         "hw_learned_init_forward_status": ([vp], C.c_int),
+        "hw_learned_init_propose": ([vp, u32, vp, vp, vp, vp], C.c_int),
         "hw_learned_init_proposal": ([vp, u32, vp, vp, vp, vp], C.c_int),
         "hw_learned_init_gradients": ([vp, vp, vp, vp, u32, vp, C.POINTER(C.c_float), vp], C.c_int),
         "hw_learned_init_train_step": ([vp, vp, vp, vp, u32, C.c_float, C.c_float, C.POINTER(C.c_float), vp],

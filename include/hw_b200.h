@@ -341,10 +341,12 @@ int hw_dme_estimate_proposal(hw_dme* d, const hw_lane_histogram* d_hist, const h
  * reference): with profiling on, every hw_dme_estimate /
  * hw_dme_estimate_proposal records for each lane, in SM clock cycles of the
  * lane's first thread: [0] model evolution, preliminary estimate and EM
- * set-up, [1] the start choice of a proposal (its two E-steps), [2] the
- * E-steps with the lane-wide convergence vote, [3] the M-steps, [4] the
- * confidence, blend and export, [5] the lane's EM iterations, [6] the whole
- * lane, [7] the SM the lane ran on.  hw_dme_phase_cycles copies the
+ * set-up, [1] the start choice of a proposal (the proposal's E-step, which
+ * the first iteration reuses when the proposal is kept, and the reference
+ * start's log-likelihood), [2] the E-steps with the lane-wide convergence
+ * vote, [3] the M-steps, [4] the confidence, blend and export, [5] the
+ * lane's EM iterations, [6] the whole lane, [7] the lane's ZMWs that kept
+ * the reference start.  hw_dme_phase_cycles copies the
  * [lanes][8] int64 table to host memory (synchronous). */
 int hw_dme_profile_phases(hw_dme* d, int enable);
 int hw_dme_phase_cycles(const hw_dme* d, int64_t* host_out, void* stream);
@@ -463,6 +465,12 @@ int hw_learned_init_forward(hw_learned_init* h, const float* d_features, uint32_
  * since the last call gave up a bounded tensor-core wait -- its rows were
  * written as NaN, which the learned start's fallback test rejects. */
 int hw_learned_init_forward_status(hw_learned_init* h);
+/* Features, forward pass and EM start of lanes * 64 ZMWs in one launch:
+ * equal to hw_learned_init_features -> hw_learned_init_forward ->
+ * hw_learned_init_proposal without the [n][304] and [n][32] intermediates.
+ * Asynchronous (hw_learned_init_forward_status reports a timed-out wait). */
+int hw_learned_init_propose(hw_learned_init* h, uint32_t lanes, const hw_lane_histogram* d_hist,
+                            const hw_baseliner_stats* d_stats, float* d_proposal, void* stream);
 /* EM start [lanes][15][64] from the outputs of lanes * 64 rows. */
 int hw_learned_init_proposal(const hw_learned_init* h, uint32_t lanes, const float* d_out,
                              const hw_lane_histogram* d_hist, float* d_proposal, void* stream);

@@ -77,6 +77,31 @@ def test_features_targets_and_proposal_kernels_match_reference():
 
 
 @pytest.mark.gpu
+def test_fused_proposal_equals_the_three_steps():
+    """hw_learned_init_propose (features, tensor-core forward pass and EM
+    start in one launch) gives the bits of features -> forward -> proposal,
+    on an odd lane count (a half-filled last tile) and a random network."""
+    from hw_b200 import filters as Fl, learned_init as L
+    cfg, _, (hist, stats, hfi, mfi, models) = _dme_inputs(seed=6, lanes=3)
+    lanes = hist.shape[0]
+    pool = L.Pool(cfg, lanes, Fl.numpy_to_struct(hist), Fl.numpy_to_struct(stats), hfi, Fl.numpy_to_struct(models),
+                  mfi)
+    rng = np.random.default_rng(9)
+    p, norm = _random_net(rng, scale=0.7)
+    norm[:R.FEAT] = 0.05 * rng.standard_normal(R.FEAT)
+    norm[R.FEAT:2 * R.FEAT] = rng.uniform(0.5, 2.0, R.FEAT)
+    norm[2 * R.FEAT:2 * R.FEAT + R.OUT_USED] = rng.standard_normal(R.OUT_USED)
+    norm[2 * R.FEAT + R.OUT:2 * R.FEAT + R.OUT + R.OUT_USED] = rng.uniform(0.5, 2.0, R.OUT_USED)
+    net = L.Network(max_batch=256, seed=3)
+    net.set(p, norm)
+    three = net.proposal(pool, net.forward(L.features(pool))).cpu().numpy()
+    fused = net.propose(pool).cpu().numpy()
+    net.forward_status()
+    assert np.isfinite(three).all()
+    assert three.tobytes() == fused.tobytes()
+
+
+@pytest.mark.gpu
 def test_forward_and_gradients_match_reference():
     """BF16 tensor-core forward and backward against the CPU reference with
     the same BF16 rounding points; they differ only by FP32 accumulation order
