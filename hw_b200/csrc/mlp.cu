@@ -50,8 +50,11 @@ constexpr int kFeatThreads = 256;
 __device__ __forceinline__ void FeatureRow(const hw_lane_histogram& H, const hw_baseliner_stats& st, int z,
                                            float& inv, float& fMean, float& fVar)
 {
-    float total = 0.0f;
-    for (int b = 0; b < kBins; ++b) total += (float)H.bin_count[b][z];
+    // the integer total (below 2^24 for any histogram the accumulator fills,
+    // so equal to the float sum in any order)
+    uint32_t count = 0;
+    for (int b = 0; b < kBins; ++b) count += H.bin_count[b][z];
+    const float total = (float)count;
     inv = total > 0.0f ? 1.0f / total : 0.0f;
     const float lb = H.low_bound[z], bs = H.bin_size[z];
     const hw_stat_accum_state& S = st.baseline_stats;
@@ -281,7 +284,7 @@ __global__ void __launch_bounds__(128) GemmKernel(const TA* __restrict__ A, long
 // is bounded: past about a second the CTA writes NaN rows (a proposal the
 // DME's fallback test rejects), sets *err and returns.
 constexpr int kTcRows = 128;
-constexpr int kTcThreads = 128;
+constexpr int kTcThreads = 512;        // 16 warps: warp w reads TMEM lanes 32 (w % 4) .. + 31
 constexpr uint32_t kTcCols = 256;                                      // TMEM columns
 constexpr int kTcA = kTcRows * kFeat * 2;                             // 77,824 B: input tile, then activations
 constexpr int kTcW = kHidden * kHidden * 2;                           // 131,072 B: the largest weight block
@@ -406,6 +409,7 @@ __device__ __forceinline__ void StageInputFromHist(const hw_lane_histogram* __re
                                                    const float* __restrict__ mean, const float* __restrict__ scale,
                                                    uint8_t* dst, float* rowInv, float* rowMean, float* rowVar)
 {
+    if (threadIdx.x < kTcRows)
     {
         const long row = row0 + threadIdx.x;
         if (row < n)
@@ -473,13 +477,14 @@ __device__ __forceinline__ void TmemLoad32(uint32_t taddr, float (&v)[32])
 }
 
 // Hidden-layer epilogue: bias, GELU, BF16 into the A tile (K = 256 layout).
+// Warp w takes row 32 (w % 4) + lane, columns 64 (w / 4) .. + 63.
 __device__ __forceinline__ void HiddenEpilogue(uint32_t tbase, const float* __restrict__ bias, uint8_t* a)
 {
-    const int warp = threadIdx.x >> 5, r = threadIdx.x;
-    for (int c0 = 0; c0 < kHidden; c0 += 32)
+    const int warp = threadIdx.x >> 5, quad = warp & 3, r = quad * 32 + (threadIdx.x & 31);
+    for (int c0 = (warp >> 2) * 64; c0 < (warp >> 2) * 64 + 64; c0 += 32)
     {
         float v[32];
-        TmemLoad32(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+        TmemLoad32(tbase + ((uint32_t)(quad * 32) << 16) + (uint32_t)c0, v);
 #pragma unroll
         for (int q = 0; q < 4; ++q)
         {
@@ -529,7 +534,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) ForwardTcKernel(TcArgs p)
     const uint32_t aAddr = SmemU32(A), wAddr = SmemU32(W), barAddr = SmemU32(&bar);
     const int warp = threadIdx.x >> 5;
     const long row0 = (long)blockIdx.x * kTcRows;
-    const long myRow = row0 + threadIdx.x;
+    // the output rows: warps 0..3, one row a thread
+    const bool outWarp = warp < 4;
+    const long myRow = row0 + (threadIdx.x & (kTcRows - 1));
 
     if (warp == 0)
     {
@@ -583,7 +590,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) ForwardTcKernel(TcArgs p)
         if (threadIdx.x == 0) MmaChain(tbase, aAddr, wAddr, kHidden, kOut, barAddr);
         ok = WaitMmas(barAddr, parity);
     }
-    if (ok)
+    if (ok && outWarp)
     {
         float v[32];
         TmemLoad32(tbase + ((uint32_t)(warp * 32) << 16), v);
@@ -607,10 +614,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) ForwardTcKernel(TcArgs p)
             }
         }
     }
-    else
+    else if (!ok)
     {
         if (threadIdx.x == 0) atomicCAS(p.err, 0, HW_ERR_TIMEOUT);
-        if (myRow < n)
+        if (outWarp && myRow < n)
         {
             const float nan = __int_as_float(0x7fc00000);
             if (kHist)
