@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned-init", action="store_true",
                     help="skip the learned DME initializer measurement (config 3)")
+    ap.add_argument("--no-other-configs", action="store_true",
+                    help="skip the uneven-pool (config 2) and streaming (config 4) measurements")
     ap.add_argument("--engine", choices=["fused", "analyzers"], default="fused",
                     help="fused: all pools through hw_chunk_fused; analyzers: one hw_analyzer per pool")
     return ap.parse_args()
@@ -559,14 +561,47 @@ def main():
     for a in profiled:
         a.close()
     learned = None
+    net = None
     if rank == 0 and world == 1 and not args.no_learned_init:
         # BASELINE metric part 2: EM iterations from the learned start vs the
         # plain start (2.1M training ZMWs of the uneven-pool generator,
         # 262K held-out ZMWs), measured after the timed regions.
         from hw_b200 import learned_init
         t0 = time.time()
-        _, learned = learned_init.run()
+        net, learned = learned_init.run()
         learned["seconds"] = time.time() - t0
+        ph = learned.get("dme_phases", {})
+        if ph:
+            learned["dme_stage_ms_4096_lanes"] = {
+                "plain_start": ph["plain"]["estimate_ms"],
+                "learned_start": ph["learned"]["network_ms"] + ph["learned"]["estimate_ms"]}
+
+    other = None
+    if rank == 0 and world == 1 and not args.no_other_configs:
+        # the other single-GPU configurations, after the timed regions: uneven
+        # pools through the tuned fused engine, and the streaming run with
+        # the reference start and (when trained above) the learned start
+        from hw_b200 import streaming, uneven, workloads
+        other = {}
+        t0 = time.time()
+        u = uneven.run(variants=("fused_tuned",))
+        other["uneven_pools"] = {k: u[k] for k in ("pools", "zmws", "lanes_min", "lanes_max", "chunk_lengths",
+                                                   "timed_steps", "warmup_steps", "fused_tuned_ms_per_step",
+                                                   "fused_tuned_zmw_frames_per_s", "fused_tuned_launches_per_step")}
+        other["uneven_pools"]["workload"] = ("500 pools, lanes log-uniform in [1, 2048], chunks of 128/256/512 "
+                                             "frames, uneven-pool generator, dynamic DME")
+        other["uneven_pools"]["seconds"] = time.time() - t0
+        t0 = time.time()
+        scfg = workloads.chip_config()
+        st = {"workload": "streaming: 2,097,152 ZMWs (8 pools of 4096 lanes) x 128 chunks of 512 frames, "
+                          "generated on the GPU (decay 20%, +15 DN step in 1% of ZMWs), dynamic DME",
+              "plain_em": streaming.run_chain(scfg, 8, 4096, 128)}
+        if net is not None:
+            st["learned_init"] = streaming.run_chain(scfg, 8, 4096, 128, net)
+        st["seconds"] = time.time() - t0
+        other["streaming"] = st
+    if net is not None:
+        net.close()
 
     if rank == 0:
         out = {
@@ -582,6 +617,7 @@ def main():
             "clocks": clk,
             "stage_ms": {k: v[0] / K for k, v in stage.items()},
             "learned_init": learned,
+            "other_configs": other,
         }
         print(json.dumps(out), flush=True)
     if world > 1:
