@@ -398,6 +398,48 @@ def run(train_pools=8, eval_pools=1, lanes=4096, fit_iters=1000, epochs=40, batc
     return net, metrics
 
 
+def network_timing(lanes=4096, reps=4, seed=1):
+    """Device time of the network on lanes * 64 ZMWs (synthetic histograms
+    and statistics, a randomly initialised network): the three-step path
+    (features, tensor-core forward pass, proposal) and the fused proposal,
+    each a launch; the last of `reps` repetitions is reported."""
+    rng = np.random.default_rng(seed)
+    hist = np.zeros(lanes, abi.LANE_HIST_DT)
+    hist["bin_count"] = rng.integers(0, 40, hist["bin_count"].shape)
+    hist["low_bound"] = rng.uniform(-50, 0, hist["low_bound"].shape)
+    hist["bin_size"] = rng.uniform(0.5, 2, hist["bin_size"].shape)
+    st = np.zeros(lanes, abi.BLSTATS_DT)
+    st["baseline_stats"]["moment0"] = 1000.0
+    st["baseline_stats"]["moment1"] = 3000.0
+    st["baseline_stats"]["moment2"] = 30000.0
+    pool = Pool(data_config(), lanes, torch.from_numpy(hist.view(np.uint8)).cuda(),
+                torch.from_numpy(st.view(np.uint8)).cuda(), None, None, None)
+    net = Network(max_batch=4096, seed=seed)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        ev[0].record()
+        f = features(pool)
+        ev[1].record()
+        y = net.forward(f)
+        ev[2].record()
+        p3 = net.proposal(pool, y)
+        ev[3].record()
+        pf = net.propose(pool)
+        ev[4].record()
+        ev[4].synchronize()
+    net.forward_status()
+    rows = lanes * abi.LANE
+    fwd = ev[1].elapsed_time(ev[2])
+    flops = 2.0 * rows * (FEAT * 256 + 256 * 256 + 256 * OUT)
+    out = {"rows": rows, "features_ms": ev[0].elapsed_time(ev[1]), "forward_ms": fwd,
+           "proposal_ms": ev[2].elapsed_time(ev[3]), "fused_propose_ms": ev[3].elapsed_time(ev[4]),
+           "forward_tflops": flops / (fwd / 1e3) / 1e12,
+           "fused_equals_three_steps": bool(torch.equal(p3, pf))}
+    net.close()
+    return out
+
+
 if __name__ == "__main__":
     import argparse
     import json
@@ -408,7 +450,11 @@ if __name__ == "__main__":
     ap.add_argument("--fit-iters", type=int, default=1000)
     ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--save", default=None)
+    ap.add_argument("--network-timing", action="store_true", help="time the network alone (no training)")
     a = ap.parse_args()
+    if a.network_timing:
+        print(json.dumps(network_timing(a.lanes)))
+        raise SystemExit(0)
     net, m = run(a.train_pools, a.eval_pools, a.lanes, a.fit_iters, a.epochs, log=print)
     if a.save:
         net.save(a.save)
