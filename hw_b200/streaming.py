@@ -74,6 +74,7 @@ def run_chain(cfg, pools, lpp, chunks, net=None):
         "analysis_ms_per_chunk": ana_ms / chunks,
         "generation_ms_per_chunk": gen_ms / chunks,
         "dme_ms_total": stage.get("dme", (0.0, 0))[0],
+        "stage_ms_per_chunk": {k: v[0] / chunks for k, v in stage.items()},
         "estimates": estimates,
         "em_lane_iterations_mean": float(it.mean()),
         "emitting_pool_chunks": emitted,
