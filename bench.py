@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--next-rows", action="store_true",
                     help="time the HF metrics, repacking, BAZ and preliminary HQ stages, GPU and CPU")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-groups", type=int, default=4,
+                    help="pool groups the end-to-end leg pipelines its copies over (fused engine)")
     ap.add_argument("--no-learned-init", action="store_true",
                     help="skip the learned DME initializer measurement (config 3)")
     ap.add_argument("--no-other-configs", action="store_true",
@@ -461,6 +463,39 @@ def main():
             c += 1
         torch.cuda.synchronize()
         KE = K
+        # Copy/compute pipelining over pool groups: each group's chunk slice
+        # is uploaded, analysed and downloaded on its own, so a step's first
+        # upload and last download cover one group, not the whole chip.  With
+        # the fused engine each group is its own engine (same pool ids, so
+        # the same estimation stagger), brought to this chunk untimed.
+        G = max(1, min(args.e2e_groups, args.pools)) if args.engine == "fused" else args.pools
+        if args.pools % G:
+            G = 1
+        ppg = args.pools // G
+        if args.engine == "fused" and G > 1:
+            units = []
+            for g in range(G):
+                ids = list(range(g * ppg, (g + 1) * ppg))
+                eg = Fl.FusedEngine(cfg, [lpp] * ppg, [FRAMES] * ppg, pool_ids=ids)
+                eg.enable_hf_metrics(4096, cfg.frame_rate, True, cart)
+                units.append((eg, ids))
+            for cc in range(c):
+                gen.next(cc * FRAMES, FRAMES, out=buf)
+                for eg, ids in units:
+                    eg.process([buf[p * lpp:(p + 1) * lpp] for p in ids])
+            torch.cuda.synchronize()
+        elif args.engine == "fused":
+            units = [(engine, list(range(args.pools)))]
+        else:
+            units = [(analyzers[p], [p]) for p in range(args.pools)]
+
+        def run_unit(u, chunk_slice, outs):
+            eg, ids = units[u]
+            if args.engine == "fused":
+                eg.process([chunk_slice[i * lpp:(i + 1) * lpp] for i in range(len(ids))], outs)
+            else:
+                eg(chunk_slice, (c + k) * FRAMES, *outs[0])
+
         host_chunks = []
         tmp = torch.empty((total_lanes, FRAMES, 64), dtype=torch.int16, device="cuda")
         for k in range(min(KE, 16)):
@@ -469,9 +504,12 @@ def main():
             h.copy_(tmp)
             host_chunks.append(h)
         del tmp
-        in_dev = [torch.empty((total_lanes, FRAMES, 64), dtype=torch.int16, device="cuda") for _ in range(2)]
-        out_dev = [[(torch.empty_like(dp), torch.empty_like(dl), torch.empty_like(do)) for dp, dl, do in outputs]
-                   for _ in range(2)]
+        U = len(units)
+        rows = [(units[u][1][0] * lpp, (units[u][1][-1] + 1) * lpp) for u in range(U)]
+        in_dev = [[torch.empty((r1 - r0, FRAMES, 64), dtype=torch.int16, device="cuda") for r0, r1 in rows]
+                  for _ in range(2)]
+        out_dev = [[[(torch.empty_like(outputs[p][0]), torch.empty_like(outputs[p][1]),
+                      torch.empty_like(outputs[p][2])) for p in units[u][1]] for u in range(U)] for _ in range(2)]
         host_out = [(torch.empty(dp.numel(), dtype=torch.uint8, pin_memory=True),
                      torch.empty(dl.shape, dtype=torch.int32, pin_memory=True),
                      torch.empty(do.shape, dtype=torch.int32, pin_memory=True)) for dp, dl, do in outputs]
@@ -479,9 +517,9 @@ def main():
                    if args.engine == "fused" else [])
         metrics_bytes = 0
         s_h2d, s_d2h = torch.cuda.Stream(), torch.cuda.Stream()
-        ev_h2d = [torch.cuda.Event() for _ in range(2)]
-        ev_comp = [torch.cuda.Event() for _ in range(2)]
-        ev_d2h = [torch.cuda.Event() for _ in range(2)]
+        ev_h2d = [[torch.cuda.Event() for _ in range(U)] for _ in range(2)]
+        ev_comp = [[torch.cuda.Event() for _ in range(U)] for _ in range(2)]
+        ev_d2h = [[torch.cuda.Event() for _ in range(U)] for _ in range(2)]
         torch.cuda.synchronize()
         barrier()
         e0.record(stream)
@@ -489,29 +527,35 @@ def main():
         s_d2h.wait_stream(stream)
         for k in range(KE):
             b = k % 2
-            with torch.cuda.stream(s_h2d):
+            src = host_chunks[k % len(host_chunks)]
+            for u in range(U):
+                r0, r1 = rows[u]
+                with torch.cuda.stream(s_h2d):
+                    if k >= 2:
+                        s_h2d.wait_event(ev_comp[b][u])     # step k-2 has read in_dev[b][u]
+                    in_dev[b][u].copy_(src[r0:r1], non_blocking=True)
+                    ev_h2d[b][u].record(s_h2d)
+                stream.wait_event(ev_h2d[b][u])
                 if k >= 2:
-                    s_h2d.wait_event(ev_comp[b])        # step k-2 has read in_dev[b]
-                in_dev[b].copy_(host_chunks[k % len(host_chunks)], non_blocking=True)
-                ev_h2d[b].record(s_h2d)
-            stream.wait_event(ev_h2d[b])
-            if k >= 2:
-                stream.wait_event(ev_d2h[b])            # step k-2's outputs are on the host
-            run_chunk(in_dev[b], c + k, out_dev[b])
-            ev_comp[b].record(stream)
-            with torch.cuda.stream(s_d2h):
-                s_d2h.wait_event(ev_comp[b])
-                for (dp, dl, do), (hp, hl, ho) in zip(out_dev[b], host_out):
-                    hl.copy_(dl, non_blocking=True)
-                    ho.copy_(do, non_blocking=True)
-                    hp.copy_(dp, non_blocking=True)
-                if args.engine == "fused":
-                    # HF metrics records of the pools that completed a block
-                    for p, em in enumerate(engine.metrics_emitted()):
-                        if em:
-                            hf_host[p].copy_(engine.metrics[p], non_blocking=True)
-                            metrics_bytes += engine.metrics[p].numel()
-                ev_d2h[b].record(s_d2h)
+                    stream.wait_event(ev_d2h[b][u])         # step k-2's outputs are on the host
+                run_unit(u, in_dev[b][u], out_dev[b][u])
+                ev_comp[b][u].record(stream)
+                with torch.cuda.stream(s_d2h):
+                    s_d2h.wait_event(ev_comp[b][u])
+                    for p, (dp, dl, do) in zip(units[u][1], out_dev[b][u]):
+                        hp, hl, ho = host_out[p]
+                        hl.copy_(dl, non_blocking=True)
+                        ho.copy_(do, non_blocking=True)
+                        hp.copy_(dp, non_blocking=True)
+                    if args.engine == "fused":
+                        # HF metrics records of the pools that completed a block
+                        eg = units[u][0]
+                        for i, em in enumerate(eg.metrics_emitted()):
+                            if em:
+                                p = units[u][1][i]
+                                hf_host[p].copy_(eg.metrics[i], non_blocking=True)
+                                metrics_bytes += eg.metrics[i].numel()
+                    ev_d2h[b][u].record(s_d2h)
         stream.wait_stream(s_d2h)
         e1.record(stream)
         torch.cuda.synchronize()
@@ -523,8 +567,14 @@ def main():
         e2e = {"value": zf_step * KE * world / (ms_e2e / 1e3), "unit": "ZMW-frames/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / KE, "steps": KE,
                "phase": "same K steps of the estimation cycle as value",
-               "overlap": "copies on their own streams, double-buffered against the analysis; the first "
-                          "upload and the last download overlap no analysis"}
+               "overlap": f"copies on their own streams, double-buffered against the analysis, pipelined over "
+                          f"{U} pool group(s) of {ppg * lpp} lanes (one engine each); a step's first upload and "
+                          f"last download cover one group"}
+        if args.engine == "fused":
+            for eg, _ in units:
+                if eg is not engine:
+                    eg.finish()
+                    eg.close()
         del host_chunks, in_dev, out_dev
 
     # Roofline of the dominant kernel (the frame labeler) from the live stage timers.
