@@ -520,6 +520,7 @@ def main():
         ev_h2d = [[torch.cuda.Event() for _ in range(U)] for _ in range(2)]
         ev_comp = [[torch.cuda.Event() for _ in range(U)] for _ in range(2)]
         ev_d2h = [[torch.cuda.Event() for _ in range(U)] for _ in range(2)]
+        ev_step = [torch.cuda.Event(enable_timing=True) for _ in range(KE)]
         torch.cuda.synchronize()
         barrier()
         e0.record(stream)
@@ -556,17 +557,23 @@ def main():
                                 hf_host[p].copy_(eg.metrics[i], non_blocking=True)
                                 metrics_bytes += eg.metrics[i].numel()
                     ev_d2h[b][u].record(s_d2h)
+            ev_step[k].record(stream)
         stream.wait_stream(s_d2h)
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
         ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+        # where the time went: the analysis of step k ends at ev_step[k]
+        marks = [e0.elapsed_time(ev) for ev in ev_step]
+        timeline = {"first_step_done_ms": marks[0],
+                    "step_ms_after_first": [b_ - a_ for a_, b_ in zip(marks, marks[1:])],
+                    "last_download_ms": ms_e2e - marks[-1]}
         c += KE
         h2d = total_lanes * FRAMES * 64 * 2
         d2h = sum(dp.numel() + dl.numel() * 4 + do.numel() * 4 for dp, dl, do in outputs) + metrics_bytes // KE
         e2e = {"value": zf_step * KE * world / (ms_e2e / 1e3), "unit": "ZMW-frames/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / KE, "steps": KE,
-               "phase": "same K steps of the estimation cycle as value",
+               "phase": "same K steps of the estimation cycle as value", "timeline": timeline,
                "overlap": f"copies on their own streams, double-buffered against the analysis, pipelined over "
                           f"{U} pool group(s) of {ppg * lpp} lanes (one engine each); a step's first upload and "
                           f"last download cover one group"}
