@@ -177,7 +177,7 @@ __device__ __forceinline__ float NineWayRow(const KParams& k, float score, const
     for (int q = 2; q < 6; ++q)
     {
         const int p0 = 2 * q + 1;          // sources p0, p0 + 1
-        const float2 v = add2(f2(add_rn(score, k.trans[R][p0]), add_rn(score, k.trans[R][p0 + 1])), ll.p[q]);
+        const float2 v = add2(add2(f2(score), f2(k.trans[R][p0], k.trans[R][p0 + 1])), ll.p[q]);
         Pick<Margin>(v.x, (uint32_t)(p0 - 4) << shift, mv, sv, c);
         Pick<Margin>(v.y, (uint32_t)(p0 - 3) << shift, mv, sv, c);
     }
@@ -194,8 +194,8 @@ __device__ __forceinline__ float2 TwoWayRows(const KParams& k, float2 s, const S
 {
     constexpr int shift = (R <= 4) ? 20 + R - 1 : 24 + R - 9;
     constexpr int a0 = 2 * qa + 1, b0 = 2 * qb + 1;
-    const float2 first = add2(f2(add_rn(s.x, k.trans[R][a0]), add_rn(s.y, k.trans[R + 1][a0 + 1])), ll.p[qa]);
-    const float2 second = add2(f2(add_rn(s.x, k.trans[R][b0]), add_rn(s.y, k.trans[R + 1][b0 + 1])), ll.p[qb]);
+    const float2 first = add2(add2(s, f2(k.trans[R][a0], k.trans[R + 1][a0 + 1])), ll.p[qa]);
+    const float2 second = add2(add2(s, f2(k.trans[R][b0], k.trans[R + 1][b0 + 1])), ll.p[qb]);
     const bool gx = second.x >= first.x, gy = second.y >= first.y;
     if constexpr (Margin)
     {
