@@ -423,17 +423,20 @@ __device__ __forceinline__ float EmEStep(const KParams& k, const EmHist& h, cons
         // Far tails: with every t finite and below -106, llb = tmax +
         // log(se) with 1 <= se <= 5 stays below -104.3, where hw_expf
         // returns exactly 0, so bp is 0 without evaluating it.
-        const bool allFinite = isfinite(t01.x) & isfinite(t01.y) & isfinite(t23.x) & isfinite(t23.y) & isfinite(t4);
+        // (a finite sum means every t is finite; an infinite or NaN t, or a
+        // sum that merely overflows, only forgoes the shortcut)
+        const float2 tsum = add2(t01, t23);
+        const bool allFinite = isfinite(add_rn(add_rn(tsum.x, tsum.y), t4));
         const bool tail = !needTau & allFinite & (tmax < -106.0f);
         float bp = 0.0f, llb = 0.0f;
         if (!tail)
         {
             const float2 ntmax = f2(-tmax);
-            const float2 e01 = hw_expf2(add2(t01, ntmax), nz), e23 = hw_expf2(add2(t23, ntmax), nz);
+            const float2 e01 = hw_expf2_np(add2(t01, ntmax), nz), e23 = hw_expf2_np(add2(t23, ntmax), nz);
             float se = add_rn(e01.x, e01.y);
             se = add_rn(se, e23.x);
             se = add_rn(se, e23.y);
-            se = add_rn(se, hw_expf(t4 - tmax));
+            se = add_rn(se, hw_expf_np(t4 - tmax));
             llb = add_rn(tmax, hw_logf(se));
             bp = hw_expf(llb);
         }
@@ -442,9 +445,9 @@ __device__ __forceinline__ float EmEStep(const KParams& k, const EmHist& h, cons
         if (needTau)
         {
             const float2 nllb = f2(-llb);
-            tau01 = hw_expf2(add2(t01, nllb), nz);
-            tau23 = hw_expf2(add2(t23, nllb), nz);
-            tau4 = hw_expf(t4 - llb);
+            tau01 = hw_expf2_np(add2(t01, nllb), nz);
+            tau23 = hw_expf2_np(add2(t23, nllb), nz);
+            tau4 = hw_expf_np(t4 - llb);
             bpS[(size_t)b * kLane + z] = bp;
             tau0S[(size_t)b * kLane + z] = tau01.x;
         }
@@ -614,7 +617,11 @@ __device__ __forceinline__ int ChooseStart(const KParams& k, const EmHist& h, co
     return 0;
 }
 
-template <bool Mapped>
+// Learned: the start comes from A.proposal (with the fallback test); Clock:
+// the per-lane phase clock of A.phases.  Both are compile-time so that the
+// reference-start variant carries neither the start choice's values nor the
+// clock's counters through its EM loop (they cost registers there).
+template <bool Mapped, bool Learned, bool Clock>
 __global__ void __launch_bounds__(kLane, 10) DmeEstimateKernel(DmeArgs A, KParams k)
 {
     LaneMap map = A.map;
@@ -635,7 +642,7 @@ __global__ void __launch_bounds__(kLane, 10) DmeEstimateKernel(DmeArgs A, KParam
     float* facS = tau0S + (size_t)(kBins + 1) * kLane;
 
     // phase clock (thread 0, when asked for): see DmeArgs::phases
-    const bool clk = A.phases != nullptr && z == 0;
+    const bool clk = Clock && z == 0;
     long long tc[5] = {0, 0, 0, 0, 0};
     long long tMark = clk ? clock64() : 0;
     const long long tBegin = tMark;
@@ -662,7 +669,7 @@ __global__ void __launch_bounds__(kLane, 10) DmeEstimateKernel(DmeArgs A, KParam
     bool safe = false, haveE = false;
     float llE = 0.0f;
     int fellBack = 0;
-    if (A.proposal)
+    if constexpr (Learned)
     {
         float llPlain;
         haveE = !ChooseStart(k, h, r, A.proposal + (size_t)l * 15 * kLane, true, bpS, tau0S, facS, v, llPlain, llE,
@@ -698,8 +705,16 @@ __global__ void __launch_bounds__(kLane, 10) DmeEstimateKernel(DmeArgs A, KParam
     int it = 0;
     for (; it < iterLimit; ++it)
     {
-        const float ll = haveE ? llE : EmEStep(k, h, v, r, bpS, tau0S, facS, ci, mom1, varinv, safe);
-        haveE = false;
+        float ll;
+        if constexpr (Learned)
+        {
+            ll = haveE ? llE : EmEStep(k, h, v, r, bpS, tau0S, facS, ci, mom1, varinv, safe);
+            haveE = false;
+        }
+        else
+        {
+            ll = EmEStep(k, h, v, r, bpS, tau0S, facS, ci, mom1, varinv, safe);
+        }
         const float prev = logLike;
         logLike = ll;
         const float delta = ll - prev;
@@ -817,8 +832,22 @@ cudaError_t LaunchDmeEstimate(const DmeArgs& a, const KParams& k, cudaStream_t s
 {
     const int blocks = a.map.Lanes(a.lanes);
     if (blocks == 0) return cudaSuccess;
-    if (a.map.On()) DmeEstimateKernel<true><<<blocks, kLane, 0, s>>>(a, k);
-    else DmeEstimateKernel<false><<<blocks, kLane, 0, s>>>(a, k);
+    const bool learned = a.proposal != nullptr, clock = a.phases != nullptr;
+    if (a.map.On())
+    {
+        if (learned) DmeEstimateKernel<true, true, false><<<blocks, kLane, 0, s>>>(a, k);
+        else DmeEstimateKernel<true, false, false><<<blocks, kLane, 0, s>>>(a, k);
+    }
+    else if (!clock)
+    {
+        if (learned) DmeEstimateKernel<false, true, false><<<blocks, kLane, 0, s>>>(a, k);
+        else DmeEstimateKernel<false, false, false><<<blocks, kLane, 0, s>>>(a, k);
+    }
+    else
+    {
+        if (learned) DmeEstimateKernel<false, true, true><<<blocks, kLane, 0, s>>>(a, k);
+        else DmeEstimateKernel<false, false, true><<<blocks, kLane, 0, s>>>(a, k);
+    }
     return cudaGetLastError();
 }
 

@@ -98,6 +98,57 @@ __device__ __forceinline__ float2 hw_expf2(float2 x, float2 nz)
     return out;
 }
 
+// hw_expf / hw_expf2 for arguments that are never above 0 (or NaN): the
+// E-step's exponents t - tmax and t - llb, where llb >= tmax >= t.  The
+// overflow selection of the general routine can never fire there, so it is
+// left out; every other step, and so every result, is the same.
+__device__ __forceinline__ float hw_expf_np(float x)
+{
+    const bool isNan = x != x;
+    const bool lo = x < -103.97208404541016f;
+    const float xc = (isNan | lo) ? 0.0f : x;
+    const float z = floorf(fma_rn(xc, 1.44269504088896341f, 0.5f));
+    float r = fma_rn(z, -0.693359375f, xc);
+    r = fma_rn(z, 2.12194440e-4f, r);
+    float p = 1.9875691500e-4f;
+    p = fma_rn(p, r, 1.3981999507e-3f);
+    p = fma_rn(p, r, 8.3334519073e-3f);
+    p = fma_rn(p, r, 4.1665795894e-2f);
+    p = fma_rn(p, r, 1.6666665459e-1f);
+    p = fma_rn(p, r, 5.0000001201e-1f);
+    const float r2 = mul_rn(r, r);
+    const float y = add_rn(fma_rn(p, r2, r), 1.0f);
+    float out = scale2(y, (int)z);
+    out = lo ? 0.0f : out;
+    return isNan ? x : out;
+}
+
+__device__ __forceinline__ float2 hw_expf2_np(float2 x, float2 nz)
+{
+    const bool nanX = x.x != x.x, loX = x.x < -103.97208404541016f;
+    const bool nanY = x.y != x.y, loY = x.y < -103.97208404541016f;
+    const float2 xc = f2((nanX | loX) ? 0.0f : x.x, (nanY | loY) ? 0.0f : x.y);
+    const float2 zf = fma2(xc, f2(1.44269504088896341f), f2(0.5f));
+    const float2 z = f2(floorf(zf.x), floorf(zf.y));
+    float2 r = fma2(z, f2(-0.693359375f), xc);
+    r = fma2(z, f2(2.12194440e-4f), r);
+    float2 p = fma2(f2(1.9875691500e-4f), r, f2(1.3981999507e-3f));
+    p = fma2(p, r, f2(8.3334519073e-3f));
+    p = fma2(p, r, f2(4.1665795894e-2f));
+    p = fma2(p, r, f2(1.6666665459e-1f));
+    p = fma2(p, r, f2(5.0000001201e-1f));
+    const float2 r2 = mul2(r, r);
+    const float2 y = add2(fma2(p, r2, r), f2(1.0f));
+    const int nx = (int)z.x, ny = (int)z.y;
+    const int nx1 = nx >> 1, ny1 = ny >> 1;
+    float2 out = mulz2(mul2(y, f2(pow2i(nx1), pow2i(ny1))), f2(pow2i(nx - nx1), pow2i(ny - ny1)), nz);
+    out.x = loX ? 0.0f : out.x;
+    out.y = loY ? 0.0f : out.y;
+    out.x = nanX ? x.x : out.x;
+    out.y = nanY ? x.y : out.y;
+    return out;
+}
+
 // Device error word shared by the kernels of one launch: the first failing
 // check stores its code; the host reads it after the launch.
 struct ErrWord
