@@ -553,7 +553,9 @@ __global__ void __launch_bounds__(Threads, LabelerMinBlocks(Threads)) LabelerKer
     }
     else
     {
-        int16_t* out = A.labels + map.Block(l, F) + z;
+        // the labels block sits at the chunk's offset (derived from the
+        // chunk pointer, so the lane map need not stay live through the loop)
+        int16_t* out = A.labels + (chunk - A.trace);
         for (int f0 = F - kBatch; f0 >= 0; f0 -= kBatch)
         {
             uint32_t w[kBatch];
@@ -581,7 +583,7 @@ __global__ void __launch_bounds__(Threads, LabelerMinBlocks(Threads)) LabelerKer
     for (int f = 0; f < kLatent; ++f)
     {
         const int16_t v = pl[(size_t)f * kLane];
-        if (A.latOut) A.latOut[((size_t)l * kLatent + f) * kLane + z] = v;
+        if (A.latOut) A.latOut[(pl - A.prevLat) + (size_t)f * kLane] = v;   // same [lane][frame][64] layout
         pl[(size_t)f * kLane] = chunk[(size_t)(anchor + f) * kLane];
     }
 }
