@@ -662,22 +662,6 @@ __global__ void __launch_bounds__(kLane, 10) DmeEstimateKernel(DmeArgs A, KParam
     EmReg r;
     DmePrelude(k, A.models[l], A.stats[l], h, tModel, tEst, det, v, r);
     lap(0);
-    // With a learned start that is kept, its E-step in ChooseStart is the
-    // first iteration's E-step (same start, same histogram), so the loop
-    // takes it instead of computing it again.
-    float ci[5], mom1[5], varinv[5];
-    bool safe = false, haveE = false;
-    float llE = 0.0f;
-    int fellBack = 0;
-    if constexpr (Learned)
-    {
-        float llPlain;
-        haveE = !ChooseStart(k, h, r, A.proposal + (size_t)l * 15 * kLane, true, bpS, tau0S, facS, v, llPlain, llE,
-                             ci, mom1, varinv, safe);
-        fellBack = __syncthreads_count(!haveE);
-    }
-    lap(1);
-
     // Values needed only before and after the EM iterations (the prior model
     // and the estimates at the latest converged iteration) wait in per-thread
     // shared-memory columns, which keeps them out of registers in the loop.
@@ -687,6 +671,49 @@ __global__ void __launch_bounds__(kLane, 10) DmeEstimateKernel(DmeArgs A, KParam
     auto muEst = [&](int i) -> float& { return shEst[5 + i][z]; };
     auto varEst = [&](int i) -> float& { return shEst[10 + i][z]; };
     for (int i = 0; i < 5; ++i) { rhoEst(i) = v.rho[i]; muEst(i) = v.mu[i]; varEst(i) = v.var[i]; }
+
+    // The learned start (the same decisions as ChooseStart): the reference
+    // start's log-likelihood alone, then the proposal's full E-step, which
+    // becomes the first iteration's E-step when the proposal is kept.  The
+    // reference start waits in shEst meanwhile (its scale is EmScale of its
+    // means, as DmePrelude sets it), so only one start is in registers.
+    float ci[5], mom1[5], varinv[5];
+    bool safe = false, haveE = false;
+    float llE = 0.0f;
+    int fellBack = 0;
+    if constexpr (Learned)
+    {
+        float llPlain;
+        {
+            float ciX[5], momX[5], vinvX[5];
+            bool safeX;
+            llPlain = EmEStep<false>(k, h, v, r, bpS, tau0S, facS, ciX, momX, vinvX, safeX);
+        }
+        const float* Q = A.proposal + (size_t)l * 15 * kLane;
+#pragma unroll
+        for (int i = 0; i < 5; ++i)
+        {
+            v.rho[i] = Q[i * kLane + z];
+            v.mu[i] = Q[(5 + i) * kLane + z];
+            v.var[i] = Q[(10 + i) * kLane + z];
+        }
+        v.s = EmScale(k, v.mu);
+        const float llProp = EmEStep(k, h, v, r, bpS, tau0S, facS, ci, mom1, varinv, safe);
+        haveE = llProp >= llPlain;
+        if (haveE)
+        {
+            llE = llProp;
+            for (int i = 0; i < 5; ++i) { rhoEst(i) = v.rho[i]; muEst(i) = v.mu[i]; varEst(i) = v.var[i]; }
+        }
+        else
+        {
+#pragma unroll
+            for (int i = 0; i < 5; ++i) { v.rho[i] = rhoEst(i); v.mu[i] = muEst(i); v.var[i] = varEst(i); }
+            v.s = EmScale(k, v.mu);
+        }
+        fellBack = __syncthreads_count(!haveE);
+    }
+    lap(1);
     {
         shDet[0][z] = det.bw; shDet[1][z] = det.bm; shDet[2][z] = det.bv; shDet[3][z] = det.conf;
 #pragma unroll
@@ -703,18 +730,9 @@ __global__ void __launch_bounds__(kLane, 10) DmeEstimateKernel(DmeArgs A, KParam
 
     const int iterLimit = k.emIterLimit;
     int it = 0;
-    for (; it < iterLimit; ++it)
-    {
-        float ll;
-        if constexpr (Learned)
-        {
-            ll = haveE ? llE : EmEStep(k, h, v, r, bpS, tau0S, facS, ci, mom1, varinv, safe);
-            haveE = false;
-        }
-        else
-        {
-            ll = EmEStep(k, h, v, r, bpS, tau0S, facS, ci, mom1, varinv, safe);
-        }
+    // An EM iteration after its E-step (log-likelihood ll): convergence
+    // bookkeeping, the lane vote and the M-step; true when the lane stops.
+    auto finishIteration = [&](float ll) -> bool {
         const float prev = logLike;
         logLike = ll;
         const float delta = ll - prev;
@@ -731,10 +749,26 @@ __global__ void __launch_bounds__(kLane, 10) DmeEstimateKernel(DmeArgs A, KParam
         }
         const int allDone = __syncthreads_and(mConverged | (zStatus != 0));
         lap(2);
-        if (!k.iterToLimit && allDone) break;
+        if (!k.iterToLimit && allDone) return true;
         EmMStep(k, h, r, safe, bpS, tau0S, facS, ci, mom1, varinv, v, zStatus);
         lap(3);
+        return false;
+    };
+    bool stopped = false;
+    if constexpr (Learned)
+    {
+        // the first iteration apart: a kept proposal's E-step is already done
+        // (peeled, so its values are not carried around the loop)
+        if (it < iterLimit)
+        {
+            const float ll = haveE ? llE : EmEStep(k, h, v, r, bpS, tau0S, facS, ci, mom1, varinv, safe);
+            stopped = finishIteration(ll);
+            if (!stopped) ++it;
+        }
     }
+    if (!stopped)
+        for (; it < iterLimit; ++it)
+            if (finishIteration(EmEStep(k, h, v, r, bpS, tau0S, facS, ci, mom1, varinv, safe))) break;
     const int laneIters = it + 1 < iterLimit ? it + 1 : iterLimit;
 
     if (!mConverged) zStatus |= 1;

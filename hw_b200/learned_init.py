@@ -373,6 +373,21 @@ def dme_phases(net, pool, pool_id=0, sm_mhz=None):
         if use_net:
             out["zmws_kept_reference_start"] = float(ph[:, 7].sum() / (lanes * abi.LANE))
             out["lanes_with_a_kept_reference_start"] = float((ph[:, 7] > 0).mean())
+        # the same estimate without the phase clock (the kernel variant the
+        # product runs): its launch time is the stage's
+        dme = Fl.DmeEmEstimator(cfg, pool_id, lanes)
+        models = pool.models.clone()
+        torch.cuda.synchronize()
+        ev[2].record()
+        if use_net:
+            dme.estimate_proposal(pool.hist, pool.hist_fi, pool.stats, models, pool.model_fi, prop, diag=False)
+        else:
+            dme.estimate(pool.hist, pool.hist_fi, pool.stats, models, pool.model_fi, diag=False)
+        ev[3].record()
+        ev[3].synchronize()
+        dme.close()
+        out["estimate_ms_with_clock"] = out["estimate_ms"]
+        out["estimate_ms"] = ev[2].elapsed_time(ev[3])
         return out
 
     one(False), one(True)   # warm-up: module loading and first-launch costs
