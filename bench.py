@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--next-rows", action="store_true",
                     help="time the HF metrics, repacking, BAZ and preliminary HQ stages, GPU and CPU")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-buffers", type=int, default=3,
+                    help="device input/output buffers per group in the end-to-end leg")
     ap.add_argument("--e2e-groups", type=int, default=4,
                     help="pool groups the end-to-end leg pipelines its copies over (fused engine)")
     ap.add_argument("--no-learned-init", action="store_true",
@@ -505,11 +507,12 @@ def main():
             host_chunks.append(h)
         del tmp
         U = len(units)
+        NB = max(2, args.e2e_buffers)    # input and output buffers per group: copies may run NB - 1 steps ahead
         rows = [(units[u][1][0] * lpp, (units[u][1][-1] + 1) * lpp) for u in range(U)]
         in_dev = [[torch.empty((r1 - r0, FRAMES, 64), dtype=torch.int16, device="cuda") for r0, r1 in rows]
-                  for _ in range(2)]
+                  for _ in range(NB)]
         out_dev = [[[(torch.empty_like(outputs[p][0]), torch.empty_like(outputs[p][1]),
-                      torch.empty_like(outputs[p][2])) for p in units[u][1]] for u in range(U)] for _ in range(2)]
+                      torch.empty_like(outputs[p][2])) for p in units[u][1]] for u in range(U)] for _ in range(NB)]
         host_out = [(torch.empty(dp.numel(), dtype=torch.uint8, pin_memory=True),
                      torch.empty(dl.shape, dtype=torch.int32, pin_memory=True),
                      torch.empty(do.shape, dtype=torch.int32, pin_memory=True)) for dp, dl, do in outputs]
@@ -517,9 +520,9 @@ def main():
                    if args.engine == "fused" else [])
         metrics_bytes = 0
         s_h2d, s_d2h = torch.cuda.Stream(), torch.cuda.Stream()
-        ev_h2d = [[torch.cuda.Event() for _ in range(U)] for _ in range(2)]
-        ev_comp = [[torch.cuda.Event() for _ in range(U)] for _ in range(2)]
-        ev_d2h = [[torch.cuda.Event() for _ in range(U)] for _ in range(2)]
+        ev_h2d = [[torch.cuda.Event() for _ in range(U)] for _ in range(NB)]
+        ev_comp = [[torch.cuda.Event() for _ in range(U)] for _ in range(NB)]
+        ev_d2h = [[torch.cuda.Event() for _ in range(U)] for _ in range(NB)]
         ev_step = [torch.cuda.Event(enable_timing=True) for _ in range(KE)]
         torch.cuda.synchronize()
         barrier()
@@ -527,18 +530,18 @@ def main():
         s_h2d.wait_stream(stream)
         s_d2h.wait_stream(stream)
         for k in range(KE):
-            b = k % 2
+            b = k % NB
             src = host_chunks[k % len(host_chunks)]
             for u in range(U):
                 r0, r1 = rows[u]
                 with torch.cuda.stream(s_h2d):
-                    if k >= 2:
-                        s_h2d.wait_event(ev_comp[b][u])     # step k-2 has read in_dev[b][u]
+                    if k >= NB:
+                        s_h2d.wait_event(ev_comp[b][u])     # step k-NB has read in_dev[b][u]
                     in_dev[b][u].copy_(src[r0:r1], non_blocking=True)
                     ev_h2d[b][u].record(s_h2d)
                 stream.wait_event(ev_h2d[b][u])
-                if k >= 2:
-                    stream.wait_event(ev_d2h[b][u])         # step k-2's outputs are on the host
+                if k >= NB:
+                    stream.wait_event(ev_d2h[b][u])         # step k-NB's outputs are on the host
                 run_unit(u, in_dev[b][u], out_dev[b][u])
                 ev_comp[b][u].record(stream)
                 with torch.cuda.stream(s_d2h):
@@ -574,7 +577,7 @@ def main():
         e2e = {"value": zf_step * KE * world / (ms_e2e / 1e3), "unit": "ZMW-frames/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / KE, "steps": KE,
                "phase": "same K steps of the estimation cycle as value", "timeline": timeline,
-               "overlap": f"copies on their own streams, double-buffered against the analysis, pipelined over "
+               "overlap": f"copies on their own streams, {NB} buffers deep against the analysis, pipelined over "
                           f"{U} pool group(s) of {ppg * lpp} lanes (one engine each); a step's first upload and "
                           f"last download cover one group"}
         if args.engine == "fused":
