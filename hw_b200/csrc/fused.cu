@@ -69,12 +69,19 @@ enum List
     L_LP1,        // frame labeler + pulse accumulator in one kernel, 1/2/4 lanes a block
     L_LP2,
     L_LP4,
+    L_LABEL1L,    // the same six for pools that run the DME this step (after it)
+    L_LABEL2L,
+    L_LABEL4L,
+    L_LP1L,
+    L_LP2L,
+    L_LP4L,
     L_HF,         // HF metrics filter
     L_ZERO,       // pools that emit nothing this step
     kNumLists
 };
 
 int LanesPerCta(int list) { return 1 << ((list - L_LABEL1) % 3); }
+bool FusedPulses(int list) { return (list - L_LABEL1) % 6 >= 3; }
 
 // Per pool: hw_analyzer's schedule state.
 struct PoolRt
@@ -205,6 +212,10 @@ struct hw_fused
     // captured) and replayed on the caller's stream
     bool graphs = false;
     cudaStream_t capStream = nullptr;
+    // a second stream on which the labeling of pools without an estimate
+    // runs beside the DME of the pools with one (fork and join by events)
+    cudaStream_t side = nullptr;
+    cudaEvent_t evFork = nullptr, evJoin = nullptr;
     std::map<std::vector<int64_t>, cudaGraphExec_t> graphCache;
     std::map<std::vector<int64_t>, int> planSeen;
     uint32_t lastLaunches = 0, lastGraphLaunches = 0;
@@ -240,6 +251,9 @@ struct hw_fused
         for (auto& g : graphCache) cudaGraphExecDestroy(g.second);
         for (auto e : evPool) cudaEventDestroy(e);
         if (capStream) cudaStreamDestroy(capStream);
+        if (side) cudaStreamDestroy(side);
+        if (evFork) cudaEventDestroy(evFork);
+        if (evJoin) cudaEventDestroy(evJoin);
         for (int b = 0; b < 2; ++b)
         {
             if (ev[b]) cudaEventDestroy(ev[b]);
@@ -327,7 +341,9 @@ int hw_fused::Schedule(hw_pool_chunk* table, int b, int32_t counts[kNumLists], i
             uint32_t fuse = 0, lpc = 2;
             auto t = tuning.find(P.F);
             if (t != tuning.end()) { fuse = t->second.first; lpc = t->second.second; }
-            append((fuse ? L_LP1 : L_LABEL1) + (lpc == 1 ? 0 : lpc == 2 ? 1 : 2));
+            // a pool whose models the DME replaces this step is labeled after
+            // it; the others' labeling may overlap the DME
+            append((ran ? L_LABEL1L : L_LABEL1) + (fuse ? 3 : 0) + (lpc == 1 ? 0 : lpc == 2 ? 1 : 2));
         };
         int rc = HW_OK;
         if (cfg.model_estimation_mode == HW_FIXED_ESTIMATIONS)
@@ -438,6 +454,45 @@ int hw_fused::Launch(cudaStream_t s, const int32_t counts[kNumLists], const int 
         End(t, s);
         ++n;
     }
+    // Labeling of one list (+ the pulse accumulator, fused or after it).
+    auto label = [&](int l, cudaStream_t st) -> int {
+        const bool fuse = FusedPulses(l);
+        LabelerArgs la{bls, models, labels, latent, score, latModel, latLabel, latRoi, latTrc, prevLat, tb, L,
+                       maxFList[l]};
+        la.map = map(l);
+        PulseArgs pa{labels, latent, bls, models, nullptr, nullptr, nullptr, paStats, segStart, segFirst, segLast,
+                     segMax, segTotal, segM2, segLabel, L, maxFList[l], 0};
+        pa.map = map(l);
+        size_t t = Begin(HW_STAGE_LABELER, st);
+        HWF_CUDA(LaunchLabeler(la, k, st, fuse ? &pa : nullptr, LanesPerCta(l)), "hw_chunk_fused: labeler");
+        End(t, st);
+        n += 2;
+        if (!fuse)
+        {
+            t = Begin(HW_STAGE_PULSES, st);
+            HWF_CUDA(LaunchPulses(pa, k, st), "hw_chunk_fused: pulse accumulator");
+            End(t, st);
+            ++n;
+        }
+        return HW_OK;
+    };
+    int early = 0;
+    for (int l = L_LABEL1; l <= L_LP4; ++l) early += counts[l] ? 1 : 0;
+    // With a DME this step, the other pools' labeling overlaps it on the
+    // side stream (not while the stage timers run: they time one stream)
+    const bool overlap = counts[L_DME] && early && !profiling;
+    if (overlap)
+    {
+        HWF_CUDA(cudaEventRecord(evFork, s), "hw_chunk_fused: fork");
+        HWF_CUDA(cudaStreamWaitEvent(side, evFork, 0), "hw_chunk_fused: fork");
+        for (int l = L_LABEL1; l <= L_LP4; ++l)
+            if (counts[l])
+            {
+                const int rc = label(l, side);
+                if (rc) return rc;
+            }
+        HWF_CUDA(cudaEventRecord(evJoin, side), "hw_chunk_fused: join");
+    }
     if (counts[L_DME])
     {
         DmeArgs a{hist, acc, models, diag, dmeScratch, err, L, 0, 0};
@@ -455,28 +510,13 @@ int hw_fused::Launch(cudaStream_t s, const int32_t counts[kNumLists], const int 
         End(t, s);
         n += 2;
     }
-    for (int l = L_LABEL1; l <= L_LP4; ++l)
-    {
-        if (!counts[l]) continue;
-        const bool fuse = l >= L_LP1;
-        LabelerArgs la{bls, models, labels, latent, score, latModel, latLabel, latRoi, latTrc, prevLat, tb, L,
-                       maxFList[l]};
-        la.map = map(l);
-        PulseArgs pa{labels, latent, bls, models, nullptr, nullptr, nullptr, paStats, segStart, segFirst, segLast,
-                     segMax, segTotal, segM2, segLabel, L, maxFList[l], 0};
-        pa.map = map(l);
-        size_t t = Begin(HW_STAGE_LABELER, s);
-        HWF_CUDA(LaunchLabeler(la, k, s, fuse ? &pa : nullptr, LanesPerCta(l)), "hw_chunk_fused: labeler");
-        End(t, s);
-        n += 2;
-        if (!fuse)
+    if (overlap) HWF_CUDA(cudaStreamWaitEvent(s, evJoin, 0), "hw_chunk_fused: join");
+    for (int l = overlap ? L_LABEL1L : L_LABEL1; l <= L_LP4L; ++l)
+        if (counts[l])
         {
-            t = Begin(HW_STAGE_PULSES, s);
-            HWF_CUDA(LaunchPulses(pa, k, s), "hw_chunk_fused: pulse accumulator");
-            End(t, s);
-            ++n;
+            const int rc = label(l, s);
+            if (rc) return rc;
         }
-    }
     if (counts[L_HF])
     {
         HfEngineArgs a{};
@@ -646,6 +686,9 @@ int hw_fused_create(const hw_config* cfg, uint32_t n_pools, const uint32_t* pool
         HWF_CUDA(cudaHostGetDevicePointer((void**)&f->mErr[b], f->hErr[b], 0), where);
         HWF_CUDA(cudaEventCreateWithFlags(&f->ev[b], cudaEventDisableTiming), where);
     }
+    HWF_CUDA(cudaStreamCreateWithFlags(&f->side, cudaStreamNonBlocking), where);
+    HWF_CUDA(cudaEventCreateWithFlags(&f->evFork, cudaEventDisableTiming), where);
+    HWF_CUDA(cudaEventCreateWithFlags(&f->evJoin, cudaEventDisableTiming), where);
     HWF_CUDA(cudaDeviceSynchronize(), where);
     *out = f.release();
     return HW_OK;
