@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--next-rows", action="store_true",
                     help="time the HF metrics, repacking, BAZ and preliminary HQ stages, GPU and CPU")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--overlap", type=int, default=1, choices=[0, 1, 2],
+                    help="fused engine's use of its second stream (hw_fused_set_overlap)")
     ap.add_argument("--e2e-buffers", type=int, default=3,
                     help="device input/output buffers per group in the end-to-end leg")
     ap.add_argument("--e2e-groups", type=int, default=4,
@@ -359,6 +361,7 @@ def main():
         # HF metrics included (4096-frame blocks, the reference's trained
         # activity classifier when its table is in the checkout)
         engine = Fl.FusedEngine(cfg, [lpp] * args.pools, [FRAMES] * args.pools)
+        engine.set_overlap(args.overlap)
         cart_file = os.path.join(ROOT, "hw_b200", "data", "trained_cart.npz")
         cart = dict(np.load(cart_file)) if os.path.exists(cart_file) else None
         engine.enable_hf_metrics(4096, cfg.frame_rate, True, cart)
@@ -479,6 +482,7 @@ def main():
             for g in range(G):
                 ids = list(range(g * ppg, (g + 1) * ppg))
                 eg = Fl.FusedEngine(cfg, [lpp] * ppg, [FRAMES] * ppg, pool_ids=ids)
+                eg.set_overlap(args.overlap)
                 eg.enable_hf_metrics(4096, cfg.frame_rate, True, cart)
                 units.append((eg, ids))
             for cc in range(c):

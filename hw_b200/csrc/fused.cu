@@ -212,10 +212,11 @@ struct hw_fused
     // captured) and replayed on the caller's stream
     bool graphs = false;
     cudaStream_t capStream = nullptr;
-    // a second stream on which the labeling of pools without an estimate
-    // runs beside the DME of the pools with one (fork and join by events)
+    // a second stream for the statistics merge, histogram, DME and reset,
+    // beside the main stream's initialisation and labeling (see Launch)
     cudaStream_t side = nullptr;
-    cudaEvent_t evFork = nullptr, evJoin = nullptr;
+    cudaEvent_t evFork = nullptr, evHist = nullptr, evInit = nullptr, evJoin = nullptr;
+    int overlapMode = 1;              // hw_fused_set_overlap
     std::map<std::vector<int64_t>, cudaGraphExec_t> graphCache;
     std::map<std::vector<int64_t>, int> planSeen;
     uint32_t lastLaunches = 0, lastGraphLaunches = 0;
@@ -253,6 +254,8 @@ struct hw_fused
         if (capStream) cudaStreamDestroy(capStream);
         if (side) cudaStreamDestroy(side);
         if (evFork) cudaEventDestroy(evFork);
+        if (evHist) cudaEventDestroy(evHist);
+        if (evInit) cudaEventDestroy(evInit);
         if (evJoin) cudaEventDestroy(evJoin);
         for (int b = 0; b < 2; ++b)
         {
@@ -432,30 +435,53 @@ int hw_fused::Launch(cudaStream_t s, const int32_t counts[kNumLists], const int 
             End(t, s);
             ++n;
         }
-    if (counts[L_AGG])
-    {
-        const size_t t = Begin(HW_STAGE_AGGREGATE, s);
-        HWF_CUDA(LaunchAggMerge(acc, stats, L, s, map(L_AGG)), "hw_chunk_fused: statistics merge");
-        End(t, s);
+    auto doAgg = [&](cudaStream_t st) -> int {
+        if (!counts[L_AGG]) return HW_OK;
+        const size_t t = Begin(HW_STAGE_AGGREGATE, st);
+        HWF_CUDA(LaunchAggMerge(acc, stats, L, st, map(L_AGG)), "hw_chunk_fused: statistics merge");
+        End(t, st);
         ++n;
-    }
-    if (counts[L_HIST])
-    {
-        const size_t t = Begin(HW_STAGE_HISTOGRAM, s);
-        HWF_CUDA(LaunchHistAdd(hist, edgePrev, edgeBits, bls, maxFList[L_HIST], models, L, s, map(L_HIST)),
+        return HW_OK;
+    };
+    auto doHist = [&](cudaStream_t st) -> int {
+        if (!counts[L_HIST]) return HW_OK;
+        const size_t t = Begin(HW_STAGE_HISTOGRAM, st);
+        HWF_CUDA(LaunchHistAdd(hist, edgePrev, edgeBits, bls, maxFList[L_HIST], models, L, st, map(L_HIST)),
                  "hw_chunk_fused: histogram");
-        End(t, s);
+        End(t, st);
         ++n;
-    }
-    if (counts[L_INIT])
-    {
-        const size_t t = Begin(HW_STAGE_MODEL_INIT, s);
-        HWF_CUDA(LaunchInitModels(models, acc, L, k, s, map(L_INIT)), "hw_chunk_fused: model initialisation");
-        End(t, s);
+        return HW_OK;
+    };
+    auto doInit = [&](cudaStream_t st) -> int {
+        if (!counts[L_INIT]) return HW_OK;
+        const size_t t = Begin(HW_STAGE_MODEL_INIT, st);
+        HWF_CUDA(LaunchInitModels(models, acc, L, k, st, map(L_INIT)), "hw_chunk_fused: model initialisation");
+        End(t, st);
         ++n;
-    }
+        return HW_OK;
+    };
+    auto doDme = [&](cudaStream_t st) -> int {
+        if (!counts[L_DME]) return HW_OK;
+        DmeArgs a{hist, acc, models, diag, dmeScratch, err, L, 0, 0};
+        a.map = map(L_DME);
+        const size_t t = Begin(HW_STAGE_DME, st);
+        HWF_CUDA(LaunchDmeEstimate(a, k, st), "hw_chunk_fused: DME");
+        End(t, st);
+        ++n;
+        return HW_OK;
+    };
+    auto doReset = [&](cudaStream_t st) -> int {
+        if (!counts[L_RESET]) return HW_OK;
+        const size_t t = Begin(HW_STAGE_HIST_RESET, st);
+        HWF_CUDA(LaunchHistResetStats(hist, acc, L, k, err, st, map(L_RESET)), "hw_chunk_fused: histogram reset");
+        HWF_CUDA(LaunchAggReset(acc, L, st, map(L_RESET)), "hw_chunk_fused: aggregator reset");
+        End(t, st);
+        n += 2;
+        return HW_OK;
+    };
     // Labeling of one list (+ the pulse accumulator, fused or after it).
     auto label = [&](int l, cudaStream_t st) -> int {
+        if (!counts[l]) return HW_OK;
         const bool fuse = FusedPulses(l);
         LabelerArgs la{bls, models, labels, latent, score, latModel, latLabel, latRoi, latTrc, prevLat, tb, L,
                        maxFList[l]};
@@ -476,47 +502,76 @@ int hw_fused::Launch(cudaStream_t s, const int32_t counts[kNumLists], const int 
         }
         return HW_OK;
     };
-    int early = 0;
-    for (int l = L_LABEL1; l <= L_LP4; ++l) early += counts[l] ? 1 : 0;
-    // With a DME this step, the other pools' labeling overlaps it on the
-    // side stream (not while the stage timers run: they time one stream)
-    const bool overlap = counts[L_DME] && early && !profiling;
-    if (overlap)
+    int rc;
+    const int ov = overlapMode;
+    if (profiling || ov == 0)
     {
+        // one stream in the reference's order (the stage timers time one stream)
+        if ((rc = doAgg(s)) || (rc = doHist(s)) || (rc = doInit(s)) || (rc = doDme(s)) || (rc = doReset(s))) return rc;
+        for (int l = L_LABEL1; l <= L_LP4L; ++l)
+            if ((rc = label(l, s))) return rc;
+    }
+    else if (ov == 1)
+    {
+        // Merge, histogram and initialisation in order; with a DME this step,
+        // the DME and reset run on the side stream beside the labeling of the
+        // pools without an estimate, and the estimating pools are labeled
+        // after them.
+        if ((rc = doAgg(s)) || (rc = doHist(s)) || (rc = doInit(s))) return rc;
+        int early = 0;
+        for (int l = L_LABEL1; l <= L_LP4; ++l) early += counts[l] ? 1 : 0;
+        if (counts[L_DME] && early)
+        {
+            HWF_CUDA(cudaEventRecord(evFork, s), "hw_chunk_fused: fork");
+            HWF_CUDA(cudaStreamWaitEvent(side, evFork, 0), "hw_chunk_fused: fork");
+            if ((rc = doDme(side)) || (rc = doReset(side))) return rc;
+            HWF_CUDA(cudaEventRecord(evJoin, side), "hw_chunk_fused: join");
+            for (int l = L_LABEL1; l <= L_LP4; ++l)
+                if ((rc = label(l, s))) return rc;
+            HWF_CUDA(cudaStreamWaitEvent(s, evJoin, 0), "hw_chunk_fused: join");
+        }
+        else
+        {
+            if ((rc = doDme(s)) || (rc = doReset(s))) return rc;
+            for (int l = L_LABEL1; l <= L_LP4; ++l)
+                if ((rc = label(l, s))) return rc;
+        }
+        for (int l = L_LABEL1L; l <= L_LP4L; ++l)
+            if ((rc = label(l, s))) return rc;
+    }
+    else
+    {
+        // The histogram beside the labeling too.  Side:
+        // statistics merge, histogram, DME, histogram reset.  Main: model
+        // initialisation, then the labeling of the pools without an
+        // estimate, beside the side stream's work; the estimating pools are
+        // labeled after it.  Orderings kept from the single-stream sequence:
+        // the histogram reads the models before the initialisation writes
+        // them and the initialisation reads the merged statistics (main waits
+        // for the histogram when it initialises); the DME of a pool
+        // initialised this step reads its new models and the reset clears
+        // statistics the initialisation read (side waits for the
+        // initialisation); labeling reads the DME's models (main waits for
+        // the side stream before the estimating pools' labeling).
         HWF_CUDA(cudaEventRecord(evFork, s), "hw_chunk_fused: fork");
         HWF_CUDA(cudaStreamWaitEvent(side, evFork, 0), "hw_chunk_fused: fork");
-        for (int l = L_LABEL1; l <= L_LP4; ++l)
-            if (counts[l])
-            {
-                const int rc = label(l, side);
-                if (rc) return rc;
-            }
-        HWF_CUDA(cudaEventRecord(evJoin, side), "hw_chunk_fused: join");
-    }
-    if (counts[L_DME])
-    {
-        DmeArgs a{hist, acc, models, diag, dmeScratch, err, L, 0, 0};
-        a.map = map(L_DME);
-        const size_t t = Begin(HW_STAGE_DME, s);
-        HWF_CUDA(LaunchDmeEstimate(a, k, s), "hw_chunk_fused: DME");
-        End(t, s);
-        ++n;
-    }
-    if (counts[L_RESET])
-    {
-        const size_t t = Begin(HW_STAGE_HIST_RESET, s);
-        HWF_CUDA(LaunchHistResetStats(hist, acc, L, k, err, s, map(L_RESET)), "hw_chunk_fused: histogram reset");
-        HWF_CUDA(LaunchAggReset(acc, L, s, map(L_RESET)), "hw_chunk_fused: aggregator reset");
-        End(t, s);
-        n += 2;
-    }
-    if (overlap) HWF_CUDA(cudaStreamWaitEvent(s, evJoin, 0), "hw_chunk_fused: join");
-    for (int l = overlap ? L_LABEL1L : L_LABEL1; l <= L_LP4L; ++l)
-        if (counts[l])
+        if ((rc = doAgg(side)) || (rc = doHist(side))) return rc;
+        HWF_CUDA(cudaEventRecord(evHist, side), "hw_chunk_fused: fork");
+        if (counts[L_INIT])
         {
-            const int rc = label(l, s);
-            if (rc) return rc;
+            HWF_CUDA(cudaStreamWaitEvent(s, evHist, 0), "hw_chunk_fused: fork");
+            if ((rc = doInit(s))) return rc;
         }
+        HWF_CUDA(cudaEventRecord(evInit, s), "hw_chunk_fused: fork");
+        HWF_CUDA(cudaStreamWaitEvent(side, evInit, 0), "hw_chunk_fused: fork");
+        if ((rc = doDme(side)) || (rc = doReset(side))) return rc;
+        HWF_CUDA(cudaEventRecord(evJoin, side), "hw_chunk_fused: join");
+        for (int l = L_LABEL1; l <= L_LP4; ++l)
+            if ((rc = label(l, s))) return rc;
+        HWF_CUDA(cudaStreamWaitEvent(s, evJoin, 0), "hw_chunk_fused: join");
+        for (int l = L_LABEL1L; l <= L_LP4L; ++l)
+            if ((rc = label(l, s))) return rc;
+    }
     if (counts[L_HF])
     {
         HfEngineArgs a{};
@@ -688,6 +743,8 @@ int hw_fused_create(const hw_config* cfg, uint32_t n_pools, const uint32_t* pool
     }
     HWF_CUDA(cudaStreamCreateWithFlags(&f->side, cudaStreamNonBlocking), where);
     HWF_CUDA(cudaEventCreateWithFlags(&f->evFork, cudaEventDisableTiming), where);
+    HWF_CUDA(cudaEventCreateWithFlags(&f->evHist, cudaEventDisableTiming), where);
+    HWF_CUDA(cudaEventCreateWithFlags(&f->evInit, cudaEventDisableTiming), where);
     HWF_CUDA(cudaEventCreateWithFlags(&f->evJoin, cudaEventDisableTiming), where);
     HWF_CUDA(cudaDeviceSynchronize(), where);
     *out = f.release();
@@ -872,6 +929,13 @@ int hw_chunk_fused(hw_fused* f, hw_pool_chunk* table, uint32_t n_pools, void* st
     f->lastLaunches = launches + 2;     // + the table and failure-word kernels
     f->lastGraphLaunches = graphLaunches;
     ++f->step;
+    return HW_OK;
+}
+
+int hw_fused_set_overlap(hw_fused* f, int32_t mode)
+{
+    if (!f || mode < 0 || mode > 2) return Fail(HW_ERR_INVALID_ARG, "hw_fused_set_overlap: mode must be 0, 1 or 2");
+    f->overlapMode = mode;
     return HW_OK;
 }
 

@@ -426,6 +426,11 @@ class FusedEngine(_Handle):
     def use_graphs(self, enable=True):
         check(lib().hw_fused_use_graphs(self._h, 1 if enable else 0))
 
+    def set_overlap(self, mode=1):
+        """hw_fused_set_overlap: 0 one stream, 1 (default) the DME beside the
+        labeling, 2 also the histogram."""
+        check(lib().hw_fused_set_overlap(self._h, int(mode)))
+
     def enable_hf_metrics(self, frames_per_block=4096, frame_rate=100.0, realtime_activity_labels=True, cart=None):
         """Adds the HF metrics filter; pool p's block metrics land in
         self.metrics[p] on steps where metrics_emitted()[p] is set."""

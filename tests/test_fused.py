@@ -34,13 +34,14 @@ def _same_pulses(cfg, L, a, b, lens):
     return True
 
 
-def _compare(mode, graphs, u8, steps, tuning=None):
+def _compare(mode, graphs, u8, steps, tuning=None, overlap=1):
     import torch
     from hw_b200 import filters as Fl
     cfg = workloads.small_config()
     cfg.model_estimation_mode = mode
     ids = [3 * p + 1 for p in range(len(LANES))]      # stagger classes differ from the positions
     eng = Fl.FusedEngine(cfg, LANES, FRAMES, pool_ids=ids, graphs=graphs, tuning=tuning)
+    eng.set_overlap(overlap)
     ans = [Fl.BatchAnalyzer(cfg, i, L, F) for i, L, F in zip(ids, LANES, FRAMES)]
     gens = [Fl.TraceGenerator(L, workload=2, zmw_offset=1000 * p) for p, L in enumerate(LANES)]
     emitted = estimated = 0
@@ -72,6 +73,16 @@ def test_fused_equals_per_pool_analyzers(mode):
     assert emitted > 0
     if mode != abi.FIXED_ESTIMATIONS:
         assert estimated > 0
+
+
+@pytest.mark.parametrize("overlap", [0, 1, 2])
+def test_fused_stream_overlap_modes_equal_per_pool_analyzers(overlap):
+    """Every use of the engine's second stream (one stream; the DME beside the
+    labeling; the merge, histogram and DME beside it) gives the per-pool
+    analyzers' results, with and without graph replay."""
+    for graphs in (False, True):
+        emitted, estimated, _ = _compare(abi.DYNAMIC_ESTIMATIONS, graphs=graphs, u8=False, steps=28, overlap=overlap)
+        assert emitted > 0 and estimated > 0
 
 
 def test_fused_graphs_replay_identically():
