@@ -170,26 +170,35 @@ def labeler_alg_bytes_per_zmw(F):
     return 4 * F + 96 + 64 + 12 + 32 + 48 + 4
 
 
-def cpu_baseline(cfg, lanes, steps, warmup, threads):
+def cpu_baseline(cfg, lanes, steps, warmup, threads, pools=1, lanes_per_pool=0):
     """The oracle (CPU restatement of the reference Host* path) on a sample of
     lanes of the chip workload, traces from the oracle's host generator (the
-    CUDA library is not loaded).  Returns (ZMW-frames/s, seconds timed)."""
+    CUDA library is not loaded).  The sample's lanes are split over `pools`
+    pools with the GPU run's pool ids, each the first lanes of that pool's
+    ZMW range (`lanes_per_pool` lanes a pool on the GPU), and it times the
+    same chunks: every step then carries the same share of DME estimates as
+    the GPU's, whatever the step count.  Returns (ZMW-frames/s, seconds timed)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     from hw_b200 import workloads
     oracle.set_threads(threads)
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from harness import OracleBackend, Pipeline
-    backend = OracleBackend(cfg, lanes, FRAMES, 0)
-    pipe = Pipeline(backend, cfg, 0)
-    gen = oracle.TraceGenerator(lanes, workload=1, zmw_offset=0)
-    n0 = workloads.startup_chunks(cfg, 1, FRAMES, latency=backend.startup_latency()) + warmup
+    pools = max(1, min(pools, lanes))
+    split = [lanes // pools + (1 if p < lanes % pools else 0) for p in range(pools)]
+    units = []
+    for p, lp in enumerate(split):
+        backend = OracleBackend(cfg, lp, FRAMES, p)
+        gen = oracle.TraceGenerator(lp, workload=1, zmw_offset=p * lanes_per_pool * 64)
+        units.append((Pipeline(backend, cfg, p), gen))
+    n0 = workloads.startup_chunks(cfg, pools, FRAMES, latency=units[0][0].bl_latency) + warmup
     total = n0 + steps
     t_timed = 0.0
     for c in range(total):
-        chunk = gen.next(c * FRAMES, FRAMES)
+        chunks = [gen.next(c * FRAMES, FRAMES) for _, gen in units]
         t0 = time.perf_counter()
-        pipe.process(chunk, c * FRAMES)
+        for (pipe, _), chunk in zip(units, chunks):
+            pipe.process(chunk, c * FRAMES)
         dt = time.perf_counter() - t0
         if c >= n0:
             t_timed += dt
@@ -322,9 +331,11 @@ def main():
         # The reference path on the host cores: rank 0 alone, no CUDA and no
         # collective (the other ranks exit at once).
         if rank == 0:
-            rate, secs = cpu_baseline(cfg, args.cpu_lanes, max(args.steps, 1), args.warmup, threads)
-            sample = (f"{args.cpu_lanes} lanes ({args.cpu_lanes * 64} ZMWs) of the workload x {args.steps} "
-                      f"steady-state 512-frame chunks after start-up, {secs:.1f} s of CPU time")
+            rate, secs = cpu_baseline(cfg, args.cpu_lanes, max(args.steps, 1), args.warmup, threads,
+                                      args.pools, args.lanes_per_pool)
+            sample = (f"{args.cpu_lanes} lanes ({args.cpu_lanes * 64} ZMWs) of the workload, spread over its "
+                      f"{args.pools} pools, x {args.steps} steady-state 512-frame chunks after start-up "
+                      f"(the GPU run's chunks), {secs:.1f} s of CPU time")
             zf_step = args.cpu_lanes * 64 * FRAMES
             out = {"metric": "ZMW-frames/s", "value": rate, "unit": "ZMW-frames/s", "impl": "reference",
                    "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -615,10 +626,11 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, secs = cpu_baseline(cfg, args.cpu_lanes, args.cpu_steps, args.warmup, threads)
+        rate, secs = cpu_baseline(cfg, args.cpu_lanes, args.cpu_steps, args.warmup, threads,
+                                  args.pools, args.lanes_per_pool)
         cpu = {"value": rate, "unit": "ZMW-frames/s", "cores": threads, "kind": "port",
-               "sample": f"{args.cpu_lanes} lanes ({args.cpu_lanes * 64} ZMWs) x {args.cpu_steps} "
-                         f"steady-state 512-frame chunks after start-up ({secs:.1f} s)"}
+               "sample": f"{args.cpu_lanes} lanes ({args.cpu_lanes * 64} ZMWs) spread over the {args.pools} "
+                         f"pools x {args.cpu_steps} steady-state 512-frame chunks after start-up ({secs:.1f} s)"}
 
     if args.engine == "fused":
         engine.finish()
