@@ -17,9 +17,12 @@ analyses its own chip-sized ZMW range (weak scaling, no data exchange).
 
   value : ZMW-frames/s with the chunks already in HBM
   e2e   : the same K steps through hw_chunk_fused with every step's chunk
-          copied from pinned host memory and all pulse outputs copied back
-          inside the timed region (copies on their own streams, double
-          buffered; the first upload and the last download overlap nothing)
+          copied from pinned host memory and its results copied back inside
+          the timed region: every ZMW's pulse and overflow counts, the valid
+          pulse records (packed by hw_pulses_compact; --e2e-download slots
+          copies every slot instead) and the HF metrics blocks; copies on
+          their own streams, pipelined over pool groups whose engines run on
+          two streams (the first upload and the last download overlap nothing)
 
 --impl reference times the oracle (the CPU restatement of the reference's
 Host* path) on the host cores over a lane sample of the same workload, with
@@ -74,6 +77,11 @@ def parse():
                     help="device input/output buffers per group in the end-to-end leg")
     ap.add_argument("--e2e-groups", type=int, default=4,
                     help="pool groups the end-to-end leg pipelines its copies over (fused engine)")
+    ap.add_argument("--e2e-streams", type=int, default=2,
+                    help="streams the end-to-end leg's group engines run on (group u on stream u mod n)")
+    ap.add_argument("--e2e-download", choices=["packed", "slots"], default="packed",
+                    help="end-to-end leg's pulse download: the valid records packed by hw_pulses_compact, "
+                         "or every pulse slot")
     ap.add_argument("--no-learned-init", action="store_true",
                     help="skip the learned DME initializer measurement (config 3)")
     ap.add_argument("--no-other-configs", action="store_true",
@@ -461,10 +469,10 @@ def main():
     value = zf_step * K * world / (ms / 1e3)
 
     # End-to-end through the C ABI: every step copies its chunk from pinned
-    # host memory to the device, analyses it and copies all pulse outputs back
-    # to pinned host memory.  Copies run on their own streams, double-buffered
-    # against the analysis: step k's upload and step k-1's download overlap
-    # step k's kernels.
+    # host memory to the device, analyses it and copies its results back to
+    # pinned host memory.  Copies run on their own streams, buffered against
+    # the analysis: step k's upload and step k-1's download overlap step k's
+    # kernels.
     e2e = None
     if not args.no_e2e:
         # The same K steps from the same phase of the estimation cycle as
@@ -534,38 +542,93 @@ def main():
         hf_host = ([torch.empty(m.numel(), dtype=torch.uint8, pin_memory=True) for m in engine.metrics]
                    if args.engine == "fused" else [])
         metrics_bytes = 0
+        # Packed download: hw_pulses_compact packs each pool's valid records
+        # after the analysis, and the host copies exactly that many bytes.
+        # The count is read from the compactor's mapped slot once the group's
+        # analysis has passed, a few groups after it was queued (the host
+        # stays that far ahead of the device), so the copy of those records
+        # is queued then.
+        packed = args.e2e_download == "packed"
+        max_calls = int(cfg.max_calls_per_zmw)
+        rec_bytes = outputs[0][0].numel() // (outputs[0][1].numel() * max_calls)
+        if packed:
+            compactors = [Fl.PulseCompactor(dl.numel()) for _, dl, _ in outputs]
+            packed_dev = [[[(torch.empty_like(outputs[p][0]),
+                             torch.empty(outputs[p][1].numel() + 1, dtype=torch.int64, device="cuda"))
+                            for p in units[u][1]] for u in range(U)] for _ in range(NB)]
+        pending = []
+        # a compactor's two count slots alternate per call, so a group's
+        # count is read before that engine's call two steps later is queued
+        DEFER = max(1, 2 * U - 1)
+        record_bytes = 0
+
+        def download_records(b_, u_, slots_):
+            # on a stream of their own: queued behind the next groups'
+            # count copies, which wait for those groups' analysis, they
+            # would pile up to the end of the run
+            ev_comp[b_][u_].synchronize()
+            n_bytes = 0
+            with torch.cuda.stream(s_rec):
+                s_rec.wait_event(ev_small[b_][u_])
+                for p, (co, _), sl in zip(units[u_][1], packed_dev[b_][u_], slots_):
+                    nb_ = compactors[p].total(sl) * rec_bytes
+                    if nb_:
+                        host_out[p][0][:nb_].copy_(co.view(-1)[:nb_], non_blocking=True)
+                    n_bytes += nb_
+                ev_d2h[b_][u_].record(s_rec)
+            return n_bytes
         s_h2d, s_d2h = torch.cuda.Stream(), torch.cuda.Stream()
+        # group engines on NS streams: one group's DME (a latency-bound
+        # launch of 2.8 waves) overlaps the next group's stages
+        NS = max(1, min(args.e2e_streams, U))
+        s_comp = [stream] + [torch.cuda.Stream() for _ in range(NS - 1)]
+        s_mark = torch.cuda.Stream()
+        s_rec = torch.cuda.Stream()         # the packed records' copies, queued late
+        ev_small = [[torch.cuda.Event() for _ in range(U)] for _ in range(NB)]
         ev_h2d = [[torch.cuda.Event() for _ in range(U)] for _ in range(NB)]
         ev_comp = [[torch.cuda.Event() for _ in range(U)] for _ in range(NB)]
         ev_d2h = [[torch.cuda.Event() for _ in range(U)] for _ in range(NB)]
         ev_step = [torch.cuda.Event(enable_timing=True) for _ in range(KE)]
+        if packed:
+            # load the compaction kernels before the timed region
+            for u in range(U):
+                for p, (dp, dl, _), (co, off) in zip(units[u][1], out_dev[0][u], packed_dev[0][u]):
+                    compactors[p].total(compactors[p](dp, dl, max_calls, co, off))
         torch.cuda.synchronize()
         barrier()
         e0.record(stream)
-        s_h2d.wait_stream(stream)
-        s_d2h.wait_stream(stream)
+        for s_ in [s_h2d, s_d2h, s_mark, s_rec] + s_comp[1:]:
+            s_.wait_stream(stream)
         for k in range(KE):
             b = k % NB
             src = host_chunks[k % len(host_chunks)]
             for u in range(U):
                 r0, r1 = rows[u]
+                su = s_comp[u % NS]
                 with torch.cuda.stream(s_h2d):
                     if k >= NB:
                         s_h2d.wait_event(ev_comp[b][u])     # step k-NB has read in_dev[b][u]
                     in_dev[b][u].copy_(src[r0:r1], non_blocking=True)
                     ev_h2d[b][u].record(s_h2d)
-                stream.wait_event(ev_h2d[b][u])
+                su.wait_event(ev_h2d[b][u])
                 if k >= NB:
-                    stream.wait_event(ev_d2h[b][u])         # step k-NB's outputs are on the host
-                run_unit(u, in_dev[b][u], out_dev[b][u])
-                ev_comp[b][u].record(stream)
+                    su.wait_event(ev_d2h[b][u])             # step k-NB's outputs are on the host
+                with torch.cuda.stream(su):
+                    run_unit(u, in_dev[b][u], out_dev[b][u])
+                    slots = ([compactors[p](dp, dl, max_calls, co, off)
+                              for p, (dp, dl, _), (co, off) in zip(units[u][1], out_dev[b][u], packed_dev[b][u])]
+                             if packed else None)
+                ev_comp[b][u].record(su)
+                s_mark.wait_event(ev_comp[b][u])
                 with torch.cuda.stream(s_d2h):
                     s_d2h.wait_event(ev_comp[b][u])
                     for p, (dp, dl, do) in zip(units[u][1], out_dev[b][u]):
                         hp, hl, ho = host_out[p]
                         hl.copy_(dl, non_blocking=True)
                         ho.copy_(do, non_blocking=True)
-                        hp.copy_(dp, non_blocking=True)
+                        if not packed:
+                            hp.copy_(dp, non_blocking=True)
+                            record_bytes += dp.numel()
                     if args.engine == "fused":
                         # HF metrics records of the pools that completed a block
                         eg = units[u][0]
@@ -574,9 +637,19 @@ def main():
                                 p = units[u][1][i]
                                 hf_host[p].copy_(eg.metrics[i], non_blocking=True)
                                 metrics_bytes += eg.metrics[i].numel()
-                    ev_d2h[b][u].record(s_d2h)
-            ev_step[k].record(stream)
-        stream.wait_stream(s_d2h)
+                    if packed:
+                        ev_small[b][u].record(s_d2h)
+                    else:
+                        ev_d2h[b][u].record(s_d2h)
+                if packed:
+                    pending.append((b, u, slots))
+                    while len(pending) > DEFER:
+                        record_bytes += download_records(*pending.pop(0))
+            ev_step[k].record(s_mark)                       # every group of step k analysed
+        while pending:
+            record_bytes += download_records(*pending.pop(0))
+        for s_ in [s_d2h, s_mark, s_rec] + s_comp[1:]:
+            stream.wait_stream(s_)
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
@@ -588,18 +661,25 @@ def main():
                     "last_download_ms": ms_e2e - marks[-1]}
         c += KE
         h2d = total_lanes * FRAMES * 64 * 2
-        d2h = sum(dp.numel() + dl.numel() * 4 + do.numel() * 4 for dp, dl, do in outputs) + metrics_bytes // KE
+        d2h = (record_bytes + metrics_bytes) // KE + sum(dl.numel() * 4 + do.numel() * 4 for _, dl, do in outputs)
         e2e = {"value": zf_step * KE * world / (ms_e2e / 1e3), "unit": "ZMW-frames/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / KE, "steps": KE,
                "phase": "same K steps of the estimation cycle as value", "timeline": timeline,
                "overlap": f"copies on their own streams, {NB} buffers deep against the analysis, pipelined over "
-                          f"{U} pool group(s) of {ppg * lpp} lanes (one engine each); a step's first upload and "
-                          f"last download cover one group"}
+                          f"{U} pool group(s) of {ppg * lpp} lanes (one engine each, on {NS} stream(s)); a step's "
+                          f"first upload and last download cover one group",
+               "download": ("the valid pulse records, packed by hw_pulses_compact, with every ZMW's pulse and "
+                            "overflow counts and the HF metrics blocks" if packed else
+                            "every pulse slot, with every ZMW's pulse and overflow counts and the HF metrics blocks")}
         if args.engine == "fused":
             for eg, _ in units:
                 if eg is not engine:
                     eg.finish()
                     eg.close()
+        if packed:
+            for cp in compactors:
+                cp.close()
+            del packed_dev
         del host_chunks, in_dev, out_dev
 
     # Roofline of the dominant kernel (the frame labeler) from the live stage timers.
