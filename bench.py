@@ -9,7 +9,8 @@ pool re-estimates its detection models every 4000 frames, staggered by
 pool).  The run first streams the start-up chunks (untimed) until every pool
 is in its periodic estimation cycle; a step is then one chunk of the whole
 chip through baseliner -> statistics -> histogram -> (EM when due) ->
-labeler -> pulses (+ HF metrics), all pools in one hw_chunk_fused call.  The
+labeler -> pulses (+ HF metrics), each pool through its own hw_chunk_fused
+engine, the four engines on four streams (--groups, --streams).  The
 8-step estimation cycle runs one EM per pool, so K steps from a given phase
 of the cycle hold a phase-dependent number of EMs; both timed legs below
 start at the same phase and run the same K steps.  With --gpus N each rank
@@ -75,10 +76,11 @@ def parse():
                     help="fused engine's use of its second stream (hw_fused_set_overlap)")
     ap.add_argument("--e2e-buffers", type=int, default=3,
                     help="device input/output buffers per group in the end-to-end leg")
-    ap.add_argument("--e2e-groups", type=int, default=4,
-                    help="pool groups the end-to-end leg pipelines its copies over (fused engine)")
-    ap.add_argument("--e2e-streams", type=int, default=2,
-                    help="streams the end-to-end leg's group engines run on (group u on stream u mod n)")
+    ap.add_argument("--groups", type=int, default=4,
+                    help="fused engines the pools are split over (pool groups; both legs, and the end-to-end "
+                         "leg pipelines its copies over them)")
+    ap.add_argument("--streams", type=int, default=4,
+                    help="streams the group engines run on (group u on stream u mod n)")
     ap.add_argument("--e2e-download", choices=["packed", "slots"], default="packed",
                     help="end-to-end leg's pulse download: the valid records packed by hw_pulses_compact, "
                          "or every pulse slot")
@@ -375,31 +377,65 @@ def main():
     gen = Fl.TraceGenerator(total_lanes, workload=1, zmw_offset=zmw_offset(rank, zmws))
     lpp = args.lanes_per_pool
     stream = torch.cuda.current_stream()
+    serial = [False]
     if args.engine == "fused":
-        # every pool in one engine: each stage is one launch over all lanes,
-        # HF metrics included (4096-frame blocks, the reference's trained
-        # activity classifier when its table is in the checkout)
-        engine = Fl.FusedEngine(cfg, [lpp] * args.pools, [FRAMES] * args.pools)
-        engine.set_overlap(args.overlap)
-        cart_file = os.path.join(ROOT, "hw_b200", "data", "trained_cart.npz")
-        cart = dict(np.load(cart_file)) if os.path.exists(cart_file) else None
-        engine.enable_hf_metrics(4096, cfg.frame_rate, True, cart)
-        profiled = [engine]
-        outputs = [engine.outputs(p) for p in range(args.pools)]
-        lanes_per_launch = total_lanes
+        # The pools in G groups, one engine each (a group keeps its pools' ids
+        # and so their estimation stagger): each stage is one launch over the
+        # lanes of a group's pools, HF metrics included (4096-frame blocks,
+        # the reference's trained activity classifier).  The engines run on
+        # NS streams, so one group's DME (a latency-bound launch) shares the
+        # GPU with other groups' stages.
+        G = max(1, min(args.groups, args.pools))
+        if args.pools % G:
+            G = 1
+        ppg = args.pools // G
+        NS = max(1, min(args.streams, G))
+        cart = dict(np.load(os.path.join(ROOT, "hw_b200", "data", "trained_cart.npz")))
+        engines = []
+        for g in range(G):
+            ids = list(range(g * ppg, (g + 1) * ppg))
+            eg = Fl.FusedEngine(cfg, [lpp] * ppg, [FRAMES] * ppg, pool_ids=ids)
+            eg.set_overlap(args.overlap)
+            eg.enable_hf_metrics(4096, cfg.frame_rate, True, cart)
+            engines.append((eg, ids))
+        s_comp = [stream] + [torch.cuda.Stream() for _ in range(NS - 1)]
+        profiled = [eg for eg, _ in engines]
+        outputs = [engines[p // ppg][0].outputs(p % ppg) for p in range(args.pools)]
+        pool_metrics = [eg.metrics[i] for eg, ids in engines for i in range(len(ids))]
 
-        def run_chunk(chunk, c, outs=None):
-            engine.process([chunk[p * lpp:(p + 1) * lpp] for p in range(args.pools)], outs)
+        def run_units(chunk, outs=None):
+            for u, (eg, ids) in enumerate(engines):
+                with torch.cuda.stream(stream if serial[0] else s_comp[u % NS]):
+                    eg.process([chunk[p * lpp:(p + 1) * lpp] for p in ids], outs[u] if outs else None)
     else:
+        G, NS, s_comp = args.pools, 1, [stream]
         analyzers = [Fl.BatchAnalyzer(cfg, p, lpp, FRAMES) for p in range(args.pools)]
         profiled = analyzers
         outputs = [(a.pulses, a.lens, a.ovf) for a in analyzers]
-        lanes_per_launch = lpp
 
-        def run_chunk(chunk, c, outs=None):
+        def run_units(chunk, c, outs=None):
             for p, a in enumerate(analyzers):
                 o = outs[p] if outs is not None else (None, None, None)
                 a(chunk[p * lpp:(p + 1) * lpp], c * FRAMES, *o)
+
+    def fork():
+        for s_ in s_comp[1:]:
+            s_.wait_stream(stream)
+
+    def join():
+        for s_ in s_comp[1:]:
+            stream.wait_stream(s_)
+
+    def run_chunk(chunk, c, sync=True):
+        # sync: the chunk buffer is reused by the caller's next step
+        if sync:
+            fork()
+        if args.engine == "fused":
+            run_units(chunk)
+        else:
+            run_units(chunk, c)
+        if sync:
+            join()
 
     # Start-up and warm-up (untimed).
     n_start = startup_chunks(cfg, args.pools)
@@ -435,8 +471,10 @@ def main():
     time.sleep(0.3)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
+    fork()
     for k in range(K):
-        run_chunk(dev_chunks[k], c + k)
+        run_chunk(dev_chunks[k], c + k, sync=False)
+    join()
     e1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
@@ -449,9 +487,11 @@ def main():
     for a in profiled:
         a.profile(True)
         a.stage_times()
+    serial[0] = True        # one stream: the stage timers time the stream they run on
     for k in range(K):
         run_chunk(dev_chunks[k], c + k)
     torch.cuda.synchronize()
+    serial[0] = False
     c += K
     del dev_chunks
     stage = {}
@@ -463,7 +503,7 @@ def main():
         a.profile(False)
     launches = sum(n * KERNELS_PER_STAGE[k] for k, (_, n) in stage.items())
     if args.engine == "fused":
-        launches += 2 * K      # per step: the step-table upload and the failure-word kernels
+        launches += 2 * K * G      # per step and engine: the step-table upload and the failure-word kernels
 
     zf_step = zmws * FRAMES
     value = zf_step * K * world / (ms / 1e3)
@@ -487,32 +527,15 @@ def main():
             c += 1
         torch.cuda.synchronize()
         KE = K
-        # Copy/compute pipelining over pool groups: each group's chunk slice
-        # is uploaded, analysed and downloaded on its own, so a step's first
-        # upload and last download cover one group, not the whole chip.  With
-        # the fused engine each group is its own engine (same pool ids, so
-        # the same estimation stagger), brought to this chunk untimed.
-        G = max(1, min(args.e2e_groups, args.pools)) if args.engine == "fused" else args.pools
-        if args.pools % G:
-            G = 1
-        ppg = args.pools // G
-        if args.engine == "fused" and G > 1:
-            units = []
-            for g in range(G):
-                ids = list(range(g * ppg, (g + 1) * ppg))
-                eg = Fl.FusedEngine(cfg, [lpp] * ppg, [FRAMES] * ppg, pool_ids=ids)
-                eg.set_overlap(args.overlap)
-                eg.enable_hf_metrics(4096, cfg.frame_rate, True, cart)
-                units.append((eg, ids))
-            for cc in range(c):
-                gen.next(cc * FRAMES, FRAMES, out=buf)
-                for eg, ids in units:
-                    eg.process([buf[p * lpp:(p + 1) * lpp] for p in ids])
-            torch.cuda.synchronize()
-        elif args.engine == "fused":
-            units = [(engine, list(range(args.pools)))]
+        # Copy/compute pipelining over the pool groups: each group's chunk
+        # slice is uploaded, analysed by its engine and downloaded on its
+        # own, so a step's first upload and last download cover one group,
+        # not the whole chip.
+        if args.engine == "fused":
+            units = engines
         else:
             units = [(analyzers[p], [p]) for p in range(args.pools)]
+        ppg = len(units[0][1])
 
         def run_unit(u, chunk_slice, outs):
             eg, ids = units[u]
@@ -539,7 +562,7 @@ def main():
         host_out = [(torch.empty(dp.numel(), dtype=torch.uint8, pin_memory=True),
                      torch.empty(dl.shape, dtype=torch.int32, pin_memory=True),
                      torch.empty(do.shape, dtype=torch.int32, pin_memory=True)) for dp, dl, do in outputs]
-        hf_host = ([torch.empty(m.numel(), dtype=torch.uint8, pin_memory=True) for m in engine.metrics]
+        hf_host = ([torch.empty(m.numel(), dtype=torch.uint8, pin_memory=True) for m in pool_metrics]
                    if args.engine == "fused" else [])
         metrics_bytes = 0
         # Packed download: hw_pulses_compact packs each pool's valid records
@@ -578,10 +601,6 @@ def main():
                 ev_d2h[b_][u_].record(s_rec)
             return n_bytes
         s_h2d, s_d2h = torch.cuda.Stream(), torch.cuda.Stream()
-        # group engines on NS streams: one group's DME (a latency-bound
-        # launch of 2.8 waves) overlaps the next group's stages
-        NS = max(1, min(args.e2e_streams, U))
-        s_comp = [stream] + [torch.cuda.Stream() for _ in range(NS - 1)]
         s_mark = torch.cuda.Stream()
         s_rec = torch.cuda.Stream()         # the packed records' copies, queued late
         ev_small = [[torch.cuda.Event() for _ in range(U)] for _ in range(NB)]
@@ -671,11 +690,6 @@ def main():
                "download": ("the valid pulse records, packed by hw_pulses_compact, with every ZMW's pulse and "
                             "overflow counts and the HF metrics blocks" if packed else
                             "every pulse slot, with every ZMW's pulse and overflow counts and the HF metrics blocks")}
-        if args.engine == "fused":
-            for eg, _ in units:
-                if eg is not engine:
-                    eg.finish()
-                    eg.close()
         if packed:
             for cp in compactors:
                 cp.close()
@@ -685,16 +699,20 @@ def main():
     # Roofline of the dominant kernel (the frame labeler) from the live stage timers.
     peaks = measured_peaks()
     lab_ms, lab_n = stage.get("labeler", (0.0, 0))
-    lab_bytes_launch = labeler_alg_bytes_per_zmw(FRAMES) * lanes_per_launch * 64
     roof = None
     if lab_n:
-        avg_s = lab_ms / lab_n / 1e3
-        achieved = lab_bytes_launch / avg_s / 1e9
+        # the stage pass labels every ZMW once a step, in launches of
+        # different sizes (a step with an estimate labels the estimating
+        # pools in a launch of their own): bytes and time are totals over
+        # the pass, per launch their averages
+        zmw_labeled = zmws * K
+        lab_bytes_launch = labeler_alg_bytes_per_zmw(FRAMES) * zmw_labeled / lab_n
+        achieved = labeler_alg_bytes_per_zmw(FRAMES) * zmw_labeled / (lab_ms / 1e3) / 1e9
         peak = peaks["hbm_gbs"] if peaks else 6650.0
         prof = labeler_dram_profile()
         traffic = None
         if prof:
-            traffic = prof["dram_bytes_per_zmw_frame"] * lanes_per_launch * 64 * FRAMES
+            traffic = prof["dram_bytes_per_zmw_frame"] * zmw_labeled * FRAMES / lab_n
         roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
                 "kernel": "LabelerKernel", "launch_ms": lab_ms / lab_n,
@@ -713,7 +731,8 @@ def main():
                          f"pools x {args.cpu_steps} steady-state 512-frame chunks after start-up ({secs:.1f} s)"}
 
     if args.engine == "fused":
-        engine.finish()
+        for eg, _ in engines:
+            eg.finish()
     for a in profiled:
         a.close()
     learned = None
@@ -767,8 +786,9 @@ def main():
             "config": {"workload": WORKLOAD,
                        "zmws_per_gpu": zmws, "frames_per_chunk": FRAMES, "pools": args.pools,
                        "startup_chunks": n_start, "inputs": "1 GiB chunk per step, larger than L2",
-                       "engine": "hw_chunk_fused (one launch per stage over all pools)" if args.engine == "fused"
-                                 else "one hw_analyzer per pool"},
+                       "engine": (f"hw_chunk_fused: {G} engine(s) of {ppg} pool(s) (one launch per stage over an "
+                                  f"engine's pools) on {NS} stream(s)" if args.engine == "fused"
+                                  else "one hw_analyzer per pool")},
             "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
             "clocks": clk,
             "stage_ms": {k: v[0] / K for k, v in stage.items()},
