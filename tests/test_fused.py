@@ -85,6 +85,53 @@ def test_fused_stream_overlap_modes_equal_per_pool_analyzers(overlap):
         assert emitted > 0 and estimated > 0
 
 
+def test_fused_engines_on_concurrent_streams_equal_per_pool_analyzers():
+    """Pool groups, one engine each, run on their own streams at once (the
+    layout bench.py times): the engines share no device state, so every
+    pool's results equal its per-pool analyzer's, with and without graphs."""
+    import torch
+    from hw_b200 import filters as Fl
+    cfg = workloads.small_config()
+    cfg.model_estimation_mode = abi.DYNAMIC_ESTIMATIONS
+    lanes = [24, 40, 16, 32, 8, 48]
+    frames = [512, 512, 256, 512, 128, 256]
+    ids = [3 * p + 1 for p in range(len(lanes))]
+    groups = [[0, 1], [2, 3], [4], [5]]
+    engs = [Fl.FusedEngine(cfg, [lanes[p] for p in g], [frames[p] for p in g], pool_ids=[ids[p] for p in g],
+                           graphs=(u % 2 == 1)) for u, g in enumerate(groups)]
+    ans = [Fl.BatchAnalyzer(cfg, i, L, F) for i, L, F in zip(ids, lanes, frames)]
+    gens = [Fl.TraceGenerator(L, workload=2, zmw_offset=1000 * p) for p, L in enumerate(lanes)]
+    main = torch.cuda.current_stream()
+    streams = [torch.cuda.Stream() for _ in groups]
+    emitted = estimated = 0
+    for step in range(28):
+        chunks = _chunks(gens, frames, step, False)
+        res = []
+        for s, e, g in zip(streams, engs, groups):
+            s.wait_stream(main)
+            with torch.cuda.stream(s):
+                res.append(e.process([chunks[p] for p in g]))
+        for s in streams:
+            main.wait_stream(s)
+        for (em, est), e, g in zip(res, engs, groups):
+            for i, p in enumerate(g):
+                pulses, lens, ovf, e1, s1 = ans[p](chunks[p], step * frames[p])
+                assert (bool(em[i]), bool(est[i])) == (e1, s1), (step, p)
+                pp, pl, po = e.outputs(i)
+                assert torch.equal(pl, lens) and torch.equal(po, ovf), (step, p)
+                if e1:
+                    emitted += 1
+                    assert _same_pulses(cfg, lanes[p], pulses, pp, lens), (step, p)
+                estimated += int(s1)
+    for e, g in zip(engs, groups):
+        e.finish()
+        for i, p in enumerate(g):
+            m0, fi0 = ans[p].models()
+            m1, fi1 = e.models(i)
+            assert fi0 == fi1 and torch.equal(m0, m1), p
+    assert emitted > 0 and estimated > 0
+
+
 def test_fused_graphs_replay_identically():
     emitted, estimated, graph_steps = _compare(abi.DYNAMIC_ESTIMATIONS, graphs=True, u8=False, steps=28)
     assert emitted > 0 and estimated > 0
