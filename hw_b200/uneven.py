@@ -8,6 +8,8 @@ Ways of running the same pools on the same traces, each timed on its own:
   * fused engine (hw_chunk_fused): every stage of a step is one launch over
     the lanes of all pools that take it; `fused_tuned` with the autotuner's
     kernel choices, `fused_graphs` replaying each step plan as a CUDA graph;
+    `fused_streams` deals the pools over four tuned engines that run on four
+    streams, so one engine's stages share the GPU with the others';
   * pool set (hw_pool_set): pools that share chunk length and stagger class
     run as one batched analyzer, one launch per stage and class;
   * one analyzer per pool, each with its own launches (what a per-pool
@@ -93,6 +95,35 @@ def run(n_pools=500, steps=4, warmup_steps=None, variants=("fused_tuned", "fused
             out[v + "_launches_per_step"] = list(eng.last_step())
             eng.close()
             del bufs
+        elif v == "fused_streams":
+            # the pools dealt round-robin over four tuned engines (each keeps
+            # its pools' ids), the engines on four streams
+            G = 4
+            groups = [list(range(g, n_pools, G)) for g in range(G)]
+            engs = [Fl.FusedEngine(cfg, lanes[idx], frames[idx], pool_ids=idx, tuning="auto") for idx in groups]
+            side = [torch.cuda.Stream() for _ in range(G - 1)]
+            bufs = per_pool_buffers()
+
+            def fill(step):
+                for p, (g, F) in enumerate(zip(gens, frames)):
+                    g.next(step * int(F), int(F), out=bufs[p])
+                return bufs
+
+            def on_streams(step, ch):
+                for s_ in side:
+                    s_.wait_stream(stream)
+                for e, idx, s_ in zip(engs, groups, [stream] + side):
+                    with torch.cuda.stream(s_):
+                        e.process([ch[p] for p in idx])
+                for s_ in side:
+                    stream.wait_stream(s_)
+            ms = _timed(on_streams, gens, frames, warmup_steps, steps, stream, fill)
+            last = [e.last_step() for e in engs]
+            out[v + "_launches_per_step"] = [sum(x[0] for x in last), sum(x[1] for x in last)]
+            for e in engs:
+                e.finish()
+                e.close()
+            del bufs
         elif v == "pool_set":
             ps = Fl.PoolSet(cfg, lanes, frames)
 
@@ -133,7 +164,7 @@ def main():
     ap.add_argument("--pools", type=int, default=500)
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup-steps", type=int, default=None)
-    ap.add_argument("--variants", default="fused_tuned,fused,pool_set,per_pool")
+    ap.add_argument("--variants", default="fused_tuned,fused_streams,fused,pool_set,per_pool")
     a = ap.parse_args()
     print(json.dumps(run(a.pools, a.steps, a.warmup_steps, tuple(a.variants.split(",")))))
 
