@@ -179,3 +179,56 @@ def test_analyzer_with_learned_start_runs_dynamic_schedule():
     an.set_learned_init(None)
     an(gen.next(16 * F, F), 16 * F)
     torch.cuda.synchronize()
+
+
+@pytest.mark.gpu
+def test_analyzers_on_streams_with_learned_start_equal_serial():
+    """Analyzers with the learned start run at once on two streams, each
+    stream with its own copy of the network (a network handle holds its
+    forward pass's scratch), give the results of the same analyzers run one
+    after another on one stream."""
+    import torch
+    from hw_b200 import abi, filters as Fl, learned_init as L, workloads
+    cfg = workloads.small_config()
+    cfg.model_estimation_mode = abi.DYNAMIC_ESTIMATIONS
+    net, _ = L.run(train_pools=1, eval_pools=1, lanes=256, fit_iters=200, epochs=5, batch=1024, seed=2)
+    net2 = L.Network(max_batch=net.max_batch)
+    net2.set(*net.get())
+    lanes, F, pools = 32, 512, 4
+    serial = [Fl.BatchAnalyzer(cfg, p, lanes, F) for p in range(pools)]
+    conc = [Fl.BatchAnalyzer(cfg, p, lanes, F) for p in range(pools)]
+    for p in range(pools):
+        serial[p].set_learned_init(net)
+        conc[p].set_learned_init(net if p % 2 == 0 else net2)
+    gens = [Fl.TraceGenerator(lanes, workload=2, zmw_offset=5000 * p) for p in range(pools)]
+    main = torch.cuda.current_stream()
+    side = [torch.cuda.Stream(), torch.cuda.Stream()]
+    estimated = emitted = 0
+    for c in range(20):
+        chunks = [g.next(c * F, F) for g in gens]
+        for s in side:
+            s.wait_stream(main)
+        res = []
+        for p in range(pools):
+            with torch.cuda.stream(side[p % 2]):
+                res.append(conc[p](chunks[p], c * F))
+        for s in side:
+            main.wait_stream(s)
+        for p in range(pools):
+            pulses0, lens0, ovf0, em0, est0 = serial[p](chunks[p], c * F)
+            pulses1, lens1, ovf1, em1, est1 = res[p]
+            assert (em0, est0) == (em1, est1), (c, p)
+            assert torch.equal(lens0, lens1) and torch.equal(ovf0, ovf1), (c, p)
+            q0 = Fl.struct_to_numpy(pulses0, abi.PULSE_DT).reshape(lanes * 64, cfg.max_calls_per_zmw)
+            q1 = Fl.struct_to_numpy(pulses1, abi.PULSE_DT).reshape(lanes * 64, cfg.max_calls_per_zmw)
+            n = np.minimum(lens0.cpu().numpy().reshape(-1), cfg.max_calls_per_zmw)
+            for z in range(lanes * 64):
+                assert np.array_equal(q0[z, :n[z]].view(np.uint8), q1[z, :n[z]].view(np.uint8)), (c, p, z)
+            estimated += int(est0)
+            emitted += int(em0)
+    for p in range(pools):
+        m0, fi0 = serial[p].models()
+        m1, fi1 = conc[p].models()
+        assert fi0 == fi1 and torch.equal(m0, m1), p
+    assert estimated >= pools and emitted > 0
+    net2.close()
