@@ -196,9 +196,39 @@ def cpu_baseline(cfg, lanes, steps, warmup, threads, pools=1, lanes_per_pool=0):
     from harness import OracleBackend, Pipeline
     pools = max(1, min(pools, lanes))
     split = [lanes // pools + (1 if p < lanes % pools else 0) for p in range(pools)]
+    stage_s = {}
+    timing = [False]
+
+    class Timed:
+        """The oracle backend with each stage call timed (wall clock)."""
+        STAGE = {"baseline": "baseline", "agg_add": "aggregate", "agg_get": "aggregate", "agg_reset": "aggregate",
+                 "hist_reset": "hist_reset", "hist_add": "histogram", "hist_get": "histogram",
+                 "init_models": "model_init", "estimate": "dme", "label": "labeler", "pulses": "pulses"}
+
+        def __init__(self, b):
+            self._b = b
+            self.lanes, self.F = b.lanes, b.F
+
+        def startup_latency(self):
+            return self._b.startup_latency()
+
+        def __getattr__(self, name):
+            fn = getattr(self._b, name)
+            stage = Timed.STAGE.get(name)
+            if stage is None:
+                return fn
+
+            def call(*a):
+                t0 = time.perf_counter()
+                r = fn(*a)
+                if timing[0]:
+                    stage_s[stage] = stage_s.get(stage, 0.0) + time.perf_counter() - t0
+                return r
+            return call
+
     units = []
     for p, lp in enumerate(split):
-        backend = OracleBackend(cfg, lp, FRAMES, p)
+        backend = Timed(OracleBackend(cfg, lp, FRAMES, p))
         gen = oracle.TraceGenerator(lp, workload=1, zmw_offset=p * lanes_per_pool * 64)
         units.append((Pipeline(backend, cfg, p), gen))
     n0 = workloads.startup_chunks(cfg, pools, FRAMES, latency=units[0][0].bl_latency) + warmup
@@ -206,6 +236,7 @@ def cpu_baseline(cfg, lanes, steps, warmup, threads, pools=1, lanes_per_pool=0):
     t_timed = 0.0
     for c in range(total):
         chunks = [gen.next(c * FRAMES, FRAMES) for _, gen in units]
+        timing[0] = c >= n0
         t0 = time.perf_counter()
         for (pipe, _), chunk in zip(units, chunks):
             pipe.process(chunk, c * FRAMES)
@@ -213,7 +244,9 @@ def cpu_baseline(cfg, lanes, steps, warmup, threads, pools=1, lanes_per_pool=0):
         if c >= n0:
             t_timed += dt
     zf = lanes * 64 * FRAMES * steps
-    return zf / t_timed, t_timed
+    stages = {k: {"ms_per_step": v * 1e3 / steps, "zmw_frames_per_s": zf / v if v > 0 else None}
+              for k, v in stage_s.items()}
+    return zf / t_timed, t_timed, stages
 
 
 def next_rows(threads):
@@ -341,8 +374,8 @@ def main():
         # The reference path on the host cores: rank 0 alone, no CUDA and no
         # collective (the other ranks exit at once).
         if rank == 0:
-            rate, secs = cpu_baseline(cfg, args.cpu_lanes, max(args.steps, 1), args.warmup, threads,
-                                      args.pools, args.lanes_per_pool)
+            rate, secs, stages = cpu_baseline(cfg, args.cpu_lanes, max(args.steps, 1), args.warmup, threads,
+                                              args.pools, args.lanes_per_pool)
             sample = (f"{args.cpu_lanes} lanes ({args.cpu_lanes * 64} ZMWs) of the workload, spread over its "
                       f"{args.pools} pools, x {args.steps} steady-state 512-frame chunks after start-up "
                       f"(the GPU run's chunks), {secs:.1f} s of CPU time")
@@ -354,7 +387,7 @@ def main():
                    "config": {"workload": WORKLOAD, "zmws_per_gpu": zmws, "frames_per_chunk": FRAMES,
                               "pools": args.pools, "cpu_sample_lanes": args.cpu_lanes},
                    "cpu_baseline": {"value": rate, "unit": "ZMW-frames/s", "cores": threads, "kind": "port",
-                                    "sample": sample},
+                                    "sample": sample, "stages": stages},
                    "e2e": {"value": rate, "unit": "ZMW-frames/s", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}}
             print(json.dumps(out), flush=True)
@@ -724,9 +757,9 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, secs = cpu_baseline(cfg, args.cpu_lanes, args.cpu_steps, args.warmup, threads,
-                                  args.pools, args.lanes_per_pool)
-        cpu = {"value": rate, "unit": "ZMW-frames/s", "cores": threads, "kind": "port",
+        rate, secs, stages = cpu_baseline(cfg, args.cpu_lanes, args.cpu_steps, args.warmup, threads,
+                                          args.pools, args.lanes_per_pool)
+        cpu = {"value": rate, "unit": "ZMW-frames/s", "cores": threads, "kind": "port", "stages": stages,
                "sample": f"{args.cpu_lanes} lanes ({args.cpu_lanes * 64} ZMWs) spread over the {args.pools} "
                          f"pools x {args.cpu_steps} steady-state 512-frame chunks after start-up ({secs:.1f} s)"}
 

@@ -30,4 +30,7 @@ def test_reference_arm_line_and_libraries():
     assert cb["kind"] == "port" and cb["value"] == m["value"] and cb["cores"] >= 1
     # the 8 sample lanes are spread over the workload's 4 pools
     assert "4 pools" in cb["sample"]
+    # per-stage CPU times of the sample
+    for stage in ("baseline", "histogram", "labeler", "pulses"):
+        assert cb["stages"][stage]["ms_per_step"] > 0, stage
     assert lines[-1] == "LOADED False True"
