@@ -1,6 +1,7 @@
 // Device-side helpers shared by the hw_b200 kernels.
 #pragma once
 
+#include <cstring>
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
 #include <nvtx3/nvToolsExt.h>
@@ -184,6 +185,12 @@ struct KParams
     uint8_t analogMap[kAnalogs];
     // -0.0f, read at run time by the packed products (mulz2)
     float negZero;
+    // labeler, 9-way rows 0, 5, 6, 7, 8 (index 0..4): the transition
+    // constants (T[R][5], T[R][9]) of the source groups 5..8 and 9..12, and
+    // whether every such row's constants are equal within each group (then
+    // the rows take the grouped arg-max)
+    float2 grp9[5];
+    int grouped9;
 };
 
 inline void FillParams(const hw_config& cfg, const hwp::Derived& d, KParams* k)
@@ -218,6 +225,19 @@ inline void FillParams(const hw_config& cfg, const hwp::Derived& d, KParams* k)
     k->roiUpper = cfg.roi_upper_threshold; k->roiLower = cfg.roi_lower_threshold;
     k->ampThresh = d.ampThresh; k->widthThresh = d.widthThresh; k->maxCalls = (int)cfg.max_calls_per_zmw;
     k->negZero = -0.0f;
+    // Grouped 9-way rows: bitwise-equal, non-NaN constants within each group.
+    const int rows9[5] = {0, 5, 6, 7, 8};
+    bool grouped = true;
+    for (int i = 0; i < 5; ++i)
+    {
+        const float* t = d.trans[rows9[i]];
+        k->grp9[i] = make_float2(t[5], t[9]);
+        for (int g = 5; g <= 9; g += 4)
+            for (int s = g; s < g + 4; ++s)
+                grouped &= (t[s] == t[s]) && std::memcmp(&t[s], &t[g], sizeof(float)) == 0;
+        grouped &= (t[0] == t[0]);
+    }
+    k->grouped9 = grouped ? 1 : 0;
 }
 
 // ModelSignalCovar, DetectionModelHost.cpp:237-245

@@ -186,6 +186,58 @@ __device__ __forceinline__ float NineWayRow(const KParams& k, float score, const
     return mv;
 }
 
+// Grouped 9-way rows.  When a row's transition constants are equal within
+// each source group (t_A for states 5..8, t_B for 9..12; KParams::grouped9),
+// its candidates of group G are RN(a_G + ll[s]) with a_G = RN(score + t_G)
+// the same for the whole group, and RN(a_G + x) is monotone in x.  So the
+// group's best value is RN(a_G + m_G), m_G the group's largest ll, reached
+// by the last state holding m_G, unless a later state of the group rounds
+// to the same sum: that needs RN(a_G + m'_G) == RN(a_G + m_G), m'_G the
+// largest ll after that state, and sends the frame to the generic rows.  m_G,
+// its last position and m'_G are shared by the five 9-way rows of a frame.
+struct GroupMax
+{
+    float m;        // largest ll of the group
+    float after;    // largest ll after its last position (NaN: none)
+    uint32_t pos;   // last position of m, 0..3
+};
+
+// Right to left with strict comparisons: the last position of the maximum.
+__device__ __forceinline__ GroupMax ScanGroup(float2 lo, float2 hi)
+{
+    GroupMax g{hi.y, __int_as_float(0x7fffffff), 3u};
+    auto step = [&](float v, uint32_t p) {
+        const bool gt = v > g.m;
+        g.after = gt ? g.m : g.after;
+        g.m = gt ? v : g.m;
+        g.pos = gt ? p : g.pos;
+    };
+    step(hi.x, 2u);
+    step(lo.y, 1u);
+    step(lo.x, 0u);
+    return g;
+}
+
+// One grouped 9-way row (index i of rows 0, 5, 6, 7, 8): returns the row's
+// value; base receives the winner's code (0 for state 0, s - 4 for s in
+// 5..12) unshifted; slow is set when the group winner is not certain.
+template <int i>
+__device__ __forceinline__ float GroupedRow(const KParams& k, float score, float ll0, float2 gm, float2 gafter,
+                                            uint32_t codeA, uint32_t codeB, uint32_t& base, bool& slow)
+{
+    constexpr int R = (i == 0) ? 0 : i + 4;
+    const float c0 = add_rn(add_rn(score, k.trans[R][0]), ll0);
+    const float2 a = add2(f2(score), k.grp9[i]);
+    const float2 gv = add2(a, gm);          // the groups' best candidates
+    const float2 nv = add2(a, gafter);      // the best after each group's winner
+    const bool geA = gv.x >= c0;
+    const float mv = geA ? gv.x : c0;
+    const bool geB = gv.y >= mv;
+    base = geB ? codeB : (geA ? codeA : 0u);
+    slow |= geB ? (nv.y == gv.y) : (geA & (nv.x == gv.x));
+    return geB ? gv.y : mv;
+}
+
 // Two 2-way rows, R and R + 1, with scores s.x, s.y: their first sources are
 // the pair qa, their second the pair qb.
 template <int R, int qa, int qb, bool Margin>
@@ -211,19 +263,56 @@ __device__ __forceinline__ float2 TwoWayRows(const KParams& k, float2 s, const S
 
 // One Viterbi recursion step; returns the packed traceback word.  With
 // Margin, gap[r] receives row r's decision gap.
-template <bool Margin = false>
+template <bool Margin = false, bool Grouped = false>
 __device__ __forceinline__ uint32_t ViterbiStep(const KParams& k, const ZScorer& sc, float data, bool isRoi,
                                                 StateLL& ll, float* gap = nullptr)
 {
+    static_assert(!(Margin && Grouped), "margins come from the generic rows");
     float sco[9];
     sc.Scores(data, sco, f2(k.negZero));
     uint32_t cd[9];
     float gl[kStates];
-    const float n0 = NineWayRow<0, Margin>(k, sco[0], ll, cd[0], gl[0]);
-    const float n5 = NineWayRow<5, Margin>(k, sco[5], ll, cd[1], gl[5]);
-    const float n6 = NineWayRow<6, Margin>(k, sco[6], ll, cd[2], gl[6]);
-    const float n7 = NineWayRow<7, Margin>(k, sco[7], ll, cd[3], gl[7]);
-    const float n8 = NineWayRow<8, Margin>(k, sco[8], ll, cd[4], gl[8]);
+    float n0, n5, n6, n7, n8;
+    if constexpr (Grouped)
+    {
+        const GroupMax gA = ScanGroup(ll.p[2], ll.p[3]), gB = ScanGroup(ll.p[4], ll.p[5]);
+        const float2 gm = f2(gA.m, gB.m), ga = f2(gA.after, gB.after);
+        const uint32_t codeA = 1u + gA.pos, codeB = 5u + gB.pos;
+        // a NaN among the rows' inputs (or an inf - inf) takes the generic rows
+        const float2 lsum = add2(add2(ll.p[2], ll.p[3]), add2(ll.p[4], ll.p[5]));
+        const float ssum = add_rn(add_rn(add_rn(sco[0], sco[5]), add_rn(sco[6], sco[7])), sco[8]);
+        bool slow = isnan(add_rn(add_rn(lsum.x, lsum.y), add_rn(ll.s0, ssum)));
+        uint32_t b0, b5, b6, b7, b8;
+        n0 = GroupedRow<0>(k, sco[0], ll.s0, gm, ga, codeA, codeB, b0, slow);
+        n5 = GroupedRow<1>(k, sco[5], ll.s0, gm, ga, codeA, codeB, b5, slow);
+        n6 = GroupedRow<2>(k, sco[6], ll.s0, gm, ga, codeA, codeB, b6, slow);
+        n7 = GroupedRow<3>(k, sco[7], ll.s0, gm, ga, codeA, codeB, b7, slow);
+        n8 = GroupedRow<4>(k, sco[8], ll.s0, gm, ga, codeA, codeB, b8, slow);
+        if (slow)
+        {
+            n0 = NineWayRow<0, false>(k, sco[0], ll, cd[0], gl[0]);
+            n5 = NineWayRow<5, false>(k, sco[5], ll, cd[1], gl[5]);
+            n6 = NineWayRow<6, false>(k, sco[6], ll, cd[2], gl[6]);
+            n7 = NineWayRow<7, false>(k, sco[7], ll, cd[3], gl[7]);
+            n8 = NineWayRow<8, false>(k, sco[8], ll, cd[4], gl[8]);
+        }
+        else
+        {
+            cd[0] = b0;
+            cd[1] = b5 << 4;
+            cd[2] = b6 << 8;
+            cd[3] = b7 << 12;
+            cd[4] = b8 << 16;
+        }
+    }
+    else
+    {
+        n0 = NineWayRow<0, Margin>(k, sco[0], ll, cd[0], gl[0]);
+        n5 = NineWayRow<5, Margin>(k, sco[5], ll, cd[1], gl[5]);
+        n6 = NineWayRow<6, Margin>(k, sco[6], ll, cd[2], gl[6]);
+        n7 = NineWayRow<7, Margin>(k, sco[7], ll, cd[3], gl[7]);
+        n8 = NineWayRow<8, Margin>(k, sco[8], ll, cd[4], gl[8]);
+    }
     // full rows: (r, r + 4); down rows: (r - 8, r - 4)
     const float2 n12 = TwoWayRows<1, 0, 2, Margin>(k, f2(sco[1], sco[2]), ll, cd[5], gl[1], gl[2]);
     const float2 n34 = TwoWayRows<3, 1, 3, Margin>(k, f2(sco[3], sco[4]), ll, cd[6], gl[3], gl[4]);
@@ -299,11 +388,12 @@ constexpr int LabelerMinBlocks(int threads) { return threads == 64 ? 10 : thread
 // Margin (single-pool launch only): the decision gaps of every frame and
 // state go to the scratch A.gap [lanes][F + 16][13][64], and the traceback
 // writes each label's best-path margin to A.margin.
-template <bool Mapped, bool Fuse, int Threads, bool Margin = false>
+template <bool Mapped, bool Fuse, int Threads, bool Margin = false, bool Grouped = false>
 __global__ void __launch_bounds__(Threads, LabelerMinBlocks(Threads)) LabelerKernel(LabelerArgs A, KParams k,
                                                                                      PulseArgs P)
 {
     static_assert(!Margin || (!Mapped && !Fuse), "margins come from the single-pool labeler");
+    static_assert(!(Margin && Grouped), "margins come from the generic rows");
     LaneMap map = A.map;
     if (!Mapped) map.list = nullptr;      // the single-pool variant compiles without the lane list
     int l, z;
@@ -400,7 +490,7 @@ __global__ void __launch_bounds__(Threads, LabelerMinBlocks(Threads)) LabelerKer
         }
         else
         {
-            tb[(size_t)lf * kLane] = ViterbiStep(k, sc, x, isRoi, ll);
+            tb[(size_t)lf * kLane] = ViterbiStep<false, Grouped>(k, sc, x, isRoi, ll);
         }
     };
     sc.Setup(k, oldM, z);
@@ -599,7 +689,7 @@ __global__ void LabelerModelCopyKernel(hw_lane_model* dst, const hw_lane_model* 
     reinterpret_cast<uint32_t*>(dst)[w] = reinterpret_cast<const uint32_t*>(src)[w];
 }
 
-template <bool Mapped, bool Fuse, int Threads, bool Margin = false>
+template <bool Mapped, bool Fuse, int Threads, bool Margin = false, bool Grouped = false>
 cudaError_t LaunchLabelerT(const LabelerArgs& a, const KParams& k, const PulseArgs& p, int lanes, cudaStream_t s)
 {
     const int blocks = (lanes * kLane + Threads - 1) / Threads;
@@ -613,15 +703,24 @@ cudaError_t LaunchLabelerT(const LabelerArgs& a, const KParams& k, const PulseAr
     if (e != cudaSuccess) return e;
     if (smem > 48 * 1024 && (dev < 0 || dev >= 64 || !attrSet[dev]))
     {
-        e = cudaFuncSetAttribute(LabelerKernel<Mapped, Fuse, Threads, Margin>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(LabelerKernel<Mapped, Fuse, Threads, Margin, Grouped>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(((1024 + kLookback + kStitch + 15) / 16 > 1024 / kBatch
                                             ? (1024 + kLookback + kStitch + 15) / 16 : 1024 / kBatch) *
                                        Threads * sizeof(uint32_t)));
         if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < 64) attrSet[dev] = true;
     }
-    LabelerKernel<Mapped, Fuse, Threads, Margin><<<blocks, Threads, smem, s>>>(a, k, p);
+    LabelerKernel<Mapped, Fuse, Threads, Margin, Grouped><<<blocks, Threads, smem, s>>>(a, k, p);
     return cudaGetLastError();
+}
+
+// The generic or the grouped 9-way rows (KParams::grouped9) of one variant.
+template <bool Mapped, bool Fuse, int Threads>
+cudaError_t LaunchLabelerG(const LabelerArgs& a, const KParams& k, const PulseArgs& p, int lanes, cudaStream_t s)
+{
+    return k.grouped9 ? LaunchLabelerT<Mapped, Fuse, Threads, false, true>(a, k, p, lanes, s)
+                      : LaunchLabelerT<Mapped, Fuse, Threads, false, false>(a, k, p, lanes, s);
 }
 
 cudaError_t LaunchLabeler(const LabelerArgs& a, const KParams& k, cudaStream_t s, const PulseArgs* fusedPulses,
@@ -637,7 +736,7 @@ cudaError_t LaunchLabeler(const LabelerArgs& a, const KParams& k, cudaStream_t s
         if (fusedPulses || lanesPerCta != 2) return cudaErrorInvalidValue;
         if (a.margin && !a.gap) return cudaErrorInvalidValue;
         e = a.margin ? LaunchLabelerT<false, false, 128, true>(a, k, none, lanes, s)
-                     : LaunchLabelerT<false, false, 128>(a, k, none, lanes, s);
+                     : LaunchLabelerG<false, false, 128>(a, k, none, lanes, s);
     }
     else if (a.margin)
     {
@@ -645,16 +744,16 @@ cudaError_t LaunchLabeler(const LabelerArgs& a, const KParams& k, cudaStream_t s
     }
     else if (fusedPulses)
     {
-        if (lanesPerCta == 1) e = LaunchLabelerT<true, true, 64>(a, k, *fusedPulses, lanes, s);
-        else if (lanesPerCta == 2) e = LaunchLabelerT<true, true, 128>(a, k, *fusedPulses, lanes, s);
-        else if (lanesPerCta == 4) e = LaunchLabelerT<true, true, 256>(a, k, *fusedPulses, lanes, s);
+        if (lanesPerCta == 1) e = LaunchLabelerG<true, true, 64>(a, k, *fusedPulses, lanes, s);
+        else if (lanesPerCta == 2) e = LaunchLabelerG<true, true, 128>(a, k, *fusedPulses, lanes, s);
+        else if (lanesPerCta == 4) e = LaunchLabelerG<true, true, 256>(a, k, *fusedPulses, lanes, s);
         else return cudaErrorInvalidValue;
     }
     else
     {
-        if (lanesPerCta == 1) e = LaunchLabelerT<true, false, 64>(a, k, none, lanes, s);
-        else if (lanesPerCta == 2) e = LaunchLabelerT<true, false, 128>(a, k, none, lanes, s);
-        else if (lanesPerCta == 4) e = LaunchLabelerT<true, false, 256>(a, k, none, lanes, s);
+        if (lanesPerCta == 1) e = LaunchLabelerG<true, false, 64>(a, k, none, lanes, s);
+        else if (lanesPerCta == 2) e = LaunchLabelerG<true, false, 128>(a, k, none, lanes, s);
+        else if (lanesPerCta == 4) e = LaunchLabelerG<true, false, 256>(a, k, none, lanes, s);
         else return cudaErrorInvalidValue;
     }
     if (e != cudaSuccess) return e;

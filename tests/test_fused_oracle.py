@@ -81,3 +81,27 @@ def test_uneven_pools_small_configuration_equal_oracle():
     cfg = workloads.small_config()
     emitted, estimated, overflowed = _run(cfg, steps=40)
     assert emitted > 0 and estimated > 0 and overflowed > 0, (emitted, estimated, overflowed)
+
+
+def _varied_kinetics(cfg):
+    """Per-analog pulse widths and inter-pulse distances: the 9-way rows'
+    transition constants then differ within each source group, so the
+    labeler takes its generic rows instead of the grouped ones."""
+    for a, (pw, ipd) in enumerate(zip((0.07, 0.08, 0.09, 0.10), (0.12, 0.14, 0.16, 0.18))):
+        cfg.analogs[a].pulse_width_s = pw
+        cfg.analogs[a].ipd_s = ipd
+    return cfg
+
+
+def _grouped(cfg):
+    import oracle
+    T = oracle.transition_matrix(cfg)
+    rows = T[[0, 5, 6, 7, 8]]
+    return bool((rows[:, 5:9] == rows[:, 5:6]).all() and (rows[:, 9:13] == rows[:, 9:10]).all())
+
+
+def test_uneven_pools_generic_viterbi_rows_equal_oracle():
+    cfg = _varied_kinetics(workloads.small_config())
+    assert _grouped(workloads.small_config()) and not _grouped(cfg)
+    emitted, estimated, overflowed = _run(cfg, steps=40)
+    assert emitted > 0 and estimated > 0, (emitted, estimated, overflowed)

@@ -315,3 +315,16 @@ def test_pool_set_equals_per_pool_analyzers():
                 for z in range(64):
                     assert np.array_equal(q0[l, z, :n[l, z]].view(np.uint8), q1[l, z, :n[l, z]].view(np.uint8))
     assert emitted_any
+
+
+def test_generic_viterbi_rows_bit_exact():
+    """Per-analog kinetics break the equal transition constants within the
+    9-way rows' source groups: the single-pool labeler's generic rows, stage
+    by stage against the oracle."""
+    cfg = workloads.small_config()
+    for a, (pw, ipd) in enumerate(zip((0.07, 0.08, 0.09, 0.10), (0.12, 0.14, 0.16, 0.18))):
+        cfg.analogs[a].pulse_width_s = pw
+        cfg.analogs[a].ipd_s = ipd
+    tr = synth.traces(4, 512 * 8, seed=3)
+    stages = _lockstep(cfg, tr, 512)
+    assert {"labels", "pulses"} <= stages
