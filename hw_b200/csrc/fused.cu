@@ -217,6 +217,11 @@ struct hw_fused
     cudaStream_t side = nullptr;
     cudaEvent_t evFork = nullptr, evHist = nullptr, evInit = nullptr, evJoin = nullptr;
     int overlapMode = 1;              // hw_fused_set_overlap
+    // learned EM start (hw_fused_set_learned_init), not owned: the proposal
+    // of each estimating pool is written to lProp [lane][15][64] before the DME
+    hw_learned_init* net = nullptr;
+    float* lProp = nullptr;
+    std::vector<int> dmePools;        // pools that run the DME this step
     std::map<std::vector<int64_t>, cudaGraphExec_t> graphCache;
     std::map<std::vector<int64_t>, int> planSeen;
     uint32_t lastLaunches = 0, lastGraphLaunches = 0;
@@ -267,7 +272,7 @@ struct hw_fused
         void* bufs[] = {st16, st32, stats, acc, hist, edgePrev, edgeBits, models, diag, dmeScratch, latModel,
                         latLabel, latRoi, latTrc, prevLat, tb, bls, labels, latent, score, paStats, segStart,
                         segFirst, segLast, segMax, segTotal, segM2, segLabel, err, dPoolOf, dFrameOff, dSteps,
-                        dLists, hfState, hfLeft, hfRight, hfFeature, hfThr, hfValue};
+                        dLists, hfState, hfLeft, hfRight, hfFeature, hfThr, hfValue, lProp};
         for (void* p : bufs) cudaFree(p);
     }
 
@@ -280,6 +285,7 @@ struct hw_fused
 int hw_fused::Schedule(hw_pool_chunk* table, int b, int32_t counts[kNumLists], int maxFList[kNumLists])
 {
     for (int s = 0; s < kNumLists; ++s) { counts[s] = 0; maxFList[s] = 0; }
+    dmePools.clear();
     int32_t* lists = hLists[b];
     const int minFrames = (int)cfg.min_frames_for_estimate;
     for (size_t p = 0; p < pools.size(); ++p)
@@ -327,6 +333,7 @@ int hw_fused::Schedule(hw_pool_chunk* table, int b, int32_t counts[kNumLists], i
                     st.tModel = Center(P.modelFi);
                     st.tEst = Center(P.histFi);
                     append(L_DME);
+                    dmePools.push_back((int)p);
                     P.diagValid = true;
                     P.modelFi = P.histFi;
                 }
@@ -465,6 +472,20 @@ int hw_fused::Launch(cudaStream_t s, const int32_t counts[kNumLists], const int 
         DmeArgs a{hist, acc, models, diag, dmeScratch, err, L, 0, 0};
         a.map = map(L_DME);
         const size_t t = Begin(HW_STAGE_DME, st);
+        if (net)
+        {
+            // the network's proposal for each estimating pool's lanes (the
+            // DME reads it by engine lane), then the learned-start estimate
+            for (int p : dmePools)
+            {
+                const PoolRt& P = pools[p];
+                const int prc = hw_learned_init_propose(net, P.lanes, hist + P.lane0, acc + P.lane0,
+                                                        lProp + (size_t)P.lane0 * 15 * kLane, st);
+                if (prc) return prc;
+                ++n;
+            }
+            a.proposal = lProp;
+        }
         HWF_CUDA(LaunchDmeEstimate(a, k, st), "hw_chunk_fused: DME");
         End(t, st);
         ++n;
@@ -896,6 +917,10 @@ int hw_chunk_fused(hw_fused* f, hw_pool_chunk* table, uint32_t n_pools, void* st
             key.push_back(counts[l]);
             key.push_back(maxFList[l]);
         }
+        // the learned start's proposal launches cover the estimating pools'
+        // lane ranges: a plan is also which pools those are
+        if (f->net)
+            for (int p : f->dmePools) key.push_back(-1 - (int64_t)p);
         auto it = f->graphCache.find(key);
         if (it == f->graphCache.end() && ++f->planSeen[key] >= 2)
         {
@@ -929,6 +954,24 @@ int hw_chunk_fused(hw_fused* f, hw_pool_chunk* table, uint32_t n_pools, void* st
     f->lastLaunches = launches + 2;     // + the table and failure-word kernels
     f->lastGraphLaunches = graphLaunches;
     ++f->step;
+    return HW_OK;
+}
+
+int hw_fused_set_learned_init(hw_fused* f, hw_learned_init* net)
+{
+    if (!f) return Fail(HW_ERR_INVALID_ARG, "NULL engine");
+    if (net && !f->lProp)
+    {
+        const int rc = Alloc(&f->lProp, (size_t)f->lanes * 15 * kLane, "hw_fused_set_learned_init");
+        if (rc) return rc;
+    }
+    if (net != f->net)
+    {
+        for (auto& g : f->graphCache) cudaGraphExecDestroy(g.second);
+        f->graphCache.clear();
+        f->planSeen.clear();
+    }
+    f->net = net;
     return HW_OK;
 }
 

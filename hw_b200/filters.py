@@ -431,6 +431,12 @@ class FusedEngine(_Handle):
         labeling, 2 also the histogram."""
         check(lib().hw_fused_set_overlap(self._h, int(mode)))
 
+    def set_learned_init(self, net):
+        """Start every estimate from `net`'s proposal (a learned_init.Network,
+        kept alive by the engine), or the reference start (None)."""
+        check(lib().hw_fused_set_learned_init(self._h, None if net is None else net._h))
+        self._net = net
+
     def enable_hf_metrics(self, frames_per_block=4096, frame_rate=100.0, realtime_activity_labels=True, cart=None):
         """Adds the HF metrics filter; pool p's block metrics land in
         self.metrics[p] on steps where metrics_emitted()[p] is set."""

@@ -76,6 +76,7 @@ def lib():
         "hw_fused_destroy": ([vp], C.c_int),
         "hw_chunk_fused": ([vp, vp, u32, vp], C.c_int),
         "hw_fused_set_overlap": ([vp, i32], C.c_int),
+        "hw_fused_set_learned_init": ([vp, vp], C.c_int),
         "hw_fused_finish": ([vp, vp], C.c_int),
         "hw_fused_use_graphs": ([vp, i32], C.c_int),
         "hw_fused_set_tuning": ([vp, vp, u32], C.c_int),

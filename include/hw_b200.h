@@ -943,6 +943,12 @@ int hw_chunk_fused(hw_fused* f, hw_pool_chunk* table, uint32_t n_pools, void* st
  * statistics merge and histogram beside the labeling (measured on the chip
  * workload: 2% slower for a 16,384-lane engine, within 1% for 4096 lanes). */
 int hw_fused_set_overlap(hw_fused* f, int32_t mode);
+/* Starts every estimate of the engine's pools from net's proposal, as
+ * hw_analyzer_set_learned_init does for one pool (per ZMW the proposal is
+ * kept unless its log-likelihood is below the reference start's); NULL
+ * restores the reference start.  net is not owned and must outlive the
+ * steps that use it; engines on different streams may share one. */
+int hw_fused_set_learned_init(hw_fused* f, hw_learned_init* net);
 /* Waits for the enqueued steps and returns any failure they reported. */
 int hw_fused_finish(hw_fused* f, void* stream);
 int hw_fused_use_graphs(hw_fused* f, int32_t enable);

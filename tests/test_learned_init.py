@@ -232,3 +232,54 @@ def test_analyzers_on_streams_with_learned_start_equal_serial():
         assert fi0 == fi1 and torch.equal(m0, m1), p
     assert estimated >= pools and emitted > 0
     net2.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("graphs", [False, True])
+def test_fused_engine_with_learned_start_equals_analyzers(graphs):
+    """hw_fused_set_learned_init: pools of uneven sizes and chunk lengths in
+    one engine, every estimate from the network's proposal, give the results
+    of one analyzer per pool with the same network (graphs replay the plans of
+    the steps, which include the estimating pools); the models differ from
+    those of the reference start."""
+    import torch
+    from hw_b200 import abi, filters as Fl, learned_init as L, workloads
+    cfg = workloads.small_config()
+    cfg.model_estimation_mode = abi.DYNAMIC_ESTIMATIONS
+    net, _ = L.run(train_pools=1, eval_pools=1, lanes=256, fit_iters=200, epochs=5, batch=1024, seed=2)
+    lanes, frames, ids = [24, 40, 16], [512, 256, 512], [1, 4, 7]
+    eng = Fl.FusedEngine(cfg, lanes, frames, pool_ids=ids, graphs=graphs)
+    eng.set_learned_init(net)
+    plain = Fl.FusedEngine(cfg, lanes, frames, pool_ids=ids)
+    ans = [Fl.BatchAnalyzer(cfg, i, n, F) for i, n, F in zip(ids, lanes, frames)]
+    for a in ans:
+        a.set_learned_init(net)
+    gens = [Fl.TraceGenerator(n, workload=2, zmw_offset=1000 * p) for p, n in enumerate(lanes)]
+    estimated = emitted = 0
+    for step in range(28):
+        chunks = [g.next(step * F, F) for g, F in zip(gens, frames)]
+        em, est = eng.process(chunks)
+        plain.process(chunks)
+        for p, (an, n) in enumerate(zip(ans, lanes)):
+            pulses, lens, ovf, e1, s1 = an(chunks[p], step * frames[p])
+            assert (bool(em[p]), bool(est[p])) == (e1, s1), (step, p)
+            pp, pl, po = eng.outputs(p)
+            assert torch.equal(pl, lens) and torch.equal(po, ovf), (step, p)
+            if e1:
+                emitted += 1
+                q0 = Fl.struct_to_numpy(pulses, abi.PULSE_DT).reshape(n * 64, cfg.max_calls_per_zmw)
+                q1 = Fl.struct_to_numpy(pp, abi.PULSE_DT).reshape(n * 64, cfg.max_calls_per_zmw)
+                cnt = np.minimum(lens.cpu().numpy().reshape(-1), cfg.max_calls_per_zmw)
+                for z in range(n * 64):
+                    assert np.array_equal(q0[z, :cnt[z]].view(np.uint8), q1[z, :cnt[z]].view(np.uint8)), (step, p, z)
+            estimated += int(s1)
+    eng.finish()
+    plain.finish()
+    differs = False
+    for p, an in enumerate(ans):
+        m0, fi0 = an.models()
+        m1, fi1 = eng.models(p)
+        assert fi0 == fi1 and torch.equal(m0, m1), p
+        m2, _ = plain.models(p)
+        differs |= not torch.equal(m1, m2)
+    assert estimated >= 3 and emitted > 0 and differs
