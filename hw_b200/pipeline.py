@@ -1,6 +1,7 @@
 """The whole basecaller path on one B200 at chip size: sensor packets ->
 ingest repacking -> the trace-analysis chain with HF metrics (one fused
-engine over 4 pools of 4096 lanes, 512-frame chunks, reference defaults) ->
+engine over 4 pools of 4096 lanes, 512-frame chunks, reference defaults;
+--streams N: one engine per pool on N streams) ->
 BAZ encoding with the preliminary HQ stage (one per pool: production
 encoding, 8-chunk metric blocks, the reference's defaults: lookback 10,
 preliminary HQ off, so every ZMW is HQ from the first block) ->
@@ -14,7 +15,7 @@ The run first streams the start-up chunks, then times K steps (CUDA events
 on the stream and the host clock around them) and reports ZMW-frames/s for
 the whole path, the share of each part, and the checkpoint bytes.
 
-    python -m hw_b200.pipeline [--steps 24] [--warmup-steps 40]
+    python -m hw_b200.pipeline [--steps 24] [--warmup-steps 40] [--streams 1]
 """
 import argparse
 import json
@@ -38,9 +39,12 @@ def packets_from_traces(tr):
     return tr.view(lanes // 2, 2, F, 64).permute(0, 2, 1, 3).contiguous().view(torch.uint8).reshape(-1)
 
 
-def run(steps=24, warmup_steps=40, n_inputs=8, pools=POOLS, lanes=LANES, cfg=None, collect=None):
+def run(steps=24, warmup_steps=40, n_inputs=8, pools=POOLS, lanes=LANES, cfg=None, collect=None, streams=1):
     """collect: a list that receives (step, pool, checkpoint copy) for every
-    checkpoint (tests)."""
+    checkpoint (tests).  streams > 1: one fused engine per pool, pool p's
+    analysis and BAZ / preliminary HQ stage on stream p mod streams (one
+    pool's DME shares the GPU with the other pools' stages); 1: one fused
+    engine over every pool on one stream."""
     POOLS, LANES = pools, lanes
     cfg = workloads.chip_config() if cfg is None else cfg
     nz = POOLS * LANES * 64
@@ -53,9 +57,14 @@ def run(steps=24, warmup_steps=40, n_inputs=8, pools=POOLS, lanes=LANES, cfg=Non
     del gen
     rp = Fl.Repacker(nz, LANES, F)
     chunks = rp.new_chunks()
-    eng = Fl.FusedEngine(cfg, [LANES] * POOLS, [F] * POOLS, tuning="auto")
+    S = max(1, min(streams, POOLS))
     cart = dict(np.load(os.path.join(ROOT, "hw_b200", "data", "trained_cart.npz")))
-    eng.enable_hf_metrics(4096, cfg.frame_rate, True, cart)
+    groups = [list(range(POOLS))] if S == 1 else [[p] for p in range(POOLS)]
+    units = []
+    for g in groups:
+        e = Fl.FusedEngine(cfg, [LANES] * len(g), [F] * len(g), pool_ids=g, tuning="auto")
+        e.enable_hf_metrics(4096, cfg.frame_rate, True, cart)
+        units.append((e, g))
     hq = [Fl.PrelimHq(LANES * 64, chunks_per_block=8, lookback=10, enable=False) for _ in range(POOLS)]
     # each pool's checkpoints land in its own pinned buffer, copied on a side
     # stream that overlaps the next steps' analysis
@@ -63,8 +72,9 @@ def run(steps=24, warmup_steps=40, n_inputs=8, pools=POOLS, lanes=LANES, cfg=Non
     copy_stream = torch.cuda.Stream()
     copied = [None] * POOLS
     s = torch.cuda.current_stream()
+    side = [torch.cuda.Stream() for _ in range(S - 1)]
     ev = {k: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for k in ("repack", "chain", "hq")}
+          for k in ("repack", "analysis")}
     acc = {k: 0.0 for k in ev}
     ck_bytes, ck_count = 0, 0
 
@@ -79,38 +89,42 @@ def run(steps=24, warmup_steps=40, n_inputs=8, pools=POOLS, lanes=LANES, cfg=Non
         rp(tab, packets[c % n_inputs], first, chunks)
         if timed:
             ev["repack"][1].record(s)
-            ev["chain"][0].record(s)
-        emitted, _ = eng.process(chunks)
-        m_em = eng.metrics_emitted()
+            ev["analysis"][0].record(s)
+        for s_ in side:
+            s_.wait_stream(s)
+        for u, (eng, g) in enumerate(units):
+            su = s if u % S == 0 else side[u % S - 1]
+            with torch.cuda.stream(su):
+                emitted, _ = eng.process([chunks[p] for p in g])
+                m_em = eng.metrics_emitted()
+                for i, p in enumerate(g):
+                    if not emitted[i]:
+                        continue
+                    pulses, lens, _ = eng.outputs(i)
+                    out = hq[p].process(pulses, lens, cfg.max_calls_per_zmw,
+                                        metrics=eng.metrics[i] if m_em[i] else None)
+                    if out is not None and collect is not None:
+                        collect.append((c, p, {k: (v.clone() if torch.is_tensor(v) else v) for k, v in out.items()}))
+                    if out is not None:
+                        n = out["bytes"].numel()
+                        if copied[p] is not None:
+                            copied[p].synchronize()   # the pool's previous checkpoint is out
+                        if n > host[p].numel():
+                            host[p] = torch.empty(n + n // 4, dtype=torch.uint8, pin_memory=True)
+                        ready = torch.cuda.Event()
+                        ready.record(su)
+                        with torch.cuda.stream(copy_stream):
+                            copy_stream.wait_event(ready)
+                            host[p][:n].copy_(out["bytes"], non_blocking=True)
+                            copied[p] = torch.cuda.Event()
+                            copied[p].record(copy_stream)
+                        if timed:
+                            ck_bytes += n
+                            ck_count += 1
+        for s_ in side:
+            s.wait_stream(s_)
         if timed:
-            ev["chain"][1].record(s)
-            ev["hq"][0].record(s)
-        for p in range(POOLS):
-            if not emitted[p]:
-                continue
-            pulses, lens, _ = eng.outputs(p)
-            out = hq[p].process(pulses, lens, cfg.max_calls_per_zmw,
-                                metrics=eng.metrics[p] if m_em[p] else None)
-            if out is not None and collect is not None:
-                collect.append((c, p, {k: (v.clone() if torch.is_tensor(v) else v) for k, v in out.items()}))
-            if out is not None:
-                n = out["bytes"].numel()
-                if copied[p] is not None:
-                    copied[p].synchronize()   # the pool's previous checkpoint is out
-                if n > host[p].numel():
-                    host[p] = torch.empty(n + n // 4, dtype=torch.uint8, pin_memory=True)
-                ready = torch.cuda.Event()
-                ready.record(s)
-                with torch.cuda.stream(copy_stream):
-                    copy_stream.wait_event(ready)
-                    host[p][:n].copy_(out["bytes"], non_blocking=True)
-                    copied[p] = torch.cuda.Event()
-                    copied[p].record(copy_stream)
-                if timed:
-                    ck_bytes += n
-                    ck_count += 1
-        if timed:
-            ev["hq"][1].record(s)
+            ev["analysis"][1].record(s)
 
     for c in range(warmup_steps):
         step(c, False)
@@ -129,9 +143,13 @@ def run(steps=24, warmup_steps=40, n_inputs=8, pools=POOLS, lanes=LANES, cfg=Non
     wall = time.perf_counter() - t0
     ms = e0.elapsed_time(e1)
     zf = nz * F * steps
+    for e, _ in units:
+        e.finish()
+        e.close()
     return {"workload": f"sensor packets -> repacking -> chain with HF metrics ({POOLS} pools x {LANES} lanes, "
-                        f"{F}-frame chunks, fused engine) -> BAZ encoding + preliminary HQ (per pool) -> "
-                        f"checkpoints to pinned host memory; {steps} steps after {warmup_steps}",
+                        f"{F}-frame chunks, {len(units)} fused engine(s) on {S} stream(s)) -> BAZ encoding + "
+                        f"preliminary HQ (per pool) -> checkpoints to pinned host memory; {steps} steps after "
+                        f"{warmup_steps}",
             "zmw_frames_per_s": zf / (ms / 1e3), "zmw_frames_per_s_host_clock": zf / wall,
             "ms_per_step": ms / steps,
             "ms_per_step_by_part": {k: v / steps for k, v in acc.items()},
@@ -142,8 +160,9 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--steps", type=int, default=24)
     ap.add_argument("--warmup-steps", type=int, default=40)
+    ap.add_argument("--streams", type=int, default=1, help="one engine per pool on this many streams (1: one engine)")
     a = ap.parse_args()
-    print(json.dumps(run(a.steps, a.warmup_steps)))
+    print(json.dumps(run(a.steps, a.warmup_steps, streams=a.streams)))
 
 
 if __name__ == "__main__":

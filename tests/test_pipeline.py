@@ -9,14 +9,18 @@ from hw_b200 import abi
 
 
 @pytest.mark.gpu
-def test_pipeline_checkpoints_equal_stage_by_stage():
+@pytest.mark.parametrize("streams", [1, 2])
+def test_pipeline_checkpoints_equal_stage_by_stage(streams):
+    """streams = 1: one engine over both pools; 2: an engine per pool, each on
+    its own stream with its pool's BAZ / preliminary HQ stage."""
     import torch
     import oracle
     from hw_b200 import filters as Fl, pipeline, workloads
     cfg = workloads.small_config()
     pools, lanes, F, n_inputs = 2, 32, pipeline.F, 8
     got = []
-    pipeline.run(steps=16, warmup_steps=8, n_inputs=n_inputs, pools=pools, lanes=lanes, cfg=cfg, collect=got)
+    pipeline.run(steps=16, warmup_steps=8, n_inputs=n_inputs, pools=pools, lanes=lanes, cfg=cfg, collect=got,
+                 streams=streams)
     assert len(got) >= 2 * pools
     # the same traces: the generator's first n_inputs chunks, used in turn
     gen = Fl.TraceGenerator(pools * lanes, workload=1)
