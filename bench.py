@@ -79,6 +79,8 @@ def parse():
     ap.add_argument("--groups", type=int, default=4,
                     help="fused engines the pools are split over (pool groups; both legs, and the end-to-end "
                          "leg pipelines its copies over them)")
+    ap.add_argument("--split", type=int, default=1,
+                    help="engines each pool's lanes are split over (same pool id, so the same schedule)")
     ap.add_argument("--streams", type=int, default=4,
                     help="streams the group engines run on (group u on stream u mod n)")
     ap.add_argument("--e2e-download", choices=["packed", "slots"], default="packed",
@@ -418,30 +420,36 @@ def main():
         # the reference's trained activity classifier).  The engines run on
         # NS streams, so one group's DME (a latency-bound launch) shares the
         # GPU with other groups' stages.
-        G = max(1, min(args.groups, args.pools))
-        if args.pools % G:
+        # With --split S each pool's lanes form S sub-pools of lpp / S lanes
+        # that keep the pool's id (lanes are independent, and the schedule
+        # depends on the id only); below, "pools" of an engine are sub-pools.
+        SP = max(1, args.split) if lpp % max(1, args.split) == 0 else 1
+        ul = lpp // SP
+        nsub = args.pools * SP
+        G = max(1, min(args.groups * SP, nsub))
+        if nsub % G:
             G = 1
-        ppg = args.pools // G
+        ppg = nsub // G
         NS = max(1, min(args.streams, G))
         cart = dict(np.load(os.path.join(ROOT, "hw_b200", "data", "trained_cart.npz")))
         engines = []
         for g in range(G):
             ids = list(range(g * ppg, (g + 1) * ppg))
-            eg = Fl.FusedEngine(cfg, [lpp] * ppg, [FRAMES] * ppg, pool_ids=ids)
+            eg = Fl.FusedEngine(cfg, [ul] * ppg, [FRAMES] * ppg, pool_ids=[i // SP for i in ids])
             eg.set_overlap(args.overlap)
             eg.enable_hf_metrics(4096, cfg.frame_rate, True, cart)
             engines.append((eg, ids))
         s_comp = [stream] + [torch.cuda.Stream() for _ in range(NS - 1)]
         profiled = [eg for eg, _ in engines]
-        outputs = [engines[p // ppg][0].outputs(p % ppg) for p in range(args.pools)]
+        outputs = [engines[p // ppg][0].outputs(p % ppg) for p in range(nsub)]
         pool_metrics = [eg.metrics[i] for eg, ids in engines for i in range(len(ids))]
 
         def run_units(chunk, outs=None):
             for u, (eg, ids) in enumerate(engines):
                 with torch.cuda.stream(stream if serial[0] else s_comp[u % NS]):
-                    eg.process([chunk[p * lpp:(p + 1) * lpp] for p in ids], outs[u] if outs else None)
+                    eg.process([chunk[p * ul:(p + 1) * ul] for p in ids], outs[u] if outs else None)
     else:
-        G, NS, s_comp = args.pools, 1, [stream]
+        G, NS, s_comp, ul, SP = args.pools, 1, [stream], lpp, 1
         analyzers = [Fl.BatchAnalyzer(cfg, p, lpp, FRAMES) for p in range(args.pools)]
         profiled = analyzers
         outputs = [(a.pulses, a.lens, a.ovf) for a in analyzers]
@@ -573,7 +581,7 @@ def main():
         def run_unit(u, chunk_slice, outs):
             eg, ids = units[u]
             if args.engine == "fused":
-                eg.process([chunk_slice[i * lpp:(i + 1) * lpp] for i in range(len(ids))], outs)
+                eg.process([chunk_slice[i * ul:(i + 1) * ul] for i in range(len(ids))], outs)
             else:
                 eg(chunk_slice, (c + k) * FRAMES, *outs[0])
 
@@ -587,7 +595,7 @@ def main():
         del tmp
         U = len(units)
         NB = max(2, args.e2e_buffers)    # input and output buffers per group: copies may run NB - 1 steps ahead
-        rows = [(units[u][1][0] * lpp, (units[u][1][-1] + 1) * lpp) for u in range(U)]
+        rows = [(units[u][1][0] * ul, (units[u][1][-1] + 1) * ul) for u in range(U)]
         in_dev = [[torch.empty((r1 - r0, FRAMES, 64), dtype=torch.int16, device="cuda") for r0, r1 in rows]
                   for _ in range(NB)]
         out_dev = [[[(torch.empty_like(outputs[p][0]), torch.empty_like(outputs[p][1]),
@@ -718,7 +726,7 @@ def main():
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / KE, "steps": KE,
                "phase": "same K steps of the estimation cycle as value", "timeline": timeline,
                "overlap": f"copies on their own streams, {NB} buffers deep against the analysis, pipelined over "
-                          f"{U} pool group(s) of {ppg * lpp} lanes (one engine each, on {NS} stream(s)); a step's "
+                          f"{U} pool group(s) of {ppg * ul} lanes (one engine each, on {NS} stream(s)); a step's "
                           f"first upload and last download cover one group",
                "download": ("the valid pulse records, packed by hw_pulses_compact, with every ZMW's pulse and "
                             "overflow counts and the HF metrics blocks" if packed else
@@ -822,8 +830,9 @@ def main():
             "config": {"workload": WORKLOAD,
                        "zmws_per_gpu": zmws, "frames_per_chunk": FRAMES, "pools": args.pools,
                        "startup_chunks": n_start, "inputs": "1 GiB chunk per step, larger than L2",
-                       "engine": (f"hw_chunk_fused: {G} engine(s) of {ppg} pool(s) (one launch per stage over an "
-                                  f"engine's pools) on {NS} stream(s)" if args.engine == "fused"
+                       "engine": (f"hw_chunk_fused: {G} engine(s) of {ppg} pool(s) of {ul} lanes (one launch per "
+                                  f"stage over an engine's pools{'; each pool split over %d engines' % SP if SP > 1 else ''}) "
+                                  f"on {NS} stream(s)" if args.engine == "fused"
                                   else "one hw_analyzer per pool")},
             "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
             "clocks": clk,
