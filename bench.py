@@ -719,12 +719,28 @@ def main():
         timeline = {"first_step_done_ms": marks[0],
                     "step_ms_after_first": [b_ - a_ for a_, b_ in zip(marks, marks[1:])],
                     "last_download_ms": ms_e2e - marks[-1]}
+        # untimed check: the host holds the last step's results (counts, and
+        # the packed records or every slot) as they are on the device
+        bl = (KE - 1) % NB
+        verified = True
+        for u in range(U):
+            for j, p in enumerate(units[u][1]):
+                dp, dl, do = out_dev[bl][u][j]
+                hp, hl, ho = host_out[p]
+                verified &= torch.equal(hl, dl.cpu()) and torch.equal(ho, do.cpu())
+                if packed:
+                    co, off = packed_dev[bl][u][j]
+                    nb_ = int(off[-1].item()) * rec_bytes
+                    verified &= torch.equal(hp[:nb_], co.view(-1)[:nb_].cpu())
+                else:
+                    verified &= torch.equal(hp, dp.cpu())
         c += KE
         h2d = total_lanes * FRAMES * 64 * 2
         d2h = (record_bytes + metrics_bytes) // KE + sum(dl.numel() * 4 + do.numel() * 4 for _, dl, do in outputs)
         e2e = {"value": zf_step * KE * world / (ms_e2e / 1e3), "unit": "ZMW-frames/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e / KE, "steps": KE,
                "phase": "same K steps of the estimation cycle as value", "timeline": timeline,
+               "verified": bool(verified),
                "overlap": f"copies on their own streams, {NB} buffers deep against the analysis, pipelined over "
                           f"{U} pool group(s) of {ppg * ul} lanes (one engine each, on {NS} stream(s)); a step's "
                           f"first upload and last download cover one group",
