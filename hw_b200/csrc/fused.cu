@@ -1008,6 +1008,18 @@ int hw_fused_models(const hw_fused* f, uint32_t pool, hw_lane_model* d_out, hw_f
     return HW_OK;
 }
 
+int hw_fused_last_diag(const hw_fused* f, uint32_t pool, hw_dme_diag* d_out, int32_t* valid, void* stream)
+{
+    if (!f || !d_out || pool >= f->pools.size()) return Fail(HW_ERR_INVALID_ARG, "bad argument");
+    const PoolRt& P = f->pools[pool];
+    if (valid) *valid = P.diagValid ? 1 : 0;
+    if (!P.diagValid) return HW_OK;
+    HWF_CUDA(cudaMemcpyAsync(d_out, f->diag + P.lane0, sizeof(hw_dme_diag) * P.lanes, cudaMemcpyDeviceToDevice,
+                             reinterpret_cast<cudaStream_t>(stream)),
+             "hw_fused_last_diag");
+    return HW_OK;
+}
+
 int hw_fused_profile(hw_fused* f, int32_t enable)
 {
     if (!f) return Fail(HW_ERR_INVALID_ARG, "NULL engine");

@@ -492,6 +492,13 @@ class FusedEngine(_Handle):
         """(pulses, lens, overflows) of pool p's last step."""
         return self.pulses[p], self.lens[p], self.ovf[p]
 
+    def last_diag(self, p):
+        """Pool p's DME diagnostics of its latest estimate (None before it)."""
+        out = struct_buffer(abi.DME_DIAG_DT, int(self.lanes[p]))
+        valid = C.c_int32()
+        check(lib().hw_fused_last_diag(self._h, int(p), _p(out), C.byref(valid), _stream()))
+        return out if valid.value else None
+
     def models(self, p):
         out = struct_buffer(abi.LANE_MODEL_DT, int(self.lanes[p]))
         fi = abi.FrameInterval()

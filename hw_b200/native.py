@@ -81,6 +81,7 @@ def lib():
         "hw_fused_use_graphs": ([vp, i32], C.c_int),
         "hw_fused_set_tuning": ([vp, vp, u32], C.c_int),
         "hw_fused_models": ([vp, u32, vp, C.POINTER(FI), vp], C.c_int),
+        "hw_fused_last_diag": ([vp, u32, vp, C.POINTER(i32), vp], C.c_int),
         "hw_fused_last_step": ([vp, C.POINTER(u32), C.POINTER(u32)], C.c_int),
         "hw_fused_profile": ([vp, i32], C.c_int),
         "hw_repacker_create": ([u32, u32, u32, i32, PPV], C.c_int),

@@ -28,17 +28,21 @@ FRAMES = 512
 FRAME_RATE = 100.0
 
 
-def run_chain(cfg, pools, lpp, chunks, net=None, streams=1):
+def run_chain(cfg, pools, lpp, chunks, net=None, streams=1, engine="analyzers"):
     """One streaming run.  With streams > 1 the pools' analyzers are dealt
     round-robin over that many streams (each with its own copy of the
     learned start's network: a network handle holds its forward pass's
     scratch) and run at once; the stage timers, which time the stream they
     run on, stay off, and only the DME's total is taken from its diagnostics
-    (lane iterations).  With one stream every stage is timed."""
+    (lane iterations).  With one stream every stage is timed.  engine:
+    "analyzers" (one hw_analyzer per pool) or "fused" (one one-pool
+    hw_chunk_fused engine per pool)."""
     from . import learned_init
     total = pools * lpp
     gen = Fl.TraceGenerator(total, workload=4)
-    analyzers = [Fl.BatchAnalyzer(cfg, p, lpp, FRAMES) for p in range(pools)]
+    fused = engine == "fused"
+    analyzers = ([Fl.FusedEngine(cfg, [lpp], [FRAMES], pool_ids=[p]) for p in range(pools)] if fused
+                 else [Fl.BatchAnalyzer(cfg, p, lpp, FRAMES) for p in range(pools)])
     stream = torch.cuda.current_stream()
     S = max(1, min(streams, pools))
     side = [torch.cuda.Stream() for _ in range(S - 1)]
@@ -66,7 +70,11 @@ def run_chain(cfg, pools, lpp, chunks, net=None, streams=1):
         flags = []
         for p, a in enumerate(analyzers):
             with torch.cuda.stream(stream if p % S == 0 else side[p % S - 1]):
-                flags.append(a(buf[p * lpp:(p + 1) * lpp], c * FRAMES))
+                if fused:
+                    em, est = a.process([buf[p * lpp:(p + 1) * lpp]])
+                    flags.append((None, None, None, bool(em[0]), bool(est[0])))
+                else:
+                    flags.append(a(buf[p * lpp:(p + 1) * lpp], c * FRAMES))
         for s_ in side:
             stream.wait_stream(s_)
         ev[2].record(stream)
@@ -77,7 +85,7 @@ def run_chain(cfg, pools, lpp, chunks, net=None, streams=1):
             emitted += int(em)
             if est:
                 estimates += 1
-                d = Fl.struct_to_numpy(a.last_diag(), abi.DME_DIAG_DT)
+                d = Fl.struct_to_numpy(a.last_diag(0) if fused else a.last_diag(), abi.DME_DIAG_DT)
                 lane_iters.append(d["lane_iterations"].astype(np.float64))
     stage = {}
     for a in analyzers:
@@ -86,6 +94,8 @@ def run_chain(cfg, pools, lpp, chunks, net=None, streams=1):
                 s = stage.setdefault(k, [0.0, 0])
                 s[0] += t
                 s[1] += n
+        if fused:
+            a.finish()
         a.close()
     for n in nets[1:]:
         n.close()
@@ -99,6 +109,7 @@ def run_chain(cfg, pools, lpp, chunks, net=None, streams=1):
         "analysis_ms_per_chunk": ana_ms / chunks,
         "generation_ms_per_chunk": gen_ms / chunks,
         "streams": S,
+        "engine": engine,
         "estimates": estimates,
         "em_lane_iterations_mean": float(it.mean()),
         "emitting_pool_chunks": emitted,
@@ -116,6 +127,8 @@ def main():
     ap.add_argument("--chunks", type=int, default=128)
     ap.add_argument("--weights", default=None, help="trained learned-initializer weights (npz)")
     ap.add_argument("--streams", type=int, default=1, help="streams the pools' analyzers run on")
+    ap.add_argument("--engine", choices=["analyzers", "fused"], default="analyzers",
+                    help="one hw_analyzer per pool, or one one-pool fused engine per pool")
     a = ap.parse_args()
     from . import learned_init
     cfg = workloads.chip_config()
@@ -130,8 +143,8 @@ def main():
     inf = learned_init.Network(max_batch=a.lanes_per_pool * abi.LANE)
     inf.set(*net.get())
     net.close()
-    plain = run_chain(cfg, a.pools, a.lanes_per_pool, a.chunks, streams=a.streams)
-    learned = run_chain(cfg, a.pools, a.lanes_per_pool, a.chunks, inf, streams=a.streams)
+    plain = run_chain(cfg, a.pools, a.lanes_per_pool, a.chunks, streams=a.streams, engine=a.engine)
+    learned = run_chain(cfg, a.pools, a.lanes_per_pool, a.chunks, inf, streams=a.streams, engine=a.engine)
     out = {"workload": f"streaming: {a.pools * a.lanes_per_pool * abi.LANE} ZMWs x {a.chunks} chunks of {FRAMES} "
                        "frames, generated on the GPU (decay 20%, +15 DN step in 1% of ZMWs), dynamic DME",
            "plain_em": plain, "learned_init": learned}

@@ -957,6 +957,9 @@ int hw_fused_use_graphs(hw_fused* f, int32_t enable);
 int hw_fused_set_tuning(hw_fused* f, const hw_fused_tuning* tuning, uint32_t n);
 /* Device copy of pool p's current models and their frame interval. */
 int hw_fused_models(const hw_fused* f, uint32_t pool, hw_lane_model* d_out, hw_frame_interval* fi, void* stream);
+/* Pool `pool`'s diagnostics of its latest estimate ([lanes] hw_dme_diag), as
+ * hw_analyzer_last_diag; *valid = 0 (and nothing copied) before its first. */
+int hw_fused_last_diag(const hw_fused* f, uint32_t pool, hw_dme_diag* d_out, int32_t* valid, void* stream);
 /* Stage timers with the meaning of hw_analyzer_profile / _stage_times (the
  * HW_STAGE_* indices; a fused labeler + pulse kernel counts as the labeler).
  * While profiling, steps are launched kernel by kernel, not from graphs. */

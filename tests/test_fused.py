@@ -215,3 +215,30 @@ def test_fused_hf_metrics_equal_standalone_filter(mode):
                     assert np.array_equal(a[name], b[name], equal_nan=a[name].dtype.kind == "f"), (step, p, name)
     eng.finish()
     assert blocks > 0
+
+
+def test_fused_last_diag_equals_per_pool_analyzers():
+    """hw_fused_last_diag gives each pool's diagnostics of its latest
+    estimate, equal to its per-pool analyzer's; none before the first."""
+    from hw_b200 import filters as Fl
+    cfg = workloads.small_config()
+    cfg.model_estimation_mode = abi.DYNAMIC_ESTIMATIONS
+    lanes, frames, ids = [3, 2], [512, 256], [1, 4]
+    eng = Fl.FusedEngine(cfg, lanes, frames, pool_ids=ids)
+    ans = [Fl.BatchAnalyzer(cfg, i, n, F) for i, n, F in zip(ids, lanes, frames)]
+    gens = [Fl.TraceGenerator(n, workload=2, zmw_offset=1000 * p) for p, n in enumerate(lanes)]
+    assert eng.last_diag(0) is None
+    seen = 0
+    for step in range(24):
+        chunks = [g.next(step * F, F) for g, F in zip(gens, frames)]
+        eng.process(chunks)
+        for p, an in enumerate(ans):
+            an(chunks[p], step * frames[p])
+            d0, d1 = an.last_diag(), eng.last_diag(p)
+            assert (d0 is None) == (d1 is None), (step, p)
+            if d0 is not None:
+                seen += 1
+                assert np.array_equal(Fl.struct_to_numpy(d0, abi.DME_DIAG_DT).view(np.uint8),
+                                      Fl.struct_to_numpy(d1, abi.DME_DIAG_DT).view(np.uint8)), (step, p)
+    eng.finish()
+    assert seen > 0
